@@ -1,0 +1,185 @@
+/*
+ * delta_ray_b200 -- C ABI of the B200-native differentiable edge-sampling path tracer.
+ *
+ * This is the drop-in replacement for the reference renderer's FFI: the
+ * pybind11 module `delta_ray` (delta_ray.cpp:1838-1920) whose one compute entry
+ * point is
+ *     delta_ray.render(Camera, [Shape], [Material], [Light], (W, H), d_image,
+ *                      num_samples, max_bounces, seed, print_progress)
+ *         -> RenderResult                                  (delta_ray.cpp:1017)
+ * The reference decides forward vs backward by the rank of d_image
+ * (delta_ray.cpp:1029); here they are two entry points.  The reference builds
+ * its scene on every call (delta_ray.cpp:1030); here the scene is built once by
+ * dr_scene_create and reused, and dr_scene_update refreshes vertex positions.
+ *
+ * Conventions
+ *  - Plain C types only; every pointer inside a descriptor may be host or
+ *    device memory (CUDA unified addressing tells them apart) unless stated.
+ *  - Matrices are 4x4 row-major float32, exactly the reference's numpy layout.
+ *  - All calls are stream-ordered on the given cudaStream_t (passed as void*,
+ *    NULL = legacy default stream).  Image and gradient outputs are device
+ *    pointers.  A scene must not be used by two calls concurrently.
+ *  - Every call returns a dr_status; on failure dr_last_error() describes it.
+ *    Device-side failures are reported through a status word, never a trap.
+ */
+#ifndef DELTA_RAY_B200_H
+#define DELTA_RAY_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define DR_ABI_VERSION 1
+
+typedef enum {
+    DR_OK = 0,
+    DR_ERR_INVALID_ARGUMENT = 1,
+    DR_ERR_CUDA = 2,
+    DR_ERR_OUT_OF_MEMORY = 3,
+    DR_ERR_DEVICE_STATUS = 4, /* a kernel reported an error word (bounds, queue overflow) */
+    DR_ERR_NOT_SUPPORTED = 5
+} dr_status;
+
+/* Camera (camera.h:12-22 of the reference).  fov_factor = tan(fov / 2),
+ * aspect_ratio = width / height.  Only cam_to_world, fov_factor and
+ * aspect_ratio shape the camera rays (camera.h:49-84); world_to_cam and
+ * clip_near shape edge projection (camera.h:218-242). */
+typedef struct {
+    const float *cam_to_world;  /* [16] */
+    const float *world_to_cam;  /* [16] */
+    const float *sample_to_cam; /* [16] */
+    const float *cam_to_sample; /* [16] */
+    float fov_factor;
+    float aspect_ratio;
+    float clip_near;
+    int fisheye;
+} dr_camera_desc;
+
+/* Material (material.h:14-22).  A channel with tex_w == tex_h == 0 is a
+ * constant ([3] or [1]); otherwise it is a [tex_h][tex_w][c] texture with
+ * bilinear wrap-around lookup (material.h:108-203). */
+typedef struct {
+    const float *diffuse;   /* [3] or [h][w][3] */
+    int diffuse_w, diffuse_h;
+    const float *specular;  /* [3] or [h][w][3] */
+    int specular_w, specular_h;
+    const float *roughness; /* [1] or [h][w][1] */
+    int roughness_w, roughness_h;
+    const float *diffuse_uv_scale;   /* [2] */
+    const float *specular_uv_scale;  /* [2] */
+    const float *roughness_uv_scale; /* [2] */
+    int two_sided;
+} dr_material_desc;
+
+/* Triangle mesh (shape.h:11-18). */
+typedef struct {
+    const float *vertices; /* [num_vertices][3] */
+    int num_vertices;
+    const int *indices;    /* [num_triangles][3] */
+    int num_triangles;
+    const float *uvs;      /* [num_vertices][2] or NULL */
+    const float *normals;  /* [num_vertices][3] or NULL (shading normals) */
+    int material_id;
+} dr_shape_desc;
+
+/* Area light (light.h:15-18): every triangle of shape_id emits intensity. */
+typedef struct {
+    int shape_id;
+    const float *intensity; /* [3] */
+} dr_light_desc;
+
+typedef struct {
+    dr_camera_desc camera;
+    const dr_material_desc *materials;
+    int num_materials;
+    const dr_shape_desc *shapes;
+    int num_shapes;
+    const dr_light_desc *lights;
+    int num_lights;
+    /* Optional Blinn-Phong LTC table, 128*128 row-major 3x3 float32 matrices
+     * indexed [roughness_bin + theta_bin * 128] (ltc.inc:2-4,
+     * material.h:464-476).  NULL selects the table built into the library. */
+    const float *ltc_table;
+} dr_scene_desc;
+
+/* How the per-secondary-point edge position derivative is pushed back
+ * through the path (delta_ray.cpp:976-1002).  The reference *sets* the
+ * adjoint once per edge, so only the last edge of each shading point
+ * survives; DR_DP_SUM adds every edge (the unbiased estimator). */
+typedef enum { DR_DP_REFERENCE_LAST = 0, DR_DP_SUM = 1 } dr_dp_mode;
+
+typedef struct {
+    int width;
+    int height;
+    int spp;          /* samples per pixel (num_samples) */
+    int max_bounces;
+    uint64_t seed;
+    /* Number of primary-edge samples in the backward pass; <= 0 selects
+     * spp * width * height, the reference's total over all its threads
+     * (delta_ray.cpp:1474-1475 with one thread). */
+    int64_t primary_edge_samples;
+    int dp_mode;      /* dr_dp_mode */
+    int reserved[8];  /* must be zero */
+} dr_render_desc;
+
+/* Gradient layout: one flat float32 buffer, in this order
+ *   d_cam_to_world[16] d_world_to_cam[16] d_sample_to_cam[16] d_cam_to_sample[16]
+ *   for each material: d_diffuse (3 or h*w*3), d_specular (3 or h*w*3),
+ *                      d_roughness (1 or h*w)
+ *   for each shape:    d_vertices (3V), then d_normals (3V) when the shape has normals
+ *   for each light:    d_intensity (3)
+ * (the fields of RenderResult / DCamera / DMaterial / DShape / DLight,
+ * delta_ray.cpp:1007-1015).  dr_scene_grad_layout reports the offsets. */
+typedef struct {
+    size_t total;                 /* floats in the flat buffer */
+    size_t camera;                /* offset of d_cam_to_world; the other 3 follow */
+    const size_t *material;       /* [num_materials * 3]: diffuse, specular, roughness */
+    const size_t *shape_vertices; /* [num_shapes] */
+    const size_t *shape_normals;  /* [num_shapes], (size_t)-1 when absent */
+    const size_t *light;          /* [num_lights] */
+} dr_grad_layout;
+
+typedef struct dr_scene dr_scene;
+
+/* Library/ABI version; lets a binding check what it loaded. */
+int dr_abi_version(void);
+
+/* Builds the device scene: geometry, LBVH, light samplers, edge list,
+ * primary-edge sampler and edge trees (scene.cpp:19-136). */
+dr_status dr_scene_create(const dr_scene_desc *desc, int device, dr_scene **out);
+
+/* Replaces vertex positions (same topology) and rebuilds what depends on
+ * them; `desc` must describe the same meshes as at creation. */
+dr_status dr_scene_update(dr_scene *scene, const dr_scene_desc *desc);
+
+dr_status dr_scene_destroy(dr_scene *scene);
+
+dr_status dr_scene_grad_layout(const dr_scene *scene, dr_grad_layout *layout);
+
+/* Forward render: image [H][W][3] float32 (device), the mean over spp
+ * samples of each pixel (delta_ray.cpp:1190-1333, render_sample_fast
+ * :640-692).  Overwrites the image. */
+dr_status dr_render_forward(dr_scene *scene, const dr_render_desc *rd, float *image_dev,
+                            void *stream);
+
+/* Backward render (delta_ray.cpp:694-1005 and :1468-1550): given the image
+ * adjoint d_image [H][W][3] (device), overwrites grad_dev (device, flat
+ * layout above) with every parameter gradient.  image_dev may be NULL;
+ * otherwise the re-rendered image is written there too. */
+dr_status dr_render_backward(dr_scene *scene, const dr_render_desc *rd, const float *d_image_dev,
+                             float *grad_dev, float *image_dev, void *stream);
+
+/* Kernel launch count of the last render call on this scene (for tooling). */
+dr_status dr_scene_last_launch_count(const dr_scene *scene, int *count);
+
+/* Copies the last error message of the calling thread into buf. */
+size_t dr_last_error(char *buf, size_t len);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* DELTA_RAY_B200_H */
