@@ -1,0 +1,204 @@
+// CUDA kernels of the renderer: LBVH build and the forward pixel-sample kernel.
+// The per-sample logic lives in the dr_*.cuh headers; kernels here only map
+// threads to work and reduce results.
+#include "dr_bvh.cuh"
+#include "dr_kernels.h"
+#include "dr_shading.cuh"
+
+#include <cub/cub.cuh>
+
+// ---------------------------------------------------------------------------
+// LBVH build
+// ---------------------------------------------------------------------------
+__global__ void k_bvh_morton(BvhBuildIn in, uint32_t *keys, int *vals) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= in.n) return;
+    keys[i] = tri_morton(in, i);
+    vals[i] = i;
+}
+
+__global__ void k_bvh_leaves(const int *sorted_ids, const float *vtx, const int4 *tri, int n, float4 *leaf_tris,
+                             Box *leaf_boxes) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int t = sorted_ids[i];
+    int4 id = tri[t];
+    float4 a, b, c;
+    a.x = vtx[3 * id.x]; a.y = vtx[3 * id.x + 1]; a.z = vtx[3 * id.x + 2]; a.w = dr_i2f(t);
+    b.x = vtx[3 * id.y]; b.y = vtx[3 * id.y + 1]; b.z = vtx[3 * id.y + 2]; b.w = 0.f;
+    c.x = vtx[3 * id.z]; c.y = vtx[3 * id.z + 1]; c.z = vtx[3 * id.z + 2]; c.w = 0.f;
+    leaf_tris[3 * i] = a;
+    leaf_tris[3 * i + 1] = b;
+    leaf_tris[3 * i + 2] = c;
+    leaf_boxes[i] = tri_box(a, b, c);
+}
+
+__global__ void k_bvh_internal(const uint32_t *keys, int n, int2 *children, int *parent_internal, int *parent_leaf) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n - 1) return;
+    lbvh_internal(keys, n, i, children, parent_internal, parent_leaf);
+}
+
+__device__ __forceinline__ Box load_box_cg(const Box *b) {
+    Box r;
+    const float *f = (const float *)b;
+    for (int k = 0; k < 3; k++) {
+        r.lo[k] = __ldcg(f + k);
+        r.hi[k] = __ldcg(f + 3 + k);
+    }
+    return r;
+}
+
+__global__ void k_bvh_refit(int n, const int *parent_leaf, const int *parent_internal, const int2 *children,
+                            const Box *leaf_boxes, Box *node_boxes, int *flags, float4 *nodes) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    int p = parent_leaf[i];
+    // each internal node is finished by the second of its two children; the
+    // walk is bounded by the tree height (< n)
+    for (int guard = 0; guard < n; guard++) {
+        __threadfence();
+        if (atomicAdd(flags + p, 1) == 0) return;
+        __threadfence();
+        int2 c = children[p];
+        Box b0 = c.x < 0 ? leaf_boxes[~c.x] : load_box_cg(node_boxes + c.x);
+        Box b1 = c.y < 0 ? leaf_boxes[~c.y] : load_box_cg(node_boxes + c.y);
+        Box u = box_union(b0, b1);
+        float *dst = (float *)(node_boxes + p);
+        for (int k = 0; k < 3; k++) {
+            __stcg(dst + k, u.lo[k]);
+            __stcg(dst + 3 + k, u.hi[k]);
+        }
+        write_node(nodes + 4 * p, b0, b1, c.x, c.y);
+        if (p == 0) return;
+        p = parent_internal[p];
+    }
+}
+
+static inline int blocks_for(long long n, int bs) { return (int)((n + bs - 1) / bs); }
+
+cudaError_t dr_build_lbvh(const float *vtx, const int4 *tri, int n, float3 lo, float3 hi, float4 *nodes,
+                          float4 *leaf_tris, void *scratch, size_t scratch_bytes, cudaStream_t st, int *launches) {
+    if (n <= 0) return cudaSuccess;
+    BvhBuildIn in;
+    in.vtx = vtx;
+    in.tri = tri;
+    in.n = n;
+    in.lo = lo;
+    float3 ext = hi - lo;
+    in.inv_ext = f3(ext.x > 0.f ? 1.f / ext.x : 0.f, ext.y > 0.f ? 1.f / ext.y : 0.f, ext.z > 0.f ? 1.f / ext.z : 0.f);
+    char *p = (char *)scratch;
+    auto take = [&](size_t bytes) {
+        char *r = p;
+        p += (bytes + 255) & ~(size_t)255;
+        return (void *)r;
+    };
+    uint32_t *keys = (uint32_t *)take(sizeof(uint32_t) * n);
+    uint32_t *keys2 = (uint32_t *)take(sizeof(uint32_t) * n);
+    int *vals = (int *)take(sizeof(int) * n);
+    int *vals2 = (int *)take(sizeof(int) * n);
+    Box *leaf_boxes = (Box *)take(sizeof(Box) * n);
+    Box *node_boxes = (Box *)take(sizeof(Box) * n);
+    int2 *children = (int2 *)take(sizeof(int2) * n);
+    int *parent_internal = (int *)take(sizeof(int) * n);
+    int *parent_leaf = (int *)take(sizeof(int) * n);
+    int *flags = (int *)take(sizeof(int) * n);
+    size_t used = (size_t)(p - (char *)scratch);
+    size_t sort_bytes = 0;
+    cub::DeviceRadixSort::SortPairs(nullptr, sort_bytes, keys, keys2, vals, vals2, n, 0, 30, st);
+    if (used + sort_bytes > scratch_bytes) return cudaErrorMemoryAllocation;
+    void *sort_tmp = take(sort_bytes);
+    const int bs = 256;
+    k_bvh_morton<<<blocks_for(n, bs), bs, 0, st>>>(in, keys, vals);
+    cub::DeviceRadixSort::SortPairs(sort_tmp, sort_bytes, keys, keys2, vals, vals2, n, 0, 30, st);
+    k_bvh_leaves<<<blocks_for(n, bs), bs, 0, st>>>(vals2, vtx, tri, n, leaf_tris, leaf_boxes);
+    *launches += 3;
+    if (n > 1) {
+        cudaMemsetAsync(flags, 0, sizeof(int) * n, st);
+        k_bvh_internal<<<blocks_for(n - 1, bs), bs, 0, st>>>(keys2, n, children, parent_internal, parent_leaf);
+        k_bvh_refit<<<blocks_for(n, bs), bs, 0, st>>>(n, parent_leaf, parent_internal, children, leaf_boxes,
+                                                       node_boxes, flags, nodes);
+        *launches += 2;
+    }
+    return cudaGetLastError();
+}
+
+size_t dr_lbvh_scratch_bytes(int n) {
+    size_t sort_bytes = 0;
+    cub::DeviceRadixSort::SortPairs(nullptr, sort_bytes, (uint32_t *)nullptr, (uint32_t *)nullptr, (int *)nullptr,
+                                    (int *)nullptr, n, 0, 30);
+    size_t per = 4 * sizeof(uint32_t) + 2 * sizeof(Box) + sizeof(int2) + 3 * sizeof(int);
+    return (per + 64) * (size_t)n + sort_bytes + 16 * 256;
+}
+
+__global__ void k_trace_rays(DevScene s, const float *rays, long long n, int *tri, float *t) {
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i >= n) return;
+    const float *r = rays + 6 * i;
+    Hit h = trace_closest(s, f3(r[0], r[1], r[2]), f3(r[3], r[4], r[5]), 1e-3f);
+    tri[i] = h.tri;
+    t[i] = h.t;
+}
+
+cudaError_t dr_launch_trace(const DevScene &s, const float *rays, long long n, int *tri, float *t, cudaStream_t st,
+                            int *launches) {
+    if (n <= 0) return cudaSuccess;
+    k_trace_rays<<<blocks_for(n, 256), 256, 0, st>>>(s, rays, n, tri, t);
+    *launches += 1;
+    return cudaGetLastError();
+}
+
+// ---------------------------------------------------------------------------
+// Forward render: one pixel sample per (pixel, lane) and a segmented warp
+// reduction over the 2^lanes_log2 lanes of a pixel.
+// ---------------------------------------------------------------------------
+DEV float3 pixel_sample(const DevScene &s, int x, int y, int W, int H, int spp, int si, int B, uint64_t seed) {
+    Rng r;
+    r.init(seed, kStreamPixel, ((uint64_t)y * W + x) * spp + si, 0);
+    float sub_x = r.next() / spp;
+    float sub_y = r.next() / spp;
+    Ray ray = sample_primary(s.cam, float((x + sub_x) / W), float((y + sub_y) / H));
+    if (abs_sum(ray.d) == 0.f) return f3(0.f);
+    Hit h = trace_closest(s, ray.o, ray.d, 1e-3f);
+    if (h.tri < 0) return f3(0.f);
+    SurfacePoint sp = intersect_tri(load_tri(s, h.tri), ray.o, ray.d);
+    LightSample ls = draw_light(r);
+    float3 c = shade(s, -ray.d, h.tri, sp, ls, r, B, true);
+    return c * (1.f / spp);
+}
+
+__global__ void __launch_bounds__(256) k_render_forward(DevScene s, int W, int H, int spp, int B, uint64_t seed,
+                                                        int lanes_log2, float *img) {
+    long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    int G = 1 << lanes_log2;
+    long long pix = gid >> lanes_log2;
+    int lane = (int)(gid & (G - 1));
+    float3 acc = f3(0.f);
+    bool active = pix < (long long)W * H;
+    if (active) {
+        int x = (int)(pix % W), y = (int)(pix / W);
+        for (int si = lane; si < spp; si += G) acc += pixel_sample(s, x, y, W, H, spp, si, B, seed);
+    }
+    for (int off = G >> 1; off >= 1; off >>= 1) {
+        acc.x += __shfl_down_sync(0xffffffffu, acc.x, off);
+        acc.y += __shfl_down_sync(0xffffffffu, acc.y, off);
+        acc.z += __shfl_down_sync(0xffffffffu, acc.z, off);
+    }
+    if (active && lane == 0) {
+        img[3 * pix] = acc.x;
+        img[3 * pix + 1] = acc.y;
+        img[3 * pix + 2] = acc.z;
+    }
+}
+
+cudaError_t dr_launch_forward(const DevScene &s, int W, int H, int spp, int B, uint64_t seed, float *img,
+                              cudaStream_t st, int *launches) {
+    int lanes_log2 = 0;
+    while ((1 << (lanes_log2 + 1)) <= spp && (1 << (lanes_log2 + 1)) <= 32 && spp % (1 << (lanes_log2 + 1)) == 0)
+        lanes_log2++;
+    long long threads = ((long long)W * H) << lanes_log2;
+    const int bs = 256;
+    k_render_forward<<<blocks_for(threads, bs), bs, 0, st>>>(s, W, H, spp, B, seed, lanes_log2, img);
+    *launches += 1;
+    return cudaGetLastError();
+}

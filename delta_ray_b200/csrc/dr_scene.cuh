@@ -1,0 +1,127 @@
+// Device-resident scene: flat, read-only arrays in HBM, one struct of raw
+// pointers passed by value to every kernel.
+//
+// Geometry is global over all shapes: vertex i of shape s lives at
+// shapes[s].vtx_off + i, triangle j at shapes[s].tri_off + j.  Global triangle
+// ids therefore order (shape, triangle) exactly as the reference's Embree
+// (geomID, primID) pairs (scene.cpp:100-135).
+#pragma once
+
+#include "dr_common.cuh"
+
+struct DevCamera {
+    M4 c2w, w2c;
+    float fov, aspect, clip_near;
+    int fisheye;
+};
+
+struct DevMaterial {
+    float kd[3], ks[3], rough;  // constant channels
+    int tex_kd, tex_ks, tex_r;  // texel offsets in DevScene::texels, -1 for constants
+    int kd_w, kd_h, ks_w, ks_h, r_w, r_h;
+    float uv_kd[2], uv_ks[2], uv_r[2];
+    int two_sided;
+    int grad_kd, grad_ks, grad_r;  // offsets in the flat gradient
+};
+
+struct DevShape {
+    int vtx_off, tri_off, nv, nt;
+    int mat, light;  // light: index of the light using this shape, -1 if none
+    int has_uv, has_n;
+    int grad_v, grad_n;  // flat gradient offsets (grad_n = -1 without normals)
+};
+
+struct DevLight {
+    int shape;
+    float I[3];
+    int cdf_off;  // offset of the triangle CDF (ntri + 1 floats) and func (ntri floats)
+    int ntri;
+    float area;   // total area (scene.cpp:40-47)
+    float func_int;
+    float bc[3], br;  // bounding sphere of the light's AABB (aabb.h:266-270)
+    int grad;         // flat gradient offset of d_intensity
+};
+
+struct DevEdge { int shape, v0, v1, f0, f1; };  // local vertex / triangle ids
+
+struct DevEdgeNode {
+    float lo[3], hi[3];
+    float axis[3], angle;
+    int offset;  // leaf: first edge; interior: index of the second child
+    int nprims;  // 0 for interior nodes
+    float total_length;
+    int pad;
+};
+
+struct DevScene {
+    DevCamera cam;
+    // geometry
+    const float *vtx;  // [V][3] global
+    const float *nrm;  // [V][3] or null
+    const float *uv;   // [V][2] or null
+    const int4 *tri;   // global vertex ids (x, y, z) and shape id (w)
+    const int *tri_local;
+    int num_tris;
+    // LBVH
+    const float4 *bvh_nodes;  // 4 float4 per internal node (two child boxes + child ids)
+    const float4 *bvh_tris;   // 3 float4 per leaf, leaf order (xyz, .w of the first = tri id)
+    int bvh_root;             // >= 0 internal node, < 0 leaf (~leaf slot)
+    // shapes, materials, lights
+    const DevShape *shapes;
+    int num_shapes;
+    const DevMaterial *mats;
+    int num_mats;
+    const float *texels;
+    const DevLight *lights;
+    int num_lights;
+    const float *light_sel_cdf;  // [num_lights + 1]
+    const float *light_sel_func; // [num_lights]
+    float light_sel_func_int;
+    float total_light_intensity;
+    const float *light_tri_cdf;   // per light: ntri + 1 entries at cdf_off
+    const float *light_tri_func;  // per light: ntri entries at cdf_off
+    // edges
+    const DevEdge *prim_edges;
+    int num_prim_edges;
+    const float *prim_cdf;  // [n + 1]
+    const float *prim_func; // [n]
+    float prim_func_int;
+    const DevEdgeNode *sil_nodes;
+    const DevEdge *sil_edges;
+    int num_sil_nodes;
+    const DevEdgeNode *nrm_nodes;
+    const DevEdge *nrm_edges;
+    int num_nrm_nodes;
+    const float *ltc;  // 128*128 row-major 3x3
+    int grad_total;
+};
+
+// --- accessors -------------------------------------------------------------
+DEV float3 vtx3(const float *DR_RESTRICT a, int i) {
+    return f3(dr_ldg(a + 3 * i), dr_ldg(a + 3 * i + 1), dr_ldg(a + 3 * i + 2));
+}
+DEV DevShape shape_of(const DevScene &s, int shape) { return s.shapes[shape]; }
+DEV float3 shape_vertex(const DevScene &s, int shape, int local_v) {
+    return vtx3(s.vtx, s.shapes[shape].vtx_off + local_v);
+}
+DEV int4 tri_vids(const DevScene &s, int tri) { return s.tri[tri]; }
+DEV float3 face_normal(const DevScene &s, int shape, int local_tri) {
+    int4 t = s.tri[s.shapes[shape].tri_off + local_tri];
+    float3 a = vtx3(s.vtx, t.x), b = vtx3(s.vtx, t.y), c = vtx3(s.vtx, t.z);
+    return normalize(cross(b - a, c - a));
+}
+
+// pbrt Distribution1D::sample_discrete (distribution.h:56-63) over a cdf of
+// count + 1 entries: upper_bound, then clamp to [0, count - 1].
+DEV int sample_discrete(const float *cdf, const float *func, float func_int, int count, float u, float *pmf) {
+    int lo = 0, hi = count + 1;  // first index with cdf[i] > u
+    while (lo < hi) {
+        int mid = (lo + hi) >> 1;
+        if (dr_ldg(cdf + mid) > u) hi = mid;
+        else lo = mid + 1;
+    }
+    int off = lo - 1;
+    off = off <= 0 ? 0 : (off >= count - 1 ? count - 1 : off);
+    if (pmf) *pmf = dr_ldg(func + off) / (func_int * count);
+    return off;
+}

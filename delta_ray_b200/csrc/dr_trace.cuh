@@ -1,0 +1,330 @@
+// Ray casting on the LBVH and analytic re-intersection of the hit triangle.
+//
+// Hit rule (identical to the oracle's CPU BVH, so hit ids agree): a triangle is
+// hit when Moller-Trumbore gives u >= 0, v >= 0, u + v <= 1 and
+// tnear < t < tfar; the smallest t wins, equal t goes to the lower global
+// triangle id.  The hit test is written with round-to-nearest intrinsics so
+// that it evaluates exactly the same IEEE operations as the CPU oracle.
+//
+// Ray intervals follow scene.cpp of the reference: closest hit on
+// (1e-3, inf) (scene.cpp:188-189), shadow rays on (1e-3 d, (1 - 1e-3) d)
+// (scene.cpp:159-160).  The hit point itself is recomputed by intersect_tri
+// exactly as intersect.h:100-148 does.
+#pragma once
+
+#include "dr_scene.cuh"
+
+#ifdef DR_HOST_BUILD
+HD float fmul_rn(float a, float b) { return a * b; }
+HD float fadd_rn(float a, float b) { return a + b; }
+HD float fsub_rn(float a, float b) { return a - b; }
+HD float frcp_rn(float a) { return 1.f / a; }
+#else
+DEV float fmul_rn(float a, float b) { return __fmul_rn(a, b); }
+DEV float fadd_rn(float a, float b) { return __fadd_rn(a, b); }
+DEV float fsub_rn(float a, float b) { return __fsub_rn(a, b); }
+DEV float frcp_rn(float a) { return __frcp_rn(a); }
+#endif
+
+#define DR_INF dr_i2f(0x7f800000)
+
+// Node-visit counter, only in the CPU build of this code used by the tests.
+#ifdef DR_HOST_BUILD
+extern thread_local long long g_dr_visits;
+#define DR_COUNT_VISIT() (g_dr_visits++)
+#else
+#define DR_COUNT_VISIT()
+#endif
+#define DR_STACK 64
+
+// Moller-Trumbore with no contraction: the exact operation sequence of the
+// oracle's hit test.  Returns false on a miss.
+DEV bool hit_triangle(float4 a, float4 b, float4 c, float3 o, float3 d, float &t_out) {
+    float e1x = fsub_rn(b.x, a.x), e1y = fsub_rn(b.y, a.y), e1z = fsub_rn(b.z, a.z);
+    float e2x = fsub_rn(c.x, a.x), e2y = fsub_rn(c.y, a.y), e2z = fsub_rn(c.z, a.z);
+    float sx = fsub_rn(o.x, a.x), sy = fsub_rn(o.y, a.y), sz = fsub_rn(o.z, a.z);
+    float px = fsub_rn(fmul_rn(d.y, e2z), fmul_rn(d.z, e2y));
+    float py = fsub_rn(fmul_rn(d.z, e2x), fmul_rn(d.x, e2z));
+    float pz = fsub_rn(fmul_rn(d.x, e2y), fmul_rn(d.y, e2x));
+    float det = fadd_rn(fadd_rn(fmul_rn(e1x, px), fmul_rn(e1y, py)), fmul_rn(e1z, pz));
+    if (det == 0.f) return false;
+    float inv = frcp_rn(det);
+    float u = fmul_rn(fadd_rn(fadd_rn(fmul_rn(sx, px), fmul_rn(sy, py)), fmul_rn(sz, pz)), inv);
+    if (u < 0.f || u > 1.f) return false;
+    float qx = fsub_rn(fmul_rn(sy, e1z), fmul_rn(sz, e1y));
+    float qy = fsub_rn(fmul_rn(sz, e1x), fmul_rn(sx, e1z));
+    float qz = fsub_rn(fmul_rn(sx, e1y), fmul_rn(sy, e1x));
+    float v = fmul_rn(fadd_rn(fadd_rn(fmul_rn(d.x, qx), fmul_rn(d.y, qy)), fmul_rn(d.z, qz)), inv);
+    if (v < 0.f || fadd_rn(u, v) > 1.f) return false;
+    t_out = fmul_rn(fadd_rn(fadd_rn(fmul_rn(e2x, qx), fmul_rn(e2y, qy)), fmul_rn(e2z, qz)), inv);
+    return true;
+}
+
+HD float safe_inv(float x) {
+    const float big = 1e30f;
+    if (x == 0.f) return big;
+    float r = 1.f / x;
+    return r > big ? big : (r < -big ? -big : r);
+}
+
+// Slab test of one child box against [0, tmax]; returns the entry distance
+// (>= 0) or -1 on a miss.  The far distance is widened by 2 gamma(3) (pbrt) so
+// that a hit lying on a box face is never culled.
+DEV float box_entry(float lx, float ly, float lz, float hx, float hy, float hz, float3 o, float3 inv, float tmax) {
+    float t0x = (lx - o.x) * inv.x, t1x = (hx - o.x) * inv.x;
+    float t0y = (ly - o.y) * inv.y, t1y = (hy - o.y) * inv.y;
+    float t0z = (lz - o.z) * inv.z, t1z = (hz - o.z) * inv.z;
+    float tn = fmaxf(fmaxf(fminf(t0x, t1x), fminf(t0y, t1y)), fmaxf(fminf(t0z, t1z), 0.f));
+    float tf = fminf(fminf(fmaxf(t0x, t1x), fmaxf(t0y, t1y)), fminf(fmaxf(t0z, t1z), tmax * 1.0000004f));
+    tf *= 1.0000004f;
+    return tn <= tf ? tn : -1.f;
+}
+
+struct Hit {
+    int tri;  // global triangle id, -1 for a miss
+    float t;
+};
+
+// Closest hit on (tnear, inf).
+DEV Hit trace_closest(const DevScene &s, float3 o, float3 d, float tnear) {
+    Hit h;
+    h.tri = -1;
+    h.t = DR_INF;
+    if (s.num_tris == 0) return h;
+    float3 inv = f3(safe_inv(d.x), safe_inv(d.y), safe_inv(d.z));
+    int stack[DR_STACK];
+    int sp = 0;
+    int node = s.bvh_root;
+    while (true) {
+        DR_COUNT_VISIT();
+        if (node < 0) {
+            int leaf = ~node;
+            float4 a = dr_ldg(s.bvh_tris + 3 * leaf), b = dr_ldg(s.bvh_tris + 3 * leaf + 1),
+                   c = dr_ldg(s.bvh_tris + 3 * leaf + 2);
+            float t;
+            if (hit_triangle(a, b, c, o, d, t) && t > tnear) {
+                int id = dr_f2i(a.w);
+                if (t < h.t || (t == h.t && id < h.tri)) {
+                    h.t = t;
+                    h.tri = id;
+                }
+            }
+            if (sp == 0) break;
+            node = stack[--sp];
+            continue;
+        }
+        const float4 *n = s.bvh_nodes + 4 * node;
+        float4 n0 = dr_ldg(n), n1 = dr_ldg(n + 1), n2 = dr_ldg(n + 2), n3 = dr_ldg(n + 3);
+        float e0 = box_entry(n0.x, n0.y, n0.z, n0.w, n1.x, n1.y, o, inv, h.t);
+        float e1 = box_entry(n1.z, n1.w, n2.x, n2.y, n2.z, n2.w, o, inv, h.t);
+        int c0 = dr_f2i(n3.x), c1 = dr_f2i(n3.y);
+        bool h0 = e0 >= 0.f, h1 = e1 >= 0.f;
+        if (h0 && h1) {
+            int nearc = e0 <= e1 ? c0 : c1, farc = e0 <= e1 ? c1 : c0;
+            if (sp < DR_STACK) stack[sp++] = farc;
+            node = nearc;
+        } else if (h0) {
+            node = c0;
+        } else if (h1) {
+            node = c1;
+        } else {
+            if (sp == 0) break;
+            node = stack[--sp];
+        }
+    }
+    return h;
+}
+
+// Any hit on (tnear, tfar).
+DEV bool trace_any(const DevScene &s, float3 o, float3 d, float tnear, float tfar) {
+    if (s.num_tris == 0) return false;
+    float3 inv = f3(safe_inv(d.x), safe_inv(d.y), safe_inv(d.z));
+    int stack[DR_STACK];
+    int sp = 0;
+    int node = s.bvh_root;
+    while (true) {
+        if (node < 0) {
+            int leaf = ~node;
+            float4 a = dr_ldg(s.bvh_tris + 3 * leaf), b = dr_ldg(s.bvh_tris + 3 * leaf + 1),
+                   c = dr_ldg(s.bvh_tris + 3 * leaf + 2);
+            float t;
+            if (hit_triangle(a, b, c, o, d, t) && t > tnear && t < tfar) return true;
+            if (sp == 0) break;
+            node = stack[--sp];
+            continue;
+        }
+        const float4 *n = s.bvh_nodes + 4 * node;
+        float4 n0 = dr_ldg(n), n1 = dr_ldg(n + 1), n2 = dr_ldg(n + 2), n3 = dr_ldg(n + 3);
+        float e0 = box_entry(n0.x, n0.y, n0.z, n0.w, n1.x, n1.y, o, inv, tfar);
+        float e1 = box_entry(n1.z, n1.w, n2.x, n2.y, n2.z, n2.w, o, inv, tfar);
+        int c0 = dr_f2i(n3.x), c1 = dr_f2i(n3.y);
+        bool h0 = e0 >= 0.f, h1 = e1 >= 0.f;
+        if (h0 && h1) {
+            if (sp < DR_STACK) stack[sp++] = c1;
+            node = c0;
+        } else if (h0) {
+            node = c0;
+        } else if (h1) {
+            node = c1;
+        } else {
+            if (sp == 0) break;
+            node = stack[--sp];
+        }
+    }
+    return false;
+}
+
+// occluded(scene, ray, max_t) of the reference (scene.cpp:147-166)
+DEV bool occluded(const DevScene &s, float3 o, float3 d, float max_t) {
+    return trace_any(s, o, d, max_t * 1e-3f, max_t * (1.f - 1e-3f));
+}
+
+// ---------------------------------------------------------------------------
+// Surface points and analytic re-intersection (intersect.h:100-148)
+// ---------------------------------------------------------------------------
+struct SurfacePoint {
+    float3 p, ng;
+    Frame f;
+    float2 uv;
+};
+
+struct TriData {
+    float3 v0, v1, v2;
+    float3 n0, n1, n2;
+    float2 t0, t1, t2;  // uvs (defaults (0,0),(1,0),(1,1): intersect.h:115-117)
+    bool has_n;
+    int shape;
+};
+
+DEV TriData load_tri(const DevScene &s, int tri) {
+    TriData td;
+    int4 id = tri_vids(s, tri);
+    td.shape = id.w;
+    td.v0 = vtx3(s.vtx, id.x);
+    td.v1 = vtx3(s.vtx, id.y);
+    td.v2 = vtx3(s.vtx, id.z);
+    DevShape sh = s.shapes[id.w];
+    td.has_n = sh.has_n != 0;
+    if (td.has_n) {
+        td.n0 = vtx3(s.nrm, id.x);
+        td.n1 = vtx3(s.nrm, id.y);
+        td.n2 = vtx3(s.nrm, id.z);
+    } else {
+        td.n0 = td.n1 = td.n2 = f3(0.f);
+    }
+    if (sh.has_uv) {
+        td.t0.x = dr_ldg(s.uv + 2 * id.x); td.t0.y = dr_ldg(s.uv + 2 * id.x + 1);
+        td.t1.x = dr_ldg(s.uv + 2 * id.y); td.t1.y = dr_ldg(s.uv + 2 * id.y + 1);
+        td.t2.x = dr_ldg(s.uv + 2 * id.z); td.t2.y = dr_ldg(s.uv + 2 * id.z + 1);
+    } else {
+        td.t0.x = 0.f; td.t0.y = 0.f;
+        td.t1.x = 1.f; td.t1.y = 0.f;
+        td.t2.x = 1.f; td.t2.y = 1.f;
+    }
+    return td;
+}
+
+struct IsectFwd {  // forward intermediates of intersect_tri, kept for its adjoint
+    float3 e1, e2, pvec, s, qvec, cg, ns;
+    float div, ru, rv, rt, u, v, w, t;
+    bool div_fixed, flip;
+};
+
+DEV SurfacePoint intersect_tri(const TriData &td, float3 o, float3 d, IsectFwd *fw = nullptr) {
+    IsectFwd f;
+    f.e1 = td.v1 - td.v0;
+    f.e2 = td.v2 - td.v0;
+    f.pvec = cross(d, f.e2);
+    f.div = dot(f.pvec, f.e1);
+    f.div_fixed = f.div == 0.f;
+    if (f.div_fixed) f.div = 1e-8f;  // intersect.h:80-83
+    f.s = o - td.v0;
+    f.ru = dot(f.s, f.pvec);
+    f.u = f.ru / f.div;
+    f.qvec = cross(f.s, f.e1);
+    f.rv = dot(d, f.qvec);
+    f.v = f.rv / f.div;
+    f.rt = dot(f.e2, f.qvec);
+    f.t = f.rt / f.div;
+    f.w = 1.f - (f.u + f.v);
+    SurfacePoint sp;
+    sp.uv.x = f.w * td.t0.x + f.u * td.t1.x + f.v * td.t2.x;
+    sp.uv.y = f.w * td.t0.y + f.u * td.t1.y + f.v * td.t2.y;
+    sp.p = o + d * f.t;
+    f.cg = cross(td.v1 - td.v0, td.v2 - td.v0);
+    float3 gn = normalize(f.cg);
+    float3 sn = gn;
+    f.flip = false;
+    if (td.has_n) {
+        f.ns = f.w * td.n0 + f.u * td.n1 + f.v * td.n2;
+        sn = normalize(f.ns);
+        if (dot(gn, sn) < 0.f) {
+            gn = -gn;
+            f.flip = true;
+        }
+    }
+    sp.ng = gn;
+    sp.f = make_frame(sn);
+    if (fw) *fw = f;
+    return sp;
+}
+
+struct TriGrad {
+    float3 v0, v1, v2, n0, n1, n2;
+};
+
+// Adjoint of intersect_tri.  d_p, d_ng, d_frame, d_uv are output adjoints;
+// accumulates vertex / normal adjoints into g and ray adjoints into d_o, d_d.
+DEV void d_intersect_tri(const TriData &td, float3 o, float3 d, const IsectFwd &f, float3 d_p, float3 d_ng,
+                         const Frame &d_frame, float2 d_uv, TriGrad &g, float3 &d_o, float3 &d_d) {
+    float3 gn0 = normalize(f.cg);
+    float3 sn = td.has_n ? normalize(f.ns) : gn0;
+    float3 d_sn = d_make_frame(sn, d_frame);
+    float d_u = 0.f, d_v = 0.f, d_w = 0.f;
+    float3 d_gn;
+    if (td.has_n) {
+        float3 d_ns = d_normalize(f.ns, d_sn);
+        d_w += dot(d_ns, td.n0);
+        d_u += dot(d_ns, td.n1);
+        d_v += dot(d_ns, td.n2);
+        g.n0 += f.w * d_ns;
+        g.n1 += f.u * d_ns;
+        g.n2 += f.v * d_ns;
+        d_gn = f.flip ? -d_ng : d_ng;
+    } else {
+        d_gn = d_ng + d_sn;
+    }
+    float3 d_cg = d_normalize(f.cg, d_gn);
+    float3 d_e1 = f3(0.f), d_e2 = f3(0.f);
+    d_cross(f.e1, f.e2, d_cg, d_e1, d_e2);
+    // hit = o + d t
+    d_o += d_p;
+    d_d += d_p * f.t;
+    float d_t = dot(d_p, d);
+    // uv = w t0 + u t1 + v t2
+    d_w += d_uv.x * td.t0.x + d_uv.y * td.t0.y;
+    d_u += d_uv.x * td.t1.x + d_uv.y * td.t1.y;
+    d_v += d_uv.x * td.t2.x + d_uv.y * td.t2.y;
+    d_u -= d_w;
+    d_v -= d_w;
+    float inv = 1.f / f.div;
+    float d_ru = d_u * inv, d_rv = d_v * inv, d_rt = d_t * inv;
+    float d_div = -(d_u * f.ru + d_v * f.rv + d_t * f.rt) * inv * inv;
+    if (f.div_fixed) d_div = 0.f;
+    float3 d_s = d_ru * f.pvec;
+    float3 d_pvec = d_ru * f.s;
+    d_d += d_rv * f.qvec;
+    float3 d_qvec = d_rv * d;
+    d_e2 += d_rt * f.qvec;
+    d_qvec += d_rt * f.e2;
+    d_cross(f.s, f.e1, d_qvec, d_s, d_e1);
+    d_o += d_s;
+    g.v0 -= d_s;
+    d_pvec += d_div * f.e1;
+    d_e1 += d_div * f.pvec;
+    d_cross(d, f.e2, d_pvec, d_d, d_e2);
+    g.v1 += d_e1;
+    g.v0 -= d_e1;
+    g.v2 += d_e2;
+    g.v0 -= d_e2;
+}

@@ -1,0 +1,222 @@
+"""Drop-in replacement of the reference's render_pytorch.RenderFunction.
+
+``RenderFunction.serialize_scene(cam, materials, shapes, lights, resolution,
+num_samples, max_bounces)`` returns the same flat argument list as the
+reference (render_pytorch.py:13-55), and ``RenderFunction.apply(seed, *args)``
+renders it (render_pytorch.py:58-233); ``loss.backward()`` returns one
+gradient per argument (render_pytorch.py:236-333).  Differences:
+
+* rendering runs on the GPU through libdr_b200.so; inputs may be CPU or CUDA
+  tensors, the image is a CUDA tensor (``RenderOptions.output_device``
+  changes that) and gradients come back on each input's own device;
+* the scene is built once in forward and reused by backward (the reference
+  rebuilds it in both passes);
+* a ``RenderOptions`` object may be appended after ``max_bounces``;
+* uv-scale gradients are None: the reference computes them but never
+  accumulates them (delta_ray.cpp:853-859, :1127-1128).
+"""
+import ctypes as C
+
+import torch
+
+from . import _abi, _lib
+
+
+class RenderOptions:
+    """Optional trailing argument of RenderFunction.apply.
+
+    primary_edge_samples: number of primary-edge samples in backward
+        (0 = spp * width * height, the reference's total).
+    dp_mode: _abi.DR_DP_REFERENCE_LAST (the reference's behaviour) or
+        _abi.DR_DP_SUM (sum every sampled edge's position derivative).
+    ltc_table: optional [128*128*9] float32 Blinn-Phong LTC table.
+    output_device: device of the returned image (default: the render device).
+    device: CUDA device index to render on (default: current device).
+    """
+
+    def __init__(self, primary_edge_samples=0, dp_mode=_abi.DR_DP_REFERENCE_LAST, ltc_table=None,
+                 output_device=None, device=None):
+        self.primary_edge_samples = int(primary_edge_samples)
+        self.dp_mode = int(dp_mode)
+        self.ltc_table = ltc_table
+        self.output_device = output_device
+        self.device = device
+
+
+class Scene:
+    """A device scene (dr_scene) built from unpacked RenderFunction arguments."""
+
+    def __init__(self, cam, materials, shapes, lights, device_index, ltc_table=None):
+        L = _lib.lib()
+        self.device_index = int(device_index)
+        self.device = torch.device("cuda", self.device_index)
+        self.materials = materials
+        self.shapes = shapes
+        self.sd = _abi.SceneDesc.from_scene(cam, materials, shapes, lights, self.device, ltc_table)
+        handle = C.c_void_p()
+        with torch.cuda.device(self.device_index):
+            torch.cuda.current_stream().synchronize()
+            _lib.check(L.dr_scene_create(C.byref(self.sd.desc), self.device_index, C.byref(handle)))
+        self.handle = handle
+        lay = _abi.dr_grad_layout()
+        _lib.check(L.dr_scene_grad_layout(self.handle, C.byref(lay)))
+        self.grad_total = int(lay.total)
+        if self.grad_total != self.sd.grad_total:
+            raise RuntimeError("gradient layout mismatch between library and binding")
+
+    def _stream(self):
+        return C.c_void_p(torch.cuda.current_stream(self.device).cuda_stream)
+
+    def forward(self, width, height, spp, max_bounces, seed, opts=None):
+        opts = opts or RenderOptions()
+        img = torch.empty((height, width, 3), dtype=torch.float32, device=self.device)
+        rd = _abi.render_desc(width, height, spp, max_bounces, seed, opts.primary_edge_samples, opts.dp_mode)
+        with torch.cuda.device(self.device_index):
+            _lib.check(_lib.lib().dr_render_forward(self.handle, C.byref(rd), C.c_void_p(img.data_ptr()),
+                                                    self._stream()))
+        return img
+
+    def backward(self, width, height, spp, max_bounces, seed, d_image, opts=None, want_image=False):
+        opts = opts or RenderOptions()
+        d_image = d_image.detach().to(device=self.device, dtype=torch.float32).contiguous()
+        if tuple(d_image.shape) != (height, width, 3):
+            raise ValueError(f"d_image must be [{height}, {width}, 3]")
+        grad = torch.empty(self.grad_total, dtype=torch.float32, device=self.device)
+        img = torch.empty((height, width, 3), dtype=torch.float32, device=self.device) if want_image else None
+        rd = _abi.render_desc(width, height, spp, max_bounces, seed, opts.primary_edge_samples, opts.dp_mode)
+        with torch.cuda.device(self.device_index):
+            _lib.check(_lib.lib().dr_render_backward(
+                self.handle, C.byref(rd), C.c_void_p(d_image.data_ptr()), C.c_void_p(grad.data_ptr()),
+                C.c_void_p(img.data_ptr()) if img is not None else None, self._stream()))
+        return grad, img
+
+    def trace(self, rays):
+        """Closest hit (global triangle id, t) of rays [n, 6] on the device."""
+        rays = rays.detach().to(device=self.device, dtype=torch.float32).contiguous().reshape(-1, 6)
+        n = rays.shape[0]
+        tri = torch.empty(n, dtype=torch.int32, device=self.device)
+        t = torch.empty(n, dtype=torch.float32, device=self.device)
+        with torch.cuda.device(self.device_index):
+            _lib.check(_lib.lib().dr_trace_rays(self.handle, C.c_void_p(rays.data_ptr()), n,
+                                                C.c_void_p(tri.data_ptr()), C.c_void_p(t.data_ptr()),
+                                                self._stream()))
+        return tri, t
+
+    def split_grad(self, flat):
+        return self.sd.split_grad(flat, self.materials, self.shapes)
+
+    def launch_count(self):
+        n = C.c_int()
+        _lib.check(_lib.lib().dr_scene_last_launch_count(self.handle, C.byref(n)))
+        return n.value
+
+    def close(self):
+        if getattr(self, "handle", None):
+            _lib.lib().dr_scene_destroy(self.handle)
+            self.handle = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+
+def unpack_args(args):
+    """Splits the flat argument list (render_pytorch.py:61-135 of the reference)."""
+    i = 0
+
+    def take():
+        nonlocal i
+        v = args[i]
+        i += 1
+        return v
+    nm, ns, nl = take(), take(), take()
+    cam = dict(cam_to_world=take(), world_to_cam=take(), sample_to_cam=take(), cam_to_sample=take(),
+               fov_factor=float(take()), aspect_ratio=float(take()), clip_near=float(take()),
+               fisheye=bool(take()))
+    mats = []
+    for _ in range(nm):
+        mats.append(dict(diffuse=take(), specular=take(), roughness=take(), diffuse_uv_scale=take(),
+                         specular_uv_scale=take(), roughness_uv_scale=take(), two_sided=bool(take())))
+    shps = []
+    for _ in range(ns):
+        shps.append(dict(vertices=take(), indices=take(), uvs=take(), normals=take(),
+                         material_id=int(take())))
+    lts = []
+    for _ in range(nl):
+        lts.append(dict(shape_id=int(take()), intensity=take()))
+    resolution = take()
+    spp = int(take())
+    max_bounces = int(take())
+    opts = None
+    if i < len(args) and isinstance(args[i], RenderOptions):
+        opts = take()
+    if i != len(args):
+        raise ValueError("unexpected trailing arguments to RenderFunction")
+    return cam, mats, shps, lts, (int(resolution[0]), int(resolution[1])), spp, max_bounces, opts
+
+
+class RenderFunction(torch.autograd.Function):
+    """Differentiable render of a serialized scene (see module docstring)."""
+
+    @staticmethod
+    def serialize_scene(cam, materials, shapes, lights, resolution, num_samples, max_bounces):
+        args = [len(materials), len(shapes), len(lights), cam.cam_to_world, cam.world_to_cam,
+                cam.sample_to_cam, cam.cam_to_sample,
+                float(torch.as_tensor(cam.fov_factor).reshape(-1)[0]), cam.aspect_ratio,
+                float(torch.as_tensor(cam.clip_near).reshape(-1)[0]), cam.fisheye]
+        for m in materials:
+            args += [m.diffuse_reflectance, m.specular_reflectance, m.roughness, m.diffuse_uv_scale,
+                     m.specular_uv_scale, m.roughness_uv_scale, m.two_sided]
+        for s in shapes:
+            args += [s.vertices, s.indices, s.uvs, s.normals, s.mat_id]
+        for l in lights:
+            args += [l.shape_id, l.intensity]
+        args += [resolution, num_samples, max_bounces]
+        return args
+
+    @staticmethod
+    def forward(ctx, seed, *args):
+        cam, mats, shps, lts, (W, H), spp, B, opts = unpack_args(args)
+        opts = opts or RenderOptions()
+        dev = opts.device if opts.device is not None else torch.cuda.current_device()
+        scene = Scene(cam, mats, shps, lts, dev, opts.ltc_table)
+        img = scene.forward(W, H, spp, B, seed, opts)
+        ctx.scene = scene
+        ctx.render = (W, H, spp, B, int(seed), opts)
+        ctx.arg_devices = [a.device if torch.is_tensor(a) else None for a in args]
+        ctx.nargs = len(args)
+        ctx.counts = (len(mats), len(shps), len(lts))
+        ctx.has_normals = [s["normals"] is not None for s in shps]
+        if opts.output_device is not None:
+            img = img.to(opts.output_device)
+        return img
+
+    @staticmethod
+    def backward(ctx, grad_img):
+        W, H, spp, B, seed, opts = ctx.render
+        scene = ctx.scene
+        flat, _ = scene.backward(W, H, spp, B, seed, grad_img, opts)
+        g = scene.split_grad(flat)
+        nm, ns, nl = ctx.counts
+        out = [None, None, None, None]  # seed, num_materials, num_shapes, num_lights
+        out += [g["d_cam_to_world"], g["d_world_to_cam"], g["d_sample_to_cam"], g["d_cam_to_sample"]]
+        out += [None, None, None, None]  # fov_factor, aspect_ratio, clip_near, fisheye
+        for i in range(nm):
+            out += [g["d_diffuse"][i], g["d_specular"][i], g["d_roughness"][i], None, None, None, None]
+        for i in range(ns):
+            out += [g["d_vertices"][i], None, None, g["d_normals"][i] if ctx.has_normals[i] else None, None]
+        for i in range(nl):
+            out += [None, g["d_intensity"][i]]
+        out += [None, None, None]
+        while len(out) < ctx.nargs + 1:
+            out.append(None)  # RenderOptions
+        # gradients live on each input's device
+        res = [None]
+        for grad, dev in zip(out[1:], ctx.arg_devices):
+            if grad is not None and dev is not None:
+                grad = grad.to(dev)
+            res.append(grad)
+        ctx.scene = None
+        return tuple(res)

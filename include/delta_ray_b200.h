@@ -34,6 +34,12 @@ extern "C" {
 
 #define DR_ABI_VERSION 1
 
+#if defined(__GNUC__)
+#define DR_API __attribute__((visibility("default")))
+#else
+#define DR_API
+#endif
+
 typedef enum {
     DR_OK = 0,
     DR_ERR_INVALID_ARGUMENT = 1,
@@ -145,38 +151,46 @@ typedef struct {
 typedef struct dr_scene dr_scene;
 
 /* Library/ABI version; lets a binding check what it loaded. */
-int dr_abi_version(void);
+DR_API int dr_abi_version(void);
 
 /* Builds the device scene: geometry, LBVH, light samplers, edge list,
  * primary-edge sampler and edge trees (scene.cpp:19-136). */
-dr_status dr_scene_create(const dr_scene_desc *desc, int device, dr_scene **out);
+DR_API dr_status dr_scene_create(const dr_scene_desc *desc, int device, dr_scene **out);
 
 /* Replaces vertex positions (same topology) and rebuilds what depends on
  * them; `desc` must describe the same meshes as at creation. */
-dr_status dr_scene_update(dr_scene *scene, const dr_scene_desc *desc);
+DR_API dr_status dr_scene_update(dr_scene *scene, const dr_scene_desc *desc);
 
-dr_status dr_scene_destroy(dr_scene *scene);
+DR_API dr_status dr_scene_destroy(dr_scene *scene);
 
-dr_status dr_scene_grad_layout(const dr_scene *scene, dr_grad_layout *layout);
+DR_API dr_status dr_scene_grad_layout(const dr_scene *scene, dr_grad_layout *layout);
 
 /* Forward render: image [H][W][3] float32 (device), the mean over spp
  * samples of each pixel (delta_ray.cpp:1190-1333, render_sample_fast
  * :640-692).  Overwrites the image. */
-dr_status dr_render_forward(dr_scene *scene, const dr_render_desc *rd, float *image_dev,
+DR_API dr_status dr_render_forward(dr_scene *scene, const dr_render_desc *rd, float *image_dev,
                             void *stream);
 
 /* Backward render (delta_ray.cpp:694-1005 and :1468-1550): given the image
  * adjoint d_image [H][W][3] (device), overwrites grad_dev (device, flat
  * layout above) with every parameter gradient.  image_dev may be NULL;
  * otherwise the re-rendered image is written there too. */
-dr_status dr_render_backward(dr_scene *scene, const dr_render_desc *rd, const float *d_image_dev,
+DR_API dr_status dr_render_backward(dr_scene *scene, const dr_render_desc *rd, const float *d_image_dev,
                              float *grad_dev, float *image_dev, void *stream);
 
+/* Closest hits of n rays [n][6] (origin, direction; device memory) on
+ * (1e-3, inf): global triangle id (-1 on a miss; ids run over shapes in
+ * order, then triangles) and distance.  Replaces the reference's
+ * nearest_hit (scene.cpp:177-202) and uses the same hit rule as the
+ * renderer's own traversal. */
+DR_API dr_status dr_trace_rays(dr_scene *scene, const float *rays_dev, int64_t n, int *tri_dev, float *t_dev,
+                        void *stream);
+
 /* Kernel launch count of the last render call on this scene (for tooling). */
-dr_status dr_scene_last_launch_count(const dr_scene *scene, int *count);
+DR_API dr_status dr_scene_last_launch_count(const dr_scene *scene, int *count);
 
 /* Copies the last error message of the calling thread into buf. */
-size_t dr_last_error(char *buf, size_t len);
+DR_API size_t dr_last_error(char *buf, size_t len);
 
 #ifdef __cplusplus
 }

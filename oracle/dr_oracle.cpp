@@ -2380,6 +2380,13 @@ int dro_trace(const dr_scene_desc *desc, const float *rays /*[n][6]*/, long long
     return 0;
 }
 
+// One raw Philox4x32-10 block (known-answer tests).
+void dro_philox_raw(const uint32_t *ctr, const uint32_t *key, uint32_t *out) {
+    uint32_t c[4] = {ctr[0], ctr[1], ctr[2], ctr[3]};
+    philox4x32_10(c, key[0], key[1]);
+    for (int i = 0; i < 4; i++) out[i] = c[i];
+}
+
 // Philox draws, for checking the GPU generator bit for bit.
 void dro_philox(uint64_t seed, uint32_t kind, uint64_t id, uint32_t sub, int n, float *out) {
     PhiloxSampler s(seed, kind, id, sub);

@@ -44,6 +44,7 @@ def load():
         lib.dro_philox.argtypes = [C.c_uint64, C.c_uint32, C.c_uint64, C.c_uint32, C.c_int,
                                    C.c_void_p]
         lib.dro_scene_info.argtypes = [C.POINTER(_abi.dr_scene_desc), C.c_void_p]
+        lib.dro_philox_raw.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p]
         _lib = lib
     return _lib
 
@@ -104,6 +105,15 @@ def philox(seed, kind, ident, sub, n):
     lib = load()
     out = np.zeros(n, np.float32)
     lib.dro_philox(int(seed), int(kind), int(ident), int(sub), int(n), out.ctypes.data)
+    return out
+
+
+def philox_raw(ctr, key):
+    lib = load()
+    c = np.ascontiguousarray(np.asarray(ctr, np.uint32))
+    k = np.ascontiguousarray(np.asarray(key, np.uint32))
+    out = np.zeros(4, np.uint32)
+    lib.dro_philox_raw(c.ctypes.data, k.ctypes.data, out.ctypes.data)
     return out
 
 

@@ -1,0 +1,103 @@
+"""Small scenes for the parity tests (beyond the benchmark workloads).
+
+Each builder returns a ``delta_ray_b200.workloads.Workload`` that exercises a
+feature of the reference path: the Blinn-Phong lobe and its LTC edge sampling
+(material.h:257-489), textures with uv scaling (material.h:108-239), two-sided
+materials (pathtrace.h:116-133, material.h:264-268), shading normals and the
+directional edge tree (intersect.h:128-141, edge_tree.cpp:219-250), and the
+fisheye camera (camera.h:51-71).
+"""
+import numpy as np
+import torch
+
+from delta_ray_b200 import workloads
+from delta_ray_b200.light import Light
+from delta_ray_b200.material import Material
+from delta_ray_b200.shape import Shape
+
+_t = workloads._t
+
+
+def glossy_shadow(seed=0, resolution=(48, 40), spp=2, max_bounces=2):
+    wl = workloads.soft_shadow(seed, resolution, spp, max_bounces)
+    rng = np.random.default_rng(seed + 100)
+    for m in wl.materials[:2]:
+        m.specular_reflectance = _t(rng.uniform(0.2, 0.6, 3))
+        m.roughness = _t([rng.uniform(0.05, 0.4)])
+    wl.materials[0].two_sided = True
+    wl.name = "glossy_shadow"
+    return wl
+
+
+def textured(seed=0, resolution=(40, 40), spp=2, max_bounces=2):
+    wl = workloads.soft_shadow(seed, resolution, spp, max_bounces)
+    rng = np.random.default_rng(seed + 200)
+    ground = wl.shapes[0]
+    v = ground.vertices.numpy()
+    uv = ((v[:, [0, 2]] + 5.0) / 10.0).astype(np.float32)
+    ground.uvs = _t(uv)
+    m = wl.materials[0]
+    m.diffuse_reflectance = _t(rng.uniform(0.2, 0.9, (8, 8, 3)))
+    m.specular_reflectance = _t(rng.uniform(0.0, 0.3, (4, 4, 3)))
+    m.roughness = _t(rng.uniform(0.1, 0.6, (4, 4, 1)))
+    m.diffuse_uv_scale = _t([1.5, 2.0])
+    m.specular_uv_scale = m.diffuse_uv_scale
+    m.roughness_uv_scale = m.diffuse_uv_scale
+    wl.name = "textured"
+    return wl
+
+
+def _icosphere(subdiv):
+    t = (1.0 + 5 ** 0.5) / 2.0
+    v = [[-1, t, 0], [1, t, 0], [-1, -t, 0], [1, -t, 0], [0, -1, t], [0, 1, t], [0, -1, -t],
+         [0, 1, -t], [t, 0, -1], [t, 0, 1], [-t, 0, -1], [-t, 0, 1]]
+    f = [[0, 11, 5], [0, 5, 1], [0, 1, 7], [0, 7, 10], [0, 10, 11], [1, 5, 9], [5, 11, 4],
+         [11, 10, 2], [10, 7, 6], [7, 1, 8], [3, 9, 4], [3, 4, 2], [3, 2, 6], [3, 6, 8],
+         [3, 8, 9], [4, 9, 5], [2, 4, 11], [6, 2, 10], [8, 6, 7], [9, 8, 1]]
+    v = [np.array(x, np.float64) / np.linalg.norm(x) for x in v]
+    for _ in range(subdiv):
+        cache, nf = {}, []
+
+        def mid(a, b):
+            key = (min(a, b), max(a, b))
+            if key not in cache:
+                m = v[a] + v[b]
+                v.append(m / np.linalg.norm(m))
+                cache[key] = len(v) - 1
+            return cache[key]
+        for a, b, c in f:
+            ab, bc, ca = mid(a, b), mid(b, c), mid(c, a)
+            nf += [[a, ab, ca], [b, bc, ab], [c, ca, bc], [ab, bc, ca]]
+        f = nf
+    return np.array(v, np.float32), np.array(f, np.int32)
+
+
+def smooth_sphere(seed=0, resolution=(40, 40), spp=2, max_bounces=1, subdiv=1):
+    """An icosphere with per-vertex shading normals on a ground plane."""
+    wl = workloads.soft_shadow(seed, resolution, spp, max_bounces)
+    v, f = _icosphere(subdiv)
+    center = np.array([0.3, 1.2, 0.2], np.float32)
+    verts = (v * 1.0 + center).astype(np.float32)
+    wl.shapes[1] = Shape(_t(verts), _t(f, np.int32), None, _t(v), 1)
+    wl.materials[1].specular_reflectance = _t([0.3, 0.3, 0.3])
+    wl.materials[1].roughness = _t([0.2])
+    wl.name = "smooth_sphere"
+    return wl
+
+
+def fisheye(seed=0, resolution=(32, 32), spp=2, max_bounces=1):
+    wl = workloads.soft_shadow(seed, resolution, spp, max_bounces)
+    res = wl.resolution
+    wl.camera = workloads._camera([0, 6, -6], [0, 0, 0], [0, 1, 0], 45.0, res, fisheye=True)
+    wl.name = "fisheye"
+    return wl
+
+
+def heightfield_small(seed=0, resolution=(40, 32), spp=2, max_bounces=2, grid=10):
+    wl = workloads.heightfield(seed, resolution, spp, max_bounces, grid=grid, patch=grid)
+    wl.name = "heightfield_small"
+    return wl
+
+
+SCENES = {"glossy_shadow": glossy_shadow, "textured": textured, "smooth_sphere": smooth_sphere,
+          "fisheye": fisheye, "heightfield_small": heightfield_small}
