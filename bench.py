@@ -1,0 +1,373 @@
+#!/usr/bin/env python
+"""Forward+backward throughput of the B200 differentiable path tracer.
+
+Workload: the soft-shadow scene (ground + 4-triangle blocker + area light),
+512x512, 16 spp, max_bounces 1 -- one "step" renders the image and runs the
+full backward (path adjoint, secondary edges, primary edges) against an
+all-ones image adjoint.  Metric: pixel samples per second (fwd+bwd).
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+
+N > 1 runs under torchrun; every rank renders its own replica of the workload
+(samples are independent; no collective on the data path), and `value` is the
+sum over ranks, timed as the max over ranks.  `--impl reference` times the
+reference's own CPU renderer (oracle/_ref, compiled from the reference sources
+with their flags) on this machine's cores on a bounded sample of the workload.
+"""
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "fwd+bwd samples/s"
+UNIT = "samples/s"
+WORKLOAD = dict(name="soft_shadow", resolution=(512, 512), spp=16, max_bounces=1, scene_seed=0)
+# reference CPU arm: a bounded slice of the same workload
+REF_RES = (192, 192)
+
+
+def parse():
+    p = argparse.ArgumentParser()
+    p.add_argument("--gpus", type=int, default=1)
+    p.add_argument("--steps", type=int, default=10)
+    p.add_argument("--warmup", type=int, default=3)
+    p.add_argument("--impl", default="b200", choices=["b200", "reference"])
+    p.add_argument("--no-cpu-baseline", action="store_true")
+    return p.parse_args()
+
+
+def dist_info():
+    return (int(os.environ.get("RANK", 0)), int(os.environ.get("LOCAL_RANK", 0)),
+            int(os.environ.get("WORLD_SIZE", 1)))
+
+
+def build_workload(res=None):
+    from delta_ray_b200 import workloads
+    w = WORKLOAD
+    return workloads.soft_shadow(seed=w["scene_seed"], resolution=res or w["resolution"], spp=w["spp"],
+                                 max_bounces=w["max_bounces"])
+
+
+# ---------------------------------------------------------------------------
+# clocks during the timed region
+# ---------------------------------------------------------------------------
+class ClockSampler:
+    QUERY = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.QUERY}",
+                                          "--format=csv,noheader,nounits", "-lms", "200"],
+                                         stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except Exception:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if not self.proc:
+            return None
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        self.thread.join(timeout=2)
+        sm, mx, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for l in self.lines:
+            f = [x.strip() for x in l.split(",")]
+            if len(f) < 9:
+                continue
+            try:
+                sm.append(float(f[1]))
+                mx.append(float(f[2]))
+            except ValueError:
+                continue
+            for n, v in zip(names, f[5:9]):
+                if v.lower().startswith("active"):
+                    reasons.add(n)
+        if not sm:
+            return None
+        return {"sm_mhz": statistics.median(sm), "sm_max_mhz": max(mx), "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+# ---------------------------------------------------------------------------
+# algorithmic work model (bytes a launch must move at minimum)
+# ---------------------------------------------------------------------------
+def ray_bytes(num_tris):
+    """Per ray: origin+direction 24 B, hit record 16 B, 3 vertices 36 B and one
+    64-B node pair per BVH level (ceil(log2 T) levels)."""
+    return 24 + 16 + 36 + 64 * max(1, math.ceil(math.log2(max(2, num_tris))))
+
+
+def stage_bytes(stage, wl, counts):
+    """Algorithmic bytes of one launch of a backward/forward stage."""
+    W, H = wl.resolution
+    spp, B = wl.spp, wl.max_bounces
+    br = ray_bytes(wl.num_triangles)
+    shade = 32 + 28  # path state read/write + material record per shading vertex
+    n = W * H * spp
+    points, items = counts
+    rays_path = 1 + 2 * B  # upper bound: camera ray, then a shadow and a BSDF ray per bounce
+    if stage in ("k_render_forward",):
+        return n * (rays_path * br + B * shade) + W * H * 12
+    if stage == "k_backward_paths":
+        return n * (rays_path * br + B * shade) + W * H * 24 + points * 96
+    if stage == "k_edge_traverse":
+        return points * 96 + items * 20
+    if stage == "k_edge_eval":
+        # two straddling rays, two shadow rays of the emitter evaluations
+        return items * (4 * br + 2 * shade + 96 + 20 + 12)
+    if stage == "k_dp_propagate":
+        return points * (96 + 36 + 12 * 3)
+    if stage == "k_primary_edges":
+        # two camera rays + two shaded paths per sample, plus edge/vertex reads
+        return n * (2 * (1 + rays_path) * br + 2 * B * shade + 24 + 12)
+    return 0
+
+
+def load_peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            d = json.load(f)
+        return float(d["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def load_traffic(stage):
+    """DRAM bytes per launch of `stage` from the committed ncu summary, if any."""
+    try:
+        with open(os.path.join(ROOT, "profiles", "traffic.json")) as f:
+            d = json.load(f)
+        return d.get(stage)
+    except Exception:
+        return None
+
+
+# ---------------------------------------------------------------------------
+# reference CPU renderer
+# ---------------------------------------------------------------------------
+def reference_step(wl, seed):
+    import numpy as np
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import ref_runner
+    W, H = wl.resolution
+    t0 = time.perf_counter()
+    ref_runner.render_reference(wl, seed)
+    ref_runner.render_reference(wl, seed, d_image=np.ones((H, W, 3), np.float32))
+    return time.perf_counter() - t0
+
+
+def cpu_baseline():
+    """The reference's own CPU path (oracle/_ref, -O3 -ffast-math, its thread pool
+    on all host cores) on a bounded 192x192 slice of the workload."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import ref_runner
+    if not ref_runner.reference_available():
+        return None
+    wl = build_workload(REF_RES)
+    W, H = wl.resolution
+    reference_step(wl, 0)  # page in
+    t = reference_step(wl, 1)
+    samples = W * H * wl.spp
+    return {"value": samples / t, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
+            "sample": f"{W}x{H} at {wl.spp} spp of the same scene (forward call + backward call), "
+                      f"{t:.1f} s"}
+
+
+def run_reference(args):
+    rank, _, world = dist_info()
+    if rank != 0:
+        return 0
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import ref_runner
+    if not ref_runner.reference_available():
+        print(json.dumps({"impl": "reference", "unavailable": "reference build oracle/_ref missing"}))
+        return 0
+    wl = build_workload(REF_RES)
+    W, H = wl.resolution
+    for i in range(args.warmup):
+        reference_step(wl, 100 + i)
+    ts = [reference_step(wl, i) for i in range(args.steps)]
+    total = sum(ts)
+    samples = W * H * wl.spp
+    value = samples * args.steps / total
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps, "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scene)",
+            "impl": "reference",
+            "config": {"workload": "soft_shadow 512x512 16spp max_bounces=1 (reference timed on a "
+                                   f"{W}x{H} slice)", "resolution": [W, H], "spp": wl.spp,
+                       "max_bounces": wl.max_bounces, "l2": "n/a (CPU)"},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
+                             "sample": f"{W}x{H} x {wl.spp} spp per step (forward + backward calls)"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
+    print(json.dumps(line))
+    return 0
+
+
+# ---------------------------------------------------------------------------
+# B200 arm
+# ---------------------------------------------------------------------------
+def run_b200(args):
+    import numpy as np
+    import torch
+    from delta_ray_b200 import RenderFunction, _abi
+    from delta_ray_b200.render_pytorch import Scene
+
+    rank, local_rank, world = dist_info()
+    dist = None
+    if world > 1:
+        import torch.distributed as dist
+        torch.cuda.set_device(local_rank)
+        dist.init_process_group("nccl", timeout=__import__("datetime").timedelta(seconds=120))
+    dev = torch.device("cuda", local_rank)
+    torch.cuda.set_device(dev)
+
+    wl = build_workload()
+    W, H = wl.resolution
+    spp, B = wl.spp, wl.max_bounces
+    samples = W * H * spp
+    cam, mats, shps, lts = _abi.scene_dicts(wl.camera, wl.materials, wl.shapes, wl.lights)
+    scene = Scene(cam, mats, shps, lts, local_rank)
+    d_img = torch.ones((H, W, 3), dtype=torch.float32, device=dev)
+    flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)  # 256 MB > 126 MB L2
+
+    def step(seed):
+        scene.forward(W, H, spp, B, seed)
+        scene.backward(W, H, spp, B, seed, d_img)
+
+    for i in range(args.warmup):
+        step(1000 + i)
+    # per-stage profile (untimed): stage times and work counts for the roofline
+    scene.set_profiling(True)
+    scene.forward(W, H, spp, B, 7)
+    stages = list(scene.last_timings())
+    scene.backward(W, H, spp, B, 7, d_img)
+    stages += scene.last_timings()
+    counts = scene.last_counts()
+    scene.set_profiling(False)
+    launches_per_step = 0
+    scene.forward(W, H, spp, B, 8)
+    launches_per_step += scene.launch_count()
+    scene.backward(W, H, spp, B, 8, d_img)
+    launches_per_step += scene.launch_count()
+
+    clocks = ClockSampler(local_rank)
+    if dist:
+        dist.barrier()
+    torch.cuda.synchronize()
+    clocks.start()
+    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
+    for k in range(args.steps):
+        flush.zero_()  # L2 flush between timed steps (outside the events)
+        ev[k][0].record()
+        step(k)
+        ev[k][1].record()
+    torch.cuda.synchronize()
+    if dist:
+        dist.barrier()
+    clk = clocks.stop()
+    total_ms = sum(a.elapsed_time(b) for a, b in ev)
+    t = torch.tensor([total_ms], device=dev)
+    if dist:
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    total_ms = float(t.item())
+    ms_per_step = total_ms / args.steps
+    value = world * samples / (ms_per_step / 1e3)
+
+    # end to end through the public API with host tensors: upload, scene build,
+    # forward, loss read-back, backward, gradients back to the host
+    wl_e2e = build_workload()
+    wl_e2e.shapes[1].vertices.requires_grad_(True)
+    wl_e2e.lights[0].intensity.requires_grad_(True)
+    wl_e2e.materials[0].diffuse_reflectance.requires_grad_(True)
+    args_e2e = wl_e2e.serialize()
+    h2d = sum(a.numel() * a.element_size() for a in args_e2e if torch.is_tensor(a))
+    d2h = 4 + sum(x.numel() * x.element_size() for x in (wl_e2e.shapes[1].vertices, wl_e2e.lights[0].intensity,
+                                                           wl_e2e.materials[0].diffuse_reflectance))
+
+    def e2e_step(seed):
+        for x in (wl_e2e.shapes[1].vertices, wl_e2e.lights[0].intensity, wl_e2e.materials[0].diffuse_reflectance):
+            x.grad = None
+        img = RenderFunction.apply(seed, *args_e2e)
+        loss = img.sum()
+        loss.item()
+        loss.backward()
+    for i in range(2):
+        e2e_step(500 + i)
+    torch.cuda.synchronize()
+    e2e_steps = max(3, min(args.steps, 5))
+    t0 = time.perf_counter()
+    for k in range(e2e_steps):
+        e2e_step(600 + k)
+    torch.cuda.synchronize()
+    e2e_s = (time.perf_counter() - t0) / e2e_steps
+    e2e_t = torch.tensor([e2e_s], device=dev)
+    if dist:
+        dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
+    e2e_value = world * samples / float(e2e_t.item())
+
+    # roofline of the dominant stage
+    peak, peak_kind = load_peaks()
+    dom = max(stages, key=lambda s: s[1]) if stages else ("", 0.0)
+    dom_bytes = stage_bytes(dom[0], wl, counts)
+    achieved = dom_bytes / (dom[1] / 1e3) / 1e9 if dom[1] > 0 else 0.0
+    roofline = {"bound": "hbm", "kernel": dom[0], "achieved": achieved, "peak": peak, "unit": "GB/s",
+                "frac": achieved / peak, "peak_kind": peak_kind, "traffic": load_traffic(dom[0]),
+                "algorithmic_bytes_per_launch": dom_bytes,
+                "stage_ms": {n: round(ms, 4) for n, ms in stages},
+                "points": counts[0], "edge_items": counts[1]}
+
+    line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
+            "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scene)",
+            "config": {"workload": "soft_shadow 512x512 16spp max_bounces=1 fwd+bwd",
+                       "resolution": [W, H], "spp": spp, "max_bounces": B, "triangles": wl.num_triangles,
+                       "parallelism": f"replicas x{world}", "l2": "flushed between steps (256 MB write)"},
+            "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
+            "gpu_launches": launches_per_step * args.steps, "roofline": roofline, "clocks": clk}
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        try:
+            line["cpu_baseline"] = cpu_baseline()
+        except Exception as e:  # baseline is informative only
+            line["cpu_baseline"] = {"unavailable": str(e)[:200]}
+    if rank == 0:
+        print(json.dumps(line))
+    scene.close()
+    if dist:
+        dist.destroy_process_group()
+    return 0
+
+
+def main():
+    args = parse()
+    if args.impl == "reference":
+        return run_reference(args)
+    return run_b200(args)
+
+
+if __name__ == "__main__":
+    sys.exit(main())

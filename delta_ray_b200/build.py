@@ -16,6 +16,9 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libdr_b200.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
+# The backward kernels keep IEEE operation order (no FMA contraction) so that
+# edge-sampling decisions see the same bits as the reference's CPU arithmetic.
+PER_FILE_FLAGS = {"dr_backward.cu": ["-fmad=false"]}
 NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr", "-Xcompiler", "-fPIC",
               "-Xcompiler", "-fvisibility=hidden", "-I", os.path.join(ROOT, "include")]
 
@@ -47,7 +50,8 @@ def build(verbose=False, extra_flags=()):
         obj = os.path.join(objdir, os.path.basename(src) + ".o")
         objs.append(obj)
         if _stale(obj, [src] + hdrs + [__file__]):
-            cmd = [nvcc, *ARCH, *NVCC_FLAGS, *extra_flags, "-c", src, "-o", obj]
+            cmd = [nvcc, *ARCH, *NVCC_FLAGS, *PER_FILE_FLAGS.get(os.path.basename(src), []), *extra_flags,
+                   "-c", src, "-o", obj]
             if verbose:
                 print(" ".join(cmd))
             procs.append((src, subprocess.Popen(cmd, stdout=subprocess.PIPE, stderr=subprocess.STDOUT)))

@@ -7,6 +7,7 @@
 // silhouettes clipped to the screen, and the two median-split edge trees.  It
 // runs once per scene (the reference reruns it twice per optimisation step).
 #include "../../include/delta_ray_b200.h"
+#include "dr_host_scene.h"
 #include "dr_kernels.h"
 
 #include <algorithm>
@@ -71,409 +72,9 @@ template <typename T> std::vector<T> fetch(const T *src, size_t count, const cha
     return v;
 }
 
-// ---- small host vector helpers (same float expressions as the device) ----
-struct V3 { float x, y, z; };
-inline V3 v3(float x, float y, float z) { return V3{x, y, z}; }
-inline V3 operator+(V3 a, V3 b) { return v3(a.x + b.x, a.y + b.y, a.z + b.z); }
-inline V3 operator-(V3 a, V3 b) { return v3(a.x - b.x, a.y - b.y, a.z - b.z); }
-inline V3 operator-(V3 a) { return v3(-a.x, -a.y, -a.z); }
-inline V3 operator*(V3 a, float s) { return v3(a.x * s, a.y * s, a.z * s); }
-inline V3 operator*(float s, V3 a) { return v3(s * a.x, s * a.y, s * a.z); }
-inline V3 operator/(V3 a, float s) { float i = 1.f / s; return a * i; }
-inline float dot(V3 a, V3 b) { return a.x * b.x + a.y * b.y + a.z * b.z; }
-inline V3 cross(V3 a, V3 b) { return v3(a.y * b.z - a.z * b.y, a.z * b.x - a.x * b.z, a.x * b.y - a.y * b.x); }
-inline float length(V3 a) { return std::sqrt(a.x * a.x + a.y * a.y + a.z * a.z); }
-inline V3 normalize(V3 a) { return a / length(a); }
-inline float get(V3 a, int i) { return i == 0 ? a.x : (i == 1 ? a.y : a.z); }
-inline void set(V3 &a, int i, float v) { if (i == 0) a.x = v; else if (i == 1) a.y = v; else a.z = v; }
-inline float luminance(V3 a) { return 0.212671f * a.x + 0.715160f * a.y + 0.072169f * a.z; }
-
-struct HAABB {
-    V3 lo{INFINITY, INFINITY, INFINITY}, hi{-INFINITY, -INFINITY, -INFINITY};
-    void add(V3 p) {
-        lo = v3(std::min(lo.x, p.x), std::min(lo.y, p.y), std::min(lo.z, p.z));
-        hi = v3(std::max(hi.x, p.x), std::max(hi.y, p.y), std::max(hi.z, p.z));
-    }
-    void add(const HAABB &b) { add(b.lo); add(b.hi); }
-};
-
-struct HCam {
-    float c2w[16], w2c[16];
-    float fov, aspect, clip_near;
-    bool fisheye;
-};
-
-V3 xfm_point(const float *M, V3 p) {
-    float t0 = M[0] * p.x + M[1] * p.y + M[2] * p.z + M[3];
-    float t1 = M[4] * p.x + M[5] * p.y + M[6] * p.z + M[7];
-    float t2 = M[8] * p.x + M[9] * p.y + M[10] * p.z + M[11];
-    float t3 = M[12] * p.x + M[13] * p.y + M[14] * p.z + M[15];
-    float inv_w = 1.f / t3;
-    return v3(t0, t1, t2) * inv_w;
-}
-
-struct V2 { float x, y; };
-
-V2 project_local(const HCam &c, V3 l) {
-    if (c.fisheye) {
-        V3 d = normalize(l);
-        float phi = std::atan2(d.y, d.x), theta = std::acos(d.z), r = theta * 2.f / DR_PI;
-        return V2{0.5f * (-r * std::cos(phi) + 1.f), 0.5f * (-r * std::sin(phi) + 1.f)};
-    }
-    return V2{(-l.x / (l.z * c.fov) + 1.f) * 0.5f, (-l.y / (l.z * c.fov * c.aspect) + 1.f) * 0.5f};
-}
-
-// camera.h:216-242
-bool project(const HCam &c, V3 p0, V3 p1, V2 *s0, V2 *s1) {
-    V3 a = xfm_point(c.w2c, p0), b = xfm_point(c.w2c, p1);
-    if (a.z < c.clip_near && b.z < c.clip_near) return false;
-    if (a.z < c.clip_near) {
-        V3 dir = a - b;
-        float t = -(b.z - c.clip_near) / dir.z;
-        a = b + t * dir;
-    } else if (b.z < c.clip_near) {
-        V3 dir = b - a;
-        float t = -(a.z - c.clip_near) / dir.z;
-        b = a + t * dir;
-    }
-    *s0 = project_local(c, a);
-    *s1 = project_local(c, b);
-    return true;
-}
-
-// Cohen-Sutherland clip to [0,1]^2 (line_clip.h:13-102)
-bool clip_line(V2 a, V2 b, V2 *oa, V2 *ob) {
-    auto code = [](V2 v) {
-        int c = 0;
-        if (v.x < 0.f) c |= 1; else if (v.x > 1.f) c |= 2;
-        if (v.y < 0.f) c |= 4; else if (v.y > 1.f) c |= 8;
-        return c;
-    };
-    int c0 = code(a), c1 = code(b);
-    for (int guard = 0; guard < 64; guard++) {
-        if (!(c0 | c1)) { *oa = a; *ob = b; return true; }
-        if (c0 & c1) return false;
-        int out = c0 ? c0 : c1;
-        V2 v{0.f, 0.f};
-        if (out & 8) { v.x = a.x + (b.x - a.x) * (1.f - a.y) / (b.y - a.y); v.y = 1.f; }
-        else if (out & 4) { v.x = a.x + (b.x - a.x) * (0.f - a.y) / (b.y - a.y); v.y = 0.f; }
-        else if (out & 2) { v.y = a.y + (b.y - a.y) * (1.f - a.x) / (b.x - a.x); v.x = 1.f; }
-        else { v.y = a.y + (b.y - a.y) * (0.f - a.x) / (b.x - a.x); v.x = 0.f; }
-        if (out == c0) { a = v; c0 = code(a); } else { b = v; c1 = code(b); }
-    }
-    return false;
-}
-
-struct HShape {
-    std::vector<float> v, n, uv;
-    std::vector<int> idx;
-    int nv = 0, nt = 0, mat = 0, light = -1;
-    V3 vtx(int i) const { return v3(v[3 * i], v[3 * i + 1], v[3 * i + 2]); }
-    V3 nrm(int i) const { return v3(n[3 * i], n[3 * i + 1], n[3 * i + 2]); }
-    V3 face_normal(int t) const {
-        V3 a = vtx(idx[3 * t]), b = vtx(idx[3 * t + 1]), c = vtx(idx[3 * t + 2]);
-        return normalize(cross(b - a, c - a));
-    }
-};
-
-// pbrt Distribution1D (distribution.h:7-36)
-struct HDist {
-    std::vector<float> func, cdf;
-    float func_int = 0.f;
-    void build(const std::vector<float> &f) {
-        int n = (int)f.size();
-        func = f;
-        cdf.assign(n + 1, 0.f);
-        for (int i = 1; i <= n; i++) cdf[i] = cdf[i - 1] + func[i - 1] / n;
-        func_int = cdf[n];
-        for (int i = 1; i <= n; i++) cdf[i] = func_int == 0.f ? float(i) / float(n) : cdf[i] / func_int;
-    }
-};
-
-struct PrimInfo {
-    int prim;
-    V3 n0, n1, sc, dc;
-    HAABB sb, db;
-};
-
-struct BuildNode {
-    HAABB sb;
-    V3 axis;
-    float angle;
-    int first = 0, n = 0;
-    std::unique_ptr<BuildNode> c[2];
-};
-
-struct HostScene;
-
-// edge_tree.cpp:49-173 (median split; std::nth_element with the same
-// comparator so that equal centroids resolve as in the reference)
-template <bool DIR>
-std::unique_ptr<BuildNode> build_node(const std::vector<DevEdge> &edges, std::vector<PrimInfo> &pi, int start, int end,
-                                      int *total, std::vector<DevEdge> &ordered) {
-    auto node = std::make_unique<BuildNode>();
-    (*total)++;
-    HAABB sb;
-    for (int i = start; i < end; i++) sb.add(pi[i].sb);
-    V3 nsum = v3(0.f, 0.f, 0.f);
-    for (int i = start; i < end; i++) nsum = nsum + pi[i].n0 + pi[i].n1;
-    V3 axis = normalize(nsum);
-    float cmin = 1.f;
-    for (int i = start; i < end; i++) {
-        cmin = std::min(cmin, dot(pi[i].n0, axis));
-        cmin = std::min(cmin, dot(pi[i].n1, axis));
-    }
-    node->sb = sb;
-    node->axis = axis;
-    node->angle = std::acos(cmin);
-    int n = end - start;
-    auto leaf = [&]() {
-        node->first = (int)ordered.size();
-        for (int i = start; i < end; i++) ordered.push_back(edges[pi[i].prim]);
-        node->n = n;
-    };
-    if (n == 1) {
-        leaf();
-        return node;
-    }
-    HAABB scb, dcb;
-    for (int i = start; i < end; i++) {
-        scb.add(pi[i].sc);
-        if (DIR) dcb.add(pi[i].dc);
-    }
-    int dim = -1;
-    float maxe = -INFINITY;
-    for (int a = 0; a < 3; a++) {
-        float e = get(scb.hi, a) - get(scb.lo, a);
-        if (e > maxe) { dim = a; maxe = e; }
-    }
-    if (DIR) {
-        for (int a = 0; a < 3; a++) {
-            float e = get(dcb.hi, a) - get(dcb.lo, a);
-            if (e > maxe) { dim = a + 3; maxe = e; }
-        }
-    }
-    const HAABB &cb = dim < 3 ? scb : dcb;
-    bool spatial = dim < 3;
-    if (dim >= 3) dim -= 3;
-    if (get(cb.hi, dim) == get(cb.lo, dim)) {
-        leaf();
-        return node;
-    }
-    int mid = (start + end) / 2;
-    std::nth_element(&pi[start], &pi[mid], &pi[end - 1] + 1, [dim, spatial](const PrimInfo &a, const PrimInfo &b) {
-        return spatial ? get(a.sc, dim) < get(b.sc, dim) : get(a.dc, dim) < get(b.dc, dim);
-    });
-    node->c[0] = build_node<DIR>(edges, pi, start, mid, total, ordered);
-    node->c[1] = build_node<DIR>(edges, pi, mid, end, total, ordered);
-    return node;
-}
-
-struct HostScene {
-    HCam cam;
-    std::vector<HShape> shapes;
-    std::vector<DevMaterial> mats;
-    std::vector<float> texels;
-    std::vector<DevLight> lights;
-    std::vector<float> light_tri_cdf, light_tri_func;
-    HDist light_sel;
-    float total_light_intensity = 0.f;
-    std::vector<DevEdge> prim_edges;
-    HDist prim_dist;
-    std::vector<DevEdgeNode> sil_nodes, nrm_nodes;
-    std::vector<DevEdge> sil_edges, nrm_edges;
-    std::vector<float> ltc;
-    size_t grad_total = 0;
-    std::vector<size_t> grad_mat, grad_vtx, grad_nrm, grad_light;
-
-    V3 ev0(const DevEdge &e) const { return shapes[e.shape].vtx(e.v0); }
-    V3 ev1(const DevEdge &e) const { return shapes[e.shape].vtx(e.v1); }
-
-    V3 non_shared(const DevEdge &e, int f) const {
-        const HShape &s = shapes[e.shape];
-        for (int i = 0; i < 3; i++) {
-            int v = s.idx[3 * f + i];
-            if (v != e.v0 && v != e.v1) return s.vtx(v);
-        }
-        return v3(0.f, 0.f, 0.f);
-    }
-    // edge.h:59-79
-    bool is_silhouette(V3 p, const DevEdge &e) const {
-        if (shapes[e.shape].n.empty()) return true;
-        if (e.f0 == -1 || e.f1 == -1) return true;
-        V3 v0 = ev0(e), v1 = ev1(e), a = non_shared(e, e.f0), b = non_shared(e, e.f1);
-        V3 n0 = normalize(cross(v0 - a, v1 - a)), n1 = normalize(cross(v1 - b, v0 - b));
-        bool f0 = dot(p - v0, n0) > 0.f && dot(p - v1, n0) > 0.f && dot(p - a, n0) > 0.f;
-        bool f1 = dot(p - v0, n1) > 0.f && dot(p - v1, n1) > 0.f && dot(p - b, n1) > 0.f;
-        return (f0 && !f1) || (!f0 && f1);
-    }
-
-    int flatten(std::vector<DevEdgeNode> &nodes, const std::vector<DevEdge> &ordered, const BuildNode *b, int *off) {
-        int my = (*off)++;
-        DevEdgeNode &ln = nodes[my];
-        ln.lo[0] = b->sb.lo.x; ln.lo[1] = b->sb.lo.y; ln.lo[2] = b->sb.lo.z;
-        ln.hi[0] = b->sb.hi.x; ln.hi[1] = b->sb.hi.y; ln.hi[2] = b->sb.hi.z;
-        ln.axis[0] = b->axis.x; ln.axis[1] = b->axis.y; ln.axis[2] = b->axis.z;
-        ln.angle = b->angle;
-        ln.pad = 0;
-        if (b->n > 0) {
-            ln.offset = b->first;
-            ln.nprims = b->n;
-            float tl = 0.f;
-            for (int i = 0; i < b->n; i++) {
-                const DevEdge &e = ordered[b->first + i];
-                tl += length(ev1(e) - ev0(e));
-            }
-            ln.total_length = tl;
-        } else {
-            nodes[my].nprims = 0;
-            flatten(nodes, ordered, b->c[0].get(), off);
-            int second = flatten(nodes, ordered, b->c[1].get(), off);
-            nodes[my].offset = second;
-            nodes[my].total_length = nodes[my + 1].total_length + nodes[second].total_length;
-        }
-        return my;
-    }
-
-    template <bool DIR> void build_tree(const std::vector<DevEdge> &edges, std::vector<DevEdgeNode> &nodes,
-                                        std::vector<DevEdge> &ordered) {
-        nodes.clear();
-        ordered.clear();
-        if (edges.empty()) return;
-        std::vector<PrimInfo> pi(edges.size());
-        HAABB world;
-        for (size_t i = 0; i < edges.size(); i++) {
-            HAABB b;
-            b.add(ev0(edges[i]));
-            b.add(ev1(edges[i]));
-            pi[i].prim = (int)i;
-            pi[i].sb = b;
-            pi[i].sc = 0.5f * b.lo + 0.5f * b.hi;
-            pi[i].n0 = pi[i].n1 = v3(0.f, 0.f, 0.f);
-            world.add(b);
-        }
-        if (DIR) {
-            float factor = length(world.hi - world.lo) / 8.f;
-            for (size_t i = 0; i < edges.size(); i++) {
-                const DevEdge &e = edges[i];
-                const HShape &sh = shapes[e.shape];
-                V3 sn = normalize(sh.nrm(e.v0) + sh.nrm(e.v1));
-                V3 n0 = sh.face_normal(e.f0), n1 = sh.face_normal(e.f1);
-                if (dot(n0, sn) < 0.f) n0 = -n0;
-                if (dot(n1, sn) < 0.f) n1 = -n1;
-                pi[i].n0 = n0;
-                pi[i].n1 = n1;
-                HAABB d;
-                d.add(n0 * factor);
-                d.add(n1 * factor);
-                pi[i].db = d;
-                pi[i].dc = 0.5f * (d.lo + d.hi);
-            }
-        }
-        int total = 0;
-        auto root = build_node<DIR>(edges, pi, 0, (int)edges.size(), &total, ordered);
-        nodes.resize(total);
-        int off = 0;
-        flatten(nodes, ordered, root.get(), &off);
-    }
-
-    void preprocess() {
-        // lights (scene.cpp:26-52)
-        std::vector<float> imp;
-        total_light_intensity = 0.f;
-        light_tri_cdf.clear();
-        light_tri_func.clear();
-        for (size_t li = 0; li < lights.size(); li++) {
-            DevLight &L = lights[li];
-            float lum = luminance(v3(L.I[0], L.I[1], L.I[2]));
-            imp.push_back(lum);
-            total_light_intensity += lum;
-            const HShape &sh = shapes[L.shape];
-            std::vector<float> areas;
-            HAABB b;
-            float asum = 0.f;
-            for (int t = 0; t < sh.nt; t++) {
-                V3 a = sh.vtx(sh.idx[3 * t]), bb = sh.vtx(sh.idx[3 * t + 1]), cc = sh.vtx(sh.idx[3 * t + 2]);
-                float ar = 0.5f * length(cross(bb - a, cc - a));
-                asum += ar;
-                areas.push_back(ar);
-                b.add(a);
-                b.add(bb);
-                b.add(cc);
-            }
-            HDist d;
-            d.build(areas);
-            L.cdf_off = (int)light_tri_cdf.size();
-            L.ntri = sh.nt;
-            L.func_int = d.func_int;
-            L.area = asum;
-            V3 c = (b.lo + b.hi) / 2.f;
-            L.bc[0] = c.x; L.bc[1] = c.y; L.bc[2] = c.z;
-            V3 dd = b.hi - c;
-            L.br = length(dd);
-            light_tri_cdf.insert(light_tri_cdf.end(), d.cdf.begin(), d.cdf.end());
-            light_tri_func.insert(light_tri_func.end(), d.func.begin(), d.func.end());
-            light_tri_func.push_back(0.f);  // keep func and cdf offsets aligned (ntri + 1 slots)
-        }
-        if (!imp.empty()) light_sel.build(imp);
-        // unique edges in (shape, v0, v1) order (scene.cpp:54-97)
-        std::map<std::tuple<int, int, int>, DevEdge> emap;
-        for (int si = 0; si < (int)shapes.size(); si++) {
-            const HShape &sh = shapes[si];
-            for (int t = 0; t < sh.nt; t++) {
-                int ind[3] = {sh.idx[3 * t], sh.idx[3 * t + 1], sh.idx[3 * t + 2]};
-                for (int k = 0; k < 3; k++) {
-                    int a = ind[k], b = ind[(k + 1) % 3];
-                    if (a > b) std::swap(a, b);
-                    auto key = std::make_tuple(si, a, b);
-                    auto it = emap.find(key);
-                    if (it == emap.end()) emap[key] = DevEdge{si, a, b, t, -1};
-                    else it->second.f1 = t;
-                }
-            }
-        }
-        std::vector<DevEdge> edges;
-        for (auto &kv : emap) {
-            const DevEdge &e = kv.second;
-            V3 d = ev0(e) - ev1(e);
-            if (std::fabs(d.x) + std::fabs(d.y) + std::fabs(d.z) < 1e-10f) continue;
-            if (e.f1 != -1) {
-                float ang = std::fabs(dot(shapes[e.shape].face_normal(e.f0), shapes[e.shape].face_normal(e.f1)));
-                if (ang == 1.f || ang == -1.f) continue;
-            }
-            edges.push_back(e);
-        }
-        // primary edges (edge_tree.cpp:263-294)
-        prim_edges.clear();
-        std::vector<float> lens;
-        V3 org = xfm_point(cam.c2w, v3(0.f, 0.f, 0.f));
-        for (const DevEdge &e : edges) {
-            V2 a, b;
-            float dist = 0.f;
-            if (project(cam, ev0(e), ev1(e), &a, &b)) {
-                V2 ca, cb;
-                if (clip_line(a, b, &ca, &cb))
-                    dist = std::sqrt((cb.x - ca.x) * (cb.x - ca.x) + (cb.y - ca.y) * (cb.y - ca.y));
-            }
-            if (!is_silhouette(org, e)) dist = 0.f;
-            if (dist > 0.f) {
-                prim_edges.push_back(e);
-                lens.push_back(dist);
-            }
-        }
-        prim_dist = HDist();
-        if (!lens.empty()) prim_dist.build(lens);
-        std::vector<DevEdge> sil, nrm;
-        for (const DevEdge &e : edges) {
-            if (e.f0 == -1 || e.f1 == -1 || shapes[e.shape].n.empty()) sil.push_back(e);
-            else nrm.push_back(e);
-        }
-        build_tree<false>(sil, sil_nodes, sil_edges);
-        build_tree<true>(nrm, nrm_nodes, nrm_edges);
-    }
-};
-
 }  // namespace
+
+using namespace drhost;
 
 struct dr_scene {
     int device = 0;
@@ -484,177 +85,33 @@ struct dr_scene {
     // backward workspace (grown on demand)
     DevBuf ws_pt, ws_items, ws_item_w, ws_item_dp, ws_pt_last, ws_counts;
     DevScene ds;
-    int num_vertices = 0, num_tris = 0;
+    StageTimer timer;
+    bool timer_ready = false;
+    std::vector<std::pair<std::string, float>> timings;
+    long long last_points = 0, last_items = 0;
+    int num_vertices = 0, num_tris = 0, num_sms = 148;
+    ~dr_scene() {
+        if (timer_ready)
+            for (int i = 0; i <= StageTimer::kMax; i++) cudaEventDestroy(timer.ev[i]);
+    }
     int last_launches = 0;
-    std::vector<size_t> layout_mat, layout_vtx, layout_nrm, layout_light;
 };
 
 namespace {
 
-// Blinn-Phong LTC table used when the caller supplies none: isotropic
-// identity matrices, i.e. edges are importance-sampled by the cosine lobe.
-std::vector<float> default_ltc() {
-    std::vector<float> t(128 * 128 * 9, 0.f);
-    for (int i = 0; i < 128 * 128; i++) t[9 * i] = t[9 * i + 4] = t[9 * i + 8] = 1.f;
-    return t;
-}
-
-void load_desc(dr_scene *sc, const dr_scene_desc *d) {
-    if (!d) throw DrError(DR_ERR_INVALID_ARGUMENT, "scene descriptor is NULL");
-    if (d->num_shapes < 0 || d->num_materials < 0 || d->num_lights < 0)
-        throw DrError(DR_ERR_INVALID_ARGUMENT, "negative count in scene descriptor");
-    HostScene &h = sc->h;
-    h = HostScene();
-    auto m16 = [&](const float *p, float *dst, const char *what) {
-        auto v = fetch(p, 16, what);
-        std::memcpy(dst, v.data(), 64);
-    };
-    m16(d->camera.cam_to_world, h.cam.c2w, "cam_to_world");
-    m16(d->camera.world_to_cam, h.cam.w2c, "world_to_cam");
-    h.cam.fov = d->camera.fov_factor;
-    h.cam.aspect = d->camera.aspect_ratio;
-    h.cam.clip_near = d->camera.clip_near;
-    h.cam.fisheye = d->camera.fisheye != 0;
-    size_t g = 64;
-    for (int i = 0; i < d->num_materials; i++) {
-        const dr_material_desc &m = d->materials[i];
-        DevMaterial dm;
-        std::memset(&dm, 0, sizeof(dm));
-        auto channel = [&](const float *p, int w, int hh, int ch, float *cval, int *tex, int *ow, int *oh,
-                           int *grad, const char *what) {
-            if (w < 0 || hh < 0 || (w == 0) != (hh == 0)) throw DrError(DR_ERR_INVALID_ARGUMENT, what);
-            *grad = (int)g;
-            if (w == 0) {
-                auto v = fetch(p, ch, what);
-                for (int c = 0; c < ch; c++) cval[c] = v[c];
-                *tex = -1;
-                *ow = *oh = 0;
-                g += ch;
-            } else {
-                auto v = fetch(p, (size_t)w * hh * ch, what);
-                *tex = (int)h.texels.size();
-                h.texels.insert(h.texels.end(), v.begin(), v.end());
-                *ow = w;
-                *oh = hh;
-                g += (size_t)w * hh * ch;
-            }
-        };
-        channel(m.diffuse, m.diffuse_w, m.diffuse_h, 3, dm.kd, &dm.tex_kd, &dm.kd_w, &dm.kd_h, &dm.grad_kd, "diffuse");
-        channel(m.specular, m.specular_w, m.specular_h, 3, dm.ks, &dm.tex_ks, &dm.ks_w, &dm.ks_h, &dm.grad_ks,
-                "specular");
-        channel(m.roughness, m.roughness_w, m.roughness_h, 1, &dm.rough, &dm.tex_r, &dm.r_w, &dm.r_h, &dm.grad_r,
-                "roughness");
-        auto uvs = [&](const float *p, float *dst, const char *what) {
-            auto v = fetch(p, 2, what);
-            dst[0] = v[0];
-            dst[1] = v[1];
-        };
-        uvs(m.diffuse_uv_scale, dm.uv_kd, "diffuse_uv_scale");
-        uvs(m.specular_uv_scale, dm.uv_ks, "specular_uv_scale");
-        uvs(m.roughness_uv_scale, dm.uv_r, "roughness_uv_scale");
-        dm.two_sided = m.two_sided != 0;
-        h.mats.push_back(dm);
-        sc->layout_mat.push_back((size_t)dm.grad_kd);
-        sc->layout_mat.push_back((size_t)dm.grad_ks);
-        sc->layout_mat.push_back((size_t)dm.grad_r);
-    }
-    for (int i = 0; i < d->num_shapes; i++) {
-        const dr_shape_desc &s = d->shapes[i];
-        if (s.num_vertices < 0 || s.num_triangles < 0) throw DrError(DR_ERR_INVALID_ARGUMENT, "negative mesh size");
-        if (s.material_id < 0 || s.material_id >= d->num_materials)
-            throw DrError(DR_ERR_INVALID_ARGUMENT, "shape material_id out of range");
-        HShape hs;
-        hs.nv = s.num_vertices;
-        hs.nt = s.num_triangles;
-        hs.mat = s.material_id;
-        hs.v = fetch(s.vertices, 3 * (size_t)hs.nv, "vertices");
-        hs.idx = fetch(s.indices, 3 * (size_t)hs.nt, "indices");
-        for (int v : hs.idx)
-            if (v < 0 || v >= hs.nv) throw DrError(DR_ERR_INVALID_ARGUMENT, "triangle index out of range");
-        if (s.uvs) hs.uv = fetch(s.uvs, 2 * (size_t)hs.nv, "uvs");
-        if (s.normals) hs.n = fetch(s.normals, 3 * (size_t)hs.nv, "normals");
-        sc->layout_vtx.push_back(g);
-        g += 3 * (size_t)hs.nv;
-        if (s.normals) {
-            sc->layout_nrm.push_back(g);
-            g += 3 * (size_t)hs.nv;
-        } else {
-            sc->layout_nrm.push_back((size_t)-1);
-        }
-        h.shapes.push_back(std::move(hs));
-    }
-    for (int i = 0; i < d->num_lights; i++) {
-        const dr_light_desc &l = d->lights[i];
-        if (l.shape_id < 0 || l.shape_id >= d->num_shapes)
-            throw DrError(DR_ERR_INVALID_ARGUMENT, "light shape_id out of range");
-        DevLight L;
-        std::memset(&L, 0, sizeof(L));
-        L.shape = l.shape_id;
-        auto I = fetch(l.intensity, 3, "intensity");
-        L.I[0] = I[0]; L.I[1] = I[1]; L.I[2] = I[2];
-        L.grad = (int)g;
-        sc->layout_light.push_back(g);
-        g += 3;
-        h.shapes[L.shape].light = i;
-        h.lights.push_back(L);
-    }
-    h.grad_total = g;
-    if (g > (size_t)0x7fffffff) throw DrError(DR_ERR_INVALID_ARGUMENT, "scene too large for 32-bit gradient offsets");
-    h.ltc = d->ltc_table ? fetch(d->ltc_table, 128 * 128 * 9, "ltc_table") : default_ltc();
-}
-
 void upload_scene(dr_scene *sc, cudaStream_t st) {
     HostScene &h = sc->h;
     check_cuda(cudaSetDevice(sc->device), "cudaSetDevice");
-    std::vector<float> vtx, nrm, uv;
-    std::vector<int4> tri;
-    std::vector<int> tri_local;
-    std::vector<DevShape> shapes;
-    bool any_n = false, any_uv = false;
-    for (auto &s : h.shapes) { any_n |= !s.n.empty(); any_uv |= !s.uv.empty(); }
-    HAABB bounds;
-    for (int si = 0; si < (int)h.shapes.size(); si++) {
-        const HShape &s = h.shapes[si];
-        DevShape ds;
-        ds.vtx_off = (int)(vtx.size() / 3);
-        ds.tri_off = (int)tri.size();
-        ds.nv = s.nv;
-        ds.nt = s.nt;
-        ds.mat = s.mat;
-        ds.light = s.light;
-        ds.has_uv = !s.uv.empty();
-        ds.has_n = !s.n.empty();
-        ds.grad_v = (int)sc->layout_vtx[si];
-        ds.grad_n = sc->layout_nrm[si] == (size_t)-1 ? -1 : (int)sc->layout_nrm[si];
-        vtx.insert(vtx.end(), s.v.begin(), s.v.end());
-        if (any_n) {
-            if (ds.has_n) nrm.insert(nrm.end(), s.n.begin(), s.n.end());
-            else nrm.insert(nrm.end(), 3 * (size_t)s.nv, 0.f);
-        }
-        if (any_uv) {
-            if (ds.has_uv) uv.insert(uv.end(), s.uv.begin(), s.uv.end());
-            else uv.insert(uv.end(), 2 * (size_t)s.nv, 0.f);
-        }
-        for (int t = 0; t < s.nt; t++) {
-            int4 q;
-            q.x = ds.vtx_off + s.idx[3 * t];
-            q.y = ds.vtx_off + s.idx[3 * t + 1];
-            q.z = ds.vtx_off + s.idx[3 * t + 2];
-            q.w = si;
-            tri.push_back(q);
-            tri_local.push_back(t);
-        }
-        for (int i = 0; i < s.nv; i++) bounds.add(s.vtx(i));
-        shapes.push_back(ds);
-    }
-    sc->num_vertices = (int)(vtx.size() / 3);
-    sc->num_tris = (int)tri.size();
-    sc->vtx.upload(vtx);
-    sc->nrm.upload(nrm);
-    sc->uv.upload(uv);
-    sc->tri.upload(tri);
-    sc->tri_local.upload(tri_local);
-    sc->shapes.upload(shapes);
+    FlatScene f;
+    flatten(h, f);
+    sc->num_vertices = (int)(f.vtx.size() / 3);
+    sc->num_tris = (int)f.tri.size();
+    sc->vtx.upload(f.vtx);
+    sc->nrm.upload(f.nrm);
+    sc->uv.upload(f.uv);
+    sc->tri.upload(f.tri);
+    sc->tri_local.upload(f.tri_local);
+    sc->shapes.upload(f.shapes);
     sc->mats.upload(h.mats);
     sc->texels.upload(h.texels);
     sc->lights.upload(h.lights);
@@ -678,59 +135,69 @@ void upload_scene(dr_scene *sc, cudaStream_t st) {
     if (n > 0) {
         size_t sb = dr_lbvh_scratch_bytes(n);
         sc->bvh_scratch.reserve(sb);
-        float3 lo, hi;
-        lo.x = bounds.lo.x; lo.y = bounds.lo.y; lo.z = bounds.lo.z;
-        hi.x = bounds.hi.x; hi.y = bounds.hi.y; hi.z = bounds.hi.z;
-        check_cuda(dr_build_lbvh(sc->vtx.as<float>(), sc->tri.as<int4>(), n, lo, hi, sc->bvh_nodes.as<float4>(),
+        check_cuda(dr_build_lbvh(sc->vtx.as<float>(), sc->tri.as<int4>(), n, f.lo, f.hi, sc->bvh_nodes.as<float4>(),
                                  sc->bvh_tris.as<float4>(), sc->bvh_scratch.p, sc->bvh_scratch.bytes, st,
                                  &sc->last_launches),
                    "LBVH build");
         check_cuda(cudaStreamSynchronize(st), "LBVH build");
         sc->bvh_scratch.release();
     }
-    DevScene &ds = sc->ds;
-    std::memset(&ds, 0, sizeof(ds));
-    std::memcpy(ds.cam.c2w.m, h.cam.c2w, 64);
-    std::memcpy(ds.cam.w2c.m, h.cam.w2c, 64);
-    ds.cam.fov = h.cam.fov;
-    ds.cam.aspect = h.cam.aspect;
-    ds.cam.clip_near = h.cam.clip_near;
-    ds.cam.fisheye = h.cam.fisheye;
-    ds.vtx = sc->vtx.as<float>();
-    ds.nrm = any_n ? sc->nrm.as<float>() : nullptr;
-    ds.uv = any_uv ? sc->uv.as<float>() : nullptr;
-    ds.tri = sc->tri.as<int4>();
-    ds.tri_local = sc->tri_local.as<int>();
-    ds.num_tris = n;
-    ds.bvh_nodes = sc->bvh_nodes.as<float4>();
-    ds.bvh_tris = sc->bvh_tris.as<float4>();
-    ds.bvh_root = n > 1 ? 0 : ~0;
-    ds.shapes = sc->shapes.as<DevShape>();
-    ds.num_shapes = (int)h.shapes.size();
-    ds.mats = sc->mats.as<DevMaterial>();
-    ds.num_mats = (int)h.mats.size();
-    ds.texels = sc->texels.as<float>();
-    ds.lights = sc->lights.as<DevLight>();
-    ds.num_lights = (int)h.lights.size();
-    ds.light_sel_cdf = sc->light_sel_cdf.as<float>();
-    ds.light_sel_func = sc->light_sel_func.as<float>();
-    ds.light_sel_func_int = h.light_sel.func_int;
-    ds.total_light_intensity = h.total_light_intensity;
-    ds.light_tri_cdf = sc->light_tri_cdf.as<float>();
-    ds.light_tri_func = sc->light_tri_func.as<float>();
-    ds.prim_edges = sc->prim_edges.as<DevEdge>();
-    ds.num_prim_edges = (int)h.prim_edges.size();
-    ds.prim_cdf = sc->prim_cdf.as<float>();
-    ds.prim_func = sc->prim_func.as<float>();
-    ds.prim_func_int = h.prim_dist.func_int;
-    ds.sil_nodes = sc->sil_nodes.as<DevEdgeNode>();
-    ds.sil_edges = sc->sil_edges.as<DevEdge>();
-    ds.num_sil_nodes = (int)h.sil_nodes.size();
-    ds.nrm_nodes = sc->nrm_nodes.as<DevEdgeNode>();
-    ds.nrm_edges = sc->nrm_edges.as<DevEdge>();
-    ds.num_nrm_nodes = (int)h.nrm_nodes.size();
-    ds.ltc = sc->ltc.as<float>();
-    ds.grad_total = (int)h.grad_total;
+    ScenePtrs ptr;
+    ptr.vtx = sc->vtx.as<float>();
+    ptr.nrm = sc->nrm.as<float>();
+    ptr.uv = sc->uv.as<float>();
+    ptr.tri = sc->tri.as<int4>();
+    ptr.tri_local = sc->tri_local.as<int>();
+    ptr.bvh_nodes = sc->bvh_nodes.as<float4>();
+    ptr.bvh_tris = sc->bvh_tris.as<float4>();
+    ptr.shapes = sc->shapes.as<DevShape>();
+    ptr.mats = sc->mats.as<DevMaterial>();
+    ptr.texels = sc->texels.as<float>();
+    ptr.lights = sc->lights.as<DevLight>();
+    ptr.light_sel_cdf = sc->light_sel_cdf.as<float>();
+    ptr.light_sel_func = sc->light_sel_func.as<float>();
+    ptr.light_tri_cdf = sc->light_tri_cdf.as<float>();
+    ptr.light_tri_func = sc->light_tri_func.as<float>();
+    ptr.prim_edges = sc->prim_edges.as<DevEdge>();
+    ptr.prim_cdf = sc->prim_cdf.as<float>();
+    ptr.prim_func = sc->prim_func.as<float>();
+    ptr.sil_nodes = sc->sil_nodes.as<DevEdgeNode>();
+    ptr.sil_edges = sc->sil_edges.as<DevEdge>();
+    ptr.nrm_nodes = sc->nrm_nodes.as<DevEdgeNode>();
+    ptr.nrm_edges = sc->nrm_edges.as<DevEdge>();
+    ptr.ltc = sc->ltc.as<float>();
+    fill_devscene(sc->ds, h, f, ptr);
+}
+
+// Shared-memory gradient cache of the backward kernels: everything when the
+// flat gradient is small, else the camera + material block and the lights.
+GradCacheCfg grad_cache_cfg(const HostScene &h) {
+    const int cap = 6144;  // floats (24 KB of shared memory per block)
+    GradCacheCfg c;
+    int total = (int)h.grad_total;
+    if (total <= cap) {
+        c.head = total;
+        c.tail_begin = total;
+        c.tail_len = 0;
+        return c;
+    }
+    int first_vtx = h.layout_vtx.empty() ? total : (int)h.layout_vtx[0];
+    c.head = std::min(first_vtx, cap / 2);
+    int first_light = h.layout_light.empty() ? total : (int)h.layout_light[0];
+    c.tail_begin = first_light;
+    c.tail_len = std::min(total - first_light, cap / 2);
+    return c;
+}
+
+void collect_timings(dr_scene *sc, cudaStream_t st) {
+    sc->timings.clear();
+    if (!sc->timer.on) return;
+    check_cuda(cudaStreamSynchronize(st), "timing sync");
+    for (int i = 0; i < sc->timer.n; i++) {
+        float ms = 0.f;
+        cudaEventElapsedTime(&ms, sc->timer.ev[i], sc->timer.ev[i + 1]);
+        sc->timings.emplace_back(sc->timer.names[i], ms);
+    }
 }
 
 void check_render_desc(const dr_scene *sc, const dr_render_desc *rd) {
@@ -753,6 +220,9 @@ template <typename F> dr_status guard(F f) {
     } catch (const DrError &e) {
         g_last_error = e.what();
         return e.code;
+    } catch (const SceneError &e) {
+        g_last_error = e.what();
+        return (dr_status)e.code;
     } catch (const std::exception &e) {
         g_last_error = e.what();
         return DR_ERR_INVALID_ARGUMENT;
@@ -775,7 +245,8 @@ dr_status dr_scene_create(const dr_scene_desc *desc, int device, dr_scene **out)
         check_cuda(cudaSetDevice(device), "cudaSetDevice");
         std::unique_ptr<dr_scene> sc(new dr_scene());
         sc->device = device;
-        load_desc(sc.get(), desc);
+        check_cuda(cudaDeviceGetAttribute(&sc->num_sms, cudaDevAttrMultiProcessorCount, device), "device query");
+        load_desc(sc->h, desc, [](auto p, size_t n, const char *w) { return fetch(p, n, w); });
         sc->h.preprocess();
         sc->last_launches = 0;
         upload_scene(sc.get(), 0);
@@ -794,11 +265,7 @@ dr_status dr_scene_update(dr_scene *scene, const dr_scene_desc *desc) {
             if (desc->shapes[i].num_vertices != sizes[i].first || desc->shapes[i].num_triangles != sizes[i].second)
                 throw DrError(DR_ERR_INVALID_ARGUMENT, "update must keep every mesh's topology");
         check_cuda(cudaSetDevice(scene->device), "cudaSetDevice");
-        scene->layout_mat.clear();
-        scene->layout_vtx.clear();
-        scene->layout_nrm.clear();
-        scene->layout_light.clear();
-        load_desc(scene, desc);
+        load_desc(scene->h, desc, [](auto p, size_t n, const char *w) { return fetch(p, n, w); });
         scene->h.preprocess();
         scene->last_launches = 0;
         upload_scene(scene, 0);
@@ -818,10 +285,10 @@ dr_status dr_scene_grad_layout(const dr_scene *scene, dr_grad_layout *layout) {
         if (!scene || !layout) throw DrError(DR_ERR_INVALID_ARGUMENT, "NULL argument");
         layout->total = scene->h.grad_total;
         layout->camera = 0;
-        layout->material = scene->layout_mat.data();
-        layout->shape_vertices = scene->layout_vtx.data();
-        layout->shape_normals = scene->layout_nrm.data();
-        layout->light = scene->layout_light.data();
+        layout->material = scene->h.layout_mat.data();
+        layout->shape_vertices = scene->h.layout_vtx.data();
+        layout->shape_normals = scene->h.layout_nrm.data();
+        layout->light = scene->h.layout_light.data();
     });
 }
 
@@ -832,8 +299,9 @@ dr_status dr_render_forward(dr_scene *scene, const dr_render_desc *rd, float *im
         check_cuda(cudaSetDevice(scene->device), "cudaSetDevice");
         scene->last_launches = 0;
         check_cuda(dr_launch_forward(scene->ds, rd->width, rd->height, rd->spp, rd->max_bounces, rd->seed, image_dev,
-                                     (cudaStream_t)stream, &scene->last_launches),
+                                     (cudaStream_t)stream, &scene->last_launches, &scene->timer),
                    "forward launch");
+        collect_timings(scene, (cudaStream_t)stream);
     });
 }
 
@@ -854,14 +322,14 @@ dr_status dr_render_backward(dr_scene *scene, const dr_render_desc *rd, const fl
         long long cap_items = std::max<long long>(npix * 8, 1 << 16);
         for (int attempt = 0; attempt < 4; attempt++) {
             scene->ws_pt.reserve(sizeof(float) * DR_PT_FLOATS * cap_points);
-            scene->ws_pt_last.reserve(sizeof(int) * cap_points);
+            scene->ws_pt_last.reserve(sizeof(unsigned long long) * cap_points);
             scene->ws_items.reserve(sizeof(int4) * cap_items);
             scene->ws_item_w.reserve(sizeof(float) * cap_items);
             scene->ws_item_dp.reserve(sizeof(float) * 3 * cap_items);
             scene->ws_counts.reserve(sizeof(int) * 4);
             BackwardWorkspace ws;
             ws.pt = scene->ws_pt.as<float>();
-            ws.pt_last = scene->ws_pt_last.as<int>();
+            ws.pt_last = scene->ws_pt_last.as<unsigned long long>();
             ws.cap_points = cap_points;
             ws.items = scene->ws_items.as<int4>();
             ws.item_w = scene->ws_item_w.as<float>();
@@ -874,13 +342,17 @@ dr_status dr_render_backward(dr_scene *scene, const dr_render_desc *rd, const fl
             check_cuda(cudaMemsetAsync(grad_dev, 0, sizeof(float) * scene->h.grad_total, st), "memset");
             check_cuda(dr_launch_backward(scene->ds, rd->width, rd->height, rd->spp, rd->max_bounces, rd->seed,
                                           d_image_dev, grad_dev, image_dev, rd->primary_edge_samples, rd->dp_mode,
-                                          ws, st, &scene->last_launches),
+                                          ws, grad_cache_cfg(scene->h), scene->num_sms, st, &scene->last_launches,
+                                          &scene->timer),
                        "backward launch");
             int counts[4];
             check_cuda(cudaMemcpyAsync(counts, scene->ws_counts.p, sizeof(counts), cudaMemcpyDeviceToHost, st),
                        "status read");
             check_cuda(cudaStreamSynchronize(st), "backward");
             int status = counts[2];
+            scene->last_points = counts[0];
+            scene->last_items = counts[1];
+            collect_timings(scene, st);
             if (status & (DR_STATUS_POINT_OVERFLOW | DR_STATUS_ITEM_OVERFLOW)) {
                 if (status & DR_STATUS_POINT_OVERFLOW) cap_points *= 2;
                 if (status & DR_STATUS_ITEM_OVERFLOW) cap_items = std::max(cap_items * 2, (long long)counts[1] + 1);
@@ -903,6 +375,41 @@ dr_status dr_trace_rays(dr_scene *scene, const float *rays_dev, int64_t n, int *
         check_cuda(dr_launch_trace(scene->ds, rays_dev, n, tri_dev, t_dev, (cudaStream_t)stream,
                                    &scene->last_launches),
                    "trace launch");
+    });
+}
+
+dr_status dr_scene_set_profiling(dr_scene *scene, int enable) {
+    return guard([&]() {
+        if (!scene) throw DrError(DR_ERR_INVALID_ARGUMENT, "scene is NULL");
+        check_cuda(cudaSetDevice(scene->device), "cudaSetDevice");
+        if (enable && !scene->timer_ready) {
+            for (int i = 0; i <= StageTimer::kMax; i++)
+                check_cuda(cudaEventCreate(&scene->timer.ev[i]), "cudaEventCreate");
+            scene->timer_ready = true;
+        }
+        scene->timer.on = enable != 0;
+    });
+}
+
+dr_status dr_scene_last_timings(const dr_scene *scene, int index, char *name, size_t name_len, float *ms) {
+    return guard([&]() {
+        if (!scene || !ms) throw DrError(DR_ERR_INVALID_ARGUMENT, "NULL argument");
+        if (index < 0 || index >= (int)scene->timings.size()) throw DrError(DR_ERR_INVALID_ARGUMENT, "no such stage");
+        const auto &t = scene->timings[index];
+        if (name && name_len > 0) {
+            size_t c = std::min(t.first.size(), name_len - 1);
+            std::memcpy(name, t.first.data(), c);
+            name[c] = 0;
+        }
+        *ms = t.second;
+    });
+}
+
+dr_status dr_scene_last_counts(const dr_scene *scene, int64_t *points, int64_t *items) {
+    return guard([&]() {
+        if (!scene || !points || !items) throw DrError(DR_ERR_INVALID_ARGUMENT, "NULL argument");
+        *points = scene->last_points;
+        *items = scene->last_items;
     });
 }
 

@@ -1,0 +1,732 @@
+// Edge sampling on the device: the boundary terms of the derivative.
+//
+//   is_silhouette           edge.h:59-79
+//   box_cone                aabb.cpp:98-311 (GeometricTools box/cone test)
+//   bsdf_bound              edge_tree.cpp:345-480
+//   contains_silhouette     edge_tree.cpp:482-497
+//   traverse_edges          edge_tree.cpp:511-725, recursion replaced by an
+//                           explicit stack that keeps the same depth-first
+//                           order (left child first), so random draws are
+//                           consumed in the reference's order
+//   shading_edge_sample     delta_ray.cpp:45-365 (LTC line sampling, two rays
+//                           straddling the edge, dp/dv0/dv1)
+//   primary_edge_sample     delta_ray.cpp:377-557 (screen-space boundary
+//                           term, forward differences to world space)
+#pragma once
+
+#include "dr_shading.cuh"
+
+DEV float3 shape_vtx(const DevScene &s, int shape, int v) { return vtx3(s.vtx, s.shapes[shape].vtx_off + v); }
+DEV float3 edge_v0(const DevScene &s, const DevEdge &e) { return shape_vtx(s, e.shape, e.v0); }
+DEV float3 edge_v1(const DevScene &s, const DevEdge &e) { return shape_vtx(s, e.shape, e.v1); }
+
+DEV float3 non_shared_vertex(const DevScene &s, const DevEdge &e, int f) {
+    int4 t = s.tri[s.shapes[e.shape].tri_off + f];
+    int off = s.shapes[e.shape].vtx_off;
+    int v[3] = {t.x - off, t.y - off, t.z - off};
+    for (int i = 0; i < 3; i++)
+        if (v[i] != e.v0 && v[i] != e.v1) return shape_vtx(s, e.shape, v[i]);
+    return f3(0.f);
+}
+
+DEV bool is_silhouette(const DevScene &s, float3 p, const DevEdge &e) {
+    if (!s.shapes[e.shape].has_n) return true;
+    if (e.f0 == -1 || e.f1 == -1) return true;
+    float3 v0 = edge_v0(s, e), v1 = edge_v1(s, e);
+    float3 a = non_shared_vertex(s, e, e.f0), b = non_shared_vertex(s, e, e.f1);
+    float3 n0 = normalize(cross(v0 - a, v1 - a)), n1 = normalize(cross(v1 - b, v0 - b));
+    bool f0 = dot(p - v0, n0) > 0.f && dot(p - v1, n0) > 0.f && dot(p - a, n0) > 0.f;
+    bool f1 = dot(p - v0, n1) > 0.f && dot(p - v1, n1) > 0.f && dot(p - b, n1) > 0.f;
+    return (f0 && !f1) || (!f0 && f1);
+}
+
+// ---------------------------------------------------------------------------
+// Box / cone intersection.  The apex region (per axis: beyond the slab's upper
+// face, inside, below its lower face) selects the silhouette polygon of the
+// box seen from the apex; corner j has +extent on axis a iff bit a of j is
+// set.  Same table as aabb.cpp:106-132 so that boundary cases agree.
+// ---------------------------------------------------------------------------
+struct ConeSpec { float3 o, d; float cos_angle; };
+
+DEV int cone_poly(int lookup, int i) {
+    // packed: 4 bits per corner, count in the top nibble
+    const unsigned long long tab[27] = {
+        0x6000000000154623ull, 0x6000000000023154ull, 0x6000000000023754ull, 0x6000000000046231ull,
+        0x4000000000000231ull, 0x6000000000023751ull, 0x6000000000046731ull, 0x6000000000026731ull,
+        0x6000000000026751ull, 0x6000000000015462ull, 0x4000000000000154ull, 0x6000000000013754ull,
+        0x4000000000000462ull, 0x0000000000000000ull, 0x4000000000001375ull, 0x6000000000046732ull,
+        0x4000000000002673ull, 0x6000000000132675ull, 0x6000000000015762ull, 0x6000000000015764ull,
+        0x6000000000013764ull, 0x6000000000045762ull, 0x4000000000004576ull, 0x6000000000137645ull,
+        0x6000000000045732ull, 0x6000000000264573ull, 0x6000000000132645ull};
+    unsigned long long w = tab[lookup];
+    if (i < 0) return (int)(w >> 60);
+    int n = (int)(w >> 60);
+    return (int)((w >> (4 * (n - 1 - i))) & 0xF);
+}
+
+DEV bool box_cone(const float *lo, const float *hi, const ConeSpec &cone) {
+    if (cone.cos_angle <= 0.f) return true;
+    float3 C = f3(0.5f * (lo[0] + hi[0]), 0.5f * (lo[1] + hi[1]), 0.5f * (lo[2] + hi[2]));
+    float3 E = f3(0.5f * (hi[0] - lo[0]), 0.5f * (hi[1] - lo[1]), 0.5f * (hi[2] - lo[2]));
+    float3 CmV = C - cone.o;
+    float DdCmV = dot(cone.d, CmV);
+    float rad = E.x * fabsf(cone.d.x) + E.y * fabsf(cone.d.y) + E.z * fabsf(cone.d.z);
+    if (DdCmV + rad <= 0.f) return false;
+    int ix = CmV.x < -E.x ? 2 : (CmV.x > E.x ? 0 : 1);
+    int iy = CmV.y < -E.y ? 2 : (CmV.y > E.y ? 0 : 1);
+    int iz = CmV.z < -E.z ? 2 : (CmV.z > E.z ? 0 : 1);
+    int lookup = ix + 3 * iy + 9 * iz;
+    if (lookup == 13) return true;
+    int np = cone_poly(lookup, -1);
+    float c2 = cone.cos_angle * cone.cos_angle;
+    float3 X[8], PmV[8];
+    float DdPmV[8], sDd[8], sLen[8];
+    int imax = -1, jmax = -1;
+    for (int i = 0; i < np; i++) {
+        int j = cone_poly(lookup, i);
+        X[j] = f3((j & 1) ? E.x : -E.x, (j & 2) ? E.y : -E.y, (j & 4) ? E.z : -E.z);
+        DdPmV[j] = dot(cone.d, X[j]) + DdCmV;
+        if (DdPmV[j] > 0.f) {
+            PmV[j] = X[j] + CmV;
+            sDd[j] = DdPmV[j] * DdPmV[j];
+            sLen[j] = dot(PmV[j], PmV[j]);
+            if (sDd[j] - c2 * sLen[j] > 0.f) return true;
+            if (imax == -1 || sDd[j] * sLen[jmax] > sDd[jmax] * sLen[j]) {
+                imax = i;
+                jmax = j;
+            }
+        }
+    }
+    if (imax == -1) return false;
+    float mLen = sLen[jmax], mDd = DdPmV[jmax];
+    float3 mX = X[jmax], mP = PmV[jmax];
+    for (int side = 0; side < 2; side++) {
+        int s, k0;
+        float fder;
+        if (side == 0) {
+            int jn = cone_poly(lookup, imax < np - 1 ? imax + 1 : 0);
+            int jd = jn - jmax;
+            s = jd > 0 ? 1 : -1;
+            k0 = (jd < 0 ? -jd : jd) >> 1;
+            fder = s * (comp(cone.d, k0) * mLen - mDd * comp(mP, k0));
+        } else {
+            int jp = cone_poly(lookup, imax > 0 ? imax - 1 : np - 1);
+            int jd = jmax - jp;
+            s = jd > 0 ? 1 : -1;
+            k0 = (jd < 0 ? -jd : jd) >> 1;
+            fder = -s * (comp(cone.d, k0) * mLen - mDd * comp(mP, k0));
+        }
+        if (fder > 0.f) {
+            int k1 = (k0 + 1) % 3, k2 = (k1 + 1) % 3;
+            float numer = comp(mP, k1) * comp(mP, k1) + comp(mP, k2) * comp(mP, k2);
+            float denom = comp(cone.d, k1) * comp(mP, k1) + comp(cone.d, k2) * comp(mP, k2);
+            float3 M;
+            comp_set(M, k0, numer * comp(cone.d, k0));
+            comp_set(M, k1, denom * (comp(mX, k1) + comp(CmV, k1)));
+            comp_set(M, k2, denom * (comp(mX, k2) + comp(CmV, k2)));
+            float DdM = dot(cone.d, M);
+            if (DdM * DdM - c2 * dot(M, M) > 0.f) return true;
+            float det = s * (comp(cone.d, k1) * comp(mP, k2) - comp(cone.d, k2) * comp(mP, k1));
+            return det <= 0.f;
+        }
+    }
+    return false;
+}
+
+// ---------------------------------------------------------------------------
+// Edge-tree node bounds
+// ---------------------------------------------------------------------------
+DEV float min_sq_bound(float lo, float hi) {
+    if (lo <= 0.f && hi >= 0.f) return 0.f;
+    if (lo < 0.f && hi < 0.f) return hi * hi;
+    return lo * lo;
+}
+DEV float max_sq_bound(float lo, float hi) { return fmaxf(lo * lo, hi * hi); }
+
+DEV float3 node_corner(const DevEdgeNode &n, int i) {
+    return f3((i & 1) ? n.hi[0] : n.lo[0], (i & 2) ? n.hi[1] : n.lo[1], (i & 4) ? n.hi[2] : n.lo[2]);
+}
+
+DEV float bsdf_bound(const DevEdgeNode &node, float3 wi, const SurfacePoint &sp, float dl, float sl, float rough) {
+    float cos_max = 0.f;
+    for (int i = 0; i < 8; i++)
+        if (dot(sp.f.n, node_corner(node, i) - sp.p) > 0.f) {
+            cos_max = 1.f;
+            break;
+        }
+    if (cos_max <= 0.f) return 0.f;
+    float maxp = 0.f;
+    if (sl > 0.f) {
+        float3 hy = normalize(cross(sp.f.n, wi));
+        Frame hf;
+        hf.t = normalize(cross(wi, hy));
+        hf.b = hy;
+        hf.n = wi;
+        float3 lo = f3(DR_INF), hi = f3(-DR_INF);
+        for (int i = 0; i < 8; i++) {
+            float3 c = to_local(hf, node_corner(node, i) - sp.p);
+            lo = f3(fminf(lo.x, c.x), fminf(lo.y, c.y), fminf(lo.z, c.z));
+            hi = f3(fmaxf(hi.x, c.x), fmaxf(hi.y, c.y), fmaxf(hi.z, c.z));
+        }
+        float cphi = 0.f;
+        float hx = hi.x;
+        if (hx > 0.f) cphi = hx / sqrtf(min_sq_bound(lo.y, hi.y) + hx * hx);
+        else if (hx == 0.f) cphi = fmaxf(cphi, 0.f);
+        else cphi = hx / sqrtf(max_sq_bound(lo.y, hi.y) + hx * hx);
+        float cto_min, cto_max;
+        if (lo.z > 0.f) cto_min = lo.z / (max_sq_bound(lo.x, hi.x) + max_sq_bound(lo.y, hi.y) + lo.z * lo.z);
+        else cto_min = lo.z / (min_sq_bound(lo.x, hi.x) + min_sq_bound(lo.y, hi.y) + lo.z * lo.z);
+        if (hi.z > 0.f) cto_max = hi.z / (min_sq_bound(lo.x, hi.x) + min_sq_bound(lo.y, hi.y) + hi.z * hi.z);
+        else cto_max = hi.z / (max_sq_bound(lo.x, hi.x) + max_sq_bound(lo.y, hi.y) + hi.z * hi.z);
+        float cth_min = sqrtf((cto_min + 1.f) / 2.f), cth_max = sqrtf((cto_max + 1.f) / 2.f);
+        float3 ln = to_local(hf, sp.f.n);
+        float chmax = cphi >= 0.f ? sqrtf(ln.z * ln.z / (ln.z * ln.z + ln.x * ln.x * cphi * cphi)) : 1.f;
+        if (chmax > cth_max) chmax = cth_max;
+        else if (chmax < cth_min) chmax = cth_min;
+        float shmax = sqrtf(fmaxf(1.f - chmax * chmax, 0.f));
+        float hdn = fminf(fabsf(ln.x * shmax * cphi) + ln.z * chmax, 1.f);
+        float e = roughness_to_phong(rough);
+        maxp = powf(hdn, e) * (e + 2.f) / float(2 * 3.14159265358979323846);
+    }
+    return cos_max * (dl / DR_PI + sl * maxp);
+}
+
+DEV bool contains_silhouette(const DevEdgeNode &node, float3 p) {
+    float3 c = f3(0.5f * (node.lo[0] + node.hi[0]), 0.5f * (node.lo[1] + node.hi[1]), 0.5f * (node.lo[2] + node.hi[2]));
+    // bounding sphere as aabb.h:266-270: center (lo + hi) / 2, radius |hi - center|
+    float3 cs = f3((node.lo[0] + node.hi[0]) / 2.f, (node.lo[1] + node.hi[1]) / 2.f, (node.lo[2] + node.hi[2]) / 2.f);
+    float r = length(f3(node.hi[0], node.hi[1], node.hi[2]) - cs);
+    float3 d = cs - p;
+    float l = length(d);
+    float vt = r / l;
+    if (vt >= 1.f) return true;
+    float va = atanf(vt);
+    d = d / l;
+    float ang = acosf(dot(-d, f3(node.axis[0], node.axis[1], node.axis[2])));
+    float range = node.angle + va;
+    (void)c;
+    return ang - range <= float(3.14159265358979323846 / 2.f) && ang + range >= float(3.14159265358979323846 / 2.f);
+}
+
+DEV float node_importance(const DevEdgeNode &node, float bb, float3 p) {
+    float3 c = f3(0.5f * (node.lo[0] + node.hi[0]), 0.5f * (node.lo[1] + node.hi[1]), 0.5f * (node.lo[2] + node.hi[2]));
+    return bb * node.total_length / length_sq(p - c);
+}
+
+DEV bool node_inside(const DevEdgeNode &n, float3 p) {
+    return p.x >= n.lo[0] && p.x <= n.hi[0] && p.y >= n.lo[1] && p.y <= n.hi[1] && p.z >= n.lo[2] && p.z <= n.hi[2];
+}
+
+// Stochastic traversal of one edge tree in one mode (edge_tree.cpp:511-652).
+// emit(tree_edge_index, weight) is called for every silhouette edge of every
+// reached leaf, in the reference's order.  Returns false if the stack limit
+// was hit (never for trees of depth < DR_EDGE_STACK).
+#define DR_EDGE_STACK 64
+template <bool CONE, class Emit>
+DEV bool traverse_mode(const DevScene &s, const DevEdgeNode *nodes, const DevEdge *edges, bool dir_bounds, float3 wi,
+                       const SurfacePoint &sp, float dl, float sl, float rough, const ConeSpec &cone, float root_bb,
+                       float pmf, Rng &rng, Emit &emit) {
+    struct Item { int node; float bb, cpmf, apmf; };
+    Item st[DR_EDGE_STACK];
+    int sp_ = 0;
+    st[sp_++] = Item{0, root_bb, pmf, pmf};
+    bool ok = true;
+    while (sp_ > 0) {
+        Item it = st[--sp_];
+        if (it.bb <= 0.f) continue;
+        const DevEdgeNode &node = nodes[it.node];
+        if (node.nprims > 0) {
+            float denom = it.cpmf * it.cpmf + it.apmf * it.apmf;
+            float w = CONE ? it.cpmf / denom : it.apmf / denom;
+            for (int i = 0; i < node.nprims; i++) {
+                int ei = node.offset + i;
+                if (is_silhouette(s, sp.p, edges[ei])) emit(ei, w);
+            }
+            continue;
+        }
+        int li = it.node + 1, ri = node.offset;
+        const DevEdgeNode &L = nodes[li], &R = nodes[ri];
+        bool all_split = it.bb > 1.f || node_inside(node, sp.p);
+        bool lcs = true, rcs = true;
+        if (dir_bounds) {
+            lcs = contains_silhouette(L, sp.p);
+            rcs = contains_silhouette(R, sp.p);
+        }
+        float lbb = lcs ? bsdf_bound(L, wi, sp, dl, sl, rough) : 0.f;
+        float rbb = rcs ? bsdf_bound(R, wi, sp, dl, sl, rough) : 0.f;
+        float il = lcs ? node_importance(L, lbb, sp.p) : 0.f;
+        float ir = rcs ? node_importance(R, rbb, sp.p) : 0.f;
+        if (il + ir <= 1e-10f) continue;
+        bool lhc = box_cone(L.lo, L.hi, cone), rhc = box_cone(R.lo, R.hi, cone);
+        bool cone_split = all_split || (lhc && rhc && lcs && rcs && cone.cos_angle > 0.95f);
+        float ilc = lhc ? il : 0.f, irc = rhc ? ir : 0.f;
+        if (CONE && ilc + irc <= 1e-10f) continue;
+        float plc = 0.f, prc = 0.f, pla = 0.f, pra = 0.f;
+        if (cone_split) {
+            plc = prc = 1.f;
+        } else if (ilc + irc > 1e-10f) {
+            plc = ilc / (ilc + irc);
+            prc = 1.f - plc;
+        }
+        if (all_split) {
+            pla = pra = 1.f;
+        } else {
+            pla = il / (il + ir);
+            pra = 1.f - pla;
+        }
+        bool split = CONE ? cone_split : all_split;
+        Item left{li, lbb, plc * it.cpmf, pla * it.apmf}, right{ri, rbb, prc * it.cpmf, pra * it.apmf};
+        if (split) {
+            if (sp_ + 2 > DR_EDGE_STACK) {
+                ok = false;
+                continue;
+            }
+            // depth first, left subtree before right
+            if (rcs) st[sp_++] = right;
+            if (lcs) st[sp_++] = left;
+        } else {
+            float u = rng.next();
+            bool go_left = CONE ? u < plc : u < pla;
+            if (sp_ + 1 > DR_EDGE_STACK) {
+                ok = false;
+                continue;
+            }
+            st[sp_++] = go_left ? left : right;
+        }
+    }
+    return ok;
+}
+
+// All edges sampled for one shading point (edge_tree.cpp:654-725).
+// emit(tree, edge_index, weight); tree 0 = silhouette tree, 1 = normal tree.
+template <class Emit>
+DEV bool traverse_edges(const DevScene &s, float3 wi, int stri, const SurfacePoint &sp, const ConeSpec &cone, Rng &rng,
+                        Emit &emit) {
+    if (dot(wi, sp.f.n) < 0.f) return true;
+    int tree;
+    float pmf = 1.f;
+    if (s.num_nrm_nodes == 0 && s.num_sil_nodes == 0) return true;
+    if (s.num_nrm_nodes == 0) {
+        tree = 0;
+    } else if (s.num_sil_nodes == 0) {
+        tree = 1;
+    } else {
+        float ni = s.nrm_nodes[0].total_length, si = s.sil_nodes[0].total_length;
+        float np = ni / (ni + si), spm = si / (ni + si);
+        float u = rng.next();
+        if (u < np) {
+            tree = 1;
+            pmf = np;
+        } else {
+            tree = 0;
+            pmf = spm;
+        }
+    }
+    const DevEdgeNode *nodes = tree ? s.nrm_nodes : s.sil_nodes;
+    const DevEdge *edges = tree ? s.nrm_edges : s.sil_edges;
+    const DevMaterial &m = s.mats[material_of_tri(s, stri)];
+    float dl = luminance(get_kd(s, m, sp.uv)), sl = luminance(get_ks(s, m, sp.uv));
+    float rough = get_rough(s, m, sp.uv);
+    float b = bsdf_bound(nodes[0], wi, sp, dl, sl, rough);
+    auto em = [&](int ei, float w) { emit(tree, ei, w); };
+    bool ok = traverse_mode<true>(s, nodes, edges, tree == 1, wi, sp, dl, sl, rough, cone, b, pmf, rng, em);
+    ok &= traverse_mode<false>(s, nodes, edges, tree == 1, wi, sp, dl, sl, rough, cone, b, pmf, rng, em);
+    return ok;
+}
+
+// LTC matrix lookup (material.h:464-476): nearest entry of the 128x128 table
+DEV M3 ltc_matrix(const DevScene &s, int mi, const SurfacePoint &sp, float3 wi) {
+    float r = get_rough(s, s.mats[mi], sp.uv);
+    float ct = dot(wi, sp.f.n);
+    float th = acosf(ct);
+    int rid = int(r * (128 - 1));
+    int tid = int(((double)th / (3.14159265358979323846 / 2.f)) * (128 - 1));
+    rid = rid < 0 ? 0 : (rid > 127 ? 127 : rid);
+    tid = tid < 0 ? 0 : (tid > 127 ? 127 : tid);
+    M3 m;
+    const float *p = s.ltc + 9 * (rid + tid * 128);
+    for (int i = 0; i < 9; i++) m.m[i] = dr_ldg(p + i);
+    return m;
+}
+
+// d p / d dir of a ray hitting the plane through p with normal n (vector.h:690-716)
+DEV M3 intersect_jacobian(float3 dir, float3 p, float3 n) {
+    M3 m;
+    float d = -dot(p, n);
+    float dn = dot(dir, n);
+    if (fabsf(dn) < 1e-10f) {
+        for (int i = 0; i < 9; i++) m.m[i] = 0.f;
+        return m;
+    }
+    float inv2 = 1.f / (dn * dn);
+    float t = -d / dn;
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) m.m[3 * i + j] = (i == j ? t : 0.f) + comp(dir, i) * d * comp(n, j) * inv2;
+    return m;
+}
+DEV M3 normalize_jacobian(float3 x) {
+    float d2 = length_sq(x);
+    float d = sqrtf(d2);
+    float inv = 1.f / (d * d2);
+    M3 m;
+    for (int i = 0; i < 3; i++)
+        for (int j = 0; j < 3; j++) m.m[3 * i + j] = ((i == j ? d2 : 0.f) - comp(x, i) * comp(x, j)) * inv;
+    return m;
+}
+
+struct EdgeResult { float3 dp, dv0, dv1; };
+
+// Secondary edge sample (delta_ray.cpp:45-365).  `rng` holds the item's
+// secondary samples (for the two shade calls, replayed from the same state).
+DEV EdgeResult shading_edge_sample(const DevScene &s, const EdgeSample &es, const DevEdge &edge, const LightSample &ls,
+                                   const Rng &rng, int nbounces, float3 wi, int stri, const SurfacePoint &sp,
+                                   float3 weight, float3 d_color, bool direct_only) {
+    EdgeResult none;
+    none.dp = none.dv0 = none.dv1 = f3(0.f);
+    if (stri < 0) return none;
+    if (!is_silhouette(s, sp.p, edge)) return none;
+    float3 v0 = edge_v0(s, edge), v1 = edge_v1(s, edge);
+    if (abs_sum(v1 - v0) == 1e-10f) return none;
+    int mi = material_of_tri(s, stri);
+    const DevMaterial &mat = s.mats[mi];
+    float3 kd = get_kd(s, mat, sp.uv), ks = get_ks(s, mat, sp.uv);
+    float dw = luminance(kd), sw = luminance(ks), ws = dw + sw;
+    if (ws <= 0.f) return none;
+    float dpmf = dw / ws, spmf = sw / ws;
+    float3 n = sp.f.n;
+    float3 fx = normalize(wi - n * dot(wi, n));
+    float3 fy = cross(n, fx);
+    M3 frame = m3_rows(fx, fy, n);
+    M3 m, minv;
+    float mpmf;
+    if (es.bsdf_component <= dpmf) {
+        minv = frame;
+        m = inverse(minv);
+        mpmf = dpmf;
+    } else {
+        minv = mul(inverse(ltc_matrix(s, mi, sp, wi)), frame);
+        m = inverse(minv);
+        mpmf = spmf;
+    }
+    float3 a = mul(minv, v0 - sp.p), b = mul(minv, v1 - sp.p);
+    if (a.z <= 0.f && b.z <= 0.f) return none;
+    if (a.z < 0.f) a = (a * b.z - b * a.z) / (b.z - a.z);
+    if (b.z < 0.f) b = (a * b.z - b * a.z) / (b.z - a.z);
+    float3 vod = b - a;
+    if (abs_sum(vod) < 1e-10f) return none;
+    float3 wt = normalize(vod);
+    float l0 = dot(a, wt), l1 = dot(b, wt);
+    float3 vo = a - l0 * wt;
+    float d = length(vo);
+    auto I = [&](float l) {
+        return (l / (d * (d * d + l * l)) + atanf(l / d) / (d * d)) * vo.z + (l * l / (d * (d * d + l * l))) * wt.z;
+    };
+    float Il0 = I(l0), Il1 = I(l1);
+    float norm = Il1 - Il0;
+    if (norm <= 1e-10f) return none;
+    auto cdf = [&](float l) { return (I(l) - Il0) / norm; };
+    auto pdf = [&](float l) {
+        float ds = d * d + l * l;
+        return 2.f * d * (vo + l * wt).z / (norm * ds * ds);
+    };
+    float lb = l0, ub = l1;
+    if (lb > ub) {
+        float t = lb;
+        lb = ub;
+        ub = t;
+    }
+    float l = 0.5f * (lb + ub);
+    for (int it = 0; it < 20; it++) {
+        if (!(l >= lb && l <= ub)) l = 0.5f * (lb + ub);
+        float value = cdf(l) - es.u;
+        if (fabsf(value) < 1e-5f || it == 19) break;
+        if (value > 0.f) ub = l;
+        else lb = l;
+        l -= value / pdf(l);
+    }
+    if (pdf(l) <= 0.f) return none;
+    float3 sample_p = mul(m, vo + l * wt);
+    float3 split_n = normalize(cross(v0 - sp.p, v1 - sp.p));
+    float delta = 1e-3f * length(sample_p);
+    float3 sdir = normalize(sample_p);
+    float3 rdir = normalize(sdir + delta * split_n), ldir = normalize(sdir - delta * split_n);
+    Hit hr = trace_closest(s, sp.p, rdir, 1e-3f), hl = trace_closest(s, sp.p, ldir, 1e-3f);
+    SurfacePoint pr, pl;
+    int rsh = -1, rlt = -1, lsh = -1, llt = -1;
+    if (hr.tri >= 0) {
+        pr = intersect_tri(load_tri(s, hr.tri), sp.p, rdir);
+        rsh = s.tri[hr.tri].w;
+        rlt = s.tri_local[hr.tri];
+    }
+    if (hl.tri >= 0) {
+        pl = intersect_tri(load_tri(s, hl.tri), sp.p, ldir);
+        lsh = s.tri[hl.tri].w;
+        llt = s.tri_local[hl.tri];
+    }
+    bool rc = rsh == edge.shape && (rlt == edge.f0 || rlt == edge.f1);
+    bool lc = lsh == edge.shape && (llt == edge.f0 || llt == edge.f1);
+    if ((!rc && !lc) || (rc && lc) || (hr.tri >= 0 && hr.tri == stri) || (hl.tri >= 0 && hl.tri == stri)) return none;
+    float3 eb = bsdf(s, mi, sp, wi, sdir);
+    if (sum(eb) < 1e-6f) return none;
+    float3 shr = f3(0.f), shl = f3(0.f);
+    if (!direct_only) {
+        shr = shade(s, -sdir, hr.tri, pr, ls, rng, nbounces, false);
+        shl = shade(s, -sdir, hl.tri, pl, ls, rng, nbounces, false);
+        if (hr.tri >= 0) {
+            float3 dir = pr.p - sp.p;
+            float d2 = length_sq(dir);
+            if (d2 > 0.f) shr = shr / fmaxf(d2, 1e-2f) * fabsf(dot(normalize(dir), pr.ng));
+            else shr = f3(0.f);
+        }
+        if (hl.tri >= 0) {
+            float3 dir = pl.p - sp.p;
+            float d2 = length_sq(dir);
+            if (d2 > 0.f) shl = shl / fmaxf(d2, 1e-2f) * fabsf(dot(normalize(dir), pl.ng));
+            else shl = f3(0.f);
+        }
+    }
+    float3 er = eval_light(s, wi, stri, sp, hr.tri, pr) + eb * shr;
+    float3 el = eval_light(s, wi, stri, sp, hl.tri, pl) + eb * shl;
+    if (hr.tri >= 0) {
+        float3 dir = pr.p - sp.p;
+        if (length(dir) * fabsf(dot(normalize(dir), pr.ng)) < 1e-3f) return none;
+    }
+    if (hl.tri >= 0) {
+        float3 dir = pl.p - sp.p;
+        if (length(dir) * fabsf(dot(normalize(dir), pl.ng)) < 1e-3f) return none;
+    }
+    EdgeResult res = none;
+    float pdf_l = pdf(l);
+    auto accum = [&](const SurfacePoint &lp, float3 ev) {
+        M3 nj = normalize_jacobian(sample_p);
+        M3 ij = intersect_jacobian(sdir, lp.p, lp.ng);
+        float line_j = length(mul(mul(mul(ij, nj), m), wt)) / (mpmf * pdf_l);
+        float3 p = sp.p, x = lp.p;
+        float3 d0 = v0 - p, d1 = v1 - p;
+        float dirac_j = length(cross(d0, d1));
+        float w = line_j / dirac_j;
+        float3 dp = w * (cross(d1, d0) + cross(x - p, d1) + cross(d0, x - p));
+        float3 dv0 = w * cross(d1, x - p);
+        float3 dv1 = w * cross(x - p, d0);
+        float we = dot(ev * weight, d_color);
+        res.dp += dp * we;
+        res.dv0 += dv0 * we;
+        res.dv1 += dv1 * we;
+    };
+    if (hr.tri >= 0 && abs_sum(er) > 0.f) accum(pr, er);
+    if (hl.tri >= 0 && abs_sum(el) > 0.f) accum(pl, -el);
+    return res;
+}
+
+// ---------------------------------------------------------------------------
+// Primary edges (camera.h:86-313, delta_ray.cpp:377-557)
+// ---------------------------------------------------------------------------
+DEV float3 unproject(const DevCamera &c, float sx, float sy) {
+    if (c.fisheye) {
+        float x = 2.f * (sx - 0.5f), y = 2.f * (sy - 0.5f);
+        float r = sqrtf(x * x + y * y), phi = atan2f(y, x), theta = r * DR_PI / 2.f;
+        return f3(-cosf(phi) * sinf(theta), -sinf(phi) * sinf(theta), cosf(theta));
+    }
+    float ndcx = (sx - 0.5f) * -2.f, ndcy = (sy - 0.5f) * -2.f / c.aspect;
+    return f3(c.fov * ndcx, c.fov * ndcy, 1.f);
+}
+DEV void d_unproject(const DevCamera &c, float sx, float sy, float3 &dx, float3 &dy) {
+    if (c.fisheye) {
+        float x = 2.f * (sx - 0.5f), y = 2.f * (sy - 0.5f);
+        float r = sqrtf(x * x + y * y), phi = atan2f(y, x), theta = r * DR_PI / 2.f;
+        float sp = sinf(phi), cp = cosf(phi), st = sinf(theta), ct = cosf(theta);
+        float dxdphi = sp * st, dxdth = -cp * ct, dydphi = -cp * st, dydth = -sp * ct, dzdth = -st;
+        float dphidx = -y / (r * r), dphidy = x / (r * r);
+        float dthdx = (DR_PI / 2.f) * x / r, dthdy = (DR_PI / 2.f) * y / r;
+        dx = 2.f * f3(dxdphi * dphidx + dxdth * dthdx, dydphi * dphidx + dydth * dthdx, dzdth * dthdx);
+        dy = 2.f * f3(dxdphi * dphidy + dxdth * dthdy, dydphi * dphidy + dydth * dthdy, dzdth * dthdy);
+        return;
+    }
+    dx = f3(-2.f * c.fov, 0.f, 0.f);
+    dy = f3(0.f, -2.f * c.fov / c.aspect, 0.f);
+}
+DEV float2 project_local(const DevCamera &c, float3 l) {
+    float2 r;
+    if (c.fisheye) {
+        float3 d = normalize(l);
+        float phi = atan2f(d.y, d.x), theta = acosf(d.z), rr = theta * 2.f / DR_PI;
+        r.x = 0.5f * (-rr * cosf(phi) + 1.f);
+        r.y = 0.5f * (-rr * sinf(phi) + 1.f);
+        return r;
+    }
+    r.x = (-l.x / (l.z * c.fov) + 1.f) * 0.5f;
+    r.y = (-l.y / (l.z * c.fov * c.aspect) + 1.f) * 0.5f;
+    return r;
+}
+DEV float3 d_project_local(const DevCamera &c, float3 l, float dx, float dy) {
+    if (c.fisheye) {
+        float3 d = normalize(l);
+        float phi = atan2f(d.y, d.x), theta = acosf(d.z), r = theta * 2.f / DR_PI;
+        float dr = -0.5f * (cosf(phi) * dx + sinf(phi) * dy);
+        float dphi = 0.5f * r * sinf(phi) * dx - 0.5f * r * cosf(phi) * dy;
+        float dtheta = dr * (2.f / DR_PI);
+        float dcos = -dtheta / sqrtf(1.f - d.z * d.z);
+        float t = d.x * d.x + d.y * d.y;
+        return d_normalize(l, f3(-dphi * d.y / t, dphi * d.x / t, dcos));
+    }
+    float zf = l.z * c.fov;
+    float zfy = zf * c.aspect;
+    return f3(dx * (-1.f / zf), dy * (-1.f / zfy),
+              dx * (c.fov * l.x / (zf * zf)) + dy * (c.fov * c.aspect * l.y / (zfy * zfy)));
+}
+DEV bool project(const DevCamera &c, float3 p0, float3 p1, float2 &s0, float2 &s1) {
+    float3 a = xfm_point(c.w2c, p0), b = xfm_point(c.w2c, p1);
+    if (a.z < c.clip_near && b.z < c.clip_near) return false;
+    if (a.z < c.clip_near) {
+        float3 dir = a - b;
+        float t = -(b.z - c.clip_near) / dir.z;
+        a = b + t * dir;
+    } else if (b.z < c.clip_near) {
+        float3 dir = b - a;
+        float t = -(a.z - c.clip_near) / dir.z;
+        b = a + t * dir;
+    }
+    s0 = project_local(c, a);
+    s1 = project_local(c, b);
+    return true;
+}
+// d_project (camera.h:244-313), including its +clip_near sign
+DEV void d_project(const DevCamera &c, float3 p0, float3 p1, float dp0x, float dp0y, float dp1x, float dp1y, float *dw2c) {
+    float3 a = xfm_point(c.w2c, p0), b = xfm_point(c.w2c, p1);
+    float3 ca = a, cb = b;
+    if (a.z < c.clip_near) {
+        float3 dir = a - b;
+        float t = -(b.z + c.clip_near) / dir.z;
+        ca = b + t * dir;
+    } else if (b.z < c.clip_near) {
+        float3 dir = b - a;
+        float t = -(a.z + c.clip_near) / dir.z;
+        cb = a + t * dir;
+    }
+    float3 dca = d_project_local(c, ca, dp0x, dp0y), dcb = d_project_local(c, cb, dp1x, dp1y);
+    float3 da = f3(0.f), db = f3(0.f);
+    if (a.z < c.clip_near) {
+        float3 dir = a - b;
+        float t = -(b.z + c.clip_near) / dir.z;
+        db += dca;
+        float dt = dot(dir, dca);
+        float3 ddir = t * dca;
+        db.z += -dt / dir.z;
+        ddir.z += dt * (b.z / (dir.z * dir.z));
+        da += ddir;
+        db -= ddir;
+        db += dcb;
+    } else if (b.z < c.clip_near) {
+        float3 dir = b - a;
+        float t = -(a.z + c.clip_near) / dir.z;
+        da += dcb;
+        float dt = dot(dir, dcb);
+        float3 ddir = t * dcb;
+        da.z += -dt / dir.z;
+        ddir.z += dt * (a.z / (dir.z * dir.z));
+        db += ddir;
+        da -= ddir;
+        da += dca;
+    } else {
+        da = dca;
+        db = dcb;
+    }
+    d_xfm_point(c.w2c, p0, da, dw2c);
+    d_xfm_point(c.w2c, p1, db, dw2c);
+}
+DEV bool in_screen(const DevCamera &c, float2 p) {
+    if (!c.fisheye) return p.x >= 0.f && p.x < 1.f && p.y >= 0.f && p.y < 1.f;
+    return (p.x - 0.5f) * (p.x - 0.5f) + (p.y - 0.5f) * (p.y - 0.5f) < 0.25f;
+}
+
+struct PrimaryEdgeResult {
+    bool ok;
+    DevEdge edge;
+    float3 dv0, dv1;
+    float dw2c[16];
+};
+
+DEV void primary_edge_sample(const DevScene &s, const EdgeSample &es, const DevEdge &edge, const LightSample &ls,
+                             const Rng &rng, int B, const float *d_image, int W, int H, float weight,
+                             PrimaryEdgeResult &r) {
+    r.ok = false;
+    const DevCamera &cam = s.cam;
+    float3 v0 = edge_v0(s, edge), v1 = edge_v1(s, edge);
+    float2 s0, s1;
+    if (!project(cam, v0, v1, s0, s1)) return;
+    float3 d0 = unproject(cam, s0.x, s0.y), d1 = unproject(cam, s1.x, s1.y);
+    float3 vd = d1 - d0;
+    float t = es.u;
+    float3 l0 = xfm_point(cam.w2c, v0), l1 = xfm_point(cam.w2c, v1);
+    float3 ept3 = d0 + t * vd;
+    float3 elocal = l0 + t * l1;  // as written in delta_ray.cpp:403
+    float2 ept = project_local(cam, ept3);
+    if (!in_screen(cam, ept)) return;
+    int xi = int(ept.x * W), yi = int(ept.y * H);
+    const float *dc = d_image + 3 * ((size_t)yi * W + xi);
+    float3 d_color = f3(dr_ldg(dc), dr_ldg(dc + 1), dr_ldg(dc + 2));
+    float delta = 1e-4f * length(elocal);
+    float3 split_n = normalize(cross(d0, d1));
+    float3 rdir = normalize(ept3 + delta * split_n);
+    float2 rpt = project_local(cam, rdir);
+    Ray rray = sample_primary(cam, rpt.x, rpt.y);
+    Hit hr = trace_closest(s, rray.o, rray.d, 1e-3f);
+    float3 ldir = normalize(ept3 - delta * split_n);
+    float2 lpt = project_local(cam, ldir);
+    Ray lray = sample_primary(cam, lpt.x, lpt.y);
+    Hit hl = trace_closest(s, lray.o, lray.d, 1e-3f);
+    bool rc = hr.tri >= 0 && s.tri[hr.tri].w == edge.shape &&
+              (s.tri_local[hr.tri] == edge.f0 || s.tri_local[hr.tri] == edge.f1);
+    bool lc = hl.tri >= 0 && s.tri[hl.tri].w == edge.shape &&
+              (s.tri_local[hl.tri] == edge.f0 || s.tri_local[hl.tri] == edge.f1);
+    if (!rc && !lc) return;
+    float3 rcol = f3(0.f), lcol = f3(0.f);
+    if (hr.tri >= 0) rcol = shade(s, -rray.d, hr.tri, intersect_tri(load_tri(s, hr.tri), rray.o, rray.d), ls, rng, B, true);
+    if (hl.tri >= 0) lcol = shade(s, -lray.d, hl.tri, intersect_tri(load_tri(s, hl.tri), lray.o, lray.d), ls, rng, B, true);
+    float3 diff = (rcol - lcol) * weight;
+    float3 xdiff = diff, ydiff = diff;
+    if (lpt.x > rpt.x) xdiff = -xdiff;
+    if (lpt.y > rpt.y) ydiff = -ydiff;
+    float3 edir = unproject(cam, ept.x, ept.y);
+    float3 dv0x, dv0y, dv1x, dv1y, dex, dey;
+    d_unproject(cam, s0.x, s0.y, dv0x, dv0y);
+    d_unproject(cam, s1.x, s1.y, dv1x, dv1y);
+    d_unproject(cam, ept.x, ept.y, dex, dey);
+    float3 c01 = cross(d0, d1);
+    float dadx = dot(dex, c01), dady = dot(dey, c01);
+    float a0x = fabsf(dot(cross(d1, edir), dv0x)), a0y = fabsf(dot(cross(d1, edir), dv0y));
+    float a1x = fabsf(dot(cross(edir, d0), dv1x)), a1y = fabsf(dot(cross(edir, d0), dv1y));
+    float dirac_j = 1.f / sqrtf(dadx * dadx + dady * dady);
+    float3 ept3d = d0 + (t + delta) * vd;
+    float2 eptd = project_local(cam, ept3d);
+    float ddx = (eptd.x - ept.x) / delta, ddy = (eptd.y - ept.y) / delta;
+    float line_j = sqrtf(ddx * ddx + ddy * ddy);
+    float jac = line_j * dirac_j;
+    float g0x = dot(-xdiff * a0x * jac, d_color), g0y = dot(-ydiff * a0y * jac, d_color);
+    float g1x = dot(-xdiff * a1x * jac, d_color), g1y = dot(-ydiff * a1y * jac, d_color);
+    const float h = 1e-3f;
+    float2 p0[6], p1[6];
+    for (int k = 0; k < 3; k++) {
+        float3 off = f3(k == 0 ? h : 0.f, k == 1 ? h : 0.f, k == 2 ? h : 0.f);
+        if (!project(cam, v0 + off, v1, p0[k], p1[k])) return;
+    }
+    for (int k = 0; k < 3; k++) {
+        float3 off = f3(k == 0 ? h : 0.f, k == 1 ? h : 0.f, k == 2 ? h : 0.f);
+        if (!project(cam, v0, v1 + off, p0[3 + k], p1[3 + k])) return;
+    }
+    float dv0[3], dv1[3];
+    for (int k = 0; k < 3; k++) {
+        float a0 = (p0[k].x - s0.x) / h, a1 = (p0[k].y - s0.y) / h;
+        float b0 = (p1[k].x - s1.x) / h, b1 = (p1[k].y - s1.y) / h;
+        dv0[k] = g0x * a0 + g0y * a1 + g1x * b0 + g1y * b1;
+        float c0 = (p0[3 + k].x - s0.x) / h, c1 = (p0[3 + k].y - s0.y) / h;
+        float e0 = (p1[3 + k].x - s1.x) / h, e1 = (p1[3 + k].y - s1.y) / h;
+        dv1[k] = g0x * c0 + g0y * c1 + g1x * e0 + g1y * e1;
+    }
+    r.ok = true;
+    r.edge = edge;
+    r.dv0 = f3(dv0[0], dv0[1], dv0[2]);
+    r.dv1 = f3(dv1[0], dv1[1], dv1[2]);
+    for (int i = 0; i < 16; i++) r.dw2c[i] = 0.f;
+    d_project(cam, v0, v1, g0x, g0y, g1x, g1y, r.dw2c);
+}

@@ -152,21 +152,6 @@ cudaError_t dr_launch_trace(const DevScene &s, const float *rays, long long n, i
 // Forward render: one pixel sample per (pixel, lane) and a segmented warp
 // reduction over the 2^lanes_log2 lanes of a pixel.
 // ---------------------------------------------------------------------------
-DEV float3 pixel_sample(const DevScene &s, int x, int y, int W, int H, int spp, int si, int B, uint64_t seed) {
-    Rng r;
-    r.init(seed, kStreamPixel, ((uint64_t)y * W + x) * spp + si, 0);
-    float sub_x = r.next() / spp;
-    float sub_y = r.next() / spp;
-    Ray ray = sample_primary(s.cam, float((x + sub_x) / W), float((y + sub_y) / H));
-    if (abs_sum(ray.d) == 0.f) return f3(0.f);
-    Hit h = trace_closest(s, ray.o, ray.d, 1e-3f);
-    if (h.tri < 0) return f3(0.f);
-    SurfacePoint sp = intersect_tri(load_tri(s, h.tri), ray.o, ray.d);
-    LightSample ls = draw_light(r);
-    float3 c = shade(s, -ray.d, h.tri, sp, ls, r, B, true);
-    return c * (1.f / spp);
-}
-
 __global__ void __launch_bounds__(256) k_render_forward(DevScene s, int W, int H, int spp, int B, uint64_t seed,
                                                         int lanes_log2, float *img) {
     long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
@@ -192,13 +177,15 @@ __global__ void __launch_bounds__(256) k_render_forward(DevScene s, int W, int H
 }
 
 cudaError_t dr_launch_forward(const DevScene &s, int W, int H, int spp, int B, uint64_t seed, float *img,
-                              cudaStream_t st, int *launches) {
+                              cudaStream_t st, int *launches, StageTimer *timer) {
     int lanes_log2 = 0;
     while ((1 << (lanes_log2 + 1)) <= spp && (1 << (lanes_log2 + 1)) <= 32 && spp % (1 << (lanes_log2 + 1)) == 0)
         lanes_log2++;
     long long threads = ((long long)W * H) << lanes_log2;
     const int bs = 256;
+    timer->begin(st);
     k_render_forward<<<blocks_for(threads, bs), bs, 0, st>>>(s, W, H, spp, B, seed, lanes_log2, img);
+    timer->mark(st, "k_render_forward");
     *launches += 1;
     return cudaGetLastError();
 }

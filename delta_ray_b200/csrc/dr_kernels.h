@@ -6,6 +6,25 @@
 
 #include "dr_scene.cuh"
 
+// Optional per-stage timing: events recorded on the launch stream around each
+// kernel when `on` is set (costs one event record per stage).
+struct StageTimer {
+    static const int kMax = 16;
+    bool on = false;
+    int n = 0;
+    cudaEvent_t ev[kMax + 1];
+    const char *names[kMax];
+    void begin(cudaStream_t st) {
+        n = 0;
+        if (on) cudaEventRecord(ev[0], st);
+    }
+    void mark(cudaStream_t st, const char *name) {
+        if (!on || n >= kMax) return;
+        names[n++] = name;
+        cudaEventRecord(ev[n], st);
+    }
+};
+
 // LBVH over n triangles (dr_kernels.cu); `nodes` holds 4 float4 per internal
 // node, `leaf_tris` 3 float4 per triangle; scratch >= dr_lbvh_scratch_bytes(n).
 cudaError_t dr_build_lbvh(const float *vtx, const int4 *tri, int n, float3 lo, float3 hi, float4 *nodes,
@@ -16,28 +35,32 @@ cudaError_t dr_launch_trace(const DevScene &s, const float *rays, long long n, i
                             int *launches);
 
 cudaError_t dr_launch_forward(const DevScene &s, int W, int H, int spp, int B, uint64_t seed, float *img,
-                              cudaStream_t st, int *launches);
+                              cudaStream_t st, int *launches, StageTimer *timer);
 
-// Backward pass (dr_backward.cu).  `ws` is the workspace described by
-// BackwardWorkspace; status receives device error bits.
+// Backward pass (dr_backward.cu).
 struct BackwardWorkspace {
-    // secondary shading points (one slot per pixel sample at most)
-    float *pt;         // [cap_points][PT_FLOATS] packed point records
-    int *pt_count;     // [1]
+    float *pt;                   // [cap_points][DR_PT_FLOATS] shading-point records
+    int *pt_count;               // [1]
     long long cap_points;
-    // edge items produced by the edge-tree traversal
-    int4 *items;       // (point id, edge list, edge index, edge ordinal j)
-    float *item_w;     // edge weight
-    int *item_count;   // [1]
+    int4 *items;                 // sampled edges: (point, tree << 30 | edge, ordinal j, 0)
+    float *item_w;               // edge weight
+    int *item_count;             // [1]
     long long cap_items;
-    float *item_dp;    // [cap_items][3] dp of each item (0 when it had none)
-    int *pt_last;      // [cap_points] index of the last item with nonzero dp
-    int *status;       // [1] error bits
+    float *item_dp;              // [cap_items][3] position adjoint of each item
+    unsigned long long *pt_last; // [cap_points] ((j + 1) << 32 | item) of the point's last item with dp != 0
+    int *status;                 // [1] error bits
+};
+
+// Which part of the flat gradient a block caches in shared memory:
+// [0, head) and [tail_begin, tail_begin + tail_len).
+struct GradCacheCfg {
+    int head, tail_begin, tail_len;
 };
 
 cudaError_t dr_launch_backward(const DevScene &s, int W, int H, int spp, int B, uint64_t seed, const float *d_image,
                                float *grad, float *img, long long primary_edge_samples, int dp_mode,
-                               const BackwardWorkspace &ws, cudaStream_t st, int *launches);
+                               const BackwardWorkspace &ws, const GradCacheCfg &cfg, int num_sms, cudaStream_t st,
+                               int *launches, StageTimer *timer);
 
 // Words of one packed secondary-point record in BackwardWorkspace::pt.
 #define DR_PT_FLOATS 24

@@ -26,7 +26,11 @@ DEV int material_of_tri(const DevScene &s, int tri) { return s.shapes[s.tri[tri]
 // ---------------------------------------------------------------------------
 struct Ray { float3 o, d; };
 
-DEV Ray sample_primary(const DevCamera &c, float sx, float sy) {
+// `ad`: use the arithmetic of the reference's differentiated pass, where a
+// division by a differentiable value is a multiply by its reciprocal
+// (autodiff.h:161-186); the backward pass needs those exact bits for the
+// shading point that edge sampling starts from.
+DEV Ray sample_primary(const DevCamera &c, float sx, float sy, bool ad = false) {
     Ray r;
     r.o = xfm_point(c.c2w, f3(0.f));
     if (c.fisheye) {
@@ -43,7 +47,7 @@ DEV Ray sample_primary(const DevCamera &c, float sx, float sy) {
         return r;
     }
     float ndcx = (sx - 0.5f) * -2.f;
-    float ndcy = (sy - 0.5f) * -2.f / c.aspect;
+    float ndcy = ad ? ((sy - 0.5f) * -2.f) * (1.f / c.aspect) : (sy - 0.5f) * -2.f / c.aspect;
     float3 dir = f3(c.fov * ndcx, c.fov * ndcy, 1.f);
     r.d = xfm_vector(c.c2w, normalize(dir));
     return r;
@@ -374,4 +378,21 @@ DEV float3 shade(const DevScene &s, float3 wi, int ptri, const SurfacePoint &psp
         csp = bh.sp;
     }
     return color;
+}
+
+// One pixel sample's radiance contribution (render_sample_fast,
+// delta_ray.cpp:640-692; sub-pixel jitter in [0, 1/spp) as :1236-1237).
+DEV float3 pixel_sample(const DevScene &s, int x, int y, int W, int H, int spp, int si, int B, uint64_t seed) {
+    Rng r;
+    r.init(seed, kStreamPixel, ((uint64_t)y * W + x) * spp + si, 0);
+    float sub_x = r.next() / spp;
+    float sub_y = r.next() / spp;
+    Ray ray = sample_primary(s.cam, float((x + sub_x) / W), float((y + sub_y) / H));
+    if (abs_sum(ray.d) == 0.f) return f3(0.f);
+    Hit h = trace_closest(s, ray.o, ray.d, 1e-3f);
+    if (h.tri < 0) return f3(0.f);
+    SurfacePoint sp = intersect_tri(load_tri(s, h.tri), ray.o, ray.d);
+    LightSample ls = draw_light(r);
+    float3 c = shade(s, -ray.d, h.tri, sp, ls, r, B, true);
+    return c * (1.f / spp);
 }

@@ -230,7 +230,9 @@ struct IsectFwd {  // forward intermediates of intersect_tri, kept for its adjoi
     bool div_fixed, flip;
 };
 
-DEV SurfacePoint intersect_tri(const TriData &td, float3 o, float3 d, IsectFwd *fw = nullptr) {
+// `ad`: reciprocal-multiply divisions, as the reference's differentiated pass
+// computes them (see sample_primary).
+DEV SurfacePoint intersect_tri(const TriData &td, float3 o, float3 d, IsectFwd *fw = nullptr, bool ad = false) {
     IsectFwd f;
     f.e1 = td.v1 - td.v0;
     f.e2 = td.v2 - td.v0;
@@ -240,12 +242,19 @@ DEV SurfacePoint intersect_tri(const TriData &td, float3 o, float3 d, IsectFwd *
     if (f.div_fixed) f.div = 1e-8f;  // intersect.h:80-83
     f.s = o - td.v0;
     f.ru = dot(f.s, f.pvec);
-    f.u = f.ru / f.div;
     f.qvec = cross(f.s, f.e1);
     f.rv = dot(d, f.qvec);
-    f.v = f.rv / f.div;
     f.rt = dot(f.e2, f.qvec);
-    f.t = f.rt / f.div;
+    if (ad) {
+        float inv = 1.f / f.div;
+        f.u = f.ru * inv;
+        f.v = f.rv * inv;
+        f.t = f.rt * inv;
+    } else {
+        f.u = f.ru / f.div;
+        f.v = f.rv / f.div;
+        f.t = f.rt / f.div;
+    }
     f.w = 1.f - (f.u + f.v);
     SurfacePoint sp;
     sp.uv.x = f.w * td.t0.x + f.u * td.t1.x + f.v * td.t2.x;

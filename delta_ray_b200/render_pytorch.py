@@ -105,6 +105,25 @@ class Scene:
     def split_grad(self, flat):
         return self.sd.split_grad(flat, self.materials, self.shapes)
 
+    def set_profiling(self, on=True):
+        _lib.check(_lib.lib().dr_scene_set_profiling(self.handle, int(bool(on))))
+
+    def last_timings(self):
+        """[(stage name, ms)] of the last render call (profiling must be on)."""
+        out = []
+        name = C.create_string_buffer(64)
+        ms = C.c_float()
+        i = 0
+        while _lib.lib().dr_scene_last_timings(self.handle, i, name, len(name), C.byref(ms)) == 0:
+            out.append((name.value.decode(), ms.value))
+            i += 1
+        return out
+
+    def last_counts(self):
+        p, it = C.c_int64(), C.c_int64()
+        _lib.check(_lib.lib().dr_scene_last_counts(self.handle, C.byref(p), C.byref(it)))
+        return p.value, it.value
+
     def launch_count(self):
         n = C.c_int()
         _lib.check(_lib.lib().dr_scene_last_launch_count(self.handle, C.byref(n)))

@@ -186,6 +186,19 @@ DR_API dr_status dr_render_backward(dr_scene *scene, const dr_render_desc *rd, c
 DR_API dr_status dr_trace_rays(dr_scene *scene, const float *rays_dev, int64_t n, int *tri_dev, float *t_dev,
                         void *stream);
 
+/* Tooling: per-stage GPU time of the following render calls.  With
+ * profiling on, each render records CUDA events around its kernels and
+ * synchronizes its stream at the end; dr_scene_last_timings then returns
+ * stage `index` (name and milliseconds) of the last call, DR_ERR_INVALID_ARGUMENT
+ * past the last stage.  No counterpart in the reference (its only timer is the
+ * progress reporter, progress_reporter.h:7-47). */
+DR_API dr_status dr_scene_set_profiling(dr_scene *scene, int enable);
+DR_API dr_status dr_scene_last_timings(const dr_scene *scene, int index, char *name, size_t name_len, float *ms);
+
+/* Work counts of the last backward call: secondary shading points and
+ * sampled edges (tooling). */
+DR_API dr_status dr_scene_last_counts(const dr_scene *scene, int64_t *points, int64_t *items);
+
 /* Kernel launch count of the last render call on this scene (for tooling). */
 DR_API dr_status dr_scene_last_launch_count(const dr_scene *scene, int *count);
 

@@ -2076,6 +2076,8 @@ inline void scatter_material(const Scene &sc, const GradLayout &L, const MatRec 
 
 inline float adj_of(int id) { return id >= 0 ? g_tape->adj[id] : 0.f; }
 
+thread_local int g_parts = 7;  // test knob: 1 continuous, 2 secondary edges, 4 primary edges
+
 V3f render_pixel_sample(const Scene &sc, const GradLayout &L, int W, int H, int xi, int yi, float sub_x, float sub_y,
                         int spp, int B, const V3f &d_color, bool derivs, StreamPlan &sp_plan, Accum &acc,
                         int dp_mode) {
@@ -2116,7 +2118,9 @@ V3f render_pixel_sample(const Scene &sc, const GradLayout &L, int W, int H, int 
     for (int c = 0; c < 3; c++)
         if (col[c].id >= 0) tape.adj[col[c].id] = d_color[c];
     tape.sweep();
-    double *g = acc.g.data();
+    std::vector<double> g_skip;
+    if (!(g_parts & 1)) g_skip.assign(acc.g.size(), 0.0);
+    double *g = (g_parts & 1) ? acc.g.data() : g_skip.data();
     for (int i = 0; i < 16; i++) g[i] += adj_of(cam_ids[i]);
     auto scatter_isect = [&](bool with_normals) {
         for (const IsectRec &ir : R.isect) {
@@ -2133,9 +2137,13 @@ V3f render_pixel_sample(const Scene &sc, const GradLayout &L, int W, int H, int 
         }
     };
     scatter_isect(true);
-    for (const MatRec &mr : R.mat) scatter_material(sc, L, mr, acc);
-    for (const LightRec &lr : R.light)
-        for (int c = 0; c < 3; c++) g[L.light[lr.light] + c] += adj_of(lr.I[c]);
+    if (g_parts & 1) {
+        for (const MatRec &mr : R.mat) scatter_material(sc, L, mr, acc);
+        for (const LightRec &lr : R.light)
+            for (int c = 0; c < 3; c++) g[L.light[lr.light] + c] += adj_of(lr.I[c]);
+    }
+    g = acc.g.data();
+    if (!(g_parts & 2)) return color;
     // secondary edges (delta_ray.cpp:868-974)
     struct DP { int id[3]; V3f dp; };
     std::vector<DP> dps;
@@ -2225,6 +2233,9 @@ template <typename F> static void parallel_loop(long long n, int workers, long l
 
 extern "C" {
 
+int dro_render_parts(const dr_scene_desc *desc, const dr_render_desc *rd, int rng_mode, int cores, const float *d_image,
+                     float *image, float *grad, long long *stats, int nthreads, const int *shape_rank, int parts);
+
 // rng_mode 0: the reference's mt19937 scheme with `cores` edge threads;
 // shape_rank (may be NULL) orders shapes in the edge map as the reference's
 // Shape* keys did;
@@ -2233,6 +2244,11 @@ extern "C" {
 // number of secondary points and sampled edges.
 int dro_render(const dr_scene_desc *desc, const dr_render_desc *rd, int rng_mode, int cores, const float *d_image,
                float *image, float *grad, long long *stats, int nthreads, const int *shape_rank) {
+    return dro_render_parts(desc, rd, rng_mode, cores, d_image, image, grad, stats, nthreads, shape_rank, 7);
+}
+
+int dro_render_parts(const dr_scene_desc *desc, const dr_render_desc *rd, int rng_mode, int cores, const float *d_image,
+                     float *image, float *grad, long long *stats, int nthreads, const int *shape_rank, int parts) {
     Scene sc;
     build_scene(sc, desc, nullptr, shape_rank);
     if (!sc.ltc) {
@@ -2261,6 +2277,7 @@ int dro_render(const dr_scene_desc *desc, const dr_render_desc *rd, int rng_mode
         int ti = (int)ti_;
         Tape tape;
         g_tape = &tape;
+        g_parts = parts;
         std::mt19937 trng(seeds[ti]);
         MtSampler mts(&trng);
         int tx = ti % ntx, ty = ti / ntx;
@@ -2291,7 +2308,7 @@ int dro_render(const dr_scene_desc *desc, const dr_render_desc *rd, int rng_mode
         g_tape = nullptr;
     });
     // pass B: primary edges (delta_ray.cpp:1468-1550)
-    if (derivs && !sc.primary_edges.empty()) {
+    if (derivs && !sc.primary_edges.empty() && (parts & 4)) {
         long long total = rd->primary_edge_samples > 0 ? rd->primary_edge_samples : (long long)spp * W * H;
         if (rng_mode == 0) {
             int per = (int)((long long)(spp * (W * H)) / cores);

@@ -39,6 +39,8 @@ def load():
                                    C.c_int, C.c_int, C.c_void_p, C.c_void_p, C.c_void_p,
                                    C.c_void_p, C.c_int, C.c_void_p]
         lib.dro_render.restype = C.c_int
+        lib.dro_render_parts.argtypes = list(lib.dro_render.argtypes) + [C.c_int]
+        lib.dro_render_parts.restype = C.c_int
         lib.dro_trace.argtypes = [C.POINTER(_abi.dr_scene_desc), C.c_void_p, C.c_longlong,
                                   C.c_void_p, C.c_void_p, C.c_void_p]
         lib.dro_philox.argtypes = [C.c_uint64, C.c_uint32, C.c_uint64, C.c_uint32, C.c_int,
@@ -56,8 +58,9 @@ def scene_desc(wl, ltc_table=None):
 
 def oracle_render(wl, seed, d_image=None, rng_mode=REFERENCE, cores=8, ltc_table=None,
                   dp_mode=_abi.DR_DP_REFERENCE_LAST, primary_edge_samples=0, threads=0,
-                  shape_rank=None):
-    """shape_rank: sort key per shape for the edge order (see dr_oracle.cpp Scene)."""
+                  shape_rank=None, parts=7):
+    """shape_rank: sort key per shape for the edge order (see dr_oracle.cpp Scene).
+    parts: backward terms to include (1 continuous, 2 secondary edges, 4 primary edges)."""
     lib = load()
     sd = scene_desc(wl, ltc_table)
     W, H = wl.resolution
@@ -71,10 +74,10 @@ def oracle_render(wl, seed, d_image=None, rng_mode=REFERENCE, cores=8, ltc_table
     rank = None
     if shape_rank is not None:
         rank = np.ascontiguousarray(np.asarray(shape_rank, np.int32))
-    lib.dro_render(C.byref(sd.desc), C.byref(rd), int(rng_mode), int(cores),
-                   None if dimg is None else dimg.ctypes.data, image.ctypes.data,
-                   grad.ctypes.data, stats.ctypes.data, int(threads),
-                   None if rank is None else rank.ctypes.data)
+    lib.dro_render_parts(C.byref(sd.desc), C.byref(rd), int(rng_mode), int(cores),
+                         None if dimg is None else dimg.ctypes.data, image.ctypes.data,
+                         grad.ctypes.data, stats.ctypes.data, int(threads),
+                         None if rank is None else rank.ctypes.data, int(parts))
     out = {"image": image, "grad": grad, "stats": stats}
     if d_image is not None:
         cam, mats, shps, _ = _abi.scene_dicts(wl.camera, wl.materials, wl.shapes, wl.lights)

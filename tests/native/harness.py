@@ -1,0 +1,70 @@
+"""Test infrastructure: ctypes front end of tests/native/host_harness.cpp.
+
+The harness runs the renderer's per-sample kernel logic on the CPU; the
+library is built by ``build()`` into tests/_build/libhost_harness.so.
+"""
+import ctypes as C
+import os
+import subprocess
+
+import numpy as np
+import torch
+
+HERE = os.path.dirname(os.path.abspath(__file__))
+ROOT = os.path.dirname(os.path.dirname(HERE))
+LIB = os.path.join(ROOT, "tests", "_build", "libhost_harness.so")
+_lib = None
+
+
+def build():
+    src = os.path.join(HERE, "host_harness.cpp")
+    csrc = os.path.join(ROOT, "delta_ray_b200", "csrc")
+    deps = [src] + [os.path.join(csrc, f) for f in os.listdir(csrc)]
+    if os.path.exists(LIB) and all(os.path.getmtime(d) <= os.path.getmtime(LIB) for d in deps):
+        return LIB
+    os.makedirs(os.path.dirname(LIB), exist_ok=True)
+    subprocess.run(["g++", "-std=c++17", "-O2", "-fPIC", "-shared", "-DDR_HOST_BUILD", "-o", LIB, src],
+                   check=True)
+    return LIB
+
+
+def load():
+    global _lib
+    if _lib is None:
+        from delta_ray_b200 import _abi
+        build()
+        L = C.CDLL(LIB)
+        L.hh_render.argtypes = [C.POINTER(_abi.dr_scene_desc), C.POINTER(_abi.dr_render_desc), C.c_void_p,
+                                C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]
+        L.hh_trace.argtypes = [C.POINTER(_abi.dr_scene_desc), C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]
+        L.hh_trace.restype = C.c_longlong
+        _lib = L
+    return _lib
+
+
+def render(wl, seed, d_image=None, parts=7, ltc_table=None, dp_mode=0, primary_edge_samples=0):
+    from delta_ray_b200 import _abi
+    L = load()
+    cam, mats, shps, lts = _abi.scene_dicts(wl.camera, wl.materials, wl.shapes, wl.lights)
+    sd = _abi.SceneDesc.from_scene(cam, mats, shps, lts, torch.device("cpu"), ltc_table)
+    W, H = wl.resolution
+    rd = _abi.render_desc(W, H, wl.spp, wl.max_bounces, seed, primary_edge_samples, dp_mode)
+    image = np.zeros((H, W, 3), np.float32)
+    grad = np.zeros(sd.grad_total, np.float32)
+    stats = np.zeros(2, np.int64)
+    dimg = None if d_image is None else np.ascontiguousarray(np.asarray(d_image, np.float32))
+    L.hh_render(C.byref(sd.desc), C.byref(rd), None if dimg is None else dimg.ctypes.data, image.ctypes.data,
+                grad.ctypes.data, int(parts), stats.ctypes.data)
+    return {"image": image, "grad": grad, "stats": stats, "sd": sd}
+
+
+def trace(wl, rays):
+    from delta_ray_b200 import _abi
+    L = load()
+    cam, mats, shps, lts = _abi.scene_dicts(wl.camera, wl.materials, wl.shapes, wl.lights)
+    sd = _abi.SceneDesc.from_scene(cam, mats, shps, lts, torch.device("cpu"))
+    rays = np.ascontiguousarray(np.asarray(rays, np.float32).reshape(-1, 6))
+    tri = np.zeros(len(rays), np.int32)
+    t = np.zeros(len(rays), np.float32)
+    visits = L.hh_trace(C.byref(sd.desc), rays.ctypes.data, len(rays), tri.ctypes.data, t.ctypes.data)
+    return tri, t, visits

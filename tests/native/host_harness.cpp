@@ -1,28 +1,23 @@
-// Test infrastructure: the renderer's __host__ __device__ kernel logic compiled
-// for the CPU (DR_HOST_BUILD), so that tests can inspect it without a GPU.
-// Never part of the product: the product runs this code only on the GPU.
+// Test infrastructure: the renderer's per-sample kernel logic (the
+// __host__ __device__ functions of delta_ray_b200/csrc) compiled for the CPU
+// with DR_HOST_BUILD, driven sequentially.  Tests compare it with the oracle
+// and use it to inspect the traversal.  Never part of the product: the product
+// runs this code only on the GPU.
 #include <algorithm>
 #include <numeric>
 #include <vector>
 
-#include "../../delta_ray_b200/csrc/dr_bvh.cuh"
-#include "../../delta_ray_b200/csrc/dr_trace.cuh"
-
 thread_local long long g_dr_visits = 0;
+
+#include "../../delta_ray_b200/csrc/dr_backward.cuh"
+#include "../../delta_ray_b200/csrc/dr_bvh.cuh"
+#include "../../delta_ray_b200/csrc/dr_host_scene.h"
 
 namespace {
 
 // host replica of the device LBVH build (dr_kernels.cu: dr_build_lbvh)
-void build_lbvh(const float *vtx, const int4 *tri, int n, std::vector<float4> &nodes, std::vector<float4> &leaves) {
-    float3 lo = f3(1e30f), hi = f3(-1e30f);
-    for (int i = 0; i < n; i++) {
-        const int *t = &tri[i].x;
-        for (int k = 0; k < 3; k++) {
-            const float *p = vtx + 3 * t[k];
-            lo = f3(std::min(lo.x, p[0]), std::min(lo.y, p[1]), std::min(lo.z, p[2]));
-            hi = f3(std::max(hi.x, p[0]), std::max(hi.y, p[1]), std::max(hi.z, p[2]));
-        }
-    }
+void build_lbvh(const float *vtx, const int4 *tri, int n, float3 lo, float3 hi, std::vector<float4> &nodes,
+                std::vector<float4> &leaves) {
     BvhBuildIn in;
     in.vtx = vtx;
     in.tri = tri;
@@ -37,8 +32,8 @@ void build_lbvh(const float *vtx, const int4 *tri, int n, std::vector<float4> &n
     std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return keys[a] < keys[b]; });
     std::vector<uint32_t> skeys(n);
     for (int i = 0; i < n; i++) skeys[i] = keys[order[i]];
-    leaves.assign(3 * n, float4{});
-    std::vector<Box> leaf_boxes(n), node_boxes(std::max(1, n));
+    leaves.assign(3 * std::max(1, n), float4{});
+    std::vector<Box> leaf_boxes(std::max(1, n)), node_boxes(std::max(1, n));
     for (int i = 0; i < n; i++) {
         int t = order[i];
         const int *id = &tri[t].x;
@@ -73,56 +68,139 @@ void build_lbvh(const float *vtx, const int4 *tri, int n, std::vector<float4> &n
     }
 }
 
+struct HostSceneBundle {
+    drhost::HostScene h;
+    drhost::FlatScene f;
+    std::vector<float4> nodes, leaves;
+    DevScene ds;
+};
+
+struct HostSink {
+    std::vector<double> *g;
+    void add(int i, float v) { (*g)[i] += v; }
+};
+
+void make_scene(const dr_scene_desc *desc, HostSceneBundle &b) {
+    drhost::load_desc(b.h, desc, [](auto p, size_t n, const char *) {
+        using T = typename std::remove_const<typename std::remove_pointer<decltype(p)>::type>::type;
+        return std::vector<T>(p, p + n);
+    });
+    b.h.preprocess();
+    drhost::flatten(b.h, b.f);
+    build_lbvh(b.f.vtx.data(), b.f.tri.data(), (int)b.f.tri.size(), b.f.lo, b.f.hi, b.nodes, b.leaves);
+    drhost::ScenePtrs p;
+    p.vtx = b.f.vtx.data();
+    p.nrm = b.f.nrm.data();
+    p.uv = b.f.uv.data();
+    p.tri = b.f.tri.data();
+    p.tri_local = b.f.tri_local.data();
+    p.bvh_nodes = b.nodes.data();
+    p.bvh_tris = b.leaves.data();
+    p.shapes = b.f.shapes.data();
+    p.mats = b.h.mats.data();
+    p.texels = b.h.texels.data();
+    p.lights = b.h.lights.data();
+    p.light_sel_cdf = b.h.light_sel.cdf.data();
+    p.light_sel_func = b.h.light_sel.func.data();
+    p.light_tri_cdf = b.h.light_tri_cdf.data();
+    p.light_tri_func = b.h.light_tri_func.data();
+    p.prim_edges = b.h.prim_edges.data();
+    p.prim_cdf = b.h.prim_dist.cdf.data();
+    p.prim_func = b.h.prim_dist.func.data();
+    p.sil_nodes = b.h.sil_nodes.data();
+    p.sil_edges = b.h.sil_edges.data();
+    p.nrm_nodes = b.h.nrm_nodes.data();
+    p.nrm_edges = b.h.nrm_edges.data();
+    p.ltc = b.h.ltc.data();
+    drhost::fill_devscene(b.ds, b.h, b.f, p);
+}
+
 }  // namespace
 
 extern "C" {
 
-// Builds the LBVH over (vtx, tri) and traces n rays [n][6]; writes the hit
-// triangle, t, and returns the total number of BVH nodes visited.
-long long hh_trace(const float *vtx, const int *tri4, int ntri, const float *rays, int n, int *out_tri, float *out_t) {
-    std::vector<float4> nodes, leaves;
-    build_lbvh(vtx, (const int4 *)tri4, ntri, nodes, leaves);
-    DevScene s;
-    std::memset(&s, 0, sizeof(s));
-    s.num_tris = ntri;
-    s.bvh_nodes = nodes.data();
-    s.bvh_tris = leaves.data();
-    s.bvh_root = ntri > 1 ? 0 : ~0;
+// Forward (d_image == NULL) or backward render with the kernel logic on the
+// CPU.  `parts` selects the backward terms: 1 path adjoint, 2 secondary
+// edges, 4 primary edges.  stats: [points, items].
+int hh_render(const dr_scene_desc *desc, const dr_render_desc *rd, const float *d_image, float *image, float *grad,
+              int parts, long long *stats) {
+    HostSceneBundle b;
+    make_scene(desc, b);
+    const DevScene &s = b.ds;
+    int W = rd->width, H = rd->height, spp = rd->spp, B = rd->max_bounces;
+    uint64_t seed = rd->seed;
+    std::vector<double> g(b.h.grad_total, 0.0);
+    HostSink sink{&g};
+    std::vector<PointRecord> pts;
+    auto push = [&](const PointRecord &pr) { pts.push_back(pr); };
+    for (int y = 0; y < H; y++)
+        for (int x = 0; x < W; x++) {
+            float3 acc = f3(0.f);
+            float3 dc = d_image ? f3(d_image[3 * (y * W + x)], d_image[3 * (y * W + x) + 1], d_image[3 * (y * W + x) + 2])
+                                : f3(0.f);
+            for (int si = 0; si < spp; si++) {
+                if (!d_image) acc += pixel_sample(s, x, y, W, H, spp, si, B, seed);
+                else if (parts & 1) acc += backward_pixel_sample(s, x, y, W, H, spp, si, B, seed, dc, sink, push);
+                else {
+                    std::vector<double> tmp(g.size(), 0.0);
+                    HostSink ts{&tmp};
+                    acc += backward_pixel_sample(s, x, y, W, H, spp, si, B, seed, dc, ts, push);
+                }
+            }
+            image[3 * (y * W + x)] = acc.x;
+            image[3 * (y * W + x) + 1] = acc.y;
+            image[3 * (y * W + x) + 2] = acc.z;
+        }
+    long long nitems = 0;
+    if (d_image && (parts & 2)) {
+        struct Item { int pt, tree, ei, j; float w; };
+        std::vector<Item> items;
+        for (int p = 0; p < (int)pts.size(); p++) {
+            auto emit = [&](int tree, int ei, int j, float w) { items.push_back(Item{p, tree, ei, j, w}); };
+            traverse_point(s, pts[p], seed, emit);
+        }
+        nitems = (long long)items.size();
+        std::vector<int> last(pts.size(), -1);
+        std::vector<float3> last_dp(pts.size(), f3(0.f));
+        for (const Item &it : items) {
+            float3 dp = eval_item(s, pts[it.pt], it.tree, it.ei, it.j, it.w, spp, B, seed, sink);
+            if (is_zero(dp)) continue;
+            if (rd->dp_mode == DR_DP_SUM) {
+                propagate_dp(s, pts[it.pt], W, H, spp, seed, dp, sink);
+            } else if (it.j > last[it.pt]) {
+                last[it.pt] = it.j;
+                last_dp[it.pt] = dp;
+            }
+        }
+        if (rd->dp_mode != DR_DP_SUM)
+            for (size_t p = 0; p < pts.size(); p++)
+                if (last[p] >= 0) propagate_dp(s, pts[p], W, H, spp, seed, last_dp[p], sink);
+    }
+    if (d_image && (parts & 4)) {
+        long long npe = rd->primary_edge_samples > 0 ? rd->primary_edge_samples : (long long)spp * W * H;
+        for (long long i = 0; i < npe; i++) primary_edge_item(s, i, W, H, spp, B, seed, d_image, sink);
+    }
+    if (grad)
+        for (size_t i = 0; i < g.size(); i++) grad[i] = (float)g[i];
+    if (stats) {
+        stats[0] = (long long)pts.size();
+        stats[1] = nitems;
+    }
+    return 0;
+}
+
+// Builds the LBVH over the scene and traces rays [n][6]; returns node visits.
+long long hh_trace(const dr_scene_desc *desc, const float *rays, int n, int *out_tri, float *out_t) {
+    HostSceneBundle b;
+    make_scene(desc, b);
     g_dr_visits = 0;
     for (int i = 0; i < n; i++) {
         const float *r = rays + 6 * i;
-        Hit h = trace_closest(s, f3(r[0], r[1], r[2]), f3(r[3], r[4], r[5]), 1e-3f);
+        Hit h = trace_closest(b.ds, f3(r[0], r[1], r[2]), f3(r[3], r[4], r[5]), 1e-3f);
         out_tri[i] = h.tri;
         out_t[i] = h.t;
     }
     return g_dr_visits;
-}
-
-// LBVH statistics: depth histogram max and the sum of node box surface areas.
-void hh_bvh_stats(const float *vtx, const int *tri4, int ntri, double *out) {
-    std::vector<float4> nodes, leaves;
-    build_lbvh(vtx, (const int4 *)tri4, ntri, nodes, leaves);
-    int maxd = 0;
-    double area = 0.0;
-    std::vector<std::pair<int, int>> st;
-    st.push_back({0, 0});
-    while (!st.empty()) {
-        auto [nd, d] = st.back();
-        st.pop_back();
-        maxd = std::max(maxd, d);
-        if (nd < 0) continue;
-        const float4 *q = &nodes[4 * nd];
-        float b0[6] = {q[0].x, q[0].y, q[0].z, q[0].w, q[1].x, q[1].y};
-        float b1[6] = {q[1].z, q[1].w, q[2].x, q[2].y, q[2].z, q[2].w};
-        for (float *b : {b0, b1}) {
-            float dx = b[3] - b[0], dy = b[4] - b[1], dz = b[5] - b[2];
-            area += 2.0 * (dx * dy + dy * dz + dz * dx);
-        }
-        st.push_back({dr_f2i(q[3].x), d + 1});
-        st.push_back({dr_f2i(q[3].y), d + 1});
-    }
-    out[0] = maxd;
-    out[1] = area;
 }
 
 }  // extern "C"

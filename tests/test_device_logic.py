@@ -1,0 +1,59 @@
+"""The renderer's kernel logic, compiled for the CPU, against the oracle.
+
+The CUDA kernels are thin wrappers over __host__ __device__ functions
+(delta_ray_b200/csrc/*.cuh).  tests/native/host_harness.cpp compiles those
+same functions for the CPU; with the Philox streams shared by both sides, every
+sample must reproduce the oracle's tape-AD gradients to float round-off.  The
+CPU build is test infrastructure only: the product never runs it.
+"""
+import numpy as np
+import pytest
+
+from conftest import build_golden_scene, golden_cases, load_golden, rel_err
+import oracle
+from native import harness
+
+TOL = 1e-5
+
+
+@pytest.mark.parametrize("case", golden_cases())
+def test_kernel_logic_matches_oracle(case, ltc_table):
+    meta, gold = load_golden(case)
+    wl = build_golden_scene(meta)
+    seed = meta["seed"]
+    h = harness.render(wl, seed, ltc_table=ltc_table)
+    o = oracle.oracle_render(wl, seed, rng_mode=oracle.PHILOX, ltc_table=ltc_table)
+    assert rel_err(h["image"], o["image"]) < TOL
+    for parts in (1, 2, 4):
+        h = harness.render(wl, seed, gold["d_image"], parts=parts, ltc_table=ltc_table)
+        o = oracle.oracle_render(wl, seed, gold["d_image"], rng_mode=oracle.PHILOX, ltc_table=ltc_table,
+                                 parts=parts)
+        if parts == 2:
+            assert h["stats"][1] == o["stats"][1], "different edges were sampled"
+        if np.abs(o["grad"]).max() == 0:
+            assert np.abs(h["grad"]).max() == 0
+        else:
+            assert rel_err(h["grad"], o["grad"]) < TOL, f"gradient term {parts}"
+
+
+def test_dp_sum_mode_matches_oracle(ltc_table):
+    meta, gold = load_golden("soft_shadow")
+    wl = build_golden_scene(meta)
+    h = harness.render(wl, 9, gold["d_image"], parts=2, dp_mode=1)
+    o = oracle.oracle_render(wl, 9, gold["d_image"], rng_mode=oracle.PHILOX, parts=2, dp_mode=1)
+    assert rel_err(h["grad"], o["grad"]) < TOL
+
+
+def test_traversal_visits_few_nodes():
+    """Closest-hit traversal of a 130k-triangle heightfield stays logarithmic."""
+    from delta_ray_b200 import workloads
+    wl = workloads.heightfield(seed=0)
+    rng = np.random.default_rng(0)
+    n = 2000
+    o = np.tile([0.0, 7.0, -9.0], (n, 1))
+    tgt = np.stack([rng.uniform(-4, 4, n), np.zeros(n), rng.uniform(-4, 4, n)], 1)
+    d = tgt - o
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    tri, t, visits = harness.trace(wl, np.concatenate([o, d], 1))
+    assert (tri >= 0).mean() > 0.99
+    assert visits / n < 200
