@@ -16,6 +16,7 @@
 #include <cstring>
 #include <map>
 #include <memory>
+#include <mutex>
 #include <stdexcept>
 #include <string>
 #include <tuple>
@@ -72,6 +73,74 @@ template <typename T> std::vector<T> fetch(const T *src, size_t count, const cha
     return v;
 }
 
+// Backward work queues: shading points, sampled edges and their adjoints, tens
+// of bytes per pixel sample and per edge sample.  A destroyed scene hands its
+// queues to a one-slot cache per device and the next scene on that device
+// takes them from there, so a loop that builds a new scene every step (as the
+// reference's RenderFunction does) allocates them once.  Only idle queues are
+// cached; `idle` orders their reuse after the last kernels that touched them.
+struct BackwardQueues {
+    DevBuf pt, items, item_w, item_dp, pt_last, counts;
+    long long cap_items = 0;  // grown on overflow, kept with the buffers
+    cudaEvent_t idle = nullptr;
+    ~BackwardQueues() {
+        if (idle) cudaEventDestroy(idle);
+    }
+};
+
+// The caches are never destroyed: freeing device memory during static
+// destruction would race the CUDA runtime's own teardown.
+std::mutex &cache_mutex() {
+    static std::mutex *m = new std::mutex();
+    return *m;
+}
+std::map<int, std::unique_ptr<BackwardQueues>> &queue_cache() {
+    static auto *c = new std::map<int, std::unique_ptr<BackwardQueues>>();
+    return *c;
+}
+
+std::unique_ptr<BackwardQueues> take_queues(int device, cudaStream_t st) {
+    std::unique_ptr<BackwardQueues> q;
+    {
+        std::lock_guard<std::mutex> lk(cache_mutex());
+        auto it = queue_cache().find(device);
+        if (it != queue_cache().end()) q = std::move(it->second);
+    }
+    if (!q) return std::unique_ptr<BackwardQueues>(new BackwardQueues());
+    if (q->idle) check_cuda(cudaStreamWaitEvent(st, q->idle, 0), "cudaStreamWaitEvent");
+    return q;
+}
+
+void give_back_queues(int device, std::unique_ptr<BackwardQueues> q) {
+    if (!q) return;
+    std::lock_guard<std::mutex> lk(cache_mutex());
+    auto &slot = queue_cache()[device];
+    // keep the larger set; the other one is freed here
+    if (!slot || slot->cap_items < q->cap_items) slot = std::move(q);
+}
+
+// Device copies of LTC tables, one per device, shared by the scenes that use
+// the same table.
+struct LtcCache {
+    std::vector<float> host;
+    std::shared_ptr<DevBuf> dev;
+};
+std::map<int, LtcCache> &ltc_cache() {
+    static auto *c = new std::map<int, LtcCache>();
+    return *c;
+}
+
+std::shared_ptr<DevBuf> device_ltc(int device, const std::vector<float> &table) {
+    std::lock_guard<std::mutex> lk(cache_mutex());
+    LtcCache &c = ltc_cache()[device];
+    if (c.dev && c.host == table) return c.dev;
+    std::shared_ptr<DevBuf> d(new DevBuf());
+    d->upload(table);
+    c.host = table;
+    c.dev = d;
+    return d;
+}
+
 }  // namespace
 
 using namespace drhost;
@@ -81,9 +150,9 @@ struct dr_scene {
     HostScene h;
     DevBuf vtx, nrm, uv, tri, tri_local, bvh_nodes, bvh_tris, shapes, mats, texels, lights, light_sel_cdf,
         light_sel_func, light_tri_cdf, light_tri_func, prim_edges, prim_cdf, prim_func, sil_nodes, sil_edges,
-        nrm_nodes, nrm_edges, ltc, status, bvh_scratch;
-    // backward workspace (grown on demand)
-    DevBuf ws_pt, ws_items, ws_item_w, ws_item_dp, ws_pt_last, ws_counts;
+        nrm_nodes, nrm_edges, status, bvh_scratch;
+    std::shared_ptr<DevBuf> ltc;
+    std::unique_ptr<BackwardQueues> queues;  // taken at the first backward call
     DevScene ds;
     StageTimer timer;
     bool timer_ready = false;
@@ -93,6 +162,7 @@ struct dr_scene {
     ~dr_scene() {
         if (timer_ready)
             for (int i = 0; i <= StageTimer::kMax; i++) cudaEventDestroy(timer.ev[i]);
+        give_back_queues(device, std::move(queues));
     }
     int last_launches = 0;
 };
@@ -126,7 +196,7 @@ void upload_scene(dr_scene *sc, cudaStream_t st) {
     sc->sil_edges.upload(h.sil_edges);
     sc->nrm_nodes.upload(h.nrm_nodes);
     sc->nrm_edges.upload(h.nrm_edges);
-    sc->ltc.upload(h.ltc);
+    sc->ltc = device_ltc(sc->device, h.ltc);
     sc->status.reserve(sizeof(int) * 4);
     // device LBVH
     int n = sc->num_tris;
@@ -165,7 +235,7 @@ void upload_scene(dr_scene *sc, cudaStream_t st) {
     ptr.sil_edges = sc->sil_edges.as<DevEdge>();
     ptr.nrm_nodes = sc->nrm_nodes.as<DevEdgeNode>();
     ptr.nrm_edges = sc->nrm_edges.as<DevEdge>();
-    ptr.ltc = sc->ltc.as<float>();
+    ptr.ltc = sc->ltc->as<float>();
     fill_devscene(sc->ds, h, f, ptr);
 }
 
@@ -315,53 +385,76 @@ dr_status dr_render_backward(dr_scene *scene, const dr_render_desc *rd, const fl
         check_cuda(cudaSetDevice(scene->device), "cudaSetDevice");
         cudaStream_t st = (cudaStream_t)stream;
         scene->last_launches = 0;
-        long long npix = (long long)rd->width * rd->height * rd->spp;
-        // one secondary point per pixel sample and bounce before the first
-        // non-specular bounce; items: an initial guess, grown on overflow
-        long long cap_points = npix * std::max(1, std::min(rd->max_bounces, 2));
-        long long cap_items = std::max<long long>(npix * 8, 1 << 16);
-        for (int attempt = 0; attempt < 4; attempt++) {
-            scene->ws_pt.reserve(sizeof(float) * DR_PT_FLOATS * cap_points);
-            scene->ws_pt_last.reserve(sizeof(unsigned long long) * cap_points);
-            scene->ws_items.reserve(sizeof(int4) * cap_items);
-            scene->ws_item_w.reserve(sizeof(float) * cap_items);
-            scene->ws_item_dp.reserve(sizeof(float) * 3 * cap_items);
-            scene->ws_counts.reserve(sizeof(int) * 4);
-            BackwardWorkspace ws;
-            ws.pt = scene->ws_pt.as<float>();
-            ws.pt_last = scene->ws_pt_last.as<unsigned long long>();
-            ws.cap_points = cap_points;
-            ws.items = scene->ws_items.as<int4>();
-            ws.item_w = scene->ws_item_w.as<float>();
-            ws.item_dp = scene->ws_item_dp.as<float>();
+        // each pixel sample hands at most one shading point to edge sampling
+        long long cap_points = (long long)rd->width * rd->height * rd->spp;
+        if (!scene->queues) scene->queues = take_queues(scene->device, st);
+        BackwardQueues &q = *scene->queues;
+        long long cap_items = std::max(q.cap_items, std::max<long long>(cap_points * 4, 1 << 16));
+        q.pt.reserve(sizeof(float) * DR_PT_FLOATS * cap_points);
+        q.pt_last.reserve(sizeof(unsigned long long) * cap_points);
+        q.counts.reserve(sizeof(int) * 4);
+        if (!q.idle) check_cuda(cudaEventCreateWithFlags(&q.idle, cudaEventDisableTiming), "cudaEventCreate");
+        // marks the queues busy up to here on every way out, errors included
+        struct MarkIdle {
+            cudaEvent_t e;
+            cudaStream_t st;
+            ~MarkIdle() { cudaEventRecord(e, st); }
+        } mark_idle{q.idle, st};
+        GradCacheCfg cfg = grad_cache_cfg(scene->h);
+        BackwardWorkspace ws;
+        auto bind_items = [&]() {
+            q.items.reserve(sizeof(int4) * cap_items);
+            q.item_w.reserve(sizeof(float) * cap_items);
+            q.item_dp.reserve(sizeof(float) * 3 * cap_items);
+            q.cap_items = cap_items;
+            ws.items = q.items.as<int4>();
+            ws.item_w = q.item_w.as<float>();
+            ws.item_dp = q.item_dp.as<float>();
             ws.cap_items = cap_items;
-            ws.pt_count = scene->ws_counts.as<int>();
-            ws.item_count = scene->ws_counts.as<int>() + 1;
-            ws.status = scene->ws_counts.as<int>() + 2;
-            check_cuda(cudaMemsetAsync(scene->ws_counts.p, 0, sizeof(int) * 4, st), "memset");
-            check_cuda(cudaMemsetAsync(grad_dev, 0, sizeof(float) * scene->h.grad_total, st), "memset");
-            check_cuda(dr_launch_backward(scene->ds, rd->width, rd->height, rd->spp, rd->max_bounces, rd->seed,
-                                          d_image_dev, grad_dev, image_dev, rd->primary_edge_samples, rd->dp_mode,
-                                          ws, grad_cache_cfg(scene->h), scene->num_sms, st, &scene->last_launches,
-                                          &scene->timer),
-                       "backward launch");
-            int counts[4];
-            check_cuda(cudaMemcpyAsync(counts, scene->ws_counts.p, sizeof(counts), cudaMemcpyDeviceToHost, st),
+        };
+        ws.pt = q.pt.as<float>();
+        ws.pt_last = q.pt_last.as<unsigned long long>();
+        ws.cap_points = cap_points;
+        ws.pt_count = q.counts.as<int>();
+        ws.item_count = q.counts.as<int>() + 1;
+        ws.status = q.counts.as<int>() + 2;
+        bind_items();
+        int counts[4];
+        auto read_counts = [&]() {
+            check_cuda(cudaMemcpyAsync(counts, q.counts.p, sizeof(counts), cudaMemcpyDeviceToHost, st),
                        "status read");
             check_cuda(cudaStreamSynchronize(st), "backward");
-            int status = counts[2];
-            scene->last_points = counts[0];
-            scene->last_items = counts[1];
-            collect_timings(scene, st);
-            if (status & (DR_STATUS_POINT_OVERFLOW | DR_STATUS_ITEM_OVERFLOW)) {
-                if (status & DR_STATUS_POINT_OVERFLOW) cap_points *= 2;
-                if (status & DR_STATUS_ITEM_OVERFLOW) cap_items = std::max(cap_items * 2, (long long)counts[1] + 1);
-                continue;
-            }
-            if (status) throw DrError(DR_ERR_DEVICE_STATUS, "device reported status " + std::to_string(status));
-            return;
+        };
+        check_cuda(cudaMemsetAsync(q.counts.p, 0, sizeof(int) * 4, st), "memset");
+        check_cuda(cudaMemsetAsync(grad_dev, 0, sizeof(float) * scene->h.grad_total, st), "memset");
+        check_cuda(dr_launch_backward_front(scene->ds, rd->width, rd->height, rd->spp, rd->max_bounces, rd->seed,
+                                            d_image_dev, grad_dev, image_dev, rd->primary_edge_samples, rd->dp_mode,
+                                            ws, cfg, scene->num_sms, st, &scene->last_launches, &scene->timer),
+                   "backward launch");
+        read_counts();
+        for (int attempt = 0; counts[2] & DR_STATUS_ITEM_OVERFLOW; attempt++) {
+            // the traversal reported how many items it needed: grow the item
+            // queue to that (kept for later calls) and re-run the traversal
+            if (attempt == 3) throw DrError(DR_ERR_DEVICE_STATUS, "edge item queue kept overflowing");
+            cap_items = std::max(cap_items * 2, (long long)counts[1] + (counts[1] >> 3) + 1);
+            bind_items();
+            check_cuda(cudaMemsetAsync(q.counts.as<int>() + 1, 0, sizeof(int) * 2, st), "memset");
+            check_cuda(dr_launch_edge_traverse(scene->ds, rd->seed, ws, scene->num_sms, st, &scene->last_launches,
+                                               &scene->timer),
+                       "edge traversal launch");
+            read_counts();
         }
-        throw DrError(DR_ERR_DEVICE_STATUS, "edge work queues kept overflowing");
+        if (counts[2]) throw DrError(DR_ERR_DEVICE_STATUS, "device reported status " + std::to_string(counts[2]));
+        scene->timer.mark(st, "host_queue_check");
+        check_cuda(dr_launch_backward_back(scene->ds, rd->width, rd->height, rd->spp, rd->max_bounces, rd->seed,
+                                           grad_dev, rd->dp_mode, ws, cfg, scene->num_sms, st, &scene->last_launches,
+                                           &scene->timer),
+                   "backward launch");
+        read_counts();
+        scene->last_points = counts[0];
+        scene->last_items = counts[1];
+        collect_timings(scene, st);
+        if (counts[2]) throw DrError(DR_ERR_DEVICE_STATUS, "device reported status " + std::to_string(counts[2]));
     });
 }
 

@@ -57,6 +57,23 @@ __device__ __forceinline__ void block_grad_flush(const BlockGrad &b) {
 
 __device__ __forceinline__ void set_status(int *status, int bit) { atomicOr(status, bit); }
 
+// Reserves `count` consecutive slots for each lane of the (fully converged)
+// warp with one atomic: returns the lane's first slot.
+__device__ __forceinline__ long long warp_reserve(int *counter, int count) {
+    const unsigned full = 0xffffffffu;
+    int lane = threadIdx.x & 31;
+    int incl = count;
+    for (int off = 1; off < 32; off <<= 1) {
+        int v = __shfl_up_sync(full, incl, off);
+        if (lane >= off) incl += v;
+    }
+    int total = __shfl_sync(full, incl, 31);
+    long long base = 0;
+    if (lane == 31 && total > 0) base = atomicAdd(counter, total);
+    base = __shfl_sync(full, base, 31);
+    return base + incl - count;
+}
+
 inline int blocks_for(long long n, int bs) { return (int)((n + bs - 1) / bs); }
 
 }  // namespace
@@ -72,15 +89,27 @@ __global__ void __launch_bounds__(128) k_backward_paths(DevScene s, int W, int H
     int lane = (int)(gid & (G - 1));
     bool active = pix < (long long)W * H;
     float3 acc = f3(0.f);
-    if (active) {
-        int x = (int)(pix % W), y = (int)(pix / W);
-        float3 dc = f3(d_image[3 * pix], d_image[3 * pix + 1], d_image[3 * pix + 2]);
-        auto push = [&](const PointRecord &pr) {
-            long long i = atomicAdd(ws.pt_count, 1);
-            if (i < ws.cap_points) pr.store(ws.pt + (size_t)i * DR_PT_WORDS);
+    int x = active ? (int)(pix % W) : 0, y = active ? (int)(pix / W) : 0;
+    float3 dc = active ? f3(d_image[3 * pix], d_image[3 * pix + 1], d_image[3 * pix + 2]) : f3(0.f);
+    // warp-uniform trip count so that the point push can be warp-aggregated
+    int iters = (spp + G - 1) >> lanes_log2;
+    for (int it = 0; it < iters; it++) {
+        int si = lane + (it << lanes_log2);
+        PointRecord pr;
+        bool has = false;
+        if (active && si < spp) {
+            auto push = [&](const PointRecord &p) {
+                pr = p;
+                has = true;
+            };
+            acc += backward_pixel_sample(s, x, y, W, H, spp, si, B, seed, dc, bg, push);
+        }
+        __syncwarp();
+        long long slot = warp_reserve(ws.pt_count, has ? 1 : 0);
+        if (has) {
+            if (slot < ws.cap_points) pr.store(ws.pt + (size_t)slot * DR_PT_WORDS);
             else set_status(ws.status, DR_STATUS_POINT_OVERFLOW);
-        };
-        for (int si = lane; si < spp; si += G) acc += backward_pixel_sample(s, x, y, W, H, spp, si, B, seed, dc, bg, push);
+        }
     }
     for (int off = G >> 1; off >= 1; off >>= 1) {
         acc.x += __shfl_down_sync(0xffffffffu, acc.x, off);
@@ -95,17 +124,23 @@ __global__ void __launch_bounds__(128) k_backward_paths(DevScene s, int W, int H
     block_grad_flush(bg);
 }
 
+#define DR_ITEM_BUF 24
 __global__ void __launch_bounds__(128) k_edge_traverse(DevScene s, uint64_t seed, BackwardWorkspace ws) {
     long long n = min((long long)*ws.pt_count, ws.cap_points);
-    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x) {
-        PointRecord pt;
-        pt.load(ws.pt + (size_t)p * DR_PT_WORDS);
-        auto emit = [&](int tree, int ei, int j, float w) {
-            long long i = atomicAdd(ws.item_count, 1);
+    long long stride = (long long)gridDim.x * blockDim.x;
+    // warp-uniform loop: every lane of a warp takes the same number of trips
+    for (long long base = (long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < n; base += stride) {
+        long long p = base + (threadIdx.x & 31);
+        bool active = p < n;
+        int buf_e[DR_ITEM_BUF];
+        float buf_w[DR_ITEM_BUF];
+        int buf_j[DR_ITEM_BUF];
+        int nb = 0;
+        auto write_item = [&](long long i, int te, int j, float w) {
             if (i < ws.cap_items) {
                 int4 it;
                 it.x = (int)p;
-                it.y = (tree << 30) | ei;
+                it.y = te;
                 it.z = j;
                 it.w = 0;
                 ws.items[i] = it;
@@ -114,7 +149,24 @@ __global__ void __launch_bounds__(128) k_edge_traverse(DevScene s, uint64_t seed
                 set_status(ws.status, DR_STATUS_ITEM_OVERFLOW);
             }
         };
-        if (!traverse_point(s, pt, seed, emit)) set_status(ws.status, DR_STATUS_STACK_OVERFLOW);
+        if (active) {
+            PointRecord pt;
+            pt.load(ws.pt + (size_t)p * DR_PT_WORDS);
+            auto emit = [&](int tree, int ei, int j, float w) {
+                if (nb < DR_ITEM_BUF) {
+                    buf_e[nb] = (tree << 30) | ei;
+                    buf_j[nb] = j;
+                    buf_w[nb] = w;
+                    nb++;
+                } else {  // rare: more edges than the lane buffer holds
+                    write_item(atomicAdd(ws.item_count, 1), (tree << 30) | ei, j, w);
+                }
+            };
+            if (!traverse_point(s, pt, seed, emit)) set_status(ws.status, DR_STATUS_STACK_OVERFLOW);
+        }
+        __syncwarp();
+        long long slot = warp_reserve(ws.item_count, nb);
+        for (int k = 0; k < nb; k++) write_item(slot + k, buf_e[k], buf_j[k], buf_w[k]);
     }
 }
 
@@ -170,18 +222,25 @@ __global__ void __launch_bounds__(128) k_primary_edges(DevScene s, int W, int H,
     block_grad_flush(bg);
 }
 
-cudaError_t dr_launch_backward(const DevScene &s, int W, int H, int spp, int B, uint64_t seed, const float *d_image,
-                               float *grad, float *img, long long primary_edge_samples, int dp_mode,
-                               const BackwardWorkspace &ws, const GradCacheCfg &cfg, int num_sms, cudaStream_t st,
-                               int *launches, StageTimer *timer) {
+namespace {
+int path_lanes_log2(int spp) {
+    int l = 0;
+    while ((1 << (l + 1)) <= spp && (1 << (l + 1)) <= 32 && spp % (1 << (l + 1)) == 0) l++;
+    return l;
+}
+// resident-grid size for the grid-stride stages: a few blocks per SM
+int stage_grid(int num_sms) { return num_sms * 12; }
+}  // namespace
+
+cudaError_t dr_launch_backward_front(const DevScene &s, int W, int H, int spp, int B, uint64_t seed,
+                                     const float *d_image, float *grad, float *img, long long primary_edge_samples,
+                                     int dp_mode, const BackwardWorkspace &ws, const GradCacheCfg &cfg, int num_sms,
+                                     cudaStream_t st, int *launches, StageTimer *timer) {
     const int bs = 128;
     size_t smem = sizeof(float) * (size_t)(cfg.head + cfg.tail_len);
-    int lanes_log2 = 0;
-    while ((1 << (lanes_log2 + 1)) <= spp && (1 << (lanes_log2 + 1)) <= 32 && spp % (1 << (lanes_log2 + 1)) == 0)
-        lanes_log2++;
+    int lanes_log2 = path_lanes_log2(spp);
     long long threads = ((long long)W * H) << lanes_log2;
-    // resident-grid size for the grid-stride stages: a few blocks per SM
-    int grid_ws = num_sms * 12;
+    int grid_ws = stage_grid(num_sms);
     timer->begin(st);
     if (dp_mode != DR_DP_SUM) {
         cudaError_t e = cudaMemsetAsync(ws.pt_last, 0, sizeof(unsigned long long) * (size_t)ws.cap_points, st);
@@ -190,21 +249,37 @@ cudaError_t dr_launch_backward(const DevScene &s, int W, int H, int spp, int B, 
     k_backward_paths<<<blocks_for(threads, bs), bs, smem, st>>>(s, W, H, spp, B, seed, lanes_log2, d_image, grad, img,
                                                                ws, cfg);
     timer->mark(st, "k_backward_paths");
-    k_edge_traverse<<<grid_ws, bs, 0, st>>>(s, seed, ws);
-    timer->mark(st, "k_edge_traverse");
-    k_edge_eval<<<grid_ws, bs, smem, st>>>(s, W, H, spp, B, seed, dp_mode, grad, ws, cfg);
-    timer->mark(st, "k_edge_eval");
-    *launches += 3;
-    if (dp_mode != DR_DP_SUM) {
-        k_dp_propagate<<<grid_ws, bs, smem, st>>>(s, W, H, spp, seed, grad, ws, cfg);
-        timer->mark(st, "k_dp_propagate");
-        *launches += 1;
-    }
+    *launches += 1;
     long long npe = primary_edge_samples > 0 ? primary_edge_samples : (long long)spp * W * H;
     if (s.num_prim_edges > 0 && npe > 0) {
         long long nb = std::min<long long>(blocks_for(npe, bs), (long long)grid_ws * 4);
         k_primary_edges<<<(int)nb, bs, smem, st>>>(s, W, H, spp, B, seed, d_image, npe, grad, cfg);
         timer->mark(st, "k_primary_edges");
+        *launches += 1;
+    }
+    return dr_launch_edge_traverse(s, seed, ws, num_sms, st, launches, timer);
+}
+
+cudaError_t dr_launch_edge_traverse(const DevScene &s, uint64_t seed, const BackwardWorkspace &ws, int num_sms,
+                                    cudaStream_t st, int *launches, StageTimer *timer) {
+    k_edge_traverse<<<stage_grid(num_sms), 128, 0, st>>>(s, seed, ws);
+    timer->mark(st, "k_edge_traverse");
+    *launches += 1;
+    return cudaGetLastError();
+}
+
+cudaError_t dr_launch_backward_back(const DevScene &s, int W, int H, int spp, int B, uint64_t seed, float *grad,
+                                    int dp_mode, const BackwardWorkspace &ws, const GradCacheCfg &cfg, int num_sms,
+                                    cudaStream_t st, int *launches, StageTimer *timer) {
+    const int bs = 128;
+    size_t smem = sizeof(float) * (size_t)(cfg.head + cfg.tail_len);
+    int grid_ws = stage_grid(num_sms);
+    k_edge_eval<<<grid_ws, bs, smem, st>>>(s, W, H, spp, B, seed, dp_mode, grad, ws, cfg);
+    timer->mark(st, "k_edge_eval");
+    *launches += 1;
+    if (dp_mode != DR_DP_SUM) {
+        k_dp_propagate<<<grid_ws, bs, smem, st>>>(s, W, H, spp, seed, grad, ws, cfg);
+        timer->mark(st, "k_dp_propagate");
         *launches += 1;
     }
     return cudaGetLastError();

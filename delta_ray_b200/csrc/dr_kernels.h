@@ -57,10 +57,20 @@ struct GradCacheCfg {
     int head, tail_begin, tail_len;
 };
 
-cudaError_t dr_launch_backward(const DevScene &s, int W, int H, int spp, int B, uint64_t seed, const float *d_image,
-                               float *grad, float *img, long long primary_edge_samples, int dp_mode,
-                               const BackwardWorkspace &ws, const GradCacheCfg &cfg, int num_sms, cudaStream_t st,
-                               int *launches, StageTimer *timer);
+// The backward pass runs in two halves with a host check between them: the
+// front half (path adjoints, primary edges, edge traversal) fills the point
+// and item queues; when the item queue overflowed, the host grows it to the
+// reported count and re-runs only the traversal; the back half evaluates the
+// queued edge samples.
+cudaError_t dr_launch_backward_front(const DevScene &s, int W, int H, int spp, int B, uint64_t seed,
+                                     const float *d_image, float *grad, float *img, long long primary_edge_samples,
+                                     int dp_mode, const BackwardWorkspace &ws, const GradCacheCfg &cfg, int num_sms,
+                                     cudaStream_t st, int *launches, StageTimer *timer);
+cudaError_t dr_launch_edge_traverse(const DevScene &s, uint64_t seed, const BackwardWorkspace &ws, int num_sms,
+                                    cudaStream_t st, int *launches, StageTimer *timer);
+cudaError_t dr_launch_backward_back(const DevScene &s, int W, int H, int spp, int B, uint64_t seed, float *grad,
+                                    int dp_mode, const BackwardWorkspace &ws, const GradCacheCfg &cfg, int num_sms,
+                                    cudaStream_t st, int *launches, StageTimer *timer);
 
 // Words of one packed secondary-point record in BackwardWorkspace::pt.
 #define DR_PT_FLOATS 24
