@@ -16,6 +16,7 @@
 #define HD inline
 #define DEV inline
 #define DR_RESTRICT
+#define DR_TABLE static const
 struct float2 { float x, y; };
 struct float3 { float x, y, z; };
 struct float4 { float x, y, z, w; };
@@ -32,6 +33,8 @@ using std::atan; using std::atan2; using std::floor; using std::log; using std::
 #define HD __host__ __device__ __forceinline__
 #define DEV __device__ __forceinline__
 #define DR_RESTRICT __restrict__
+// small lookup tables live in constant memory, not on each thread's stack
+#define DR_TABLE static __constant__ const
 template <typename T> DEV T dr_ldg(const T *p) { return __ldg(p); }
 // fire-and-forget reduction (RED.ADD.F32); the result is not needed
 DEV void dr_atomic_add(float *p, float v) { atomicAdd(p, v); }

@@ -48,17 +48,18 @@ DEV bool is_silhouette(const DevScene &s, float3 p, const DevEdge &e) {
 // ---------------------------------------------------------------------------
 struct ConeSpec { float3 o, d; float cos_angle; };
 
+// packed: 4 bits per corner, count in the top nibble
+DR_TABLE unsigned long long kConePoly[27] = {
+    0x6000000000154623ull, 0x6000000000023154ull, 0x6000000000023754ull, 0x6000000000046231ull,
+    0x4000000000000231ull, 0x6000000000023751ull, 0x6000000000046731ull, 0x6000000000026731ull,
+    0x6000000000026751ull, 0x6000000000015462ull, 0x4000000000000154ull, 0x6000000000013754ull,
+    0x4000000000000462ull, 0x0000000000000000ull, 0x4000000000001375ull, 0x6000000000046732ull,
+    0x4000000000002673ull, 0x6000000000132675ull, 0x6000000000015762ull, 0x6000000000015764ull,
+    0x6000000000013764ull, 0x6000000000045762ull, 0x4000000000004576ull, 0x6000000000137645ull,
+    0x6000000000045732ull, 0x6000000000264573ull, 0x6000000000132645ull};
+
 DEV int cone_poly(int lookup, int i) {
-    // packed: 4 bits per corner, count in the top nibble
-    const unsigned long long tab[27] = {
-        0x6000000000154623ull, 0x6000000000023154ull, 0x6000000000023754ull, 0x6000000000046231ull,
-        0x4000000000000231ull, 0x6000000000023751ull, 0x6000000000046731ull, 0x6000000000026731ull,
-        0x6000000000026751ull, 0x6000000000015462ull, 0x4000000000000154ull, 0x6000000000013754ull,
-        0x4000000000000462ull, 0x0000000000000000ull, 0x4000000000001375ull, 0x6000000000046732ull,
-        0x4000000000002673ull, 0x6000000000132675ull, 0x6000000000015762ull, 0x6000000000015764ull,
-        0x6000000000013764ull, 0x6000000000045762ull, 0x4000000000004576ull, 0x6000000000137645ull,
-        0x6000000000045732ull, 0x6000000000264573ull, 0x6000000000132645ull};
-    unsigned long long w = tab[lookup];
+    unsigned long long w = kConePoly[lookup];
     if (i < 0) return (int)(w >> 60);
     int n = (int)(w >> 60);
     return (int)((w >> (4 * (n - 1 - i))) & 0xF);
@@ -79,27 +80,32 @@ DEV bool box_cone(const float *lo, const float *hi, const ConeSpec &cone) {
     if (lookup == 13) return true;
     int np = cone_poly(lookup, -1);
     float c2 = cone.cos_angle * cone.cos_angle;
-    float3 X[8], PmV[8];
-    float DdPmV[8], sDd[8], sLen[8];
+    // only the corner of largest cos^2 (jmax) is needed after this loop: keep
+    // it in registers rather than per-corner arrays (local memory)
     int imax = -1, jmax = -1;
+    float3 mX = f3(0.f), mP = f3(0.f);
+    float mLen = 0.f, mDd = 0.f, msDd = 0.f;
     for (int i = 0; i < np; i++) {
         int j = cone_poly(lookup, i);
-        X[j] = f3((j & 1) ? E.x : -E.x, (j & 2) ? E.y : -E.y, (j & 4) ? E.z : -E.z);
-        DdPmV[j] = dot(cone.d, X[j]) + DdCmV;
-        if (DdPmV[j] > 0.f) {
-            PmV[j] = X[j] + CmV;
-            sDd[j] = DdPmV[j] * DdPmV[j];
-            sLen[j] = dot(PmV[j], PmV[j]);
-            if (sDd[j] - c2 * sLen[j] > 0.f) return true;
-            if (imax == -1 || sDd[j] * sLen[jmax] > sDd[jmax] * sLen[j]) {
+        float3 X = f3((j & 1) ? E.x : -E.x, (j & 2) ? E.y : -E.y, (j & 4) ? E.z : -E.z);
+        float DdPmV = dot(cone.d, X) + DdCmV;
+        if (DdPmV > 0.f) {
+            float3 PmV = X + CmV;
+            float sDd = DdPmV * DdPmV;
+            float sLen = dot(PmV, PmV);
+            if (sDd - c2 * sLen > 0.f) return true;
+            if (imax == -1 || sDd * mLen > msDd * sLen) {
                 imax = i;
                 jmax = j;
+                mX = X;
+                mP = PmV;
+                mLen = sLen;
+                mDd = DdPmV;
+                msDd = sDd;
             }
         }
     }
     if (imax == -1) return false;
-    float mLen = sLen[jmax], mDd = DdPmV[jmax];
-    float3 mX = X[jmax], mP = PmV[jmax];
     for (int side = 0; side < 2; side++) {
         int s, k0;
         float fder;
