@@ -1,7 +1,9 @@
 """Loads libdr_b200.so (the CUDA renderer) and declares its C ABI.
 
 There is no fallback: if the library is missing or no CUDA device is present,
-``lib()`` raises.  Build it with ``python -m delta_ray_b200.build``.
+``lib()`` raises.  Build it with ``python -m delta_ray_b200.build``.  The
+environment variable ``DELTA_RAY_B200_LIB`` names another build of the same
+library to load instead (e.g. one compiled with different nvcc flags).
 """
 import ctypes as C
 import os
@@ -9,7 +11,7 @@ import os
 from . import _abi
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libdr_b200.so")
+LIB_PATH = os.environ.get("DELTA_RAY_B200_LIB") or os.path.join(HERE, "libdr_b200.so")
 _lib = None
 
 

@@ -16,8 +16,9 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libdr_b200.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-# The backward kernels keep IEEE operation order (no FMA contraction) so that
-# edge-sampling decisions see the same bits as the reference's CPU arithmetic.
+# The path half of the backward pass keeps IEEE operation order (no FMA
+# contraction): the first path vertex it stores decides which edges a shading
+# point sees, so it must have the bits of the reference's CPU arithmetic.
 PER_FILE_FLAGS = {"dr_backward.cu": ["-fmad=false"]}
 NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr", "-Xcompiler", "-fPIC",
               "-Xcompiler", "-fvisibility=hidden", "-I", os.path.join(ROOT, "include")]

@@ -1,0 +1,70 @@
+// Per-block helpers shared by the backward kernels: a shared-memory cache of
+// the small, shared gradient entries, device status bits and warp-aggregated
+// queue slots.
+#pragma once
+
+#include "dr_kernels.h"
+
+namespace {
+
+struct BlockGrad {
+    float *sm;
+    float *g;
+    int head, tail_begin, tail_len;
+    __device__ __forceinline__ void add(int i, float v) {
+        if (v == 0.f) return;
+        if (i < head) {
+            atomicAdd(sm + i, v);
+        } else if ((unsigned)(i - tail_begin) < (unsigned)tail_len) {
+            atomicAdd(sm + head + (i - tail_begin), v);
+        } else {
+            atomicAdd(g + i, v);
+        }
+    }
+};
+
+__device__ __forceinline__ BlockGrad block_grad_begin(float *sm, float *g, const GradCacheCfg &c) {
+    BlockGrad b;
+    b.sm = sm;
+    b.g = g;
+    b.head = c.head;
+    b.tail_begin = c.tail_begin;
+    b.tail_len = c.tail_len;
+    for (int i = threadIdx.x; i < c.head + c.tail_len; i += blockDim.x) sm[i] = 0.f;
+    __syncthreads();
+    return b;
+}
+
+__device__ __forceinline__ void block_grad_flush(const BlockGrad &b) {
+    __syncthreads();
+    for (int i = threadIdx.x; i < b.head + b.tail_len; i += blockDim.x) {
+        float v = b.sm[i];
+        if (v != 0.f) atomicAdd(b.g + (i < b.head ? i : b.tail_begin + (i - b.head)), v);
+    }
+}
+
+__device__ __forceinline__ void set_status(int *status, int bit) { atomicOr(status, bit); }
+
+// Reserves `count` consecutive slots for each lane of the (fully converged)
+// warp with one atomic: returns the lane's first slot.
+__device__ __forceinline__ long long warp_reserve(int *counter, int count) {
+    const unsigned full = 0xffffffffu;
+    int lane = threadIdx.x & 31;
+    int incl = count;
+    for (int off = 1; off < 32; off <<= 1) {
+        int v = __shfl_up_sync(full, incl, off);
+        if (lane >= off) incl += v;
+    }
+    int total = __shfl_sync(full, incl, 31);
+    long long base = 0;
+    if (lane == 31 && total > 0) base = atomicAdd(counter, total);
+    base = __shfl_sync(full, base, 31);
+    return base + incl - count;
+}
+
+inline int blocks_for(long long n, int bs) { return (int)((n + bs - 1) / bs); }
+
+// resident-grid size for the grid-stride stages: a few blocks per SM
+inline int stage_grid(int num_sms) { return num_sms * 12; }
+
+}  // namespace

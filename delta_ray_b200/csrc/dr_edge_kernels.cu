@@ -1,0 +1,114 @@
+// Backward pass, edge half: edge-tree traversal of the shading points, the
+// secondary edge samples they drew, and the primary (screen-space) edges.
+// Compiled with FMA contraction; every input comes from the stored point
+// records, whose bits the path half fixes.
+#include "../../include/delta_ray_b200.h"
+#include "dr_backward.cuh"
+#include "dr_block_grad.cuh"
+
+#define DR_ITEM_BUF 24
+__global__ void __launch_bounds__(128, 4) k_edge_traverse(DevScene s, uint64_t seed, BackwardWorkspace ws) {
+    long long n = min((long long)*ws.pt_count, ws.cap_points);
+    long long stride = (long long)gridDim.x * blockDim.x;
+    // warp-uniform loop: every lane of a warp takes the same number of trips
+    for (long long base = (long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < n; base += stride) {
+        long long p = base + (threadIdx.x & 31);
+        bool active = p < n;
+        int buf_e[DR_ITEM_BUF];
+        float buf_w[DR_ITEM_BUF];
+        int buf_j[DR_ITEM_BUF];
+        int nb = 0;
+        auto write_item = [&](long long i, int te, int j, float w) {
+            if (i < ws.cap_items) {
+                int4 it;
+                it.x = (int)p;
+                it.y = te;
+                it.z = j;
+                it.w = 0;
+                ws.items[i] = it;
+                ws.item_w[i] = w;
+            } else {
+                set_status(ws.status, DR_STATUS_ITEM_OVERFLOW);
+            }
+        };
+        if (active) {
+            PointRecord pt;
+            pt.load(ws.pt + (size_t)p * DR_PT_WORDS);
+            auto emit = [&](int tree, int ei, int j, float w) {
+                if (nb < DR_ITEM_BUF) {
+                    buf_e[nb] = (tree << 30) | ei;
+                    buf_j[nb] = j;
+                    buf_w[nb] = w;
+                    nb++;
+                } else {  // rare: more edges than the lane buffer holds
+                    write_item(atomicAdd(ws.item_count, 1), (tree << 30) | ei, j, w);
+                }
+            };
+            if (!traverse_point(s, pt, seed, emit)) set_status(ws.status, DR_STATUS_STACK_OVERFLOW);
+        }
+        __syncwarp();
+        long long slot = warp_reserve(ws.item_count, nb);
+        for (int k = 0; k < nb; k++) write_item(slot + k, buf_e[k], buf_j[k], buf_w[k]);
+    }
+}
+
+__global__ void __launch_bounds__(128, 3) k_edge_eval(DevScene s, int W, int H, int spp, int B, uint64_t seed, int dp_mode,
+                                                   float *grad, BackwardWorkspace ws, GradCacheCfg cfg) {
+    extern __shared__ float sm[];
+    BlockGrad bg = block_grad_begin(sm, grad, cfg);
+    long long n = min((long long)*ws.item_count, ws.cap_items);
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
+        int4 it = ws.items[i];
+        PointRecord pt;
+        pt.load(ws.pt + (size_t)it.x * DR_PT_WORDS);
+        int tree = it.y >> 30, ei = it.y & ((1 << 30) - 1);
+        float3 dp = eval_item(s, pt, tree, ei, it.z, ws.item_w[i], spp, B, seed, bg);
+        if (is_zero(dp)) continue;
+        if (dp_mode == DR_DP_SUM) {
+            propagate_dp(s, pt, W, H, spp, seed, dp, bg);
+        } else {
+            ws.item_dp[3 * i] = dp.x;
+            ws.item_dp[3 * i + 1] = dp.y;
+            ws.item_dp[3 * i + 2] = dp.z;
+            unsigned long long key = ((unsigned long long)(it.z + 1) << 32) | (unsigned long long)i;
+            atomicMax(ws.pt_last + it.x, key);
+        }
+    }
+    block_grad_flush(bg);
+}
+
+__global__ void __launch_bounds__(128, 3) k_primary_edges(DevScene s, int W, int H, int spp, int B, uint64_t seed,
+                                                       const float *d_image, long long n, float *grad,
+                                                       GradCacheCfg cfg) {
+    extern __shared__ float sm[];
+    BlockGrad bg = block_grad_begin(sm, grad, cfg);
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        primary_edge_item(s, i, W, H, spp, B, seed, d_image, bg);
+    block_grad_flush(bg);
+}
+
+cudaError_t dr_launch_edge_traverse(const DevScene &s, uint64_t seed, const BackwardWorkspace &ws, int num_sms,
+                                    cudaStream_t st, int *launches, StageTimer *timer) {
+    k_edge_traverse<<<stage_grid(num_sms), 128, 0, st>>>(s, seed, ws);
+    timer->mark(st, "k_edge_traverse");
+    *launches += 1;
+    return cudaGetLastError();
+}
+
+cudaError_t dr_launch_edge_eval(const DevScene &s, int W, int H, int spp, int B, uint64_t seed, int dp_mode,
+                                float *grad, const BackwardWorkspace &ws, const GradCacheCfg &cfg, int num_sms,
+                                cudaStream_t st) {
+    size_t smem = sizeof(float) * (size_t)(cfg.head + cfg.tail_len);
+    k_edge_eval<<<stage_grid(num_sms), 128, smem, st>>>(s, W, H, spp, B, seed, dp_mode, grad, ws, cfg);
+    return cudaGetLastError();
+}
+
+cudaError_t dr_launch_primary_edges(const DevScene &s, int W, int H, int spp, int B, uint64_t seed,
+                                    const float *d_image, long long n, float *grad, const GradCacheCfg &cfg,
+                                    int num_sms, cudaStream_t st) {
+    const int bs = 128;
+    size_t smem = sizeof(float) * (size_t)(cfg.head + cfg.tail_len);
+    long long nb = std::min<long long>(blocks_for(n, bs), (long long)stage_grid(num_sms) * 4);
+    k_primary_edges<<<(int)nb, bs, smem, st>>>(s, W, H, spp, B, seed, d_image, n, grad, cfg);
+    return cudaGetLastError();
+}

@@ -456,18 +456,33 @@ DEV EdgeResult shading_edge_sample(const DevScene &s, const EdgeSample &es, cons
     float delta = 1e-3f * length(sample_p);
     float3 sdir = normalize(sample_p);
     float3 rdir = normalize(sdir + delta * split_n), ldir = normalize(sdir - delta * split_n);
-    Hit hr = trace_closest(s, sp.p, rdir, 1e-3f), hl = trace_closest(s, sp.p, ldir, 1e-3f);
+    // The two sides of the edge ("right" along +split_n, then "left") run
+    // through one copy of the trace and shade code: loops, not unrolled.
+    Hit hr, hl;
     SurfacePoint pr, pl;
     int rsh = -1, rlt = -1, lsh = -1, llt = -1;
-    if (hr.tri >= 0) {
-        pr = intersect_tri(load_tri(s, hr.tri), sp.p, rdir);
-        rsh = s.tri[hr.tri].w;
-        rlt = s.tri_local[hr.tri];
-    }
-    if (hl.tri >= 0) {
-        pl = intersect_tri(load_tri(s, hl.tri), sp.p, ldir);
-        lsh = s.tri[hl.tri].w;
-        llt = s.tri_local[hl.tri];
+#pragma unroll 1
+    for (int k = 0; k < 2; k++) {
+        float3 dir = k == 0 ? rdir : ldir;
+        Hit hh = trace_closest(s, sp.p, dir, 1e-3f);
+        SurfacePoint pp;
+        int sh = -1, lt = -1;
+        if (hh.tri >= 0) {
+            pp = intersect_tri(load_tri(s, hh.tri), sp.p, dir);
+            sh = s.tri[hh.tri].w;
+            lt = s.tri_local[hh.tri];
+        }
+        if (k == 0) {
+            hr = hh;
+            pr = pp;
+            rsh = sh;
+            rlt = lt;
+        } else {
+            hl = hh;
+            pl = pp;
+            lsh = sh;
+            llt = lt;
+        }
     }
     bool rc = rsh == edge.shape && (rlt == edge.f0 || rlt == edge.f1);
     bool lc = lsh == edge.shape && (llt == edge.f0 || llt == edge.f1);
@@ -476,19 +491,19 @@ DEV EdgeResult shading_edge_sample(const DevScene &s, const EdgeSample &es, cons
     if (sum(eb) < 1e-6f) return none;
     float3 shr = f3(0.f), shl = f3(0.f);
     if (!direct_only) {
-        shr = shade(s, -sdir, hr.tri, pr, ls, rng, nbounces, false);
-        shl = shade(s, -sdir, hl.tri, pl, ls, rng, nbounces, false);
-        if (hr.tri >= 0) {
-            float3 dir = pr.p - sp.p;
-            float d2 = length_sq(dir);
-            if (d2 > 0.f) shr = shr / fmaxf(d2, 1e-2f) * fabsf(dot(normalize(dir), pr.ng));
-            else shr = f3(0.f);
-        }
-        if (hl.tri >= 0) {
-            float3 dir = pl.p - sp.p;
-            float d2 = length_sq(dir);
-            if (d2 > 0.f) shl = shl / fmaxf(d2, 1e-2f) * fabsf(dot(normalize(dir), pl.ng));
-            else shl = f3(0.f);
+#pragma unroll 1
+        for (int k = 0; k < 2; k++) {
+            int tri = k == 0 ? hr.tri : hl.tri;
+            SurfacePoint pp = k == 0 ? pr : pl;
+            float3 sh = shade(s, -sdir, tri, pp, ls, rng, nbounces, false);
+            if (tri >= 0) {
+                float3 dir = pp.p - sp.p;
+                float d2 = length_sq(dir);
+                if (d2 > 0.f) sh = sh / fmaxf(d2, 1e-2f) * fabsf(dot(normalize(dir), pp.ng));
+                else sh = f3(0.f);
+            }
+            if (k == 0) shr = sh;
+            else shl = sh;
         }
     }
     float3 er = eval_light(s, wi, stri, sp, hr.tri, pr) + eb * shr;
@@ -673,22 +688,41 @@ DEV void primary_edge_sample(const DevScene &s, const EdgeSample &es, const DevE
     float3 d_color = f3(dr_ldg(dc), dr_ldg(dc + 1), dr_ldg(dc + 2));
     float delta = 1e-4f * length(elocal);
     float3 split_n = normalize(cross(d0, d1));
-    float3 rdir = normalize(ept3 + delta * split_n);
-    float2 rpt = project_local(cam, rdir);
-    Ray rray = sample_primary(cam, rpt.x, rpt.y);
-    Hit hr = trace_closest(s, rray.o, rray.d, 1e-3f);
-    float3 ldir = normalize(ept3 - delta * split_n);
-    float2 lpt = project_local(cam, ldir);
-    Ray lray = sample_primary(cam, lpt.x, lpt.y);
-    Hit hl = trace_closest(s, lray.o, lray.d, 1e-3f);
+    // right side (+split_n) then left, through one copy of the code
+    float2 rpt, lpt;
+    Ray rray, lray;
+    Hit hr, hl;
+#pragma unroll 1
+    for (int k = 0; k < 2; k++) {
+        float3 dir = normalize(k == 0 ? ept3 + delta * split_n : ept3 - delta * split_n);
+        float2 pt = project_local(cam, dir);
+        Ray ray = sample_primary(cam, pt.x, pt.y);
+        Hit hh = trace_closest(s, ray.o, ray.d, 1e-3f);
+        if (k == 0) {
+            rpt = pt;
+            rray = ray;
+            hr = hh;
+        } else {
+            lpt = pt;
+            lray = ray;
+            hl = hh;
+        }
+    }
     bool rc = hr.tri >= 0 && s.tri[hr.tri].w == edge.shape &&
               (s.tri_local[hr.tri] == edge.f0 || s.tri_local[hr.tri] == edge.f1);
     bool lc = hl.tri >= 0 && s.tri[hl.tri].w == edge.shape &&
               (s.tri_local[hl.tri] == edge.f0 || s.tri_local[hl.tri] == edge.f1);
     if (!rc && !lc) return;
     float3 rcol = f3(0.f), lcol = f3(0.f);
-    if (hr.tri >= 0) rcol = shade(s, -rray.d, hr.tri, intersect_tri(load_tri(s, hr.tri), rray.o, rray.d), ls, rng, B, true);
-    if (hl.tri >= 0) lcol = shade(s, -lray.d, hl.tri, intersect_tri(load_tri(s, hl.tri), lray.o, lray.d), ls, rng, B, true);
+#pragma unroll 1
+    for (int k = 0; k < 2; k++) {
+        int tri = k == 0 ? hr.tri : hl.tri;
+        Ray ray = k == 0 ? rray : lray;
+        float3 col = f3(0.f);
+        if (tri >= 0) col = shade(s, -ray.d, tri, intersect_tri(load_tri(s, tri), ray.o, ray.d), ls, rng, B, true);
+        if (k == 0) rcol = col;
+        else lcol = col;
+    }
     float3 diff = (rcol - lcol) * weight;
     float3 xdiff = diff, ydiff = diff;
     if (lpt.x > rpt.x) xdiff = -xdiff;

@@ -68,6 +68,13 @@ cudaError_t dr_launch_backward_front(const DevScene &s, int W, int H, int spp, i
                                      cudaStream_t st, int *launches, StageTimer *timer);
 cudaError_t dr_launch_edge_traverse(const DevScene &s, uint64_t seed, const BackwardWorkspace &ws, int num_sms,
                                     cudaStream_t st, int *launches, StageTimer *timer);
+// Single-kernel launchers of the edge half (dr_edge_kernels.cu).
+cudaError_t dr_launch_edge_eval(const DevScene &s, int W, int H, int spp, int B, uint64_t seed, int dp_mode,
+                                float *grad, const BackwardWorkspace &ws, const GradCacheCfg &cfg, int num_sms,
+                                cudaStream_t st);
+cudaError_t dr_launch_primary_edges(const DevScene &s, int W, int H, int spp, int B, uint64_t seed,
+                                    const float *d_image, long long n, float *grad, const GradCacheCfg &cfg,
+                                    int num_sms, cudaStream_t st);
 cudaError_t dr_launch_backward_back(const DevScene &s, int W, int H, int spp, int B, uint64_t seed, float *grad,
                                     int dp_mode, const BackwardWorkspace &ws, const GradCacheCfg &cfg, int num_sms,
                                     cudaStream_t st, int *launches, StageTimer *timer);
