@@ -15,6 +15,7 @@
 #include <cstring>
 #define HD inline
 #define DEV inline
+#define DEV_NOINLINE inline
 #define DR_RESTRICT
 #define DR_TABLE static const
 struct float2 { float x, y; };
@@ -32,6 +33,10 @@ using std::atan; using std::atan2; using std::floor; using std::log; using std::
 #include <string.h>
 #define HD __host__ __device__ __forceinline__
 #define DEV __device__ __forceinline__
+// Large routines with many call sites (BVH traversal, shading) are real calls:
+// inlining every copy makes kernels of several hundred KB of code, which
+// starves the instruction cache.
+#define DEV_NOINLINE static __device__ __noinline__
 #define DR_RESTRICT __restrict__
 // small lookup tables live in constant memory, not on each thread's stack
 #define DR_TABLE static __constant__ const

@@ -542,54 +542,68 @@ DEV EdgeResult shading_edge_sample(const DevScene &s, const EdgeSample &es, cons
 // ---------------------------------------------------------------------------
 // Primary edges (camera.h:86-313, delta_ray.cpp:377-557)
 // ---------------------------------------------------------------------------
+// Fisheye branches out of line (rarely taken, large trigonometry).
+DEV_NOINLINE float3 unproject_fisheye(float sx, float sy) {
+    float x = 2.f * (sx - 0.5f), y = 2.f * (sy - 0.5f);
+    float r = sqrtf(x * x + y * y), phi = atan2f(y, x), theta = r * DR_PI / 2.f;
+    return f3(-cosf(phi) * sinf(theta), -sinf(phi) * sinf(theta), cosf(theta));
+}
+struct F3Pair { float3 a, b; };
+DEV_NOINLINE F3Pair d_unproject_fisheye(float sx, float sy) {
+    float x = 2.f * (sx - 0.5f), y = 2.f * (sy - 0.5f);
+    float r = sqrtf(x * x + y * y), phi = atan2f(y, x), theta = r * DR_PI / 2.f;
+    float sp = sinf(phi), cp = cosf(phi), st = sinf(theta), ct = cosf(theta);
+    float dxdphi = sp * st, dxdth = -cp * ct, dydphi = -cp * st, dydth = -sp * ct, dzdth = -st;
+    float dphidx = -y / (r * r), dphidy = x / (r * r);
+    float dthdx = (DR_PI / 2.f) * x / r, dthdy = (DR_PI / 2.f) * y / r;
+    F3Pair d;
+    d.a = 2.f * f3(dxdphi * dphidx + dxdth * dthdx, dydphi * dphidx + dydth * dthdx, dzdth * dthdx);
+    d.b = 2.f * f3(dxdphi * dphidy + dxdth * dthdy, dydphi * dphidy + dydth * dthdy, dzdth * dthdy);
+    return d;
+}
+DEV_NOINLINE float2 project_local_fisheye(float3 l) {
+    float2 r;
+    float3 d = normalize(l);
+    float phi = atan2f(d.y, d.x), theta = acosf(d.z), rr = theta * 2.f / DR_PI;
+    r.x = 0.5f * (-rr * cosf(phi) + 1.f);
+    r.y = 0.5f * (-rr * sinf(phi) + 1.f);
+    return r;
+}
+DEV_NOINLINE float3 d_project_local_fisheye(float3 l, float dx, float dy) {
+    float3 d = normalize(l);
+    float phi = atan2f(d.y, d.x), theta = acosf(d.z), r = theta * 2.f / DR_PI;
+    float dr = -0.5f * (cosf(phi) * dx + sinf(phi) * dy);
+    float dphi = 0.5f * r * sinf(phi) * dx - 0.5f * r * cosf(phi) * dy;
+    float dtheta = dr * (2.f / DR_PI);
+    float dcos = -dtheta / sqrtf(1.f - d.z * d.z);
+    float t = d.x * d.x + d.y * d.y;
+    return d_normalize(l, f3(-dphi * d.y / t, dphi * d.x / t, dcos));
+}
+
 DEV float3 unproject(const DevCamera &c, float sx, float sy) {
-    if (c.fisheye) {
-        float x = 2.f * (sx - 0.5f), y = 2.f * (sy - 0.5f);
-        float r = sqrtf(x * x + y * y), phi = atan2f(y, x), theta = r * DR_PI / 2.f;
-        return f3(-cosf(phi) * sinf(theta), -sinf(phi) * sinf(theta), cosf(theta));
-    }
+    if (c.fisheye) return unproject_fisheye(sx, sy);
     float ndcx = (sx - 0.5f) * -2.f, ndcy = (sy - 0.5f) * -2.f / c.aspect;
     return f3(c.fov * ndcx, c.fov * ndcy, 1.f);
 }
 DEV void d_unproject(const DevCamera &c, float sx, float sy, float3 &dx, float3 &dy) {
     if (c.fisheye) {
-        float x = 2.f * (sx - 0.5f), y = 2.f * (sy - 0.5f);
-        float r = sqrtf(x * x + y * y), phi = atan2f(y, x), theta = r * DR_PI / 2.f;
-        float sp = sinf(phi), cp = cosf(phi), st = sinf(theta), ct = cosf(theta);
-        float dxdphi = sp * st, dxdth = -cp * ct, dydphi = -cp * st, dydth = -sp * ct, dzdth = -st;
-        float dphidx = -y / (r * r), dphidy = x / (r * r);
-        float dthdx = (DR_PI / 2.f) * x / r, dthdy = (DR_PI / 2.f) * y / r;
-        dx = 2.f * f3(dxdphi * dphidx + dxdth * dthdx, dydphi * dphidx + dydth * dthdx, dzdth * dthdx);
-        dy = 2.f * f3(dxdphi * dphidy + dxdth * dthdy, dydphi * dphidy + dydth * dthdy, dzdth * dthdy);
+        F3Pair d = d_unproject_fisheye(sx, sy);
+        dx = d.a;
+        dy = d.b;
         return;
     }
     dx = f3(-2.f * c.fov, 0.f, 0.f);
     dy = f3(0.f, -2.f * c.fov / c.aspect, 0.f);
 }
 DEV float2 project_local(const DevCamera &c, float3 l) {
+    if (c.fisheye) return project_local_fisheye(l);
     float2 r;
-    if (c.fisheye) {
-        float3 d = normalize(l);
-        float phi = atan2f(d.y, d.x), theta = acosf(d.z), rr = theta * 2.f / DR_PI;
-        r.x = 0.5f * (-rr * cosf(phi) + 1.f);
-        r.y = 0.5f * (-rr * sinf(phi) + 1.f);
-        return r;
-    }
     r.x = (-l.x / (l.z * c.fov) + 1.f) * 0.5f;
     r.y = (-l.y / (l.z * c.fov * c.aspect) + 1.f) * 0.5f;
     return r;
 }
 DEV float3 d_project_local(const DevCamera &c, float3 l, float dx, float dy) {
-    if (c.fisheye) {
-        float3 d = normalize(l);
-        float phi = atan2f(d.y, d.x), theta = acosf(d.z), r = theta * 2.f / DR_PI;
-        float dr = -0.5f * (cosf(phi) * dx + sinf(phi) * dy);
-        float dphi = 0.5f * r * sinf(phi) * dx - 0.5f * r * cosf(phi) * dy;
-        float dtheta = dr * (2.f / DR_PI);
-        float dcos = -dtheta / sqrtf(1.f - d.z * d.z);
-        float t = d.x * d.x + d.y * d.y;
-        return d_normalize(l, f3(-dphi * d.y / t, dphi * d.x / t, dcos));
-    }
+    if (c.fisheye) return d_project_local_fisheye(l, dx, dy);
     float zf = l.z * c.fov;
     float zfy = zf * c.aspect;
     return f3(dx * (-1.f / zf), dy * (-1.f / zfy),

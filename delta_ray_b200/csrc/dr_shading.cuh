@@ -30,20 +30,24 @@ struct Ray { float3 o, d; };
 // division by a differentiable value is a multiply by its reciprocal
 // (autodiff.h:161-186); the backward pass needs those exact bits for the
 // shading point that edge sampling starts from.
+// Fisheye branches of the camera routines are out of line: they are rarely
+// taken and their trigonometry is large.  r.d = 0 outside the image circle.
+DEV_NOINLINE float3 fisheye_dir(float sx, float sy) {
+    float x = 2.f * (sx - 0.5f), y = 2.f * (sy - 0.5f);
+    if (x * x + y * y > 1.f) return f3(0.f);
+    float rr = sqrtf(x * x + y * y);
+    float phi = atan2f(y, x);
+    float theta = rr * DR_PI / 2.f;
+    float3 dir = f3(-cosf(phi) * sinf(theta), -sinf(phi) * sinf(theta), cosf(theta));
+    return normalize(dir);
+}
+
 DEV Ray sample_primary(const DevCamera &c, float sx, float sy, bool ad = false) {
     Ray r;
     r.o = xfm_point(c.c2w, f3(0.f));
     if (c.fisheye) {
-        float x = 2.f * (sx - 0.5f), y = 2.f * (sy - 0.5f);
-        if (x * x + y * y > 1.f) {
-            r.d = f3(0.f);
-            return r;
-        }
-        float rr = sqrtf(x * x + y * y);
-        float phi = atan2f(y, x);
-        float theta = rr * DR_PI / 2.f;
-        float3 dir = f3(-cosf(phi) * sinf(theta), -sinf(phi) * sinf(theta), cosf(theta));
-        r.d = xfm_vector(c.c2w, normalize(dir));
+        float3 d = fisheye_dir(sx, sy);
+        r.d = is_zero(d) ? d : xfm_vector(c.c2w, d);
         return r;
     }
     float ndcx = (sx - 0.5f) * -2.f;

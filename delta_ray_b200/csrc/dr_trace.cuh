@@ -85,22 +85,21 @@ struct Hit {
     float t;
 };
 
-// Closest hit on (tnear, inf).
-DEV Hit trace_closest(const DevScene &s, float3 o, float3 d, float tnear) {
+// Closest hit on (tnear, inf) in the LBVH (nodes, tris) rooted at root.
+DEV_NOINLINE Hit trace_closest_bvh(const float4 *DR_RESTRICT nodes, const float4 *DR_RESTRICT tris, int root, float3 o,
+                                   float3 d, float tnear) {
     Hit h;
     h.tri = -1;
     h.t = DR_INF;
-    if (s.num_tris == 0) return h;
     float3 inv = f3(safe_inv(d.x), safe_inv(d.y), safe_inv(d.z));
     int stack[DR_STACK];
     int sp = 0;
-    int node = s.bvh_root;
+    int node = root;
     while (true) {
         DR_COUNT_VISIT();
         if (node < 0) {
             int leaf = ~node;
-            float4 a = dr_ldg(s.bvh_tris + 3 * leaf), b = dr_ldg(s.bvh_tris + 3 * leaf + 1),
-                   c = dr_ldg(s.bvh_tris + 3 * leaf + 2);
+            float4 a = dr_ldg(tris + 3 * leaf), b = dr_ldg(tris + 3 * leaf + 1), c = dr_ldg(tris + 3 * leaf + 2);
             float t;
             if (hit_triangle(a, b, c, o, d, t) && t > tnear) {
                 int id = dr_f2i(a.w);
@@ -113,7 +112,7 @@ DEV Hit trace_closest(const DevScene &s, float3 o, float3 d, float tnear) {
             node = stack[--sp];
             continue;
         }
-        const float4 *n = s.bvh_nodes + 4 * node;
+        const float4 *n = nodes + 4 * node;
         float4 n0 = dr_ldg(n), n1 = dr_ldg(n + 1), n2 = dr_ldg(n + 2), n3 = dr_ldg(n + 3);
         float e0 = box_entry(n0.x, n0.y, n0.z, n0.w, n1.x, n1.y, o, inv, h.t);
         float e1 = box_entry(n1.z, n1.w, n2.x, n2.y, n2.z, n2.w, o, inv, h.t);
@@ -135,25 +134,34 @@ DEV Hit trace_closest(const DevScene &s, float3 o, float3 d, float tnear) {
     return h;
 }
 
+DEV Hit trace_closest(const DevScene &s, float3 o, float3 d, float tnear) {
+    if (s.num_tris == 0) {
+        Hit h;
+        h.tri = -1;
+        h.t = DR_INF;
+        return h;
+    }
+    return trace_closest_bvh(s.bvh_nodes, s.bvh_tris, s.bvh_root, o, d, tnear);
+}
+
 // Any hit on (tnear, tfar).
-DEV bool trace_any(const DevScene &s, float3 o, float3 d, float tnear, float tfar) {
-    if (s.num_tris == 0) return false;
+DEV_NOINLINE bool trace_any_bvh(const float4 *DR_RESTRICT nodes, const float4 *DR_RESTRICT tris, int root, float3 o,
+                                float3 d, float tnear, float tfar) {
     float3 inv = f3(safe_inv(d.x), safe_inv(d.y), safe_inv(d.z));
     int stack[DR_STACK];
     int sp = 0;
-    int node = s.bvh_root;
+    int node = root;
     while (true) {
         if (node < 0) {
             int leaf = ~node;
-            float4 a = dr_ldg(s.bvh_tris + 3 * leaf), b = dr_ldg(s.bvh_tris + 3 * leaf + 1),
-                   c = dr_ldg(s.bvh_tris + 3 * leaf + 2);
+            float4 a = dr_ldg(tris + 3 * leaf), b = dr_ldg(tris + 3 * leaf + 1), c = dr_ldg(tris + 3 * leaf + 2);
             float t;
             if (hit_triangle(a, b, c, o, d, t) && t > tnear && t < tfar) return true;
             if (sp == 0) break;
             node = stack[--sp];
             continue;
         }
-        const float4 *n = s.bvh_nodes + 4 * node;
+        const float4 *n = nodes + 4 * node;
         float4 n0 = dr_ldg(n), n1 = dr_ldg(n + 1), n2 = dr_ldg(n + 2), n3 = dr_ldg(n + 3);
         float e0 = box_entry(n0.x, n0.y, n0.z, n0.w, n1.x, n1.y, o, inv, tfar);
         float e1 = box_entry(n1.z, n1.w, n2.x, n2.y, n2.z, n2.w, o, inv, tfar);
@@ -172,6 +180,11 @@ DEV bool trace_any(const DevScene &s, float3 o, float3 d, float tnear, float tfa
         }
     }
     return false;
+}
+
+DEV bool trace_any(const DevScene &s, float3 o, float3 d, float tnear, float tfar) {
+    if (s.num_tris == 0) return false;
+    return trace_any_bvh(s.bvh_nodes, s.bvh_tris, s.bvh_root, o, d, tnear, tfar);
 }
 
 // occluded(scene, ray, max_t) of the reference (scene.cpp:147-166)
