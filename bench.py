@@ -255,9 +255,15 @@ def run_b200(args):
     d_img = torch.ones((H, W, 3), dtype=torch.float32, device=dev)
     flush = torch.empty(64 * 1024 * 1024, dtype=torch.float32, device=dev)  # 256 MB > 126 MB L2
 
+    from delta_ray_b200.distributed import average_gradients, rank_seed
+
     def step(seed):
-        scene.forward(W, H, spp, B, seed)
-        scene.backward(W, H, spp, B, seed, d_img)
+        # each rank renders its own sample streams; one all-reduce combines the gradients
+        s = rank_seed(seed, rank)
+        scene.forward(W, H, spp, B, s)
+        grad, _ = scene.backward(W, H, spp, B, s, d_img)
+        if dist:
+            average_gradients(grad)
 
     for i in range(args.warmup):
         step(1000 + i)
@@ -346,7 +352,7 @@ def run_b200(args):
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scene)",
             "config": {"workload": "soft_shadow 512x512 16spp max_bounces=1 fwd+bwd",
                        "resolution": [W, H], "spp": spp, "max_bounces": B, "triangles": wl.num_triangles,
-                       "parallelism": f"replicas x{world}", "l2": "flushed between steps (256 MB write)"},
+                       "parallelism": f"dp{world} (per-rank sample streams, gradient all-reduce)", "l2": "flushed between steps (256 MB write)"},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
             "gpu_launches": launches_per_step * args.steps, "roofline": roofline, "clocks": clk}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
