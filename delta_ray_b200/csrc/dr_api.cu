@@ -524,3 +524,113 @@ size_t dr_last_error(char *buf, size_t len) {
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------------------
+// dr_render_backward_noalloc: the backward pass with its work queues in a
+// fixed device array that is part of the library's module image, so that a
+// call allocates no device memory.
+// ---------------------------------------------------------------------------
+namespace {
+constexpr size_t kNoAllocScratchBytes = size_t(32) << 20;  // per device
+constexpr long long kNoAllocMaxSamples = 65536;            // width * height * spp
+constexpr int kNoAllocMaxDevices = 64;
+}  // namespace
+
+static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
+
+namespace {
+std::mutex &noalloc_mutex() {
+    static std::mutex *m = new std::mutex();
+    return *m;
+}
+void *g_noalloc_base[kNoAllocMaxDevices] = {};
+
+// Device address of this device's copy of the array, looked up on the first
+// call on each device (the caller has made `device` current).
+unsigned char *noalloc_scratch(int device) {
+    if (device < 0 || device >= kNoAllocMaxDevices) throw DrError(DR_ERR_NOT_SUPPORTED, "device index out of range");
+    std::lock_guard<std::mutex> lk(noalloc_mutex());
+    if (!g_noalloc_base[device]) {
+        void *p = nullptr;
+        check_cuda(cudaGetSymbolAddress(&p, g_noalloc_scratch), "cudaGetSymbolAddress");
+        if (!p) throw DrError(DR_ERR_CUDA, "cudaGetSymbolAddress returned NULL");
+        g_noalloc_base[device] = p;
+    }
+    return (unsigned char *)g_noalloc_base[device];
+}
+}  // namespace
+
+extern "C" {
+
+dr_status dr_render_backward_noalloc(dr_scene *scene, const dr_render_desc *rd, const float *d_image_dev,
+                                     float *grad_dev, float *image_dev, void *stream) {
+    return guard([&]() {
+        check_render_desc(scene, rd);
+        if (!d_image_dev || !grad_dev) throw DrError(DR_ERR_INVALID_ARGUMENT, "d_image and grad must be non-NULL");
+        if (rd->dp_mode != DR_DP_REFERENCE_LAST && rd->dp_mode != DR_DP_SUM)
+            throw DrError(DR_ERR_INVALID_ARGUMENT, "unknown dp_mode");
+        long long npix = (long long)rd->width * rd->height * rd->spp;
+        if (npix > kNoAllocMaxSamples)
+            throw DrError(DR_ERR_INVALID_ARGUMENT,
+                          "width * height * spp = " + std::to_string(npix) + " exceeds the " +
+                              std::to_string(kNoAllocMaxSamples) +
+                              " pixel samples of the no-alloc backward's fixed scratch; use dr_render_backward");
+        check_cuda(cudaSetDevice(scene->device), "cudaSetDevice");
+        cudaStream_t st = (cudaStream_t)stream;
+        scene->last_launches = 0;
+        unsigned char *base = noalloc_scratch(scene->device);
+        // layout: counters | point records | point keys | items | item weights | item dp
+        auto up = [](size_t b) { return (b + 255) & ~size_t(255); };
+        long long cap_points = npix;
+        size_t off = 256;
+        BackwardWorkspace ws;
+        ws.pt_count = (int *)base;
+        ws.item_count = (int *)base + 1;
+        ws.status = (int *)base + 2;
+        ws.pt = (float *)(base + off);
+        off += up(sizeof(float) * DR_PT_FLOATS * (size_t)cap_points);
+        ws.pt_last = (unsigned long long *)(base + off);
+        off += up(sizeof(unsigned long long) * (size_t)cap_points);
+        long long cap_items = (long long)((kNoAllocScratchBytes - off - 3 * 256) / (sizeof(int4) + 4 * sizeof(float)));
+        ws.items = (int4 *)(base + off);
+        off += up(sizeof(int4) * (size_t)cap_items);
+        ws.item_w = (float *)(base + off);
+        off += up(sizeof(float) * (size_t)cap_items);
+        ws.item_dp = (float *)(base + off);
+        off += up(sizeof(float) * 3 * (size_t)cap_items);
+        if (off > kNoAllocScratchBytes) throw DrError(DR_ERR_INVALID_ARGUMENT, "scratch layout does not fit");
+        ws.cap_points = cap_points;
+        ws.cap_items = cap_items;
+        // what must start at zero: the three queue counters and the gradient
+        // (the point keys of the "last edge" rule are cleared by the launcher)
+        check_cuda(cudaMemsetAsync(base, 0, sizeof(int) * 4, st), "memset");
+        check_cuda(cudaMemsetAsync(grad_dev, 0, sizeof(float) * scene->h.grad_total, st), "memset");
+        StageTimer quiet;  // no profiling events on this path
+        GradCacheCfg cfg = grad_cache_cfg(scene->h);
+        int counts[4];
+        auto read_counts = [&]() {
+            check_cuda(cudaMemcpyAsync(counts, base, sizeof(counts), cudaMemcpyDeviceToHost, st), "status read");
+            check_cuda(cudaStreamSynchronize(st), "backward");
+        };
+        check_cuda(dr_launch_backward_front(scene->ds, rd->width, rd->height, rd->spp, rd->max_bounces, rd->seed,
+                                            d_image_dev, grad_dev, image_dev, rd->primary_edge_samples, rd->dp_mode,
+                                            ws, cfg, scene->num_sms, st, &scene->last_launches, &quiet),
+                   "backward launch");
+        read_counts();
+        if (counts[2] & DR_STATUS_ITEM_OVERFLOW)
+            throw DrError(DR_ERR_DEVICE_STATUS, "the sampled edges (" + std::to_string(counts[1]) +
+                                                    ") exceed the no-alloc scratch (" + std::to_string(cap_items) +
+                                                    " items); use dr_render_backward");
+        if (counts[2]) throw DrError(DR_ERR_DEVICE_STATUS, "device reported status " + std::to_string(counts[2]));
+        check_cuda(dr_launch_backward_back(scene->ds, rd->width, rd->height, rd->spp, rd->max_bounces, rd->seed,
+                                           grad_dev, rd->dp_mode, ws, cfg, scene->num_sms, st, &scene->last_launches,
+                                           &quiet),
+                   "backward launch");
+        read_counts();
+        scene->last_points = counts[0];
+        scene->last_items = counts[1];
+        if (counts[2]) throw DrError(DR_ERR_DEVICE_STATUS, "device reported status " + std::to_string(counts[2]));
+    });
+}
+
+}  // extern "C"

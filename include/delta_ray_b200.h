@@ -178,6 +178,21 @@ DR_API dr_status dr_render_forward(dr_scene *scene, const dr_render_desc *rd, fl
 DR_API dr_status dr_render_backward(dr_scene *scene, const dr_render_desc *rd, const float *d_image_dev,
                              float *grad_dev, float *image_dev, void *stream);
 
+/* Backward render that allocates no device memory.  No counterpart in the
+ * reference (whose backward allocates per call, delta_ray.cpp:1468-1550): it
+ * serves callers that must not allocate during a render, e.g. a process whose
+ * device memory is all reserved by its own pool.  Same computation and
+ * arguments as dr_render_backward, but its work queues live in a fixed 32 MiB
+ * array per device that is part of the library's module image.  Limits:
+ * width * height * spp <= 65536 (larger calls fail with
+ * DR_ERR_INVALID_ARGUMENT); a call whose sampled edges outgrow the array
+ * fails with DR_ERR_DEVICE_STATUS and leaves a partial gradient.  All calls on
+ * one device share the array, so overlapping calls (from several threads or
+ * streams) race: serialize them.  The first call on each device looks up the
+ * array's address; make it before any stream capture. */
+DR_API dr_status dr_render_backward_noalloc(dr_scene *scene, const dr_render_desc *rd, const float *d_image_dev,
+                                            float *grad_dev, float *image_dev, void *stream);
+
 /* Closest hits of n rays [n][6] (origin, direction; device memory) on
  * (1e-3, inf): global triangle id (-1 on a miss; ids run over shapes in
  * order, then triangles) and distance.  Replaces the reference's

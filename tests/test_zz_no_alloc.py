@@ -1,0 +1,79 @@
+"""dr_render_backward_noalloc: the backward pass with its work queues in the
+library's fixed per-device scratch array, called through the C ABI and
+compared with dr_render_backward on the same scene, seed and adjoint.
+
+The file name sorts last so that the test also runs after every other GPU
+test in the same process (the scratch set-up happens on first use)."""
+import ctypes as C
+
+import numpy as np
+import pytest
+import torch
+
+from conftest import rel_err
+
+TOL = 1e-4  # float atomics reorder the gradient sums; the parity bound of the backward tests
+DR_ERR_INVALID_ARGUMENT = 1
+
+
+def _bind(L):
+    from delta_ray_b200 import _abi
+    L.dr_render_backward_noalloc.argtypes = [C.c_void_p, C.POINTER(_abi.dr_render_desc), C.c_void_p, C.c_void_p,
+                                             C.c_void_p, C.c_void_p]
+    L.dr_render_backward_noalloc.restype = C.c_int
+    return L
+
+
+def _scene(res, spp, B, seed=2):
+    from delta_ray_b200 import workloads
+    from delta_ray_b200.render_pytorch import Scene, unpack_args
+    wl = workloads.soft_shadow(seed, res, spp, B)
+    cam, mats, shps, lts, _, _, _, _ = unpack_args(wl.serialize())
+    return Scene(cam, mats, shps, lts, 0, None)
+
+
+def _noalloc(L, sc, W, H, spp, B, seed, d_image):
+    from delta_ray_b200 import _abi
+    grad = torch.full((sc.grad_total,), float("nan"), dtype=torch.float32, device="cuda")
+    img = torch.empty((H, W, 3), dtype=torch.float32, device="cuda")
+    rd = _abi.render_desc(W, H, spp, B, seed)
+    st = L.dr_render_backward_noalloc(sc.handle, C.byref(rd), C.c_void_p(d_image.data_ptr()),
+                                      C.c_void_p(grad.data_ptr()), C.c_void_p(img.data_ptr()), None)
+    torch.cuda.synchronize()
+    return st, grad, img
+
+
+@pytest.mark.gpu
+@pytest.mark.parametrize("res,spp,B", [((32, 32), 4, 1), ((40, 24), 8, 3)])
+def test_noalloc_backward_matches_backward_twice(res, spp, B):
+    from delta_ray_b200 import _lib
+    L = _bind(_lib.lib())
+    W, H = res
+    sc = _scene(res, spp, B)
+    seed = 11
+    gen = torch.Generator().manual_seed(5)
+    d_image = torch.rand((H, W, 3), generator=gen).cuda()
+    ref_grad, ref_img = sc.backward(W, H, spp, B, seed, d_image, want_image=True)
+    ref_grad = ref_grad.cpu().numpy()
+    assert np.abs(ref_grad).max() > 0
+    for _ in range(2):  # two calls in a row reuse the same scratch
+        st, grad, img = _noalloc(L, sc, W, H, spp, B, seed, d_image)
+        assert st == 0, _lib.last_error()
+        g = grad.cpu().numpy()
+        assert np.isfinite(g).all()
+        assert rel_err(g, ref_grad) < TOL
+        assert np.allclose(img.cpu().numpy(), ref_img.cpu().numpy(), rtol=1e-6, atol=1e-7)
+    sc.close()
+
+
+@pytest.mark.gpu
+def test_noalloc_backward_rejects_oversize_calls():
+    from delta_ray_b200 import _lib
+    L = _bind(_lib.lib())
+    sc = _scene((32, 32), 4, 1)
+    W, H, spp = 128, 128, 8  # 131072 pixel samples > 65536
+    d_image = torch.ones((H, W, 3), dtype=torch.float32, device="cuda")
+    st, _, _ = _noalloc(L, sc, W, H, spp, 1, 3, d_image)
+    assert st == DR_ERR_INVALID_ARGUMENT
+    assert "65536" in _lib.last_error()
+    sc.close()
