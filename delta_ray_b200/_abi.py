@@ -54,7 +54,7 @@ class dr_render_desc(C.Structure):
     _fields_ = [("width", C.c_int), ("height", C.c_int), ("spp", C.c_int),
                 ("max_bounces", C.c_int), ("seed", C.c_uint64),
                 ("primary_edge_samples", C.c_int64), ("dp_mode", C.c_int),
-                ("reserved", C.c_int * 8)]
+                ("flags", C.c_int), ("reserved", C.c_int * 7)]
 
 
 class dr_grad_layout(C.Structure):
@@ -65,15 +65,17 @@ class dr_grad_layout(C.Structure):
 
 DR_DP_REFERENCE_LAST = 0
 DR_DP_SUM = 1
+DR_FLAG_FULL_PIXEL_JITTER = 1
 
 
 def render_desc(width, height, spp, max_bounces, seed, primary_edge_samples=0,
-                dp_mode=DR_DP_REFERENCE_LAST):
+                dp_mode=DR_DP_REFERENCE_LAST, flags=0):
     rd = dr_render_desc()
     rd.width, rd.height, rd.spp, rd.max_bounces = int(width), int(height), int(spp), int(max_bounces)
     rd.seed = int(seed) & 0xFFFFFFFFFFFFFFFF
     rd.primary_edge_samples = int(primary_edge_samples)
     rd.dp_mode = int(dp_mode)
+    rd.flags = int(flags)
     return rd
 
 

@@ -270,6 +270,13 @@ void collect_timings(dr_scene *sc, cudaStream_t st) {
     }
 }
 
+// The scene's device view with this call's per-render settings.
+DevScene call_scene(const dr_scene *sc, const dr_render_desc *rd) {
+    DevScene ds = sc->ds;
+    ds.full_pixel_jitter = (rd->flags & DR_FLAG_FULL_PIXEL_JITTER) != 0;
+    return ds;
+}
+
 void check_render_desc(const dr_scene *sc, const dr_render_desc *rd) {
     if (!sc) throw DrError(DR_ERR_INVALID_ARGUMENT, "scene is NULL");
     if (!rd) throw DrError(DR_ERR_INVALID_ARGUMENT, "render descriptor is NULL");
@@ -277,8 +284,9 @@ void check_render_desc(const dr_scene *sc, const dr_render_desc *rd) {
         throw DrError(DR_ERR_INVALID_ARGUMENT, "width, height and spp must be positive, max_bounces >= 0");
     if ((long long)rd->width * rd->height > (1ll << 28))
         throw DrError(DR_ERR_INVALID_ARGUMENT, "image too large");
-    for (int i = 0; i < 8; i++)
+    for (int i = 0; i < 7; i++)
         if (rd->reserved[i] != 0) throw DrError(DR_ERR_INVALID_ARGUMENT, "reserved fields must be zero");
+    if (rd->flags & ~(int)DR_FLAG_FULL_PIXEL_JITTER) throw DrError(DR_ERR_INVALID_ARGUMENT, "unknown render flags");
     if (rd->max_bounces > 64) throw DrError(DR_ERR_NOT_SUPPORTED, "max_bounces above 64");
     if (sc->ds.num_lights == 0) throw DrError(DR_ERR_INVALID_ARGUMENT, "scene has no lights");
 }
@@ -368,7 +376,7 @@ dr_status dr_render_forward(dr_scene *scene, const dr_render_desc *rd, float *im
         if (!image_dev) throw DrError(DR_ERR_INVALID_ARGUMENT, "image is NULL");
         check_cuda(cudaSetDevice(scene->device), "cudaSetDevice");
         scene->last_launches = 0;
-        check_cuda(dr_launch_forward(scene->ds, rd->width, rd->height, rd->spp, rd->max_bounces, rd->seed, image_dev,
+        check_cuda(dr_launch_forward(call_scene(scene, rd), rd->width, rd->height, rd->spp, rd->max_bounces, rd->seed, image_dev,
                                      (cudaStream_t)stream, &scene->last_launches, &scene->timer),
                    "forward launch");
         collect_timings(scene, (cudaStream_t)stream);
@@ -382,6 +390,10 @@ dr_status dr_render_backward(dr_scene *scene, const dr_render_desc *rd, const fl
         if (!d_image_dev || !grad_dev) throw DrError(DR_ERR_INVALID_ARGUMENT, "d_image and grad must be non-NULL");
         if (rd->dp_mode != DR_DP_REFERENCE_LAST && rd->dp_mode != DR_DP_SUM)
             throw DrError(DR_ERR_INVALID_ARGUMENT, "unknown dp_mode");
+        if (scene->h.specular_bounces && rd->max_bounces >= 1)
+            throw DrError(DR_ERR_NOT_SUPPORTED,
+                          "backward through specular bounces (roughness <= 0.01 with a specular lobe) is not "
+                          "implemented; the forward render supports them");
         check_cuda(cudaSetDevice(scene->device), "cudaSetDevice");
         cudaStream_t st = (cudaStream_t)stream;
         scene->last_launches = 0;
@@ -427,7 +439,7 @@ dr_status dr_render_backward(dr_scene *scene, const dr_render_desc *rd, const fl
         };
         check_cuda(cudaMemsetAsync(q.counts.p, 0, sizeof(int) * 4, st), "memset");
         check_cuda(cudaMemsetAsync(grad_dev, 0, sizeof(float) * scene->h.grad_total, st), "memset");
-        check_cuda(dr_launch_backward_front(scene->ds, rd->width, rd->height, rd->spp, rd->max_bounces, rd->seed,
+        check_cuda(dr_launch_backward_front(call_scene(scene, rd), rd->width, rd->height, rd->spp, rd->max_bounces, rd->seed,
                                             d_image_dev, grad_dev, image_dev, rd->primary_edge_samples, rd->dp_mode,
                                             ws, cfg, scene->num_sms, st, &scene->last_launches, &scene->timer),
                    "backward launch");
@@ -439,14 +451,14 @@ dr_status dr_render_backward(dr_scene *scene, const dr_render_desc *rd, const fl
             cap_items = std::max(cap_items * 2, (long long)counts[1] + (counts[1] >> 3) + 1);
             bind_items();
             check_cuda(cudaMemsetAsync(q.counts.as<int>() + 1, 0, sizeof(int) * 2, st), "memset");
-            check_cuda(dr_launch_edge_traverse(scene->ds, rd->seed, ws, scene->num_sms, st, &scene->last_launches,
+            check_cuda(dr_launch_edge_traverse(call_scene(scene, rd), rd->seed, ws, scene->num_sms, st, &scene->last_launches,
                                                &scene->timer),
                        "edge traversal launch");
             read_counts();
         }
         if (counts[2]) throw DrError(DR_ERR_DEVICE_STATUS, "device reported status " + std::to_string(counts[2]));
         scene->timer.mark(st, "host_queue_check");
-        check_cuda(dr_launch_backward_back(scene->ds, rd->width, rd->height, rd->spp, rd->max_bounces, rd->seed,
+        check_cuda(dr_launch_backward_back(call_scene(scene, rd), rd->width, rd->height, rd->spp, rd->max_bounces, rd->seed,
                                            grad_dev, rd->dp_mode, ws, cfg, scene->num_sms, st, &scene->last_launches,
                                            &scene->timer),
                    "backward launch");
@@ -569,6 +581,10 @@ dr_status dr_render_backward_noalloc(dr_scene *scene, const dr_render_desc *rd, 
         if (!d_image_dev || !grad_dev) throw DrError(DR_ERR_INVALID_ARGUMENT, "d_image and grad must be non-NULL");
         if (rd->dp_mode != DR_DP_REFERENCE_LAST && rd->dp_mode != DR_DP_SUM)
             throw DrError(DR_ERR_INVALID_ARGUMENT, "unknown dp_mode");
+        if (scene->h.specular_bounces && rd->max_bounces >= 1)
+            throw DrError(DR_ERR_NOT_SUPPORTED,
+                          "backward through specular bounces (roughness <= 0.01 with a specular lobe) is not "
+                          "implemented; the forward render supports them");
         long long npix = (long long)rd->width * rd->height * rd->spp;
         if (npix > kNoAllocMaxSamples)
             throw DrError(DR_ERR_INVALID_ARGUMENT,
@@ -612,7 +628,7 @@ dr_status dr_render_backward_noalloc(dr_scene *scene, const dr_render_desc *rd, 
             check_cuda(cudaMemcpyAsync(counts, base, sizeof(counts), cudaMemcpyDeviceToHost, st), "status read");
             check_cuda(cudaStreamSynchronize(st), "backward");
         };
-        check_cuda(dr_launch_backward_front(scene->ds, rd->width, rd->height, rd->spp, rd->max_bounces, rd->seed,
+        check_cuda(dr_launch_backward_front(call_scene(scene, rd), rd->width, rd->height, rd->spp, rd->max_bounces, rd->seed,
                                             d_image_dev, grad_dev, image_dev, rd->primary_edge_samples, rd->dp_mode,
                                             ws, cfg, scene->num_sms, st, &scene->last_launches, &quiet),
                    "backward launch");
@@ -622,7 +638,7 @@ dr_status dr_render_backward_noalloc(dr_scene *scene, const dr_render_desc *rd, 
                                                     ") exceed the no-alloc scratch (" + std::to_string(cap_items) +
                                                     " items); use dr_render_backward");
         if (counts[2]) throw DrError(DR_ERR_DEVICE_STATUS, "device reported status " + std::to_string(counts[2]));
-        check_cuda(dr_launch_backward_back(scene->ds, rd->width, rd->height, rd->spp, rd->max_bounces, rd->seed,
+        check_cuda(dr_launch_backward_back(call_scene(scene, rd), rd->width, rd->height, rd->spp, rd->max_bounces, rd->seed,
                                            grad_dev, rd->dp_mode, ws, cfg, scene->num_sms, st, &scene->last_launches,
                                            &quiet),
                    "backward launch");

@@ -96,11 +96,12 @@ DEV float3 sampled_direction(const DevScene &s, const BSDFSample &bs, float3 wi,
 }
 
 // The pixel sample's screen position (delta_ray.cpp:1236-1237,657-658).
-DEV void pixel_sample_position(int x, int y, int W, int H, int spp, uint64_t sid, uint64_t seed, float &sx, float &sy,
-                               Rng &r) {
+DEV void pixel_sample_position(int x, int y, int W, int H, int spp, uint64_t sid, uint64_t seed, bool full_jitter,
+                               float &sx, float &sy, Rng &r) {
     r.init(seed, kStreamPixel, sid, 0);
-    float sub_x = r.next() / spp;
-    float sub_y = r.next() / spp;
+    float ux = r.next(), uy = r.next();
+    float sub_x = full_jitter ? ux : ux / spp;
+    float sub_y = full_jitter ? uy : uy / spp;
     sx = float((x + sub_x) / W);
     sy = float((y + sub_y) / H);
 }
@@ -114,7 +115,7 @@ DEV float3 backward_pixel_sample(const DevScene &s, int x, int y, int W, int H, 
     uint64_t sid = ((uint64_t)y * W + x) * spp + si;
     Rng r;
     float sx, sy;
-    pixel_sample_position(x, y, W, H, spp, sid, seed, sx, sy, r);
+    pixel_sample_position(x, y, W, H, spp, sid, seed, s.full_pixel_jitter != 0, sx, sy, r);
     Ray ray = sample_primary(s.cam, sx, sy, true);
     if (abs_sum(ray.d) == 0.f) return f3(0.f);
     Hit h0 = trace_closest(s, ray.o, ray.d, 1e-3f);
@@ -366,7 +367,7 @@ DEV void propagate_dp(const DevScene &s, const PointRecord &pt, int W, int H, in
     int x = (int)(pix % (uint64_t)W), y = (int)(pix / (uint64_t)W);
     Rng r;
     float sx, sy;
-    pixel_sample_position(x, y, W, H, spp, pt.sid, seed, sx, sy, r);
+    pixel_sample_position(x, y, W, H, spp, pt.sid, seed, s.full_pixel_jitter != 0, sx, sy, r);
     Ray ray = sample_primary(s.cam, sx, sy, true);
     TriData td = load_tri(s, pt.tri);
     IsectFwd fw;

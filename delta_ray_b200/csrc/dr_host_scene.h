@@ -230,6 +230,10 @@ struct HostScene {
     HCam cam;
     std::vector<HShape> shapes;
     std::vector<DevMaterial> mats;
+    // some material can take a "specular" BSDF sample (roughness <= 0.01 with a
+    // nonzero specular lobe, material.h:410): the backward pass does not
+    // differentiate through such bounces
+    bool specular_bounces = false;
     std::vector<float> texels;
     std::vector<DevLight> lights;
     std::vector<float> light_tri_cdf, light_tri_func;
@@ -492,6 +496,23 @@ template <class Fetch> void load_desc(HostScene &h, const dr_scene_desc *d, Fetc
         uvs(m.specular_uv_scale, dm.uv_ks, "specular_uv_scale");
         uvs(m.roughness_uv_scale, dm.uv_r, "roughness_uv_scale");
         dm.two_sided = m.two_sided != 0;
+        {
+            // can this material's BSDF sample be "specular" (material.h:410)?
+            auto range = [&](int tex, int w, int hh, int ch, const float *cval, float &lo, float &hi) {
+                lo = 1e30f;
+                hi = -1e30f;
+                size_t n = tex < 0 ? (size_t)ch : (size_t)w * hh * ch;
+                const float *v = tex < 0 ? cval : h.texels.data() + tex;
+                for (size_t k = 0; k < n; k++) {
+                    lo = std::min(lo, v[k]);
+                    hi = std::max(hi, v[k]);
+                }
+            };
+            float rlo, rhi, slo, shi;
+            range(dm.tex_r, dm.r_w, dm.r_h, 1, &dm.rough, rlo, rhi);
+            range(dm.tex_ks, dm.ks_w, dm.ks_h, 3, dm.ks, slo, shi);
+            if (rlo <= 0.01f && (shi > 0.f || slo < 0.f)) h.specular_bounces = true;
+        }
         h.mats.push_back(dm);
         h.layout_mat.push_back((size_t)dm.grad_kd);
         h.layout_mat.push_back((size_t)dm.grad_ks);
@@ -661,6 +682,7 @@ inline void fill_devscene(DevScene &ds, const HostScene &h, const FlatScene &f, 
     ds.nrm_edges = p.nrm_edges;
     ds.num_nrm_nodes = (int)h.nrm_nodes.size();
     ds.ltc = p.ltc;
+    ds.full_pixel_jitter = 0;  // set per render call
     ds.grad_total = (int)h.grad_total;
 }
 

@@ -94,6 +94,9 @@ struct DevScene {
     int num_nrm_nodes;
     const float *ltc;  // 128*128 row-major 3x3
     int grad_total;
+    // per render call: sub-pixel offsets over the whole pixel (u) instead of
+    // the reference's [0, 1/spp) (u / spp)
+    int full_pixel_jitter;
 };
 
 // --- accessors -------------------------------------------------------------

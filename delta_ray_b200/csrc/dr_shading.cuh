@@ -389,8 +389,9 @@ DEV float3 shade(const DevScene &s, float3 wi, int ptri, const SurfacePoint &psp
 DEV float3 pixel_sample(const DevScene &s, int x, int y, int W, int H, int spp, int si, int B, uint64_t seed) {
     Rng r;
     r.init(seed, kStreamPixel, ((uint64_t)y * W + x) * spp + si, 0);
-    float sub_x = r.next() / spp;
-    float sub_y = r.next() / spp;
+    float ux = r.next(), uy = r.next();
+    float sub_x = s.full_pixel_jitter ? ux : ux / spp;
+    float sub_y = s.full_pixel_jitter ? uy : uy / spp;
     Ray ray = sample_primary(s.cam, float((x + sub_x) / W), float((y + sub_y) / H));
     if (abs_sum(ray.d) == 0.f) return f3(0.f);
     Hit h = trace_closest(s, ray.o, ray.d, 1e-3f);

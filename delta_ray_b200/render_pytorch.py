@@ -32,12 +32,16 @@ class RenderOptions:
     ltc_table: optional [128*128*9] float32 Blinn-Phong LTC table.
     output_device: device of the returned image (default: the render device).
     device: CUDA device index to render on (default: current device).
+    full_pixel_jitter: spread each pixel's samples over the whole pixel (a box
+        filter, the image whose derivative the edge terms estimate) instead of
+        the reference's [0, 1/spp) sub-pixel offsets (delta_ray.cpp:1236-1237).
     """
 
     def __init__(self, primary_edge_samples=0, dp_mode=_abi.DR_DP_REFERENCE_LAST, ltc_table=None,
-                 output_device=None, device=None):
+                 output_device=None, device=None, full_pixel_jitter=False):
         self.primary_edge_samples = int(primary_edge_samples)
         self.dp_mode = int(dp_mode)
+        self.flags = _abi.DR_FLAG_FULL_PIXEL_JITTER if full_pixel_jitter else 0
         self.ltc_table = ltc_table
         self.output_device = output_device
         self.device = device
@@ -70,7 +74,8 @@ class Scene:
     def forward(self, width, height, spp, max_bounces, seed, opts=None):
         opts = opts or RenderOptions()
         img = torch.empty((height, width, 3), dtype=torch.float32, device=self.device)
-        rd = _abi.render_desc(width, height, spp, max_bounces, seed, opts.primary_edge_samples, opts.dp_mode)
+        rd = _abi.render_desc(width, height, spp, max_bounces, seed, opts.primary_edge_samples, opts.dp_mode,
+                              opts.flags)
         with torch.cuda.device(self.device_index):
             _lib.check(_lib.lib().dr_render_forward(self.handle, C.byref(rd), C.c_void_p(img.data_ptr()),
                                                     self._stream()))
@@ -83,7 +88,8 @@ class Scene:
             raise ValueError(f"d_image must be [{height}, {width}, 3]")
         grad = torch.empty(self.grad_total, dtype=torch.float32, device=self.device)
         img = torch.empty((height, width, 3), dtype=torch.float32, device=self.device) if want_image else None
-        rd = _abi.render_desc(width, height, spp, max_bounces, seed, opts.primary_edge_samples, opts.dp_mode)
+        rd = _abi.render_desc(width, height, spp, max_bounces, seed, opts.primary_edge_samples, opts.dp_mode,
+                              opts.flags)
         with torch.cuda.device(self.device_index):
             _lib.check(_lib.lib().dr_render_backward(
                 self.handle, C.byref(rd), C.c_void_p(d_image.data_ptr()), C.c_void_p(grad.data_ptr()),

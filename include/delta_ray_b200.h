@@ -117,6 +117,14 @@ typedef struct {
  * survives; DR_DP_SUM adds every edge (the unbiased estimator). */
 typedef enum { DR_DP_REFERENCE_LAST = 0, DR_DP_SUM = 1 } dr_dp_mode;
 
+/* dr_render_desc.flags.  DR_FLAG_FULL_PIXEL_JITTER spreads each pixel's
+ * samples over the whole pixel (a box filter).  Without it the sub-pixel
+ * offset is u / spp in each axis, as in the reference (delta_ray.cpp:1236-1237),
+ * so that all samples of a pixel fall in its [0, 1/spp)^2 corner: the image is
+ * then nearly point-sampled, while the primary-edge gradient is the derivative
+ * of the box-filtered image. */
+typedef enum { DR_FLAG_FULL_PIXEL_JITTER = 1 } dr_render_flags;
+
 typedef struct {
     int width;
     int height;
@@ -128,7 +136,8 @@ typedef struct {
      * (delta_ray.cpp:1474-1475 with one thread). */
     int64_t primary_edge_samples;
     int dp_mode;      /* dr_dp_mode */
-    int reserved[8];  /* must be zero */
+    int flags;        /* dr_render_flags */
+    int reserved[7];  /* must be zero */
 } dr_render_desc;
 
 /* Gradient layout: one flat float32 buffer, in this order

@@ -2295,8 +2295,13 @@ int dro_render_parts(const dr_scene_desc *desc, const dr_render_desc *rd, int rn
                         ph.reset(new PhiloxSampler(rd->seed, kPixel, sid, 0));
                         main = ph.get();
                     }
-                    float sx = main->next() / spp;
-                    float sy = main->next() / spp;
+                    // sub-pixel offset: u / spp as the reference (delta_ray.cpp:1236-1237),
+                    // or u with DR_FLAG_FULL_PIXEL_JITTER
+                    float ux = main->next();
+                    float uy = main->next();
+                    bool full = (rd->flags & DR_FLAG_FULL_PIXEL_JITTER) != 0;
+                    float sx = full ? ux : ux / spp;
+                    float sy = full ? uy : uy / spp;
                     StreamPlan plan{rng_mode, rd->seed, sid, main};
                     csum = csum + render_pixel_sample(sc, L, W, H, x, y, sx, sy, spp, B, dcol, derivs, plan, accs[tid],
                                                       rd->dp_mode);

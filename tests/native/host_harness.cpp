@@ -126,6 +126,7 @@ int hh_render(const dr_scene_desc *desc, const dr_render_desc *rd, const float *
               int parts, long long *stats) {
     HostSceneBundle b;
     make_scene(desc, b);
+    b.ds.full_pixel_jitter = (rd->flags & DR_FLAG_FULL_PIXEL_JITTER) != 0;
     const DevScene &s = b.ds;
     int W = rd->width, H = rd->height, spp = rd->spp, B = rd->max_bounces;
     uint64_t seed = rd->seed;

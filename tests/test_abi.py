@@ -43,5 +43,5 @@ def test_null_arguments_are_rejected_without_a_device():
 
 def test_render_desc_layout_matches_header():
     from delta_ray_b200 import _abi
-    # int width,height,spp,max_bounces; uint64 seed; int64 pes; int dp_mode; int reserved[8]
+    # int width,height,spp,max_bounces; uint64 seed; int64 pes; int dp_mode, flags; int reserved[7]
     assert C.sizeof(_abi.dr_render_desc) == 4 * 4 + 8 + 8 + 4 + 32 + 4  # padded to 8 bytes

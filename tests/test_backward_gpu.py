@@ -82,3 +82,24 @@ def test_backward_is_deterministic_in_expectation():
     assert not np.array_equal(g1, g2)
     big = np.abs(g1) > 0.1 * np.abs(g1).max()
     assert np.median(np.abs(g1[big] - g2[big]) / np.abs(g1[big])) < 0.5
+
+
+@pytest.mark.gpu
+def test_backward_refuses_specular_bounces():
+    """Materials that can take a "specular" BSDF sample (roughness <= 0.01 with a
+    specular lobe) are rendered forward but refused by the backward pass, which
+    does not differentiate through such bounces."""
+    import torch
+    from delta_ray_b200 import _lib, workloads
+    from delta_ray_b200.render_pytorch import Scene, unpack_args
+    wl = workloads.soft_shadow(2, (16, 16), 2, 1)
+    wl.materials[1].specular_reflectance = torch.tensor([0.5, 0.5, 0.5])
+    wl.materials[1].roughness = torch.tensor([0.005])
+    cam, mats, shps, lts, _, _, _, _ = unpack_args(wl.serialize())
+    sc = Scene(cam, mats, shps, lts, 0, None)
+    img = sc.forward(16, 16, 2, 1, 3)
+    assert torch.isfinite(img).all()
+    with pytest.raises(_lib.DrError) as e:
+        sc.backward(16, 16, 2, 1, 3, torch.ones((16, 16, 3), device="cuda"))
+    assert e.value.status == 5  # DR_ERR_NOT_SUPPORTED
+    sc.close()
