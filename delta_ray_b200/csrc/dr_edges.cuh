@@ -65,7 +65,7 @@ DEV int cone_poly(int lookup, int i) {
     return (int)((w >> (4 * (n - 1 - i))) & 0xF);
 }
 
-DEV bool box_cone(const float *lo, const float *hi, const ConeSpec &cone) {
+DEV_NOINLINE bool box_cone(const float *lo, const float *hi, const ConeSpec &cone) {
     if (cone.cos_angle <= 0.f) return true;
     float3 C = f3(0.5f * (lo[0] + hi[0]), 0.5f * (lo[1] + hi[1]), 0.5f * (lo[2] + hi[2]));
     float3 E = f3(0.5f * (hi[0] - lo[0]), 0.5f * (hi[1] - lo[1]), 0.5f * (hi[2] - lo[2]));
@@ -153,7 +153,7 @@ DEV float3 node_corner(const DevEdgeNode &n, int i) {
     return f3((i & 1) ? n.hi[0] : n.lo[0], (i & 2) ? n.hi[1] : n.lo[1], (i & 4) ? n.hi[2] : n.lo[2]);
 }
 
-DEV float bsdf_bound(const DevEdgeNode &node, float3 wi, const SurfacePoint &sp, float dl, float sl, float rough) {
+DEV_NOINLINE float bsdf_bound(const DevEdgeNode &node, float3 wi, const SurfacePoint &sp, float dl, float sl, float rough) {
     float cos_max = 0.f;
     for (int i = 0; i < 8; i++)
         if (dot(sp.f.n, node_corner(node, i) - sp.p) > 0.f) {
@@ -197,7 +197,7 @@ DEV float bsdf_bound(const DevEdgeNode &node, float3 wi, const SurfacePoint &sp,
     return cos_max * (dl / DR_PI + sl * maxp);
 }
 
-DEV bool contains_silhouette(const DevEdgeNode &node, float3 p) {
+DEV_NOINLINE bool contains_silhouette(const DevEdgeNode &node, float3 p) {
     float3 c = f3(0.5f * (node.lo[0] + node.hi[0]), 0.5f * (node.lo[1] + node.hi[1]), 0.5f * (node.lo[2] + node.hi[2]));
     // bounding sphere as aabb.h:266-270: center (lo + hi) / 2, radius |hi - center|
     float3 cs = f3((node.lo[0] + node.hi[0]) / 2.f, (node.lo[1] + node.hi[1]) / 2.f, (node.lo[2] + node.hi[2]) / 2.f);
@@ -506,8 +506,14 @@ DEV EdgeResult shading_edge_sample(const DevScene &s, const EdgeSample &es, cons
             else shl = sh;
         }
     }
-    float3 er = eval_light(s, wi, stri, sp, hr.tri, pr) + eb * shr;
-    float3 el = eval_light(s, wi, stri, sp, hl.tri, pl) + eb * shl;
+    float3 er, el;
+#pragma unroll 1
+    for (int k = 0; k < 2; k++) {
+        float3 e = k == 0 ? eval_light(s, wi, stri, sp, hr.tri, pr) + eb * shr
+                          : eval_light(s, wi, stri, sp, hl.tri, pl) + eb * shl;
+        if (k == 0) er = e;
+        else el = e;
+    }
     if (hr.tri >= 0) {
         float3 dir = pr.p - sp.p;
         if (length(dir) * fabsf(dot(normalize(dir), pr.ng)) < 1e-3f) return none;
@@ -534,8 +540,12 @@ DEV EdgeResult shading_edge_sample(const DevScene &s, const EdgeSample &es, cons
         res.dv0 += dv0 * we;
         res.dv1 += dv1 * we;
     };
-    if (hr.tri >= 0 && abs_sum(er) > 0.f) accum(pr, er);
-    if (hl.tri >= 0 && abs_sum(el) > 0.f) accum(pl, -el);
+#pragma unroll 1
+    for (int k = 0; k < 2; k++) {
+        int tri = k == 0 ? hr.tri : hl.tri;
+        float3 e = k == 0 ? er : el;
+        if (tri >= 0 && abs_sum(e) > 0.f) accum(k == 0 ? pr : pl, k == 0 ? e : -e);
+    }
     return res;
 }
 
