@@ -29,8 +29,19 @@ sys.path.insert(0, ROOT)
 
 METRIC = "fwd+bwd samples/s"
 UNIT = "samples/s"
-WORKLOAD = dict(name="soft_shadow", resolution=(512, 512), spp=16, max_bounces=1, scene_seed=0)
-# reference CPU arm: a bounded slice of the same workload
+# The headline workload is the soft-shadow scene (8 triangles, 512x512, 16 spp,
+# max_bounces 1); the heightfield (130,050 + 4 triangles, 640x480, 64 spp,
+# max_bounces 3) is the large-scene configuration.  ref_res, ref_spp: image
+# size and samples per pixel of the reference CPU arm's steps (the heightfield
+# is too slow on the CPU at full size; its time is linear in samples).
+WORKLOADS = {
+    "soft_shadow": dict(builder="soft_shadow", resolution=(512, 512), spp=16, max_bounces=1, scene_seed=0,
+                        ref_res=(512, 512), ref_spp=16),
+    "heightfield": dict(builder="heightfield", resolution=(640, 480), spp=64, max_bounces=3, scene_seed=0,
+                        ref_res=(160, 120), ref_spp=1),
+}
+WORKLOAD = WORKLOADS["soft_shadow"]
+# reference CPU arm: warm-up on a small slice of the same workload
 REF_RES = (192, 192)
 
 
@@ -41,6 +52,7 @@ def parse():
     p.add_argument("--warmup", type=int, default=3)
     p.add_argument("--impl", default="b200", choices=["b200", "reference"])
     p.add_argument("--no-cpu-baseline", action="store_true")
+    p.add_argument("--workload", default="soft_shadow", choices=sorted(WORKLOADS))
     return p.parse_args()
 
 
@@ -49,11 +61,16 @@ def dist_info():
             int(os.environ.get("WORLD_SIZE", 1)))
 
 
-def build_workload(res=None):
+def build_workload(res=None, spp=None):
     from delta_ray_b200 import workloads
     w = WORKLOAD
-    return workloads.soft_shadow(seed=w["scene_seed"], resolution=res or w["resolution"], spp=w["spp"],
-                                 max_bounces=w["max_bounces"])
+    return workloads.BUILDERS[w["builder"]](seed=w["scene_seed"], resolution=res or w["resolution"],
+                                            spp=spp or w["spp"], max_bounces=w["max_bounces"])
+
+
+def workload_label():
+    w = WORKLOAD
+    return f"{w['builder']} {w['resolution'][0]}x{w['resolution'][1]} {w['spp']}spp max_bounces={w['max_bounces']} fwd+bwd"
 
 
 # ---------------------------------------------------------------------------
@@ -192,13 +209,13 @@ def cpu_baseline():
     import ref_runner
     if not ref_runner.reference_available():
         return None
-    reference_step(build_workload(REF_RES), 0)  # page in, start the pool
-    wl = build_workload()
+    reference_step(build_workload(REF_RES, spp=1), 0)  # page in, start the pool
+    wl = build_workload(spp=WORKLOAD["ref_spp"])
     W, H = wl.resolution
     ts = [reference_step(wl, 1 + i) for i in range(2)]
     samples = W * H * wl.spp
     return {"value": 2 * samples / sum(ts), "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
-            "sample": f"2 steps of the full workload ({W}x{H} at {wl.spp} spp, forward call + backward call), "
+            "sample": f"2 steps of the workload's scene at {W}x{H}, {wl.spp} spp (forward call + backward call), "
                       f"{sum(ts):.1f} s"}
 
 
@@ -211,10 +228,10 @@ def run_reference(args):
     if not ref_runner.reference_available():
         print(json.dumps({"impl": "reference", "unavailable": "reference build oracle/_ref missing"}))
         return 0
-    small = build_workload(REF_RES)
+    small = build_workload(REF_RES, spp=1)
     for i in range(args.warmup):  # warm-up on a 192x192 slice: pages in, starts the pool
         reference_step(small, 100 + i)
-    wl = build_workload()
+    wl = build_workload(WORKLOAD["ref_res"], spp=WORKLOAD["ref_spp"])
     W, H = wl.resolution
     ts = [reference_step(wl, i) for i in range(args.steps)]
     total = sum(ts)
@@ -224,7 +241,7 @@ def run_reference(args):
             "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scene)",
             "impl": "reference",
-            "config": {"workload": "soft_shadow 512x512 16spp max_bounces=1 fwd+bwd", "resolution": [W, H],
+            "config": {"workload": workload_label(), "resolution": [W, H],
                        "spp": wl.spp,
                        "max_bounces": wl.max_bounces, "l2": "n/a (CPU)"},
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
@@ -329,10 +346,10 @@ def run_b200(args):
         loss = img.sum()
         loss.item()
         loss.backward()
-    for i in range(2):
+    for i in range(min(2, args.warmup)):
         e2e_step(500 + i)
     torch.cuda.synchronize()
-    e2e_steps = max(3, min(args.steps, 5))
+    e2e_steps = max(1, min(args.steps, 5))
     t0 = time.perf_counter()
     for k in range(e2e_steps):
         e2e_step(600 + k)
@@ -357,7 +374,7 @@ def run_b200(args):
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scene)",
-            "config": {"workload": "soft_shadow 512x512 16spp max_bounces=1 fwd+bwd",
+            "config": {"workload": workload_label(),
                        "resolution": [W, H], "spp": spp, "max_bounces": B, "triangles": wl.num_triangles,
                        "parallelism": f"dp{world} (per-rank sample streams, gradient all-reduce)", "l2": "flushed between steps (256 MB write)"},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
@@ -376,7 +393,9 @@ def run_b200(args):
 
 
 def main():
+    global WORKLOAD
     args = parse()
+    WORKLOAD = WORKLOADS[args.workload]
     if args.impl == "reference":
         return run_reference(args)
     return run_b200(args)

@@ -284,11 +284,102 @@ void check_render_desc(const dr_scene *sc, const dr_render_desc *rd) {
         throw DrError(DR_ERR_INVALID_ARGUMENT, "width, height and spp must be positive, max_bounces >= 0");
     if ((long long)rd->width * rd->height > (1ll << 28))
         throw DrError(DR_ERR_INVALID_ARGUMENT, "image too large");
+    if ((long long)rd->width * rd->height * rd->spp >= (1ll << 31))
+        throw DrError(DR_ERR_INVALID_ARGUMENT, "width * height * spp must be below 2^31 per call");
     for (int i = 0; i < 7; i++)
         if (rd->reserved[i] != 0) throw DrError(DR_ERR_INVALID_ARGUMENT, "reserved fields must be zero");
     if (rd->flags & ~(int)DR_FLAG_FULL_PIXEL_JITTER) throw DrError(DR_ERR_INVALID_ARGUMENT, "unknown render flags");
     if (rd->max_bounces > 64) throw DrError(DR_ERR_NOT_SUPPORTED, "max_bounces above 64");
     if (sc->ds.num_lights == 0) throw DrError(DR_ERR_INVALID_ARGUMENT, "scene has no lights");
+}
+
+// Item queue limit of dr_render_backward: 8 GiB of edge items (32 bytes each:
+// the item, its weight and its dp).  Edge stages with more items stream.
+constexpr long long kMaxQueueItems = (8ll << 30) / 32;
+
+void check_backward_args(const dr_scene *scene, const dr_render_desc *rd, const float *d_image_dev,
+                         const float *grad_dev) {
+    check_render_desc(scene, rd);
+    if (!d_image_dev || !grad_dev) throw DrError(DR_ERR_INVALID_ARGUMENT, "d_image and grad must be non-NULL");
+    if (rd->dp_mode != DR_DP_REFERENCE_LAST && rd->dp_mode != DR_DP_SUM)
+        throw DrError(DR_ERR_INVALID_ARGUMENT, "unknown dp_mode");
+    if (scene->h.specular_bounces && rd->max_bounces >= 1)
+        throw DrError(DR_ERR_NOT_SUPPORTED,
+                      "backward through specular bounces (roughness <= 0.01 with a specular lobe) is not "
+                      "implemented; the forward render supports them");
+}
+
+// The backward pass on the queues bound in ws (counters zeroed here).
+// Path adjoints and primary edges run first, with the edge traversal of all
+// shading points behind them; if the sampled edges outgrow the item queue,
+// `grow(n)` is asked for room for n items (it returns the capacity it bound),
+// and the edge stage then streams: points in chunks whose items fit, each
+// chunk traversed, evaluated and its position adjoints propagated before the
+// next.  Returns (shading points, edge items).
+template <class Grow>
+std::pair<long long, long long> run_backward(dr_scene *scene, const dr_render_desc *rd, const float *d_image_dev,
+                                             float *grad_dev, float *image_dev, BackwardWorkspace &ws,
+                                             cudaStream_t st, StageTimer *timer, Grow grow) {
+    const DevScene ds = call_scene(scene, rd);
+    const GradCacheCfg cfg = grad_cache_cfg(scene->h);
+    BackwardCounters c;
+    auto read = [&]() {
+        check_cuda(cudaMemcpyAsync(&c, ws.counters, sizeof(c), cudaMemcpyDeviceToHost, st), "status read");
+        check_cuda(cudaStreamSynchronize(st), "backward");
+        if (c.status & ~DR_STATUS_ITEM_OVERFLOW)
+            throw DrError(DR_ERR_DEVICE_STATUS, "device reported status " + std::to_string(c.status));
+    };
+    auto back = [&]() {
+        check_cuda(dr_launch_backward_back(ds, rd->width, rd->height, rd->spp, rd->max_bounces, rd->seed, grad_dev,
+                                           rd->dp_mode, ws, cfg, scene->num_sms, st, &scene->last_launches, timer),
+                   "backward launch");
+    };
+    check_cuda(cudaMemsetAsync(ws.counters, 0, sizeof(BackwardCounters), st), "memset");
+    check_cuda(cudaMemsetAsync(grad_dev, 0, sizeof(float) * scene->h.grad_total, st), "memset");
+    ws.pt_begin = 0;
+    ws.pt_end = ws.cap_points;
+    check_cuda(dr_launch_backward_front(ds, rd->width, rd->height, rd->spp, rd->max_bounces, rd->seed, d_image_dev,
+                                        grad_dev, image_dev, rd->primary_edge_samples, rd->dp_mode, ws, cfg,
+                                        scene->num_sms, st, &scene->last_launches, timer),
+               "backward launch");
+    read();
+    const long long P = std::min((long long)c.points, ws.cap_points);
+    long long items = 0;
+    if (!(c.status & DR_STATUS_ITEM_OVERFLOW)) {
+        timer->mark(st, "host_queue_check");
+        back();
+        items = (long long)c.items;
+    } else {
+        long long needed = (long long)c.items;
+        long long cap = grow(needed + needed / 8 + 1);
+        long long chunk = cap >= needed ? P : std::max(1ll, (long long)((double)P * cap / needed * 0.9));
+        long long p0 = 0;
+        while (p0 < P) {
+            long long p1 = std::min(P, p0 + chunk);
+            ws.pt_begin = p0;
+            ws.pt_end = p1;
+            // reset the item counter and the status word (items, status, pad)
+            check_cuda(cudaMemsetAsync(&ws.counters->items, 0, 16, st), "memset");
+            check_cuda(dr_launch_edge_traverse(ds, rd->seed, ws, scene->num_sms, st, &scene->last_launches, timer),
+                       "edge traversal launch");
+            read();
+            if (c.status & DR_STATUS_ITEM_OVERFLOW) {
+                needed = (long long)c.items;
+                cap = grow(needed + needed / 8 + 1);
+                if (cap >= needed) continue;  // the same chunk again, with room for it
+                if (p1 - p0 == 1)
+                    throw DrError(DR_ERR_OUT_OF_MEMORY, "one shading point samples " + std::to_string(needed) +
+                                                            " edges; the item queue holds " + std::to_string(cap));
+                chunk = std::max(1ll, (long long)((double)(p1 - p0) * cap / needed * 0.9));
+                continue;
+            }
+            back();
+            items += (long long)c.items;
+            p0 = p1;
+        }
+    }
+    check_cuda(cudaStreamSynchronize(st), "backward");
+    return {P, items};
 }
 
 template <typename F> dr_status guard(F f) {
@@ -386,14 +477,7 @@ dr_status dr_render_forward(dr_scene *scene, const dr_render_desc *rd, float *im
 dr_status dr_render_backward(dr_scene *scene, const dr_render_desc *rd, const float *d_image_dev, float *grad_dev,
                              float *image_dev, void *stream) {
     return guard([&]() {
-        check_render_desc(scene, rd);
-        if (!d_image_dev || !grad_dev) throw DrError(DR_ERR_INVALID_ARGUMENT, "d_image and grad must be non-NULL");
-        if (rd->dp_mode != DR_DP_REFERENCE_LAST && rd->dp_mode != DR_DP_SUM)
-            throw DrError(DR_ERR_INVALID_ARGUMENT, "unknown dp_mode");
-        if (scene->h.specular_bounces && rd->max_bounces >= 1)
-            throw DrError(DR_ERR_NOT_SUPPORTED,
-                          "backward through specular bounces (roughness <= 0.01 with a specular lobe) is not "
-                          "implemented; the forward render supports them");
+        check_backward_args(scene, rd, d_image_dev, grad_dev);
         check_cuda(cudaSetDevice(scene->device), "cudaSetDevice");
         cudaStream_t st = (cudaStream_t)stream;
         scene->last_launches = 0;
@@ -401,10 +485,10 @@ dr_status dr_render_backward(dr_scene *scene, const dr_render_desc *rd, const fl
         long long cap_points = (long long)rd->width * rd->height * rd->spp;
         if (!scene->queues) scene->queues = take_queues(scene->device, st);
         BackwardQueues &q = *scene->queues;
-        long long cap_items = std::max(q.cap_items, std::max<long long>(cap_points * 4, 1 << 16));
+        long long cap_items = std::min(kMaxQueueItems, std::max(q.cap_items, std::max<long long>(cap_points * 4, 1 << 16)));
         q.pt.reserve(sizeof(float) * DR_PT_FLOATS * cap_points);
         q.pt_last.reserve(sizeof(unsigned long long) * cap_points);
-        q.counts.reserve(sizeof(int) * 4);
+        q.counts.reserve(sizeof(BackwardCounters));
         if (!q.idle) check_cuda(cudaEventCreateWithFlags(&q.idle, cudaEventDisableTiming), "cudaEventCreate");
         // marks the queues busy up to here on every way out, errors included
         struct MarkIdle {
@@ -412,7 +496,6 @@ dr_status dr_render_backward(dr_scene *scene, const dr_render_desc *rd, const fl
             cudaStream_t st;
             ~MarkIdle() { cudaEventRecord(e, st); }
         } mark_idle{q.idle, st};
-        GradCacheCfg cfg = grad_cache_cfg(scene->h);
         BackwardWorkspace ws;
         auto bind_items = [&]() {
             q.items.reserve(sizeof(int4) * cap_items);
@@ -427,46 +510,22 @@ dr_status dr_render_backward(dr_scene *scene, const dr_render_desc *rd, const fl
         ws.pt = q.pt.as<float>();
         ws.pt_last = q.pt_last.as<unsigned long long>();
         ws.cap_points = cap_points;
-        ws.pt_count = q.counts.as<int>();
-        ws.item_count = q.counts.as<int>() + 1;
-        ws.status = q.counts.as<int>() + 2;
+        ws.counters = q.counts.as<BackwardCounters>();
         bind_items();
-        int counts[4];
-        auto read_counts = [&]() {
-            check_cuda(cudaMemcpyAsync(counts, q.counts.p, sizeof(counts), cudaMemcpyDeviceToHost, st),
-                       "status read");
-            check_cuda(cudaStreamSynchronize(st), "backward");
+        // the item queue grows to what the traversal reported, up to its limit
+        // (the grown queue is kept for later calls)
+        auto grow = [&](long long want) {
+            long long target = std::min(want, kMaxQueueItems);
+            if (target > cap_items) {
+                cap_items = target;
+                bind_items();
+            }
+            return cap_items;
         };
-        check_cuda(cudaMemsetAsync(q.counts.p, 0, sizeof(int) * 4, st), "memset");
-        check_cuda(cudaMemsetAsync(grad_dev, 0, sizeof(float) * scene->h.grad_total, st), "memset");
-        check_cuda(dr_launch_backward_front(call_scene(scene, rd), rd->width, rd->height, rd->spp, rd->max_bounces, rd->seed,
-                                            d_image_dev, grad_dev, image_dev, rd->primary_edge_samples, rd->dp_mode,
-                                            ws, cfg, scene->num_sms, st, &scene->last_launches, &scene->timer),
-                   "backward launch");
-        read_counts();
-        for (int attempt = 0; counts[2] & DR_STATUS_ITEM_OVERFLOW; attempt++) {
-            // the traversal reported how many items it needed: grow the item
-            // queue to that (kept for later calls) and re-run the traversal
-            if (attempt == 3) throw DrError(DR_ERR_DEVICE_STATUS, "edge item queue kept overflowing");
-            cap_items = std::max(cap_items * 2, (long long)counts[1] + (counts[1] >> 3) + 1);
-            bind_items();
-            check_cuda(cudaMemsetAsync(q.counts.as<int>() + 1, 0, sizeof(int) * 2, st), "memset");
-            check_cuda(dr_launch_edge_traverse(call_scene(scene, rd), rd->seed, ws, scene->num_sms, st, &scene->last_launches,
-                                               &scene->timer),
-                       "edge traversal launch");
-            read_counts();
-        }
-        if (counts[2]) throw DrError(DR_ERR_DEVICE_STATUS, "device reported status " + std::to_string(counts[2]));
-        scene->timer.mark(st, "host_queue_check");
-        check_cuda(dr_launch_backward_back(call_scene(scene, rd), rd->width, rd->height, rd->spp, rd->max_bounces, rd->seed,
-                                           grad_dev, rd->dp_mode, ws, cfg, scene->num_sms, st, &scene->last_launches,
-                                           &scene->timer),
-                   "backward launch");
-        read_counts();
-        scene->last_points = counts[0];
-        scene->last_items = counts[1];
+        auto counts = run_backward(scene, rd, d_image_dev, grad_dev, image_dev, ws, st, &scene->timer, grow);
+        scene->last_points = counts.first;
+        scene->last_items = counts.second;
         collect_timings(scene, st);
-        if (counts[2]) throw DrError(DR_ERR_DEVICE_STATUS, "device reported status " + std::to_string(counts[2]));
     });
 }
 
@@ -577,14 +636,7 @@ extern "C" {
 dr_status dr_render_backward_noalloc(dr_scene *scene, const dr_render_desc *rd, const float *d_image_dev,
                                      float *grad_dev, float *image_dev, void *stream) {
     return guard([&]() {
-        check_render_desc(scene, rd);
-        if (!d_image_dev || !grad_dev) throw DrError(DR_ERR_INVALID_ARGUMENT, "d_image and grad must be non-NULL");
-        if (rd->dp_mode != DR_DP_REFERENCE_LAST && rd->dp_mode != DR_DP_SUM)
-            throw DrError(DR_ERR_INVALID_ARGUMENT, "unknown dp_mode");
-        if (scene->h.specular_bounces && rd->max_bounces >= 1)
-            throw DrError(DR_ERR_NOT_SUPPORTED,
-                          "backward through specular bounces (roughness <= 0.01 with a specular lobe) is not "
-                          "implemented; the forward render supports them");
+        check_backward_args(scene, rd, d_image_dev, grad_dev);
         long long npix = (long long)rd->width * rd->height * rd->spp;
         if (npix > kNoAllocMaxSamples)
             throw DrError(DR_ERR_INVALID_ARGUMENT,
@@ -600,9 +652,7 @@ dr_status dr_render_backward_noalloc(dr_scene *scene, const dr_render_desc *rd, 
         long long cap_points = npix;
         size_t off = 256;
         BackwardWorkspace ws;
-        ws.pt_count = (int *)base;
-        ws.item_count = (int *)base + 1;
-        ws.status = (int *)base + 2;
+        ws.counters = (BackwardCounters *)base;
         ws.pt = (float *)(base + off);
         off += up(sizeof(float) * DR_PT_FLOATS * (size_t)cap_points);
         ws.pt_last = (unsigned long long *)(base + off);
@@ -617,35 +667,14 @@ dr_status dr_render_backward_noalloc(dr_scene *scene, const dr_render_desc *rd, 
         if (off > kNoAllocScratchBytes) throw DrError(DR_ERR_INVALID_ARGUMENT, "scratch layout does not fit");
         ws.cap_points = cap_points;
         ws.cap_items = cap_items;
-        // what must start at zero: the three queue counters and the gradient
-        // (the point keys of the "last edge" rule are cleared by the launcher)
-        check_cuda(cudaMemsetAsync(base, 0, sizeof(int) * 4, st), "memset");
-        check_cuda(cudaMemsetAsync(grad_dev, 0, sizeof(float) * scene->h.grad_total, st), "memset");
+        // what must start at zero, the queue counters and the gradient, is
+        // cleared by run_backward (the point keys of the "last edge" rule by
+        // the launcher); the queue cannot grow, so large edge stages stream
         StageTimer quiet;  // no profiling events on this path
-        GradCacheCfg cfg = grad_cache_cfg(scene->h);
-        int counts[4];
-        auto read_counts = [&]() {
-            check_cuda(cudaMemcpyAsync(counts, base, sizeof(counts), cudaMemcpyDeviceToHost, st), "status read");
-            check_cuda(cudaStreamSynchronize(st), "backward");
-        };
-        check_cuda(dr_launch_backward_front(call_scene(scene, rd), rd->width, rd->height, rd->spp, rd->max_bounces, rd->seed,
-                                            d_image_dev, grad_dev, image_dev, rd->primary_edge_samples, rd->dp_mode,
-                                            ws, cfg, scene->num_sms, st, &scene->last_launches, &quiet),
-                   "backward launch");
-        read_counts();
-        if (counts[2] & DR_STATUS_ITEM_OVERFLOW)
-            throw DrError(DR_ERR_DEVICE_STATUS, "the sampled edges (" + std::to_string(counts[1]) +
-                                                    ") exceed the no-alloc scratch (" + std::to_string(cap_items) +
-                                                    " items); use dr_render_backward");
-        if (counts[2]) throw DrError(DR_ERR_DEVICE_STATUS, "device reported status " + std::to_string(counts[2]));
-        check_cuda(dr_launch_backward_back(call_scene(scene, rd), rd->width, rd->height, rd->spp, rd->max_bounces, rd->seed,
-                                           grad_dev, rd->dp_mode, ws, cfg, scene->num_sms, st, &scene->last_launches,
-                                           &quiet),
-                   "backward launch");
-        read_counts();
-        scene->last_points = counts[0];
-        scene->last_items = counts[1];
-        if (counts[2]) throw DrError(DR_ERR_DEVICE_STATUS, "device reported status " + std::to_string(counts[2]));
+        auto counts = run_backward(scene, rd, d_image_dev, grad_dev, image_dev, ws, st, &quiet,
+                                   [&](long long) { return cap_items; });
+        scene->last_points = counts.first;
+        scene->last_items = counts.second;
     });
 }
 

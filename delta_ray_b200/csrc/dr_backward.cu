@@ -49,10 +49,10 @@ __global__ void __launch_bounds__(128, 3) k_backward_paths(DevScene s, int W, in
             acc += backward_pixel_sample(s, x, y, W, H, spp, si, B, seed, dc, bg, push);
         }
         __syncwarp();
-        long long slot = warp_reserve(ws.pt_count, has ? 1 : 0);
+        unsigned long long slot = warp_reserve(&ws.counters->points, has ? 1 : 0);
         if (has) {
-            if (slot < ws.cap_points) pr.store(ws.pt + (size_t)slot * DR_PT_WORDS);
-            else set_status(ws.status, DR_STATUS_POINT_OVERFLOW);
+            if (slot < (unsigned long long)ws.cap_points) pr.store(ws.pt + (size_t)slot * DR_PT_WORDS);
+            else set_status(&ws.counters->status, DR_STATUS_POINT_OVERFLOW);
         }
     }
     for (int off = G >> 1; off >= 1; off >>= 1) {
@@ -72,8 +72,9 @@ __global__ void __launch_bounds__(128) k_dp_propagate(DevScene s, int W, int H, 
                                                       BackwardWorkspace ws, GradCacheCfg cfg) {
     extern __shared__ float sm[];
     BlockGrad bg = block_grad_begin(sm, grad, cfg);
-    long long n = min((long long)*ws.pt_count, ws.cap_points);
-    for (long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x; p < n; p += (long long)gridDim.x * blockDim.x) {
+    long long n = min(min((long long)ws.counters->points, ws.cap_points), ws.pt_end);
+    for (long long p = ws.pt_begin + (long long)blockIdx.x * blockDim.x + threadIdx.x; p < n;
+         p += (long long)gridDim.x * blockDim.x) {
         unsigned long long key = ws.pt_last[p];
         if (key == 0) continue;
         long long i = (long long)(key & 0xffffffffull);

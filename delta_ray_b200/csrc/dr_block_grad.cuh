@@ -47,7 +47,7 @@ __device__ __forceinline__ void set_status(int *status, int bit) { atomicOr(stat
 
 // Reserves `count` consecutive slots for each lane of the (fully converged)
 // warp with one atomic: returns the lane's first slot.
-__device__ __forceinline__ long long warp_reserve(int *counter, int count) {
+__device__ __forceinline__ unsigned long long warp_reserve(unsigned long long *counter, int count) {
     const unsigned full = 0xffffffffu;
     int lane = threadIdx.x & 31;
     int incl = count;
@@ -56,10 +56,10 @@ __device__ __forceinline__ long long warp_reserve(int *counter, int count) {
         if (lane >= off) incl += v;
     }
     int total = __shfl_sync(full, incl, 31);
-    long long base = 0;
-    if (lane == 31 && total > 0) base = atomicAdd(counter, total);
+    unsigned long long base = 0;
+    if (lane == 31 && total > 0) base = atomicAdd(counter, (unsigned long long)total);
     base = __shfl_sync(full, base, 31);
-    return base + incl - count;
+    return base + (unsigned long long)(incl - count);
 }
 
 inline int blocks_for(long long n, int bs) { return (int)((n + bs - 1) / bs); }

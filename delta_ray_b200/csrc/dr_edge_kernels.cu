@@ -7,56 +7,63 @@
 #include "dr_block_grad.cuh"
 
 #define DR_ITEM_BUF 24
+// One thread per shading point in [pt_begin, pt_end).  A point's items collect
+// in a lane buffer; a full buffer reserves DR_ITEM_BUF slots with one atomic
+// (points of large glossy scenes sample thousands of edges), and the last
+// partial buffers of a warp share one atomic.
 __global__ void __launch_bounds__(128, 4) k_edge_traverse(DevScene s, uint64_t seed, BackwardWorkspace ws) {
-    long long n = min((long long)*ws.pt_count, ws.cap_points);
+    long long n = min(min((long long)ws.counters->points, ws.cap_points), ws.pt_end);
     long long stride = (long long)gridDim.x * blockDim.x;
+    unsigned long long *count = &ws.counters->items;
     // warp-uniform loop: every lane of a warp takes the same number of trips
-    for (long long base = (long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < n; base += stride) {
+    for (long long base = ws.pt_begin + (long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < n;
+         base += stride) {
         long long p = base + (threadIdx.x & 31);
         bool active = p < n;
         int buf_e[DR_ITEM_BUF];
         float buf_w[DR_ITEM_BUF];
         int buf_j[DR_ITEM_BUF];
         int nb = 0;
-        auto write_item = [&](long long i, int te, int j, float w) {
-            if (i < ws.cap_items) {
+        auto write_items = [&](unsigned long long first, int cnt) {
+            unsigned long long cap = (unsigned long long)ws.cap_items;
+            if (first + (unsigned long long)cnt > cap) set_status(&ws.counters->status, DR_STATUS_ITEM_OVERFLOW);
+            for (int k = 0; k < cnt; k++) {
+                unsigned long long i = first + (unsigned long long)k;
+                if (i >= cap) break;
                 int4 it;
                 it.x = (int)p;
-                it.y = te;
-                it.z = j;
+                it.y = buf_e[k];
+                it.z = buf_j[k];
                 it.w = 0;
                 ws.items[i] = it;
-                ws.item_w[i] = w;
-            } else {
-                set_status(ws.status, DR_STATUS_ITEM_OVERFLOW);
+                ws.item_w[i] = buf_w[k];
             }
         };
         if (active) {
             PointRecord pt;
             pt.load(ws.pt + (size_t)p * DR_PT_WORDS);
             auto emit = [&](int tree, int ei, int j, float w) {
-                if (nb < DR_ITEM_BUF) {
-                    buf_e[nb] = (tree << 30) | ei;
-                    buf_j[nb] = j;
-                    buf_w[nb] = w;
-                    nb++;
-                } else {  // rare: more edges than the lane buffer holds
-                    write_item(atomicAdd(ws.item_count, 1), (tree << 30) | ei, j, w);
+                if (nb == DR_ITEM_BUF) {
+                    write_items(atomicAdd(count, (unsigned long long)DR_ITEM_BUF), DR_ITEM_BUF);
+                    nb = 0;
                 }
+                buf_e[nb] = (tree << 30) | ei;
+                buf_j[nb] = j;
+                buf_w[nb] = w;
+                nb++;
             };
-            if (!traverse_point(s, pt, seed, emit)) set_status(ws.status, DR_STATUS_STACK_OVERFLOW);
+            if (!traverse_point(s, pt, seed, emit)) set_status(&ws.counters->status, DR_STATUS_STACK_OVERFLOW);
         }
         __syncwarp();
-        long long slot = warp_reserve(ws.item_count, nb);
-        for (int k = 0; k < nb; k++) write_item(slot + k, buf_e[k], buf_j[k], buf_w[k]);
+        write_items(warp_reserve(count, nb), nb);
     }
 }
 
-__global__ void __launch_bounds__(128, 3) k_edge_eval(DevScene s, int W, int H, int spp, int B, uint64_t seed, int dp_mode,
+__global__ void __launch_bounds__(128, 4) k_edge_eval(DevScene s, int W, int H, int spp, int B, uint64_t seed, int dp_mode,
                                                    float *grad, BackwardWorkspace ws, GradCacheCfg cfg) {
     extern __shared__ float sm[];
     BlockGrad bg = block_grad_begin(sm, grad, cfg);
-    long long n = min((long long)*ws.item_count, ws.cap_items);
+    long long n = (long long)min(ws.counters->items, (unsigned long long)ws.cap_items);
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
         int4 it = ws.items[i];
         PointRecord pt;

@@ -38,17 +38,27 @@ cudaError_t dr_launch_forward(const DevScene &s, int W, int H, int spp, int B, u
                               cudaStream_t st, int *launches, StageTimer *timer);
 
 // Backward pass (dr_backward.cu).
+// Queue counters on the device.  They are 64-bit and keep counting past a
+// queue's capacity, so the host learns how many entries a launch needed.
+struct BackwardCounters {
+    unsigned long long points;  // shading points appended by k_backward_paths
+    unsigned long long items;   // edge items appended by the last k_edge_traverse
+    int status;                 // DR_STATUS_* bits
+    int pad;
+};
+
 struct BackwardWorkspace {
     float *pt;                   // [cap_points][DR_PT_FLOATS] shading-point records
-    int *pt_count;               // [1]
     long long cap_points;
     int4 *items;                 // sampled edges: (point, tree << 30 | edge, ordinal j, 0)
     float *item_w;               // edge weight
-    int *item_count;             // [1]
     long long cap_items;
     float *item_dp;              // [cap_items][3] position adjoint of each item
     unsigned long long *pt_last; // [cap_points] ((j + 1) << 32 | item) of the point's last item with dp != 0
-    int *status;                 // [1] error bits
+    BackwardCounters *counters;
+    // points [pt_begin, min(pt_end, counters->points)) go through the edge
+    // stage (k_edge_traverse, k_edge_eval, k_dp_propagate) of one launch
+    long long pt_begin, pt_end;
 };
 
 // Which part of the flat gradient a block caches in shared memory:

@@ -77,3 +77,27 @@ def test_noalloc_backward_rejects_oversize_calls():
     assert st == DR_ERR_INVALID_ARGUMENT
     assert "65536" in _lib.last_error()
     sc.close()
+
+
+@pytest.mark.gpu
+def test_noalloc_backward_streams_large_edge_stages():
+    """A glossy heightfield whose shading points sample about 2,000 edges each:
+    the items outgrow the fixed scratch, so the no-alloc call evaluates them in
+    several passes over the points; the result must match the regular call
+    (whose item queue grows instead)."""
+    from delta_ray_b200 import _lib, workloads
+    from delta_ray_b200.render_pytorch import Scene, unpack_args
+    L = _bind(_lib.lib())
+    W, H, spp, B = 32, 24, 4, 2
+    wl = workloads.heightfield(0, (W, H), spp, B)  # 130,054 triangles
+    cam, mats, shps, lts, _, _, _, _ = unpack_args(wl.serialize())
+    sc = Scene(cam, mats, shps, lts, 0, None)
+    d_image = torch.ones((H, W, 3), dtype=torch.float32, device="cuda")
+    ref_grad, _ = sc.backward(W, H, spp, B, 21, d_image)
+    _, ref_items = sc.last_counts()
+    st, grad, _ = _noalloc(L, sc, W, H, spp, B, 21, d_image)
+    assert st == 0, _lib.last_error()
+    _, items = sc.last_counts()
+    assert items == ref_items and items > 900_000  # more than the scratch holds at once
+    assert rel_err(grad.cpu().numpy(), ref_grad.cpu().numpy()) < TOL
+    sc.close()
