@@ -30,19 +30,21 @@ sys.path.insert(0, ROOT)
 METRIC = "fwd+bwd samples/s"
 UNIT = "samples/s"
 # The headline workload is the soft-shadow scene (8 triangles, 512x512, 16 spp,
-# max_bounces 1); the heightfield (130,050 + 4 triangles, 640x480, 64 spp,
-# max_bounces 3) is the large-scene configuration.  ref_res, ref_spp: image
-# size and samples per pixel of the reference CPU arm's steps (the heightfield
-# is too slow on the CPU at full size; its time is linear in samples).
+# max_bounces 1).  The heightfield scene (130,050 + 4 triangles, glossy, 2
+# lights, max_bounces 3) runs at 160x120 and 4 spp: its shading points sample
+# about 1,100 edges each under the reference's edge-tree rules, so the full
+# 640x480 x 64 spp image would need 3e10 edge evaluations per backward call.
+# ref_res, ref_spp: image size and samples per pixel of the reference CPU arm's
+# steps (its time is linear in samples).
 WORKLOADS = {
     "soft_shadow": dict(builder="soft_shadow", resolution=(512, 512), spp=16, max_bounces=1, scene_seed=0,
                         ref_res=(512, 512), ref_spp=16),
-    "heightfield": dict(builder="heightfield", resolution=(640, 480), spp=64, max_bounces=3, scene_seed=0,
-                        ref_res=(160, 120), ref_spp=1),
+    "heightfield": dict(builder="heightfield", resolution=(160, 120), spp=4, max_bounces=3, scene_seed=0,
+                        ref_res=(80, 60), ref_spp=1),
 }
 WORKLOAD = WORKLOADS["soft_shadow"]
-# reference CPU arm: warm-up on a small slice of the same workload
-REF_RES = (192, 192)
+# reference CPU arm: page-in / warm-up steps on a small slice of the same scene
+REF_RES = (32, 32)
 
 
 def parse():
@@ -203,14 +205,14 @@ def reference_step(wl, seed):
 
 def cpu_baseline():
     """The reference's own CPU path (oracle/_ref, -O3 -ffast-math, its thread pool
-    on all host cores) on the full workload: two timed steps (about 10 s of CPU
-    work on 16 cores) after a small page-in step."""
+    on all host cores): two timed steps of the workload's scene at its reference
+    size (about 10-20 s of CPU work on 16 cores) after a small page-in step."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import ref_runner
     if not ref_runner.reference_available():
         return None
     reference_step(build_workload(REF_RES, spp=1), 0)  # page in, start the pool
-    wl = build_workload(spp=WORKLOAD["ref_spp"])
+    wl = build_workload(WORKLOAD["ref_res"], spp=WORKLOAD["ref_spp"])
     W, H = wl.resolution
     ts = [reference_step(wl, 1 + i) for i in range(2)]
     samples = W * H * wl.spp
