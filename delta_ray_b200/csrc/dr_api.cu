@@ -159,6 +159,7 @@ struct dr_scene {
     std::vector<std::pair<std::string, float>> timings;
     long long last_points = 0, last_items = 0;
     int num_vertices = 0, num_tris = 0, num_sms = 148;
+    int bvh_built_tris = 0;  // triangle count of the LBVH topology kept in bvh_scratch
     ~dr_scene() {
         if (timer_ready)
             for (int i = 0; i <= StageTimer::kMax; i++) cudaEventDestroy(timer.ev[i]);
@@ -169,7 +170,7 @@ struct dr_scene {
 
 namespace {
 
-void upload_scene(dr_scene *sc, cudaStream_t st) {
+void upload_scene(dr_scene *sc, cudaStream_t st, bool refit = false) {
     HostScene &h = sc->h;
     check_cuda(cudaSetDevice(sc->device), "cudaSetDevice");
     FlatScene f;
@@ -203,14 +204,24 @@ void upload_scene(dr_scene *sc, cudaStream_t st) {
     sc->bvh_nodes.reserve(sizeof(float4) * 4 * (size_t)std::max(1, n - 1));
     sc->bvh_tris.reserve(sizeof(float4) * 3 * (size_t)std::max(1, n));
     if (n > 0) {
+        // the build's working arrays stay with the scene: an update with new
+        // vertex positions refits the same tree (closest hits do not depend on
+        // the tree's shape, ties going to the lower triangle id)
         size_t sb = dr_lbvh_scratch_bytes(n);
-        sc->bvh_scratch.reserve(sb);
-        check_cuda(dr_build_lbvh(sc->vtx.as<float>(), sc->tri.as<int4>(), n, f.lo, f.hi, sc->bvh_nodes.as<float4>(),
-                                 sc->bvh_tris.as<float4>(), sc->bvh_scratch.p, sc->bvh_scratch.bytes, st,
-                                 &sc->last_launches),
-                   "LBVH build");
+        if (refit && sc->bvh_built_tris == n && sc->bvh_scratch.bytes >= sb) {
+            check_cuda(dr_refit_lbvh(sc->vtx.as<float>(), sc->tri.as<int4>(), n, sc->bvh_nodes.as<float4>(),
+                                     sc->bvh_tris.as<float4>(), sc->bvh_scratch.p, sc->bvh_scratch.bytes, st,
+                                     &sc->last_launches),
+                       "LBVH refit");
+        } else {
+            sc->bvh_scratch.reserve(sb);
+            check_cuda(dr_build_lbvh(sc->vtx.as<float>(), sc->tri.as<int4>(), n, f.lo, f.hi,
+                                     sc->bvh_nodes.as<float4>(), sc->bvh_tris.as<float4>(), sc->bvh_scratch.p,
+                                     sc->bvh_scratch.bytes, st, &sc->last_launches),
+                       "LBVH build");
+            sc->bvh_built_tris = n;
+        }
         check_cuda(cudaStreamSynchronize(st), "LBVH build");
-        sc->bvh_scratch.release();
     }
     ScenePtrs ptr;
     ptr.vtx = sc->vtx.as<float>();
@@ -434,10 +445,22 @@ dr_status dr_scene_update(dr_scene *scene, const dr_scene_desc *desc) {
             if (desc->shapes[i].num_vertices != sizes[i].first || desc->shapes[i].num_triangles != sizes[i].second)
                 throw DrError(DR_ERR_INVALID_ARGUMENT, "update must keep every mesh's topology");
         check_cuda(cudaSetDevice(scene->device), "cudaSetDevice");
+        // the meshes keep their triangles: the edge topology and the LBVH's
+        // topology carry over, everything that depends on positions is redone
+        std::vector<DevEdge> topo = std::move(scene->h.topo_edges);
+        bool topo_valid = scene->h.topo_valid;
+        std::vector<std::vector<int>> old_idx;
+        for (auto &sh : scene->h.shapes) old_idx.push_back(std::move(sh.idx));
         load_desc(scene->h, desc, [](auto p, size_t n, const char *w) { return fetch(p, n, w); });
+        bool same_indices = true;
+        for (int i = 0; i < desc->num_shapes && same_indices; i++) same_indices = scene->h.shapes[i].idx == old_idx[i];
+        if (same_indices && topo_valid) {
+            scene->h.topo_edges = std::move(topo);
+            scene->h.topo_valid = true;
+        }
         scene->h.preprocess();
         scene->last_launches = 0;
-        upload_scene(scene, 0);
+        upload_scene(scene, 0, same_indices);
     });
 }
 

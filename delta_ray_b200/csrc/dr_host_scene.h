@@ -7,7 +7,9 @@
 #pragma once
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
+#include <thread>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -164,12 +166,16 @@ struct BuildNode {
 struct HostScene;
 
 // edge_tree.cpp:49-173 (median split; std::nth_element with the same
-// comparator so that equal centroids resolve as in the reference)
+// comparator so that equal centroids resolve as in the reference).  A leaf
+// covers pi[start, end): leaves in depth-first order cover pi in order, so the
+// edges are laid out as pi once the tree is built.  The two halves of a
+// large node are built on two threads (disjoint ranges of pi; the result is
+// the serial one).
 template <bool DIR>
-std::unique_ptr<BuildNode> build_node(const std::vector<DevEdge> &edges, std::vector<PrimInfo> &pi, int start, int end,
-                                      int *total, std::vector<DevEdge> &ordered) {
+std::unique_ptr<BuildNode> build_node(std::vector<PrimInfo> &pi, int start, int end, std::atomic<int> *total,
+                                      int depth) {
     auto node = std::make_unique<BuildNode>();
-    (*total)++;
+    total->fetch_add(1, std::memory_order_relaxed);
     HAABB sb;
     for (int i = start; i < end; i++) sb.add(pi[i].sb);
     V3 nsum = v3(0.f, 0.f, 0.f);
@@ -185,8 +191,7 @@ std::unique_ptr<BuildNode> build_node(const std::vector<DevEdge> &edges, std::ve
     node->angle = std::acos(cmin);
     int n = end - start;
     auto leaf = [&]() {
-        node->first = (int)ordered.size();
-        for (int i = start; i < end; i++) ordered.push_back(edges[pi[i].prim]);
+        node->first = start;
         node->n = n;
     };
     if (n == 1) {
@@ -221,8 +226,14 @@ std::unique_ptr<BuildNode> build_node(const std::vector<DevEdge> &edges, std::ve
     std::nth_element(&pi[start], &pi[mid], &pi[end - 1] + 1, [dim, spatial](const PrimInfo &a, const PrimInfo &b) {
         return spatial ? get(a.sc, dim) < get(b.sc, dim) : get(a.dc, dim) < get(b.dc, dim);
     });
-    node->c[0] = build_node<DIR>(edges, pi, start, mid, total, ordered);
-    node->c[1] = build_node<DIR>(edges, pi, mid, end, total, ordered);
+    if (n >= 16384 && depth < 4) {
+        std::thread left([&]() { node->c[0] = build_node<DIR>(pi, start, mid, total, depth + 1); });
+        node->c[1] = build_node<DIR>(pi, mid, end, total, depth + 1);
+        left.join();
+    } else {
+        node->c[0] = build_node<DIR>(pi, start, mid, total, depth + 1);
+        node->c[1] = build_node<DIR>(pi, mid, end, total, depth + 1);
+    }
     return node;
 }
 
@@ -230,6 +241,10 @@ struct HostScene {
     HCam cam;
     std::vector<HShape> shapes;
     std::vector<DevMaterial> mats;
+    // unique edges of the meshes before the degenerate/coplanar filter, in
+    // (shape, v0, v1) order; valid while the triangle indices stay the same
+    std::vector<DevEdge> topo_edges;
+    bool topo_valid = false;
     // some material can take a "specular" BSDF sample (roughness <= 0.01 with a
     // nonzero specular lobe, material.h:410): the backward pass does not
     // differentiate through such bounces
@@ -332,9 +347,11 @@ struct HostScene {
                 pi[i].dc = 0.5f * (d.lo + d.hi);
             }
         }
-        int total = 0;
-        auto root = build_node<DIR>(edges, pi, 0, (int)edges.size(), &total, ordered);
-        nodes.resize(total);
+        std::atomic<int> total(0);
+        auto root = build_node<DIR>(pi, 0, (int)edges.size(), &total, 0);
+        ordered.resize(edges.size());
+        for (size_t i = 0; i < edges.size(); i++) ordered[i] = edges[pi[i].prim];
+        nodes.resize(total.load());
         int off = 0;
         flatten(nodes, ordered, root.get(), &off);
     }
@@ -378,25 +395,30 @@ struct HostScene {
             light_tri_func.push_back(0.f);  // keep func and cdf offsets aligned (ntri + 1 slots)
         }
         if (!imp.empty()) light_sel.build(imp);
-        // unique edges in (shape, v0, v1) order (scene.cpp:54-97)
-        std::map<std::tuple<int, int, int>, DevEdge> emap;
-        for (int si = 0; si < (int)shapes.size(); si++) {
-            const HShape &sh = shapes[si];
-            for (int t = 0; t < sh.nt; t++) {
-                int ind[3] = {sh.idx[3 * t], sh.idx[3 * t + 1], sh.idx[3 * t + 2]};
-                for (int k = 0; k < 3; k++) {
-                    int a = ind[k], b = ind[(k + 1) % 3];
-                    if (a > b) std::swap(a, b);
-                    auto key = std::make_tuple(si, a, b);
-                    auto it = emap.find(key);
-                    if (it == emap.end()) emap[key] = DevEdge{si, a, b, t, -1};
-                    else it->second.f1 = t;
+        // unique edges in (shape, v0, v1) order (scene.cpp:54-97); they depend
+        // on the triangle indices only, so an update with new positions reuses them
+        if (!topo_valid) {
+            std::map<std::tuple<int, int, int>, DevEdge> emap;
+            for (int si = 0; si < (int)shapes.size(); si++) {
+                const HShape &sh = shapes[si];
+                for (int t = 0; t < sh.nt; t++) {
+                    int ind[3] = {sh.idx[3 * t], sh.idx[3 * t + 1], sh.idx[3 * t + 2]};
+                    for (int k = 0; k < 3; k++) {
+                        int a = ind[k], b = ind[(k + 1) % 3];
+                        if (a > b) std::swap(a, b);
+                        auto key = std::make_tuple(si, a, b);
+                        auto it = emap.find(key);
+                        if (it == emap.end()) emap[key] = DevEdge{si, a, b, t, -1};
+                        else it->second.f1 = t;
+                    }
                 }
             }
+            topo_edges.clear();
+            for (auto &kv : emap) topo_edges.push_back(kv.second);
+            topo_valid = true;
         }
         std::vector<DevEdge> edges;
-        for (auto &kv : emap) {
-            const DevEdge &e = kv.second;
+        for (const DevEdge &e : topo_edges) {
             V3 d = ev0(e) - ev1(e);
             if (std::fabs(d.x) + std::fabs(d.y) + std::fabs(d.z) < 1e-10f) continue;
             if (e.f1 != -1) {

@@ -77,6 +77,44 @@ __global__ void k_bvh_refit(int n, const int *parent_leaf, const int *parent_int
 
 static inline int blocks_for(long long n, int bs) { return (int)((n + bs - 1) / bs); }
 
+// The build's working arrays, laid out in the caller's scratch.  After a
+// build they hold the tree's topology (sorted leaf order, parent and child
+// links), which a refit reuses.
+struct LbvhScratch {
+    uint32_t *keys, *keys2;
+    int *vals, *vals2;  // vals2: triangle id of each leaf (Morton order)
+    Box *leaf_boxes, *node_boxes;
+    int2 *children;
+    int *parent_internal, *parent_leaf, *flags;
+    void *sort_tmp;
+    size_t sort_bytes, used;
+};
+
+static LbvhScratch lbvh_layout(void *scratch, int n) {
+    LbvhScratch l;
+    char *p = (char *)scratch;
+    auto take = [&](size_t bytes) {
+        char *r = p;
+        p += (bytes + 255) & ~(size_t)255;
+        return (void *)r;
+    };
+    l.keys = (uint32_t *)take(sizeof(uint32_t) * n);
+    l.keys2 = (uint32_t *)take(sizeof(uint32_t) * n);
+    l.vals = (int *)take(sizeof(int) * n);
+    l.vals2 = (int *)take(sizeof(int) * n);
+    l.leaf_boxes = (Box *)take(sizeof(Box) * n);
+    l.node_boxes = (Box *)take(sizeof(Box) * n);
+    l.children = (int2 *)take(sizeof(int2) * n);
+    l.parent_internal = (int *)take(sizeof(int) * n);
+    l.parent_leaf = (int *)take(sizeof(int) * n);
+    l.flags = (int *)take(sizeof(int) * n);
+    l.sort_bytes = 0;
+    cub::DeviceRadixSort::SortPairs(nullptr, l.sort_bytes, l.keys, l.keys2, l.vals, l.vals2, n, 0, 30);
+    l.sort_tmp = take(l.sort_bytes);
+    l.used = (size_t)(p - (char *)scratch);
+    return l;
+}
+
 cudaError_t dr_build_lbvh(const float *vtx, const int4 *tri, int n, float3 lo, float3 hi, float4 *nodes,
                           float4 *leaf_tris, void *scratch, size_t scratch_bytes, cudaStream_t st, int *launches) {
     if (n <= 0) return cudaSuccess;
@@ -87,49 +125,42 @@ cudaError_t dr_build_lbvh(const float *vtx, const int4 *tri, int n, float3 lo, f
     in.lo = lo;
     float3 ext = hi - lo;
     in.inv_ext = f3(ext.x > 0.f ? 1.f / ext.x : 0.f, ext.y > 0.f ? 1.f / ext.y : 0.f, ext.z > 0.f ? 1.f / ext.z : 0.f);
-    char *p = (char *)scratch;
-    auto take = [&](size_t bytes) {
-        char *r = p;
-        p += (bytes + 255) & ~(size_t)255;
-        return (void *)r;
-    };
-    uint32_t *keys = (uint32_t *)take(sizeof(uint32_t) * n);
-    uint32_t *keys2 = (uint32_t *)take(sizeof(uint32_t) * n);
-    int *vals = (int *)take(sizeof(int) * n);
-    int *vals2 = (int *)take(sizeof(int) * n);
-    Box *leaf_boxes = (Box *)take(sizeof(Box) * n);
-    Box *node_boxes = (Box *)take(sizeof(Box) * n);
-    int2 *children = (int2 *)take(sizeof(int2) * n);
-    int *parent_internal = (int *)take(sizeof(int) * n);
-    int *parent_leaf = (int *)take(sizeof(int) * n);
-    int *flags = (int *)take(sizeof(int) * n);
-    size_t used = (size_t)(p - (char *)scratch);
-    size_t sort_bytes = 0;
-    cub::DeviceRadixSort::SortPairs(nullptr, sort_bytes, keys, keys2, vals, vals2, n, 0, 30, st);
-    if (used + sort_bytes > scratch_bytes) return cudaErrorMemoryAllocation;
-    void *sort_tmp = take(sort_bytes);
+    LbvhScratch l = lbvh_layout(scratch, n);
+    if (l.used > scratch_bytes) return cudaErrorMemoryAllocation;
     const int bs = 256;
-    k_bvh_morton<<<blocks_for(n, bs), bs, 0, st>>>(in, keys, vals);
-    cub::DeviceRadixSort::SortPairs(sort_tmp, sort_bytes, keys, keys2, vals, vals2, n, 0, 30, st);
-    k_bvh_leaves<<<blocks_for(n, bs), bs, 0, st>>>(vals2, vtx, tri, n, leaf_tris, leaf_boxes);
+    k_bvh_morton<<<blocks_for(n, bs), bs, 0, st>>>(in, l.keys, l.vals);
+    cub::DeviceRadixSort::SortPairs(l.sort_tmp, l.sort_bytes, l.keys, l.keys2, l.vals, l.vals2, n, 0, 30, st);
+    k_bvh_leaves<<<blocks_for(n, bs), bs, 0, st>>>(l.vals2, vtx, tri, n, leaf_tris, l.leaf_boxes);
     *launches += 3;
     if (n > 1) {
-        cudaMemsetAsync(flags, 0, sizeof(int) * n, st);
-        k_bvh_internal<<<blocks_for(n - 1, bs), bs, 0, st>>>(keys2, n, children, parent_internal, parent_leaf);
-        k_bvh_refit<<<blocks_for(n, bs), bs, 0, st>>>(n, parent_leaf, parent_internal, children, leaf_boxes,
-                                                       node_boxes, flags, nodes);
+        cudaMemsetAsync(l.flags, 0, sizeof(int) * n, st);
+        k_bvh_internal<<<blocks_for(n - 1, bs), bs, 0, st>>>(l.keys2, n, l.children, l.parent_internal,
+                                                               l.parent_leaf);
+        k_bvh_refit<<<blocks_for(n, bs), bs, 0, st>>>(n, l.parent_leaf, l.parent_internal, l.children, l.leaf_boxes,
+                                                       l.node_boxes, l.flags, nodes);
         *launches += 2;
     }
     return cudaGetLastError();
 }
 
-size_t dr_lbvh_scratch_bytes(int n) {
-    size_t sort_bytes = 0;
-    cub::DeviceRadixSort::SortPairs(nullptr, sort_bytes, (uint32_t *)nullptr, (uint32_t *)nullptr, (int *)nullptr,
-                                    (int *)nullptr, n, 0, 30);
-    size_t per = 4 * sizeof(uint32_t) + 2 * sizeof(Box) + sizeof(int2) + 3 * sizeof(int);
-    return (per + 64) * (size_t)n + sort_bytes + 16 * 256;
+cudaError_t dr_refit_lbvh(const float *vtx, const int4 *tri, int n, float4 *nodes, float4 *leaf_tris, void *scratch,
+                          size_t scratch_bytes, cudaStream_t st, int *launches) {
+    if (n <= 0) return cudaSuccess;
+    LbvhScratch l = lbvh_layout(scratch, n);
+    if (l.used > scratch_bytes) return cudaErrorMemoryAllocation;
+    const int bs = 256;
+    k_bvh_leaves<<<blocks_for(n, bs), bs, 0, st>>>(l.vals2, vtx, tri, n, leaf_tris, l.leaf_boxes);
+    *launches += 1;
+    if (n > 1) {
+        cudaMemsetAsync(l.flags, 0, sizeof(int) * n, st);
+        k_bvh_refit<<<blocks_for(n, bs), bs, 0, st>>>(n, l.parent_leaf, l.parent_internal, l.children, l.leaf_boxes,
+                                                       l.node_boxes, l.flags, nodes);
+        *launches += 1;
+    }
+    return cudaGetLastError();
 }
+
+size_t dr_lbvh_scratch_bytes(int n) { return lbvh_layout(nullptr, n).used; }
 
 __global__ void k_trace_rays(DevScene s, const float *rays, long long n, int *tri, float *t) {
     long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;

@@ -30,6 +30,10 @@ struct StageTimer {
 cudaError_t dr_build_lbvh(const float *vtx, const int4 *tri, int n, float3 lo, float3 hi, float4 *nodes,
                           float4 *leaf_tris, void *scratch, size_t scratch_bytes, cudaStream_t st, int *launches);
 size_t dr_lbvh_scratch_bytes(int n);
+// Recomputes the boxes of an LBVH built by dr_build_lbvh over the same
+// triangles (same scratch, kept since the build) for new vertex positions.
+cudaError_t dr_refit_lbvh(const float *vtx, const int4 *tri, int n, float4 *nodes, float4 *leaf_tris, void *scratch,
+                          size_t scratch_bytes, cudaStream_t st, int *launches);
 
 cudaError_t dr_launch_trace(const DevScene &s, const float *rays, long long n, int *tri, float *t, cudaStream_t st,
                             int *launches);

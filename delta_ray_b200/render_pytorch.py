@@ -68,6 +68,16 @@ class Scene:
         if self.grad_total != self.sd.grad_total:
             raise RuntimeError("gradient layout mismatch between library and binding")
 
+    def update(self, cam, materials, shapes, lights, ltc_table=None):
+        """New parameters for the same meshes (dr_scene_update): positions,
+        normals, materials, lights and camera may change; the edge topology
+        and the LBVH's tree are kept when the triangle indices are unchanged."""
+        sd = _abi.SceneDesc.from_scene(cam, materials, shapes, lights, self.device, ltc_table)
+        with torch.cuda.device(self.device_index):
+            torch.cuda.current_stream().synchronize()
+            _lib.check(_lib.lib().dr_scene_update(self.handle, C.byref(sd.desc)))
+        self.sd, self.materials, self.shapes = sd, materials, shapes
+
     def _stream(self):
         return C.c_void_p(torch.cuda.current_stream(self.device).cuda_stream)
 
