@@ -29,7 +29,7 @@ class dr_material_desc(C.Structure):
                 ("specular", c_float_p), ("specular_w", C.c_int), ("specular_h", C.c_int),
                 ("roughness", c_float_p), ("roughness_w", C.c_int), ("roughness_h", C.c_int),
                 ("diffuse_uv_scale", c_float_p), ("specular_uv_scale", c_float_p),
-                ("roughness_uv_scale", c_float_p), ("two_sided", C.c_int)]
+                ("roughness_uv_scale", c_float_p), ("two_sided", C.c_int), ("microfacet", C.c_int)]
 
 
 class dr_shape_desc(C.Structure):
@@ -47,7 +47,7 @@ class dr_scene_desc(C.Structure):
                 ("materials", C.POINTER(dr_material_desc)), ("num_materials", C.c_int),
                 ("shapes", C.POINTER(dr_shape_desc)), ("num_shapes", C.c_int),
                 ("lights", C.POINTER(dr_light_desc)), ("num_lights", C.c_int),
-                ("ltc_table", c_float_p)]
+                ("ltc_table", c_float_p), ("ltc_table_ggx", c_float_p)]
 
 
 class dr_render_desc(C.Structure):
@@ -66,6 +66,7 @@ class dr_grad_layout(C.Structure):
 DR_DP_REFERENCE_LAST = 0
 DR_DP_SUM = 1
 DR_FLAG_FULL_PIXEL_JITTER = 1
+DR_FLAG_DETACHED_PDF = 2
 
 
 def render_desc(width, height, spp, max_bounces, seed, primary_edge_samples=0,
@@ -110,7 +111,7 @@ class SceneDesc:
 
     @classmethod
     def from_scene(cls, cam, materials, shapes, lights, device=torch.device("cpu"),
-                   ltc_table=None):
+                   ltc_table=None, ltc_table_ggx=None):
         self = cls()
         f32 = torch.float32
         d = self.desc
@@ -139,6 +140,7 @@ class SceneDesc:
             md.specular_uv_scale = self._ptr(m["specular_uv_scale"], f32, device)
             md.roughness_uv_scale = self._ptr(m["roughness_uv_scale"], f32, device)
             md.two_sided = int(bool(m["two_sided"]))
+            md.microfacet = int(m.get("microfacet", 0))
         shps = (dr_shape_desc * max(1, len(shapes)))()
         for i, s in enumerate(shapes):
             sd = shps[i]
@@ -162,6 +164,7 @@ class SceneDesc:
         d.shapes, d.num_shapes = shps, len(shapes)
         d.lights, d.num_lights = lts, len(lights)
         d.ltc_table = self._ptr(ltc_table, f32, device) if ltc_table is not None else None
+        d.ltc_table_ggx = self._ptr(ltc_table_ggx, f32, device) if ltc_table_ggx is not None else None
         # flat gradient layout (include/delta_ray_b200.h)
         sizes = [("camera", 0, 64)]
         for i, m in enumerate(materials):
@@ -218,7 +221,7 @@ def scene_dicts(cam, materials, shapes, lights):
     mats = [dict(diffuse=m.diffuse_reflectance, specular=m.specular_reflectance,
                  roughness=m.roughness, diffuse_uv_scale=m.diffuse_uv_scale,
                  specular_uv_scale=m.specular_uv_scale, roughness_uv_scale=m.roughness_uv_scale,
-                 two_sided=m.two_sided) for m in materials]
+                 two_sided=m.two_sided, microfacet=getattr(m, "microfacet", 0)) for m in materials]
     shps = [dict(vertices=s.vertices, indices=s.indices, uvs=s.uvs, normals=s.normals,
                  material_id=s.mat_id) for s in shapes]
     lts = [dict(shape_id=l.shape_id, intensity=l.intensity) for l in lights]

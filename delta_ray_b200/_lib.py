@@ -49,7 +49,7 @@ def lib():
                  "dr_render_forward", "dr_render_backward", "dr_scene_last_launch_count", "dr_trace_rays",
                  "dr_scene_set_profiling", "dr_scene_last_timings", "dr_scene_last_counts"):
         getattr(L, name).restype = C.c_int
-    if L.dr_abi_version() != 1:
+    if L.dr_abi_version() != 2:
         raise ImportError("libdr_b200.so has an unexpected ABI version")
     _lib = L
     return L

@@ -132,6 +132,38 @@ DEV void d_smith_g1(const Frame &f, float3 n, float3 m, float3 v, float rough, f
     dn += d_c * v;
 }
 
+// adjoint of ggx_g1(n, m, v, A): G1 = 2 / (1 + S), S = sqrt(1 + A t2),
+// t2 = 1 / c^2 - 1, c = v.n
+DEV void d_ggx_g1(float3 n, float3 m, float3 v, float A, float d_out, float3 &dn, float3 &dv, float &dA) {
+    float c = dot(v, n);
+    if (dot(v, m) * c <= 0.f) return;
+    float q = 1.f / (c * c) - 1.f;
+    float t2 = fmaxf(q, 0.f);
+    float S = sqrtf(1.f + A * t2);
+    float dS = d_out * (-2.f / ((1.f + S) * (1.f + S)));
+    float d_t2 = dS * A / (2.f * S);
+    dA += dS * t2 / (2.f * S);
+    if (q > 0.f) {
+        float d_c = d_t2 * (-2.f / (c * c * c));
+        dv += d_c * n;
+        dn += d_c * v;
+    }
+}
+
+// partial derivatives of ggx_D(z, A) = A / (pi k^2), k = z^2 (A - 1) + 1
+DEV void ggx_D_partials(float z, float A, float &dDdz, float &dDdA) {
+    float k = z * z * (A - 1.f) + 1.f;
+    float ik3 = 1.f / (DR_PI * k * k * k);
+    dDdz = -4.f * A * z * (A - 1.f) * ik3;
+    dDdA = (k - 2.f * A * z * z) * ik3;
+}
+
+// d A / d roughness of ggx_A (A = r^4 above the clamp)
+DEV float ggx_dA_drough(float rough) {
+    float r2 = rough * rough;
+    return r2 > 1e-4f ? 4.f * r2 * rough : 0.f;
+}
+
 // adjoint of bsdf (material.h:257-351); accumulates into sg and the material gradient
 template <class G>
 DEV void d_bsdf(const DevScene &s, int mi, const SurfacePoint &sp, float3 wi, float3 wo, float3 d_out, G &g,
@@ -154,12 +186,23 @@ DEV void d_bsdf(const DevScene &s, int mi, const SurfacePoint &sp, float3 wi, fl
         float3 h = normalize(hr);
         float3 hl = to_local(sp.f, h);
         if (hl.z > 0.f) {
-            bool e_pos = 2.f / rough > 0.f;
-            float e = roughness_to_phong(rough);
-            float pz = fmaxf(hl.z, 0.f);
-            float P = powf(pz, e);
-            float D = P * (e + 2.f) * DR_INV_2PI;
-            float G1i = smith_g1(sp.f, n, h, wi, rough), G1o = smith_g1(sp.f, n, h, wo, rough);
+            const bool ggx = m.model == DR_MICROFACET_GGX;
+            bool e_pos = false;
+            float e = 0.f, pz = 0.f, P = 0.f, A = 0.f, D, G1i, G1o;
+            if (ggx) {
+                A = ggx_A(rough);
+                D = ggx_D(hl.z, A);
+                G1i = ggx_g1(n, h, wi, A);
+                G1o = ggx_g1(n, h, wo, A);
+            } else {
+                e_pos = 2.f / rough > 0.f;
+                e = roughness_to_phong(rough);
+                pz = fmaxf(hl.z, 0.f);
+                P = powf(pz, e);
+                D = P * (e + 2.f) * DR_INV_2PI;
+                G1i = smith_g1(sp.f, n, h, wi, rough);
+                G1o = smith_g1(sp.f, n, h, wo, rough);
+            }
             float Gt = G1i * G1o;
             float cd = dot(h, wo);
             float om = 1.f - cd;
@@ -178,16 +221,27 @@ DEV void d_bsdf(const DevScene &s, int mi, const SurfacePoint &sp, float3 wi, fl
             float d_cd = -d_om;
             float3 dh = d_cd * wo;
             sg.dwo += d_cd * h;
-            d_smith_g1(sp.f, n, h, wi, rough, d_G * G1o, sg.df, dn, dh, sg.dwi, dr);
-            d_smith_g1(sp.f, n, h, wo, rough, d_G * G1i, sg.df, dn, dh, sg.dwo, dr);
-            float d_P = d_D * (e + 2.f) * DR_INV_2PI;
-            float d_e = d_D * P * DR_INV_2PI;
-            float d_pz = d_P * e * powf(pz, e - 1.f);
-            d_e += d_P * P * logf(fmaxf(pz, 1e-6f));
-            if (e_pos) dr += d_e * (-2.f / (rough * rough));
+            float d_z;
+            if (ggx) {
+                float dA = 0.f, dDdz, dDdA;
+                d_ggx_g1(n, h, wi, A, d_G * G1o, dn, sg.dwi, dA);
+                d_ggx_g1(n, h, wo, A, d_G * G1i, dn, sg.dwo, dA);
+                ggx_D_partials(hl.z, A, dDdz, dDdA);
+                d_z = d_D * dDdz;
+                dA += d_D * dDdA;
+                dr += dA * ggx_dA_drough(rough);
+            } else {
+                d_smith_g1(sp.f, n, h, wi, rough, d_G * G1o, sg.df, dn, dh, sg.dwi, dr);
+                d_smith_g1(sp.f, n, h, wo, rough, d_G * G1i, sg.df, dn, dh, sg.dwo, dr);
+                float d_P = d_D * (e + 2.f) * DR_INV_2PI;
+                float d_e = d_D * P * DR_INV_2PI;
+                d_z = d_P * e * powf(pz, e - 1.f);
+                d_e += d_P * P * logf(fmaxf(pz, 1e-6f));
+                if (e_pos) dr += d_e * (-2.f / (rough * rough));
+            }
             sg.dwi += (4.f * d_denom) * n;
             dn += (4.f * d_denom) * wi;
-            d_to_local(sp.f, h, f3(0.f, 0.f, d_pz), sg.df, dh);
+            d_to_local(sp.f, h, f3(0.f, 0.f, d_z), sg.df, dh);
             float3 dhr = d_normalize(hr, dh);
             sg.dwi += dhr;
             sg.dwo += dhr;
@@ -227,23 +281,37 @@ DEV void d_bsdf_pdf(const DevScene &s, int mi, const SurfacePoint &sp, float3 wi
         float3 hl = to_local(sp.f, h);
         if (hl.z > 0.f) {
             float rough = get_rough(s, m, sp.uv);
-            bool e_pos = 2.f / rough > 0.f;
-            float e = roughness_to_phong(rough);
-            float P = powf(hl.z, e);
-            float D = P * (e + 2.f) * DR_INV_2PI;
             float dwh = dot(wo, h);
             float Q = 4.f * fabsf(dwh);
-            d_spmf += d_out * D / Q;
-            float d_D = d_out * spmf / Q;
-            float d_Q = -d_out * spmf * D / (Q * Q);
+            float d_hlz, d_Q;
+            if (m.model == DR_MICROFACET_GGX) {
+                // spdf = spmf D z / Q
+                float A = ggx_A(rough);
+                float D = ggx_D(hl.z, A);
+                d_spmf += d_out * D * hl.z / Q;
+                float d_D = d_out * spmf * hl.z / Q;
+                d_Q = -d_out * spmf * D * hl.z / (Q * Q);
+                float dDdz, dDdA;
+                ggx_D_partials(hl.z, A, dDdz, dDdA);
+                d_hlz = d_out * spmf * D / Q + d_D * dDdz;
+                dr += d_D * dDdA * ggx_dA_drough(rough);
+            } else {
+                bool e_pos = 2.f / rough > 0.f;
+                float e = roughness_to_phong(rough);
+                float P = powf(hl.z, e);
+                float D = P * (e + 2.f) * DR_INV_2PI;
+                d_spmf += d_out * D / Q;
+                float d_D = d_out * spmf / Q;
+                d_Q = -d_out * spmf * D / (Q * Q);
+                float d_P = d_D * (e + 2.f) * DR_INV_2PI;
+                float d_e = d_D * P * DR_INV_2PI;
+                d_hlz = d_P * e * powf(hl.z, e - 1.f);
+                d_e += d_P * P * logf(fmaxf(hl.z, 1e-6f));
+                if (e_pos) dr += d_e * (-2.f / (rough * rough));
+            }
             float d_dwh = 4.f * d_Q * (dwh >= 0.f ? 1.f : -1.f);
             sg.dwo += d_dwh * h;
             float3 dh = d_dwh * wo;
-            float d_P = d_D * (e + 2.f) * DR_INV_2PI;
-            float d_e = d_D * P * DR_INV_2PI;
-            float d_hlz = d_P * e * powf(hl.z, e - 1.f);
-            d_e += d_P * P * logf(fmaxf(hl.z, 1e-6f));
-            if (e_pos) dr += d_e * (-2.f / (rough * rough));
             d_to_local(sp.f, h, f3(0.f, 0.f, d_hlz), sg.df, dh);
             float3 dhr = d_normalize(hr, dh);
             sg.dwi += dhr;

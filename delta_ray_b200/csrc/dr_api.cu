@@ -119,20 +119,21 @@ void give_back_queues(int device, std::unique_ptr<BackwardQueues> q) {
     if (!slot || slot->cap_items < q->cap_items) slot = std::move(q);
 }
 
-// Device copies of LTC tables, one per device, shared by the scenes that use
-// the same table.
+// Device copies of LTC tables, one per device and lobe (Blinn-Phong, GGX),
+// shared by the scenes that use the same table.
 struct LtcCache {
     std::vector<float> host;
     std::shared_ptr<DevBuf> dev;
 };
-std::map<int, LtcCache> &ltc_cache() {
-    static auto *c = new std::map<int, LtcCache>();
+std::map<std::pair<int, int>, LtcCache> &ltc_cache() {
+    static auto *c = new std::map<std::pair<int, int>, LtcCache>();
     return *c;
 }
 
-std::shared_ptr<DevBuf> device_ltc(int device, const std::vector<float> &table) {
+// slot: 0 Blinn-Phong table, 1 GGX table
+std::shared_ptr<DevBuf> device_ltc(int device, int slot, const std::vector<float> &table) {
     std::lock_guard<std::mutex> lk(cache_mutex());
-    LtcCache &c = ltc_cache()[device];
+    LtcCache &c = ltc_cache()[std::make_pair(device, slot)];
     if (c.dev && c.host == table) return c.dev;
     std::shared_ptr<DevBuf> d(new DevBuf());
     d->upload(table);
@@ -151,7 +152,7 @@ struct dr_scene {
     DevBuf vtx, nrm, uv, tri, tri_local, bvh_nodes, bvh_tris, shapes, mats, texels, lights, light_sel_cdf,
         light_sel_func, light_tri_cdf, light_tri_func, prim_edges, prim_cdf, prim_func, sil_nodes, sil_edges,
         nrm_nodes, nrm_edges, status, bvh_scratch;
-    std::shared_ptr<DevBuf> ltc;
+    std::shared_ptr<DevBuf> ltc, ltc_ggx;
     std::unique_ptr<BackwardQueues> queues;  // taken at the first backward call
     DevScene ds;
     StageTimer timer;
@@ -197,7 +198,8 @@ void upload_scene(dr_scene *sc, cudaStream_t st, bool refit = false) {
     sc->sil_edges.upload(h.sil_edges);
     sc->nrm_nodes.upload(h.nrm_nodes);
     sc->nrm_edges.upload(h.nrm_edges);
-    sc->ltc = device_ltc(sc->device, h.ltc);
+    sc->ltc = device_ltc(sc->device, 0, h.ltc);
+    sc->ltc_ggx = device_ltc(sc->device, 1, h.ltc_ggx);
     sc->status.reserve(sizeof(int) * 4);
     // device LBVH
     int n = sc->num_tris;
@@ -247,6 +249,7 @@ void upload_scene(dr_scene *sc, cudaStream_t st, bool refit = false) {
     ptr.nrm_nodes = sc->nrm_nodes.as<DevEdgeNode>();
     ptr.nrm_edges = sc->nrm_edges.as<DevEdge>();
     ptr.ltc = sc->ltc->as<float>();
+    ptr.ltc_ggx = sc->ltc_ggx->as<float>();
     fill_devscene(sc->ds, h, f, ptr);
 }
 
@@ -285,6 +288,7 @@ void collect_timings(dr_scene *sc, cudaStream_t st) {
 DevScene call_scene(const dr_scene *sc, const dr_render_desc *rd) {
     DevScene ds = sc->ds;
     ds.full_pixel_jitter = (rd->flags & DR_FLAG_FULL_PIXEL_JITTER) != 0;
+    ds.detached_pdf = (rd->flags & DR_FLAG_DETACHED_PDF) != 0;
     return ds;
 }
 
@@ -299,7 +303,8 @@ void check_render_desc(const dr_scene *sc, const dr_render_desc *rd) {
         throw DrError(DR_ERR_INVALID_ARGUMENT, "width * height * spp must be below 2^31 per call");
     for (int i = 0; i < 7; i++)
         if (rd->reserved[i] != 0) throw DrError(DR_ERR_INVALID_ARGUMENT, "reserved fields must be zero");
-    if (rd->flags & ~(int)DR_FLAG_FULL_PIXEL_JITTER) throw DrError(DR_ERR_INVALID_ARGUMENT, "unknown render flags");
+    if (rd->flags & ~(int)(DR_FLAG_FULL_PIXEL_JITTER | DR_FLAG_DETACHED_PDF))
+        throw DrError(DR_ERR_INVALID_ARGUMENT, "unknown render flags");
     if (rd->max_bounces > 64) throw DrError(DR_ERR_NOT_SUPPORTED, "max_bounces above 64");
     if (sc->ds.num_lights == 0) throw DrError(DR_ERR_INVALID_ARGUMENT, "scene has no lights");
 }

@@ -268,7 +268,7 @@ DEV float3 backward_pixel_sample(const DevScene &s, int x, int y, int W, int H, 
         SpGrad gb;
         gb.zero();
         d_bsdf(s, mi, csp, cwi, wo, d_f, g, gb);
-        d_bsdf_pdf(s, mi, csp, cwi, wo, d_pdf, g, gb);
+        if (!s.detached_pdf) d_bsdf_pdf(s, mi, csp, cwi, wo, d_pdf, g, gb);
         if (first) {
             frame_add(g0.df, gb.df);
             g0.duv.x += gb.duv.x;

@@ -153,7 +153,8 @@ DEV float3 node_corner(const DevEdgeNode &n, int i) {
     return f3((i & 1) ? n.hi[0] : n.lo[0], (i & 2) ? n.hi[1] : n.lo[1], (i & 4) ? n.hi[2] : n.lo[2]);
 }
 
-DEV_NOINLINE float bsdf_bound(const DevEdgeNode &node, float3 wi, const SurfacePoint &sp, float dl, float sl, float rough) {
+DEV_NOINLINE float bsdf_bound(const DevEdgeNode &node, float3 wi, const SurfacePoint &sp, float dl, float sl, float rough,
+                              int model) {
     float cos_max = 0.f;
     for (int i = 0; i < 8; i++)
         if (dot(sp.f.n, node_corner(node, i) - sp.p) > 0.f) {
@@ -191,8 +192,13 @@ DEV_NOINLINE float bsdf_bound(const DevEdgeNode &node, float3 wi, const SurfaceP
         else if (chmax < cth_min) chmax = cth_min;
         float shmax = sqrtf(fmaxf(1.f - chmax * chmax, 0.f));
         float hdn = fminf(fabsf(ln.x * shmax * cphi) + ln.z * chmax, 1.f);
-        float e = roughness_to_phong(rough);
-        maxp = powf(hdn, e) * (e + 2.f) / float(2 * 3.14159265358979323846);
+        if (model == DR_MICROFACET_GGX) {
+            // the GGX D grows with n.h (A <= 1): its bound is the value at the bound of n.h
+            maxp = ggx_D(hdn, ggx_A(rough));
+        } else {
+            float e = roughness_to_phong(rough);
+            maxp = powf(hdn, e) * (e + 2.f) / float(2 * 3.14159265358979323846);
+        }
     }
     return cos_max * (dl / DR_PI + sl * maxp);
 }
@@ -230,7 +236,8 @@ DEV bool node_inside(const DevEdgeNode &n, float3 p) {
 #define DR_EDGE_STACK 64
 template <bool CONE, class Emit>
 DEV bool traverse_mode(const DevScene &s, const DevEdgeNode *nodes, const DevEdge *edges, bool dir_bounds, float3 wi,
-                       const SurfacePoint &sp, float dl, float sl, float rough, const ConeSpec &cone, float root_bb,
+                       const SurfacePoint &sp, float dl, float sl, float rough, int model, const ConeSpec &cone,
+                       float root_bb,
                        float pmf, Rng &rng, Emit &emit) {
     struct Item { int node; float bb, cpmf, apmf; };
     Item st[DR_EDGE_STACK];
@@ -258,8 +265,8 @@ DEV bool traverse_mode(const DevScene &s, const DevEdgeNode *nodes, const DevEdg
             lcs = contains_silhouette(L, sp.p);
             rcs = contains_silhouette(R, sp.p);
         }
-        float lbb = lcs ? bsdf_bound(L, wi, sp, dl, sl, rough) : 0.f;
-        float rbb = rcs ? bsdf_bound(R, wi, sp, dl, sl, rough) : 0.f;
+        float lbb = lcs ? bsdf_bound(L, wi, sp, dl, sl, rough, model) : 0.f;
+        float rbb = rcs ? bsdf_bound(R, wi, sp, dl, sl, rough, model) : 0.f;
         float il = lcs ? node_importance(L, lbb, sp.p) : 0.f;
         float ir = rcs ? node_importance(R, rbb, sp.p) : 0.f;
         if (il + ir <= 1e-10f) continue;
@@ -333,14 +340,15 @@ DEV bool traverse_edges(const DevScene &s, float3 wi, int stri, const SurfacePoi
     const DevMaterial &m = s.mats[material_of_tri(s, stri)];
     float dl = luminance(get_kd(s, m, sp.uv)), sl = luminance(get_ks(s, m, sp.uv));
     float rough = get_rough(s, m, sp.uv);
-    float b = bsdf_bound(nodes[0], wi, sp, dl, sl, rough);
+    float b = bsdf_bound(nodes[0], wi, sp, dl, sl, rough, m.model);
     auto em = [&](int ei, float w) { emit(tree, ei, w); };
-    bool ok = traverse_mode<true>(s, nodes, edges, tree == 1, wi, sp, dl, sl, rough, cone, b, pmf, rng, em);
-    ok &= traverse_mode<false>(s, nodes, edges, tree == 1, wi, sp, dl, sl, rough, cone, b, pmf, rng, em);
+    bool ok = traverse_mode<true>(s, nodes, edges, tree == 1, wi, sp, dl, sl, rough, m.model, cone, b, pmf, rng, em);
+    ok &= traverse_mode<false>(s, nodes, edges, tree == 1, wi, sp, dl, sl, rough, m.model, cone, b, pmf, rng, em);
     return ok;
 }
 
 // LTC matrix lookup (material.h:464-476): nearest entry of the 128x128 table
+// of the material's lobe
 DEV M3 ltc_matrix(const DevScene &s, int mi, const SurfacePoint &sp, float3 wi) {
     float r = get_rough(s, s.mats[mi], sp.uv);
     float ct = dot(wi, sp.f.n);
@@ -350,7 +358,7 @@ DEV M3 ltc_matrix(const DevScene &s, int mi, const SurfacePoint &sp, float3 wi) 
     rid = rid < 0 ? 0 : (rid > 127 ? 127 : rid);
     tid = tid < 0 ? 0 : (tid > 127 ? 127 : tid);
     M3 m;
-    const float *p = s.ltc + 9 * (rid + tid * 128);
+    const float *p = (s.mats[mi].model == DR_MICROFACET_GGX ? s.ltc_ggx : s.ltc) + 9 * (rid + tid * 128);
     for (int i = 0; i < 9; i++) m.m[i] = dr_ldg(p + i);
     return m;
 }

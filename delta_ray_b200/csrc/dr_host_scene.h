@@ -258,7 +258,7 @@ struct HostScene {
     HDist prim_dist;
     std::vector<DevEdgeNode> sil_nodes, nrm_nodes;
     std::vector<DevEdge> sil_edges, nrm_edges;
-    std::vector<float> ltc;
+    std::vector<float> ltc, ltc_ggx;
     size_t grad_total = 0;
     // flat gradient layout (include/delta_ray_b200.h)
     std::vector<size_t> layout_mat, layout_vtx, layout_nrm, layout_light;
@@ -518,6 +518,9 @@ template <class Fetch> void load_desc(HostScene &h, const dr_scene_desc *d, Fetc
         uvs(m.specular_uv_scale, dm.uv_ks, "specular_uv_scale");
         uvs(m.roughness_uv_scale, dm.uv_r, "roughness_uv_scale");
         dm.two_sided = m.two_sided != 0;
+        if (m.microfacet != DR_MICROFACET_BLINN_PHONG && m.microfacet != DR_MICROFACET_GGX)
+            throw SceneError("unknown microfacet model");
+        dm.model = m.microfacet;
         {
             // can this material's BSDF sample be "specular" (material.h:410)?
             auto range = [&](int tex, int w, int hh, int ch, const float *cval, float &lo, float &hi) {
@@ -583,6 +586,7 @@ template <class Fetch> void load_desc(HostScene &h, const dr_scene_desc *d, Fetc
     h.grad_total = g;
     if (g > (size_t)0x7fffffff) throw SceneError("scene too large for 32-bit gradient offsets");
     h.ltc = d->ltc_table ? fetch(d->ltc_table, 128 * 128 * 9, "ltc_table") : default_ltc();
+    h.ltc_ggx = d->ltc_table_ggx ? fetch(d->ltc_table_ggx, 128 * 128 * 9, "ltc_table_ggx") : default_ltc();
 }
 
 
@@ -658,7 +662,7 @@ struct ScenePtrs {
     const DevEdge *sil_edges;
     const DevEdgeNode *nrm_nodes;
     const DevEdge *nrm_edges;
-    const float *ltc;
+    const float *ltc, *ltc_ggx;
 };
 
 inline void fill_devscene(DevScene &ds, const HostScene &h, const FlatScene &f, const ScenePtrs &p) {
@@ -704,7 +708,9 @@ inline void fill_devscene(DevScene &ds, const HostScene &h, const FlatScene &f, 
     ds.nrm_edges = p.nrm_edges;
     ds.num_nrm_nodes = (int)h.nrm_nodes.size();
     ds.ltc = p.ltc;
+    ds.ltc_ggx = p.ltc_ggx;
     ds.full_pixel_jitter = 0;  // set per render call
+    ds.detached_pdf = 0;
     ds.grad_total = (int)h.grad_total;
 }
 

@@ -7,6 +7,7 @@
 // (geomID, primID) pairs (scene.cpp:100-135).
 #pragma once
 
+#include "../../include/delta_ray_b200.h"
 #include "dr_common.cuh"
 
 struct DevCamera {
@@ -21,6 +22,7 @@ struct DevMaterial {
     int kd_w, kd_h, ks_w, ks_h, r_w, r_h;
     float uv_kd[2], uv_ks[2], uv_r[2];
     int two_sided;
+    int model;  // DR_MICROFACET_BLINN_PHONG or DR_MICROFACET_GGX
     int grad_kd, grad_ks, grad_r;  // offsets in the flat gradient
 };
 
@@ -92,11 +94,14 @@ struct DevScene {
     const DevEdgeNode *nrm_nodes;
     const DevEdge *nrm_edges;
     int num_nrm_nodes;
-    const float *ltc;  // 128*128 row-major 3x3
+    const float *ltc;      // 128*128 row-major 3x3, Blinn-Phong lobes
+    const float *ltc_ggx;  // the same for GGX lobes
     int grad_total;
     // per render call: sub-pixel offsets over the whole pixel (u) instead of
     // the reference's [0, 1/spp) (u / spp)
     int full_pixel_jitter;
+    // per render call: the backward pass holds the BSDF sampling pdf constant
+    int detached_pdf;
 };
 
 // --- accessors -------------------------------------------------------------

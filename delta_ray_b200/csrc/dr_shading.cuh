@@ -146,6 +146,24 @@ DEV float smith_g1(const Frame &f, float3 n, float3 m, float3 v, float rough) {
     return (3.535f * a + 2.181f * a2) / (1.0f + 2.276f * a + 2.577f * a2);
 }
 
+// GGX lobe (Walter et al. 2007, "Microfacet Models for Refraction through
+// Rough Surfaces"; no counterpart in the reference): alpha = max(r^2, 1e-4),
+// A = alpha^2, D(h) = A / (pi ((n.h)^2 (A - 1) + 1)^2), exact Smith G1.
+DEV float ggx_A(float rough) {
+    float a = fmaxf(rough * rough, 1e-4f);
+    return a * a;
+}
+DEV float ggx_D(float z, float A) {
+    float k = z * z * (A - 1.f) + 1.f;
+    return A / (DR_PI * k * k);
+}
+DEV float ggx_g1(float3 n, float3 m, float3 v, float A) {
+    float c = dot(v, n);
+    if (dot(v, m) * c <= 0.f) return 0.f;
+    float t2 = fmaxf(1.f / (c * c) - 1.f, 0.f);
+    return 2.f / (1.f + sqrtf(1.f + A * t2));
+}
+
 DEV float3 bsdf(const DevScene &s, int mi, const SurfacePoint &sp, float3 wi, float3 wo) {
     const DevMaterial &m = s.mats[mi];
     float3 n = sp.f.n;
@@ -159,9 +177,16 @@ DEV float3 bsdf(const DevScene &s, int mi, const SurfacePoint &sp, float3 wi, fl
         float3 h = normalize(wi + wo);
         float3 hl = to_local(sp.f, h);
         if (hl.z > 0.f) {
-            float e = roughness_to_phong(rough);
-            float D = powf(fmaxf(hl.z, 0.f), e) * (e + 2.f) / float(2 * 3.14159265358979323846);
-            float G = smith_g1(sp.f, n, h, wi, rough) * smith_g1(sp.f, n, h, wo, rough);
+            float D, G;
+            if (m.model == DR_MICROFACET_GGX) {
+                float A = ggx_A(rough);
+                D = ggx_D(hl.z, A);
+                G = ggx_g1(n, h, wi, A) * ggx_g1(n, h, wo, A);
+            } else {
+                float e = roughness_to_phong(rough);
+                D = powf(fmaxf(hl.z, 0.f), e) * (e + 2.f) / float(2 * 3.14159265358979323846);
+                G = smith_g1(sp.f, n, h, wi, rough) * smith_g1(sp.f, n, h, wo, rough);
+            }
             float cd = dot(h, wo);
             float fr = powf(fmaxf(1.f - cd, 0.f), 5.f);
             float3 F = f3(ks.x + (1.f - ks.x) * fr, ks.y + (1.f - ks.y) * fr, ks.z + (1.f - ks.z) * fr);
@@ -188,9 +213,15 @@ DEV float bsdf_pdf(const DevScene &s, int mi, const SurfacePoint &sp, float3 wi,
         float3 h = normalize(wi + wo);
         float3 hl = to_local(sp.f, h);
         if (hl.z > 0.f) {
-            float e = roughness_to_phong(get_rough(s, m, sp.uv));
-            float D = powf(hl.z, e) * (e + 2.f) / float(2 * 3.14159265358979323846);
-            spdf = spmf * D / (4.f * fabsf(dot(wo, h)));
+            if (m.model == DR_MICROFACET_GGX) {
+                // half vectors are drawn with density D(h) (n.h)
+                float D = ggx_D(hl.z, ggx_A(get_rough(s, m, sp.uv)));
+                spdf = spmf * D * hl.z / (4.f * fabsf(dot(wo, h)));
+            } else {
+                float e = roughness_to_phong(get_rough(s, m, sp.uv));
+                float D = powf(hl.z, e) * (e + 2.f) / float(2 * 3.14159265358979323846);
+                spdf = spmf * D / (4.f * fabsf(dot(wo, h)));
+            }
         }
     }
     return dpdf + spdf;
@@ -217,10 +248,15 @@ DEV float3 sample_bsdf_dir(const DevScene &s, int mi, const SurfacePoint &sp, fl
     }
     if (sw <= 0.f) return f3(0.f);
     float rough = get_rough(s, m, sp.uv);
-    float e = roughness_to_phong(rough);
     float phi = 2.f * DR_PI * bs.u1;
     float sphi = sinf(phi), cphi = cosf(phi);
-    float ct = powf(bs.u0, 1.0f / (e + 2.0f));
+    float ct;
+    if (m.model == DR_MICROFACET_GGX) {
+        float A = ggx_A(rough);
+        ct = sqrtf((1.f - bs.u0) / (1.f + (A - 1.f) * bs.u0));
+    } else {
+        ct = powf(bs.u0, 1.0f / (roughness_to_phong(rough) + 2.0f));
+    }
     float st = sqrtf(fmaxf(1.f - ct * ct, 0.f));
     float3 h = to_world(sp.f, f3(st * cphi, st * sphi, ct));
     specular = rough <= 0.01f;

@@ -1,6 +1,8 @@
 """Material description (mirrors the reference material.py:5-19).
 
-A material is Lambertian diffuse plus a Blinn-Phong specular lobe.  Each of
+A material is Lambertian diffuse plus a specular lobe: Blinn-Phong, as in the
+reference, or GGX (``microfacet="ggx"``; alpha = roughness^2, no counterpart in
+the reference).  Each of
 ``diffuse_reflectance`` ([3] or [h, w, 3]), ``specular_reflectance`` ([3] or
 [h, w, 3]) and ``roughness`` ([1] or [h, w, 1]) is either a constant or a
 texture looked up bilinearly with wrap-around.
@@ -21,7 +23,8 @@ def _f32(values):
 class Material:
     def __init__(self, diffuse_reflectance, specular_reflectance=None,
                  roughness=None, diffuse_uv_scale=None, specular_uv_scale=None,
-                 roughness_uv_scale=None, two_sided=False, exact_uv_scales=False):
+                 roughness_uv_scale=None, two_sided=False, exact_uv_scales=False,
+                 microfacet="blinn_phong"):
         if specular_reflectance is None:
             specular_reflectance = _f32([0.0, 0.0, 0.0])
         if roughness is None:
@@ -43,3 +46,7 @@ class Material:
             self.specular_uv_scale = diffuse_uv_scale
             self.roughness_uv_scale = diffuse_uv_scale
         self.two_sided = two_sided
+        models = {"blinn_phong": 0, "ggx": 1}
+        if microfacet not in models:
+            raise ValueError(f"microfacet must be one of {sorted(models)}")
+        self.microfacet = models[microfacet]

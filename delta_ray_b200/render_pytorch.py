@@ -29,34 +29,56 @@ class RenderOptions:
         (0 = spp * width * height, the reference's total).
     dp_mode: _abi.DR_DP_REFERENCE_LAST (the reference's behaviour) or
         _abi.DR_DP_SUM (sum every sampled edge's position derivative).
-    ltc_table: optional [128*128*9] float32 Blinn-Phong LTC table.
+    ltc_table, ltc_table_ggx: [128*128*9] float32 LTC tables for edge sampling
+        of Blinn-Phong and GGX lobes; "fitted" (default) selects the tables
+        fitted to this renderer's lobes (delta_ray_b200.ltc), None identity
+        matrices (the cosine lobe); pass the reference's table (ltc.inc) to
+        sample edges as the reference does.
     output_device: device of the returned image (default: the render device).
     device: CUDA device index to render on (default: current device).
     full_pixel_jitter: spread each pixel's samples over the whole pixel (a box
         filter, the image whose derivative the edge terms estimate) instead of
         the reference's [0, 1/spp) sub-pixel offsets (delta_ray.cpp:1236-1237).
+    detached_pdf: hold the BSDF sampling pdf constant in the backward pass
+        (unbiased gradients of roughness and lobe weights) instead of
+        differentiating it at a fixed sampled direction as the reference does.
     """
 
-    def __init__(self, primary_edge_samples=0, dp_mode=_abi.DR_DP_REFERENCE_LAST, ltc_table=None,
-                 output_device=None, device=None, full_pixel_jitter=False):
+    def __init__(self, primary_edge_samples=0, dp_mode=_abi.DR_DP_REFERENCE_LAST, ltc_table="fitted",
+                 output_device=None, device=None, full_pixel_jitter=False, ltc_table_ggx="fitted",
+                 detached_pdf=False):
         self.primary_edge_samples = int(primary_edge_samples)
         self.dp_mode = int(dp_mode)
-        self.flags = _abi.DR_FLAG_FULL_PIXEL_JITTER if full_pixel_jitter else 0
+        self.flags = (_abi.DR_FLAG_FULL_PIXEL_JITTER if full_pixel_jitter else 0) | \
+            (_abi.DR_FLAG_DETACHED_PDF if detached_pdf else 0)
         self.ltc_table = ltc_table
+        self.ltc_table_ggx = ltc_table_ggx
         self.output_device = output_device
         self.device = device
+
+
+def _table(t, model):
+    """An LTC table argument: "fitted" -> the committed fit of `model`, None -> None."""
+    if isinstance(t, str):
+        if t != "fitted":
+            raise ValueError(f"unknown LTC table {t!r}")
+        from . import ltc
+        return torch.from_numpy(ltc.default_table(model))
+    return t
 
 
 class Scene:
     """A device scene (dr_scene) built from unpacked RenderFunction arguments."""
 
-    def __init__(self, cam, materials, shapes, lights, device_index, ltc_table=None):
+    def __init__(self, cam, materials, shapes, lights, device_index, ltc_table="fitted", ltc_table_ggx="fitted"):
         L = _lib.lib()
+        ltc_table, ltc_table_ggx = _table(ltc_table, 0), _table(ltc_table_ggx, 1)
+        self._tables = (ltc_table, ltc_table_ggx)
         self.device_index = int(device_index)
         self.device = torch.device("cuda", self.device_index)
         self.materials = materials
         self.shapes = shapes
-        self.sd = _abi.SceneDesc.from_scene(cam, materials, shapes, lights, self.device, ltc_table)
+        self.sd = _abi.SceneDesc.from_scene(cam, materials, shapes, lights, self.device, ltc_table, ltc_table_ggx)
         handle = C.c_void_p()
         with torch.cuda.device(self.device_index):
             torch.cuda.current_stream().synchronize()
@@ -68,11 +90,15 @@ class Scene:
         if self.grad_total != self.sd.grad_total:
             raise RuntimeError("gradient layout mismatch between library and binding")
 
-    def update(self, cam, materials, shapes, lights, ltc_table=None):
+    def update(self, cam, materials, shapes, lights, ltc_table="keep", ltc_table_ggx="keep"):
         """New parameters for the same meshes (dr_scene_update): positions,
         normals, materials, lights and camera may change; the edge topology
-        and the LBVH's tree are kept when the triangle indices are unchanged."""
-        sd = _abi.SceneDesc.from_scene(cam, materials, shapes, lights, self.device, ltc_table)
+        and the LBVH's tree are kept when the triangle indices are unchanged.
+        The LTC tables stay those of the scene unless given."""
+        t0 = self._tables[0] if isinstance(ltc_table, str) and ltc_table == "keep" else _table(ltc_table, 0)
+        t1 = self._tables[1] if isinstance(ltc_table_ggx, str) and ltc_table_ggx == "keep" else _table(ltc_table_ggx, 1)
+        self._tables = (t0, t1)
+        sd = _abi.SceneDesc.from_scene(cam, materials, shapes, lights, self.device, t0, t1)
         with torch.cuda.device(self.device_index):
             torch.cuda.current_stream().synchronize()
             _lib.check(_lib.lib().dr_scene_update(self.handle, C.byref(sd.desc)))
@@ -172,8 +198,12 @@ def unpack_args(args):
                fisheye=bool(take()))
     mats = []
     for _ in range(nm):
-        mats.append(dict(diffuse=take(), specular=take(), roughness=take(), diffuse_uv_scale=take(),
-                         specular_uv_scale=take(), roughness_uv_scale=take(), two_sided=bool(take())))
+        m = dict(diffuse=take(), specular=take(), roughness=take(), diffuse_uv_scale=take(),
+                 specular_uv_scale=take(), roughness_uv_scale=take())
+        ts = take()
+        # a GGX material serializes its two_sided slot as (two_sided, microfacet)
+        m["two_sided"], m["microfacet"] = (bool(ts[0]), int(ts[1])) if isinstance(ts, tuple) else (bool(ts), 0)
+        mats.append(m)
     shps = []
     for _ in range(ns):
         shps.append(dict(vertices=take(), indices=take(), uvs=take(), normals=take(),
@@ -202,8 +232,9 @@ class RenderFunction(torch.autograd.Function):
                 float(torch.as_tensor(cam.fov_factor).reshape(-1)[0]), cam.aspect_ratio,
                 float(torch.as_tensor(cam.clip_near).reshape(-1)[0]), cam.fisheye]
         for m in materials:
+            model = getattr(m, "microfacet", 0)
             args += [m.diffuse_reflectance, m.specular_reflectance, m.roughness, m.diffuse_uv_scale,
-                     m.specular_uv_scale, m.roughness_uv_scale, m.two_sided]
+                     m.specular_uv_scale, m.roughness_uv_scale, (m.two_sided, model) if model else m.two_sided]
         for s in shapes:
             args += [s.vertices, s.indices, s.uvs, s.normals, s.mat_id]
         for l in lights:
@@ -216,7 +247,7 @@ class RenderFunction(torch.autograd.Function):
         cam, mats, shps, lts, (W, H), spp, B, opts = unpack_args(args)
         opts = opts or RenderOptions()
         dev = opts.device if opts.device is not None else torch.cuda.current_device()
-        scene = Scene(cam, mats, shps, lts, dev, opts.ltc_table)
+        scene = Scene(cam, mats, shps, lts, dev, opts.ltc_table, opts.ltc_table_ggx)
         img = scene.forward(W, H, spp, B, seed, opts)
         ctx.scene = scene
         ctx.render = (W, H, spp, B, int(seed), opts)

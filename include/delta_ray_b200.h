@@ -32,7 +32,7 @@
 extern "C" {
 #endif
 
-#define DR_ABI_VERSION 1
+#define DR_ABI_VERSION 2
 
 #if defined(__GNUC__)
 #define DR_API __attribute__((visibility("default")))
@@ -78,7 +78,13 @@ typedef struct {
     const float *specular_uv_scale;  /* [2] */
     const float *roughness_uv_scale; /* [2] */
     int two_sided;
+    /* Specular lobe: DR_MICROFACET_BLINN_PHONG (the reference's, material.h:
+     * 257-462) or DR_MICROFACET_GGX (Walter et al. 2007: alpha = roughness^2,
+     * exact Smith G1; no counterpart in the reference). */
+    int microfacet;
 } dr_material_desc;
+
+typedef enum { DR_MICROFACET_BLINN_PHONG = 0, DR_MICROFACET_GGX = 1 } dr_microfacet;
 
 /* Triangle mesh (shape.h:11-18). */
 typedef struct {
@@ -105,10 +111,13 @@ typedef struct {
     int num_shapes;
     const dr_light_desc *lights;
     int num_lights;
-    /* Optional Blinn-Phong LTC table, 128*128 row-major 3x3 float32 matrices
-     * indexed [roughness_bin + theta_bin * 128] (ltc.inc:2-4,
-     * material.h:464-476).  NULL selects the table built into the library. */
+    /* Optional LTC tables for edge sampling of Blinn-Phong and GGX lobes,
+     * 128*128 row-major 3x3 float32 matrices indexed [roughness_bin +
+     * theta_bin * 128] (ltc.inc:2-4, material.h:464-476).  NULL selects
+     * identity matrices (edges sampled by the cosine lobe, unbiased); the
+     * Python layer passes the fitted tables of delta_ray_b200/data. */
     const float *ltc_table;
+    const float *ltc_table_ggx;
 } dr_scene_desc;
 
 /* How the per-secondary-point edge position derivative is pushed back
@@ -122,8 +131,12 @@ typedef enum { DR_DP_REFERENCE_LAST = 0, DR_DP_SUM = 1 } dr_dp_mode;
  * offset is u / spp in each axis, as in the reference (delta_ray.cpp:1236-1237),
  * so that all samples of a pixel fall in its [0, 1/spp)^2 corner: the image is
  * then nearly point-sampled, while the primary-edge gradient is the derivative
- * of the box-filtered image. */
-typedef enum { DR_FLAG_FULL_PIXEL_JITTER = 1 } dr_render_flags;
+ * of the box-filtered image.  DR_FLAG_DETACHED_PDF holds the BSDF sampling
+ * pdf constant in the backward pass.  The reference differentiates it while
+ * keeping the sampled direction fixed (pathtrace.h:248-253), which biases the
+ * gradient of every parameter that shapes the sampling (roughness, the lobe
+ * weights) by -E[contribution * d log pdf]; held constant it is unbiased. */
+typedef enum { DR_FLAG_FULL_PIXEL_JITTER = 1, DR_FLAG_DETACHED_PDF = 2 } dr_render_flags;
 
 typedef struct {
     int width;

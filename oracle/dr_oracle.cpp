@@ -408,6 +408,7 @@ struct Material {
     Tex diffuse, specular, roughness;
     float uv_d[2], uv_s[2], uv_r[2];
     bool two_sided;
+    int model = 0;  // DR_MICROFACET_BLINN_PHONG or DR_MICROFACET_GGX
 };
 struct Shape {
     const float *v; int nv;
@@ -480,6 +481,7 @@ struct EdgeTree { std::vector<EdgeNode> nodes; std::vector<Edge> edges; };
 
 struct Scene {
     Camera cam;
+    bool detached_pdf = false;
     std::vector<Shape> shapes;
     std::vector<Material> mats;
     std::vector<Light> lights;
@@ -492,7 +494,7 @@ struct Scene {
     Dist1D primary_dist;
     EdgeTree sil_tree, nrm_tree;
     drshim::Scene bvh;
-    const float *ltc = nullptr;
+    const float *ltc = nullptr, *ltc_ggx = nullptr;
     // Sort key of each shape in the edge map.  The reference keys its edge map
     // by Shape* (scene.cpp:54-79), i.e. by heap address, so its edge order can
     // differ from the shape order; tests pass the order it used.
@@ -849,7 +851,18 @@ inline MatRec *push_mat(std::vector<MatRec> *recs, int mat) {
     return &recs->back();
 }
 
-// Lambert + Blinn-Phong BSDF times cosine (material.h:257-351)
+// GGX lobe (Walter et al. 2007; no counterpart in the reference):
+// alpha = max(r^2, 1e-4), A = alpha^2, D = A / (pi ((n.h)^2 (A - 1) + 1)^2).
+template <typename T> T ggx_A(const T &rough) {
+    T a = max(rough * rough, 1e-4f);
+    return a * a;
+}
+template <typename T> T ggx_D(const T &z, const T &A) {
+    T k = z * z * (A - 1.f) + 1.f;
+    return A / (kPi * k * k);
+}
+
+// Lambert + Blinn-Phong (or GGX) BSDF times cosine (material.h:257-351)
 template <typename T>
 V3<T> bsdf(const Scene &sc, int mi, const SPoint<T> &sp, const V3<T> &wi, const V3<T> &wo, std::vector<MatRec> *recs) {
     const Material &mat = sc.mats[mi];
@@ -866,7 +879,21 @@ V3<T> bsdf(const Scene &sc, int mi, const SPoint<T> &sp, const V3<T> &wi, const 
     if (sum(ks) > T(0.f) && dot(wi, n) > T(0.f)) {
         V3<T> m = normalize(wi + wo);
         V3<T> ml = to_local(sp.f, m);
-        if (ml.z > T(0.f)) {
+        if (ml.z > T(0.f) && mat.model == DR_MICROFACET_GGX) {
+            T A = ggx_A(rough);
+            T D = ggx_D(ml.z, A);
+            auto G1 = [&](const V3<T> &v) -> T {  // exact Smith G1
+                T c = dot(v, n);
+                if (dot(v, m) * c <= T(0.f)) return T(0.f);
+                T t2 = max(1.f / (c * c) - 1.f, 0.f);
+                return 2.f / (1.f + sqrt(1.f + A * t2));
+            };
+            T G = G1(wi) * G1(wo);
+            T cd = dot(m, wo);
+            T fr = pow(max(1.f - cd, 0.f), 5.f);
+            V3<T> F{ks.x + (1.f - ks.x) * fr, ks.y + (1.f - ks.y) * fr, ks.z + (1.f - ks.z) * fr};
+            spec = F * D * G / (4.f * dot(wi, n));
+        } else if (ml.z > T(0.f)) {
             T e = roughness_to_phong(rough);
             T D = pow(max(ml.z, 0.f), e) * (e + 2.f) / float(2 * M_PI);
             auto proj_rough = [&](const V3<T> &v) -> T {
@@ -962,10 +989,16 @@ std::pair<V3<T>, bool> sample_bsdf_dir(const Scene &sc, int mi, const SPoint<T> 
     }
     if (sw <= T(0.f)) return {zero, false};
     T rough = get_roughness(mat, sp.uv, r);
-    T e = roughness_to_phong(rough);
     float phi = 2.f * kPi * bs.uv.y;
     float sphi = std::sin(phi), cphi = std::cos(phi);
-    T ct = pow(bs.uv.x, 1.0f / (e + 2.0f));
+    T ct;
+    if (mat.model == DR_MICROFACET_GGX) {
+        T A = ggx_A(rough);
+        ct = sqrt((1.f - bs.uv.x) / (1.f + (A - 1.f) * bs.uv.x));
+    } else {
+        T e = roughness_to_phong(rough);
+        ct = pow(bs.uv.x, 1.0f / (e + 2.0f));
+    }
     T st = sqrt(max(1.f - ct * ct, 0.f));
     V3<T> ml{st * cphi, st * sphi, ct};
     V3<T> m = to_world(sp.f, ml);
@@ -996,9 +1029,14 @@ T bsdf_pdf(const Scene &sc, int mi, const SPoint<T> &sp, const V3<T> &wi, const 
         V3<T> ml = to_local(sp.f, m);
         if (ml.z > T(0.f)) {
             T rough = get_roughness(mat, sp.uv, r);
-            T e = roughness_to_phong(rough);
-            T D = pow(ml.z, e) * (e + 2.f) / float(2 * M_PI);
-            spdf = spmf * D / (4.f * fabs(dot(wo, m)));
+            if (mat.model == DR_MICROFACET_GGX) {  // half vectors drawn with density D (n.h)
+                T D = ggx_D(ml.z, ggx_A(rough));
+                spdf = spmf * D * ml.z / (4.f * fabs(dot(wo, m)));
+            } else {
+                T e = roughness_to_phong(rough);
+                T D = pow(ml.z, e) * (e + 2.f) / float(2 * M_PI);
+                spdf = spmf * D / (4.f * fabs(dot(wo, m)));
+            }
         }
     }
     return dpdf + spdf;
@@ -1171,6 +1209,7 @@ V3<T> shade(const Scene &sc, const V3<T> &wi, const Isect &pis, const SPoint<T> 
         if (hit_diffuse) wo = tv<T>(fv(wo));
         int mi = sc.shapes[cis.shape].mat;
         T pdf = bsdf_pdf<T>(sc, mi, csp_, cwi, wo, R ? &R->mat : nullptr);
+        if (sc.detached_pdf) pdf = T(val(pdf));  // DR_FLAG_DETACHED_PDF: a constant in the backward pass
         if (pdf <= T(0.f)) break;
         V3<T> be = bsdf<T>(sc, mi, csp_, cwi, wo, R ? &R->mat : nullptr);
         if (sum(be) <= T(0.f)) break;
@@ -1517,8 +1556,13 @@ inline float bsdf_bound(const Scene &sc, const EdgeNode &node, const V3f &wi, co
         else if (chmax < cth_min) chmax = cth_min;
         float shmax = std::sqrt(std::max(1.f - chmax * chmax, 0.f));
         float hdn = std::min(std::fabs(ln.x * shmax * cphi) + ln.z * chmax, 1.f);
-        float e = roughness_to_phong(get_roughness<float>(mat, sp.uv, nullptr));
-        maxp = std::pow(hdn, e) * (e + 2.f) / float(2 * M_PI);
+        float rough = get_roughness<float>(mat, sp.uv, nullptr);
+        if (mat.model == DR_MICROFACET_GGX) {
+            maxp = ggx_D(hdn, ggx_A(rough));
+        } else {
+            float e = roughness_to_phong(rough);
+            maxp = std::pow(hdn, e) * (e + 2.f) / float(2 * M_PI);
+        }
     }
     return cos_max * (dl / kPi + sl * maxp);
 }
@@ -1629,7 +1673,7 @@ inline M3 ltc_matrix(const Scene &sc, int mi, const SPoint<float> &sp, const V3f
     int tid = int((th / (M_PI / 2.f)) * (128 - 1));
     rid = std::max(0, std::min(127, rid));
     tid = std::max(0, std::min(127, tid));
-    const float *m = sc.ltc + 9 * (rid + tid * 128);
+    const float *m = (sc.mats[mi].model == DR_MICROFACET_GGX ? sc.ltc_ggx : sc.ltc) + 9 * (rid + tid * 128);
     M3 r3;
     for (int i = 0; i < 3; i++)
         for (int j = 0; j < 3; j++) r3(i, j) = m[3 * i + j];
@@ -1884,6 +1928,7 @@ inline void build_scene(Scene &sc, const dr_scene_desc *d, const float *ltc_defa
         std::memcpy(mm.uv_s, m.specular_uv_scale, 8);
         std::memcpy(mm.uv_r, m.roughness_uv_scale, 8);
         mm.two_sided = m.two_sided != 0;
+        mm.model = m.microfacet;
         sc.mats.push_back(mm);
     }
     for (int i = 0; i < d->num_shapes; i++) {
@@ -1899,6 +1944,7 @@ inline void build_scene(Scene &sc, const dr_scene_desc *d, const float *ltc_defa
         sc.shapes.push_back(sh);
     }
     sc.ltc = d->ltc_table ? d->ltc_table : ltc_default;
+    sc.ltc_ggx = d->ltc_table_ggx ? d->ltc_table_ggx : ltc_default;
     // lights (scene.cpp:26-52)
     std::vector<float> imp;
     for (int i = 0; i < d->num_lights; i++) {
@@ -2251,14 +2297,14 @@ int dro_render_parts(const dr_scene_desc *desc, const dr_render_desc *rd, int rn
                      float *image, float *grad, long long *stats, int nthreads, const int *shape_rank, int parts) {
     Scene sc;
     build_scene(sc, desc, nullptr, shape_rank);
-    if (!sc.ltc) {
-        static std::vector<float> ident;
-        if (ident.empty()) {
-            ident.assign(128 * 128 * 9, 0.f);
-            for (int i = 0; i < 128 * 128; i++) ident[9 * i] = ident[9 * i + 4] = ident[9 * i + 8] = 1.f;
-        }
-        sc.ltc = ident.data();
+    sc.detached_pdf = (rd->flags & DR_FLAG_DETACHED_PDF) != 0;
+    static std::vector<float> ident;
+    if (ident.empty()) {
+        ident.assign(128 * 128 * 9, 0.f);
+        for (int i = 0; i < 128 * 128; i++) ident[9 * i] = ident[9 * i + 4] = ident[9 * i + 8] = 1.f;
     }
+    if (!sc.ltc) sc.ltc = ident.data();
+    if (!sc.ltc_ggx) sc.ltc_ggx = ident.data();
     GradLayout L = grad_layout(desc);
     const int W = rd->width, H = rd->height, spp = rd->spp, B = rd->max_bounces;
     const bool derivs = d_image != nullptr;

@@ -51,18 +51,18 @@ def load():
     return _lib
 
 
-def scene_desc(wl, ltc_table=None):
+def scene_desc(wl, ltc_table=None, ltc_table_ggx=None):
     cam, mats, shps, lts = _abi.scene_dicts(wl.camera, wl.materials, wl.shapes, wl.lights)
-    return _abi.SceneDesc.from_scene(cam, mats, shps, lts, torch.device("cpu"), ltc_table)
+    return _abi.SceneDesc.from_scene(cam, mats, shps, lts, torch.device("cpu"), ltc_table, ltc_table_ggx)
 
 
 def oracle_render(wl, seed, d_image=None, rng_mode=REFERENCE, cores=8, ltc_table=None,
                   dp_mode=_abi.DR_DP_REFERENCE_LAST, primary_edge_samples=0, threads=0,
-                  shape_rank=None, parts=7, flags=0):
+                  shape_rank=None, parts=7, flags=0, ltc_table_ggx=None):
     """shape_rank: sort key per shape for the edge order (see dr_oracle.cpp Scene).
     parts: backward terms to include (1 continuous, 2 secondary edges, 4 primary edges)."""
     lib = load()
-    sd = scene_desc(wl, ltc_table)
+    sd = scene_desc(wl, ltc_table, ltc_table_ggx)
     W, H = wl.resolution
     rd = _abi.render_desc(W, H, wl.spp, wl.max_bounces, seed, primary_edge_samples, dp_mode, flags)
     image = np.zeros((H, W, 3), np.float32)

@@ -42,11 +42,12 @@ def load():
     return _lib
 
 
-def render(wl, seed, d_image=None, parts=7, ltc_table=None, dp_mode=0, primary_edge_samples=0, flags=0):
+def render(wl, seed, d_image=None, parts=7, ltc_table=None, dp_mode=0, primary_edge_samples=0, flags=0,
+           ltc_table_ggx=None):
     from delta_ray_b200 import _abi
     L = load()
     cam, mats, shps, lts = _abi.scene_dicts(wl.camera, wl.materials, wl.shapes, wl.lights)
-    sd = _abi.SceneDesc.from_scene(cam, mats, shps, lts, torch.device("cpu"), ltc_table)
+    sd = _abi.SceneDesc.from_scene(cam, mats, shps, lts, torch.device("cpu"), ltc_table, ltc_table_ggx)
     W, H = wl.resolution
     rd = _abi.render_desc(W, H, wl.spp, wl.max_bounces, seed, primary_edge_samples, dp_mode, flags)
     image = np.zeros((H, W, 3), np.float32)

@@ -112,6 +112,7 @@ void make_scene(const dr_scene_desc *desc, HostSceneBundle &b) {
     p.nrm_nodes = b.h.nrm_nodes.data();
     p.nrm_edges = b.h.nrm_edges.data();
     p.ltc = b.h.ltc.data();
+    p.ltc_ggx = b.h.ltc_ggx.data();
     drhost::fill_devscene(b.ds, b.h, b.f, p);
 }
 
@@ -127,6 +128,7 @@ int hh_render(const dr_scene_desc *desc, const dr_render_desc *rd, const float *
     HostSceneBundle b;
     make_scene(desc, b);
     b.ds.full_pixel_jitter = (rd->flags & DR_FLAG_FULL_PIXEL_JITTER) != 0;
+    b.ds.detached_pdf = (rd->flags & DR_FLAG_DETACHED_PDF) != 0;
     const DevScene &s = b.ds;
     int W = rd->width, H = rd->height, spp = rd->spp, B = rd->max_bounces;
     uint64_t seed = rd->seed;

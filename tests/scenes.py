@@ -99,5 +99,23 @@ def heightfield_small(seed=0, resolution=(40, 32), spp=2, max_bounces=2, grid=10
     return wl
 
 
+def ggx_shadow(seed=0, resolution=(48, 40), spp=2, max_bounces=2):
+    """glossy_shadow with GGX lobes (no counterpart in the reference)."""
+    wl = glossy_shadow(seed, resolution, spp, max_bounces)
+    for m in wl.materials[:2]:
+        m.microfacet = 1
+    wl.name = "ggx_shadow"
+    return wl
+
+
+def ggx_textured(seed=0, resolution=(40, 40), spp=2, max_bounces=2):
+    """textured with a GGX lobe: textured roughness and specular reflectance."""
+    wl = textured(seed, resolution, spp, max_bounces)
+    wl.materials[0].microfacet = 1
+    wl.name = "ggx_textured"
+    return wl
+
+
 SCENES = {"glossy_shadow": glossy_shadow, "textured": textured, "smooth_sphere": smooth_sphere,
-          "fisheye": fisheye, "heightfield_small": heightfield_small}
+          "fisheye": fisheye, "heightfield_small": heightfield_small, "ggx_shadow": ggx_shadow,
+          "ggx_textured": ggx_textured}

@@ -27,7 +27,7 @@ def test_library_exports_every_declared_symbol():
     L = _lib.lib()
     for n in declared_functions():
         assert hasattr(L, n), n
-    assert L.dr_abi_version() == 1
+    assert L.dr_abi_version() == 2
 
 
 def test_null_arguments_are_rejected_without_a_device():
