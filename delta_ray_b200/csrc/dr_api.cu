@@ -81,7 +81,8 @@ template <typename T> std::vector<T> fetch(const T *src, size_t count, const cha
 // cached; `idle` orders their reuse after the last kernels that touched them.
 struct BackwardQueues {
     DevBuf pt, items, item_w, item_dp, pt_last, counts;
-    long long cap_items = 0;  // grown on overflow, kept with the buffers
+    long long cap_items = 0;     // grown on overflow, kept with the buffers
+    double points_per_sample = 1;  // shading points per pixel sample the last overflow asked for
     cudaEvent_t idle = nullptr;
     ~BackwardQueues() {
         if (idle) cudaEventDestroy(idle);
@@ -289,6 +290,7 @@ DevScene call_scene(const dr_scene *sc, const dr_render_desc *rd) {
     DevScene ds = sc->ds;
     ds.full_pixel_jitter = (rd->flags & DR_FLAG_FULL_PIXEL_JITTER) != 0;
     ds.detached_pdf = (rd->flags & DR_FLAG_DETACHED_PDF) != 0;
+    ds.specular_chains = sc->h.specular_bounces && rd->max_bounces >= 1;
     return ds;
 }
 
@@ -319,10 +321,14 @@ void check_backward_args(const dr_scene *scene, const dr_render_desc *rd, const 
     if (!d_image_dev || !grad_dev) throw DrError(DR_ERR_INVALID_ARGUMENT, "d_image and grad must be non-NULL");
     if (rd->dp_mode != DR_DP_REFERENCE_LAST && rd->dp_mode != DR_DP_SUM)
         throw DrError(DR_ERR_INVALID_ARGUMENT, "unknown dp_mode");
-    if (scene->h.specular_bounces && rd->max_bounces >= 1)
-        throw DrError(DR_ERR_NOT_SUPPORTED,
-                      "backward through specular bounces (roughness <= 0.01 with a specular lobe) is not "
-                      "implemented; the forward render supports them");
+}
+
+// Shading points a backward call starts with room for: one per pixel sample,
+// twice that when specular samples can add vertices after the first.
+long long initial_point_cap(const dr_scene *scene, const dr_render_desc *rd, double per_sample) {
+    double samples = (double)rd->width * rd->height * rd->spp;
+    double f = std::max(per_sample, (scene->h.specular_bounces && rd->max_bounces >= 2) ? 2.0 : 1.0);
+    return std::max(1ll, (long long)std::ceil(samples * f));
 }
 
 // The backward pass on the queues bound in ws (counters zeroed here).
@@ -331,18 +337,21 @@ void check_backward_args(const dr_scene *scene, const dr_render_desc *rd, const 
 // `grow(n)` is asked for room for n items (it returns the capacity it bound),
 // and the edge stage then streams: points in chunks whose items fit, each
 // chunk traversed, evaluated and its position adjoints propagated before the
-// next.  Returns (shading points, edge items).
-template <class Grow>
+// next.  If the shading points (more than one per pixel sample after specular
+// samples) outgrow their queue, `grow_points(n)` is asked for room for n and
+// the front runs again (the same points: the streams are deterministic).
+// Returns (shading points, edge items).
+template <class Grow, class GrowPoints>
 std::pair<long long, long long> run_backward(dr_scene *scene, const dr_render_desc *rd, const float *d_image_dev,
                                              float *grad_dev, float *image_dev, BackwardWorkspace &ws,
-                                             cudaStream_t st, StageTimer *timer, Grow grow) {
+                                             cudaStream_t st, StageTimer *timer, Grow grow, GrowPoints grow_points) {
     const DevScene ds = call_scene(scene, rd);
     const GradCacheCfg cfg = grad_cache_cfg(scene->h);
     BackwardCounters c;
     auto read = [&]() {
         check_cuda(cudaMemcpyAsync(&c, ws.counters, sizeof(c), cudaMemcpyDeviceToHost, st), "status read");
         check_cuda(cudaStreamSynchronize(st), "backward");
-        if (c.status & ~DR_STATUS_ITEM_OVERFLOW)
+        if (c.status & ~(DR_STATUS_ITEM_OVERFLOW | DR_STATUS_POINT_OVERFLOW))
             throw DrError(DR_ERR_DEVICE_STATUS, "device reported status " + std::to_string(c.status));
     };
     auto back = [&]() {
@@ -350,15 +359,22 @@ std::pair<long long, long long> run_backward(dr_scene *scene, const dr_render_de
                                            rd->dp_mode, ws, cfg, scene->num_sms, st, &scene->last_launches, timer),
                    "backward launch");
     };
-    check_cuda(cudaMemsetAsync(ws.counters, 0, sizeof(BackwardCounters), st), "memset");
-    check_cuda(cudaMemsetAsync(grad_dev, 0, sizeof(float) * scene->h.grad_total, st), "memset");
-    ws.pt_begin = 0;
-    ws.pt_end = ws.cap_points;
-    check_cuda(dr_launch_backward_front(ds, rd->width, rd->height, rd->spp, rd->max_bounces, rd->seed, d_image_dev,
-                                        grad_dev, image_dev, rd->primary_edge_samples, rd->dp_mode, ws, cfg,
-                                        scene->num_sms, st, &scene->last_launches, timer),
-               "backward launch");
-    read();
+    for (int attempt = 0;; attempt++) {
+        check_cuda(cudaMemsetAsync(ws.counters, 0, sizeof(BackwardCounters), st), "memset");
+        check_cuda(cudaMemsetAsync(grad_dev, 0, sizeof(float) * scene->h.grad_total, st), "memset");
+        ws.pt_begin = 0;
+        ws.pt_end = ws.cap_points;
+        check_cuda(dr_launch_backward_front(ds, rd->width, rd->height, rd->spp, rd->max_bounces, rd->seed,
+                                            d_image_dev, grad_dev, image_dev, rd->primary_edge_samples, rd->dp_mode,
+                                            ws, cfg, scene->num_sms, st, &scene->last_launches, timer),
+                   "backward launch");
+        read();
+        if (!(c.status & DR_STATUS_POINT_OVERFLOW)) break;
+        const long long needed = (long long)c.points;
+        if (attempt > 0 || grow_points(needed) < needed)
+            throw DrError(DR_ERR_OUT_OF_MEMORY, std::to_string(needed) + " shading points exceed the point queue (" +
+                                                    std::to_string(ws.cap_points) + ")");
+    }
     const long long P = std::min((long long)c.points, ws.cap_points);
     long long items = 0;
     if (!(c.status & DR_STATUS_ITEM_OVERFLOW)) {
@@ -509,13 +525,10 @@ dr_status dr_render_backward(dr_scene *scene, const dr_render_desc *rd, const fl
         check_cuda(cudaSetDevice(scene->device), "cudaSetDevice");
         cudaStream_t st = (cudaStream_t)stream;
         scene->last_launches = 0;
-        // each pixel sample hands at most one shading point to edge sampling
-        long long cap_points = (long long)rd->width * rd->height * rd->spp;
         if (!scene->queues) scene->queues = take_queues(scene->device, st);
         BackwardQueues &q = *scene->queues;
+        long long cap_points = initial_point_cap(scene, rd, q.points_per_sample);
         long long cap_items = std::min(kMaxQueueItems, std::max(q.cap_items, std::max<long long>(cap_points * 4, 1 << 16)));
-        q.pt.reserve(sizeof(float) * DR_PT_FLOATS * cap_points);
-        q.pt_last.reserve(sizeof(unsigned long long) * cap_points);
         q.counts.reserve(sizeof(BackwardCounters));
         if (!q.idle) check_cuda(cudaEventCreateWithFlags(&q.idle, cudaEventDisableTiming), "cudaEventCreate");
         // marks the queues busy up to here on every way out, errors included
@@ -535,9 +548,14 @@ dr_status dr_render_backward(dr_scene *scene, const dr_render_desc *rd, const fl
             ws.item_dp = q.item_dp.as<float>();
             ws.cap_items = cap_items;
         };
-        ws.pt = q.pt.as<float>();
-        ws.pt_last = q.pt_last.as<unsigned long long>();
-        ws.cap_points = cap_points;
+        auto bind_points = [&]() {
+            q.pt.reserve(sizeof(float) * DR_PT_FLOATS * cap_points);
+            q.pt_last.reserve(DR_PT_LAST_BYTES * cap_points);
+            ws.pt = q.pt.as<float>();
+            ws.pt_last = q.pt_last.as<unsigned long long>();
+            ws.cap_points = cap_points;
+        };
+        bind_points();
         ws.counters = q.counts.as<BackwardCounters>();
         bind_items();
         // the item queue grows to what the traversal reported, up to its limit
@@ -550,7 +568,16 @@ dr_status dr_render_backward(dr_scene *scene, const dr_render_desc *rd, const fl
             }
             return cap_items;
         };
-        auto counts = run_backward(scene, rd, d_image_dev, grad_dev, image_dev, ws, st, &scene->timer, grow);
+        // the point queue grows to what the path stage reported (the ratio is
+        // kept for later calls)
+        auto grow_points = [&](long long want) {
+            cap_points = want + want / 16 + 1;
+            q.points_per_sample = (double)cap_points / ((double)rd->width * rd->height * rd->spp);
+            bind_points();
+            return cap_points;
+        };
+        auto counts =
+            run_backward(scene, rd, d_image_dev, grad_dev, image_dev, ws, st, &scene->timer, grow, grow_points);
         scene->last_points = counts.first;
         scene->last_items = counts.second;
         collect_timings(scene, st);
@@ -677,14 +704,21 @@ dr_status dr_render_backward_noalloc(dr_scene *scene, const dr_render_desc *rd, 
         unsigned char *base = noalloc_scratch(scene->device);
         // layout: counters | point records | point keys | items | item weights | item dp
         auto up = [](size_t b) { return (b + 255) & ~size_t(255); };
+        // scenes with specular chains: room for the points of every bounce,
+        // up to half the scratch (the rest holds edge items)
         long long cap_points = npix;
+        if (scene->h.specular_bounces && rd->max_bounces >= 2) {
+            long long want = npix * std::min(rd->max_bounces, DR_MAX_LINKS + 1);
+            long long fit = (long long)(kNoAllocScratchBytes / 2 / (sizeof(float) * DR_PT_FLOATS + DR_PT_LAST_BYTES));
+            cap_points = std::max(npix, std::min(want, fit));
+        }
         size_t off = 256;
         BackwardWorkspace ws;
         ws.counters = (BackwardCounters *)base;
         ws.pt = (float *)(base + off);
         off += up(sizeof(float) * DR_PT_FLOATS * (size_t)cap_points);
         ws.pt_last = (unsigned long long *)(base + off);
-        off += up(sizeof(unsigned long long) * (size_t)cap_points);
+        off += up(DR_PT_LAST_BYTES * (size_t)cap_points);
         long long cap_items = (long long)((kNoAllocScratchBytes - off - 3 * 256) / (sizeof(int4) + 4 * sizeof(float)));
         ws.items = (int4 *)(base + off);
         off += up(sizeof(int4) * (size_t)cap_items);
@@ -700,7 +734,7 @@ dr_status dr_render_backward_noalloc(dr_scene *scene, const dr_render_desc *rd, 
         // the launcher); the queue cannot grow, so large edge stages stream
         StageTimer quiet;  // no profiling events on this path
         auto counts = run_backward(scene, rd, d_image_dev, grad_dev, image_dev, ws, st, &quiet,
-                                   [&](long long) { return cap_items; });
+                                   [&](long long) { return cap_items; }, [&](long long) { return cap_points; });
         scene->last_points = counts.first;
         scene->last_items = counts.second;
     });

@@ -22,6 +22,7 @@
 #include "dr_backward.cuh"
 #include "dr_block_grad.cuh"
 
+template <bool kChains>
 __global__ void __launch_bounds__(128, 3) k_backward_paths(DevScene s, int W, int H, int spp, int B, uint64_t seed,
                                                         int lanes_log2, const float *d_image, float *grad, float *img,
                                                         BackwardWorkspace ws, GradCacheCfg cfg) {
@@ -43,10 +44,17 @@ __global__ void __launch_bounds__(128, 3) k_backward_paths(DevScene s, int W, in
         bool has = false;
         if (active && si < spp) {
             auto push = [&](const PointRecord &p) {
-                pr = p;
-                has = true;
+                if (p.bounce == 0) {  // the first vertex: pushed warp-aggregated below
+                    pr = p;
+                    has = true;
+                    return;
+                }
+                // vertices after specular samples (rare): one atomic each
+                unsigned long long slot = atomicAdd(&ws.counters->points, 1ull);
+                if (slot < (unsigned long long)ws.cap_points) p.store(ws.pt + (size_t)slot * DR_PT_WORDS);
+                else set_status(&ws.counters->status, DR_STATUS_POINT_OVERFLOW);
             };
-            acc += backward_pixel_sample(s, x, y, W, H, spp, si, B, seed, dc, bg, push);
+            acc += backward_pixel_sample<kChains>(s, x, y, W, H, spp, si, B, seed, dc, bg, push);
         }
         __syncwarp();
         unsigned long long slot = warp_reserve(&ws.counters->points, has ? 1 : 0);
@@ -68,20 +76,33 @@ __global__ void __launch_bounds__(128, 3) k_backward_paths(DevScene s, int W, in
     block_grad_flush(bg);
 }
 
-__global__ void __launch_bounds__(128) k_dp_propagate(DevScene s, int W, int H, int spp, uint64_t seed, float *grad,
-                                                      BackwardWorkspace ws, GradCacheCfg cfg) {
+// Position adjoints of the shading points pushed back along their paths.
+// DR_DP_REFERENCE_LAST: each point's last edge with a nonzero dp (the largest
+// key ((j + 1) << 32 | item) in pt_last).  DR_DP_SUM (scenes with specular
+// chains only): the dp sums k_edge_eval accumulated for points after the first
+// vertex, whose chains are traced again here, in this IEEE compile unit.
+template <bool kChains>
+__global__ void __launch_bounds__(128) k_dp_propagate(DevScene s, int W, int H, int spp, uint64_t seed, int dp_mode,
+                                                      float *grad, BackwardWorkspace ws, GradCacheCfg cfg) {
     extern __shared__ float sm[];
     BlockGrad bg = block_grad_begin(sm, grad, cfg);
     long long n = min(min((long long)ws.counters->points, ws.cap_points), ws.pt_end);
     for (long long p = ws.pt_begin + (long long)blockIdx.x * blockDim.x + threadIdx.x; p < n;
          p += (long long)gridDim.x * blockDim.x) {
-        unsigned long long key = ws.pt_last[p];
-        if (key == 0) continue;
-        long long i = (long long)(key & 0xffffffffull);
-        float3 dp = f3(ws.item_dp[3 * i], ws.item_dp[3 * i + 1], ws.item_dp[3 * i + 2]);
+        float3 dp;
+        if (dp_mode == DR_DP_SUM) {
+            float4 a = reinterpret_cast<const float4 *>(ws.pt_last)[p];
+            dp = f3(a.x, a.y, a.z);
+            if (is_zero(dp)) continue;
+        } else {
+            unsigned long long key = ws.pt_last[p];
+            if (key == 0) continue;
+            long long i = (long long)(key & 0xffffffffull);
+            dp = f3(ws.item_dp[3 * i], ws.item_dp[3 * i + 1], ws.item_dp[3 * i + 2]);
+        }
         PointRecord pt;
         pt.load(ws.pt + (size_t)p * DR_PT_WORDS);
-        propagate_dp(s, pt, W, H, spp, seed, dp, bg);
+        propagate_dp<kChains>(s, pt, W, H, spp, seed, dp, bg);
     }
     block_grad_flush(bg);
 }
@@ -103,12 +124,18 @@ cudaError_t dr_launch_backward_front(const DevScene &s, int W, int H, int spp, i
     int lanes_log2 = path_lanes_log2(spp);
     long long threads = ((long long)W * H) << lanes_log2;
     timer->begin(st);
-    if (dp_mode != DR_DP_SUM) {
-        cudaError_t e = cudaMemsetAsync(ws.pt_last, 0, sizeof(unsigned long long) * (size_t)ws.cap_points, st);
+    if (dp_mode != DR_DP_SUM || s.specular_chains) {
+        // LAST: one key per point; SUM with chains: a float4 dp sum per point
+        size_t per = dp_mode == DR_DP_SUM ? DR_PT_LAST_BYTES : sizeof(unsigned long long);
+        cudaError_t e = cudaMemsetAsync(ws.pt_last, 0, per * (size_t)ws.cap_points, st);
         if (e != cudaSuccess) return e;
     }
-    k_backward_paths<<<blocks_for(threads, bs), bs, smem, st>>>(s, W, H, spp, B, seed, lanes_log2, d_image, grad, img,
-                                                               ws, cfg);
+    if (s.specular_chains)
+        k_backward_paths<true><<<blocks_for(threads, bs), bs, smem, st>>>(s, W, H, spp, B, seed, lanes_log2, d_image,
+                                                                         grad, img, ws, cfg);
+    else
+        k_backward_paths<false><<<blocks_for(threads, bs), bs, smem, st>>>(s, W, H, spp, B, seed, lanes_log2, d_image,
+                                                                          grad, img, ws, cfg);
     timer->mark(st, "k_backward_paths");
     *launches += 1;
     long long npe = primary_edge_samples > 0 ? primary_edge_samples : (long long)spp * W * H;
@@ -131,8 +158,9 @@ cudaError_t dr_launch_backward_back(const DevScene &s, int W, int H, int spp, in
     if (e != cudaSuccess) return e;
     timer->mark(st, "k_edge_eval");
     *launches += 1;
-    if (dp_mode != DR_DP_SUM) {
-        k_dp_propagate<<<grid_ws, bs, smem, st>>>(s, W, H, spp, seed, grad, ws, cfg);
+    if (dp_mode != DR_DP_SUM || s.specular_chains) {
+        if (s.specular_chains) k_dp_propagate<true><<<grid_ws, bs, smem, st>>>(s, W, H, spp, seed, dp_mode, grad, ws, cfg);
+        else k_dp_propagate<false><<<grid_ws, bs, smem, st>>>(s, W, H, spp, seed, dp_mode, grad, ws, cfg);
         timer->mark(st, "k_dp_propagate");
         *launches += 1;
     }

@@ -83,6 +83,43 @@ struct BounceRecord {
     float q;       // Russian-roulette survival probability (1 before bounce 5)
 };
 
+// Adjoint of the specular lobe's sampled direction (sample_bsdf_dir with
+// bs.w > dpmf): dir = 2 (wi.h) h - wi, h = to_world(f, (st cos phi, st sin phi,
+// ct)), ct from the lobe's inverse cdf at bs.u0 (roughness-dependent).  f is
+// the frame the sample used (flipped for two-sided back faces by the caller).
+// Accumulates d_f, d_wi and returns d(roughness).
+DEV float d_specular_direction(const DevScene &s, int mi, const Frame &f, float3 wi, float rough, const BSDFSample &bs,
+                               float3 d_dir, Frame &d_f, float3 &d_wi) {
+    const DevMaterial &m = s.mats[mi];
+    float phi = 2.f * DR_PI * bs.u1;
+    float sphi = sinf(phi), cphi = cosf(phi);
+    float ct, dct_dr = 0.f;
+    if (m.model == DR_MICROFACET_GGX) {
+        float A = ggx_A(rough);
+        float num = 1.f - bs.u0, den = 1.f + (A - 1.f) * bs.u0;
+        ct = sqrtf(num / den);
+        if (ct > 0.f) dct_dr = (-num * bs.u0 / (2.f * ct * den * den)) * ggx_dA_drough(rough);
+    } else {
+        float e = roughness_to_phong(rough);
+        float ie = 1.f / (e + 2.0f);
+        ct = powf(bs.u0, ie);
+        if (2.f / rough > 0.f && bs.u0 > 0.f) dct_dr = ct * logf(bs.u0) * (-ie * ie) * (-2.f / (rough * rough));
+    }
+    float st = sqrtf(fmaxf(1.f - ct * ct, 0.f));
+    float3 hl = f3(st * cphi, st * sphi, ct);
+    float3 h = to_world(f, hl);
+    float wh = dot(wi, h), hd = dot(h, d_dir);
+    d_wi += 2.f * hd * h - d_dir;
+    float3 d_h = 2.f * wh * d_dir + 2.f * hd * wi;
+    d_f.t += hl.x * d_h;
+    d_f.b += hl.y * d_h;
+    d_f.n += hl.z * d_h;
+    float3 d_hl = f3(dot(d_h, f.t), dot(d_h, f.b), dot(d_h, f.n));
+    float d_ct = d_hl.z;
+    if (st > 0.f) d_ct += (d_hl.x * cphi + d_hl.y * sphi) * (-ct / st);
+    return d_ct * dct_dr;
+}
+
 // Direction sampled at a vertex, with the two-sided flip of pathtrace.h:116-133.
 DEV float3 sampled_direction(const DevScene &s, const BSDFSample &bs, float3 wi, int tri, const SurfacePoint &sp,
                              bool &specular) {
@@ -106,9 +143,118 @@ DEV void pixel_sample_position(int x, int y, int W, int H, int spp, uint64_t sid
     sy = float((y + sub_y) / H);
 }
 
+// Geometry adjoints of one path vertex (position, shading frame, uv).
+struct VertexGrad {
+    float3 dp;
+    Frame df;
+    float2 duv;
+    HD void zero() {
+        dp = f3(0.f);
+        df = frame_zero();
+        duv.x = duv.y = 0.f;
+    }
+};
+
+// A specular sample (pathtrace.h:141-159 keeps the vertex such a sample
+// reaches differentiable): the link from vertex k to vertex k + 1, with what
+// the reverse sweep needs of vertex k.
+struct SpecLink {
+    int tri;        // triangle of vertex k + 1
+    int from;       // link that reached vertex k; -1: the first vertex; -2: vertex k is not differentiable
+    int mi;         // material of vertex k
+    bool flip;      // the sample used vertex k's frame flipped (two-sided back face)
+    bool wo_live;   // wo_k = normalize(p_{k+1} - p_k) is differentiable: every sample so far was specular
+    float3 o, dir;  // the sampled ray (origin p_k)
+    Frame f;        // vertex k's frame as the sample used it
+    float3 wi;      // vertex k's incoming direction
+    float2 uv;      // vertex k's uv
+    BSDFSample bs;  // the sample drawn at vertex k
+    VertexGrad vg;  // adjoints of vertex k + 1
+    float3 dwo;     // adjoint of wo_k
+};
+
+struct NoGrad {
+    HD void add(int, float) {}
+};
+
+// Normal adjoint of a differentiated intersection: the reference adds the
+// first vertex's normal adjoint to all three vertices (delta_ray.cpp:1261-1269).
+template <class G> DEV void scatter_tri_normals(const DevScene &s, int tri, float3 dn0, G &g) {
+    int4 id = s.tri[tri];
+    const DevShape &sh = s.shapes[id.w];
+    int b = sh.grad_n - 3 * sh.vtx_off;
+    const int v[3] = {id.x, id.y, id.z};
+    for (int k = 0; k < 3; k++) {
+        g.add(b + 3 * v[k], dn0.x);
+        g.add(b + 3 * v[k] + 1, dn0.y);
+        g.add(b + 3 * v[k] + 2, dn0.z);
+    }
+}
+
+// Reverse sweep over links[0..n), last first: vertex k + 1's adjoints go
+// through its intersection (hit triangle positions; normals when `normals`)
+// and the sampled direction (vertex k's position, frame, uv and incoming
+// direction; the roughness texels when `materials`) to vertex k.  The first
+// vertex's adjoints end in v0 and d_wi (the primary wi).
+template <class G>
+DEV void sweep_links(const DevScene &s, SpecLink *links, int n, VertexGrad &v0, float3 &d_wi, bool normals,
+                     bool materials, G &g) {
+    NoGrad ng;
+    for (int l = n - 1; l >= 0; l--) {
+        SpecLink &L = links[l];
+        TriData td = load_tri(s, L.tri);
+        IsectFwd fw;
+        SurfacePoint nsp = intersect_tri(td, L.o, L.dir, &fw, true);
+        VertexGrad *from = L.from == -1 ? &v0 : (L.from >= 0 ? &links[L.from].vg : nullptr);
+        if (L.wo_live && !is_zero(L.dwo)) {
+            float3 dv = d_normalize(nsp.p - L.o, L.dwo);
+            L.vg.dp += dv;
+            if (from) from->dp -= dv;
+        }
+        TriGrad tg;
+        tg.v0 = tg.v1 = tg.v2 = tg.n0 = tg.n1 = tg.n2 = f3(0.f);
+        float3 d_o = f3(0.f), d_dir = f3(0.f);
+        d_intersect_tri(td, L.o, L.dir, fw, L.vg.dp, f3(0.f), L.vg.df, L.vg.duv, tg, d_o, d_dir);
+        scatter_tri_vertices(s, L.tri, tg.v0, tg.v1, tg.v2, g);
+        if (normals && td.has_n) scatter_tri_normals(s, L.tri, tg.n0, g);
+        if (is_zero(d_dir) && (!from || is_zero(d_o))) continue;
+        if (from) from->dp += d_o;
+        const DevMaterial &m = s.mats[L.mi];
+        Frame dfu = frame_zero();
+        float3 dwi_k = f3(0.f);
+        float dr = d_specular_direction(s, L.mi, L.f, L.wi, get_rough(s, m, L.uv), L.bs, d_dir, dfu, dwi_k);
+        float2 duv;
+        duv.x = duv.y = 0.f;
+        if (dr != 0.f) {
+            if (materials) d_rough(s, m, L.uv, dr, g, duv);
+            else d_rough(s, m, L.uv, dr, ng, duv);
+        }
+        if (from) {
+            if (L.flip) dfu = frame_neg(dfu);
+            frame_add(from->df, dfu);
+            from->duv.x += duv.x;
+            from->duv.y += duv.y;
+        }
+        if (L.from == -1) d_wi += dwi_k;
+        else if (L.from >= 0 && links[L.from].wo_live) links[L.from].dwo -= dwi_k;  // wi_k = -wo_{k-1}
+    }
+}
+
 // Returns the sample's image contribution; accumulates its gradient into g
-// and hands its first vertex to push_point(const PointRecord&).
-template <class G, class Push>
+// and hands every secondary-edge shading point to push_point(const
+// PointRecord&): the first vertex and the vertices after it that specular
+// samples reached before the first non-specular one (pathtrace.h:218-227).
+//
+// The reference's AD (pathtrace.h:104-297) keeps the geometry of the first
+// vertex and of every vertex reached by a specular sample differentiable; an
+// outgoing direction wo_k stays differentiable while every sample so far was
+// specular; NEE at every vertex uses the primary wi.  The replay accumulates
+// each vertex's local adjoints, then a reverse sweep over the specular links
+// pushes vertex k + 1's adjoints through its intersection and the sampled
+// direction to vertex k, the roughness and the hit triangle.
+// kChains = false compiles the variant for scenes without specular samples
+// (no chain bookkeeping); both give the same result on such scenes.
+template <bool kChains, class G, class Push>
 DEV float3 backward_pixel_sample(const DevScene &s, int x, int y, int W, int H, int spp, int si, int B, uint64_t seed,
                                  float3 d_color, G &g, Push &push_point) {
     const float sw = 1.f / spp;
@@ -126,6 +272,8 @@ DEV float3 backward_pixel_sample(const DevScene &s, int x, int y, int W, int H, 
     LightSample ls = draw_light(r);
     const Rng r_sec = r;  // stream position of the first secondary sample
     const float3 wi = -ray.d;
+    const int light_pick =
+        sample_discrete(s.light_sel_cdf, s.light_sel_func, s.light_sel_func_int, s.num_lights, ls.sel, nullptr);
     // ---- pass 1: trace, keep the bounces ----
     BounceRecord rec[DR_MAX_BOUNCES];
     int nb = 0;
@@ -136,6 +284,22 @@ DEV float3 backward_pixel_sample(const DevScene &s, int x, int y, int W, int H, 
     float3 thr = f3(1.f), cwi = wi;
     int ctri = h0.tri;
     SurfacePoint csp = sp0;
+    bool want_grad = !is_zero(d_color);
+    bool all_spec = true;  // every sample so far was specular
+    if (want_grad && B >= 1) {
+        PointRecord pr;
+        pr.p = sp0.p;
+        pr.n = sp0.f.n;
+        pr.ng = sp0.ng;
+        pr.uv = sp0.uv;
+        pr.wi = wi;
+        pr.d_color = d_color;
+        pr.tri = h0.tri;
+        pr.sid = sid;
+        pr.light = light_pick;
+        pr.bounce = 0;
+        push_point(pr);
+    }
     for (int b = 0; b < B; b++) {
         SecondarySample ss = draw_secondary(r);
         float3 N = nee(s, ls, wi, ctri, csp);
@@ -145,9 +309,15 @@ DEV float3 backward_pixel_sample(const DevScene &s, int x, int y, int W, int H, 
         rec[b].X = N;
         rec[b].r = f3(0.f);
         rec[b].q = 1.f;
-        BounceHit bh = sample_bsdf_scene(s, ss.bsdf, cwi, ctri, csp);
+        bool spec;
+        float3 dir = sampled_direction(s, ss.bsdf, cwi, ctri, csp, spec);
+        if (abs_sum(dir) <= 0.f) break;
+        Hit bh = trace_closest(s, csp.p, dir, 1e-3f);
         if (bh.tri < 0) break;
-        float3 wo = normalize(bh.sp.p - csp.p);
+        // a specular sample's hit keeps the reference's AD arithmetic (its
+        // position decides which edges a later shading point sees)
+        SurfacePoint nsp = intersect_tri(load_tri(s, bh.tri), csp.p, dir, nullptr, spec);
+        float3 wo = normalize(nsp.p - csp.p);
         int mi = material_of_tri(s, ctri);
         float pdf = bsdf_pdf(s, mi, csp, cwi, wo);
         if (pdf <= 0.f) break;
@@ -155,8 +325,8 @@ DEV float3 backward_pixel_sample(const DevScene &s, int x, int y, int W, int H, 
         if (sum(f) <= 0.f) break;
         rec[b].next_tri = bh.tri;
         int nli = light_of_tri(s, bh.tri);
-        if (nli >= 0 && dot(bh.sp.f.n, -wo) > 0.f) {
-            float lpdf = light_pdf(s, bh.tri) * length_sq(bh.sp.p - csp.p) / fabsf(dot(wo, bh.sp.ng));
+        if (nli >= 0 && dot(nsp.f.n, -wo) > 0.f) {
+            float lpdf = light_pdf(s, bh.tri) * length_sq(nsp.p - csp.p) / fabsf(dot(wo, nsp.ng));
             float mis = sq(pdf) / (sq(lpdf) + sq(pdf));
             float3 em = f * light_intensity(s, nli) * (mis / pdf);
             color += thr * em;
@@ -172,28 +342,28 @@ DEV float3 backward_pixel_sample(const DevScene &s, int x, int y, int W, int H, 
             rec[b].q = q;
         }
         rec[b].r = rb;
+        all_spec = all_spec && spec;
         cwi = -wo;
         ctri = bh.tri;
-        csp = bh.sp;
+        csp = nsp;
+        // vertex b + 1 is a secondary-edge shading point while every sample was specular
+        if (kChains && want_grad && all_spec && b + 1 < B && b + 1 <= DR_MAX_LINKS) {
+            PointRecord pr;
+            pr.p = nsp.p;
+            pr.n = nsp.f.n;
+            pr.ng = nsp.ng;
+            pr.uv = nsp.uv;
+            pr.wi = cwi;
+            pr.d_color = d_color * thr;  // the edge weight carries the path throughput
+            pr.tri = bh.tri;
+            pr.sid = sid;
+            pr.light = light_pick;
+            pr.bounce = b + 1;
+            push_point(pr);
+        }
     }
     color = color * sw;
-    if (is_zero(d_color)) return color;  // render_sample_fast: no derivatives, no edges
-    // ---- the first vertex is a secondary-edge shading point ----
-    {
-        PointRecord pr;
-        pr.p = sp0.p;
-        pr.n = sp0.f.n;
-        pr.ng = sp0.ng;
-        pr.uv = sp0.uv;
-        pr.wi = wi;
-        pr.d_color = d_color;
-        pr.tri = h0.tri;
-        pr.sid = sid;
-        pr.light = sample_discrete(s.light_sel_cdf, s.light_sel_func, s.light_sel_func_int, s.num_lights, ls.sel,
-                                   nullptr);
-        pr.bounce = 0;
-        if (B >= 1) push_point(pr);
-    }
+    if (!want_grad) return color;  // render_sample_fast: no derivatives, no edges
     // ---- suffix radiance S_{k+1}, stored in rec[k].X ----
     float3 S = f3(0.f);
     for (int k = nb - 1; k >= 0; k--) {
@@ -209,9 +379,14 @@ DEV float3 backward_pixel_sample(const DevScene &s, int x, int y, int W, int H, 
         g.add(L.grad + 1, dC.y);
         g.add(L.grad + 2, dC.z);
     }
-    SpGrad g0;  // adjoints of the first vertex (frame, uv) and of wi
-    g0.zero();
-    float3 d_p0 = f3(0.f);
+    VertexGrad v0g;  // adjoints of the first vertex
+    v0g.zero();
+    float3 d_wi = f3(0.f);  // adjoint of the primary wi
+    SpecLink links[DR_MAX_LINKS];
+    int nlinks = 0;
+    int vlink = -1;            // link that reached the current vertex (-1: first vertex, or not differentiable)
+    bool vlive = true;         // the current vertex's geometry is differentiable
+    bool wi_live = true;       // the current vertex's incoming direction is differentiable
     Rng rr = r_sec;
     thr = f3(1.f);
     cwi = wi;
@@ -219,28 +394,34 @@ DEV float3 backward_pixel_sample(const DevScene &s, int x, int y, int W, int H, 
     csp = sp0;
     for (int k = 0; k < nb; k++) {
         SecondarySample ss = draw_secondary(rr);
-        const bool first = k == 0;
         float3 a = dC * thr;
+        VertexGrad *vg = !vlive ? nullptr : (vlink < 0 ? &v0g : &links[vlink].vg);
         {
             SpGrad gn;
             gn.zero();
             float3 dp = f3(0.f);
             d_nee(s, ls, wi, ctri, csp, a, g, gn, dp);
-            g0.dwi += gn.dwi;  // NEE always uses the primary wi (pathtrace.h:213-216)
-            if (first) {
-                frame_add(g0.df, gn.df);
-                g0.duv.x += gn.duv.x;
-                g0.duv.y += gn.duv.y;
-                d_p0 += dp;
+            d_wi += gn.dwi;  // NEE always uses the primary wi (pathtrace.h:213-216)
+            if (vg) {
+                frame_add(vg->df, gn.df);
+                vg->duv.x += gn.duv.x;
+                vg->duv.y += gn.duv.y;
+                vg->dp += dp;
             }
         }
         int nt = rec[k].next_tri;
         if (nt < 0) break;
-        bool spec;
-        float3 dir = sampled_direction(s, ss.bsdf, cwi, ctri, csp, spec);
-        SurfacePoint nsp = intersect_tri(load_tri(s, nt), csp.p, dir);
-        float3 wo = normalize(nsp.p - csp.p);
         int mi = material_of_tri(s, ctri);
+        SurfacePoint use = csp;
+        bool flip = s.mats[mi].two_sided && dot(cwi, csp.f.n) < 0.f;
+        if (flip) {
+            use.f = frame_neg(csp.f);
+            use.ng = -csp.ng;
+        }
+        bool spec;
+        float3 dir = sample_bsdf_dir(s, mi, use, cwi, ss.bsdf, spec);
+        SurfacePoint nsp = intersect_tri(load_tri(s, nt), csp.p, dir, nullptr, spec);
+        float3 wo = normalize(nsp.p - csp.p);
         float pdf = bsdf_pdf(s, mi, csp, cwi, wo);
         float3 f = bsdf(s, mi, csp, cwi, wo);
         float3 d_f = f3(0.f);
@@ -269,36 +450,50 @@ DEV float3 backward_pixel_sample(const DevScene &s, int x, int y, int W, int H, 
         gb.zero();
         d_bsdf(s, mi, csp, cwi, wo, d_f, g, gb);
         if (!s.detached_pdf) d_bsdf_pdf(s, mi, csp, cwi, wo, d_pdf, g, gb);
-        if (first) {
-            frame_add(g0.df, gb.df);
-            g0.duv.x += gb.duv.x;
-            g0.duv.y += gb.duv.y;
-            g0.dwi += gb.dwi;
+        if (vg) {
+            frame_add(vg->df, gb.df);
+            vg->duv.x += gb.duv.x;
+            vg->duv.y += gb.duv.y;
+        }
+        // the incoming direction: the primary wi, or -wo_{k-1} while differentiable
+        if (k == 0) d_wi += gb.dwi;
+        else if (wi_live && vlink >= 0) links[vlink].dwo -= gb.dwi;
+        // the vertex this sample reached is differentiable only for a specular sample
+        int next_link = -1;
+        if (kChains && spec && nlinks < DR_MAX_LINKS) {
+            SpecLink &L = links[nlinks];
+            L.tri = nt;
+            L.from = vlive ? vlink : -2;
+            L.mi = mi;
+            L.flip = flip;
+            L.wo_live = wi_live;
+            L.o = csp.p;
+            L.dir = dir;
+            L.f = use.f;
+            L.wi = cwi;
+            L.uv = csp.uv;
+            L.bs = ss.bsdf;
+            L.vg.zero();
+            L.dwo = L.wo_live ? gb.dwo : f3(0.f);
+            next_link = nlinks++;
         }
         thr = thr * rec[k].r;
+        wi_live = wi_live && spec;
+        vlive = next_link >= 0;
+        vlink = next_link;
         cwi = -wo;
         ctri = nt;
         csp = nsp;
     }
+    if (kChains) sweep_links(s, links, nlinks, v0g, d_wi, true, true, g);
     // ---- first vertex geometry -> triangle and camera ----
     TriGrad tg;
     tg.v0 = tg.v1 = tg.v2 = tg.n0 = tg.n1 = tg.n2 = f3(0.f);
     float3 d_o = f3(0.f), d_d = f3(0.f);
-    d_intersect_tri(td0, ray.o, ray.d, fw0, d_p0, f3(0.f), g0.df, g0.duv, tg, d_o, d_d);
-    d_d -= g0.dwi;
+    d_intersect_tri(td0, ray.o, ray.d, fw0, v0g.dp, f3(0.f), v0g.df, v0g.duv, tg, d_o, d_d);
+    d_d -= d_wi;
     scatter_tri_vertices(s, h0.tri, tg.v0, tg.v1, tg.v2, g);
-    if (td0.has_n) {
-        // the first vertex's normal adjoint goes to all three (delta_ray.cpp:1261-1269)
-        int4 id = s.tri[h0.tri];
-        const DevShape &sh = s.shapes[id.w];
-        int b = sh.grad_n - 3 * sh.vtx_off;
-        const int v[3] = {id.x, id.y, id.z};
-        for (int k = 0; k < 3; k++) {
-            g.add(b + 3 * v[k], tg.n0.x);
-            g.add(b + 3 * v[k] + 1, tg.n0.y);
-            g.add(b + 3 * v[k] + 2, tg.n0.z);
-        }
-    }
+    if (td0.has_n) scatter_tri_normals(s, h0.tri, tg.n0, g);
     d_sample_primary(s.cam, sx, sy, d_o, d_d, g, 0);
     return color;
 }
@@ -360,8 +555,11 @@ DEV float3 eval_item(const DevScene &s, const PointRecord &pt, int tree, int ei,
     return er.dp;
 }
 
-// dp of a first-vertex shading point pushed back to its triangle and the camera.
-template <class G>
+// dp of a shading point pushed back along its path to the camera and the
+// triangles' positions (the second sweep of delta_ray.cpp:975-1002, which
+// scatters neither normals nor material parameters).  A point after the first
+// vertex was reached by specular samples only: its chain is traced again.
+template <bool kChains, class G>
 DEV void propagate_dp(const DevScene &s, const PointRecord &pt, int W, int H, int spp, uint64_t seed, float3 dp, G &g) {
     uint64_t pix = pt.sid / (uint64_t)spp;
     int x = (int)(pix % (uint64_t)W), y = (int)(pix / (uint64_t)W);
@@ -369,17 +567,67 @@ DEV void propagate_dp(const DevScene &s, const PointRecord &pt, int W, int H, in
     float sx, sy;
     pixel_sample_position(x, y, W, H, spp, pt.sid, seed, s.full_pixel_jitter != 0, sx, sy, r);
     Ray ray = sample_primary(s.cam, sx, sy, true);
-    TriData td = load_tri(s, pt.tri);
+    VertexGrad v0;
+    v0.zero();
+    float3 d_wi = f3(0.f);
+    int tri0 = pt.tri;
+    if (!kChains || pt.bounce == 0) {
+        v0.dp = dp;
+    } else {
+        SpecLink links[DR_MAX_LINKS];
+        Hit h = trace_closest(s, ray.o, ray.d, 1e-3f);
+        if (h.tri < 0) return;
+        tri0 = h.tri;
+        SurfacePoint csp = intersect_tri(load_tri(s, h.tri), ray.o, ray.d, nullptr, true);
+        float3 cwi = -ray.d;
+        int ctri = h.tri;
+        draw_light(r);
+        if (pt.bounce > DR_MAX_LINKS) return;
+        const int n = pt.bounce;
+        for (int k = 0; k < n; k++) {
+            SecondarySample ss = draw_secondary(r);
+            int mi = material_of_tri(s, ctri);
+            SurfacePoint use = csp;
+            bool flip = s.mats[mi].two_sided && dot(cwi, csp.f.n) < 0.f;
+            if (flip) {
+                use.f = frame_neg(csp.f);
+                use.ng = -csp.ng;
+            }
+            bool spec;
+            float3 dir = sample_bsdf_dir(s, mi, use, cwi, ss.bsdf, spec);
+            Hit bh = trace_closest(s, csp.p, dir, 1e-3f);
+            if (bh.tri < 0 || !spec) return;  // not the chain that reached the point
+            SpecLink &L = links[k];
+            L.tri = bh.tri;
+            L.from = k - 1;
+            L.mi = mi;
+            L.flip = flip;
+            L.wo_live = true;
+            L.o = csp.p;
+            L.dir = dir;
+            L.f = use.f;
+            L.wi = cwi;
+            L.uv = csp.uv;
+            L.bs = ss.bsdf;
+            L.vg.zero();
+            L.dwo = f3(0.f);
+            SurfacePoint nsp = intersect_tri(load_tri(s, bh.tri), csp.p, dir, nullptr, true);
+            cwi = -normalize(nsp.p - csp.p);
+            ctri = bh.tri;
+            csp = nsp;
+        }
+        links[n - 1].vg.dp = dp;
+        sweep_links(s, links, n, v0, d_wi, false, false, g);
+    }
+    TriData td = load_tri(s, tri0);
     IsectFwd fw;
     intersect_tri(td, ray.o, ray.d, &fw, true);
     TriGrad tg;
     tg.v0 = tg.v1 = tg.v2 = tg.n0 = tg.n1 = tg.n2 = f3(0.f);
     float3 d_o = f3(0.f), d_d = f3(0.f);
-    Frame zf = frame_zero();
-    float2 zuv;
-    zuv.x = zuv.y = 0.f;
-    d_intersect_tri(td, ray.o, ray.d, fw, dp, f3(0.f), zf, zuv, tg, d_o, d_d);
-    scatter_tri_vertices(s, pt.tri, tg.v0, tg.v1, tg.v2, g);
+    d_intersect_tri(td, ray.o, ray.d, fw, v0.dp, f3(0.f), v0.df, v0.duv, tg, d_o, d_d);
+    d_d -= d_wi;
+    scatter_tri_vertices(s, tri0, tg.v0, tg.v1, tg.v2, g);
     d_sample_primary(s.cam, sx, sy, d_o, d_d, g, 0);
 }
 

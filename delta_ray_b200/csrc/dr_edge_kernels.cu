@@ -72,7 +72,14 @@ __global__ void __launch_bounds__(128, 4) k_edge_eval(DevScene s, int W, int H, 
         float3 dp = eval_item(s, pt, tree, ei, it.z, ws.item_w[i], spp, B, seed, bg);
         if (is_zero(dp)) continue;
         if (dp_mode == DR_DP_SUM) {
-            propagate_dp(s, pt, W, H, spp, seed, dp, bg);
+            if (pt.bounce == 0) {
+                propagate_dp<false>(s, pt, W, H, spp, seed, dp, bg);
+            } else {  // after specular samples: summed here, the chain is traced by k_dp_propagate
+                float *a = reinterpret_cast<float *>(ws.pt_last) + 4 * (size_t)it.x;
+                atomicAdd(a, dp.x);
+                atomicAdd(a + 1, dp.y);
+                atomicAdd(a + 2, dp.z);
+            }
         } else {
             ws.item_dp[3 * i] = dp.x;
             ws.item_dp[3 * i + 1] = dp.y;

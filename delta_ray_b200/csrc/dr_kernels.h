@@ -58,7 +58,11 @@ struct BackwardWorkspace {
     float *item_w;               // edge weight
     long long cap_items;
     float *item_dp;              // [cap_items][3] position adjoint of each item
-    unsigned long long *pt_last; // [cap_points] ((j + 1) << 32 | item) of the point's last item with dp != 0
+    // [cap_points] x DR_PT_LAST_BYTES: DR_DP_REFERENCE_LAST keeps ((j + 1) << 32 | item)
+    // of the point's last item with dp != 0 in the first 8 bytes; DR_DP_SUM on
+    // scenes with specular chains sums the dp of points after the first vertex
+    // as a float4
+    unsigned long long *pt_last;
     BackwardCounters *counters;
     // points [pt_begin, min(pt_end, counters->points)) go through the edge
     // stage (k_edge_traverse, k_edge_eval, k_dp_propagate) of one launch
@@ -97,6 +101,7 @@ cudaError_t dr_launch_backward_back(const DevScene &s, int W, int H, int spp, in
 #define DR_PT_FLOATS 24
 
 // Device status bits.
+#define DR_PT_LAST_BYTES 16
 #define DR_STATUS_POINT_OVERFLOW 1
 #define DR_STATUS_ITEM_OVERFLOW 2
 #define DR_STATUS_STACK_OVERFLOW 4

@@ -55,6 +55,11 @@ struct DevEdgeNode {
     int pad;
 };
 
+// Paths keep at most DR_MAX_LINKS differentiable specular vertices: later
+// ones are treated as constants and are no secondary-edge shading points, so
+// a pixel sample hands at most DR_MAX_LINKS + 1 points to edge sampling.
+#define DR_MAX_LINKS 8
+
 struct DevScene {
     DevCamera cam;
     // geometry
@@ -102,6 +107,10 @@ struct DevScene {
     int full_pixel_jitter;
     // per render call: the backward pass holds the BSDF sampling pdf constant
     int detached_pdf;
+    // per render call: specular samples can occur (a material with roughness
+    // <= 0.01 and a specular lobe, and max_bounces >= 1), so the backward pass
+    // differentiates through the vertices they reach
+    int specular_chains;
 };
 
 // --- accessors -------------------------------------------------------------

@@ -196,7 +196,10 @@ DR_API dr_status dr_render_forward(dr_scene *scene, const dr_render_desc *rd, fl
 /* Backward render (delta_ray.cpp:694-1005 and :1468-1550): given the image
  * adjoint d_image [H][W][3] (device), overwrites grad_dev (device, flat
  * layout above) with every parameter gradient.  image_dev may be NULL;
- * otherwise the re-rendered image is written there too.  The library's item
+ * otherwise the re-rendered image is written there too.  Paths are
+ * differentiated through "specular" samples (roughness <= 0.01), and the
+ * vertices such samples reach are shading points too (pathtrace.h:141-227);
+ * a path keeps at most 8 such vertices differentiable.  The library's item
  * queue holds up to 8 GiB of sampled edges; larger edge stages (glossy
  * scenes with many edges sample thousands per shading point) are evaluated
  * in several passes over the shading points. */
@@ -213,7 +216,8 @@ DR_API dr_status dr_render_backward(dr_scene *scene, const dr_render_desc *rd, c
  * DR_ERR_INVALID_ARGUMENT); sampled edges beyond the array's room (about
  * 800,000 at the largest image) are evaluated in several passes over the
  * shading points, and a single point with more edges than that fails with
- * DR_ERR_OUT_OF_MEMORY.  All calls on
+ * DR_ERR_OUT_OF_MEMORY, as do specular chains whose shading points outgrow
+ * half the array (about 150,000 points).  All calls on
  * one device share the array, so overlapping calls (from several threads or
  * streams) race: serialize them.  The first call on each device looks up the
  * array's address; make it before any stream capture. */

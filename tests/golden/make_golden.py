@@ -38,6 +38,8 @@ CASES = [
     ("smooth_sphere", "smooth_sphere", dict(seed=6, resolution=(24, 24), spp=2, max_bounces=1), 17),
     ("fisheye", "fisheye", dict(seed=7, resolution=(24, 24), spp=2, max_bounces=1), 19),
     ("heightfield_small", "heightfield_small", dict(seed=8, resolution=(24, 20), spp=2, max_bounces=2), 23),
+    ("mirror_shadow", "mirror_shadow", dict(seed=10, resolution=(24, 20), spp=2, max_bounces=3), 29),
+    ("mirror_hall", "mirror_hall", dict(seed=11, resolution=(24, 20), spp=2, max_bounces=5), 31),
 ]
 
 
@@ -70,7 +72,10 @@ def main():
     import oracle
     import ref_runner
     ltc = np.fromfile(os.path.join(ROOT, "oracle", "_ref", "ltc_tabM.f32"), np.float32)
+    only = set(sys.argv[1:])  # optional case names: regenerate those only
     for name, builder, kwargs, seed in CASES:
+        if only and name not in only:
+            continue
         wl = build_case(builder, kwargs)
         dimg = adjoint_image(wl, seed)
         fwd = ref_runner.render_reference(wl, seed, strict=True)

@@ -129,6 +129,7 @@ int hh_render(const dr_scene_desc *desc, const dr_render_desc *rd, const float *
     make_scene(desc, b);
     b.ds.full_pixel_jitter = (rd->flags & DR_FLAG_FULL_PIXEL_JITTER) != 0;
     b.ds.detached_pdf = (rd->flags & DR_FLAG_DETACHED_PDF) != 0;
+    b.ds.specular_chains = b.h.specular_bounces && rd->max_bounces >= 1;
     const DevScene &s = b.ds;
     int W = rd->width, H = rd->height, spp = rd->spp, B = rd->max_bounces;
     uint64_t seed = rd->seed;
@@ -136,6 +137,15 @@ int hh_render(const dr_scene_desc *desc, const dr_render_desc *rd, const float *
     HostSink sink{&g};
     std::vector<PointRecord> pts;
     auto push = [&](const PointRecord &pr) { pts.push_back(pr); };
+    // the kernels' two instantiations, chosen as the launchers choose them
+    auto sample = [&](int x, int y, int si, float3 dc, HostSink &gs) {
+        return s.specular_chains ? backward_pixel_sample<true>(s, x, y, W, H, spp, si, B, seed, dc, gs, push)
+                                 : backward_pixel_sample<false>(s, x, y, W, H, spp, si, B, seed, dc, gs, push);
+    };
+    auto prop = [&](const PointRecord &pt, float3 dp) {
+        if (s.specular_chains) propagate_dp<true>(s, pt, W, H, spp, seed, dp, sink);
+        else propagate_dp<false>(s, pt, W, H, spp, seed, dp, sink);
+    };
     for (int y = 0; y < H; y++)
         for (int x = 0; x < W; x++) {
             float3 acc = f3(0.f);
@@ -143,11 +153,11 @@ int hh_render(const dr_scene_desc *desc, const dr_render_desc *rd, const float *
                                 : f3(0.f);
             for (int si = 0; si < spp; si++) {
                 if (!d_image) acc += pixel_sample(s, x, y, W, H, spp, si, B, seed);
-                else if (parts & 1) acc += backward_pixel_sample(s, x, y, W, H, spp, si, B, seed, dc, sink, push);
+                else if (parts & 1) acc += sample(x, y, si, dc, sink);
                 else {
                     std::vector<double> tmp(g.size(), 0.0);
                     HostSink ts{&tmp};
-                    acc += backward_pixel_sample(s, x, y, W, H, spp, si, B, seed, dc, ts, push);
+                    acc += sample(x, y, si, dc, ts);
                 }
             }
             image[3 * (y * W + x)] = acc.x;
@@ -169,7 +179,7 @@ int hh_render(const dr_scene_desc *desc, const dr_render_desc *rd, const float *
             float3 dp = eval_item(s, pts[it.pt], it.tree, it.ei, it.j, it.w, spp, B, seed, sink);
             if (is_zero(dp)) continue;
             if (rd->dp_mode == DR_DP_SUM) {
-                propagate_dp(s, pts[it.pt], W, H, spp, seed, dp, sink);
+                prop(pts[it.pt], dp);
             } else if (it.j > last[it.pt]) {
                 last[it.pt] = it.j;
                 last_dp[it.pt] = dp;
@@ -177,7 +187,7 @@ int hh_render(const dr_scene_desc *desc, const dr_render_desc *rd, const float *
         }
         if (rd->dp_mode != DR_DP_SUM)
             for (size_t p = 0; p < pts.size(); p++)
-                if (last[p] >= 0) propagate_dp(s, pts[p], W, H, spp, seed, last_dp[p], sink);
+                if (last[p] >= 0) prop(pts[p], last_dp[p]);
     }
     if (d_image && (parts & 4)) {
         long long npe = rd->primary_edge_samples > 0 ? rd->primary_edge_samples : (long long)spp * W * H;

@@ -99,6 +99,62 @@ def heightfield_small(seed=0, resolution=(40, 32), spp=2, max_bounces=2, grid=10
     return wl
 
 
+def mirror_shadow(seed=0, resolution=(48, 40), spp=2, max_bounces=3):
+    """soft_shadow over a near-mirror ground (roughness 0.005: the reference's
+    "specular" samples, material.h:410) under a two-sided near-mirror blocker,
+    with a diffuse back wall carrying vertex normals.  Paths run camera ->
+    ground -> blocker / wall through chains of specular vertices, which are
+    secondary-edge shading points (pathtrace.h:218-227)."""
+    wl = workloads.soft_shadow(seed, resolution, spp, max_bounces)
+    g = wl.materials[0]
+    g.diffuse_reflectance = _t([0.15, 0.15, 0.15])
+    g.specular_reflectance = _t([0.7, 0.7, 0.7])
+    g.roughness = _t([0.005])
+    b = wl.materials[1]
+    b.diffuse_reflectance = _t([0.2, 0.1, 0.1])
+    b.specular_reflectance = _t([0.6, 0.6, 0.5])
+    b.roughness = _t([0.008])
+    b.two_sided = True
+    wl.materials.append(Material(diffuse_reflectance=_t([0.6, 0.5, 0.4])))
+    wv, wi = workloads._quad([0, 4, 4], 5.0, 4.0, [1, 0, 0], [0, 1, 0], normal=[0, 0, -1])
+    rng = np.random.default_rng(seed + 300)
+    wn = np.tile([0.0, 0.0, -1.0], (4, 1)) + rng.uniform(-0.2, 0.2, (4, 3))
+    wn = (wn / np.linalg.norm(wn, axis=1, keepdims=True)).astype(np.float32)
+    wl.shapes.append(Shape(_t(wv), _t(wi, np.int32), None, _t(wn), len(wl.materials) - 1))
+    wl.name = "mirror_shadow"
+    return wl
+
+
+def mirror_hall(seed=0, resolution=(32, 24), spp=2, max_bounces=5):
+    """Two facing mirrors (no diffuse lobe, roughness 0.003: every sample is
+    "specular", material.h:353-412) over a diffuse ground with a blocker and
+    an overhead light.  Camera paths bounce between the mirrors, so a pixel
+    sample has up to max_bounces shading points (pathtrace.h:218-227)."""
+    rng = np.random.default_rng(seed)
+    res = [int(resolution[0]), int(resolution[1])]
+    cam = workloads._camera([0, 2, -5], [2, 1.8, -3.5], [0, 1, 0], 60.0, res)
+    mats = [Material(diffuse_reflectance=_t(rng.uniform(0.3, 0.8, 3))),
+            Material(diffuse_reflectance=_t([0.0, 0.0, 0.0]), specular_reflectance=_t([0.85, 0.9, 0.8]),
+                     roughness=_t([0.003])),
+            Material(diffuse_reflectance=_t(rng.uniform(0.3, 0.8, 3))),
+            Material(diffuse_reflectance=_t([0.0, 0.0, 0.0]))]
+    gv, gi = workloads._quad([0, 0, 0], 5.0, 6.0, [1, 0, 0], [0, 0, 1], normal=[0, 1, 0])
+    m0v, m0i = workloads._quad([-2, 2, 0], 6.0, 2.0, [0, 0, 1], [0, 1, 0], normal=[1, 0, 0])
+    m1v, m1i = workloads._quad([2, 2, 0], 6.0, 2.0, [0, 0, 1], [0, 1, 0], normal=[-1, 0, 0])
+    bv = np.array([[-0.6, 1.2, -0.6], [0.6, 1.2, -0.6], [0.6, 1.2, 0.6], [-0.6, 1.2, 0.6], [0.0, 1.2, 0.0]])
+    bv = (bv + rng.uniform(-0.2, 0.2, size=bv.shape)).astype(np.float32)
+    bi = np.array([[4, 1, 0], [4, 2, 1], [4, 3, 2], [4, 0, 3]], np.int32)
+    lv, li = workloads._quad([0, 4.5, 0.5], 1.0, 1.0, [1, 0, 0], [0, 0, 1], normal=[0, -1, 0])
+    shapes = [Shape(_t(gv), _t(gi, np.int32), None, None, 0),
+              Shape(_t(m0v), _t(m0i, np.int32), None, None, 1),
+              Shape(_t(m1v), _t(m1i, np.int32), None, None, 1),
+              Shape(_t(bv), _t(bi, np.int32), None, None, 2),
+              Shape(_t(lv), _t(li, np.int32), None, None, 3)]
+    lights = [Light(4, _t([20.0, 20.0, 20.0]))]
+    return workloads.Workload("mirror_hall", cam, mats, shapes, lights, res, int(spp), int(max_bounces),
+                              {"seed": seed})
+
+
 def ggx_shadow(seed=0, resolution=(48, 40), spp=2, max_bounces=2):
     """glossy_shadow with GGX lobes (no counterpart in the reference)."""
     wl = glossy_shadow(seed, resolution, spp, max_bounces)
@@ -117,5 +173,6 @@ def ggx_textured(seed=0, resolution=(40, 40), spp=2, max_bounces=2):
 
 
 SCENES = {"glossy_shadow": glossy_shadow, "textured": textured, "smooth_sphere": smooth_sphere,
-          "fisheye": fisheye, "heightfield_small": heightfield_small, "ggx_shadow": ggx_shadow,
+          "fisheye": fisheye, "heightfield_small": heightfield_small, "mirror_shadow": mirror_shadow,
+          "mirror_hall": mirror_hall, "ggx_shadow": ggx_shadow,
           "ggx_textured": ggx_textured}

@@ -14,6 +14,11 @@ import oracle
 from native import harness
 
 TOL = 1e-5
+# Near-mirror lobes raise the cosine of the half vector to the power
+# 2 / roughness (667 in mirror_hall), so one float ulp of that cosine moves the
+# BSDF by ~667 ulps; five such bounces in a row leave ~1e-5 of round-off
+# between two correct evaluation orders.
+CASE_TOL = {"mirror_hall": 5e-5}
 
 
 @pytest.mark.parametrize("case", golden_cases())
@@ -33,7 +38,7 @@ def test_kernel_logic_matches_oracle(case, ltc_table):
         if np.abs(o["grad"]).max() == 0:
             assert np.abs(h["grad"]).max() == 0
         else:
-            assert rel_err(h["grad"], o["grad"]) < TOL, f"gradient term {parts}"
+            assert rel_err(h["grad"], o["grad"]) < CASE_TOL.get(case, TOL), f"gradient term {parts}"
 
 
 def test_dp_sum_mode_matches_oracle(ltc_table):

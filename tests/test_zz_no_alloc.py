@@ -67,6 +67,26 @@ def test_noalloc_backward_matches_backward_twice(res, spp, B):
 
 
 @pytest.mark.gpu
+def test_noalloc_backward_specular_chains():
+    """Specular chains (several shading points per pixel sample) fit the
+    scratch's point queue and match dr_render_backward."""
+    import scenes
+    from delta_ray_b200 import _abi, _lib
+    from delta_ray_b200.render_pytorch import Scene, unpack_args
+    L = _bind(_lib.lib())
+    wl = scenes.mirror_hall(seed=4, resolution=(40, 32), spp=2, max_bounces=5)
+    W, H = wl.resolution
+    cam, mats, shps, lts, _, _, _, _ = unpack_args(wl.serialize())
+    sc = Scene(cam, mats, shps, lts, 0, None)
+    d_image = torch.rand((H, W, 3), generator=torch.Generator().manual_seed(6)).cuda()
+    ref_grad, _ = sc.backward(W, H, 2, 5, 9, d_image)
+    st, grad, _ = _noalloc(L, sc, W, H, 2, 5, 9, d_image)
+    assert st == 0, _lib.last_error()
+    assert rel_err(grad.cpu().numpy(), ref_grad.cpu().numpy()) < TOL
+    sc.close()
+
+
+@pytest.mark.gpu
 def test_noalloc_backward_rejects_oversize_calls():
     from delta_ray_b200 import _lib
     L = _bind(_lib.lib())
