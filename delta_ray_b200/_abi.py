@@ -67,6 +67,7 @@ DR_DP_REFERENCE_LAST = 0
 DR_DP_SUM = 1
 DR_FLAG_FULL_PIXEL_JITTER = 1
 DR_FLAG_DETACHED_PDF = 2
+DR_FLAG_EDGE_LOBE_MIS = 4
 
 
 def render_desc(width, height, spp, max_bounces, seed, primary_edge_samples=0,

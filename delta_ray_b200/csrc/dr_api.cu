@@ -290,6 +290,7 @@ DevScene call_scene(const dr_scene *sc, const dr_render_desc *rd) {
     DevScene ds = sc->ds;
     ds.full_pixel_jitter = (rd->flags & DR_FLAG_FULL_PIXEL_JITTER) != 0;
     ds.detached_pdf = (rd->flags & DR_FLAG_DETACHED_PDF) != 0;
+    ds.edge_lobe_mis = (rd->flags & DR_FLAG_EDGE_LOBE_MIS) != 0;
     ds.specular_chains = sc->h.specular_bounces && rd->max_bounces >= 1;
     return ds;
 }
@@ -305,7 +306,7 @@ void check_render_desc(const dr_scene *sc, const dr_render_desc *rd) {
         throw DrError(DR_ERR_INVALID_ARGUMENT, "width * height * spp must be below 2^31 per call");
     for (int i = 0; i < 7; i++)
         if (rd->reserved[i] != 0) throw DrError(DR_ERR_INVALID_ARGUMENT, "reserved fields must be zero");
-    if (rd->flags & ~(int)(DR_FLAG_FULL_PIXEL_JITTER | DR_FLAG_DETACHED_PDF))
+    if (rd->flags & ~(int)(DR_FLAG_FULL_PIXEL_JITTER | DR_FLAG_DETACHED_PDF | DR_FLAG_EDGE_LOBE_MIS))
         throw DrError(DR_ERR_INVALID_ARGUMENT, "unknown render flags");
     if (rd->max_bounces > 64) throw DrError(DR_ERR_NOT_SUPPORTED, "max_bounces above 64");
     if (sc->ds.num_lights == 0) throw DrError(DR_ERR_INVALID_ARGUMENT, "scene has no lights");

@@ -390,6 +390,35 @@ DEV M3 normalize_jacobian(float3 x) {
 
 struct EdgeResult { float3 dp, dv0, dv1; };
 
+// Density with which a lobe's line sample (the construction of
+// delta_ray.cpp:107-160 in the lobe's space minv) picks the edge point at
+// offset q from the shading point, per unit of another parameterisation l of
+// the same edge with dq/dl = q_l.  0 where the lobe cannot sample (below its
+// horizon).  d0, d1: edge endpoints relative to the shading point.
+DEV_NOINLINE float lobe_line_density(const M3 &minv, float3 d0, float3 d1, float3 q, float3 q_l) {
+    float3 a = mul(minv, d0), b = mul(minv, d1);
+    if (a.z <= 0.f && b.z <= 0.f) return 0.f;
+    if (a.z < 0.f) a = (a * b.z - b * a.z) / (b.z - a.z);
+    if (b.z < 0.f) b = (a * b.z - b * a.z) / (b.z - a.z);
+    float3 vod = b - a;
+    if (abs_sum(vod) < 1e-10f) return 0.f;
+    float3 wt = normalize(vod);
+    float l0 = dot(a, wt), l1 = dot(b, wt);
+    float3 vo = a - l0 * wt;
+    float d = length(vo);
+    auto I = [&](float l) {
+        return (l / (d * (d * d + l * l)) + atanf(l / d) / (d * d)) * vo.z + (l * l / (d * (d * d + l * l))) * wt.z;
+    };
+    float norm = I(l1) - I(l0);
+    if (norm <= 1e-10f) return 0.f;
+    float3 y = mul(minv, q);
+    if (y.z < 0.f) return 0.f;
+    float l = dot(y, wt);
+    float ds = d * d + l * l;
+    float p = 2.f * d * (vo + l * wt).z / (norm * ds * ds);
+    return p > 0.f ? p * length(mul(minv, q_l)) : 0.f;
+}
+
 // Secondary edge sample (delta_ray.cpp:45-365).  `rng` holds the item's
 // secondary samples (for the two shade calls, replayed from the same state).
 DEV EdgeResult shading_edge_sample(const DevScene &s, const EdgeSample &es, const DevEdge &edge, const LightSample &ls,
@@ -532,10 +561,22 @@ DEV EdgeResult shading_edge_sample(const DevScene &s, const EdgeSample &es, cons
     }
     EdgeResult res = none;
     float pdf_l = pdf(l);
+    // DR_FLAG_EDGE_LOBE_MIS: the one-sample balance heuristic over the two
+    // lobes, pmf_sel pdf_sel(l) + pmf_other pdf_other(l); the reference divides
+    // by pmf_sel pdf_sel(l) alone
+    float q_mix = mpmf * pdf_l;
+    if (s.edge_lobe_mis) {
+        bool sel_diffuse = es.bsdf_component <= dpmf;
+        float opmf = sel_diffuse ? spmf : dpmf;
+        if (opmf > 0.f) {
+            M3 ominv = sel_diffuse ? mul(inverse(ltc_matrix(s, mi, sp, wi)), frame) : frame;
+            q_mix += opmf * lobe_line_density(ominv, v0 - sp.p, v1 - sp.p, sample_p, mul(m, wt));
+        }
+    }
     auto accum = [&](const SurfacePoint &lp, float3 ev) {
         M3 nj = normalize_jacobian(sample_p);
         M3 ij = intersect_jacobian(sdir, lp.p, lp.ng);
-        float line_j = length(mul(mul(mul(ij, nj), m), wt)) / (mpmf * pdf_l);
+        float line_j = length(mul(mul(mul(ij, nj), m), wt)) / q_mix;
         float3 p = sp.p, x = lp.p;
         float3 d0 = v0 - p, d1 = v1 - p;
         float dirac_j = length(cross(d0, d1));

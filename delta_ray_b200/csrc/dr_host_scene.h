@@ -711,6 +711,7 @@ inline void fill_devscene(DevScene &ds, const HostScene &h, const FlatScene &f, 
     ds.ltc_ggx = p.ltc_ggx;
     ds.full_pixel_jitter = 0;  // set per render call
     ds.detached_pdf = 0;
+    ds.edge_lobe_mis = 0;
     ds.specular_chains = 0;
     ds.grad_total = (int)h.grad_total;
 }

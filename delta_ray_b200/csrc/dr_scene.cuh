@@ -107,6 +107,9 @@ struct DevScene {
     int full_pixel_jitter;
     // per render call: the backward pass holds the BSDF sampling pdf constant
     int detached_pdf;
+    // per render call: a secondary-edge sample is divided by the two lobes'
+    // mixture density instead of the picked lobe's pmf * line pdf
+    int edge_lobe_mis;
     // per render call: specular samples can occur (a material with roughness
     // <= 0.01 and a specular lobe, and max_bounces >= 1), so the backward pass
     // differentiates through the vertices they reach

@@ -42,15 +42,21 @@ class RenderOptions:
     detached_pdf: hold the BSDF sampling pdf constant in the backward pass
         (unbiased gradients of roughness and lobe weights) instead of
         differentiating it at a fixed sampled direction as the reference does.
+    edge_lobe_mis: divide a secondary-edge sample by the two lobes' mixture
+        density at the sampled point (balance heuristic).  The reference
+        divides by the picked lobe's pick probability times its line pdf,
+        which doubles the edge term on materials with both a diffuse and a
+        specular lobe (delta_ray.cpp:88-105, 318-330).
     """
 
     def __init__(self, primary_edge_samples=0, dp_mode=_abi.DR_DP_REFERENCE_LAST, ltc_table="fitted",
                  output_device=None, device=None, full_pixel_jitter=False, ltc_table_ggx="fitted",
-                 detached_pdf=False):
+                 detached_pdf=False, edge_lobe_mis=False):
         self.primary_edge_samples = int(primary_edge_samples)
         self.dp_mode = int(dp_mode)
         self.flags = (_abi.DR_FLAG_FULL_PIXEL_JITTER if full_pixel_jitter else 0) | \
-            (_abi.DR_FLAG_DETACHED_PDF if detached_pdf else 0)
+            (_abi.DR_FLAG_DETACHED_PDF if detached_pdf else 0) | \
+            (_abi.DR_FLAG_EDGE_LOBE_MIS if edge_lobe_mis else 0)
         self.ltc_table = ltc_table
         self.ltc_table_ggx = ltc_table_ggx
         self.output_device = output_device

@@ -135,8 +135,21 @@ typedef enum { DR_DP_REFERENCE_LAST = 0, DR_DP_SUM = 1 } dr_dp_mode;
  * pdf constant in the backward pass.  The reference differentiates it while
  * keeping the sampled direction fixed (pathtrace.h:248-253), which biases the
  * gradient of every parameter that shapes the sampling (roughness, the lobe
- * weights) by -E[contribution * d log pdf]; held constant it is unbiased. */
-typedef enum { DR_FLAG_FULL_PIXEL_JITTER = 1, DR_FLAG_DETACHED_PDF = 2 } dr_render_flags;
+ * weights) by -E[contribution * d log pdf]; held constant it is unbiased.
+ * DR_FLAG_EDGE_LOBE_MIS changes the weight of a secondary-edge sample.
+ * The reference picks one lobe (diffuse or specular) with probability pmf,
+ * samples the edge by that lobe's line pdf, and divides the sample by
+ * pmf * line pdf (delta_ray.cpp:88-105, 318-330). The sample evaluates the whole
+ * BSDF, so the expectation is the edge integral once per lobe with nonzero pmf,
+ * twice the integral on materials with both lobes. With the flag the sample is
+ * divided by the mixture density, the sum over both lobes of pmf * that lobe's
+ * line pdf at the sampled point (the one-sample balance heuristic). That is
+ * unbiased wherever either lobe can sample the edge. */
+typedef enum {
+    DR_FLAG_FULL_PIXEL_JITTER = 1,
+    DR_FLAG_DETACHED_PDF = 2,
+    DR_FLAG_EDGE_LOBE_MIS = 4
+} dr_render_flags;
 
 typedef struct {
     int width;

@@ -482,6 +482,7 @@ struct EdgeTree { std::vector<EdgeNode> nodes; std::vector<Edge> edges; };
 struct Scene {
     Camera cam;
     bool detached_pdf = false;
+    bool edge_lobe_mis = false;  // DR_FLAG_EDGE_LOBE_MIS
     std::vector<Shape> shapes;
     std::vector<Material> mats;
     std::vector<Light> lights;
@@ -1682,6 +1683,34 @@ inline M3 ltc_matrix(const Scene &sc, int mi, const SPoint<float> &sp, const V3f
 
 struct EdgeResult { V3f dp{0, 0, 0}, dv0{0, 0, 0}, dv1{0, 0, 0}; };
 
+// Density with which a lobe's line sample (delta_ray.cpp:107-160, in the
+// lobe's space minv) picks the edge point at offset q from the shading point,
+// per unit of a parameter l of the edge with dq/dl = q_l; 0 below the lobe's
+// horizon.  Project addition (DR_FLAG_EDGE_LOBE_MIS), no reference counterpart.
+inline float lobe_line_density(const M3 &minv, const V3f &d0, const V3f &d1, const V3f &q, const V3f &q_l) {
+    V3f a = minv * d0, b = minv * d1;
+    if (a.z <= 0.f && b.z <= 0.f) return 0.f;
+    if (a.z < 0.f) a = (a * b.z - b * a.z) / (b.z - a.z);
+    if (b.z < 0.f) b = (a * b.z - b * a.z) / (b.z - a.z);
+    V3f vod = b - a;
+    if (abs_sum(vod) < 1e-10f) return 0.f;
+    V3f wt = normalize(vod);
+    float l0 = dot(a, wt), l1 = dot(b, wt);
+    V3f vo = a - l0 * wt;
+    float d = length(vo);
+    auto I = [&](float l) {
+        return (l / (d * (d * d + l * l)) + std::atan(l / d) / (d * d)) * vo.z + (l * l / (d * (d * d + l * l))) * wt.z;
+    };
+    float norm = I(l1) - I(l0);
+    if (norm <= 1e-10f) return 0.f;
+    V3f y = minv * q;
+    if (y.z < 0.f) return 0.f;
+    float l = dot(y, wt);
+    float ds = d * d + l * l;
+    float p = 2.f * d * (vo + l * wt).z / (norm * ds * ds);
+    return p > 0.f ? p * length(minv * q_l) : 0.f;
+}
+
 // secondary edge sample (delta_ray.cpp:45-365)
 inline EdgeResult shading_edge_sample(const Scene &sc, const EdgeSample &es, const Edge &edge, const LightSample &ls,
                                       const std::vector<SecondarySample> &ss, const V3f &wi, const Isect &sis,
@@ -1787,10 +1816,20 @@ inline EdgeResult shading_edge_sample(const Scene &sc, const EdgeSample &es, con
     };
     if (too_close(ir, hr.second) || too_close(il, hl.second)) return none;
     EdgeResult res;
+    // DR_FLAG_EDGE_LOBE_MIS: balance heuristic over the two lobes
+    float q_mix = mpmf * pdf(l);
+    if (sc.edge_lobe_mis) {
+        bool sel_diffuse = es.bsdf_component <= dpmf;
+        float opmf = sel_diffuse ? spmf : dpmf;
+        if (opmf > 0.f) {
+            M3 ominv = sel_diffuse ? inverse(ltc_matrix(sc, mi, sp, wi)) * frame : frame;
+            q_mix += opmf * lobe_line_density(ominv, v0 - sp.p, v1 - sp.p, sample_p, m * wt);
+        }
+    }
     auto accum = [&](const SPoint<float> &lp, const V3f &ev) {
         M3 nj = normalize_jacobian(sample_p);
         M3 ij = intersect_jacobian(sdir, lp.p, lp.ng);
-        float line_j = length(((ij * nj) * m) * wt) / (mpmf * pdf(l));
+        float line_j = length(((ij * nj) * m) * wt) / q_mix;
         V3f p = sp.p, x = lp.p;
         V3f d0 = v0 - p, d1 = v1 - p;
         float dirac_j = length(cross(d0, d1));
@@ -2298,6 +2337,7 @@ int dro_render_parts(const dr_scene_desc *desc, const dr_render_desc *rd, int rn
     Scene sc;
     build_scene(sc, desc, nullptr, shape_rank);
     sc.detached_pdf = (rd->flags & DR_FLAG_DETACHED_PDF) != 0;
+    sc.edge_lobe_mis = (rd->flags & DR_FLAG_EDGE_LOBE_MIS) != 0;
     static std::vector<float> ident;
     if (ident.empty()) {
         ident.assign(128 * 128 * 9, 0.f);

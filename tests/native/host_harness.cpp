@@ -129,6 +129,7 @@ int hh_render(const dr_scene_desc *desc, const dr_render_desc *rd, const float *
     make_scene(desc, b);
     b.ds.full_pixel_jitter = (rd->flags & DR_FLAG_FULL_PIXEL_JITTER) != 0;
     b.ds.detached_pdf = (rd->flags & DR_FLAG_DETACHED_PDF) != 0;
+    b.ds.edge_lobe_mis = (rd->flags & DR_FLAG_EDGE_LOBE_MIS) != 0;
     b.ds.specular_chains = b.h.specular_bounces && rd->max_bounces >= 1;
     const DevScene &s = b.ds;
     int W = rd->width, H = rd->height, spp = rd->spp, B = rd->max_bounces;

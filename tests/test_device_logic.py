@@ -125,3 +125,26 @@ def test_detached_pdf_matches_oracle(ltc_table):
     assert rel_err(h["grad"], o["grad"]) < TOL
     assert rel_err(o["image"], o0["image"]) == 0
     assert rel_err(o["grad"], o0["grad"]) > 1e-3
+
+
+def test_edge_lobe_mis_matches_oracle(ltc_table):
+    """DR_FLAG_EDGE_LOBE_MIS: a secondary-edge sample is divided by the two
+    lobes' mixture density.  On two-lobe materials the edge term roughly
+    halves; the path and primary-edge terms are unchanged."""
+    import scenes
+    from delta_ray_b200 import _abi
+    wl = scenes.SCENES["glossy_shadow"](seed=9, resolution=(24, 20), spp=2, max_bounces=2)
+    W, H = wl.resolution
+    d_image = np.ones((H, W, 3), np.float32)
+    f = _abi.DR_FLAG_EDGE_LOBE_MIS
+    for parts in (1, 2):
+        h = harness.render(wl, 33, d_image, parts=parts, ltc_table=ltc_table, flags=f)
+        o = oracle.oracle_render(wl, 33, d_image, rng_mode=oracle.PHILOX, ltc_table=ltc_table, parts=parts,
+                                 flags=f)
+        o0 = oracle.oracle_render(wl, 33, d_image, rng_mode=oracle.PHILOX, ltc_table=ltc_table, parts=parts)
+        assert rel_err(h["grad"], o["grad"]) < TOL
+        assert h["stats"][1] == o["stats"][1]
+        if parts == 1:
+            assert rel_err(o["grad"], o0["grad"]) == 0
+        else:
+            assert np.abs(o["grad"]).sum() < 0.8 * np.abs(o0["grad"]).sum()

@@ -137,7 +137,7 @@ def _with(wl, **edits):
     return w2
 
 
-def _jitter_render(wl, seed, spp=None, d_image=None, dp_mode=None):
+def _jitter_render(wl, seed, spp=None, d_image=None, dp_mode=None, flags=0):
     """Forward image sum (d_image None) or flat gradient, sub-pixel samples over the whole pixel."""
     from delta_ray_b200 import _abi
     from delta_ray_b200.render_pytorch import RenderOptions, Scene
@@ -145,6 +145,7 @@ def _jitter_render(wl, seed, spp=None, d_image=None, dp_mode=None):
     sc = Scene(cam, mats, shps, lts, 0, None)
     W, H = wl.resolution
     opts = RenderOptions(dp_mode=_abi.DR_DP_SUM if dp_mode is None else dp_mode, full_pixel_jitter=True)
+    opts.flags |= flags
     try:
         if d_image is None:
             return float(sc.forward(W, H, spp or wl.spp, wl.max_bounces, seed, opts).double().sum())
@@ -183,7 +184,7 @@ def test_linear_parameters_match_finite_differences():
         assert abs(grad[o + c] - fd) <= 2e-3 * abs(fd) + 1e-3, (c, grad[o + c], fd)
 
 
-def _fd_vs_grad(wl, shape, sel, h, spp_fd=1024, K=8, K_fd=4):
+def _fd_vs_grad(wl, shape, sel, h, spp_fd=1024, K=8, K_fd=4, flags=0):
     """(gradient mean, its standard error, FD mean, its standard error) of the
     image sum along the vertex coordinates sel = [(vertex, axis)]."""
     from stats_util import _grad_blocks
@@ -197,7 +198,7 @@ def _fd_vs_grad(wl, shape, sel, h, spp_fd=1024, K=8, K_fd=4):
         e[vi, ax] = 1.0
     g = []
     for k in range(K):
-        gk = _jitter_render(wl, 100 + k, d_image=ones)[o:o + n].reshape(-1, 3)
+        gk = _jitter_render(wl, 100 + k, d_image=ones, flags=flags)[o:o + n].reshape(-1, 3)
         g.append(sum(gk[vi, ax] for vi, ax in sel))
     fd = []
     for k in range(K_fd):  # common random numbers at +-h, many samples per pixel
@@ -205,6 +206,8 @@ def _fd_vs_grad(wl, shape, sel, h, spp_fd=1024, K=8, K_fd=4):
         lm = _jitter_render(_with(wl, **{f"shape{shape}": v - h * e}), 500 + k, spp_fd)
         fd.append((lp - lm) / (2 * h))
     g, fd = np.array(g, np.float64), np.array(fd, np.float64)
+    if K_fd == 0:
+        return g.mean(), g.std(ddof=1) / np.sqrt(K), None, None
     return g.mean(), g.std(ddof=1) / np.sqrt(K), fd.mean(), fd.std(ddof=1) / np.sqrt(K_fd)
 
 
@@ -230,3 +233,27 @@ def test_shadow_gradient_matches_finite_differences():
     g, sg, fd, sfd = _fd_vs_grad(wl, 1, [(i, 1) for i in range(nb)], 5e-2)
     assert abs(fd) > 5 * sfd
     assert abs(g - fd) < 4 * np.hypot(sg, sfd) + 0.10 * abs(fd), (g, sg, fd, sfd)
+
+
+@pytest.mark.gpu
+def test_two_lobe_shadow_edges_match_finite_differences_with_lobe_mis():
+    """A glossy ground (diffuse and specular lobes) under the raised blocker.
+    The reference divides each secondary-edge sample by the picked lobe's pmf
+    times its line pdf, so the shadow-edge term E comes out twice its
+    expectation.  DR_FLAG_EDGE_LOBE_MIS changes only that term (path and
+    primary-edge terms are bit-identical), so on common random numbers
+    g_reference = other + 2E and g_mis = other + E.  The edge term the central
+    difference implies, fd - other, must match E to the accuracy of the
+    shadow-edge estimator in the single-lobe scene (a few per cent)."""
+    from delta_ray_b200 import _abi
+    wl = _soft_shadow((128, 128), 64)
+    wl.materials[0].specular_reflectance = torch.tensor([0.3, 0.3, 0.3])
+    wl.materials[0].roughness = torch.tensor([0.3])
+    nb = wl.shapes[1].vertices.shape[0]
+    sel = [(i, 1) for i in range(nb)]
+    g1, _, fd, sfd = _fd_vs_grad(wl, 1, sel, 5e-2, flags=_abi.DR_FLAG_EDGE_LOBE_MIS)
+    g0, _, _, _ = _fd_vs_grad(wl, 1, sel, 5e-2, K_fd=0)
+    assert abs(fd) > 5 * sfd
+    e = g0 - g1
+    e_fd = fd - (g1 - e)
+    assert abs(e / e_fd - 1) < 0.10, (g0, g1, fd, e, e_fd)
