@@ -44,6 +44,9 @@ def lib():
     L.dr_scene_last_timings.argtypes = [C.c_void_p, C.c_int, C.c_char_p, C.c_size_t, C.POINTER(C.c_float)]
     L.dr_scene_last_counts.argtypes = [C.c_void_p, C.POINTER(C.c_int64), C.POINTER(C.c_int64)]
     L.dr_last_error.argtypes = [C.c_char_p, C.c_size_t]
+    L.dr_mlp_param_count.restype = C.c_int
+    L.dr_mlp_forward.argtypes = [C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p]
+    L.dr_mlp_gradient.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p]
     L.dr_last_error.restype = C.c_size_t
     for name in ("dr_scene_create", "dr_scene_update", "dr_scene_destroy", "dr_scene_grad_layout",
                  "dr_render_forward", "dr_render_backward", "dr_scene_last_launch_count", "dr_trace_rays",

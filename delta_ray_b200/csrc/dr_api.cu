@@ -9,6 +9,7 @@
 #include "../../include/delta_ray_b200.h"
 #include "dr_host_scene.h"
 #include "dr_kernels.h"
+#include "dr_mlp.h"
 
 #include <algorithm>
 #include <cmath>
@@ -582,6 +583,68 @@ dr_status dr_render_backward(dr_scene *scene, const dr_render_desc *rd, const fl
         scene->last_points = counts.first;
         scene->last_items = counts.second;
         collect_timings(scene, st);
+    });
+}
+
+int dr_mlp_param_count(void) { return kMlpParams; }
+
+namespace {
+// Device buffers of one network call: bf16 rows, packed weights, status word.
+struct MlpScratch {
+    DevBuf x16, img, status, total;
+    void bind(const float *x_dev, int64_t n, const float *params_dev, cudaStream_t st) {
+        x16.reserve(sizeof(__nv_bfloat16) * DR_MLP_IN * (size_t)std::max<int64_t>(n, 1));
+        img.reserve(kImgBytes);
+        status.reserve(sizeof(int));
+        total.reserve(sizeof(float));
+        check_cuda(cudaMemsetAsync(status.p, 0, sizeof(int), st), "memset");
+        check_cuda(dr_mlp_to_bf16(x_dev, x16.as<__nv_bfloat16>(), n * DR_MLP_IN, st), "bf16 rows");
+        check_cuda(dr_mlp_pack(params_dev, img.as<uint8_t>(), st), "weight pack");
+    }
+    void check(cudaStream_t st) {
+        int s = 0;
+        check_cuda(cudaMemcpyAsync(&s, status.p, sizeof(int), cudaMemcpyDeviceToHost, st), "status read");
+        check_cuda(cudaStreamSynchronize(st), "network");
+        if (s) throw DrError(DR_ERR_DEVICE_STATUS, "network kernel reported status " + std::to_string(s));
+    }
+};
+int current_sms() {
+    int dev = 0, sms = 148;
+    check_cuda(cudaGetDevice(&dev), "cudaGetDevice");
+    check_cuda(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev), "device query");
+    return sms;
+}
+}  // namespace
+
+dr_status dr_mlp_forward(const float *params_dev, const float *x_dev, int64_t n, float *logits_dev, void *stream) {
+    return guard([&]() {
+        if (n < 0 || (n > 0 && (!params_dev || !x_dev || !logits_dev)))
+            throw DrError(DR_ERR_INVALID_ARGUMENT, "invalid network buffers");
+        cudaStream_t st = (cudaStream_t)stream;
+        MlpScratch m;
+        m.bind(x_dev, n, params_dev, st);
+        check_cuda(dr_mlp_infer(m.img.as<uint8_t>(), params_dev, m.x16.as<__nv_bfloat16>(), n, logits_dev, nullptr,
+                                m.status.as<int>(), current_sms(), st),
+                   "network forward");
+        m.check(st);
+    });
+}
+
+dr_status dr_mlp_gradient(const float *params_dev, const float *x_dev, const float *targets_dev, int64_t n,
+                          float *grads_dev, float *loss_dev, void *stream) {
+    return guard([&]() {
+        if (n < 0 || !params_dev || !grads_dev || !loss_dev || (n > 0 && (!x_dev || !targets_dev)))
+            throw DrError(DR_ERR_INVALID_ARGUMENT, "invalid network buffers");
+        cudaStream_t st = (cudaStream_t)stream;
+        MlpScratch m;
+        m.bind(x_dev, n, params_dev, st);
+        check_cuda(cudaMemsetAsync(grads_dev, 0, sizeof(float) * kMlpParams, st), "memset");
+        check_cuda(cudaMemsetAsync(loss_dev, 0, sizeof(float), st), "memset");
+        check_cuda(dr_mlp_sum(targets_dev, n * DR_MLP_OUT, m.total.as<float>(), st), "target sum");
+        check_cuda(dr_mlp_grad(m.img.as<uint8_t>(), params_dev, m.x16.as<__nv_bfloat16>(), targets_dev, n,
+                               m.total.as<float>(), grads_dev, loss_dev, m.status.as<int>(), current_sms(), st),
+                   "network gradient");
+        m.check(st);
     });
 }
 

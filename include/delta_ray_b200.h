@@ -264,6 +264,22 @@ DR_API dr_status dr_scene_last_launch_count(const dr_scene *scene, int *count);
 /* Copies the last error message of the calling thread into buf. */
 DR_API size_t dr_last_error(char *buf, size_t len);
 
+/* The learned edge proposal's network (no counterpart in the reference): a
+ * 10 -> 64 -> 64 -> 64 -> 32 MLP (ReLU, softmax output) run on the tensor
+ * cores in bf16 with f32 accumulation.  params: dr_mlp_param_count() floats
+ * (device), W1 [64][16] (the proposal fills 10 inputs and zeroes 10..15), b1 [64], W2 [64][64],
+ * b2, W3 [64][64], b3, W4 [32][64], b4 [32]; weight[out][in] row-major.
+ * x: [n][16] f32 rows (device), rounded to bf16 as the kernels read them.
+ * dr_mlp_forward writes the logits [n][32].  dr_mlp_gradient overwrites
+ * grads with the gradient of  sum_rows sum_s -t[s] log softmax(z)[s] / T  (T
+ * the sum of all targets) and *loss with that loss.  Both synchronize the
+ * stream; they allocate their own scratch. */
+DR_API int dr_mlp_param_count(void);
+DR_API dr_status dr_mlp_forward(const float *params_dev, const float *x_dev, int64_t n, float *logits_dev,
+                                void *stream);
+DR_API dr_status dr_mlp_gradient(const float *params_dev, const float *x_dev, const float *targets_dev, int64_t n,
+                                 float *grads_dev, float *loss_dev, void *stream);
+
 #ifdef __cplusplus
 }
 #endif
