@@ -68,6 +68,12 @@ DR_DP_SUM = 1
 DR_FLAG_FULL_PIXEL_JITTER = 1
 DR_FLAG_DETACHED_PDF = 2
 DR_FLAG_EDGE_LOBE_MIS = 4
+DR_FLAG_LEARNED_PROPOSAL = 8
+
+
+class dr_proposal_desc(C.Structure):
+    _fields_ = [("train", C.c_int), ("mix", C.c_float), ("learning_rate", C.c_float), ("train_points", C.c_int64),
+                ("params", C.c_void_p)]
 
 
 def render_desc(width, height, spp, max_bounces, seed, primary_edge_samples=0,

@@ -18,6 +18,7 @@
 #include <map>
 #include <memory>
 #include <mutex>
+#include <random>
 #include <stdexcept>
 #include <string>
 #include <tuple>
@@ -148,6 +149,19 @@ std::shared_ptr<DevBuf> device_ltc(int device, int slot, const std::vector<float
 
 using namespace drhost;
 
+// The learned edge proposal of a scene: network parameters with their Adam
+// moments, and the per-call buffers (features, slot probabilities, training
+// rows and targets).
+struct ProposalState {
+    int train = 1;
+    float alpha = 0.5f, lr = 1e-3f;
+    long long train_points = 32768;
+    long long steps = 0;
+    float last_loss = 0.f;
+    DevBuf params, m, v, grads, img, loss, total, status;
+    DevBuf x, xt, q, targets;
+};
+
 struct dr_scene {
     int device = 0;
     HostScene h;
@@ -156,6 +170,8 @@ struct dr_scene {
         nrm_nodes, nrm_edges, status, bvh_scratch;
     std::shared_ptr<DevBuf> ltc, ltc_ggx;
     std::unique_ptr<BackwardQueues> queues;  // taken at the first backward call
+    std::unique_ptr<ProposalState> proposal;  // set by dr_scene_set_proposal
+    float3 lo, hi;                            // scene bounds
     DevScene ds;
     StageTimer timer;
     bool timer_ready = false;
@@ -179,6 +195,8 @@ void upload_scene(dr_scene *sc, cudaStream_t st, bool refit = false) {
     FlatScene f;
     flatten(h, f);
     sc->num_vertices = (int)(f.vtx.size() / 3);
+    sc->lo = f.lo;
+    sc->hi = f.hi;
     sc->num_tris = (int)f.tri.size();
     sc->vtx.upload(f.vtx);
     sc->nrm.upload(f.nrm);
@@ -307,7 +325,8 @@ void check_render_desc(const dr_scene *sc, const dr_render_desc *rd) {
         throw DrError(DR_ERR_INVALID_ARGUMENT, "width * height * spp must be below 2^31 per call");
     for (int i = 0; i < 7; i++)
         if (rd->reserved[i] != 0) throw DrError(DR_ERR_INVALID_ARGUMENT, "reserved fields must be zero");
-    if (rd->flags & ~(int)(DR_FLAG_FULL_PIXEL_JITTER | DR_FLAG_DETACHED_PDF | DR_FLAG_EDGE_LOBE_MIS))
+    if (rd->flags &
+        ~(int)(DR_FLAG_FULL_PIXEL_JITTER | DR_FLAG_DETACHED_PDF | DR_FLAG_EDGE_LOBE_MIS | DR_FLAG_LEARNED_PROPOSAL))
         throw DrError(DR_ERR_INVALID_ARGUMENT, "unknown render flags");
     if (rd->max_bounces > 64) throw DrError(DR_ERR_NOT_SUPPORTED, "max_bounces above 64");
     if (sc->ds.num_lights == 0) throw DrError(DR_ERR_INVALID_ARGUMENT, "scene has no lights");
@@ -346,7 +365,8 @@ long long initial_point_cap(const dr_scene *scene, const dr_render_desc *rd, dou
 template <class Grow, class GrowPoints>
 std::pair<long long, long long> run_backward(dr_scene *scene, const dr_render_desc *rd, const float *d_image_dev,
                                              float *grad_dev, float *image_dev, BackwardWorkspace &ws,
-                                             cudaStream_t st, StageTimer *timer, Grow grow, GrowPoints grow_points) {
+                                             cudaStream_t st, StageTimer *timer, Grow grow, GrowPoints grow_points,
+                                             ProposalState *prop = nullptr) {
     const DevScene ds = call_scene(scene, rd);
     const GradCacheCfg cfg = grad_cache_cfg(scene->h);
     BackwardCounters c;
@@ -368,7 +388,8 @@ std::pair<long long, long long> run_backward(dr_scene *scene, const dr_render_de
         ws.pt_end = ws.cap_points;
         check_cuda(dr_launch_backward_front(ds, rd->width, rd->height, rd->spp, rd->max_bounces, rd->seed,
                                             d_image_dev, grad_dev, image_dev, rd->primary_edge_samples, rd->dp_mode,
-                                            ws, cfg, scene->num_sms, st, &scene->last_launches, timer),
+                                            ws, cfg, scene->num_sms, st, &scene->last_launches, timer,
+                                            prop == nullptr),
                    "backward launch");
         read();
         if (!(c.status & DR_STATUS_POINT_OVERFLOW)) break;
@@ -378,6 +399,41 @@ std::pair<long long, long long> run_backward(dr_scene *scene, const dr_render_de
                                                     std::to_string(ws.cap_points) + ")");
     }
     const long long P = std::min((long long)c.points, ws.cap_points);
+    if (prop) {
+        // the proposal: features and slot probabilities of every point, then
+        // the traversal that draws edges with them
+        ProposalState &pr = *prop;
+        pr.x.reserve(sizeof(uint16_t) * 16 * (size_t)std::max(P, 1ll));
+        pr.q.reserve(sizeof(uint16_t) * 32 * (size_t)std::max(P, 1ll));
+        ws.proposal_q = pr.q.as<uint16_t>();
+        ws.proposal_alpha = pr.alpha;
+        ws.train_stride = 1;
+        ws.train_n = 0;
+        if (pr.train) {
+            ws.train_stride = std::max(1ll, P / std::max(1ll, pr.train_points));
+            ws.train_n = std::min(pr.train_points, (P + ws.train_stride - 1) / ws.train_stride);
+            pr.xt.reserve(sizeof(uint16_t) * 16 * (size_t)std::max(ws.train_n, 1ll));
+            pr.targets.reserve(sizeof(float) * 32 * (size_t)std::max(ws.train_n, 1ll));
+            check_cuda(cudaMemsetAsync(pr.targets.p, 0, sizeof(float) * 32 * (size_t)ws.train_n, st), "memset");
+            ws.train_targets = pr.targets.as<float>();
+        }
+        float3 ctr = (scene->lo + scene->hi) * 0.5f, ext = (scene->hi - scene->lo) * 0.5f;
+        float3 ih = f3(ext.x > 0.f ? 1.f / ext.x : 0.f, ext.y > 0.f ? 1.f / ext.y : 0.f, ext.z > 0.f ? 1.f / ext.z : 0.f);
+        check_cuda(cudaMemsetAsync(pr.status.p, 0, sizeof(int), st), "memset");
+        check_cuda(dr_launch_proposal_features(ds, ws, P, ctr, ih, pr.x.p, pr.train ? pr.xt.p : nullptr, st),
+                   "proposal features");
+        check_cuda(dr_mlp_infer(pr.img.as<uint8_t>(), pr.params.as<float>(), pr.x.as<__nv_bfloat16>(), P, nullptr,
+                                pr.q.as<__nv_bfloat16>(), pr.status.as<int>(), scene->num_sms, st),
+                   "proposal inference");
+        timer->mark(st, "k_mlp_infer");
+        scene->last_launches += 2;
+        check_cuda(dr_launch_edge_traverse(ds, rd->seed, ws, scene->num_sms, st, &scene->last_launches, timer),
+                   "edge traversal launch");
+        read();
+        int mst = 0;
+        check_cuda(cudaMemcpy(&mst, pr.status.p, sizeof(int), cudaMemcpyDeviceToHost), "status read");
+        if (mst) throw DrError(DR_ERR_DEVICE_STATUS, "proposal network reported status " + std::to_string(mst));
+    }
     long long items = 0;
     if (!(c.status & DR_STATUS_ITEM_OVERFLOW)) {
         timer->mark(st, "host_queue_check");
@@ -411,6 +467,31 @@ std::pair<long long, long long> run_backward(dr_scene *scene, const dr_render_de
             items += (long long)c.items;
             p0 = p1;
         }
+    }
+    if (prop && prop->train && ws.train_n > 0) {
+        // one training step on the contribution magnitudes the edges reported
+        ProposalState &pr = *prop;
+        check_cuda(dr_mlp_sum(pr.targets.as<float>(), ws.train_n * 32, pr.total.as<float>(), st), "target sum");
+        check_cuda(cudaMemsetAsync(pr.grads.p, 0, sizeof(float) * kMlpParams, st), "memset");
+        check_cuda(cudaMemsetAsync(pr.loss.p, 0, sizeof(float), st), "memset");
+        check_cuda(dr_mlp_grad(pr.img.as<uint8_t>(), pr.params.as<float>(), pr.xt.as<__nv_bfloat16>(),
+                               pr.targets.as<float>(), ws.train_n, pr.total.as<float>(), pr.grads.as<float>(),
+                               pr.loss.as<float>(), pr.status.as<int>(), scene->num_sms, st),
+                   "proposal gradient");
+        timer->mark(st, "k_mlp_grad");
+        check_cuda(dr_mlp_adam(pr.params.as<float>(), pr.grads.as<float>(), pr.m.as<float>(), pr.v.as<float>(),
+                               (int)(pr.steps + 1), pr.lr, st),
+                   "proposal update");
+        check_cuda(dr_mlp_pack(pr.params.as<float>(), pr.img.as<uint8_t>(), st), "weight pack");
+        scene->last_launches += 4;
+        float loss = 0.f;
+        int mst = 0;
+        check_cuda(cudaMemcpyAsync(&loss, pr.loss.p, sizeof(float), cudaMemcpyDeviceToHost, st), "loss read");
+        check_cuda(cudaMemcpyAsync(&mst, pr.status.p, sizeof(int), cudaMemcpyDeviceToHost, st), "status read");
+        check_cuda(cudaStreamSynchronize(st), "proposal training");
+        if (mst) throw DrError(DR_ERR_DEVICE_STATUS, "proposal network reported status " + std::to_string(mst));
+        pr.last_loss = loss;
+        pr.steps++;
     }
     check_cuda(cudaStreamSynchronize(st), "backward");
     return {P, items};
@@ -539,7 +620,7 @@ dr_status dr_render_backward(dr_scene *scene, const dr_render_desc *rd, const fl
             cudaStream_t st;
             ~MarkIdle() { cudaEventRecord(e, st); }
         } mark_idle{q.idle, st};
-        BackwardWorkspace ws;
+        BackwardWorkspace ws{};
         auto bind_items = [&]() {
             q.items.reserve(sizeof(int4) * cap_items);
             q.item_w.reserve(sizeof(float) * cap_items);
@@ -578,8 +659,14 @@ dr_status dr_render_backward(dr_scene *scene, const dr_render_desc *rd, const fl
             bind_points();
             return cap_points;
         };
-        auto counts =
-            run_backward(scene, rd, d_image_dev, grad_dev, image_dev, ws, st, &scene->timer, grow, grow_points);
+        ProposalState *prop = nullptr;
+        if (rd->flags & DR_FLAG_LEARNED_PROPOSAL) {
+            if (!scene->proposal)
+                throw DrError(DR_ERR_INVALID_ARGUMENT, "DR_FLAG_LEARNED_PROPOSAL without dr_scene_set_proposal");
+            prop = scene->proposal.get();
+        }
+        auto counts = run_backward(scene, rd, d_image_dev, grad_dev, image_dev, ws, st, &scene->timer, grow,
+                                   grow_points, prop);
         scene->last_points = counts.first;
         scene->last_items = counts.second;
         collect_timings(scene, st);
@@ -587,6 +674,66 @@ dr_status dr_render_backward(dr_scene *scene, const dr_render_desc *rd, const fl
 }
 
 int dr_mlp_param_count(void) { return kMlpParams; }
+
+dr_status dr_scene_set_proposal(dr_scene *scene, const dr_proposal_desc *d) {
+    return guard([&]() {
+        if (!scene || !d) throw DrError(DR_ERR_INVALID_ARGUMENT, "scene and desc must be non-NULL");
+        if (!(d->mix >= 0.f && d->mix <= 1.f)) throw DrError(DR_ERR_INVALID_ARGUMENT, "mix must lie in [0, 1]");
+        if (!(d->learning_rate >= 0.f)) throw DrError(DR_ERR_INVALID_ARGUMENT, "learning_rate must be >= 0");
+        check_cuda(cudaSetDevice(scene->device), "cudaSetDevice");
+        bool fresh = !scene->proposal;
+        if (fresh) {
+            auto pr = std::make_unique<ProposalState>();
+            for (DevBuf *b : {&pr->params, &pr->m, &pr->v, &pr->grads}) b->reserve(sizeof(float) * kMlpParams);
+            pr->img.reserve(kImgBytes);
+            pr->loss.reserve(sizeof(float));
+            pr->total.reserve(sizeof(float));
+            pr->status.reserve(sizeof(int));
+            scene->proposal = std::move(pr);
+        }
+        ProposalState &pr = *scene->proposal;
+        pr.train = d->train != 0;
+        pr.alpha = d->mix;
+        pr.lr = d->learning_rate;
+        pr.train_points = d->train_points > 0 ? (long long)d->train_points : 32768;
+        if (d->params || fresh) {
+            std::vector<float> p(kMlpParams);
+            if (d->params) {
+                p = fetch(d->params, kMlpParams, "params");
+            } else {  // nn.Linear's initialisation, W1 with the 10 real inputs as fan-in
+                std::mt19937 gen(0);
+                std::uniform_real_distribution<float> u(-1.f, 1.f);
+                const int ends[8] = {kMlpB1, kMlpW2, kMlpB2, kMlpW3, kMlpB3, kMlpW4, kMlpB4, kMlpParams};
+                for (int i = 0, blk = 0; i < kMlpParams; i++) {
+                    while (i >= ends[blk]) blk++;
+                    float fan = blk < 2 ? (float)DR_MLP_FEATURES : (float)DR_MLP_HIDDEN;
+                    p[i] = u(gen) / std::sqrt(fan);
+                }
+            }
+            pr.params.upload(p);
+            check_cuda(cudaMemset(pr.m.p, 0, sizeof(float) * kMlpParams), "memset");
+            check_cuda(cudaMemset(pr.v.p, 0, sizeof(float) * kMlpParams), "memset");
+            pr.steps = 0;
+            pr.last_loss = 0.f;
+            check_cuda(dr_mlp_pack(pr.params.as<float>(), pr.img.as<uint8_t>(), 0), "weight pack");
+            check_cuda(cudaDeviceSynchronize(), "weight pack");
+        }
+    });
+}
+
+dr_status dr_scene_proposal_state(const dr_scene *scene, float *params_out, float *last_loss, int64_t *steps) {
+    return guard([&]() {
+        if (!scene) throw DrError(DR_ERR_INVALID_ARGUMENT, "scene is NULL");
+        if (!scene->proposal) throw DrError(DR_ERR_INVALID_ARGUMENT, "the scene has no proposal");
+        check_cuda(cudaSetDevice(scene->device), "cudaSetDevice");
+        const ProposalState &pr = *scene->proposal;
+        if (params_out)
+            check_cuda(cudaMemcpy(params_out, pr.params.p, sizeof(float) * kMlpParams, cudaMemcpyDefault),
+                       "params read");
+        if (last_loss) *last_loss = pr.last_loss;
+        if (steps) *steps = pr.steps;
+    });
+}
 
 namespace {
 // Device buffers of one network call: bf16 rows, packed weights, status word.
@@ -757,6 +904,8 @@ dr_status dr_render_backward_noalloc(dr_scene *scene, const dr_render_desc *rd, 
     return guard([&]() {
         check_backward_args(scene, rd, d_image_dev, grad_dev);
         long long npix = (long long)rd->width * rd->height * rd->spp;
+        if (rd->flags & DR_FLAG_LEARNED_PROPOSAL)
+            throw DrError(DR_ERR_NOT_SUPPORTED, "the no-alloc backward does not run the learned proposal");
         if (npix > kNoAllocMaxSamples)
             throw DrError(DR_ERR_INVALID_ARGUMENT,
                           "width * height * spp = " + std::to_string(npix) + " exceeds the " +
@@ -777,7 +926,7 @@ dr_status dr_render_backward_noalloc(dr_scene *scene, const dr_render_desc *rd, 
             cap_points = std::max(npix, std::min(want, fit));
         }
         size_t off = 256;
-        BackwardWorkspace ws;
+        BackwardWorkspace ws{};
         ws.counters = (BackwardCounters *)base;
         ws.pt = (float *)(base + off);
         off += up(sizeof(float) * DR_PT_FLOATS * (size_t)cap_points);

@@ -118,7 +118,7 @@ int path_lanes_log2(int spp) {
 cudaError_t dr_launch_backward_front(const DevScene &s, int W, int H, int spp, int B, uint64_t seed,
                                      const float *d_image, float *grad, float *img, long long primary_edge_samples,
                                      int dp_mode, const BackwardWorkspace &ws, const GradCacheCfg &cfg, int num_sms,
-                                     cudaStream_t st, int *launches, StageTimer *timer) {
+                                     cudaStream_t st, int *launches, StageTimer *timer, bool traverse) {
     const int bs = 128;
     size_t smem = sizeof(float) * (size_t)(cfg.head + cfg.tail_len);
     int lanes_log2 = path_lanes_log2(spp);
@@ -145,6 +145,7 @@ cudaError_t dr_launch_backward_front(const DevScene &s, int W, int H, int spp, i
         timer->mark(st, "k_primary_edges");
         *launches += 1;
     }
+    if (!traverse) return cudaGetLastError();
     return dr_launch_edge_traverse(s, seed, ws, num_sms, st, launches, timer);
 }
 

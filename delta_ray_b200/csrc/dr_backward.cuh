@@ -512,27 +512,29 @@ DEV ConeSpec light_cone(const DevScene &s, int li, float3 p) {
     return c;
 }
 
-// Samples the point's edges; emit(tree, edge_index, j, weight) for every
-// sampled edge of nonzero weight, j counting all sampled edges in order.
+// Samples the point's edges; emit(tree, edge_index, j, weight, slot_code) for
+// every sampled edge of nonzero weight, j counting all sampled edges in order.
 template <class Emit>
-DEV bool traverse_point(const DevScene &s, const PointRecord &pt, uint64_t seed, Emit &emit) {
+DEV bool traverse_point(const DevScene &s, const PointRecord &pt, uint64_t seed, Emit &emit,
+                        const EdgeProposal &pr) {
     Rng prng;
     prng.init(seed, kStreamEdgePoint, pt.sid, (uint32_t)pt.bounce);
     draw_edge(prng);  // the point's edge sample; eval_item redraws it
     SurfacePoint sp = pt.surface();
     ConeSpec cone = light_cone(s, pt.light, sp.p);
     int j = 0;
-    auto em = [&](int tree, int ei, float w) {
-        if (w != 0.f) emit(tree, ei, j, w);
+    auto em = [&](int tree, int ei, float w, int code) {
+        if (w != 0.f) emit(tree, ei, j, w, code);
         j++;
     };
-    return traverse_edges(s, pt.wi, pt.tri, sp, cone, prng, em);
+    return traverse_edges(s, pt.wi, pt.tri, sp, cone, prng, em, pr);
 }
 
-// One sampled edge (delta_ray.cpp:901-973); returns dp, scatters dv0 / dv1.
+// One sampled edge (delta_ray.cpp:901-973); returns dp, scatters dv0 / dv1;
+// *mag (if given) receives the sample's contribution magnitude |dv0|_1 + |dv1|_1.
 template <class G>
 DEV float3 eval_item(const DevScene &s, const PointRecord &pt, int tree, int ei, int j, float w, int spp, int B,
-                     uint64_t seed, G &g) {
+                     uint64_t seed, G &g, float *mag = nullptr) {
     Rng prng;
     prng.init(seed, kStreamEdgePoint, pt.sid, (uint32_t)pt.bounce);
     EdgeSample es = draw_edge(prng);
@@ -543,6 +545,7 @@ DEV float3 eval_item(const DevScene &s, const PointRecord &pt, int tree, int ei,
     float3 weight = f3(1.f) * ((1.f / spp) * w);
     EdgeResult er = shading_edge_sample(s, es, edge, els, irng, B - pt.bounce - 1, pt.wi, pt.tri, pt.surface(),
                                         weight, pt.d_color, B == 1);
+    if (mag) *mag = abs_sum(er.dv0) + abs_sum(er.dv1);
     if (!is_zero(er.dv0) || !is_zero(er.dv1)) {
         const DevShape &sh = s.shapes[edge.shape];
         g.add(sh.grad_v + 3 * edge.v0 + 0, er.dv0.x);

@@ -6,6 +6,8 @@
 #include "dr_backward.cuh"
 #include "dr_block_grad.cuh"
 
+#include <cuda_bf16.h>
+
 #define DR_ITEM_BUF 24
 // One thread per shading point in [pt_begin, pt_end).  A point's items collect
 // in a lane buffer; a full buffer reserves DR_ITEM_BUF slots with one atomic
@@ -23,6 +25,7 @@ __global__ void __launch_bounds__(128, 4) k_edge_traverse(DevScene s, uint64_t s
         int buf_e[DR_ITEM_BUF];
         float buf_w[DR_ITEM_BUF];
         int buf_j[DR_ITEM_BUF];
+        uint8_t buf_c[DR_ITEM_BUF];
         int nb = 0;
         auto write_items = [&](unsigned long long first, int cnt) {
             unsigned long long cap = (unsigned long long)ws.cap_items;
@@ -34,7 +37,7 @@ __global__ void __launch_bounds__(128, 4) k_edge_traverse(DevScene s, uint64_t s
                 it.x = (int)p;
                 it.y = buf_e[k];
                 it.z = buf_j[k];
-                it.w = 0;
+                it.w = buf_c[k];
                 ws.items[i] = it;
                 ws.item_w[i] = buf_w[k];
             }
@@ -42,7 +45,7 @@ __global__ void __launch_bounds__(128, 4) k_edge_traverse(DevScene s, uint64_t s
         if (active) {
             PointRecord pt;
             pt.load(ws.pt + (size_t)p * DR_PT_WORDS);
-            auto emit = [&](int tree, int ei, int j, float w) {
+            auto emit = [&](int tree, int ei, int j, float w, int code) {
                 if (nb == DR_ITEM_BUF) {
                     write_items(atomicAdd(count, (unsigned long long)DR_ITEM_BUF), DR_ITEM_BUF);
                     nb = 0;
@@ -50,9 +53,13 @@ __global__ void __launch_bounds__(128, 4) k_edge_traverse(DevScene s, uint64_t s
                 buf_e[nb] = (tree << 30) | ei;
                 buf_j[nb] = j;
                 buf_w[nb] = w;
+                buf_c[nb] = (uint8_t)code;
                 nb++;
             };
-            if (!traverse_point(s, pt, seed, emit)) set_status(&ws.counters->status, DR_STATUS_STACK_OVERFLOW);
+            EdgeProposal pr;
+            pr.q = ws.proposal_q ? ws.proposal_q + 32 * (size_t)p : nullptr;
+            pr.alpha = ws.proposal_alpha;
+            if (!traverse_point(s, pt, seed, emit, pr)) set_status(&ws.counters->status, DR_STATUS_STACK_OVERFLOW);
         }
         __syncwarp();
         write_items(warp_reserve(count, nb), nb);
@@ -69,7 +76,14 @@ __global__ void __launch_bounds__(128, 4) k_edge_eval(DevScene s, int W, int H, 
         PointRecord pt;
         pt.load(ws.pt + (size_t)it.x * DR_PT_WORDS);
         int tree = it.y >> 30, ei = it.y & ((1 << 30) - 1);
-        float3 dp = eval_item(s, pt, tree, ei, it.z, ws.item_w[i], spp, B, seed, bg);
+        float mag = 0.f;
+        float3 dp = eval_item(s, pt, tree, ei, it.z, ws.item_w[i], spp, B, seed, bg, &mag);
+        if (ws.train_targets && mag > 0.f && it.x % ws.train_stride == 0 && it.x / ws.train_stride < ws.train_n) {
+            // the proposal's training target: contribution magnitude per cut slot
+            int code = it.w, tr = code >> 7, lw = (code >> 4) & 7, lo = code & 15, wdt = 1 << lw;
+            float *t = ws.train_targets + 32 * (size_t)(it.x / ws.train_stride) + 16 * tr + lo;
+            for (int k = 0; k < wdt; k++) atomicAdd(t + k, mag / wdt);
+        }
         if (is_zero(dp)) continue;
         if (dp_mode == DR_DP_SUM) {
             if (pt.bounce == 0) {
@@ -124,5 +138,36 @@ cudaError_t dr_launch_primary_edges(const DevScene &s, int W, int H, int spp, in
     size_t smem = sizeof(float) * (size_t)(cfg.head + cfg.tail_len);
     long long nb = std::min<long long>(blocks_for(n, bs), (long long)stage_grid(num_sms) * 4);
     k_primary_edges<<<(int)nb, bs, smem, st>>>(s, W, H, spp, B, seed, d_image, n, grad, cfg);
+    return cudaGetLastError();
+}
+
+// The learned proposal's inputs of each shading point: position normalised to
+// the scene bounds, shading normal, roughness, incoming direction.
+__global__ void k_proposal_features(DevScene s, BackwardWorkspace ws, long long n, float3 c, float3 ih,
+                                    __nv_bfloat16 *x, __nv_bfloat16 *xt) {
+    long long p = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (p >= n) return;
+    PointRecord pt;
+    pt.load(ws.pt + (size_t)p * DR_PT_WORDS);
+    float rough = get_rough(s, s.mats[material_of_tri(s, pt.tri)], pt.uv);
+    float f[16] = {(pt.p.x - c.x) * ih.x, (pt.p.y - c.y) * ih.y, (pt.p.z - c.z) * ih.z, pt.n.x, pt.n.y, pt.n.z,
+                   rough, pt.wi.x, pt.wi.y, pt.wi.z, 0.f, 0.f, 0.f, 0.f, 0.f, 0.f};
+    __nv_bfloat162 h[8];
+    for (int k = 0; k < 8; k++) h[k] = __floats2bfloat162_rn(f[2 * k], f[2 * k + 1]);
+    uint4 *dst = reinterpret_cast<uint4 *>(x + 16 * (size_t)p);
+    dst[0] = reinterpret_cast<uint4 *>(h)[0];
+    dst[1] = reinterpret_cast<uint4 *>(h)[1];
+    if (xt && p % ws.train_stride == 0 && p / ws.train_stride < ws.train_n) {
+        uint4 *dt = reinterpret_cast<uint4 *>(xt + 16 * (size_t)(p / ws.train_stride));
+        dt[0] = reinterpret_cast<uint4 *>(h)[0];
+        dt[1] = reinterpret_cast<uint4 *>(h)[1];
+    }
+}
+
+cudaError_t dr_launch_proposal_features(const DevScene &s, const BackwardWorkspace &ws, long long n, float3 c,
+                                        float3 ih, void *x, void *xt, cudaStream_t st) {
+    if (n <= 0) return cudaSuccess;
+    k_proposal_features<<<(unsigned)((n + 127) / 128), 128, 0, st>>>(s, ws, n, c, ih, (__nv_bfloat16 *)x,
+                                                                      (__nv_bfloat16 *)xt);
     return cudaGetLastError();
 }

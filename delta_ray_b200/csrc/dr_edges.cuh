@@ -229,31 +229,59 @@ DEV bool node_inside(const DevEdgeNode &n, float3 p) {
     return p.x >= n.lo[0] && p.x <= n.hi[0] && p.y >= n.lo[1] && p.y <= n.hi[1] && p.z >= n.lo[2] && p.z <= n.hi[2];
 }
 
+// The learned edge proposal of one shading point (a project addition): 32
+// bf16 probabilities over the depth-4 cut of the silhouette tree (slots
+// 0..15) and of the normal tree (16..31).  A subtree above the cut owns the
+// slots of its descendants at depth 4; a leaf above the cut owns a range.
+// q == null: the reference's sampling.
+struct EdgeProposal {
+    const uint16_t *q;
+    float alpha;  // probability of the learned descent in the defensive mixture
+};
+HD float bf16_bits_to_float(uint16_t b) { return dr_i2f((int)((uint32_t)b << 16)); }
+DEV float slot_mass(const uint16_t *q, int tree, int lo, int n) {
+    float m = 0.f;
+    for (int k = 0; k < n; k++) m += bf16_bits_to_float(q[16 * tree + lo + k]);
+    return m;
+}
+// slot range code of an item: lo | log2(width) << 4 | tree << 7
+HD int slot_code(int tree, int lo, int lw) { return lo | (lw << 4) | (tree << 7); }
+
 // Stochastic traversal of one edge tree in one mode (edge_tree.cpp:511-652).
-// emit(tree_edge_index, weight) is called for every silhouette edge of every
-// reached leaf, in the reference's order.  Returns false if the stack limit
-// was hit (never for trees of depth < DR_EDGE_STACK).
+// emit(tree_edge_index, weight, slot_code) is called for every silhouette
+// edge of every reached leaf, in the reference's order.  Returns false if the
+// stack limit was hit (never for trees of depth < DR_EDGE_STACK).
+//
+// With a proposal, the "all" mode becomes a defensive mixture: `learned`
+// (drawn once per traversal, probability alpha) picks the child at each
+// stochastic node above the cut by the proposal's slot masses, otherwise by
+// the tree's importance.  Every node tracks both path products (apmf plain,
+// lpmf learned), so the mixture's pmf alpha lpmf + (1 - alpha) apmf takes the
+// place of the all-mode pmf in the multiple-importance weights of both modes.
 #define DR_EDGE_STACK 64
 template <bool CONE, class Emit>
 DEV bool traverse_mode(const DevScene &s, const DevEdgeNode *nodes, const DevEdge *edges, bool dir_bounds, float3 wi,
                        const SurfacePoint &sp, float dl, float sl, float rough, int model, const ConeSpec &cone,
-                       float root_bb,
-                       float pmf, Rng &rng, Emit &emit) {
-    struct Item { int node; float bb, cpmf, apmf; };
+                       float root_bb, float pmf, Rng &rng, Emit &emit, const EdgeProposal &pr, int tree,
+                       bool learned) {
+    struct Item { int node; float bb, cpmf, apmf, lpmf; int slot; };  // slot: lo | log2(width) << 4
     Item st[DR_EDGE_STACK];
     int sp_ = 0;
-    st[sp_++] = Item{0, root_bb, pmf, pmf};
+    st[sp_++] = Item{0, root_bb, pmf, pmf, pmf, 4 << 4};
     bool ok = true;
     while (sp_ > 0) {
         Item it = st[--sp_];
         if (it.bb <= 0.f) continue;
         const DevEdgeNode &node = nodes[it.node];
         if (node.nprims > 0) {
-            float denom = it.cpmf * it.cpmf + it.apmf * it.apmf;
-            float w = CONE ? it.cpmf / denom : it.apmf / denom;
+            float apmf = it.apmf;
+            if (pr.q) apmf = pr.alpha * it.lpmf + (1.f - pr.alpha) * it.apmf;
+            float denom = it.cpmf * it.cpmf + apmf * apmf;
+            float w = CONE ? it.cpmf / denom : apmf / denom;
+            int code = it.slot | (tree << 7);
             for (int i = 0; i < node.nprims; i++) {
                 int ei = node.offset + i;
-                if (is_silhouette(s, sp.p, edges[ei])) emit(ei, w);
+                if (is_silhouette(s, sp.p, edges[ei])) emit(ei, w, code);
             }
             continue;
         }
@@ -287,8 +315,22 @@ DEV bool traverse_mode(const DevScene &s, const DevEdgeNode *nodes, const DevEdg
             pla = il / (il + ir);
             pra = 1.f - pla;
         }
+        // the proposal's choice above the cut (both children important, no split)
+        float pll = pla, prl = pra;
+        int lw = it.slot >> 4, lo = it.slot & 15;
+        if (pr.q && !all_split && lw > 0 && il > 0.f && ir > 0.f) {
+            int h = 1 << (lw - 1);
+            float ql = slot_mass(pr.q, tree, lo, h), qr = slot_mass(pr.q, tree, lo + h, h);
+            if (ql + qr > 0.f) {
+                pll = ql / (ql + qr);
+                prl = 1.f - pll;
+            }
+        }
+        int lslot = lw > 0 ? (lo | ((lw - 1) << 4)) : it.slot;
+        int rslot = lw > 0 ? ((lo + (1 << (lw - 1))) | ((lw - 1) << 4)) : it.slot;
         bool split = CONE ? cone_split : all_split;
-        Item left{li, lbb, plc * it.cpmf, pla * it.apmf}, right{ri, rbb, prc * it.cpmf, pra * it.apmf};
+        Item left{li, lbb, plc * it.cpmf, pla * it.apmf, pll * it.lpmf, lslot},
+            right{ri, rbb, prc * it.cpmf, pra * it.apmf, prl * it.lpmf, rslot};
         if (split) {
             if (sp_ + 2 > DR_EDGE_STACK) {
                 ok = false;
@@ -299,7 +341,7 @@ DEV bool traverse_mode(const DevScene &s, const DevEdgeNode *nodes, const DevEdg
             if (lcs) st[sp_++] = left;
         } else {
             float u = rng.next();
-            bool go_left = CONE ? u < plc : u < pla;
+            bool go_left = CONE ? u < plc : u < (learned ? pll : pla);
             if (sp_ + 1 > DR_EDGE_STACK) {
                 ok = false;
                 continue;
@@ -314,7 +356,7 @@ DEV bool traverse_mode(const DevScene &s, const DevEdgeNode *nodes, const DevEdg
 // emit(tree, edge_index, weight); tree 0 = silhouette tree, 1 = normal tree.
 template <class Emit>
 DEV bool traverse_edges(const DevScene &s, float3 wi, int stri, const SurfacePoint &sp, const ConeSpec &cone, Rng &rng,
-                        Emit &emit) {
+                        Emit &emit, const EdgeProposal &pr) {
     if (dot(wi, sp.f.n) < 0.f) return true;
     int tree;
     float pmf = 1.f;
@@ -326,6 +368,12 @@ DEV bool traverse_edges(const DevScene &s, float3 wi, int stri, const SurfacePoi
     } else {
         float ni = s.nrm_nodes[0].total_length, si = s.sil_nodes[0].total_length;
         float np = ni / (ni + si), spm = si / (ni + si);
+        if (pr.q) {  // the tree pick mixed with the proposal's tree masses
+            float qn = slot_mass(pr.q, 1, 0, 16), qs = slot_mass(pr.q, 0, 0, 16);
+            float qt = qn + qs > 0.f ? qn / (qn + qs) : np;
+            np = pr.alpha * qt + (1.f - pr.alpha) * np;
+            spm = 1.f - np;
+        }
         float u = rng.next();
         if (u < np) {
             tree = 1;
@@ -341,9 +389,12 @@ DEV bool traverse_edges(const DevScene &s, float3 wi, int stri, const SurfacePoi
     float dl = luminance(get_kd(s, m, sp.uv)), sl = luminance(get_ks(s, m, sp.uv));
     float rough = get_rough(s, m, sp.uv);
     float b = bsdf_bound(nodes[0], wi, sp, dl, sl, rough, m.model);
-    auto em = [&](int ei, float w) { emit(tree, ei, w); };
-    bool ok = traverse_mode<true>(s, nodes, edges, tree == 1, wi, sp, dl, sl, rough, m.model, cone, b, pmf, rng, em);
-    ok &= traverse_mode<false>(s, nodes, edges, tree == 1, wi, sp, dl, sl, rough, m.model, cone, b, pmf, rng, em);
+    auto em = [&](int ei, float w, int code) { emit(tree, ei, w, code); };
+    bool ok = traverse_mode<true>(s, nodes, edges, tree == 1, wi, sp, dl, sl, rough, m.model, cone, b, pmf, rng, em,
+                                  pr, tree, false);
+    bool learned = pr.q ? rng.next() < pr.alpha : false;
+    ok &= traverse_mode<false>(s, nodes, edges, tree == 1, wi, sp, dl, sl, rough, m.model, cone, b, pmf, rng, em, pr,
+                               tree, learned);
     return ok;
 }
 

@@ -67,6 +67,14 @@ struct BackwardWorkspace {
     // points [pt_begin, min(pt_end, counters->points)) go through the edge
     // stage (k_edge_traverse, k_edge_eval, k_dp_propagate) of one launch
     long long pt_begin, pt_end;
+    // learned edge proposal (null: the reference's sampling): [cap_points][32]
+    // bf16 slot probabilities, the mixture weight, and the training targets of
+    // points p = k * train_stride, k < train_n ([train_n][32] f32 contribution
+    // magnitudes per slot)
+    const uint16_t *proposal_q;
+    float proposal_alpha;
+    float *train_targets;
+    long long train_stride, train_n;
 };
 
 // Which part of the flat gradient a block caches in shared memory:
@@ -83,7 +91,13 @@ struct GradCacheCfg {
 cudaError_t dr_launch_backward_front(const DevScene &s, int W, int H, int spp, int B, uint64_t seed,
                                      const float *d_image, float *grad, float *img, long long primary_edge_samples,
                                      int dp_mode, const BackwardWorkspace &ws, const GradCacheCfg &cfg, int num_sms,
-                                     cudaStream_t st, int *launches, StageTimer *timer);
+                                     cudaStream_t st, int *launches, StageTimer *timer, bool traverse = true);
+// Features of the learned edge proposal for points [0, n): x[n][16] bf16
+// (position normalised by the scene centre c and inverse half extent ih,
+// shading normal, roughness, incoming direction, zeros); points
+// p = k * train_stride (k < train_n) are also written to xt[k].
+cudaError_t dr_launch_proposal_features(const DevScene &s, const BackwardWorkspace &ws, long long n, float3 c,
+                                        float3 ih, void *x, void *xt, cudaStream_t st);
 cudaError_t dr_launch_edge_traverse(const DevScene &s, uint64_t seed, const BackwardWorkspace &ws, int num_sms,
                                     cudaStream_t st, int *launches, StageTimer *timer);
 // Single-kernel launchers of the edge half (dr_edge_kernels.cu).

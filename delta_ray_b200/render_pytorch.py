@@ -42,6 +42,8 @@ class RenderOptions:
     detached_pdf: hold the BSDF sampling pdf constant in the backward pass
         (unbiased gradients of roughness and lobe weights) instead of
         differentiating it at a fixed sampled direction as the reference does.
+    learned_proposal: draw secondary edges with the scene's learned proposal
+        (Scene.set_proposal) and, in its training mode, train it on this call.
     edge_lobe_mis: divide a secondary-edge sample by the two lobes' mixture
         density at the sampled point (balance heuristic).  The reference
         divides by the picked lobe's pick probability times its line pdf,
@@ -51,12 +53,13 @@ class RenderOptions:
 
     def __init__(self, primary_edge_samples=0, dp_mode=_abi.DR_DP_REFERENCE_LAST, ltc_table="fitted",
                  output_device=None, device=None, full_pixel_jitter=False, ltc_table_ggx="fitted",
-                 detached_pdf=False, edge_lobe_mis=False):
+                 detached_pdf=False, edge_lobe_mis=False, learned_proposal=False):
         self.primary_edge_samples = int(primary_edge_samples)
         self.dp_mode = int(dp_mode)
         self.flags = (_abi.DR_FLAG_FULL_PIXEL_JITTER if full_pixel_jitter else 0) | \
             (_abi.DR_FLAG_DETACHED_PDF if detached_pdf else 0) | \
-            (_abi.DR_FLAG_EDGE_LOBE_MIS if edge_lobe_mis else 0)
+            (_abi.DR_FLAG_EDGE_LOBE_MIS if edge_lobe_mis else 0) | \
+            (_abi.DR_FLAG_LEARNED_PROPOSAL if learned_proposal else 0)
         self.ltc_table = ltc_table
         self.ltc_table_ggx = ltc_table_ggx
         self.output_device = output_device
@@ -149,6 +152,25 @@ class Scene:
                                                 C.c_void_p(tri.data_ptr()), C.c_void_p(t.data_ptr()),
                                                 self._stream()))
         return tri, t
+
+    def set_proposal(self, train=True, mix=0.5, learning_rate=1e-3, train_points=32768, params=None):
+        """Attach (or reconfigure) the scene's learned edge proposal, used by
+        backward calls with RenderOptions(learned_proposal=True).  params:
+        a flat tensor of proposal.param_count() floats (None keeps the
+        current ones; a fixed initialisation the first time)."""
+        p = None if params is None else torch.as_tensor(params, dtype=torch.float32).contiguous()
+        d = _abi.dr_proposal_desc(int(bool(train)), float(mix), float(learning_rate), int(train_points),
+                                  None if p is None else p.data_ptr())
+        _lib.check(_lib.lib().dr_scene_set_proposal(self.handle, C.byref(d)))
+
+    def proposal_state(self):
+        """(parameters [CPU tensor], last training loss, training steps taken)."""
+        from . import proposal
+        p = torch.empty(proposal.param_count(), dtype=torch.float32)
+        loss, steps = C.c_float(), C.c_int64()
+        _lib.check(_lib.lib().dr_scene_proposal_state(self.handle, C.c_void_p(p.data_ptr()), C.byref(loss),
+                                                      C.byref(steps)))
+        return p, float(loss.value), int(steps.value)
 
     def split_grad(self, flat):
         return self.sd.split_grad(flat, self.materials, self.shapes)

@@ -144,11 +144,15 @@ typedef enum { DR_DP_REFERENCE_LAST = 0, DR_DP_SUM = 1 } dr_dp_mode;
  * twice the integral on materials with both lobes. With the flag the sample is
  * divided by the mixture density, the sum over both lobes of pmf * that lobe's
  * line pdf at the sampled point (the one-sample balance heuristic). That is
- * unbiased wherever either lobe can sample the edge. */
+ * unbiased wherever either lobe can sample the edge.
+ * DR_FLAG_LEARNED_PROPOSAL draws secondary edges with the scene's learned
+ * proposal (dr_scene_set_proposal) and, in its training mode, takes one
+ * training step per backward call; see dr_proposal_desc. */
 typedef enum {
     DR_FLAG_FULL_PIXEL_JITTER = 1,
     DR_FLAG_DETACHED_PDF = 2,
-    DR_FLAG_EDGE_LOBE_MIS = 4
+    DR_FLAG_EDGE_LOBE_MIS = 4,
+    DR_FLAG_LEARNED_PROPOSAL = 8
 } dr_render_flags;
 
 typedef struct {
@@ -275,6 +279,33 @@ DR_API size_t dr_last_error(char *buf, size_t len);
  * the sum of all targets) and *loss with that loss.  Both synchronize the
  * stream; they allocate their own scratch. */
 DR_API int dr_mlp_param_count(void);
+
+/* The learned edge proposal of a scene (no counterpart in the reference,
+ * which samples edges by the edge trees' importance alone).  With
+ * DR_FLAG_LEARNED_PROPOSAL a backward call computes, for every shading point,
+ * the network's probabilities over the two edge trees' subtrees at depth 4
+ * from the point's position (normalised to the scene bounds), shading normal,
+ * roughness and incoming direction.  The edge trees' all-mode traversal then
+ * follows those probabilities above the cut with probability `mix` and the
+ * trees' own importance otherwise, a defensive mixture whose exact pmf enters
+ * the reference's multiple-importance weights, so the gradient stays unbiased
+ * for any network.  In training mode each such call sums the contribution
+ * magnitude |dv0| + |dv1| of every sampled edge per subtree for
+ * `train_points` shading points spread over the call's points and takes one
+ * Adam step on  sum -t log q / sum t  (t the magnitudes, q the network's
+ * probabilities). */
+typedef struct {
+    int train;             /* 1: one training step per backward call that uses the proposal */
+    float mix;             /* probability of the learned descent, in [0, 1] */
+    float learning_rate;   /* Adam step size */
+    int64_t train_points;  /* shading points per training step (<= 0: 32768) */
+    const float *params;   /* dr_mlp_param_count() floats, host or device; NULL keeps the
+                              current parameters (a fixed initialisation the first time) */
+} dr_proposal_desc;
+DR_API dr_status dr_scene_set_proposal(dr_scene *scene, const dr_proposal_desc *desc);
+/* Current parameters (params_out: host or device, may be NULL), the last
+ * training loss and the number of training steps taken. */
+DR_API dr_status dr_scene_proposal_state(const dr_scene *scene, float *params_out, float *last_loss, int64_t *steps);
 DR_API dr_status dr_mlp_forward(const float *params_dev, const float *x_dev, int64_t n, float *logits_dev,
                                 void *stream);
 DR_API dr_status dr_mlp_gradient(const float *params_dev, const float *x_dev, const float *targets_dev, int64_t n,

@@ -38,6 +38,7 @@ def load():
                                 C.c_void_p, C.c_void_p, C.c_int, C.c_void_p]
         L.hh_trace.argtypes = [C.POINTER(_abi.dr_scene_desc), C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]
         L.hh_trace.restype = C.c_longlong
+        L.hh_set_proposal.argtypes = [C.c_int, C.c_float]
         _lib = L
     return _lib
 
@@ -69,3 +70,8 @@ def trace(wl, rays):
     t = np.zeros(len(rays), np.float32)
     visits = L.hh_trace(C.byref(sd.desc), rays.ctypes.data, len(rays), tri.ctypes.data, t.ctypes.data)
     return tri, t, visits
+
+
+def set_proposal(seed, alpha):
+    """Synthetic learned proposal of later renders (seed 0: none)."""
+    load().hh_set_proposal(int(seed), float(alpha))

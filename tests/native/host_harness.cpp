@@ -4,10 +4,17 @@
 // and use it to inspect the traversal.  Never part of the product: the product
 // runs this code only on the GPU.
 #include <algorithm>
+#include <cstring>
 #include <numeric>
 #include <vector>
 
 thread_local long long g_dr_visits = 0;
+
+// Synthetic learned proposal for the harness (hh_set_proposal): per shading
+// point, 32 skewed pseudo-random slot probabilities from a hash of the point's
+// sample id and bounce.
+static int g_prop_seed = 0;
+static float g_prop_alpha = 0.f;
 
 #include "../../delta_ray_b200/csrc/dr_backward.cuh"
 #include "../../delta_ray_b200/csrc/dr_bvh.cuh"
@@ -169,9 +176,34 @@ int hh_render(const dr_scene_desc *desc, const dr_render_desc *rd, const float *
     if (d_image && (parts & 2)) {
         struct Item { int pt, tree, ei, j; float w; };
         std::vector<Item> items;
+        std::vector<uint16_t> q(32);
         for (int p = 0; p < (int)pts.size(); p++) {
-            auto emit = [&](int tree, int ei, int j, float w) { items.push_back(Item{p, tree, ei, j, w}); };
-            traverse_point(s, pts[p], seed, emit);
+            auto emit = [&](int tree, int ei, int j, float w, int) { items.push_back(Item{p, tree, ei, j, w}); };
+            EdgeProposal pr;
+            pr.q = nullptr;
+            pr.alpha = g_prop_alpha;
+            if (g_prop_seed) {
+                float v[32], sum = 0.f;
+                for (int k = 0; k < 32; k++) {
+                    uint64_t h = (pts[p].sid + 1) * 0x9E3779B97F4A7C15ull ^ ((uint64_t)pts[p].bounce << 40) ^
+                                 ((uint64_t)k << 48) ^ (uint64_t)g_prop_seed * 0xD1B54A32D192ED03ull;
+                    h ^= h >> 31;
+                    h *= 0xBF58476D1CE4E5B9ull;
+                    h ^= h >> 29;
+                    float u = (float)((h >> 40) + 1) / (float)(1ull << 24);
+                    v[k] = u * u * u * u;
+                    sum += v[k];
+                }
+                for (int k = 0; k < 32; k++) {  // to bf16 bits, round to nearest even
+                    float f = v[k] / sum;
+                    uint32_t b;
+                    memcpy(&b, &f, 4);
+                    b += 0x7FFFu + ((b >> 16) & 1u);
+                    q[k] = (uint16_t)(b >> 16);
+                }
+                pr.q = q.data();
+            }
+            traverse_point(s, pts[p], seed, emit, pr);
         }
         nitems = (long long)items.size();
         std::vector<int> last(pts.size(), -1);
@@ -201,6 +233,12 @@ int hh_render(const dr_scene_desc *desc, const dr_render_desc *rd, const float *
         stats[1] = nitems;
     }
     return 0;
+}
+
+// The synthetic proposal of later hh_render calls (seed 0: none).
+void hh_set_proposal(int seed, float alpha) {
+    g_prop_seed = seed;
+    g_prop_alpha = alpha;
 }
 
 // Builds the LBVH over the scene and traces rays [n][6]; returns node visits.

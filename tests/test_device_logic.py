@@ -148,3 +148,28 @@ def test_edge_lobe_mis_matches_oracle(ltc_table):
             assert rel_err(o["grad"], o0["grad"]) == 0
         else:
             assert np.abs(o["grad"]).sum() < 0.8 * np.abs(o0["grad"]).sum()
+
+
+def test_learned_proposal_traversal_is_unbiased():
+    """The all-mode traversal driven by a (synthetic, pseudo-random) learned
+    proposal in a defensive mixture: over independent seeds its secondary-edge
+    gradient has the mean of the trees' own sampling (z-scores of the mean
+    difference behave like N(0, 1))."""
+    import scenes
+    wl = scenes.SCENES["heightfield_small"](seed=8, resolution=(16, 12), spp=2, max_bounces=1)
+    W, H = wl.resolution
+    d = np.ones((H, W, 3), np.float32)
+    K = 64
+    runs = {}
+    try:
+        for name, (ps, a) in {"plain": (0, 0.0), "learned": (7, 0.8)}.items():
+            harness.set_proposal(ps, a)
+            runs[name] = np.stack([harness.render(wl, 1000 * (ps + 1) + s, d, parts=2)["grad"] for s in range(K)])
+    finally:
+        harness.set_proposal(0, 0.0)
+    mp, ml = runs["plain"].mean(0), runs["learned"].mean(0)
+    se = np.hypot(runs["plain"].std(0, ddof=1), runs["learned"].std(0, ddof=1)) / np.sqrt(K)
+    m = se > 1e-3 * se.max()
+    z = (ml - mp)[m] / se[m]
+    assert m.sum() > 30
+    assert np.sqrt((z ** 2).mean()) < 1.4 and (np.abs(z) < 3).mean() >= 0.95, z
