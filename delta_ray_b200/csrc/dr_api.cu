@@ -420,8 +420,10 @@ std::pair<long long, long long> run_backward(dr_scene *scene, const dr_render_de
         float3 ctr = (scene->lo + scene->hi) * 0.5f, ext = (scene->hi - scene->lo) * 0.5f;
         float3 ih = f3(ext.x > 0.f ? 1.f / ext.x : 0.f, ext.y > 0.f ? 1.f / ext.y : 0.f, ext.z > 0.f ? 1.f / ext.z : 0.f);
         check_cuda(cudaMemsetAsync(pr.status.p, 0, sizeof(int), st), "memset");
+        timer->mark(st, "host_point_count");
         check_cuda(dr_launch_proposal_features(ds, ws, P, ctr, ih, pr.x.p, pr.train ? pr.xt.p : nullptr, st),
                    "proposal features");
+        timer->mark(st, "k_proposal_features");
         check_cuda(dr_mlp_infer(pr.img.as<uint8_t>(), pr.params.as<float>(), pr.x.as<__nv_bfloat16>(), P, nullptr,
                                 pr.q.as<__nv_bfloat16>(), pr.status.as<int>(), scene->num_sms, st),
                    "proposal inference");
@@ -471,6 +473,7 @@ std::pair<long long, long long> run_backward(dr_scene *scene, const dr_render_de
     if (prop && prop->train && ws.train_n > 0) {
         // one training step on the contribution magnitudes the edges reported
         ProposalState &pr = *prop;
+        timer->mark(st, "proposal_targets");
         check_cuda(dr_mlp_sum(pr.targets.as<float>(), ws.train_n * 32, pr.total.as<float>(), st), "target sum");
         check_cuda(cudaMemsetAsync(pr.grads.p, 0, sizeof(float) * kMlpParams, st), "memset");
         check_cuda(cudaMemsetAsync(pr.loss.p, 0, sizeof(float), st), "memset");

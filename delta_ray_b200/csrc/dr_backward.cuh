@@ -514,7 +514,7 @@ DEV ConeSpec light_cone(const DevScene &s, int li, float3 p) {
 
 // Samples the point's edges; emit(tree, edge_index, j, weight, slot_code) for
 // every sampled edge of nonzero weight, j counting all sampled edges in order.
-template <class Emit>
+template <bool PROP, class Emit>
 DEV bool traverse_point(const DevScene &s, const PointRecord &pt, uint64_t seed, Emit &emit,
                         const EdgeProposal &pr) {
     Rng prng;
@@ -527,12 +527,14 @@ DEV bool traverse_point(const DevScene &s, const PointRecord &pt, uint64_t seed,
         if (w != 0.f) emit(tree, ei, j, w, code);
         j++;
     };
-    return traverse_edges(s, pt.wi, pt.tri, sp, cone, prng, em, pr);
+    return traverse_edges<PROP>(s, pt.wi, pt.tri, sp, cone, prng, em, pr);
 }
 
 // One sampled edge (delta_ray.cpp:901-973); returns dp, scatters dv0 / dv1;
 // *mag (if given) receives the sample's contribution magnitude |dv0|_1 + |dv1|_1.
-template <class G>
+// EXT = false compiles the variant without DR_FLAG_EDGE_LOBE_MIS and without
+// the magnitude (the kernels choose it when neither is in use).
+template <bool EXT = true, class G>
 DEV float3 eval_item(const DevScene &s, const PointRecord &pt, int tree, int ei, int j, float w, int spp, int B,
                      uint64_t seed, G &g, float *mag = nullptr) {
     Rng prng;
@@ -543,9 +545,9 @@ DEV float3 eval_item(const DevScene &s, const PointRecord &pt, int tree, int ei,
     LightSample els = draw_light(irng);
     const DevEdge &edge = tree ? s.nrm_edges[ei] : s.sil_edges[ei];
     float3 weight = f3(1.f) * ((1.f / spp) * w);
-    EdgeResult er = shading_edge_sample(s, es, edge, els, irng, B - pt.bounce - 1, pt.wi, pt.tri, pt.surface(),
+    EdgeResult er = shading_edge_sample<EXT>(s, es, edge, els, irng, B - pt.bounce - 1, pt.wi, pt.tri, pt.surface(),
                                         weight, pt.d_color, B == 1);
-    if (mag) *mag = abs_sum(er.dv0) + abs_sum(er.dv1);
+    if (EXT && mag) *mag = abs_sum(er.dv0) + abs_sum(er.dv1);
     if (!is_zero(er.dv0) || !is_zero(er.dv1)) {
         const DevShape &sh = s.shapes[edge.shape];
         g.add(sh.grad_v + 3 * edge.v0 + 0, er.dv0.x);

@@ -13,6 +13,7 @@
 // in a lane buffer; a full buffer reserves DR_ITEM_BUF slots with one atomic
 // (points of large glossy scenes sample thousands of edges), and the last
 // partial buffers of a warp share one atomic.
+template <bool PROP>
 __global__ void __launch_bounds__(128, 4) k_edge_traverse(DevScene s, uint64_t seed, BackwardWorkspace ws) {
     long long n = min(min((long long)ws.counters->points, ws.cap_points), ws.pt_end);
     long long stride = (long long)gridDim.x * blockDim.x;
@@ -59,13 +60,15 @@ __global__ void __launch_bounds__(128, 4) k_edge_traverse(DevScene s, uint64_t s
             EdgeProposal pr;
             pr.q = ws.proposal_q ? ws.proposal_q + 32 * (size_t)p : nullptr;
             pr.alpha = ws.proposal_alpha;
-            if (!traverse_point(s, pt, seed, emit, pr)) set_status(&ws.counters->status, DR_STATUS_STACK_OVERFLOW);
+            if (!traverse_point<PROP>(s, pt, seed, emit, pr))
+                set_status(&ws.counters->status, DR_STATUS_STACK_OVERFLOW);
         }
         __syncwarp();
         write_items(warp_reserve(count, nb), nb);
     }
 }
 
+template <bool EXT>
 __global__ void __launch_bounds__(128, 4) k_edge_eval(DevScene s, int W, int H, int spp, int B, uint64_t seed, int dp_mode,
                                                    float *grad, BackwardWorkspace ws, GradCacheCfg cfg) {
     extern __shared__ float sm[];
@@ -77,8 +80,8 @@ __global__ void __launch_bounds__(128, 4) k_edge_eval(DevScene s, int W, int H, 
         pt.load(ws.pt + (size_t)it.x * DR_PT_WORDS);
         int tree = it.y >> 30, ei = it.y & ((1 << 30) - 1);
         float mag = 0.f;
-        float3 dp = eval_item(s, pt, tree, ei, it.z, ws.item_w[i], spp, B, seed, bg, &mag);
-        if (ws.train_targets && mag > 0.f && it.x % ws.train_stride == 0 && it.x / ws.train_stride < ws.train_n) {
+        float3 dp = eval_item<EXT>(s, pt, tree, ei, it.z, ws.item_w[i], spp, B, seed, bg, &mag);
+        if (EXT && ws.train_targets && mag > 0.f && it.x % ws.train_stride == 0 && it.x / ws.train_stride < ws.train_n) {
             // the proposal's training target: contribution magnitude per cut slot
             int code = it.w, tr = code >> 7, lw = (code >> 4) & 7, lo = code & 15, wdt = 1 << lw;
             float *t = ws.train_targets + 32 * (size_t)(it.x / ws.train_stride) + 16 * tr + lo;
@@ -117,7 +120,8 @@ __global__ void __launch_bounds__(128, 3) k_primary_edges(DevScene s, int W, int
 
 cudaError_t dr_launch_edge_traverse(const DevScene &s, uint64_t seed, const BackwardWorkspace &ws, int num_sms,
                                     cudaStream_t st, int *launches, StageTimer *timer) {
-    k_edge_traverse<<<stage_grid(num_sms), 128, 0, st>>>(s, seed, ws);
+    if (ws.proposal_q) k_edge_traverse<true><<<stage_grid(num_sms), 128, 0, st>>>(s, seed, ws);
+    else k_edge_traverse<false><<<stage_grid(num_sms), 128, 0, st>>>(s, seed, ws);
     timer->mark(st, "k_edge_traverse");
     *launches += 1;
     return cudaGetLastError();
@@ -127,7 +131,10 @@ cudaError_t dr_launch_edge_eval(const DevScene &s, int W, int H, int spp, int B,
                                 float *grad, const BackwardWorkspace &ws, const GradCacheCfg &cfg, int num_sms,
                                 cudaStream_t st) {
     size_t smem = sizeof(float) * (size_t)(cfg.head + cfg.tail_len);
-    k_edge_eval<<<stage_grid(num_sms), 128, smem, st>>>(s, W, H, spp, B, seed, dp_mode, grad, ws, cfg);
+    if (s.edge_lobe_mis || ws.train_targets)
+        k_edge_eval<true><<<stage_grid(num_sms), 128, smem, st>>>(s, W, H, spp, B, seed, dp_mode, grad, ws, cfg);
+    else
+        k_edge_eval<false><<<stage_grid(num_sms), 128, smem, st>>>(s, W, H, spp, B, seed, dp_mode, grad, ws, cfg);
     return cudaGetLastError();
 }
 

@@ -259,15 +259,32 @@ HD int slot_code(int tree, int lo, int lw) { return lo | (lw << 4) | (tree << 7)
 // lpmf learned), so the mixture's pmf alpha lpmf + (1 - alpha) apmf takes the
 // place of the all-mode pmf in the multiple-importance weights of both modes.
 #define DR_EDGE_STACK 64
-template <bool CONE, class Emit>
+// Stack entry of the traversal; with a proposal (PROP) it also carries the
+// learned path product and the subtree's slot range (lo | log2(width) << 4).
+template <bool PROP> struct EdgeItem { int node; float bb, cpmf, apmf, lpmf; int slot; };
+template <> struct EdgeItem<false> { int node; float bb, cpmf, apmf; };
+template <bool PROP> HD EdgeItem<PROP> edge_item(int node, float bb, float c, float a, float l, int slot) {
+    EdgeItem<PROP> it;
+    it.node = node;
+    it.bb = bb;
+    it.cpmf = c;
+    it.apmf = a;
+    if constexpr (PROP) {
+        it.lpmf = l;
+        it.slot = slot;
+    }
+    return it;
+}
+
+template <bool CONE, bool PROP, class Emit>
 DEV bool traverse_mode(const DevScene &s, const DevEdgeNode *nodes, const DevEdge *edges, bool dir_bounds, float3 wi,
                        const SurfacePoint &sp, float dl, float sl, float rough, int model, const ConeSpec &cone,
                        float root_bb, float pmf, Rng &rng, Emit &emit, const EdgeProposal &pr, int tree,
                        bool learned) {
-    struct Item { int node; float bb, cpmf, apmf, lpmf; int slot; };  // slot: lo | log2(width) << 4
+    using Item = EdgeItem<PROP>;
     Item st[DR_EDGE_STACK];
     int sp_ = 0;
-    st[sp_++] = Item{0, root_bb, pmf, pmf, pmf, 4 << 4};
+    st[sp_++] = edge_item<PROP>(0, root_bb, pmf, pmf, pmf, 4 << 4);
     bool ok = true;
     while (sp_ > 0) {
         Item it = st[--sp_];
@@ -275,10 +292,13 @@ DEV bool traverse_mode(const DevScene &s, const DevEdgeNode *nodes, const DevEdg
         const DevEdgeNode &node = nodes[it.node];
         if (node.nprims > 0) {
             float apmf = it.apmf;
-            if (pr.q) apmf = pr.alpha * it.lpmf + (1.f - pr.alpha) * it.apmf;
+            int code = 0;
+            if constexpr (PROP) {
+                apmf = pr.alpha * it.lpmf + (1.f - pr.alpha) * it.apmf;
+                code = it.slot | (tree << 7);
+            }
             float denom = it.cpmf * it.cpmf + apmf * apmf;
             float w = CONE ? it.cpmf / denom : apmf / denom;
-            int code = it.slot | (tree << 7);
             for (int i = 0; i < node.nprims; i++) {
                 int ei = node.offset + i;
                 if (is_silhouette(s, sp.p, edges[ei])) emit(ei, w, code);
@@ -316,21 +336,28 @@ DEV bool traverse_mode(const DevScene &s, const DevEdgeNode *nodes, const DevEdg
             pra = 1.f - pla;
         }
         // the proposal's choice above the cut (both children important, no split)
-        float pll = pla, prl = pra;
-        int lw = it.slot >> 4, lo = it.slot & 15;
-        if (pr.q && !all_split && lw > 0 && il > 0.f && ir > 0.f) {
-            int h = 1 << (lw - 1);
-            float ql = slot_mass(pr.q, tree, lo, h), qr = slot_mass(pr.q, tree, lo + h, h);
-            if (ql + qr > 0.f) {
-                pll = ql / (ql + qr);
-                prl = 1.f - pll;
+        float pll = pla;
+        Item left, right;
+        if constexpr (PROP) {
+            float prl = pra;
+            int lw = it.slot >> 4, lo = it.slot & 15;
+            if (!all_split && lw > 0 && il > 0.f && ir > 0.f) {
+                int h = 1 << (lw - 1);
+                float ql = slot_mass(pr.q, tree, lo, h), qr = slot_mass(pr.q, tree, lo + h, h);
+                if (ql + qr > 0.f) {
+                    pll = ql / (ql + qr);
+                    prl = 1.f - pll;
+                }
             }
+            int lslot = lw > 0 ? (lo | ((lw - 1) << 4)) : it.slot;
+            int rslot = lw > 0 ? ((lo + (1 << (lw - 1))) | ((lw - 1) << 4)) : it.slot;
+            left = edge_item<PROP>(li, lbb, plc * it.cpmf, pla * it.apmf, pll * it.lpmf, lslot);
+            right = edge_item<PROP>(ri, rbb, prc * it.cpmf, pra * it.apmf, prl * it.lpmf, rslot);
+        } else {
+            left = edge_item<PROP>(li, lbb, plc * it.cpmf, pla * it.apmf, 0.f, 0);
+            right = edge_item<PROP>(ri, rbb, prc * it.cpmf, pra * it.apmf, 0.f, 0);
         }
-        int lslot = lw > 0 ? (lo | ((lw - 1) << 4)) : it.slot;
-        int rslot = lw > 0 ? ((lo + (1 << (lw - 1))) | ((lw - 1) << 4)) : it.slot;
         bool split = CONE ? cone_split : all_split;
-        Item left{li, lbb, plc * it.cpmf, pla * it.apmf, pll * it.lpmf, lslot},
-            right{ri, rbb, prc * it.cpmf, pra * it.apmf, prl * it.lpmf, rslot};
         if (split) {
             if (sp_ + 2 > DR_EDGE_STACK) {
                 ok = false;
@@ -354,7 +381,7 @@ DEV bool traverse_mode(const DevScene &s, const DevEdgeNode *nodes, const DevEdg
 
 // All edges sampled for one shading point (edge_tree.cpp:654-725).
 // emit(tree, edge_index, weight); tree 0 = silhouette tree, 1 = normal tree.
-template <class Emit>
+template <bool PROP, class Emit>
 DEV bool traverse_edges(const DevScene &s, float3 wi, int stri, const SurfacePoint &sp, const ConeSpec &cone, Rng &rng,
                         Emit &emit, const EdgeProposal &pr) {
     if (dot(wi, sp.f.n) < 0.f) return true;
@@ -368,7 +395,7 @@ DEV bool traverse_edges(const DevScene &s, float3 wi, int stri, const SurfacePoi
     } else {
         float ni = s.nrm_nodes[0].total_length, si = s.sil_nodes[0].total_length;
         float np = ni / (ni + si), spm = si / (ni + si);
-        if (pr.q) {  // the tree pick mixed with the proposal's tree masses
+        if (PROP) {  // the tree pick mixed with the proposal's tree masses
             float qn = slot_mass(pr.q, 1, 0, 16), qs = slot_mass(pr.q, 0, 0, 16);
             float qt = qn + qs > 0.f ? qn / (qn + qs) : np;
             np = pr.alpha * qt + (1.f - pr.alpha) * np;
@@ -390,11 +417,11 @@ DEV bool traverse_edges(const DevScene &s, float3 wi, int stri, const SurfacePoi
     float rough = get_rough(s, m, sp.uv);
     float b = bsdf_bound(nodes[0], wi, sp, dl, sl, rough, m.model);
     auto em = [&](int ei, float w, int code) { emit(tree, ei, w, code); };
-    bool ok = traverse_mode<true>(s, nodes, edges, tree == 1, wi, sp, dl, sl, rough, m.model, cone, b, pmf, rng, em,
-                                  pr, tree, false);
-    bool learned = pr.q ? rng.next() < pr.alpha : false;
-    ok &= traverse_mode<false>(s, nodes, edges, tree == 1, wi, sp, dl, sl, rough, m.model, cone, b, pmf, rng, em, pr,
-                               tree, learned);
+    bool ok = traverse_mode<true, PROP>(s, nodes, edges, tree == 1, wi, sp, dl, sl, rough, m.model, cone, b, pmf, rng,
+                                        em, pr, tree, false);
+    bool learned = PROP ? rng.next() < pr.alpha : false;
+    ok &= traverse_mode<false, PROP>(s, nodes, edges, tree == 1, wi, sp, dl, sl, rough, m.model, cone, b, pmf, rng, em,
+                                     pr, tree, learned);
     return ok;
 }
 
@@ -470,8 +497,17 @@ DEV_NOINLINE float lobe_line_density(const M3 &minv, float3 d0, float3 d1, float
     return p > 0.f ? p * length(mul(minv, q_l)) : 0.f;
 }
 
+// Line density of the lobe that was not picked, at the sampled point (out of
+// line: only DR_FLAG_EDGE_LOBE_MIS needs it).
+DEV_NOINLINE float other_lobe_density(const DevScene &s, int mi, const SurfacePoint &sp, float3 wi, const M3 &frame,
+                                      bool sel_diffuse, float3 v0, float3 v1, float3 sample_p, float3 q_l) {
+    M3 ominv = sel_diffuse ? mul(inverse(ltc_matrix(s, mi, sp, wi)), frame) : frame;
+    return lobe_line_density(ominv, v0 - sp.p, v1 - sp.p, sample_p, q_l);
+}
+
 // Secondary edge sample (delta_ray.cpp:45-365).  `rng` holds the item's
 // secondary samples (for the two shade calls, replayed from the same state).
+template <bool EXT = true>
 DEV EdgeResult shading_edge_sample(const DevScene &s, const EdgeSample &es, const DevEdge &edge, const LightSample &ls,
                                    const Rng &rng, int nbounces, float3 wi, int stri, const SurfacePoint &sp,
                                    float3 weight, float3 d_color, bool direct_only) {
@@ -616,13 +652,11 @@ DEV EdgeResult shading_edge_sample(const DevScene &s, const EdgeSample &es, cons
     // lobes, pmf_sel pdf_sel(l) + pmf_other pdf_other(l); the reference divides
     // by pmf_sel pdf_sel(l) alone
     float q_mix = mpmf * pdf_l;
-    if (s.edge_lobe_mis) {
+    if (EXT && s.edge_lobe_mis) {
         bool sel_diffuse = es.bsdf_component <= dpmf;
         float opmf = sel_diffuse ? spmf : dpmf;
-        if (opmf > 0.f) {
-            M3 ominv = sel_diffuse ? mul(inverse(ltc_matrix(s, mi, sp, wi)), frame) : frame;
-            q_mix += opmf * lobe_line_density(ominv, v0 - sp.p, v1 - sp.p, sample_p, mul(m, wt));
-        }
+        if (opmf > 0.f)
+            q_mix += opmf * other_lobe_density(s, mi, sp, wi, frame, sel_diffuse, v0, v1, sample_p, mul(m, wt));
     }
     auto accum = [&](const SurfacePoint &lp, float3 ev) {
         M3 nj = normalize_jacobian(sample_p);

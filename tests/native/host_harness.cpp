@@ -203,7 +203,8 @@ int hh_render(const dr_scene_desc *desc, const dr_render_desc *rd, const float *
                 }
                 pr.q = q.data();
             }
-            traverse_point(s, pts[p], seed, emit, pr);
+            if (pr.q) traverse_point<true>(s, pts[p], seed, emit, pr);
+            else traverse_point<false>(s, pts[p], seed, emit, pr);
         }
         nitems = (long long)items.size();
         std::vector<int> last(pts.size(), -1);
