@@ -60,6 +60,7 @@ __global__ void __launch_bounds__(128, 4) k_edge_traverse(DevScene s, uint64_t s
             EdgeProposal pr;
             pr.q = ws.proposal_q ? ws.proposal_q + 32 * (size_t)p : nullptr;
             pr.alpha = ws.proposal_alpha;
+            pr.codes = ws.train_targets != nullptr;
             if (!traverse_point<PROP>(s, pt, seed, emit, pr))
                 set_status(&ws.counters->status, DR_STATUS_STACK_OVERFLOW);
         }
@@ -82,10 +83,8 @@ __global__ void __launch_bounds__(128, 4) k_edge_eval(DevScene s, int W, int H, 
         float mag = 0.f;
         float3 dp = eval_item<EXT>(s, pt, tree, ei, it.z, ws.item_w[i], spp, B, seed, bg, &mag);
         if (EXT && ws.train_targets && mag > 0.f && it.x % ws.train_stride == 0 && it.x / ws.train_stride < ws.train_n) {
-            // the proposal's training target: contribution magnitude per cut slot
-            int code = it.w, tr = code >> 7, lw = (code >> 4) & 7, lo = code & 15, wdt = 1 << lw;
-            float *t = ws.train_targets + 32 * (size_t)(it.x / ws.train_stride) + 16 * tr + lo;
-            for (int k = 0; k < wdt; k++) atomicAdd(t + k, mag / wdt);
+            // the proposal's training target: contribution magnitude per direction bin
+            atomicAdd(ws.train_targets + 32 * (size_t)(it.x / ws.train_stride) + (it.w & 31), mag);
         }
         if (is_zero(dp)) continue;
         if (dp_mode == DR_DP_SUM) {

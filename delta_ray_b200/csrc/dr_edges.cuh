@@ -230,22 +230,27 @@ DEV bool node_inside(const DevEdgeNode &n, float3 p) {
 }
 
 // The learned edge proposal of one shading point (a project addition): 32
-// bf16 probabilities over the depth-4 cut of the silhouette tree (slots
-// 0..15) and of the normal tree (16..31).  A subtree above the cut owns the
-// slots of its descendants at depth 4; a leaf above the cut owns a range.
-// q == null: the reference's sampling.
+// bf16 probabilities over directions from the point, in the shading frame:
+// 4 bands of cos(theta) (split at -1/2, 0, 1/2) times 8 azimuth octants
+// (dir_bin).  q == null: the reference's sampling.
 struct EdgeProposal {
     const uint16_t *q;
     float alpha;  // probability of the learned descent in the defensive mixture
+    bool codes;   // emit each edge's direction bin (training)
 };
 HD float bf16_bits_to_float(uint16_t b) { return dr_i2f((int)((uint32_t)b << 16)); }
-DEV float slot_mass(const uint16_t *q, int tree, int lo, int n) {
-    float m = 0.f;
-    for (int k = 0; k < n; k++) m += bf16_bits_to_float(q[16 * tree + lo + k]);
-    return m;
+DEV int dir_bin(const Frame &f, float3 d) {
+    float x = dot(d, f.t), y = dot(d, f.b), z = dot(d, f.n);
+    float z2 = z * z, r2 = x * x + y * y + z2;
+    int band = z < 0.f ? (4.f * z2 > r2 ? 0 : 1) : (4.f * z2 > r2 ? 3 : 2);
+    int oct = (y < 0.f ? 4 : 0) | (x < 0.f ? 2 : 0) | (fabsf(x) < fabsf(y) ? 1 : 0);
+    return band * 8 + oct;
 }
-// slot range code of an item: lo | log2(width) << 4 | tree << 7
-HD int slot_code(int tree, int lo, int lw) { return lo | (lw << 4) | (tree << 7); }
+// The proposal's weight of a node: its probability for the direction of the box centre.
+DEV float node_dir_weight(const uint16_t *q, const Frame &f, float3 p, const DevEdgeNode &n) {
+    float3 c = f3(0.5f * (n.lo[0] + n.hi[0]), 0.5f * (n.lo[1] + n.hi[1]), 0.5f * (n.lo[2] + n.hi[2]));
+    return bf16_bits_to_float(q[dir_bin(f, c - p)]);
+}
 
 // Stochastic traversal of one edge tree in one mode (edge_tree.cpp:511-652).
 // emit(tree_edge_index, weight, slot_code) is called for every silhouette
@@ -254,25 +259,25 @@ HD int slot_code(int tree, int lo, int lw) { return lo | (lw << 4) | (tree << 7)
 //
 // With a proposal, the "all" mode becomes a defensive mixture: `learned`
 // (drawn once per traversal, probability alpha) picks the child at each
-// stochastic node above the cut by the proposal's slot masses, otherwise by
-// the tree's importance.  Every node tracks both path products (apmf plain,
-// lpmf learned), so the mixture's pmf alpha lpmf + (1 - alpha) apmf takes the
-// place of the all-mode pmf in the multiple-importance weights of both modes.
+// stochastic node in proportion to the tree's importance times the
+// proposal's weight of the direction towards the child, otherwise by the
+// importance alone.  Every node tracks both path products (apmf plain, lpmf
+// learned), so the mixture's pmf alpha lpmf + (1 - alpha) apmf takes the place
+// of the all-mode pmf in the multiple-importance weights of both modes.  The
+// emitted code is the direction bin of the edge's midpoint (the training
+// target's slot).
 #define DR_EDGE_STACK 64
 // Stack entry of the traversal; with a proposal (PROP) it also carries the
-// learned path product and the subtree's slot range (lo | log2(width) << 4).
-template <bool PROP> struct EdgeItem { int node; float bb, cpmf, apmf, lpmf; int slot; };
+// learned path product.
+template <bool PROP> struct EdgeItem { int node; float bb, cpmf, apmf, lpmf; };
 template <> struct EdgeItem<false> { int node; float bb, cpmf, apmf; };
-template <bool PROP> HD EdgeItem<PROP> edge_item(int node, float bb, float c, float a, float l, int slot) {
+template <bool PROP> HD EdgeItem<PROP> edge_item(int node, float bb, float c, float a, float l) {
     EdgeItem<PROP> it;
     it.node = node;
     it.bb = bb;
     it.cpmf = c;
     it.apmf = a;
-    if constexpr (PROP) {
-        it.lpmf = l;
-        it.slot = slot;
-    }
+    if constexpr (PROP) it.lpmf = l;
     return it;
 }
 
@@ -284,7 +289,7 @@ DEV bool traverse_mode(const DevScene &s, const DevEdgeNode *nodes, const DevEdg
     using Item = EdgeItem<PROP>;
     Item st[DR_EDGE_STACK];
     int sp_ = 0;
-    st[sp_++] = edge_item<PROP>(0, root_bb, pmf, pmf, pmf, 4 << 4);
+    st[sp_++] = edge_item<PROP>(0, root_bb, pmf, pmf, pmf);
     bool ok = true;
     while (sp_ > 0) {
         Item it = st[--sp_];
@@ -292,16 +297,16 @@ DEV bool traverse_mode(const DevScene &s, const DevEdgeNode *nodes, const DevEdg
         const DevEdgeNode &node = nodes[it.node];
         if (node.nprims > 0) {
             float apmf = it.apmf;
-            int code = 0;
-            if constexpr (PROP) {
-                apmf = pr.alpha * it.lpmf + (1.f - pr.alpha) * it.apmf;
-                code = it.slot | (tree << 7);
-            }
+            if constexpr (PROP) apmf = pr.alpha * it.lpmf + (1.f - pr.alpha) * it.apmf;
             float denom = it.cpmf * it.cpmf + apmf * apmf;
             float w = CONE ? it.cpmf / denom : apmf / denom;
             for (int i = 0; i < node.nprims; i++) {
                 int ei = node.offset + i;
-                if (is_silhouette(s, sp.p, edges[ei])) emit(ei, w, code);
+                if (!is_silhouette(s, sp.p, edges[ei])) continue;
+                int code = 0;
+                if constexpr (PROP)
+                    if (pr.codes) code = dir_bin(sp.f, 0.5f * (edge_v0(s, edges[ei]) + edge_v1(s, edges[ei])) - sp.p);
+                emit(ei, w, code);
             }
             continue;
         }
@@ -335,27 +340,24 @@ DEV bool traverse_mode(const DevScene &s, const DevEdgeNode *nodes, const DevEdg
             pla = il / (il + ir);
             pra = 1.f - pla;
         }
-        // the proposal's choice above the cut (both children important, no split)
+        // the proposal's choice (both children important, no split): importance
+        // times the learned weight of the direction towards each child
         float pll = pla;
         Item left, right;
         if constexpr (PROP) {
             float prl = pra;
-            int lw = it.slot >> 4, lo = it.slot & 15;
-            if (!all_split && lw > 0 && il > 0.f && ir > 0.f) {
-                int h = 1 << (lw - 1);
-                float ql = slot_mass(pr.q, tree, lo, h), qr = slot_mass(pr.q, tree, lo + h, h);
-                if (ql + qr > 0.f) {
-                    pll = ql / (ql + qr);
+            if (!all_split && il > 0.f && ir > 0.f) {
+                float gl = il * node_dir_weight(pr.q, sp.f, sp.p, L), gr = ir * node_dir_weight(pr.q, sp.f, sp.p, R);
+                if (gl + gr > 0.f) {
+                    pll = gl / (gl + gr);
                     prl = 1.f - pll;
                 }
             }
-            int lslot = lw > 0 ? (lo | ((lw - 1) << 4)) : it.slot;
-            int rslot = lw > 0 ? ((lo + (1 << (lw - 1))) | ((lw - 1) << 4)) : it.slot;
-            left = edge_item<PROP>(li, lbb, plc * it.cpmf, pla * it.apmf, pll * it.lpmf, lslot);
-            right = edge_item<PROP>(ri, rbb, prc * it.cpmf, pra * it.apmf, prl * it.lpmf, rslot);
+            left = edge_item<PROP>(li, lbb, plc * it.cpmf, pla * it.apmf, pll * it.lpmf);
+            right = edge_item<PROP>(ri, rbb, prc * it.cpmf, pra * it.apmf, prl * it.lpmf);
         } else {
-            left = edge_item<PROP>(li, lbb, plc * it.cpmf, pla * it.apmf, 0.f, 0);
-            right = edge_item<PROP>(ri, rbb, prc * it.cpmf, pra * it.apmf, 0.f, 0);
+            left = edge_item<PROP>(li, lbb, plc * it.cpmf, pla * it.apmf, 0.f);
+            right = edge_item<PROP>(ri, rbb, prc * it.cpmf, pra * it.apmf, 0.f);
         }
         bool split = CONE ? cone_split : all_split;
         if (split) {
@@ -395,12 +397,6 @@ DEV bool traverse_edges(const DevScene &s, float3 wi, int stri, const SurfacePoi
     } else {
         float ni = s.nrm_nodes[0].total_length, si = s.sil_nodes[0].total_length;
         float np = ni / (ni + si), spm = si / (ni + si);
-        if (PROP) {  // the tree pick mixed with the proposal's tree masses
-            float qn = slot_mass(pr.q, 1, 0, 16), qs = slot_mass(pr.q, 0, 0, 16);
-            float qt = qn + qs > 0.f ? qn / (qn + qs) : np;
-            np = pr.alpha * qt + (1.f - pr.alpha) * np;
-            spm = 1.f - np;
-        }
         float u = rng.next();
         if (u < np) {
             tree = 1;

@@ -5,9 +5,11 @@ A 10 -> 64 -> 64 -> 64 -> 32 MLP with ReLU hidden layers and a softmax
 output, run and trained by the library's tensor-core kernels in bf16 with f32
 accumulation.  Its inputs are a shading point's position (normalised to the
 scene bounds), shading normal, roughness and incoming direction; its 32
-outputs are probabilities over the cut of the two edge trees at depth 4 (16
-subtrees each), with which edge sampling draws subtrees before it falls back
-to the trees' own importance below the cut.
+outputs are probabilities over directions from the point (4 bands of
+cos(theta) times 8 azimuth sectors in the shading frame).  Edge sampling
+weights each edge-tree child's importance by the probability of the
+direction towards it, so the network can learn what the importance bound
+does not model, such as occlusion.
 
 ``init_params``  a fresh parameter vector (PyTorch nn.Linear initialisation)
 ``forward``      logits of rows x [n, 16] (inputs 10..15 zero for the proposal)

@@ -283,14 +283,16 @@ DR_API int dr_mlp_param_count(void);
 /* The learned edge proposal of a scene (no counterpart in the reference,
  * which samples edges by the edge trees' importance alone).  With
  * DR_FLAG_LEARNED_PROPOSAL a backward call computes, for every shading point,
- * the network's probabilities over the two edge trees' subtrees at depth 4
- * from the point's position (normalised to the scene bounds), shading normal,
- * roughness and incoming direction.  The edge trees' all-mode traversal then
- * follows those probabilities above the cut with probability `mix` and the
- * trees' own importance otherwise, a defensive mixture whose exact pmf enters
- * the reference's multiple-importance weights, so the gradient stays unbiased
- * for any network.  In training mode each such call sums the contribution
- * magnitude |dv0| + |dv1| of every sampled edge per subtree for
+ * the network's probabilities over 32 directions from the point (4 bands of
+ * cos(theta) times 8 azimuth sectors in the shading frame) from the point's
+ * position (normalised to the scene bounds), shading normal, roughness and
+ * incoming direction.  With probability `mix` the edge trees' all-mode
+ * traversal then picks children in proportion to their importance times the
+ * probability of the direction towards them, and by importance alone
+ * otherwise: a defensive mixture whose exact pmf enters the reference's
+ * multiple-importance weights, so the gradient stays unbiased for any
+ * network.  In training mode each such call sums the contribution magnitude
+ * |dv0| + |dv1| of every sampled edge per direction of its midpoint for
  * `train_points` shading points spread over the call's points and takes one
  * Adam step on  sum -t log q / sum t  (t the magnitudes, q the network's
  * probabilities). */

@@ -182,6 +182,7 @@ int hh_render(const dr_scene_desc *desc, const dr_render_desc *rd, const float *
             EdgeProposal pr;
             pr.q = nullptr;
             pr.alpha = g_prop_alpha;
+            pr.codes = false;
             if (g_prop_seed) {
                 float v[32], sum = 0.f;
                 for (int k = 0; k < 32; k++) {
