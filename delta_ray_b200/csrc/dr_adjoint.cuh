@@ -41,17 +41,10 @@ struct SpGrad {
 // (the floor-floor texel's adjoint lands on the ceil-ceil texel and so on),
 // the uv adjoint is returned through d_uv.  `finite_only` skips non-finite
 // contributions as delta_ray.cpp:846-851 does for constant roughness.
+// the texel part, out of line (many call sites)
 template <class G>
-DEV void d_tex_channel(const DevScene &s, int off, int w, int h, int ch, int grad_base, const float *uv_scale,
-                       float2 uv, const float *dval, G &g, float2 &d_uv, bool finite_only) {
-    if (off < 0) {
-        for (int c = 0; c < ch; c++) {
-            float v = dval[c];
-            if (finite_only && !dr_isfinite(v)) continue;
-            g.add(grad_base + c, v);
-        }
-        return;
-    }
+DEV_NOINLINE void d_tex_texels(const DevScene &s, int off, int w, int h, int ch, int grad_base, const float *uv_scale,
+                               float2 uv, const float *dval, G &g, float2 &d_uv) {
     float2 su = scale_uv(uv, uv_scale);
     TexFoot t = tex_foot(w, h, su);
     float du = 0.f, dv = 0.f;
@@ -69,6 +62,19 @@ DEV void d_tex_channel(const DevScene &s, int off, int w, int h, int ch, int gra
     }
     d_uv.x += du * (float)w * uv_scale[0];
     d_uv.y += dv * (float)h * uv_scale[1];
+}
+template <class G>
+DEV void d_tex_channel(const DevScene &s, int off, int w, int h, int ch, int grad_base, const float *uv_scale,
+                       float2 uv, const float *dval, G &g, float2 &d_uv, bool finite_only) {
+    if (off < 0) {
+        for (int c = 0; c < ch; c++) {
+            float v = dval[c];
+            if (finite_only && !dr_isfinite(v)) continue;
+            g.add(grad_base + c, v);
+        }
+        return;
+    }
+    d_tex_texels(s, off, w, h, ch, grad_base, uv_scale, uv, dval, g, d_uv);
 }
 
 template <class G> DEV void d_kd(const DevScene &s, const DevMaterial &m, float2 uv, float3 d, G &g, float2 &duv) {

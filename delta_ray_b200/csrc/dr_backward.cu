@@ -22,7 +22,7 @@
 #include "dr_backward.cuh"
 #include "dr_block_grad.cuh"
 
-template <bool kChains>
+template <bool kChains, int BMAX>
 __global__ void __launch_bounds__(128, 3) k_backward_paths(DevScene s, int W, int H, int spp, int B, uint64_t seed,
                                                         int lanes_log2, const float *d_image, float *grad, float *img,
                                                         BackwardWorkspace ws, GradCacheCfg cfg) {
@@ -54,7 +54,7 @@ __global__ void __launch_bounds__(128, 3) k_backward_paths(DevScene s, int W, in
                 if (slot < (unsigned long long)ws.cap_points) p.store(ws.pt + (size_t)slot * DR_PT_WORDS);
                 else set_status(&ws.counters->status, DR_STATUS_POINT_OVERFLOW);
             };
-            acc += backward_pixel_sample<kChains>(s, x, y, W, H, spp, si, B, seed, dc, bg, push);
+            acc += backward_pixel_sample<kChains, BMAX>(s, x, y, W, H, spp, si, B, seed, dc, bg, push);
         }
         __syncwarp();
         unsigned long long slot = warp_reserve(&ws.counters->points, has ? 1 : 0);
@@ -130,12 +130,10 @@ cudaError_t dr_launch_backward_front(const DevScene &s, int W, int H, int spp, i
         cudaError_t e = cudaMemsetAsync(ws.pt_last, 0, per * (size_t)ws.cap_points, st);
         if (e != cudaSuccess) return e;
     }
-    if (s.specular_chains)
-        k_backward_paths<true><<<blocks_for(threads, bs), bs, smem, st>>>(s, W, H, spp, B, seed, lanes_log2, d_image,
-                                                                         grad, img, ws, cfg);
-    else
-        k_backward_paths<false><<<blocks_for(threads, bs), bs, smem, st>>>(s, W, H, spp, B, seed, lanes_log2, d_image,
-                                                                          grad, img, ws, cfg);
+    // variants: specular chains or not, direct lighting (B = 1) or not
+    auto kernel = s.specular_chains ? (B == 1 ? k_backward_paths<true, 1> : k_backward_paths<true, DR_MAX_BOUNCES>)
+                                    : (B == 1 ? k_backward_paths<false, 1> : k_backward_paths<false, DR_MAX_BOUNCES>);
+    kernel<<<blocks_for(threads, bs), bs, smem, st>>>(s, W, H, spp, B, seed, lanes_log2, d_image, grad, img, ws, cfg);
     timer->mark(st, "k_backward_paths");
     *launches += 1;
     long long npe = primary_edge_samples > 0 ? primary_edge_samples : (long long)spp * W * H;

@@ -254,7 +254,9 @@ DEV void sweep_links(const DevScene &s, SpecLink *links, int n, VertexGrad &v0, 
 // direction to vertex k, the roughness and the hit triangle.
 // kChains = false compiles the variant for scenes without specular samples
 // (no chain bookkeeping); both give the same result on such scenes.
-template <bool kChains, class G, class Push>
+// BMAX bounds max_bounces at compile time (1 for direct lighting, whose
+// variant drops the bounce-record array and the loops' later trips).
+template <bool kChains, int BMAX = DR_MAX_BOUNCES, class G, class Push>
 DEV float3 backward_pixel_sample(const DevScene &s, int x, int y, int W, int H, int spp, int si, int B, uint64_t seed,
                                  float3 d_color, G &g, Push &push_point) {
     const float sw = 1.f / spp;
@@ -275,7 +277,8 @@ DEV float3 backward_pixel_sample(const DevScene &s, int x, int y, int W, int H, 
     const int light_pick =
         sample_discrete(s.light_sel_cdf, s.light_sel_func, s.light_sel_func_int, s.num_lights, ls.sel, nullptr);
     // ---- pass 1: trace, keep the bounces ----
-    BounceRecord rec[DR_MAX_BOUNCES];
+    if (B > BMAX) B = BMAX;
+    BounceRecord rec[BMAX];
     int nb = 0;
     float3 color = f3(0.f);
     int li0 = light_of_tri(s, h0.tri);
@@ -534,7 +537,7 @@ DEV bool traverse_point(const DevScene &s, const PointRecord &pt, uint64_t seed,
 // *mag (if given) receives the sample's contribution magnitude |dv0|_1 + |dv1|_1.
 // EXT = false compiles the variant without DR_FLAG_EDGE_LOBE_MIS and without
 // the magnitude (the kernels choose it when neither is in use).
-template <bool EXT = true, class G>
+template <bool EXT = true, bool MAYBE_GI = true, class G>
 DEV float3 eval_item(const DevScene &s, const PointRecord &pt, int tree, int ei, int j, float w, int spp, int B,
                      uint64_t seed, G &g, float *mag = nullptr) {
     Rng prng;
@@ -545,7 +548,7 @@ DEV float3 eval_item(const DevScene &s, const PointRecord &pt, int tree, int ei,
     LightSample els = draw_light(irng);
     const DevEdge &edge = tree ? s.nrm_edges[ei] : s.sil_edges[ei];
     float3 weight = f3(1.f) * ((1.f / spp) * w);
-    EdgeResult er = shading_edge_sample<EXT>(s, es, edge, els, irng, B - pt.bounce - 1, pt.wi, pt.tri, pt.surface(),
+    EdgeResult er = shading_edge_sample<EXT, MAYBE_GI>(s, es, edge, els, irng, B - pt.bounce - 1, pt.wi, pt.tri, pt.surface(),
                                         weight, pt.d_color, B == 1);
     if (EXT && mag) *mag = abs_sum(er.dv0) + abs_sum(er.dv1);
     if (!is_zero(er.dv0) || !is_zero(er.dv1)) {
@@ -637,7 +640,7 @@ DEV void propagate_dp(const DevScene &s, const PointRecord &pt, int W, int H, in
 }
 
 // Primary-edge sample i (delta_ray.cpp:1478-1522).
-template <class G>
+template <int BMAX = 1 << 30, class G>
 DEV void primary_edge_item(const DevScene &s, long long i, int W, int H, int spp, int B, uint64_t seed,
                            const float *d_image, G &g) {
     if (s.num_prim_edges == 0) return;
@@ -650,7 +653,7 @@ DEV void primary_edge_item(const DevScene &s, long long i, int W, int H, int spp
     EdgeSample es = draw_edge(r);
     LightSample ls = draw_light(r);
     PrimaryEdgeResult pr;
-    primary_edge_sample(s, es, s.prim_edges[id], ls, r, B, d_image, W, H, w / spp, pr);
+    primary_edge_sample<BMAX>(s, es, s.prim_edges[id], ls, r, B, d_image, W, H, w / spp, pr);
     if (!pr.ok) return;
     const DevShape &sh = s.shapes[pr.edge.shape];
     g.add(sh.grad_v + 3 * pr.edge.v0 + 0, pr.dv0.x);

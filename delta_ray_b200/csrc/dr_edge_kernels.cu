@@ -69,7 +69,9 @@ __global__ void __launch_bounds__(128, 4) k_edge_traverse(DevScene s, uint64_t s
     }
 }
 
-template <bool EXT>
+// EXT: DR_FLAG_EDGE_LOBE_MIS or proposal training in use; GI: max_bounces > 1
+// (the shade calls of the two sides); the launcher picks the variant.
+template <bool EXT, bool GI>
 __global__ void __launch_bounds__(128, 4) k_edge_eval(DevScene s, int W, int H, int spp, int B, uint64_t seed, int dp_mode,
                                                    float *grad, BackwardWorkspace ws, GradCacheCfg cfg) {
     extern __shared__ float sm[];
@@ -81,7 +83,7 @@ __global__ void __launch_bounds__(128, 4) k_edge_eval(DevScene s, int W, int H, 
         pt.load(ws.pt + (size_t)it.x * DR_PT_WORDS);
         int tree = it.y >> 30, ei = it.y & ((1 << 30) - 1);
         float mag = 0.f;
-        float3 dp = eval_item<EXT>(s, pt, tree, ei, it.z, ws.item_w[i], spp, B, seed, bg, &mag);
+        float3 dp = eval_item<EXT, GI>(s, pt, tree, ei, it.z, ws.item_w[i], spp, B, seed, bg, &mag);
         if (EXT && ws.train_targets && mag > 0.f && it.x % ws.train_stride == 0 && it.x / ws.train_stride < ws.train_n) {
             // the proposal's training target: contribution magnitude per direction bin
             atomicAdd(ws.train_targets + 32 * (size_t)(it.x / ws.train_stride) + (it.w & 31), mag);
@@ -107,13 +109,14 @@ __global__ void __launch_bounds__(128, 4) k_edge_eval(DevScene s, int W, int H, 
     block_grad_flush(bg);
 }
 
+template <int BMAX>
 __global__ void __launch_bounds__(128, 3) k_primary_edges(DevScene s, int W, int H, int spp, int B, uint64_t seed,
                                                        const float *d_image, long long n, float *grad,
                                                        GradCacheCfg cfg) {
     extern __shared__ float sm[];
     BlockGrad bg = block_grad_begin(sm, grad, cfg);
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
-        primary_edge_item(s, i, W, H, spp, B, seed, d_image, bg);
+        primary_edge_item<BMAX>(s, i, W, H, spp, B, seed, d_image, bg);
     block_grad_flush(bg);
 }
 
@@ -130,10 +133,10 @@ cudaError_t dr_launch_edge_eval(const DevScene &s, int W, int H, int spp, int B,
                                 float *grad, const BackwardWorkspace &ws, const GradCacheCfg &cfg, int num_sms,
                                 cudaStream_t st) {
     size_t smem = sizeof(float) * (size_t)(cfg.head + cfg.tail_len);
-    if (s.edge_lobe_mis || ws.train_targets)
-        k_edge_eval<true><<<stage_grid(num_sms), 128, smem, st>>>(s, W, H, spp, B, seed, dp_mode, grad, ws, cfg);
-    else
-        k_edge_eval<false><<<stage_grid(num_sms), 128, smem, st>>>(s, W, H, spp, B, seed, dp_mode, grad, ws, cfg);
+    const bool ext = s.edge_lobe_mis || ws.train_targets;
+    auto kernel = ext ? (B > 1 ? k_edge_eval<true, true> : k_edge_eval<true, false>)
+                      : (B > 1 ? k_edge_eval<false, true> : k_edge_eval<false, false>);
+    kernel<<<stage_grid(num_sms), 128, smem, st>>>(s, W, H, spp, B, seed, dp_mode, grad, ws, cfg);
     return cudaGetLastError();
 }
 
@@ -143,7 +146,8 @@ cudaError_t dr_launch_primary_edges(const DevScene &s, int W, int H, int spp, in
     const int bs = 128;
     size_t smem = sizeof(float) * (size_t)(cfg.head + cfg.tail_len);
     long long nb = std::min<long long>(blocks_for(n, bs), (long long)stage_grid(num_sms) * 4);
-    k_primary_edges<<<(int)nb, bs, smem, st>>>(s, W, H, spp, B, seed, d_image, n, grad, cfg);
+    auto kernel = B == 1 ? k_primary_edges<1> : k_primary_edges<(1 << 30)>;
+    kernel<<<(int)nb, bs, smem, st>>>(s, W, H, spp, B, seed, d_image, n, grad, cfg);
     return cudaGetLastError();
 }
 

@@ -503,7 +503,7 @@ DEV_NOINLINE float other_lobe_density(const DevScene &s, int mi, const SurfacePo
 
 // Secondary edge sample (delta_ray.cpp:45-365).  `rng` holds the item's
 // secondary samples (for the two shade calls, replayed from the same state).
-template <bool EXT = true>
+template <bool EXT = true, bool MAYBE_GI = true>
 DEV EdgeResult shading_edge_sample(const DevScene &s, const EdgeSample &es, const DevEdge &edge, const LightSample &ls,
                                    const Rng &rng, int nbounces, float3 wi, int stri, const SurfacePoint &sp,
                                    float3 weight, float3 d_color, bool direct_only) {
@@ -610,7 +610,7 @@ DEV EdgeResult shading_edge_sample(const DevScene &s, const EdgeSample &es, cons
     float3 eb = bsdf(s, mi, sp, wi, sdir);
     if (sum(eb) < 1e-6f) return none;
     float3 shr = f3(0.f), shl = f3(0.f);
-    if (!direct_only) {
+    if (MAYBE_GI && !direct_only) {
 #pragma unroll 1
         for (int k = 0; k < 2; k++) {
             int tri = k == 0 ? hr.tri : hl.tri;
@@ -821,6 +821,7 @@ struct PrimaryEdgeResult {
     float dw2c[16];
 };
 
+template <int BMAX = 1 << 30>
 DEV void primary_edge_sample(const DevScene &s, const EdgeSample &es, const DevEdge &edge, const LightSample &ls,
                              const Rng &rng, int B, const float *d_image, int W, int H, float weight,
                              PrimaryEdgeResult &r) {
@@ -873,7 +874,8 @@ DEV void primary_edge_sample(const DevScene &s, const EdgeSample &es, const DevE
         int tri = k == 0 ? hr.tri : hl.tri;
         Ray ray = k == 0 ? rray : lray;
         float3 col = f3(0.f);
-        if (tri >= 0) col = shade(s, -ray.d, tri, intersect_tri(load_tri(s, tri), ray.o, ray.d), ls, rng, B, true);
+        if (tri >= 0)
+            col = shade<BMAX>(s, -ray.d, tri, intersect_tri(load_tri(s, tri), ray.o, ray.d), ls, rng, B, true);
         if (k == 0) rcol = col;
         else lcol = col;
     }

@@ -87,8 +87,8 @@ DEV float tex_fetch(const DevScene &s, int off, int w, int ch, int y, int x, int
     return dr_ldg(s.texels + off + (y * w + x) * ch + c);
 }
 
-DEV float3 tex3(const DevScene &s, int off, int w, int h, const float *cval, float2 uv) {
-    if (off < 0) return f3(cval[0], cval[1], cval[2]);
+// Bilinear lookups out of line (called from many sites); constants inline.
+DEV_NOINLINE float3 tex3_bilinear(const DevScene &s, int off, int w, int h, float2 uv) {
     TexFoot t = tex_foot(w, h, uv);
     float3 r;
     for (int c = 0; c < 3; c++) {
@@ -98,13 +98,20 @@ DEV float3 tex3(const DevScene &s, int off, int w, int h, const float *cval, flo
     }
     return r;
 }
+DEV float3 tex3(const DevScene &s, int off, int w, int h, const float *cval, float2 uv) {
+    if (off < 0) return f3(cval[0], cval[1], cval[2]);
+    return tex3_bilinear(s, off, w, h, uv);
+}
 
-DEV float tex1(const DevScene &s, int off, int w, int h, float cval, float2 uv) {
-    if (off < 0) return cval;
+DEV_NOINLINE float tex1_bilinear(const DevScene &s, int off, int w, int h, float2 uv) {
     TexFoot t = tex_foot(w, h, uv);
     float ff = tex_fetch(s, off, w, 1, t.yf, t.xf, 0), fc = tex_fetch(s, off, w, 1, t.yc, t.xf, 0);
     float cf = tex_fetch(s, off, w, 1, t.yf, t.xc, 0), cc = tex_fetch(s, off, w, 1, t.yc, t.xc, 0);
     return ff * (1.f - t.u) * (1.f - t.v) + fc * (1.f - t.u) * t.v + cf * t.u * (1.f - t.v) + cc * t.u * t.v;
+}
+DEV float tex1(const DevScene &s, int off, int w, int h, float cval, float2 uv) {
+    if (off < 0) return cval;
+    return tex1_bilinear(s, off, w, h, uv);
 }
 
 DEV float2 scale_uv(float2 uv, const float *sc) {
@@ -377,8 +384,11 @@ DEV BounceHit sample_bsdf_scene(const DevScene &s, const BSDFSample &bs, float3 
 
 // shade (pathtrace.h:179-297), forward only.  `rng` is positioned at the first
 // secondary sample; it is taken by value so callers can replay the same draws.
+// BMAX bounds max_bounces at compile time (1: the direct-lighting variant).
+template <int BMAX = 1 << 30>
 DEV float3 shade(const DevScene &s, float3 wi, int ptri, const SurfacePoint &psp, const LightSample &ls, Rng rng,
                  int max_bounces, bool include_primary_light) {
+    if (max_bounces > BMAX) max_bounces = BMAX;
     float3 color = f3(0.f);
     if (ptri < 0) return color;
     if (include_primary_light) {
