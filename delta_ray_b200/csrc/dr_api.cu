@@ -82,7 +82,7 @@ template <typename T> std::vector<T> fetch(const T *src, size_t count, const cha
 // reference's RenderFunction does) allocates them once.  Only idle queues are
 // cached; `idle` orders their reuse after the last kernels that touched them.
 struct BackwardQueues {
-    DevBuf pt, items, item_w, item_dp, pt_last, counts;
+    DevBuf pt, items, item_w, item_dp, pt_last, counts, survivors;
     long long cap_items = 0;     // grown on overflow, kept with the buffers
     double points_per_sample = 1;  // shading points per pixel sample the last overflow asked for
     cudaEvent_t idle = nullptr;
@@ -332,9 +332,10 @@ void check_render_desc(const dr_scene *sc, const dr_render_desc *rd) {
     if (sc->ds.num_lights == 0) throw DrError(DR_ERR_INVALID_ARGUMENT, "scene has no lights");
 }
 
-// Item queue limit of dr_render_backward: 8 GiB of edge items (32 bytes each:
-// the item, its weight and its dp).  Edge stages with more items stream.
-constexpr long long kMaxQueueItems = (8ll << 30) / 32;
+// Item queue limit of dr_render_backward: 8 GiB of edge items (64 bytes each:
+// the item, its weight, its dp and its slot in the survivor queue of the
+// evaluation wavefront).  Edge stages with more items stream.
+constexpr long long kMaxQueueItems = (8ll << 30) / 64;
 
 void check_backward_args(const dr_scene *scene, const dr_render_desc *rd, const float *d_image_dev,
                          const float *grad_dev) {
@@ -628,10 +629,12 @@ dr_status dr_render_backward(dr_scene *scene, const dr_render_desc *rd, const fl
             q.items.reserve(sizeof(int4) * cap_items);
             q.item_w.reserve(sizeof(float) * cap_items);
             q.item_dp.reserve(sizeof(float) * 3 * cap_items);
+            q.survivors.reserve(sizeof(float4) * 2 * cap_items);
             q.cap_items = cap_items;
             ws.items = q.items.as<int4>();
             ws.item_w = q.item_w.as<float>();
             ws.item_dp = q.item_dp.as<float>();
+            ws.survivors = q.survivors.as<float4>();
             ws.cap_items = cap_items;
         };
         auto bind_points = [&]() {
@@ -918,7 +921,7 @@ dr_status dr_render_backward_noalloc(dr_scene *scene, const dr_render_desc *rd, 
         cudaStream_t st = (cudaStream_t)stream;
         scene->last_launches = 0;
         unsigned char *base = noalloc_scratch(scene->device);
-        // layout: counters | point records | point keys | items | item weights | item dp
+        // layout: counters | point records | point keys | items | item weights | item dp | survivors
         auto up = [](size_t b) { return (b + 255) & ~size_t(255); };
         // scenes with specular chains: room for the points of every bounce,
         // up to half the scratch (the rest holds edge items)
@@ -935,13 +938,16 @@ dr_status dr_render_backward_noalloc(dr_scene *scene, const dr_render_desc *rd, 
         off += up(sizeof(float) * DR_PT_FLOATS * (size_t)cap_points);
         ws.pt_last = (unsigned long long *)(base + off);
         off += up(DR_PT_LAST_BYTES * (size_t)cap_points);
-        long long cap_items = (long long)((kNoAllocScratchBytes - off - 3 * 256) / (sizeof(int4) + 4 * sizeof(float)));
+        long long cap_items = (long long)((kNoAllocScratchBytes - off - 4 * 256) /
+                                          (sizeof(int4) + 4 * sizeof(float) + 2 * sizeof(float4)));
         ws.items = (int4 *)(base + off);
         off += up(sizeof(int4) * (size_t)cap_items);
         ws.item_w = (float *)(base + off);
         off += up(sizeof(float) * (size_t)cap_items);
         ws.item_dp = (float *)(base + off);
         off += up(sizeof(float) * 3 * (size_t)cap_items);
+        ws.survivors = (float4 *)(base + off);
+        off += up(sizeof(float4) * 2 * (size_t)cap_items);
         if (off > kNoAllocScratchBytes) throw DrError(DR_ERR_INVALID_ARGUMENT, "scratch layout does not fit");
         ws.cap_points = cap_points;
         ws.cap_items = cap_items;

@@ -153,10 +153,8 @@ cudaError_t dr_launch_backward_back(const DevScene &s, int W, int H, int spp, in
     const int bs = 128;
     size_t smem = sizeof(float) * (size_t)(cfg.head + cfg.tail_len);
     int grid_ws = stage_grid(num_sms);
-    cudaError_t e = dr_launch_edge_eval(s, W, H, spp, B, seed, dp_mode, grad, ws, cfg, num_sms, st);
+    cudaError_t e = dr_launch_edge_eval(s, W, H, spp, B, seed, dp_mode, grad, ws, cfg, num_sms, st, launches, timer);
     if (e != cudaSuccess) return e;
-    timer->mark(st, "k_edge_eval");
-    *launches += 1;
     if (dp_mode != DR_DP_SUM || s.specular_chains) {
         if (s.specular_chains) k_dp_propagate<true><<<grid_ws, bs, smem, st>>>(s, W, H, spp, seed, dp_mode, grad, ws, cfg);
         else k_dp_propagate<false><<<grid_ws, bs, smem, st>>>(s, W, H, spp, seed, dp_mode, grad, ws, cfg);

@@ -537,19 +537,27 @@ DEV bool traverse_point(const DevScene &s, const PointRecord &pt, uint64_t seed,
 // *mag (if given) receives the sample's contribution magnitude |dv0|_1 + |dv1|_1.
 // EXT = false compiles the variant without DR_FLAG_EDGE_LOBE_MIS and without
 // the magnitude (the kernels choose it when neither is in use).
-template <bool EXT = true, bool MAYBE_GI = true, class G>
-DEV float3 eval_item(const DevScene &s, const PointRecord &pt, int tree, int ei, int j, float w, int spp, int B,
-                     uint64_t seed, G &g, float *mag = nullptr) {
+// The item's line sample (first phase); false: the item contributes nothing.
+template <bool EXT = true>
+DEV bool item_line(const DevScene &s, const PointRecord &pt, int tree, int ei, uint64_t seed, EdgeLine &el) {
     Rng prng;
     prng.init(seed, kStreamEdgePoint, pt.sid, (uint32_t)pt.bounce);
     EdgeSample es = draw_edge(prng);
+    const DevEdge &edge = tree ? s.nrm_edges[ei] : s.sil_edges[ei];
+    return edge_line_sample<EXT>(s, es, edge, pt.wi, pt.tri, pt.surface(), el);
+}
+
+// The item's shading (second phase) from its line sample; as eval_item.
+template <bool EXT = true, bool MAYBE_GI = true, class G>
+DEV float3 item_shade(const DevScene &s, const PointRecord &pt, int tree, int ei, int j, float w, int spp, int B,
+                      uint64_t seed, G &g, float *mag, const EdgeLine &el) {
     Rng irng;
     irng.init(seed, kStreamEdgeItem, pt.sid, ((uint32_t)pt.bounce << 16) | (uint32_t)j);
     LightSample els = draw_light(irng);
     const DevEdge &edge = tree ? s.nrm_edges[ei] : s.sil_edges[ei];
     float3 weight = f3(1.f) * ((1.f / spp) * w);
-    EdgeResult er = shading_edge_sample<EXT, MAYBE_GI>(s, es, edge, els, irng, B - pt.bounce - 1, pt.wi, pt.tri, pt.surface(),
-                                        weight, pt.d_color, B == 1);
+    EdgeResult er = edge_shade_sample<MAYBE_GI>(s, el, edge, els, irng, B - pt.bounce - 1, pt.wi, pt.tri,
+                                                pt.surface(), weight, pt.d_color, B == 1);
     if (EXT && mag) *mag = abs_sum(er.dv0) + abs_sum(er.dv1);
     if (!is_zero(er.dv0) || !is_zero(er.dv1)) {
         const DevShape &sh = s.shapes[edge.shape];
@@ -561,6 +569,17 @@ DEV float3 eval_item(const DevScene &s, const PointRecord &pt, int tree, int ei,
         g.add(sh.grad_v + 3 * edge.v1 + 2, er.dv1.z);
     }
     return er.dp;
+}
+
+template <bool EXT = true, bool MAYBE_GI = true, class G>
+DEV float3 eval_item(const DevScene &s, const PointRecord &pt, int tree, int ei, int j, float w, int spp, int B,
+                     uint64_t seed, G &g, float *mag = nullptr) {
+    EdgeLine el;
+    if (!item_line<EXT>(s, pt, tree, ei, seed, el)) {
+        if (EXT && mag) *mag = 0.f;
+        return f3(0.f);
+    }
+    return item_shade<EXT, MAYBE_GI>(s, pt, tree, ei, j, w, spp, B, seed, g, mag, el);
 }
 
 // dp of a shading point pushed back along its path to the camera and the

@@ -69,8 +69,39 @@ __global__ void __launch_bounds__(128, 4) k_edge_traverse(DevScene s, uint64_t s
     }
 }
 
+// What follows an item's evaluation: the proposal's training target and the
+// position adjoint (pushed back now in DR_DP_SUM mode, else keyed for the
+// reference's "last edge" rule).
+template <bool EXT, class G>
+__device__ __forceinline__ void finish_item(const DevScene &s, const BackwardWorkspace &ws, const int4 &it,
+                                            long long i, const PointRecord &pt, float3 dp, float mag, int W, int H,
+                                            int spp, uint64_t seed, int dp_mode, G &bg) {
+    if (EXT && ws.train_targets && mag > 0.f && it.x % ws.train_stride == 0 && it.x / ws.train_stride < ws.train_n) {
+        // the proposal's training target: contribution magnitude per direction bin
+        atomicAdd(ws.train_targets + 32 * (size_t)(it.x / ws.train_stride) + (it.w & 31), mag);
+    }
+    if (is_zero(dp)) return;
+    if (dp_mode == DR_DP_SUM) {
+        if (pt.bounce == 0) {
+            propagate_dp<false>(s, pt, W, H, spp, seed, dp, bg);
+        } else {  // after specular samples: summed here, the chain is traced by k_dp_propagate
+            float *a = reinterpret_cast<float *>(ws.pt_last) + 4 * (size_t)it.x;
+            atomicAdd(a, dp.x);
+            atomicAdd(a + 1, dp.y);
+            atomicAdd(a + 2, dp.z);
+        }
+    } else {
+        ws.item_dp[3 * i] = dp.x;
+        ws.item_dp[3 * i + 1] = dp.y;
+        ws.item_dp[3 * i + 2] = dp.z;
+        unsigned long long key = ((unsigned long long)(it.z + 1) << 32) | (unsigned long long)i;
+        atomicMax(ws.pt_last + it.x, key);
+    }
+}
+
 // EXT: DR_FLAG_EDGE_LOBE_MIS or proposal training in use; GI: max_bounces > 1
 // (the shade calls of the two sides); the launcher picks the variant.
+// One thread evaluates each item whole (the no-alloc backward's path).
 template <bool EXT, bool GI>
 __global__ void __launch_bounds__(128, 4) k_edge_eval(DevScene s, int W, int H, int spp, int B, uint64_t seed, int dp_mode,
                                                    float *grad, BackwardWorkspace ws, GradCacheCfg cfg) {
@@ -84,27 +115,60 @@ __global__ void __launch_bounds__(128, 4) k_edge_eval(DevScene s, int W, int H, 
         int tree = it.y >> 30, ei = it.y & ((1 << 30) - 1);
         float mag = 0.f;
         float3 dp = eval_item<EXT, GI>(s, pt, tree, ei, it.z, ws.item_w[i], spp, B, seed, bg, &mag);
-        if (EXT && ws.train_targets && mag > 0.f && it.x % ws.train_stride == 0 && it.x / ws.train_stride < ws.train_n) {
-            // the proposal's training target: contribution magnitude per direction bin
-            atomicAdd(ws.train_targets + 32 * (size_t)(it.x / ws.train_stride) + (it.w & 31), mag);
+        finish_item<EXT>(s, ws, it, i, pt, dp, mag, W, H, spp, seed, dp_mode, bg);
+    }
+    block_grad_flush(bg);
+}
+
+// Edge evaluation as a two-kernel wavefront.  k_edge_line: the line sample of
+// every item (silhouette test, LTC lobe, point on the edge); the survivors
+// (often half the items: edges in the point's own plane, below the lobe's
+// horizon or outside the clipped segment end here) are compacted, so that
+// k_edge_shade runs its rays and shading with full warps.
+template <bool EXT>
+__global__ void __launch_bounds__(128, 4) k_edge_line(DevScene s, uint64_t seed, BackwardWorkspace ws) {
+    long long n = (long long)min(ws.counters->items, (unsigned long long)ws.cap_items);
+    long long stride = (long long)gridDim.x * blockDim.x;
+    // warp-uniform loop: the survivor append is warp-aggregated
+    for (long long base = (long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < n; base += stride) {
+        long long i = base + (threadIdx.x & 31);
+        EdgeLine el;
+        bool ok = false;
+        if (i < n) {
+            int4 it = ws.items[i];
+            PointRecord pt;
+            pt.load(ws.pt + (size_t)it.x * DR_PT_WORDS);
+            ok = item_line<EXT>(s, pt, it.y >> 30, it.y & ((1 << 30) - 1), seed, el);
         }
-        if (is_zero(dp)) continue;
-        if (dp_mode == DR_DP_SUM) {
-            if (pt.bounce == 0) {
-                propagate_dp<false>(s, pt, W, H, spp, seed, dp, bg);
-            } else {  // after specular samples: summed here, the chain is traced by k_dp_propagate
-                float *a = reinterpret_cast<float *>(ws.pt_last) + 4 * (size_t)it.x;
-                atomicAdd(a, dp.x);
-                atomicAdd(a + 1, dp.y);
-                atomicAdd(a + 2, dp.z);
-            }
-        } else {
-            ws.item_dp[3 * i] = dp.x;
-            ws.item_dp[3 * i + 1] = dp.y;
-            ws.item_dp[3 * i + 2] = dp.z;
-            unsigned long long key = ((unsigned long long)(it.z + 1) << 32) | (unsigned long long)i;
-            atomicMax(ws.pt_last + it.x, key);
+        __syncwarp();
+        unsigned long long slot = warp_reserve(&ws.counters->survivors, ok ? 1 : 0);
+        if (ok) {
+            ws.survivors[2 * slot] = make_float4(__int_as_float((int)i), el.sample_p.x, el.sample_p.y, el.sample_p.z);
+            ws.survivors[2 * slot + 1] = make_float4(el.mwt.x, el.mwt.y, el.mwt.z, el.q);
         }
+    }
+}
+
+template <bool EXT, bool GI>
+__global__ void __launch_bounds__(128, 4) k_edge_shade(DevScene s, int W, int H, int spp, int B, uint64_t seed,
+                                                    int dp_mode, float *grad, BackwardWorkspace ws, GradCacheCfg cfg) {
+    extern __shared__ float sm[];
+    BlockGrad bg = block_grad_begin(sm, grad, cfg);
+    long long n = (long long)min(ws.counters->survivors, (unsigned long long)ws.cap_items);
+    for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
+        float4 a = ws.survivors[2 * k], b = ws.survivors[2 * k + 1];
+        long long i = __float_as_int(a.x);
+        EdgeLine el;
+        el.sample_p = f3(a.y, a.z, a.w);
+        el.mwt = f3(b.x, b.y, b.z);
+        el.q = b.w;
+        int4 it = ws.items[i];
+        PointRecord pt;
+        pt.load(ws.pt + (size_t)it.x * DR_PT_WORDS);
+        int tree = it.y >> 30, ei = it.y & ((1 << 30) - 1);
+        float mag = 0.f;
+        float3 dp = item_shade<EXT, GI>(s, pt, tree, ei, it.z, ws.item_w[i], spp, B, seed, bg, &mag, el);
+        finish_item<EXT>(s, ws, it, i, pt, dp, mag, W, H, spp, seed, dp_mode, bg);
     }
     block_grad_flush(bg);
 }
@@ -131,12 +195,28 @@ cudaError_t dr_launch_edge_traverse(const DevScene &s, uint64_t seed, const Back
 
 cudaError_t dr_launch_edge_eval(const DevScene &s, int W, int H, int spp, int B, uint64_t seed, int dp_mode,
                                 float *grad, const BackwardWorkspace &ws, const GradCacheCfg &cfg, int num_sms,
-                                cudaStream_t st) {
+                                cudaStream_t st, int *launches, StageTimer *timer) {
     size_t smem = sizeof(float) * (size_t)(cfg.head + cfg.tail_len);
     const bool ext = s.edge_lobe_mis || ws.train_targets;
-    auto kernel = ext ? (B > 1 ? k_edge_eval<true, true> : k_edge_eval<true, false>)
-                      : (B > 1 ? k_edge_eval<false, true> : k_edge_eval<false, false>);
-    kernel<<<stage_grid(num_sms), 128, smem, st>>>(s, W, H, spp, B, seed, dp_mode, grad, ws, cfg);
+    const int grid = stage_grid(num_sms);
+    if (!ws.survivors) {
+        auto kernel = ext ? (B > 1 ? k_edge_eval<true, true> : k_edge_eval<true, false>)
+                          : (B > 1 ? k_edge_eval<false, true> : k_edge_eval<false, false>);
+        kernel<<<grid, 128, smem, st>>>(s, W, H, spp, B, seed, dp_mode, grad, ws, cfg);
+        timer->mark(st, "k_edge_eval");
+        *launches += 1;
+        return cudaGetLastError();
+    }
+    cudaError_t e = cudaMemsetAsync(&ws.counters->survivors, 0, sizeof(unsigned long long), st);
+    if (e != cudaSuccess) return e;
+    if (ext) k_edge_line<true><<<grid, 128, 0, st>>>(s, seed, ws);
+    else k_edge_line<false><<<grid, 128, 0, st>>>(s, seed, ws);
+    timer->mark(st, "k_edge_line");
+    auto shade = ext ? (B > 1 ? k_edge_shade<true, true> : k_edge_shade<true, false>)
+                     : (B > 1 ? k_edge_shade<false, true> : k_edge_shade<false, false>);
+    shade<<<grid, 128, smem, st>>>(s, W, H, spp, B, seed, dp_mode, grad, ws, cfg);
+    timer->mark(st, "k_edge_shade");
+    *launches += 2;
     return cudaGetLastError();
 }
 

@@ -501,14 +501,22 @@ DEV_NOINLINE float other_lobe_density(const DevScene &s, int mi, const SurfacePo
     return lobe_line_density(ominv, v0 - sp.p, v1 - sp.p, sample_p, q_l);
 }
 
-// Secondary edge sample (delta_ray.cpp:45-365).  `rng` holds the item's
-// secondary samples (for the two shade calls, replayed from the same state).
-template <bool EXT = true, bool MAYBE_GI = true>
-DEV EdgeResult shading_edge_sample(const DevScene &s, const EdgeSample &es, const DevEdge &edge, const LightSample &ls,
-                                   const Rng &rng, int nbounces, float3 wi, int stri, const SurfacePoint &sp,
-                                   float3 weight, float3 d_color, bool direct_only) {
-    EdgeResult none;
-    none.dp = none.dv0 = none.dv1 = f3(0.f);
+// Secondary edge sample (delta_ray.cpp:45-365), in two phases: the line
+// sample on the edge (edge_line_sample: the silhouette test, the LTC lobe, the
+// point on the edge and the density it was drawn with) and the shading of the
+// two sides (edge_shade_sample: rays, shading, Jacobians).  The backward pass
+// runs them as two kernels with the surviving line samples compacted in
+// between; shading_edge_sample runs both.
+struct EdgeLine {
+    float3 sample_p;  // the sampled point on the edge, relative to the shading point
+    float3 mwt;       // d sample_p / d l (the lobe transform times the line direction)
+    float q;          // density of l: the picked lobe's pmf times its line pdf (or the lobe mixture)
+};
+
+template <bool EXT = true>
+DEV bool edge_line_sample(const DevScene &s, const EdgeSample &es, const DevEdge &edge, float3 wi, int stri,
+                          const SurfacePoint &sp, EdgeLine &out) {
+    const bool none = false;
     if (stri < 0) return none;
     if (!is_silhouette(s, sp.p, edge)) return none;
     float3 v0 = edge_v0(s, edge), v1 = edge_v1(s, edge);
@@ -572,6 +580,31 @@ DEV EdgeResult shading_edge_sample(const DevScene &s, const EdgeSample &es, cons
     }
     if (pdf(l) <= 0.f) return none;
     float3 sample_p = mul(m, vo + l * wt);
+    // DR_FLAG_EDGE_LOBE_MIS: the one-sample balance heuristic over the two
+    // lobes, pmf_sel pdf_sel(l) + pmf_other pdf_other(l); the reference divides
+    // by pmf_sel pdf_sel(l) alone
+    float q_mix = mpmf * pdf(l);
+    if (EXT && s.edge_lobe_mis) {
+        bool sel_diffuse = es.bsdf_component <= dpmf;
+        float opmf = sel_diffuse ? spmf : dpmf;
+        if (opmf > 0.f)
+            q_mix += opmf * other_lobe_density(s, mi, sp, wi, frame, sel_diffuse, v0, v1, sample_p, mul(m, wt));
+    }
+    out.sample_p = sample_p;
+    out.mwt = mul(m, wt);
+    out.q = q_mix;
+    return true;
+}
+
+template <bool MAYBE_GI = true>
+DEV EdgeResult edge_shade_sample(const DevScene &s, const EdgeLine &el_, const DevEdge &edge, const LightSample &ls,
+                                 const Rng &rng, int nbounces, float3 wi, int stri, const SurfacePoint &sp,
+                                 float3 weight, float3 d_color, bool direct_only) {
+    EdgeResult none;
+    none.dp = none.dv0 = none.dv1 = f3(0.f);
+    const float3 sample_p = el_.sample_p;
+    float3 v0 = edge_v0(s, edge), v1 = edge_v1(s, edge);
+    int mi = material_of_tri(s, stri);
     float3 split_n = normalize(cross(v0 - sp.p, v1 - sp.p));
     float delta = 1e-3f * length(sample_p);
     float3 sdir = normalize(sample_p);
@@ -643,21 +676,10 @@ DEV EdgeResult shading_edge_sample(const DevScene &s, const EdgeSample &es, cons
         if (length(dir) * fabsf(dot(normalize(dir), pl.ng)) < 1e-3f) return none;
     }
     EdgeResult res = none;
-    float pdf_l = pdf(l);
-    // DR_FLAG_EDGE_LOBE_MIS: the one-sample balance heuristic over the two
-    // lobes, pmf_sel pdf_sel(l) + pmf_other pdf_other(l); the reference divides
-    // by pmf_sel pdf_sel(l) alone
-    float q_mix = mpmf * pdf_l;
-    if (EXT && s.edge_lobe_mis) {
-        bool sel_diffuse = es.bsdf_component <= dpmf;
-        float opmf = sel_diffuse ? spmf : dpmf;
-        if (opmf > 0.f)
-            q_mix += opmf * other_lobe_density(s, mi, sp, wi, frame, sel_diffuse, v0, v1, sample_p, mul(m, wt));
-    }
     auto accum = [&](const SurfacePoint &lp, float3 ev) {
         M3 nj = normalize_jacobian(sample_p);
         M3 ij = intersect_jacobian(sdir, lp.p, lp.ng);
-        float line_j = length(mul(mul(mul(ij, nj), m), wt)) / q_mix;
+        float line_j = length(mul(mul(ij, nj), el_.mwt)) / el_.q;
         float3 p = sp.p, x = lp.p;
         float3 d0 = v0 - p, d1 = v1 - p;
         float dirac_j = length(cross(d0, d1));
@@ -677,6 +699,19 @@ DEV EdgeResult shading_edge_sample(const DevScene &s, const EdgeSample &es, cons
         if (tri >= 0 && abs_sum(e) > 0.f) accum(k == 0 ? pr : pl, k == 0 ? e : -e);
     }
     return res;
+}
+
+template <bool EXT = true, bool MAYBE_GI = true>
+DEV EdgeResult shading_edge_sample(const DevScene &s, const EdgeSample &es, const DevEdge &edge, const LightSample &ls,
+                                   const Rng &rng, int nbounces, float3 wi, int stri, const SurfacePoint &sp,
+                                   float3 weight, float3 d_color, bool direct_only) {
+    EdgeLine el;
+    if (!edge_line_sample<EXT>(s, es, edge, wi, stri, sp, el)) {
+        EdgeResult none;
+        none.dp = none.dv0 = none.dv1 = f3(0.f);
+        return none;
+    }
+    return edge_shade_sample<MAYBE_GI>(s, el, edge, ls, rng, nbounces, wi, stri, sp, weight, d_color, direct_only);
 }
 
 // ---------------------------------------------------------------------------

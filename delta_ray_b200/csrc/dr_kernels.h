@@ -49,6 +49,7 @@ struct BackwardCounters {
     unsigned long long items;   // edge items appended by the last k_edge_traverse
     int status;                 // DR_STATUS_* bits
     int pad;
+    unsigned long long survivors;  // line samples k_edge_line kept for k_edge_shade
 };
 
 struct BackwardWorkspace {
@@ -71,6 +72,10 @@ struct BackwardWorkspace {
     // bf16 slot probabilities, the mixture weight, and the training targets of
     // points p = k * train_stride, k < train_n ([train_n][32] f32 contribution
     // magnitudes per slot)
+    // line samples that survived the first phase of edge evaluation:
+    // [cap_items][2] float4 (item index bits, sample_p; d sample_p / d l, density);
+    // null: one kernel evaluates each item whole
+    float4 *survivors;
     const uint16_t *proposal_q;
     float proposal_alpha;
     float *train_targets;
@@ -100,10 +105,11 @@ cudaError_t dr_launch_proposal_features(const DevScene &s, const BackwardWorkspa
                                         float3 ih, void *x, void *xt, cudaStream_t st);
 cudaError_t dr_launch_edge_traverse(const DevScene &s, uint64_t seed, const BackwardWorkspace &ws, int num_sms,
                                     cudaStream_t st, int *launches, StageTimer *timer);
-// Single-kernel launchers of the edge half (dr_edge_kernels.cu).
+// Launchers of the edge half (dr_edge_kernels.cu).  Edge evaluation: the
+// two-kernel wavefront when ws.survivors is bound, one kernel otherwise.
 cudaError_t dr_launch_edge_eval(const DevScene &s, int W, int H, int spp, int B, uint64_t seed, int dp_mode,
                                 float *grad, const BackwardWorkspace &ws, const GradCacheCfg &cfg, int num_sms,
-                                cudaStream_t st);
+                                cudaStream_t st, int *launches, StageTimer *timer);
 cudaError_t dr_launch_primary_edges(const DevScene &s, int W, int H, int spp, int B, uint64_t seed,
                                     const float *d_image, long long n, float *grad, const GradCacheCfg &cfg,
                                     int num_sms, cudaStream_t st);

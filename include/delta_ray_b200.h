@@ -231,7 +231,7 @@ DR_API dr_status dr_render_backward(dr_scene *scene, const dr_render_desc *rd, c
  * array per device that is part of the library's module image.  Limits:
  * width * height * spp <= 65536 (larger calls fail with
  * DR_ERR_INVALID_ARGUMENT); sampled edges beyond the array's room (about
- * 800,000 at the largest image) are evaluated in several passes over the
+ * 400,000 at the largest image) are evaluated in several passes over the
  * shading points, and a single point with more edges than that fails with
  * DR_ERR_OUT_OF_MEMORY, as do specular chains whose shading points outgrow
  * half the array (about 150,000 points).  All calls on
