@@ -82,7 +82,7 @@ template <typename T> std::vector<T> fetch(const T *src, size_t count, const cha
 // reference's RenderFunction does) allocates them once.  Only idle queues are
 // cached; `idle` orders their reuse after the last kernels that touched them.
 struct BackwardQueues {
-    DevBuf pt, items, item_w, item_dp, pt_last, counts, survivors;
+    DevBuf pt, items, item_w, item_dp, pt_last, counts, survivors, tasks;
     long long cap_items = 0;     // grown on overflow, kept with the buffers
     double points_per_sample = 1;  // shading points per pixel sample the last overflow asked for
     cudaEvent_t idle = nullptr;
@@ -304,6 +304,12 @@ void collect_timings(dr_scene *sc, cudaStream_t st) {
     }
 }
 
+// Edge trees above this many nodes are walked in two stages (k_edge_expand,
+// k_edge_tasks): their points' walks are long and uneven.
+constexpr int kSplitTraversalNodes = 4096;
+// Task queue of the two-stage walk: up to 64 subtrees per point, at most 1 GiB.
+constexpr long long kTasksPerPoint = 64, kMaxTasks = (1ll << 30) / sizeof(EdgeTask);
+
 // The scene's device view with this call's per-render settings.
 DevScene call_scene(const dr_scene *sc, const dr_render_desc *rd) {
     DevScene ds = sc->ds;
@@ -311,6 +317,7 @@ DevScene call_scene(const dr_scene *sc, const dr_render_desc *rd) {
     ds.detached_pdf = (rd->flags & DR_FLAG_DETACHED_PDF) != 0;
     ds.edge_lobe_mis = (rd->flags & DR_FLAG_EDGE_LOBE_MIS) != 0;
     ds.specular_chains = sc->h.specular_bounces && rd->max_bounces >= 1;
+    ds.split_traversal = sc->ds.num_sil_nodes > kSplitTraversalNodes || sc->ds.num_nrm_nodes > kSplitTraversalNodes;
     return ds;
 }
 
@@ -647,6 +654,12 @@ dr_status dr_render_backward(dr_scene *scene, const dr_render_desc *rd, const fl
         bind_points();
         ws.counters = q.counts.as<BackwardCounters>();
         bind_items();
+        if (call_scene(scene, rd).split_traversal) {
+            long long cap_tasks = std::min(kMaxTasks, std::max(1ll << 16, kTasksPerPoint * cap_points));
+            q.tasks.reserve(sizeof(EdgeTask) * cap_tasks);
+            ws.tasks = q.tasks.as<EdgeTask>();
+            ws.cap_tasks = cap_tasks;
+        }
         // the item queue grows to what the traversal reported, up to its limit
         // (the grown queue is kept for later calls)
         auto grow = [&](long long want) {

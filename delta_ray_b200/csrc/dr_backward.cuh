@@ -516,21 +516,44 @@ DEV ConeSpec light_cone(const DevScene &s, int li, float3 p) {
 }
 
 // Samples the point's edges; emit(tree, edge_index, j, weight, slot_code) for
-// every sampled edge of nonzero weight, j counting all sampled edges in order.
-template <bool PROP, class Emit>
-DEV bool traverse_point(const DevScene &s, const PointRecord &pt, uint64_t seed, Emit &emit,
-                        const EdgeProposal &pr) {
+// every sampled edge of nonzero weight, j its key in the traversal order
+// (mode << 27 | edge index: keys grow in the order the reference visits).
+// CUT > 0: subtrees at depth CUT go to defer(code, bb, cpmf, apmf, lpmf)
+// (EdgeTask fields) instead of being walked here.
+template <bool PROP, int CUT = 0, class Emit, class Defer = NoDefer>
+DEV bool traverse_point(const DevScene &s, const PointRecord &pt, uint64_t seed, Emit &emit, const EdgeProposal &pr,
+                        Defer *defer = nullptr) {
     Rng prng;
     prng.init(seed, kStreamEdgePoint, pt.sid, (uint32_t)pt.bounce);
     draw_edge(prng);  // the point's edge sample; eval_item redraws it
+    NodeRng nrng;
+    nrng.seed = seed;
+    nrng.sid = pt.sid;
+    nrng.bounce = (uint32_t)pt.bounce;
     SurfacePoint sp = pt.surface();
     ConeSpec cone = light_cone(s, pt.light, sp.p);
-    int j = 0;
-    auto em = [&](int tree, int ei, float w, int code) {
-        if (w != 0.f) emit(tree, ei, j, w, code);
-        j++;
+    auto em = [&](int tree, int ei, int key, float w, int code) {
+        if (w != 0.f) emit(tree, ei, key, w, code);
     };
-    return traverse_edges<PROP>(s, pt.wi, pt.tri, sp, cone, prng, em, pr);
+    NoDefer nd;
+    if constexpr (CUT > 0) return traverse_edges<PROP, CUT>(s, pt.wi, pt.tri, sp, cone, prng, nrng, em, pr, *defer);
+    return traverse_edges<PROP, 0>(s, pt.wi, pt.tri, sp, cone, prng, nrng, em, pr, nd);
+}
+
+// Walks one handed-on subtree of the point (see traverse_point).
+template <bool PROP, class Emit>
+DEV bool traverse_point_task(const DevScene &s, const PointRecord &pt, uint64_t seed, const EdgeTask &task,
+                             Emit &emit, const EdgeProposal &pr) {
+    NodeRng nrng;
+    nrng.seed = seed;
+    nrng.sid = pt.sid;
+    nrng.bounce = (uint32_t)pt.bounce;
+    SurfacePoint sp = pt.surface();
+    ConeSpec cone = light_cone(s, pt.light, sp.p);
+    auto em = [&](int tree, int ei, int key, float w, int code) {
+        if (w != 0.f) emit(tree, ei, key, w, code);
+    };
+    return traverse_subtree<PROP>(s, pt.wi, pt.tri, sp, cone, nrng, task, em, pr);
 }
 
 // One sampled edge (delta_ray.cpp:901-973); returns dp, scatters dv0 / dv1;
@@ -552,7 +575,7 @@ template <bool EXT = true, bool MAYBE_GI = true, class G>
 DEV float3 item_shade(const DevScene &s, const PointRecord &pt, int tree, int ei, int j, float w, int spp, int B,
                       uint64_t seed, G &g, float *mag, const EdgeLine &el) {
     Rng irng;
-    irng.init(seed, kStreamEdgeItem, pt.sid, ((uint32_t)pt.bounce << 16) | (uint32_t)j);
+    irng.init(seed, kStreamEdgeItem, pt.sid, ((uint32_t)pt.bounce << 28) | (uint32_t)j);
     LightSample els = draw_light(irng);
     const DevEdge &edge = tree ? s.nrm_edges[ei] : s.sil_edges[ei];
     float3 weight = f3(1.f) * ((1.f / spp) * w);

@@ -299,7 +299,13 @@ HD void philox4x32_10(uint32_t &c0, uint32_t &c1, uint32_t &c2, uint32_t &c3, ui
     }
 }
 
-enum DrStreamKind : uint32_t { kStreamPixel = 0, kStreamEdgePoint = 1, kStreamEdgeItem = 2, kStreamPrimaryEdge = 3 };
+enum DrStreamKind : uint32_t {
+    kStreamPixel = 0,
+    kStreamEdgePoint = 1,
+    kStreamEdgeItem = 2,
+    kStreamPrimaryEdge = 3,
+    kStreamEdgeNode = 4
+};
 
 struct Rng {
     uint32_t k0, k1, id_lo, id_hi, sub, idx;
@@ -327,6 +333,23 @@ struct Rng {
         return (float)(x >> 8) * (1.f / 16777216.f);
     }
 };
+
+// The draws of an edge-tree traversal are keyed by node instead of by stream
+// position, so that the set of sampled edges does not depend on the order in
+// which the nodes are visited (a project convention, mirrored by the oracle):
+// stream kStreamEdgeNode of the point's sample id, sub = bounce << 28 |
+// mode << 27 | node (mode 0 cone, 1 all).
+struct NodeRng {
+    uint64_t seed, sid;
+    uint32_t bounce;
+    HD float draw(int mode, int node) const {
+        Rng r;
+        r.init(seed, kStreamEdgeNode, sid, (bounce << 28) | ((uint32_t)mode << 27) | (uint32_t)node);
+        return r.next();
+    }
+};
+// Node id of the learned proposal's once-per-traversal mixture draw.
+#define DR_NODE_MIX_DRAW 0x7FFFFFF
 
 // Sample records.  Field-fill order reproduces the reference compiled by GCC,
 // which evaluates function arguments right to left (light.h:46-51,

@@ -13,60 +13,143 @@
 // in a lane buffer; a full buffer reserves DR_ITEM_BUF slots with one atomic
 // (points of large glossy scenes sample thousands of edges), and the last
 // partial buffers of a warp share one atomic.
+// A lane's buffer of sampled edges: a full buffer reserves DR_ITEM_BUF slots
+// of the item queue with one atomic; flush_warp() (all lanes of a converged
+// warp) writes the rest with one atomic per warp.
+struct ItemWriter {
+    const BackwardWorkspace &ws;
+    int buf_p[DR_ITEM_BUF], buf_e[DR_ITEM_BUF], buf_j[DR_ITEM_BUF];
+    float buf_w[DR_ITEM_BUF];
+    uint8_t buf_c[DR_ITEM_BUF];
+    int nb = 0;
+    __device__ explicit ItemWriter(const BackwardWorkspace &w) : ws(w) {}
+    __device__ void write(unsigned long long first, int cnt) {
+        unsigned long long cap = (unsigned long long)ws.cap_items;
+        if (first + (unsigned long long)cnt > cap) set_status(&ws.counters->status, DR_STATUS_ITEM_OVERFLOW);
+        for (int k = 0; k < cnt; k++) {
+            unsigned long long i = first + (unsigned long long)k;
+            if (i >= cap) break;
+            int4 it;
+            it.x = buf_p[k];
+            it.y = buf_e[k];
+            it.z = buf_j[k];
+            it.w = buf_c[k];
+            ws.items[i] = it;
+            ws.item_w[i] = buf_w[k];
+        }
+    }
+    __device__ void add(int p, int tree, int ei, int j, float w, int code) {
+        if (nb == DR_ITEM_BUF) {
+            write(atomicAdd(&ws.counters->items, (unsigned long long)DR_ITEM_BUF), DR_ITEM_BUF);
+            nb = 0;
+        }
+        buf_p[nb] = p;
+        buf_e[nb] = (tree << 30) | ei;
+        buf_j[nb] = j;
+        buf_w[nb] = w;
+        buf_c[nb] = (uint8_t)code;
+        nb++;
+    }
+    __device__ void flush_warp() {
+        __syncwarp();
+        write(warp_reserve(&ws.counters->items, nb), nb);
+        nb = 0;
+    }
+};
+
+__device__ __forceinline__ EdgeProposal point_proposal(const BackwardWorkspace &ws, long long p) {
+    EdgeProposal pr;
+    pr.q = ws.proposal_q ? ws.proposal_q + 32 * (size_t)p : nullptr;
+    pr.alpha = ws.proposal_alpha;
+    pr.codes = ws.train_targets != nullptr;
+    return pr;
+}
+
+// One thread per shading point in [pt_begin, pt_end) walks the point's trees
+// (small trees: every point's walk is short).
 template <bool PROP>
 __global__ void __launch_bounds__(128, 4) k_edge_traverse(DevScene s, uint64_t seed, BackwardWorkspace ws) {
     long long n = min(min((long long)ws.counters->points, ws.cap_points), ws.pt_end);
     long long stride = (long long)gridDim.x * blockDim.x;
-    unsigned long long *count = &ws.counters->items;
+    ItemWriter out(ws);
     // warp-uniform loop: every lane of a warp takes the same number of trips
     for (long long base = ws.pt_begin + (long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < n;
          base += stride) {
         long long p = base + (threadIdx.x & 31);
-        bool active = p < n;
-        int buf_e[DR_ITEM_BUF];
-        float buf_w[DR_ITEM_BUF];
-        int buf_j[DR_ITEM_BUF];
-        uint8_t buf_c[DR_ITEM_BUF];
-        int nb = 0;
-        auto write_items = [&](unsigned long long first, int cnt) {
-            unsigned long long cap = (unsigned long long)ws.cap_items;
-            if (first + (unsigned long long)cnt > cap) set_status(&ws.counters->status, DR_STATUS_ITEM_OVERFLOW);
-            for (int k = 0; k < cnt; k++) {
-                unsigned long long i = first + (unsigned long long)k;
-                if (i >= cap) break;
-                int4 it;
-                it.x = (int)p;
-                it.y = buf_e[k];
-                it.z = buf_j[k];
-                it.w = buf_c[k];
-                ws.items[i] = it;
-                ws.item_w[i] = buf_w[k];
-            }
-        };
-        if (active) {
+        if (p < n) {
             PointRecord pt;
             pt.load(ws.pt + (size_t)p * DR_PT_WORDS);
-            auto emit = [&](int tree, int ei, int j, float w, int code) {
-                if (nb == DR_ITEM_BUF) {
-                    write_items(atomicAdd(count, (unsigned long long)DR_ITEM_BUF), DR_ITEM_BUF);
-                    nb = 0;
-                }
-                buf_e[nb] = (tree << 30) | ei;
-                buf_j[nb] = j;
-                buf_w[nb] = w;
-                buf_c[nb] = (uint8_t)code;
-                nb++;
-            };
-            EdgeProposal pr;
-            pr.q = ws.proposal_q ? ws.proposal_q + 32 * (size_t)p : nullptr;
-            pr.alpha = ws.proposal_alpha;
-            pr.codes = ws.train_targets != nullptr;
-            if (!traverse_point<PROP>(s, pt, seed, emit, pr))
+            auto emit = [&](int tree, int ei, int j, float w, int code) { out.add((int)p, tree, ei, j, w, code); };
+            if (!traverse_point<PROP>(s, pt, seed, emit, point_proposal(ws, p)))
                 set_status(&ws.counters->status, DR_STATUS_STACK_OVERFLOW);
         }
-        __syncwarp();
-        write_items(warp_reserve(count, nb), nb);
+        out.flush_warp();
     }
+}
+
+// Large trees, first stage: each point's walk stops DR_TASK_CUT levels below
+// the roots and hands the subtrees there on as tasks (a lane buffers 8 and
+// reserves their slots with one atomic; if the task queue is full, the lane
+// walks them itself).  The node-keyed draws make the sampled edges the same
+// as those of the one-pass walk.
+#define DR_TASK_CUT 8
+#define DR_TASK_BUF 8
+template <bool PROP>
+__global__ void __launch_bounds__(128, 4) k_edge_expand(DevScene s, uint64_t seed, BackwardWorkspace ws) {
+    long long n = min(min((long long)ws.counters->points, ws.cap_points), ws.pt_end);
+    long long stride = (long long)gridDim.x * blockDim.x;
+    ItemWriter out(ws);
+    for (long long base = ws.pt_begin + (long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < n;
+         base += stride) {
+        long long p = base + (threadIdx.x & 31);
+        if (p < n) {
+            PointRecord pt;
+            pt.load(ws.pt + (size_t)p * DR_PT_WORDS);
+            const EdgeProposal pr = point_proposal(ws, p);
+            auto emit = [&](int tree, int ei, int j, float w, int code) { out.add((int)p, tree, ei, j, w, code); };
+            EdgeTask tb[DR_TASK_BUF];
+            int nt = 0;
+            bool ok = true;
+            auto flush = [&]() {
+                unsigned long long first = atomicAdd(&ws.counters->tasks, (unsigned long long)nt);
+                if (first + (unsigned long long)nt <= (unsigned long long)ws.cap_tasks) {
+                    for (int k = 0; k < nt; k++) ws.tasks[first + k] = tb[k];
+                } else {  // no room: walk them here
+                    for (int k = 0; k < nt; k++) ok &= traverse_point_task<PROP>(s, pt, seed, tb[k], emit, pr);
+                }
+                nt = 0;
+            };
+            auto defer = [&](int code, float bb, float c, float a, float l) {
+                if (nt == DR_TASK_BUF) flush();
+                tb[nt++] = EdgeTask{(int)p, code, bb, c, a, l};
+            };
+            ok &= traverse_point<PROP, DR_TASK_CUT>(s, pt, seed, emit, pr, &defer);
+            if (nt > 0) flush();
+            if (!ok) set_status(&ws.counters->status, DR_STATUS_STACK_OVERFLOW);
+        }
+        out.flush_warp();
+    }
+}
+
+// Large trees, second stage: one thread per handed-on subtree.
+template <bool PROP>
+__global__ void __launch_bounds__(128, 4) k_edge_tasks(DevScene s, uint64_t seed, BackwardWorkspace ws) {
+    long long n = (long long)min(ws.counters->tasks, (unsigned long long)ws.cap_tasks);
+    long long stride = (long long)gridDim.x * blockDim.x;
+    ItemWriter out(ws);
+    for (long long base = (long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < n; base += stride) {
+        long long k = base + (threadIdx.x & 31);
+        if (k < n) {
+            EdgeTask t = ws.tasks[k];
+            PointRecord pt;
+            pt.load(ws.pt + (size_t)t.point * DR_PT_WORDS);
+            auto emit = [&](int tree, int ei, int j, float w, int code) { out.add(t.point, tree, ei, j, w, code); };
+            if (!traverse_point_task<PROP>(s, pt, seed, t, emit, point_proposal(ws, t.point)))
+                set_status(&ws.counters->status, DR_STATUS_STACK_OVERFLOW);
+        }
+        if (out.nb == DR_ITEM_BUF) out.flush_warp();  // keeps lanes' buffers from carrying over long
+    }
+    out.flush_warp();
 }
 
 // What follows an item's evaluation: the proposal's training target and the
@@ -186,7 +269,20 @@ __global__ void __launch_bounds__(128, 3) k_primary_edges(DevScene s, int W, int
 
 cudaError_t dr_launch_edge_traverse(const DevScene &s, uint64_t seed, const BackwardWorkspace &ws, int num_sms,
                                     cudaStream_t st, int *launches, StageTimer *timer) {
-    if (ws.proposal_q) k_edge_traverse<true><<<stage_grid(num_sms), 128, 0, st>>>(s, seed, ws);
+    const bool prop = ws.proposal_q != nullptr;
+    if (ws.tasks && s.split_traversal) {
+        cudaError_t e = cudaMemsetAsync(&ws.counters->tasks, 0, sizeof(unsigned long long), st);
+        if (e != cudaSuccess) return e;
+        if (prop) k_edge_expand<true><<<stage_grid(num_sms), 128, 0, st>>>(s, seed, ws);
+        else k_edge_expand<false><<<stage_grid(num_sms), 128, 0, st>>>(s, seed, ws);
+        timer->mark(st, "k_edge_expand");
+        if (prop) k_edge_tasks<true><<<stage_grid(num_sms), 128, 0, st>>>(s, seed, ws);
+        else k_edge_tasks<false><<<stage_grid(num_sms), 128, 0, st>>>(s, seed, ws);
+        timer->mark(st, "k_edge_tasks");
+        *launches += 2;
+        return cudaGetLastError();
+    }
+    if (prop) k_edge_traverse<true><<<stage_grid(num_sms), 128, 0, st>>>(s, seed, ws);
     else k_edge_traverse<false><<<stage_grid(num_sms), 128, 0, st>>>(s, seed, ws);
     timer->mark(st, "k_edge_traverse");
     *launches += 1;

@@ -281,20 +281,26 @@ template <bool PROP> HD EdgeItem<PROP> edge_item(int node, float bb, float c, fl
     return it;
 }
 
-template <bool CONE, bool PROP, class Emit>
+#define DR_NODE_MASK ((1 << 27) - 1)
+
+// CUT > 0: interior nodes at depth CUT below the start are handed to
+// defer(node, bb, cpmf, apmf, lpmf) instead of being walked (inside the walk
+// an item's node field carries its depth in bits 27..31).
+template <bool CONE, bool PROP, int CUT = 0, class Emit, class Defer>
 DEV bool traverse_mode(const DevScene &s, const DevEdgeNode *nodes, const DevEdge *edges, bool dir_bounds, float3 wi,
                        const SurfacePoint &sp, float dl, float sl, float rough, int model, const ConeSpec &cone,
-                       float root_bb, float pmf, Rng &rng, Emit &emit, const EdgeProposal &pr, int tree,
-                       bool learned) {
+                       const EdgeTask &start, const NodeRng &rng, Emit &emit, const EdgeProposal &pr, int tree,
+                       bool learned, Defer &defer) {
     using Item = EdgeItem<PROP>;
     Item st[DR_EDGE_STACK];
     int sp_ = 0;
-    st[sp_++] = edge_item<PROP>(0, root_bb, pmf, pmf, pmf);
+    st[sp_++] = edge_item<PROP>(start.code & DR_NODE_MASK, start.bb, start.cpmf, start.apmf, start.lpmf);
     bool ok = true;
     while (sp_ > 0) {
         Item it = st[--sp_];
         if (it.bb <= 0.f) continue;
-        const DevEdgeNode &node = nodes[it.node];
+        const int nid = it.node & DR_NODE_MASK;
+        const DevEdgeNode &node = nodes[nid];
         if (node.nprims > 0) {
             float apmf = it.apmf;
             if constexpr (PROP) apmf = pr.alpha * it.lpmf + (1.f - pr.alpha) * it.apmf;
@@ -306,11 +312,18 @@ DEV bool traverse_mode(const DevScene &s, const DevEdgeNode *nodes, const DevEdg
                 int code = 0;
                 if constexpr (PROP)
                     if (pr.codes) code = dir_bin(sp.f, 0.5f * (edge_v0(s, edges[ei]) + edge_v1(s, edges[ei])) - sp.p);
-                emit(ei, w, code);
+                emit(ei, (CONE ? 0 : 1) << 27 | ei, w, code);
             }
             continue;
         }
-        int li = it.node + 1, ri = node.offset;
+        if (CUT > 0 && (it.node >> 27) == CUT) {  // hand the subtree on
+            float lp = 0.f;
+            if constexpr (PROP) lp = it.lpmf;
+            defer(nid, it.bb, it.cpmf, it.apmf, lp);
+            continue;
+        }
+        const int cdepth = CUT > 0 ? ((it.node >> 27) + 1) << 27 : 0;  // the children's depth bits
+        int li = nid + 1, ri = node.offset;
         const DevEdgeNode &L = nodes[li], &R = nodes[ri];
         bool all_split = it.bb > 1.f || node_inside(node, sp.p);
         bool lcs = true, rcs = true;
@@ -353,11 +366,11 @@ DEV bool traverse_mode(const DevScene &s, const DevEdgeNode *nodes, const DevEdg
                     prl = 1.f - pll;
                 }
             }
-            left = edge_item<PROP>(li, lbb, plc * it.cpmf, pla * it.apmf, pll * it.lpmf);
-            right = edge_item<PROP>(ri, rbb, prc * it.cpmf, pra * it.apmf, prl * it.lpmf);
+            left = edge_item<PROP>(li | cdepth, lbb, plc * it.cpmf, pla * it.apmf, pll * it.lpmf);
+            right = edge_item<PROP>(ri | cdepth, rbb, prc * it.cpmf, pra * it.apmf, prl * it.lpmf);
         } else {
-            left = edge_item<PROP>(li, lbb, plc * it.cpmf, pla * it.apmf, 0.f);
-            right = edge_item<PROP>(ri, rbb, prc * it.cpmf, pra * it.apmf, 0.f);
+            left = edge_item<PROP>(li | cdepth, lbb, plc * it.cpmf, pla * it.apmf, 0.f);
+            right = edge_item<PROP>(ri | cdepth, rbb, prc * it.cpmf, pra * it.apmf, 0.f);
         }
         bool split = CONE ? cone_split : all_split;
         if (split) {
@@ -369,7 +382,7 @@ DEV bool traverse_mode(const DevScene &s, const DevEdgeNode *nodes, const DevEdg
             if (rcs) st[sp_++] = right;
             if (lcs) st[sp_++] = left;
         } else {
-            float u = rng.next();
+            float u = rng.draw(CONE ? 0 : 1, nid);
             bool go_left = CONE ? u < plc : u < (learned ? pll : pla);
             if (sp_ + 1 > DR_EDGE_STACK) {
                 ok = false;
@@ -383,9 +396,17 @@ DEV bool traverse_mode(const DevScene &s, const DevEdgeNode *nodes, const DevEdg
 
 // All edges sampled for one shading point (edge_tree.cpp:654-725).
 // emit(tree, edge_index, weight); tree 0 = silhouette tree, 1 = normal tree.
-template <bool PROP, class Emit>
+// emit(tree, edge_index, key, weight, code): key = mode << 27 | edge index
+// (the traversal order of the reference: cone mode first, then depth first).
+// `rng` draws the tree pick; `nrng` the traversal's choices.
+// No subtree is handed on.
+struct NoDefer {
+    HD void operator()(int, float, float, float, float) {}
+};
+
+template <bool PROP, int CUT = 0, class Emit, class Defer>
 DEV bool traverse_edges(const DevScene &s, float3 wi, int stri, const SurfacePoint &sp, const ConeSpec &cone, Rng &rng,
-                        Emit &emit, const EdgeProposal &pr) {
+                        const NodeRng &nrng, Emit &emit, const EdgeProposal &pr, Defer &defer) {
     if (dot(wi, sp.f.n) < 0.f) return true;
     int tree;
     float pmf = 1.f;
@@ -412,13 +433,43 @@ DEV bool traverse_edges(const DevScene &s, float3 wi, int stri, const SurfacePoi
     float dl = luminance(get_kd(s, m, sp.uv)), sl = luminance(get_ks(s, m, sp.uv));
     float rough = get_rough(s, m, sp.uv);
     float b = bsdf_bound(nodes[0], wi, sp, dl, sl, rough, m.model);
-    auto em = [&](int ei, float w, int code) { emit(tree, ei, w, code); };
-    bool ok = traverse_mode<true, PROP>(s, nodes, edges, tree == 1, wi, sp, dl, sl, rough, m.model, cone, b, pmf, rng,
-                                        em, pr, tree, false);
-    bool learned = PROP ? rng.next() < pr.alpha : false;
-    ok &= traverse_mode<false, PROP>(s, nodes, edges, tree == 1, wi, sp, dl, sl, rough, m.model, cone, b, pmf, rng, em,
-                                     pr, tree, learned);
+    auto em = [&](int ei, int key, float w, int code) { emit(tree, ei, key, w, code); };
+    EdgeTask root;
+    root.point = 0;
+    root.code = 0;
+    root.bb = b;
+    root.cpmf = root.apmf = root.lpmf = pmf;
+    auto dc = [&](int node, float bb, float c, float a, float l) { defer(node | (tree << 29), bb, c, a, l); };
+    bool ok = traverse_mode<true, PROP, CUT>(s, nodes, edges, tree == 1, wi, sp, dl, sl, rough, m.model, cone, root,
+                                             nrng, em, pr, tree, false, dc);
+    bool learned = PROP ? nrng.draw(1, DR_NODE_MIX_DRAW) < pr.alpha : false;
+    auto da = [&](int node, float bb, float c, float a, float l) { defer(node | (tree << 29) | (1 << 30), bb, c, a, l); };
+    ok &= traverse_mode<false, PROP, CUT>(s, nodes, edges, tree == 1, wi, sp, dl, sl, rough, m.model, cone, root, nrng,
+                                          em, pr, tree, learned, da);
     return ok;
+}
+
+// Walks one handed-on subtree of a point's traversal (the point's setup is
+// recomputed: tree and mode come with the task).
+template <bool PROP, class Emit>
+DEV bool traverse_subtree(const DevScene &s, float3 wi, int stri, const SurfacePoint &sp, const ConeSpec &cone,
+                          const NodeRng &nrng, const EdgeTask &task, Emit &emit, const EdgeProposal &pr) {
+    const int tree = (task.code >> 29) & 1, mode = (task.code >> 30) & 1;
+    const DevEdgeNode *nodes = tree ? s.nrm_nodes : s.sil_nodes;
+    const DevEdge *edges = tree ? s.nrm_edges : s.sil_edges;
+    const DevMaterial &m = s.mats[material_of_tri(s, stri)];
+    float dl = luminance(get_kd(s, m, sp.uv)), sl = luminance(get_ks(s, m, sp.uv));
+    float rough = get_rough(s, m, sp.uv);
+    auto em = [&](int ei, int key, float w, int code) { emit(tree, ei, key, w, code); };
+    NoDefer nd;
+    EdgeTask start = task;
+    start.code = task.code & DR_NODE_MASK;  // depth bits cleared: walked to the leaves
+    if (mode == 0)
+        return traverse_mode<true, PROP>(s, nodes, edges, tree == 1, wi, sp, dl, sl, rough, m.model, cone, start,
+                                         nrng, em, pr, tree, false, nd);
+    bool learned = PROP ? nrng.draw(1, DR_NODE_MIX_DRAW) < pr.alpha : false;
+    return traverse_mode<false, PROP>(s, nodes, edges, tree == 1, wi, sp, dl, sl, rough, m.model, cone, start, nrng,
+                                      em, pr, tree, learned, nd);
 }
 
 // LTC matrix lookup (material.h:464-476): nearest entry of the 128x128 table

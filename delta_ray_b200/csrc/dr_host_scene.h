@@ -713,6 +713,7 @@ inline void fill_devscene(DevScene &ds, const HostScene &h, const FlatScene &f, 
     ds.detached_pdf = 0;
     ds.edge_lobe_mis = 0;
     ds.specular_chains = 0;
+    ds.split_traversal = 0;
     ds.grad_total = (int)h.grad_total;
 }
 

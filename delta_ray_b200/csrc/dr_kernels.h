@@ -50,6 +50,7 @@ struct BackwardCounters {
     int status;                 // DR_STATUS_* bits
     int pad;
     unsigned long long survivors;  // line samples k_edge_line kept for k_edge_shade
+    unsigned long long tasks;      // subtrees k_edge_expand handed on to k_edge_tasks
 };
 
 struct BackwardWorkspace {
@@ -76,6 +77,10 @@ struct BackwardWorkspace {
     // [cap_items][2] float4 (item index bits, sample_p; d sample_p / d l, density);
     // null: one kernel evaluates each item whole
     float4 *survivors;
+    // subtrees of large trees' traversals handed on to a second stage
+    // (null: one thread walks each point whole)
+    EdgeTask *tasks;
+    long long cap_tasks;
     const uint16_t *proposal_q;
     float proposal_alpha;
     float *train_targets;

@@ -60,6 +60,15 @@ struct DevEdgeNode {
 // a pixel sample hands at most DR_MAX_LINKS + 1 points to edge sampling.
 #define DR_MAX_LINKS 8
 
+// A subtree of a point's edge-tree traversal, to be walked on its own (the
+// node-keyed draws make its result independent of who walks it and when):
+// the point, node | tree << 29 | mode << 30, the node's bound and the three
+// path pmfs (cone, all, learned).
+struct EdgeTask {
+    int point, code;
+    float bb, cpmf, apmf, lpmf;
+};
+
 struct DevScene {
     DevCamera cam;
     // geometry
@@ -114,6 +123,9 @@ struct DevScene {
     // <= 0.01 and a specular lobe, and max_bounces >= 1), so the backward pass
     // differentiates through the vertices they reach
     int specular_chains;
+    // the edge trees are large: traversals run in two stages (k_edge_expand,
+    // then one thread per handed-on subtree)
+    int split_traversal;
 };
 
 // --- accessors -------------------------------------------------------------

@@ -346,6 +346,13 @@ inline void d_xfm_point(const M4<float> &M, const V3f &p, const V3f &d_out, floa
 // ===================================================================
 struct Sampler {
     virtual float next() = 0;
+    // the draw of an edge-tree traversal's stochastic choice at node nid in
+    // mode (0 cone, 1 all): the next draw in the reference's scheme
+    virtual float node(int mode, int nid) {
+        (void)mode;
+        (void)nid;
+        return next();
+    }
     virtual ~Sampler() {}
 };
 
@@ -378,14 +385,24 @@ inline void philox4x32_10(uint32_t c[4], uint32_t k0, uint32_t k1) {
     }
 }
 
-enum StreamKind : uint32_t { kPixel = 0, kEdgePoint = 1, kEdgeItem = 2, kPrimaryEdge = 3 };
+enum StreamKind : uint32_t { kPixel = 0, kEdgePoint = 1, kEdgeItem = 2, kPrimaryEdge = 3, kEdgeNode = 4 };
 
 struct PhiloxSampler : Sampler {
+    uint64_t seed;
     uint32_t k0, k1, id_lo, id_hi, sub, idx = 0;
     uint32_t buf[4];
-    PhiloxSampler(uint64_t seed, uint32_t kind, uint64_t id, uint32_t sub_)
-        : k0((uint32_t)seed), k1(kind ^ (uint32_t)(seed >> 32)), id_lo((uint32_t)id),
+    PhiloxSampler(uint64_t seed_, uint32_t kind, uint64_t id, uint32_t sub_)
+        : seed(seed_), k0((uint32_t)seed_), k1(kind ^ (uint32_t)(seed_ >> 32)), id_lo((uint32_t)id),
           id_hi((uint32_t)(id >> 32)), sub(sub_) {}
+    // The product's traversal draws are keyed by node, not by stream position
+    // (project convention, so that a traversal's result does not depend on
+    // the order of its visits): stream kEdgeNode of the same sample id,
+    // sub = bounce << 28 | mode << 27 | node (this sampler's sub is the bounce).
+    float node(int mode, int nid) override {
+        PhiloxSampler d(seed, kEdgeNode, ((uint64_t)id_hi << 32) | id_lo,
+                        (sub << 28) | ((uint32_t)mode << 27) | (uint32_t)nid);
+        return d.next();
+    }
     float next() override {
         uint32_t lane = idx & 3u;
         if (lane == 0) {
@@ -1512,7 +1529,10 @@ inline bool box_cone(const AABB &b, const Cone &cone) {
     return false;
 }
 
-struct EdgeW { Edge e; float w; };
+// A sampled edge with its weight and its key in the traversal order:
+// mode << 27 | index of the edge in its tree (cone-mode edges first, then in
+// depth-first order, which is the order of the tree's edge array).
+struct EdgeW { Edge e; float w; int key; };
 
 // bsdf_bound (edge_tree.cpp:345-480)
 inline float min_sq(float lo, float hi) {
@@ -1598,7 +1618,7 @@ void sample_edge(int nid, float nbb, const Scene &sc, const EdgeTree &t, const V
         float w = CONE ? cpmf / (cpmf * cpmf + apmf * apmf) : apmf / (cpmf * cpmf + apmf * apmf);
         for (int i = 0; i < node.nprims; i++) {
             const Edge &e = t.edges[node.offset + i];
-            if (is_silhouette(sc, sp.p, e)) out.push_back(EdgeW{e, w});
+            if (is_silhouette(sc, sp.p, e)) out.push_back(EdgeW{e, w, ((CONE ? 0 : 1) << 27) | (node.offset + i)});
         }
         return;
     }
@@ -1628,7 +1648,7 @@ void sample_edge(int nid, float nbb, const Scene &sc, const EdgeTree &t, const V
         if (lcs) sample_edge<DIR, CONE>(nid + 1, lbb, sc, t, wi, is, sp, dl, sl, cone, out, plc * cpmf, pla * apmf, rng);
         if (rcs) sample_edge<DIR, CONE>(node.offset, rbb, sc, t, wi, is, sp, dl, sl, cone, out, prc * cpmf, pra * apmf, rng);
     } else {
-        float u = rng.next();
+        float u = rng.node(CONE ? 0 : 1, nid);
         bool left = CONE ? u < plc : u < pla;
         if (left) sample_edge<DIR, CONE>(nid + 1, lbb, sc, t, wi, is, sp, dl, sl, cone, out, plc * cpmf, pla * apmf, rng);
         else sample_edge<DIR, CONE>(node.offset, rbb, sc, t, wi, is, sp, dl, sl, cone, out, prc * cpmf, pra * apmf, rng);
@@ -2260,7 +2280,8 @@ V3f render_pixel_sample(const Scene &sc, const GradLayout &L, int W, int H, int 
             std::unique_ptr<PhiloxSampler> estream;
             Sampler *erng = &rng;
             if (sp_plan.mode == 1) {
-                estream.reset(new PhiloxSampler(sp_plan.seed, kEdgeItem, sp_plan.sample_id, ((uint32_t)k << 16) | (uint32_t)j));
+                estream.reset(new PhiloxSampler(sp_plan.seed, kEdgeItem, sp_plan.sample_id,
+                                                ((uint32_t)k << 28) | (uint32_t)ew.key));
                 erng = estream.get();
             }
             LightSample els = draw_light(*erng);

@@ -39,6 +39,7 @@ def load():
         L.hh_trace.argtypes = [C.POINTER(_abi.dr_scene_desc), C.c_void_p, C.c_int, C.c_void_p, C.c_void_p]
         L.hh_trace.restype = C.c_longlong
         L.hh_set_proposal.argtypes = [C.c_int, C.c_float]
+        L.hh_set_split.argtypes = [C.c_int]
         _lib = L
     return _lib
 
@@ -75,3 +76,8 @@ def trace(wl, rays):
 def set_proposal(seed, alpha):
     """Synthetic learned proposal of later renders (seed 0: none)."""
     load().hh_set_proposal(int(seed), float(alpha))
+
+
+def set_split(on):
+    """Walk large traversals in two stages (subtrees handed on at depth 4)."""
+    load().hh_set_split(int(bool(on)))

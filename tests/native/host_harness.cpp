@@ -15,6 +15,10 @@ thread_local long long g_dr_visits = 0;
 // sample id and bounce.
 static int g_prop_seed = 0;
 static float g_prop_alpha = 0.f;
+// hh_set_split(1): walk each point's trees to depth 4, hand the subtrees
+// there on as tasks and walk those after all points (the GPU's two-stage
+// traversal of large trees)
+static int g_split = 0;
 
 #include "../../delta_ray_b200/csrc/dr_backward.cuh"
 #include "../../delta_ray_b200/csrc/dr_bvh.cuh"
@@ -204,8 +208,22 @@ int hh_render(const dr_scene_desc *desc, const dr_render_desc *rd, const float *
                 }
                 pr.q = q.data();
             }
-            if (pr.q) traverse_point<true>(s, pts[p], seed, emit, pr);
-            else traverse_point<false>(s, pts[p], seed, emit, pr);
+            if (g_split) {
+                std::vector<EdgeTask> tasks;
+                auto defer = [&](int code, float bb, float c, float a, float l) {
+                    tasks.push_back(EdgeTask{p, code, bb, c, a, l});
+                };
+                if (pr.q) traverse_point<true, 4>(s, pts[p], seed, emit, pr, &defer);
+                else traverse_point<false, 4>(s, pts[p], seed, emit, pr, &defer);
+                for (const EdgeTask &t : tasks) {
+                    if (pr.q) traverse_point_task<true>(s, pts[p], seed, t, emit, pr);
+                    else traverse_point_task<false>(s, pts[p], seed, t, emit, pr);
+                }
+            } else if (pr.q) {
+                traverse_point<true>(s, pts[p], seed, emit, pr);
+            } else {
+                traverse_point<false>(s, pts[p], seed, emit, pr);
+            }
         }
         nitems = (long long)items.size();
         std::vector<int> last(pts.size(), -1);
@@ -236,6 +254,8 @@ int hh_render(const dr_scene_desc *desc, const dr_render_desc *rd, const float *
     }
     return 0;
 }
+
+void hh_set_split(int on) { g_split = on; }
 
 // The synthetic proposal of later hh_render calls (seed 0: none).
 void hh_set_proposal(int seed, float alpha) {

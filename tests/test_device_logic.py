@@ -173,3 +173,24 @@ def test_learned_proposal_traversal_is_unbiased():
     z = (ml - mp)[m] / se[m]
     assert m.sum() > 30
     assert np.sqrt((z ** 2).mean()) < 1.4 and (np.abs(z) < 3).mean() >= 0.95, z
+
+
+@pytest.mark.parametrize("proposal", [False, True])
+def test_two_stage_traversal_samples_the_same_edges(proposal):
+    """Subtrees handed on at depth 4 and walked separately (the GPU's traversal
+    of large trees) sample exactly the edges of the one-pass walk: the
+    traversal's draws are keyed by node, its items by mode and edge index."""
+    import scenes
+    wl = scenes.SCENES["heightfield_small"](seed=8, resolution=(24, 20), spp=2, max_bounces=2)
+    W, H = wl.resolution
+    d = np.random.default_rng(4).uniform(0.5, 1.5, (H, W, 3)).astype(np.float32)
+    harness.set_proposal(7 if proposal else 0, 0.6)
+    try:
+        one = harness.render(wl, 12, d, parts=2)
+        harness.set_split(True)
+        two = harness.render(wl, 12, d, parts=2)
+    finally:
+        harness.set_split(False)
+        harness.set_proposal(0, 0.0)
+    assert one["stats"][1] == two["stats"][1] and one["stats"][1] > 0
+    assert rel_err(two["grad"], one["grad"]) < 1e-6
