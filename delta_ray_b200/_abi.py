@@ -71,6 +71,26 @@ DR_FLAG_EDGE_LOBE_MIS = 4
 DR_FLAG_LEARNED_PROPOSAL = 8
 
 
+def camera_desc(cam, keep):
+    """dr_camera_desc of a camera dict (scene_dicts' layout); the float32
+    host copies of the matrices are appended to `keep`."""
+    cd = dr_camera_desc()
+    for name in ("cam_to_world", "world_to_cam", "sample_to_cam", "cam_to_sample"):
+        t = torch.as_tensor(cam[name], dtype=torch.float32).detach().cpu().contiguous()
+        keep.append(t)
+        setattr(cd, name, C.cast(t.data_ptr(), c_float_p))
+    cd.fov_factor = float(cam["fov_factor"])
+    cd.aspect_ratio = float(cam["aspect_ratio"])
+    cd.clip_near = float(cam["clip_near"])
+    cd.fisheye = int(bool(cam["fisheye"]))
+    return cd
+
+
+class dr_view_desc(C.Structure):
+    _fields_ = [("camera", dr_camera_desc), ("render", dr_render_desc), ("d_image", C.c_void_p),
+                ("image", C.c_void_p)]
+
+
 class dr_proposal_desc(C.Structure):
     _fields_ = [("train", C.c_int), ("mix", C.c_float), ("learning_rate", C.c_float), ("train_points", C.c_int64),
                 ("params", C.c_void_p)]

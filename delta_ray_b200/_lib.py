@@ -46,6 +46,8 @@ def lib():
     L.dr_last_error.argtypes = [C.c_char_p, C.c_size_t]
     L.dr_mlp_param_count.restype = C.c_int
     L.dr_scene_set_proposal.argtypes = [C.c_void_p, C.POINTER(_abi.dr_proposal_desc)]
+    L.dr_render_backward_views.argtypes = [C.c_void_p, C.c_int, C.POINTER(_abi.dr_view_desc), C.c_void_p, C.c_void_p,
+                                           C.c_void_p]
     L.dr_scene_proposal_state.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(C.c_float), C.POINTER(C.c_int64)]
     L.dr_mlp_forward.argtypes = [C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p]
     L.dr_mlp_gradient.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p]

@@ -171,6 +171,7 @@ struct dr_scene {
     std::shared_ptr<DevBuf> ltc, ltc_ggx;
     std::unique_ptr<BackwardQueues> queues;  // taken at the first backward call
     std::unique_ptr<ProposalState> proposal;  // set by dr_scene_set_proposal
+    DevBuf view_grad, view_prim_edges, view_prim_cdf, view_prim_func;  // dr_render_backward_views
     float3 lo, hi;                            // scene bounds
     DevScene ds;
     StageTimer timer;
@@ -374,8 +375,8 @@ template <class Grow, class GrowPoints>
 std::pair<long long, long long> run_backward(dr_scene *scene, const dr_render_desc *rd, const float *d_image_dev,
                                              float *grad_dev, float *image_dev, BackwardWorkspace &ws,
                                              cudaStream_t st, StageTimer *timer, Grow grow, GrowPoints grow_points,
-                                             ProposalState *prop = nullptr) {
-    const DevScene ds = call_scene(scene, rd);
+                                             ProposalState *prop = nullptr, const DevScene *view = nullptr) {
+    const DevScene ds = view ? *view : call_scene(scene, rd);
     const GradCacheCfg cfg = grad_cache_cfg(scene->h);
     BackwardCounters c;
     auto read = [&]() {
@@ -612,6 +613,83 @@ dr_status dr_render_forward(dr_scene *scene, const dr_render_desc *rd, float *im
     });
 }
 
+namespace {
+// The backward pass of dr_render_backward on the library's cached queues;
+// `view` (may be null) replaces the scene's device view (another camera).
+void backward_on_queues(dr_scene *scene, const dr_render_desc *rd, const DevScene *view, const float *d_image_dev,
+                        float *grad_dev, float *image_dev, cudaStream_t st) {
+    if (!scene->queues) scene->queues = take_queues(scene->device, st);
+    BackwardQueues &q = *scene->queues;
+    long long cap_points = initial_point_cap(scene, rd, q.points_per_sample);
+    long long cap_items = std::min(kMaxQueueItems, std::max(q.cap_items, std::max<long long>(cap_points * 4, 1 << 16)));
+    q.counts.reserve(sizeof(BackwardCounters));
+    if (!q.idle) check_cuda(cudaEventCreateWithFlags(&q.idle, cudaEventDisableTiming), "cudaEventCreate");
+    // marks the queues busy up to here on every way out, errors included
+    struct MarkIdle {
+        cudaEvent_t e;
+        cudaStream_t st;
+        ~MarkIdle() { cudaEventRecord(e, st); }
+    } mark_idle{q.idle, st};
+    BackwardWorkspace ws{};
+    auto bind_items = [&]() {
+        q.items.reserve(sizeof(int4) * cap_items);
+        q.item_w.reserve(sizeof(float) * cap_items);
+        q.item_dp.reserve(sizeof(float) * 3 * cap_items);
+        q.survivors.reserve(sizeof(float4) * 2 * cap_items);
+        q.cap_items = cap_items;
+        ws.items = q.items.as<int4>();
+        ws.item_w = q.item_w.as<float>();
+        ws.item_dp = q.item_dp.as<float>();
+        ws.survivors = q.survivors.as<float4>();
+        ws.cap_items = cap_items;
+    };
+    auto bind_points = [&]() {
+        q.pt.reserve(sizeof(float) * DR_PT_FLOATS * cap_points);
+        q.pt_last.reserve(DR_PT_LAST_BYTES * cap_points);
+        ws.pt = q.pt.as<float>();
+        ws.pt_last = q.pt_last.as<unsigned long long>();
+        ws.cap_points = cap_points;
+    };
+    bind_points();
+    ws.counters = q.counts.as<BackwardCounters>();
+    bind_items();
+    if (view ? view->split_traversal : call_scene(scene, rd).split_traversal) {
+        long long cap_tasks = std::min(kMaxTasks, std::max(1ll << 16, kTasksPerPoint * cap_points));
+        q.tasks.reserve(sizeof(EdgeTask) * cap_tasks);
+        ws.tasks = q.tasks.as<EdgeTask>();
+        ws.cap_tasks = cap_tasks;
+    }
+    // the item queue grows to what the traversal reported, up to its limit
+    // (the grown queue is kept for later calls)
+    auto grow = [&](long long want) {
+        long long target = std::min(want, kMaxQueueItems);
+        if (target > cap_items) {
+            cap_items = target;
+            bind_items();
+        }
+        return cap_items;
+    };
+    // the point queue grows to what the path stage reported (the ratio is
+    // kept for later calls)
+    auto grow_points = [&](long long want) {
+        cap_points = want + want / 16 + 1;
+        q.points_per_sample = (double)cap_points / ((double)rd->width * rd->height * rd->spp);
+        bind_points();
+        return cap_points;
+    };
+    ProposalState *prop = nullptr;
+    if (rd->flags & DR_FLAG_LEARNED_PROPOSAL) {
+        if (!scene->proposal)
+            throw DrError(DR_ERR_INVALID_ARGUMENT, "DR_FLAG_LEARNED_PROPOSAL without dr_scene_set_proposal");
+        prop = scene->proposal.get();
+    }
+    auto counts = run_backward(scene, rd, d_image_dev, grad_dev, image_dev, ws, st, &scene->timer, grow, grow_points,
+                               prop, view);
+    scene->last_points = counts.first;
+    scene->last_items = counts.second;
+}
+}  // namespace
+
 dr_status dr_render_backward(dr_scene *scene, const dr_render_desc *rd, const float *d_image_dev, float *grad_dev,
                              float *image_dev, void *stream) {
     return guard([&]() {
@@ -619,75 +697,69 @@ dr_status dr_render_backward(dr_scene *scene, const dr_render_desc *rd, const fl
         check_cuda(cudaSetDevice(scene->device), "cudaSetDevice");
         cudaStream_t st = (cudaStream_t)stream;
         scene->last_launches = 0;
-        if (!scene->queues) scene->queues = take_queues(scene->device, st);
-        BackwardQueues &q = *scene->queues;
-        long long cap_points = initial_point_cap(scene, rd, q.points_per_sample);
-        long long cap_items = std::min(kMaxQueueItems, std::max(q.cap_items, std::max<long long>(cap_points * 4, 1 << 16)));
-        q.counts.reserve(sizeof(BackwardCounters));
-        if (!q.idle) check_cuda(cudaEventCreateWithFlags(&q.idle, cudaEventDisableTiming), "cudaEventCreate");
-        // marks the queues busy up to here on every way out, errors included
-        struct MarkIdle {
-            cudaEvent_t e;
-            cudaStream_t st;
-            ~MarkIdle() { cudaEventRecord(e, st); }
-        } mark_idle{q.idle, st};
-        BackwardWorkspace ws{};
-        auto bind_items = [&]() {
-            q.items.reserve(sizeof(int4) * cap_items);
-            q.item_w.reserve(sizeof(float) * cap_items);
-            q.item_dp.reserve(sizeof(float) * 3 * cap_items);
-            q.survivors.reserve(sizeof(float4) * 2 * cap_items);
-            q.cap_items = cap_items;
-            ws.items = q.items.as<int4>();
-            ws.item_w = q.item_w.as<float>();
-            ws.item_dp = q.item_dp.as<float>();
-            ws.survivors = q.survivors.as<float4>();
-            ws.cap_items = cap_items;
-        };
-        auto bind_points = [&]() {
-            q.pt.reserve(sizeof(float) * DR_PT_FLOATS * cap_points);
-            q.pt_last.reserve(DR_PT_LAST_BYTES * cap_points);
-            ws.pt = q.pt.as<float>();
-            ws.pt_last = q.pt_last.as<unsigned long long>();
-            ws.cap_points = cap_points;
-        };
-        bind_points();
-        ws.counters = q.counts.as<BackwardCounters>();
-        bind_items();
-        if (call_scene(scene, rd).split_traversal) {
-            long long cap_tasks = std::min(kMaxTasks, std::max(1ll << 16, kTasksPerPoint * cap_points));
-            q.tasks.reserve(sizeof(EdgeTask) * cap_tasks);
-            ws.tasks = q.tasks.as<EdgeTask>();
-            ws.cap_tasks = cap_tasks;
+        backward_on_queues(scene, rd, nullptr, d_image_dev, grad_dev, image_dev, st);
+        collect_timings(scene, st);
+    });
+}
+
+dr_status dr_render_backward_views(dr_scene *scene, int n_views, const dr_view_desc *views, float *grad_dev,
+                                   float *camera_grads_dev, void *stream) {
+    return guard([&]() {
+        if (!scene || n_views < 0 || (n_views > 0 && !views) || !grad_dev)
+            throw DrError(DR_ERR_INVALID_ARGUMENT, "invalid view batch");
+        check_cuda(cudaSetDevice(scene->device), "cudaSetDevice");
+        cudaStream_t st = (cudaStream_t)stream;
+        scene->last_launches = 0;
+        const long long total = scene->h.grad_total;
+        check_cuda(cudaMemsetAsync(grad_dev, 0, sizeof(float) * total, st), "memset");
+        scene->view_grad.reserve(sizeof(float) * total);
+        float *vg = scene->view_grad.as<float>();
+        long long points = 0, items = 0;
+        for (int v = 0; v < n_views; v++) {
+            const dr_view_desc &vw = views[v];
+            check_backward_args(scene, &vw.render, vw.d_image, vg);
+            HCam hc;
+            auto m16 = [&](const float *p, float *dst, const char *what) {
+                std::vector<float> m = fetch(p, 16, what);
+                std::memcpy(dst, m.data(), 64);
+            };
+            m16(vw.camera.cam_to_world, hc.c2w, "view cam_to_world");
+            m16(vw.camera.world_to_cam, hc.w2c, "view world_to_cam");
+            hc.fov = vw.camera.fov_factor;
+            hc.aspect = vw.camera.aspect_ratio;
+            hc.clip_near = vw.camera.clip_near;
+            hc.fisheye = vw.camera.fisheye != 0;
+            // the view's primary-edge sampler (the previous view's kernels have finished)
+            std::vector<DevEdge> pe;
+            HDist pd;
+            scene->h.primary_for(hc, pe, pd);
+            scene->view_prim_edges.upload(pe);
+            scene->view_prim_cdf.upload(pd.cdf);
+            scene->view_prim_func.upload(pd.func);
+            DevScene ds = call_scene(scene, &vw.render);
+            std::memcpy(ds.cam.c2w.m, hc.c2w, 64);
+            std::memcpy(ds.cam.w2c.m, hc.w2c, 64);
+            ds.cam.fov = hc.fov;
+            ds.cam.aspect = hc.aspect;
+            ds.cam.clip_near = hc.clip_near;
+            ds.cam.fisheye = hc.fisheye;
+            ds.prim_edges = scene->view_prim_edges.as<DevEdge>();
+            ds.num_prim_edges = (int)pe.size();
+            ds.prim_cdf = scene->view_prim_cdf.as<float>();
+            ds.prim_func = scene->view_prim_func.as<float>();
+            ds.prim_func_int = pd.func_int;
+            backward_on_queues(scene, &vw.render, &ds, vw.d_image, vg, vw.image, st);
+            points += scene->last_points;
+            items += scene->last_items;
+            check_cuda(dr_launch_accumulate(grad_dev + 64, vg + 64, total - 64, st), "gradient sum");
+            if (camera_grads_dev)
+                check_cuda(cudaMemcpyAsync(camera_grads_dev + 64 * (size_t)v, vg, 64 * sizeof(float),
+                                           cudaMemcpyDeviceToDevice, st),
+                           "camera gradient");
+            check_cuda(cudaStreamSynchronize(st), "view");
         }
-        // the item queue grows to what the traversal reported, up to its limit
-        // (the grown queue is kept for later calls)
-        auto grow = [&](long long want) {
-            long long target = std::min(want, kMaxQueueItems);
-            if (target > cap_items) {
-                cap_items = target;
-                bind_items();
-            }
-            return cap_items;
-        };
-        // the point queue grows to what the path stage reported (the ratio is
-        // kept for later calls)
-        auto grow_points = [&](long long want) {
-            cap_points = want + want / 16 + 1;
-            q.points_per_sample = (double)cap_points / ((double)rd->width * rd->height * rd->spp);
-            bind_points();
-            return cap_points;
-        };
-        ProposalState *prop = nullptr;
-        if (rd->flags & DR_FLAG_LEARNED_PROPOSAL) {
-            if (!scene->proposal)
-                throw DrError(DR_ERR_INVALID_ARGUMENT, "DR_FLAG_LEARNED_PROPOSAL without dr_scene_set_proposal");
-            prop = scene->proposal.get();
-        }
-        auto counts = run_backward(scene, rd, d_image_dev, grad_dev, image_dev, ws, st, &scene->timer, grow,
-                                   grow_points, prop);
-        scene->last_points = counts.first;
-        scene->last_items = counts.second;
+        scene->last_points = points;
+        scene->last_items = items;
         collect_timings(scene, st);
     });
 }

@@ -255,6 +255,7 @@ struct HostScene {
     HDist light_sel;
     float total_light_intensity = 0.f;
     std::vector<DevEdge> prim_edges;
+    std::vector<DevEdge> kept_edges;  // edges after dropping degenerate and flat ones
     HDist prim_dist;
     std::vector<DevEdgeNode> sil_nodes, nrm_nodes;
     std::vector<DevEdge> sil_edges, nrm_edges;
@@ -356,6 +357,30 @@ struct HostScene {
         flatten(nodes, ordered, root.get(), &off);
     }
 
+    // The primary-edge sampler of camera c (edge_tree.cpp:263-294): the kept
+    // edges that are silhouettes from the camera, by clipped screen length.
+    void primary_for(const HCam &c, std::vector<DevEdge> &pe, HDist &pd) const {
+        pe.clear();
+        std::vector<float> lens;
+        V3 org = xfm_point(c.c2w, v3(0.f, 0.f, 0.f));
+        for (const DevEdge &e : kept_edges) {
+            V2 a, b;
+            float dist = 0.f;
+            if (project(c, ev0(e), ev1(e), &a, &b)) {
+                V2 ca, cb;
+                if (clip_line(a, b, &ca, &cb))
+                    dist = std::sqrt((cb.x - ca.x) * (cb.x - ca.x) + (cb.y - ca.y) * (cb.y - ca.y));
+            }
+            if (!is_silhouette(org, e)) dist = 0.f;
+            if (dist > 0.f) {
+                pe.push_back(e);
+                lens.push_back(dist);
+            }
+        }
+        pd = HDist();
+        if (!lens.empty()) pd.build(lens);
+    }
+
     void preprocess() {
         // lights (scene.cpp:26-52)
         std::vector<float> imp;
@@ -427,26 +452,8 @@ struct HostScene {
             }
             edges.push_back(e);
         }
-        // primary edges (edge_tree.cpp:263-294)
-        prim_edges.clear();
-        std::vector<float> lens;
-        V3 org = xfm_point(cam.c2w, v3(0.f, 0.f, 0.f));
-        for (const DevEdge &e : edges) {
-            V2 a, b;
-            float dist = 0.f;
-            if (project(cam, ev0(e), ev1(e), &a, &b)) {
-                V2 ca, cb;
-                if (clip_line(a, b, &ca, &cb))
-                    dist = std::sqrt((cb.x - ca.x) * (cb.x - ca.x) + (cb.y - ca.y) * (cb.y - ca.y));
-            }
-            if (!is_silhouette(org, e)) dist = 0.f;
-            if (dist > 0.f) {
-                prim_edges.push_back(e);
-                lens.push_back(dist);
-            }
-        }
-        prim_dist = HDist();
-        if (!lens.empty()) prim_dist.build(lens);
+        kept_edges = edges;
+        primary_for(cam, prim_edges, prim_dist);
         std::vector<DevEdge> sil, nrm;
         for (const DevEdge &e : edges) {
             if (e.f0 == -1 || e.f1 == -1 || shapes[e.shape].n.empty()) sil.push_back(e);

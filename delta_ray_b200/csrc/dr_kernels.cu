@@ -220,3 +220,15 @@ cudaError_t dr_launch_forward(const DevScene &s, int W, int H, int spp, int B, u
     *launches += 1;
     return cudaGetLastError();
 }
+
+__global__ void k_accumulate(float *dst, const float *src, long long n) {
+    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
+        dst[i] += src[i];
+}
+
+cudaError_t dr_launch_accumulate(float *dst, const float *src, long long n, cudaStream_t st) {
+    if (n <= 0) return cudaSuccess;
+    long long blocks = (n + 255) / 256;
+    k_accumulate<<<(int)(blocks < 4096 ? blocks : 4096), 256, 0, st>>>(dst, src, n);
+    return cudaGetLastError();
+}

@@ -110,6 +110,8 @@ cudaError_t dr_launch_proposal_features(const DevScene &s, const BackwardWorkspa
                                         float3 ih, void *x, void *xt, cudaStream_t st);
 cudaError_t dr_launch_edge_traverse(const DevScene &s, uint64_t seed, const BackwardWorkspace &ws, int num_sms,
                                     cudaStream_t st, int *launches, StageTimer *timer);
+// dst[0..n) += src[0..n)
+cudaError_t dr_launch_accumulate(float *dst, const float *src, long long n, cudaStream_t st);
 // Launchers of the edge half (dr_edge_kernels.cu).  Edge evaluation: the
 // two-kernel wavefront when ws.survivors is bound, one kernel otherwise.
 cudaError_t dr_launch_edge_eval(const DevScene &s, int W, int H, int spp, int B, uint64_t seed, int dp_mode,

@@ -141,6 +141,35 @@ class Scene:
                 C.c_void_p(img.data_ptr()) if img is not None else None, self._stream()))
         return grad, img
 
+    def backward_views(self, views, opts=None):
+        """Backward render of several views in one call.  views: a list of
+        dicts with keys camera (a Camera or a scene_dicts camera dict),
+        width, height, spp, max_bounces, seed, d_image ([H, W, 3]).  Returns
+        (flat gradient summed over the views, with a zero camera block;
+        camera gradients [n_views, 64], one block per view)."""
+        opts = opts or RenderOptions()
+        keep, descs = [], (_abi.dr_view_desc * max(1, len(views)))()
+        for k, v in enumerate(views):
+            cam = v["camera"]
+            if not isinstance(cam, dict):
+                cam = _abi.scene_dicts(cam, [], [], [])[0]
+            d = torch.as_tensor(v["d_image"]).detach().to(device=self.device, dtype=torch.float32).contiguous()
+            if tuple(d.shape) != (v["height"], v["width"], 3):
+                raise ValueError(f"view {k}: d_image must be [{v['height']}, {v['width']}, 3]")
+            keep.append(d)
+            descs[k].camera = _abi.camera_desc(cam, keep)
+            descs[k].render = _abi.render_desc(v["width"], v["height"], v["spp"], v["max_bounces"], v["seed"],
+                                               opts.primary_edge_samples, opts.dp_mode, opts.flags)
+            descs[k].d_image = d.data_ptr()
+            descs[k].image = None
+        grad = torch.empty(self.grad_total, dtype=torch.float32, device=self.device)
+        cam_grads = torch.empty((max(1, len(views)), 64), dtype=torch.float32, device=self.device)
+        with torch.cuda.device(self.device_index):
+            _lib.check(_lib.lib().dr_render_backward_views(self.handle, len(views), descs,
+                                                           C.c_void_p(grad.data_ptr()),
+                                                           C.c_void_p(cam_grads.data_ptr()), self._stream()))
+        return grad, cam_grads[:len(views)]
+
     def trace(self, rays):
         """Closest hit (global triangle id, t) of rays [n, 6] on the device."""
         rays = rays.detach().to(device=self.device, dtype=torch.float32).contiguous().reshape(-1, 6)

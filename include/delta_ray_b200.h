@@ -223,6 +223,29 @@ DR_API dr_status dr_render_forward(dr_scene *scene, const dr_render_desc *rd, fl
 DR_API dr_status dr_render_backward(dr_scene *scene, const dr_render_desc *rd, const float *d_image_dev,
                              float *grad_dev, float *image_dev, void *stream);
 
+/* One view of a multi-view backward render: a camera (the layout of
+ * dr_scene_desc.camera), its render settings and its image adjoint
+ * (d_image [render.height][render.width][3], device); image (device, may be
+ * NULL) receives the view's re-rendered image. */
+typedef struct {
+    dr_camera_desc camera;
+    dr_render_desc render;
+    const float *d_image;
+    float *image;
+} dr_view_desc;
+
+/* Backward render of several views of the scene in one call (no counterpart
+ * in the reference, which renders one camera per call): each view is rendered
+ * with its own camera, resolution, samples, bounces and seed on the
+ * library's queues, and its primary edges are sampled from its own camera.
+ * grad_dev (flat layout) receives the sum over the views of every
+ * non-camera gradient, with its camera block zero; camera_grads_dev
+ * ([n_views][64] floats, device, may be NULL) receives each view's camera
+ * gradient (cam_to_world, world_to_cam, sample_to_cam, cam_to_sample).
+ * Returns after the stream has finished. */
+DR_API dr_status dr_render_backward_views(dr_scene *scene, int n_views, const dr_view_desc *views, float *grad_dev,
+                                          float *camera_grads_dev, void *stream);
+
 /* Backward render that allocates no device memory.  No counterpart in the
  * reference (whose backward allocates per call, delta_ray.cpp:1468-1550): it
  * serves callers that must not allocate during a render, e.g. a process whose

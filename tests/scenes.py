@@ -172,7 +172,38 @@ def ggx_textured(seed=0, resolution=(40, 40), spp=2, max_bounces=2):
     return wl
 
 
+def icosphere_room(seed=0, resolution=(48, 40), spp=2, max_bounces=2, n_spheres=12, subdiv=(1, 2)):
+    """A closed box room (12 triangles, 10 units a side, facing inwards) with
+    a ceiling light and seeded icospheres (subdivision levels in `subdiv`,
+    radii U(0.3, 1.2), shading normals): a reduced stand-in for the batched
+    multi-view configuration (200 spheres of levels 3-5, about 1M triangles)."""
+    rng = np.random.default_rng(seed)
+    res = [int(resolution[0]), int(resolution[1])]
+    cam = workloads._camera([0, 5, -4.5], [0, 3, 0], [0, 1, 0], 60.0, res)
+    mats = [Material(diffuse_reflectance=_t([0.6, 0.6, 0.55])), Material(diffuse_reflectance=_t([0.0, 0.0, 0.0]))]
+    shapes = []
+    h = 5.0
+    walls = [([0, 0, 0], [1, 0, 0], [0, 0, 1], [0, 1, 0]), ([0, 2 * h, 0], [1, 0, 0], [0, 0, 1], [0, -1, 0]),
+             ([-h, h, 0], [0, 0, 1], [0, 1, 0], [1, 0, 0]), ([h, h, 0], [0, 0, 1], [0, 1, 0], [-1, 0, 0]),
+             ([0, h, -h], [1, 0, 0], [0, 1, 0], [0, 0, 1]), ([0, h, h], [1, 0, 0], [0, 1, 0], [0, 0, -1])]
+    for c, ax, ay, nrm in walls:
+        v, f = workloads._quad(c, h, h, ax, ay, normal=nrm)
+        shapes.append(Shape(_t(v), _t(f, np.int32), None, None, 0))
+    lv, lf = workloads._quad([0, 2 * h - 0.01, 0], 1.5, 1.5, [1, 0, 0], [0, 0, 1], normal=[0, -1, 0])
+    shapes.append(Shape(_t(lv), _t(lf, np.int32), None, None, 1))
+    lights = [Light(len(shapes) - 1, _t([12.0, 12.0, 12.0]))]
+    for k in range(n_spheres):
+        mats.append(Material(diffuse_reflectance=_t(rng.uniform(0.2, 0.9, 3)),
+                             specular_reflectance=_t(rng.uniform(0.0, 0.4, 3)), roughness=_t([rng.uniform(0.1, 0.5)])))
+        v, f = _icosphere(int(rng.integers(subdiv[0], subdiv[1] + 1)))
+        r = rng.uniform(0.3, 1.2)
+        c = np.array([rng.uniform(-3.5, 3.5), rng.uniform(r, 4.0), rng.uniform(-3.5, 3.5)], np.float32)
+        shapes.append(Shape(_t((v * r + c).astype(np.float32)), _t(f, np.int32), None, _t(v), len(mats) - 1))
+    return workloads.Workload("icosphere_room", cam, mats, shapes, lights, res, int(spp), int(max_bounces),
+                              {"seed": seed})
+
+
 SCENES = {"glossy_shadow": glossy_shadow, "textured": textured, "smooth_sphere": smooth_sphere,
           "fisheye": fisheye, "heightfield_small": heightfield_small, "mirror_shadow": mirror_shadow,
-          "mirror_hall": mirror_hall, "ggx_shadow": ggx_shadow,
+          "mirror_hall": mirror_hall, "icosphere_room": icosphere_room, "ggx_shadow": ggx_shadow,
           "ggx_textured": ggx_textured}

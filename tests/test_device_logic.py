@@ -194,3 +194,18 @@ def test_two_stage_traversal_samples_the_same_edges(proposal):
         harness.set_proposal(0, 0.0)
     assert one["stats"][1] == two["stats"][1] and one["stats"][1] > 0
     assert rel_err(two["grad"], one["grad"]) < 1e-6
+
+
+def test_icosphere_room_kernel_logic_matches_oracle():
+    """The multi-view stand-in scene (closed room, icospheres with shading
+    normals, glossy lobes, two bounces): every gradient part to float round-off."""
+    import scenes
+    wl = scenes.icosphere_room(seed=3, n_spheres=8, subdiv=(1, 2), resolution=(32, 24), spp=2, max_bounces=2)
+    W, H = wl.resolution
+    d = np.random.default_rng(1).uniform(0.5, 1.5, (H, W, 3)).astype(np.float32)
+    for parts in (1, 2, 4):
+        h = harness.render(wl, 6, d, parts=parts)
+        o = oracle.oracle_render(wl, 6, d, rng_mode=oracle.PHILOX, parts=parts)
+        if parts == 2:
+            assert h["stats"][1] == o["stats"][1]
+        assert rel_err(h["grad"], o["grad"]) < TOL, parts
