@@ -27,7 +27,8 @@ __global__ void __launch_bounds__(128, 3) k_backward_paths(DevScene s, int W, in
                                                         int lanes_log2, const float *d_image, float *grad, float *img,
                                                         BackwardWorkspace ws, GradCacheCfg cfg) {
     extern __shared__ float sm[];
-    BlockGrad bg = block_grad_begin(sm, grad, cfg);
+    BlockGradWarp bg;
+    static_cast<BlockGrad &>(bg) = block_grad_begin(sm, grad, cfg);
     long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     int G = 1 << lanes_log2;
     long long pix = gid >> lanes_log2;
@@ -85,7 +86,8 @@ template <bool kChains>
 __global__ void __launch_bounds__(128) k_dp_propagate(DevScene s, int W, int H, int spp, uint64_t seed, int dp_mode,
                                                       float *grad, BackwardWorkspace ws, GradCacheCfg cfg) {
     extern __shared__ float sm[];
-    BlockGrad bg = block_grad_begin(sm, grad, cfg);
+    BlockGradWarp bg;
+    static_cast<BlockGrad &>(bg) = block_grad_begin(sm, grad, cfg);
     long long n = min(min((long long)ws.counters->points, ws.cap_points), ws.pt_end);
     for (long long p = ws.pt_begin + (long long)blockIdx.x * blockDim.x + threadIdx.x; p < n;
          p += (long long)gridDim.x * blockDim.x) {

@@ -23,6 +23,20 @@ struct BlockGrad {
     }
 };
 
+// The same cache, for kernels whose warps mostly add to the same entries
+// (path adjoints, primary edges, position adjoints in small scenes:
+// neighbouring samples hit the same triangle and material): a full warp adding
+// to one entry sums with shuffles and adds once.
+struct BlockGradWarp : BlockGrad {
+    __device__ __forceinline__ void add(int i, float v) {
+        if (__activemask() == 0xffffffffu && __match_any_sync(0xffffffffu, i) == 0xffffffffu) {
+            for (int off = 16; off > 0; off >>= 1) v += __shfl_xor_sync(0xffffffffu, v, off);
+            if ((threadIdx.x & 31) != 0) return;
+        }
+        BlockGrad::add(i, v);
+    }
+};
+
 __device__ __forceinline__ BlockGrad block_grad_begin(float *sm, float *g, const GradCacheCfg &c) {
     BlockGrad b;
     b.sm = sm;

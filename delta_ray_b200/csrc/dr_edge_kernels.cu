@@ -261,7 +261,8 @@ __global__ void __launch_bounds__(128, 3) k_primary_edges(DevScene s, int W, int
                                                        const float *d_image, long long n, float *grad,
                                                        GradCacheCfg cfg) {
     extern __shared__ float sm[];
-    BlockGrad bg = block_grad_begin(sm, grad, cfg);
+    BlockGradWarp bg;
+    static_cast<BlockGrad &>(bg) = block_grad_begin(sm, grad, cfg);
     for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
         primary_edge_item<BMAX>(s, i, W, H, spp, B, seed, d_image, bg);
     block_grad_flush(bg);
