@@ -41,6 +41,11 @@ WORKLOADS = {
                         ref_res=(512, 512), ref_spp=16),
     "heightfield": dict(builder="heightfield", resolution=(160, 120), spp=4, max_bounces=3, scene_seed=0,
                         ref_res=(80, 60), ref_spp=1),
+    # the same heightfield with GGX lobes; the reference has no GGX material, so
+    # its arm reports this workload unavailable
+    "heightfield_ggx": dict(builder="heightfield", resolution=(160, 120), spp=4, max_bounces=3, scene_seed=0,
+                            ref_res=None, ref_spp=None, options={"microfacet": "ggx"},
+                            no_reference="the reference's materials are Blinn-Phong only (no GGX lobe)"),
 }
 WORKLOAD = WORKLOADS["soft_shadow"]
 # reference CPU arm: page-in / warm-up steps on a small slice of the same scene
@@ -70,12 +75,15 @@ def build_workload(res=None, spp=None):
     from delta_ray_b200 import workloads
     w = WORKLOAD
     return workloads.BUILDERS[w["builder"]](seed=w["scene_seed"], resolution=res or w["resolution"],
-                                            spp=spp or w["spp"], max_bounces=w["max_bounces"])
+                                            spp=spp or w["spp"], max_bounces=w["max_bounces"],
+                                            **w.get("options", {}))
 
 
 def workload_label():
     w = WORKLOAD
-    return f"{w['builder']} {w['resolution'][0]}x{w['resolution'][1]} {w['spp']}spp max_bounces={w['max_bounces']} fwd+bwd"
+    opts = "".join(f" {k}={v}" for k, v in w.get("options", {}).items())
+    return (f"{w['builder']} {w['resolution'][0]}x{w['resolution'][1]} {w['spp']}spp "
+            f"max_bounces={w['max_bounces']}{opts} fwd+bwd")
 
 
 # ---------------------------------------------------------------------------
@@ -323,7 +331,7 @@ def cpu_baseline():
     size (about 10-20 s of CPU work on 16 cores) after a small page-in step."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import ref_runner
-    if not ref_runner.reference_available():
+    if not ref_runner.reference_available() or WORKLOAD.get("no_reference"):
         return None
     reference_step(build_workload(REF_RES, spp=1), 0)  # page in, start the pool
     wl = build_workload(WORKLOAD["ref_res"], spp=WORKLOAD["ref_spp"])
@@ -344,8 +352,11 @@ def run_reference(args):
     if not ref_runner.reference_available():
         print(json.dumps({"impl": "reference", "unavailable": "reference build oracle/_ref missing"}))
         return 0
+    if WORKLOAD.get("no_reference"):
+        print(json.dumps({"impl": "reference", "unavailable": WORKLOAD["no_reference"]}))
+        return 0
     small = build_workload(REF_RES, spp=1)
-    for i in range(args.warmup):  # warm-up on a 192x192 slice: pages in, starts the pool
+    for i in range(args.warmup):  # warm-up on a 32x32 slice: pages in, starts the pool
         reference_step(small, 100 + i)
     wl = build_workload(WORKLOAD["ref_res"], spp=WORKLOAD["ref_spp"])
     W, H = wl.resolution
@@ -362,7 +373,7 @@ def run_reference(args):
                        "max_bounces": wl.max_bounces, "l2": "n/a (CPU)"},
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
                              "sample": f"{W}x{H} x {wl.spp} spp per step (forward call + backward call), "
-                                       f"{args.warmup} warm-up steps on a 192x192 slice"},
+                                       f"{args.warmup} warm-up steps on a 32x32 slice"},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
     return 0

@@ -114,8 +114,11 @@ def soft_shadow(seed=0, resolution=(512, 512), spp=16, max_bounces=1):
 
 
 def heightfield(seed=0, resolution=(640, 480), spp=64, max_bounces=3, grid=256,
-                patch=32):
-    """Glossy heightfield; one shape (and material) per ``patch`` x ``patch`` block."""
+                patch=32, microfacet="blinn_phong"):
+    """Glossy heightfield; one shape (and material) per ``patch`` x ``patch`` block.
+
+    ``microfacet`` picks the patches' specular lobe: "blinn_phong" (the
+    reference's material model) or "ggx"."""
     rng = np.random.default_rng(seed)
     res = [int(resolution[0]), int(resolution[1])]
     cam = _camera([0, 7, -9], [0, 0, 0], [0, 1, 0], 45.0, res)
@@ -145,7 +148,7 @@ def heightfield(seed=0, resolution=(640, 480), spp=64, max_bounces=3, grid=256,
             spec = rng.uniform(0.04, 0.9)
             mats.append(Material(diffuse_reflectance=_t(rng.uniform(0.2, 0.7, 3)),
                                  specular_reflectance=_t([spec, spec, spec]),
-                                 roughness=_t([rng.uniform(0.05, 0.5)])))
+                                 roughness=_t([rng.uniform(0.05, 0.5)]), microfacet=microfacet))
             shapes.append(Shape(_t(sub), _t(np.array(idx, np.int32), np.int32), None, None,
                                 len(mats) - 1))
     mats.append(Material(diffuse_reflectance=_t([0.0, 0.0, 0.0])))

@@ -172,6 +172,14 @@ def ggx_textured(seed=0, resolution=(40, 40), spp=2, max_bounces=2):
     return wl
 
 
+def ggx_heightfield(seed=0, resolution=(40, 32), spp=2, max_bounces=2):
+    """A 10 x 10-vertex heightfield in 4 patches with GGX lobes."""
+    wl = workloads.heightfield(seed=seed, resolution=resolution, spp=spp, max_bounces=max_bounces, grid=10,
+                               patch=5, microfacet="ggx")
+    wl.name = "ggx_heightfield"
+    return wl
+
+
 def icosphere_room(seed=0, resolution=(48, 40), spp=2, max_bounces=2, n_spheres=12, subdiv=(1, 2)):
     """A closed box room (12 triangles, 10 units a side, facing inwards) with
     a ceiling light and seeded icospheres (subdivision levels in `subdiv`,
@@ -206,4 +214,4 @@ def icosphere_room(seed=0, resolution=(48, 40), spp=2, max_bounces=2, n_spheres=
 SCENES = {"glossy_shadow": glossy_shadow, "textured": textured, "smooth_sphere": smooth_sphere,
           "fisheye": fisheye, "heightfield_small": heightfield_small, "mirror_shadow": mirror_shadow,
           "mirror_hall": mirror_hall, "icosphere_room": icosphere_room, "ggx_shadow": ggx_shadow,
-          "ggx_textured": ggx_textured}
+          "ggx_textured": ggx_textured, "ggx_heightfield": ggx_heightfield}

@@ -18,7 +18,9 @@ TOL = 1e-5
 # 2 / roughness (667 in mirror_hall), so one float ulp of that cosine moves the
 # BSDF by ~667 ulps; five such bounces in a row leave ~1e-5 of round-off
 # between two correct evaluation orders.
-CASE_TOL = {"mirror_hall": 5e-5}
+# GGX patches of roughness down to 0.05 (alpha 0.0025) divide by alpha^2 in
+# the normal distribution, which amplifies rounding in the same way.
+CASE_TOL = {"mirror_hall": 5e-5, "ggx_heightfield": 5e-5}
 
 
 @pytest.mark.parametrize("case", golden_cases())
@@ -80,7 +82,7 @@ def test_full_pixel_jitter_matches_oracle(case, ltc_table):
     assert rel_err(o0["image"], o["image"]) > 1e-3  # the flag changes where samples land
 
 
-@pytest.mark.parametrize("builder", ["ggx_shadow", "ggx_textured"])
+@pytest.mark.parametrize("builder", ["ggx_shadow", "ggx_textured", "ggx_heightfield"])
 def test_ggx_kernel_logic_matches_oracle(builder, ltc_table):
     """GGX lobes: the hand-written adjoints against the oracle's tape AD (the
     reference has no GGX, so this pins the product to the restatement only)."""
@@ -98,7 +100,7 @@ def test_ggx_kernel_logic_matches_oracle(builder, ltc_table):
         if parts == 2:
             assert h["stats"][1] == o["stats"][1], "different edges were sampled"
         assert np.abs(o["grad"]).max() > 0
-        assert rel_err(h["grad"], o["grad"]) < TOL, f"gradient term {parts}"
+        assert rel_err(h["grad"], o["grad"]) < CASE_TOL.get(builder, TOL), f"gradient term {parts}"
 
 
 def test_detached_pdf_matches_oracle(ltc_table):

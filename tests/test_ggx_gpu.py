@@ -20,7 +20,7 @@ def _scene(wl, ltc, ggx):
     return Scene(cam, mats, shps, lts, 0, None if ltc is None else torch.from_numpy(ltc), torch.from_numpy(ggx))
 
 
-@pytest.mark.parametrize("builder", ["ggx_shadow", "ggx_textured"])
+@pytest.mark.parametrize("builder", ["ggx_shadow", "ggx_textured", "ggx_heightfield"])
 def test_ggx_matches_oracle(builder, ltc_table):
     import scenes
     from delta_ray_b200 import ltc
