@@ -296,7 +296,9 @@ def measure_proposal(dev, K=32, train_calls=60):
 def load_traffic(stage):
     """DRAM bytes (read + write) per launch of `stage` from the committed ncu
     summary profiles/dram_traffic.txt ("<kernel> <bytes>" lines), if any; the
-    edge-evaluation stage sums its wavefront's two kernels."""
+    edge-evaluation stage sums its wavefront's three kernels."""
+    if WORKLOAD is not WORKLOADS["soft_shadow"]:
+        return None  # the table was captured on the soft-shadow workload
     table = {}
     try:
         with open(os.path.join(ROOT, "profiles", "dram_traffic.txt")) as f:
@@ -306,8 +308,9 @@ def load_traffic(stage):
                     table[parts[0]] = int(parts[1])
     except (OSError, ValueError):
         return None
-    if stage == "k_edge_eval" and "k_edge_line" in table and "k_edge_shade" in table:
-        return table["k_edge_line"] + table["k_edge_shade"]
+    if stage == "k_edge_eval":
+        wave = ("k_edge_line", "k_edge_rays", "k_edge_shade")
+        return sum(table[k] for k in wave) if all(k in table for k in wave) else None
     return table.get(stage)
 
 
@@ -488,12 +491,19 @@ def run_b200(args):
     e2e_value = world * samples / float(e2e_t.item())
 
     # roofline of the dominant stage; the edge-evaluation wavefront (line
-    # samples, then shading of the survivors) counts as one stage
+    # samples, their rays, shading of the rest) counts as one stage
     peak, peak_kind = load_peaks()
-    merged = [s_ for s_ in stages if s_[0] not in ("k_edge_line", "k_edge_shade")]
-    wave = [s_ for s_ in stages if s_[0] in ("k_edge_line", "k_edge_shade")]
+    # and so does the two-stage traversal of large edge trees (k_edge_expand,
+    # then k_edge_tasks)
+    wave_names = ("k_edge_line", "k_edge_rays", "k_edge_shade")
+    split_names = ("k_edge_expand", "k_edge_tasks")
+    merged = [s_ for s_ in stages if s_[0] not in wave_names + split_names]
+    wave = [s_ for s_ in stages if s_[0] in wave_names]
+    split = [s_ for s_ in stages if s_[0] in split_names]
     if wave:
         merged.append(("k_edge_eval", sum(ms for _, ms in wave)))
+    if split:
+        merged.append(("k_edge_traverse", sum(ms for _, ms in split)))
     dom = max(merged, key=lambda s: s[1]) if merged else ("", 0.0)
     dom_bytes = stage_bytes(dom[0], wl, counts)
     achieved = dom_bytes / (dom[1] / 1e3) / 1e9 if dom[1] > 0 else 0.0

@@ -82,7 +82,7 @@ template <typename T> std::vector<T> fetch(const T *src, size_t count, const cha
 // reference's RenderFunction does) allocates them once.  Only idle queues are
 // cached; `idle` orders their reuse after the last kernels that touched them.
 struct BackwardQueues {
-    DevBuf pt, items, item_w, item_dp, pt_last, counts, survivors, tasks;
+    DevBuf pt, items, item_w, item_dp, pt_last, counts, survivors, hits, tasks;
     long long cap_items = 0;     // grown on overflow, kept with the buffers
     double points_per_sample = 1;  // shading points per pixel sample the last overflow asked for
     cudaEvent_t idle = nullptr;
@@ -636,11 +636,13 @@ void backward_on_queues(dr_scene *scene, const dr_render_desc *rd, const DevScen
         q.item_w.reserve(sizeof(float) * cap_items);
         q.item_dp.reserve(sizeof(float) * 3 * cap_items);
         q.survivors.reserve(sizeof(float4) * 2 * cap_items);
+        q.hits.reserve(sizeof(int4) * cap_items);
         q.cap_items = cap_items;
         ws.items = q.items.as<int4>();
         ws.item_w = q.item_w.as<float>();
         ws.item_dp = q.item_dp.as<float>();
         ws.survivors = q.survivors.as<float4>();
+        ws.hits = q.hits.as<int4>();
         ws.cap_items = cap_items;
     };
     auto bind_points = [&]() {
@@ -1006,7 +1008,7 @@ dr_status dr_render_backward_noalloc(dr_scene *scene, const dr_render_desc *rd, 
         cudaStream_t st = (cudaStream_t)stream;
         scene->last_launches = 0;
         unsigned char *base = noalloc_scratch(scene->device);
-        // layout: counters | point records | point keys | items | item weights | item dp | survivors
+        // layout: counters | point records | point keys | items | item weights | item dp | survivors | hits
         auto up = [](size_t b) { return (b + 255) & ~size_t(255); };
         // scenes with specular chains: room for the points of every bounce,
         // up to half the scratch (the rest holds edge items)
@@ -1023,8 +1025,8 @@ dr_status dr_render_backward_noalloc(dr_scene *scene, const dr_render_desc *rd, 
         off += up(sizeof(float) * DR_PT_FLOATS * (size_t)cap_points);
         ws.pt_last = (unsigned long long *)(base + off);
         off += up(DR_PT_LAST_BYTES * (size_t)cap_points);
-        long long cap_items = (long long)((kNoAllocScratchBytes - off - 4 * 256) /
-                                          (sizeof(int4) + 4 * sizeof(float) + 2 * sizeof(float4)));
+        long long cap_items = (long long)((kNoAllocScratchBytes - off - 5 * 256) /
+                                          (2 * sizeof(int4) + 4 * sizeof(float) + 2 * sizeof(float4)));
         ws.items = (int4 *)(base + off);
         off += up(sizeof(int4) * (size_t)cap_items);
         ws.item_w = (float *)(base + off);
@@ -1033,6 +1035,8 @@ dr_status dr_render_backward_noalloc(dr_scene *scene, const dr_render_desc *rd, 
         off += up(sizeof(float) * 3 * (size_t)cap_items);
         ws.survivors = (float4 *)(base + off);
         off += up(sizeof(float4) * 2 * (size_t)cap_items);
+        ws.hits = (int4 *)(base + off);
+        off += up(sizeof(int4) * (size_t)cap_items);
         if (off > kNoAllocScratchBytes) throw DrError(DR_ERR_INVALID_ARGUMENT, "scratch layout does not fit");
         ws.cap_points = cap_points;
         ws.cap_items = cap_items;

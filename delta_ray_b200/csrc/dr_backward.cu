@@ -4,8 +4,11 @@
 //                      pixel's samples, image, and the shading-point records
 //   k_edge_traverse    one thread per shading point: edge-tree traversal,
 //                      appends (point, edge, weight) items
-//   k_edge_eval        one thread per item: two straddling rays, shading of
-//                      both sides, dv0/dv1 scatter and dp
+//   k_edge_line        one thread per item: the line sample on the edge
+//   k_edge_rays        one thread per surviving line sample: two straddling
+//                      rays and the tests on their hits
+//   k_edge_shade       one thread per kept sample: shading of both sides,
+//                      dv0/dv1 scatter and dp
 //   k_dp_propagate     one thread per point: the point's dp through its
 //                      triangle and the camera (reference "last edge" rule)
 //   k_primary_edges    one thread per primary-edge sample
@@ -80,7 +83,7 @@ __global__ void __launch_bounds__(128, 3) k_backward_paths(DevScene s, int W, in
 // Position adjoints of the shading points pushed back along their paths.
 // DR_DP_REFERENCE_LAST: each point's last edge with a nonzero dp (the largest
 // key ((j + 1) << 32 | item) in pt_last).  DR_DP_SUM (scenes with specular
-// chains only): the dp sums k_edge_eval accumulated for points after the first
+// chains only): the dp sums k_edge_shade accumulated for points after the first
 // vertex, whose chains are traced again here, in this IEEE compile unit.
 template <bool kChains>
 __global__ void __launch_bounds__(128) k_dp_propagate(DevScene s, int W, int H, int spp, uint64_t seed, int dp_mode,

@@ -570,17 +570,20 @@ DEV bool item_line(const DevScene &s, const PointRecord &pt, int tree, int ei, u
     return edge_line_sample<EXT>(s, es, edge, pt.wi, pt.tri, pt.surface(), el);
 }
 
-// The item's shading (second phase) from its line sample; as eval_item.
+// The item's shading from its line sample; as eval_item.  `hits` (may be
+// null): the closest hits of the sample's two rays, which edge_rays kept.
 template <bool EXT = true, bool MAYBE_GI = true, class G>
 DEV float3 item_shade(const DevScene &s, const PointRecord &pt, int tree, int ei, int j, float w, int spp, int B,
-                      uint64_t seed, G &g, float *mag, const EdgeLine &el) {
+                      uint64_t seed, G &g, float *mag, const EdgeLine &el, const EdgeHits *hits = nullptr) {
     Rng irng;
     irng.init(seed, kStreamEdgeItem, pt.sid, ((uint32_t)pt.bounce << 28) | (uint32_t)j);
     LightSample els = draw_light(irng);
     const DevEdge &edge = tree ? s.nrm_edges[ei] : s.sil_edges[ei];
     float3 weight = f3(1.f) * ((1.f / spp) * w);
-    EdgeResult er = edge_shade_sample<MAYBE_GI>(s, el, edge, els, irng, B - pt.bounce - 1, pt.wi, pt.tri,
-                                                pt.surface(), weight, pt.d_color, B == 1);
+    EdgeResult er = hits ? edge_shade_hits<MAYBE_GI>(s, el, edge, els, irng, B - pt.bounce - 1, pt.wi, pt.tri,
+                                                     pt.surface(), weight, pt.d_color, B == 1, *hits)
+                         : edge_shade_sample<MAYBE_GI>(s, el, edge, els, irng, B - pt.bounce - 1, pt.wi, pt.tri,
+                                                       pt.surface(), weight, pt.d_color, B == 1);
     if (EXT && mag) *mag = abs_sum(er.dv0) + abs_sum(er.dv1);
     if (!is_zero(er.dv0) || !is_zero(er.dv1)) {
         const DevShape &sh = s.shapes[edge.shape];

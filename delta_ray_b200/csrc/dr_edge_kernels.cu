@@ -182,32 +182,17 @@ __device__ __forceinline__ void finish_item(const DevScene &s, const BackwardWor
     }
 }
 
+// Edge evaluation as a three-kernel wavefront, each stage compacting what it
+// keeps so that the next runs with full warps.  k_edge_line: the line sample
+// of every item (silhouette test, LTC lobe, point on the edge); often half the
+// items end here (edges in the point's own plane, below the lobe's horizon or
+// outside the clipped segment).  k_edge_rays: the two rays of each survivor and
+// the tests on their hits; with direct lighting only, a sample neither of whose
+// rays hits an emitter ends here too.  k_edge_shade: the shading and the
+// Jacobians of the rest.
+//
 // EXT: DR_FLAG_EDGE_LOBE_MIS or proposal training in use; GI: max_bounces > 1
 // (the shade calls of the two sides); the launcher picks the variant.
-// One thread evaluates each item whole (the no-alloc backward's path).
-template <bool EXT, bool GI>
-__global__ void __launch_bounds__(128, 4) k_edge_eval(DevScene s, int W, int H, int spp, int B, uint64_t seed, int dp_mode,
-                                                   float *grad, BackwardWorkspace ws, GradCacheCfg cfg) {
-    extern __shared__ float sm[];
-    BlockGrad bg = block_grad_begin(sm, grad, cfg);
-    long long n = (long long)min(ws.counters->items, (unsigned long long)ws.cap_items);
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x) {
-        int4 it = ws.items[i];
-        PointRecord pt;
-        pt.load(ws.pt + (size_t)it.x * DR_PT_WORDS);
-        int tree = it.y >> 30, ei = it.y & ((1 << 30) - 1);
-        float mag = 0.f;
-        float3 dp = eval_item<EXT, GI>(s, pt, tree, ei, it.z, ws.item_w[i], spp, B, seed, bg, &mag);
-        finish_item<EXT>(s, ws, it, i, pt, dp, mag, W, H, spp, seed, dp_mode, bg);
-    }
-    block_grad_flush(bg);
-}
-
-// Edge evaluation as a two-kernel wavefront.  k_edge_line: the line sample of
-// every item (silhouette test, LTC lobe, point on the edge); the survivors
-// (often half the items: edges in the point's own plane, below the lobe's
-// horizon or outside the clipped segment end here) are compacted, so that
-// k_edge_shade runs its rays and shading with full warps.
 template <bool EXT>
 __global__ void __launch_bounds__(128, 4) k_edge_line(DevScene s, uint64_t seed, BackwardWorkspace ws) {
     long long n = (long long)min(ws.counters->items, (unsigned long long)ws.cap_items);
@@ -232,13 +217,44 @@ __global__ void __launch_bounds__(128, 4) k_edge_line(DevScene s, uint64_t seed,
     }
 }
 
+template <bool DIRECT>
+__global__ void __launch_bounds__(128, 4) k_edge_rays(DevScene s, BackwardWorkspace ws) {
+    long long n = (long long)min(ws.counters->survivors, (unsigned long long)ws.cap_items);
+    long long stride = (long long)gridDim.x * blockDim.x;
+    // warp-uniform loop: the append is warp-aggregated
+    for (long long base = (long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < n; base += stride) {
+        long long k = base + (threadIdx.x & 31);
+        EdgeHits eh;
+        bool ok = false;
+        if (k < n) {
+            float4 a = ws.survivors[2 * k];
+            int4 it = ws.items[__float_as_int(a.x)];
+            // the point's position and triangle: words 0-2 and 17 of its record
+            const float *w = ws.pt + (size_t)it.x * DR_PT_WORDS;
+            EdgeLine el;
+            el.sample_p = f3(a.y, a.z, a.w);
+            int tree = it.y >> 30, ei = it.y & ((1 << 30) - 1);
+            const DevEdge &edge = tree ? s.nrm_edges[ei] : s.sil_edges[ei];
+            ok = edge_rays(s, el, edge, dr_f2i(w[17]), f3(w[0], w[1], w[2]), DIRECT, eh);
+        }
+        __syncwarp();
+        unsigned long long slot = warp_reserve(&ws.counters->hits, ok ? 1 : 0);
+        if (ok) ws.hits[slot] = make_int4((int)k, eh.r, eh.l, 0);
+    }
+}
+
 template <bool EXT, bool GI>
 __global__ void __launch_bounds__(128, 4) k_edge_shade(DevScene s, int W, int H, int spp, int B, uint64_t seed,
                                                     int dp_mode, float *grad, BackwardWorkspace ws, GradCacheCfg cfg) {
     extern __shared__ float sm[];
     BlockGrad bg = block_grad_begin(sm, grad, cfg);
-    long long n = (long long)min(ws.counters->survivors, (unsigned long long)ws.cap_items);
-    for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x) {
+    long long n = (long long)min(ws.counters->hits, (unsigned long long)ws.cap_items);
+    for (long long h = (long long)blockIdx.x * blockDim.x + threadIdx.x; h < n; h += (long long)gridDim.x * blockDim.x) {
+        int4 hr = ws.hits[h];
+        EdgeHits eh;
+        eh.r = hr.y;
+        eh.l = hr.z;
+        long long k = hr.x;
         float4 a = ws.survivors[2 * k], b = ws.survivors[2 * k + 1];
         long long i = __float_as_int(a.x);
         EdgeLine el;
@@ -250,7 +266,7 @@ __global__ void __launch_bounds__(128, 4) k_edge_shade(DevScene s, int W, int H,
         pt.load(ws.pt + (size_t)it.x * DR_PT_WORDS);
         int tree = it.y >> 30, ei = it.y & ((1 << 30) - 1);
         float mag = 0.f;
-        float3 dp = item_shade<EXT, GI>(s, pt, tree, ei, it.z, ws.item_w[i], spp, B, seed, bg, &mag, el);
+        float3 dp = item_shade<EXT, GI>(s, pt, tree, ei, it.z, ws.item_w[i], spp, B, seed, bg, &mag, el, &eh);
         finish_item<EXT>(s, ws, it, i, pt, dp, mag, W, H, spp, seed, dp_mode, bg);
     }
     block_grad_flush(bg);
@@ -296,24 +312,20 @@ cudaError_t dr_launch_edge_eval(const DevScene &s, int W, int H, int spp, int B,
     size_t smem = sizeof(float) * (size_t)(cfg.head + cfg.tail_len);
     const bool ext = s.edge_lobe_mis || ws.train_targets;
     const int grid = stage_grid(num_sms);
-    if (!ws.survivors) {
-        auto kernel = ext ? (B > 1 ? k_edge_eval<true, true> : k_edge_eval<true, false>)
-                          : (B > 1 ? k_edge_eval<false, true> : k_edge_eval<false, false>);
-        kernel<<<grid, 128, smem, st>>>(s, W, H, spp, B, seed, dp_mode, grad, ws, cfg);
-        timer->mark(st, "k_edge_eval");
-        *launches += 1;
-        return cudaGetLastError();
-    }
-    cudaError_t e = cudaMemsetAsync(&ws.counters->survivors, 0, sizeof(unsigned long long), st);
+    // the survivor and hit counters (adjacent)
+    cudaError_t e = cudaMemsetAsync(&ws.counters->survivors, 0, 2 * sizeof(unsigned long long), st);
     if (e != cudaSuccess) return e;
     if (ext) k_edge_line<true><<<grid, 128, 0, st>>>(s, seed, ws);
     else k_edge_line<false><<<grid, 128, 0, st>>>(s, seed, ws);
     timer->mark(st, "k_edge_line");
+    if (B > 1) k_edge_rays<false><<<grid, 128, 0, st>>>(s, ws);
+    else k_edge_rays<true><<<grid, 128, 0, st>>>(s, ws);
+    timer->mark(st, "k_edge_rays");
     auto shade = ext ? (B > 1 ? k_edge_shade<true, true> : k_edge_shade<true, false>)
                      : (B > 1 ? k_edge_shade<false, true> : k_edge_shade<false, false>);
     shade<<<grid, 128, smem, st>>>(s, W, H, spp, B, seed, dp_mode, grad, ws, cfg);
     timer->mark(st, "k_edge_shade");
-    *launches += 2;
+    *launches += 3;
     return cudaGetLastError();
 }
 

@@ -647,57 +647,82 @@ DEV bool edge_line_sample(const DevScene &s, const EdgeSample &es, const DevEdge
     return true;
 }
 
+// The two rays of an edge sample, one on each side of the edge: their closest
+// hits and the tests that need nothing but the hits (delta_ray.cpp:223-313:
+// exactly one side must hit a face of the edge, neither may hit the shading
+// point's own triangle, neither hit may lie on a near-degenerate segment).
+// With direct lighting only (DIRECT_ONLY), a sample neither of whose sides hits
+// an emitter contributes nothing and ends here too.
+struct EdgeHits {
+    int r, l;  // closest-hit triangles of the "right" (+split_n) and "left" ray, -1 for none
+};
+
+DEV void edge_side_dirs(const EdgeLine &el, float3 v0, float3 v1, float3 p, float3 &sdir, float3 &rdir, float3 &ldir) {
+    float3 split_n = normalize(cross(v0 - p, v1 - p));
+    float delta = 1e-3f * length(el.sample_p);
+    sdir = normalize(el.sample_p);
+    rdir = normalize(sdir + delta * split_n);
+    ldir = normalize(sdir - delta * split_n);
+}
+
+DEV bool edge_rays(const DevScene &s, const EdgeLine &el, const DevEdge &edge, int stri, float3 p, bool direct_only,
+                   EdgeHits &out) {
+    float3 sdir, rdir, ldir;
+    edge_side_dirs(el, edge_v0(s, edge), edge_v1(s, edge), p, sdir, rdir, ldir);
+    int hit[2];
+    bool conn[2];
+    // both sides through one copy of the trace code: a loop, not unrolled
+#pragma unroll 1
+    for (int k = 0; k < 2; k++) {
+        float3 dir = k == 0 ? rdir : ldir;
+        Hit hh = trace_closest(s, p, dir, 1e-3f);
+        hit[k] = hh.tri;
+        conn[k] = false;
+        if (hh.tri >= 0) {
+            int lt = s.tri_local[hh.tri];
+            conn[k] = s.tri[hh.tri].w == edge.shape && (lt == edge.f0 || lt == edge.f1);
+        }
+    }
+    if (conn[0] == conn[1] || (hit[0] >= 0 && hit[0] == stri) || (hit[1] >= 0 && hit[1] == stri)) return false;
+#pragma unroll 1
+    for (int k = 0; k < 2; k++) {
+        if (hit[k] < 0) continue;
+        SurfacePoint pp = intersect_tri(load_tri(s, hit[k]), p, k == 0 ? rdir : ldir);
+        float3 dir = pp.p - p;
+        if (length(dir) * fabsf(dot(normalize(dir), pp.ng)) < 1e-3f) return false;
+    }
+    if (direct_only && (hit[0] < 0 || light_of_tri(s, hit[0]) < 0) && (hit[1] < 0 || light_of_tri(s, hit[1]) < 0))
+        return false;
+    out.r = hit[0];
+    out.l = hit[1];
+    return true;
+}
+
+// The shading of an edge sample whose rays edge_rays kept: the emitters and
+// (with more bounces) the radiance seen on each side, the BSDF toward the
+// edge, and the Jacobians of the sample w.r.t. the shading point and the
+// edge's end points.
 template <bool MAYBE_GI = true>
-DEV EdgeResult edge_shade_sample(const DevScene &s, const EdgeLine &el_, const DevEdge &edge, const LightSample &ls,
-                                 const Rng &rng, int nbounces, float3 wi, int stri, const SurfacePoint &sp,
-                                 float3 weight, float3 d_color, bool direct_only) {
+DEV EdgeResult edge_shade_hits(const DevScene &s, const EdgeLine &el_, const DevEdge &edge, const LightSample &ls,
+                               const Rng &rng, int nbounces, float3 wi, int stri, const SurfacePoint &sp,
+                               float3 weight, float3 d_color, bool direct_only, const EdgeHits &hits) {
     EdgeResult none;
     none.dp = none.dv0 = none.dv1 = f3(0.f);
     const float3 sample_p = el_.sample_p;
     float3 v0 = edge_v0(s, edge), v1 = edge_v1(s, edge);
     int mi = material_of_tri(s, stri);
-    float3 split_n = normalize(cross(v0 - sp.p, v1 - sp.p));
-    float delta = 1e-3f * length(sample_p);
-    float3 sdir = normalize(sample_p);
-    float3 rdir = normalize(sdir + delta * split_n), ldir = normalize(sdir - delta * split_n);
-    // The two sides of the edge ("right" along +split_n, then "left") run
-    // through one copy of the trace and shade code: loops, not unrolled.
-    Hit hr, hl;
+    float3 sdir, rdir, ldir;
+    edge_side_dirs(el_, v0, v1, sp.p, sdir, rdir, ldir);
     SurfacePoint pr, pl;
-    int rsh = -1, rlt = -1, lsh = -1, llt = -1;
-#pragma unroll 1
-    for (int k = 0; k < 2; k++) {
-        float3 dir = k == 0 ? rdir : ldir;
-        Hit hh = trace_closest(s, sp.p, dir, 1e-3f);
-        SurfacePoint pp;
-        int sh = -1, lt = -1;
-        if (hh.tri >= 0) {
-            pp = intersect_tri(load_tri(s, hh.tri), sp.p, dir);
-            sh = s.tri[hh.tri].w;
-            lt = s.tri_local[hh.tri];
-        }
-        if (k == 0) {
-            hr = hh;
-            pr = pp;
-            rsh = sh;
-            rlt = lt;
-        } else {
-            hl = hh;
-            pl = pp;
-            lsh = sh;
-            llt = lt;
-        }
-    }
-    bool rc = rsh == edge.shape && (rlt == edge.f0 || rlt == edge.f1);
-    bool lc = lsh == edge.shape && (llt == edge.f0 || llt == edge.f1);
-    if ((!rc && !lc) || (rc && lc) || (hr.tri >= 0 && hr.tri == stri) || (hl.tri >= 0 && hl.tri == stri)) return none;
+    if (hits.r >= 0) pr = intersect_tri(load_tri(s, hits.r), sp.p, rdir);
+    if (hits.l >= 0) pl = intersect_tri(load_tri(s, hits.l), sp.p, ldir);
     float3 eb = bsdf(s, mi, sp, wi, sdir);
     if (sum(eb) < 1e-6f) return none;
     float3 shr = f3(0.f), shl = f3(0.f);
     if (MAYBE_GI && !direct_only) {
 #pragma unroll 1
         for (int k = 0; k < 2; k++) {
-            int tri = k == 0 ? hr.tri : hl.tri;
+            int tri = k == 0 ? hits.r : hits.l;
             SurfacePoint pp = k == 0 ? pr : pl;
             float3 sh = shade(s, -sdir, tri, pp, ls, rng, nbounces, false);
             if (tri >= 0) {
@@ -713,18 +738,10 @@ DEV EdgeResult edge_shade_sample(const DevScene &s, const EdgeLine &el_, const D
     float3 er, el;
 #pragma unroll 1
     for (int k = 0; k < 2; k++) {
-        float3 e = k == 0 ? eval_light(s, wi, stri, sp, hr.tri, pr) + eb * shr
-                          : eval_light(s, wi, stri, sp, hl.tri, pl) + eb * shl;
+        float3 e = k == 0 ? eval_light(s, wi, stri, sp, hits.r, pr) + eb * shr
+                          : eval_light(s, wi, stri, sp, hits.l, pl) + eb * shl;
         if (k == 0) er = e;
         else el = e;
-    }
-    if (hr.tri >= 0) {
-        float3 dir = pr.p - sp.p;
-        if (length(dir) * fabsf(dot(normalize(dir), pr.ng)) < 1e-3f) return none;
-    }
-    if (hl.tri >= 0) {
-        float3 dir = pl.p - sp.p;
-        if (length(dir) * fabsf(dot(normalize(dir), pl.ng)) < 1e-3f) return none;
     }
     EdgeResult res = none;
     auto accum = [&](const SurfacePoint &lp, float3 ev) {
@@ -745,11 +762,25 @@ DEV EdgeResult edge_shade_sample(const DevScene &s, const EdgeLine &el_, const D
     };
 #pragma unroll 1
     for (int k = 0; k < 2; k++) {
-        int tri = k == 0 ? hr.tri : hl.tri;
+        int tri = k == 0 ? hits.r : hits.l;
         float3 e = k == 0 ? er : el;
         if (tri >= 0 && abs_sum(e) > 0.f) accum(k == 0 ? pr : pl, k == 0 ? e : -e);
     }
     return res;
+}
+
+// The whole shading of an edge sample: edge_rays, then edge_shade_hits.
+template <bool MAYBE_GI = true>
+DEV EdgeResult edge_shade_sample(const DevScene &s, const EdgeLine &el, const DevEdge &edge, const LightSample &ls,
+                                 const Rng &rng, int nbounces, float3 wi, int stri, const SurfacePoint &sp,
+                                 float3 weight, float3 d_color, bool direct_only) {
+    EdgeHits hits;
+    if (!edge_rays(s, el, edge, stri, sp.p, direct_only || !MAYBE_GI, hits)) {
+        EdgeResult none;
+        none.dp = none.dv0 = none.dv1 = f3(0.f);
+        return none;
+    }
+    return edge_shade_hits<MAYBE_GI>(s, el, edge, ls, rng, nbounces, wi, stri, sp, weight, d_color, direct_only, hits);
 }
 
 template <bool EXT = true, bool MAYBE_GI = true>

@@ -49,7 +49,8 @@ struct BackwardCounters {
     unsigned long long items;   // edge items appended by the last k_edge_traverse
     int status;                 // DR_STATUS_* bits
     int pad;
-    unsigned long long survivors;  // line samples k_edge_line kept for k_edge_shade
+    unsigned long long survivors;  // line samples k_edge_line kept for k_edge_rays
+    unsigned long long hits;       // samples k_edge_rays kept for k_edge_shade (follows survivors)
     unsigned long long tasks;      // subtrees k_edge_expand handed on to k_edge_tasks
 };
 
@@ -67,16 +68,18 @@ struct BackwardWorkspace {
     unsigned long long *pt_last;
     BackwardCounters *counters;
     // points [pt_begin, min(pt_end, counters->points)) go through the edge
-    // stage (k_edge_traverse, k_edge_eval, k_dp_propagate) of one launch
+    // stage (traversal, edge evaluation, k_dp_propagate) of one launch
     long long pt_begin, pt_end;
     // learned edge proposal (null: the reference's sampling): [cap_points][32]
     // bf16 slot probabilities, the mixture weight, and the training targets of
     // points p = k * train_stride, k < train_n ([train_n][32] f32 contribution
     // magnitudes per slot)
     // line samples that survived the first phase of edge evaluation:
-    // [cap_items][2] float4 (item index bits, sample_p; d sample_p / d l, density);
-    // null: one kernel evaluates each item whole
+    // [cap_items][2] float4 (item index bits, sample_p; d sample_p / d l, density)
     float4 *survivors;
+    // [cap_items] (survivor index, closest-hit triangle of the right and the
+    // left ray, 0): the line samples whose rays k_edge_rays kept
+    int4 *hits;
     // subtrees of large trees' traversals handed on to a second stage
     // (null: one thread walks each point whole)
     EdgeTask *tasks;
@@ -112,8 +115,8 @@ cudaError_t dr_launch_edge_traverse(const DevScene &s, uint64_t seed, const Back
                                     cudaStream_t st, int *launches, StageTimer *timer);
 // dst[0..n) += src[0..n)
 cudaError_t dr_launch_accumulate(float *dst, const float *src, long long n, cudaStream_t st);
-// Launchers of the edge half (dr_edge_kernels.cu).  Edge evaluation: the
-// two-kernel wavefront when ws.survivors is bound, one kernel otherwise.
+// Launchers of the edge half (dr_edge_kernels.cu).  Edge evaluation is a
+// three-kernel wavefront: line samples, their rays, their shading.
 cudaError_t dr_launch_edge_eval(const DevScene &s, int W, int H, int spp, int B, uint64_t seed, int dp_mode,
                                 float *grad, const BackwardWorkspace &ws, const GradCacheCfg &cfg, int num_sms,
                                 cudaStream_t st, int *launches, StageTimer *timer);

@@ -254,7 +254,7 @@ DR_API dr_status dr_render_backward_views(dr_scene *scene, int n_views, const dr
  * array per device that is part of the library's module image.  Limits:
  * width * height * spp <= 65536 (larger calls fail with
  * DR_ERR_INVALID_ARGUMENT); sampled edges beyond the array's room (about
- * 400,000 at the largest image) are evaluated in several passes over the
+ * 330,000 at the largest image) are evaluated in several passes over the
  * shading points, and a single point with more edges than that fails with
  * DR_ERR_OUT_OF_MEMORY, as do specular chains whose shading points outgrow
  * half the array (about 150,000 points).  All calls on
