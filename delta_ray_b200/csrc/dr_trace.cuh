@@ -134,6 +134,31 @@ DEV_NOINLINE Hit trace_closest_bvh(const float4 *DR_RESTRICT nodes, const float4
     return h;
 }
 
+// Scenes of at most DR_LINEAR_TRIS triangles are traced by testing every
+// triangle: a loop that all lanes of a warp run in step, with no stack.  Both
+// ways keep the smallest t, ties going to the smaller triangle id, so they
+// agree unless the walk's widened box test (2 gamma(3)) rounds a hit lying
+// within ~1e-6 of the closest one out of its box.
+#define DR_LINEAR_TRIS 16
+
+DEV_NOINLINE Hit trace_closest_linear(const float4 *DR_RESTRICT tris, int n, float3 o, float3 d, float tnear) {
+    Hit h;
+    h.tri = -1;
+    h.t = DR_INF;
+    for (int i = 0; i < n; i++) {
+        float4 a = dr_ldg(tris + 3 * i), b = dr_ldg(tris + 3 * i + 1), c = dr_ldg(tris + 3 * i + 2);
+        float t;
+        if (hit_triangle(a, b, c, o, d, t) && t > tnear) {
+            int id = dr_f2i(a.w);
+            if (t < h.t || (t == h.t && id < h.tri)) {
+                h.t = t;
+                h.tri = id;
+            }
+        }
+    }
+    return h;
+}
+
 DEV Hit trace_closest(const DevScene &s, float3 o, float3 d, float tnear) {
     if (s.num_tris == 0) {
         Hit h;
@@ -141,6 +166,7 @@ DEV Hit trace_closest(const DevScene &s, float3 o, float3 d, float tnear) {
         h.t = DR_INF;
         return h;
     }
+    if (s.num_tris <= DR_LINEAR_TRIS) return trace_closest_linear(s.bvh_tris, s.num_tris, o, d, tnear);
     return trace_closest_bvh(s.bvh_nodes, s.bvh_tris, s.bvh_root, o, d, tnear);
 }
 
@@ -182,8 +208,19 @@ DEV_NOINLINE bool trace_any_bvh(const float4 *DR_RESTRICT nodes, const float4 *D
     return false;
 }
 
+DEV_NOINLINE bool trace_any_linear(const float4 *DR_RESTRICT tris, int n, float3 o, float3 d, float tnear,
+                                   float tfar) {
+    for (int i = 0; i < n; i++) {
+        float4 a = dr_ldg(tris + 3 * i), b = dr_ldg(tris + 3 * i + 1), c = dr_ldg(tris + 3 * i + 2);
+        float t;
+        if (hit_triangle(a, b, c, o, d, t) && t > tnear && t < tfar) return true;
+    }
+    return false;
+}
+
 DEV bool trace_any(const DevScene &s, float3 o, float3 d, float tnear, float tfar) {
     if (s.num_tris == 0) return false;
+    if (s.num_tris <= DR_LINEAR_TRIS) return trace_any_linear(s.bvh_tris, s.num_tris, o, d, tnear, tfar);
     return trace_any_bvh(s.bvh_nodes, s.bvh_tris, s.bvh_root, o, d, tnear, tfar);
 }
 

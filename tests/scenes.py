@@ -215,3 +215,18 @@ SCENES = {"glossy_shadow": glossy_shadow, "textured": textured, "smooth_sphere":
           "fisheye": fisheye, "heightfield_small": heightfield_small, "mirror_shadow": mirror_shadow,
           "mirror_hall": mirror_hall, "icosphere_room": icosphere_room, "ggx_shadow": ggx_shadow,
           "ggx_textured": ggx_textured, "ggx_heightfield": ggx_heightfield}
+
+
+def scene_rays(wl, n, seed=0):
+    """n rays [n, 6] (float32): origins in a box twice the scene's size, half of
+    them aimed at random points of the scene's bounding box, half in random
+    directions (misses and grazing hits)."""
+    v = np.concatenate([np.asarray(sh.vertices, np.float64).reshape(-1, 3) for sh in wl.shapes])
+    lo, hi = v.min(0), v.max(0)
+    c, e = (lo + hi) / 2, np.maximum(hi - lo, 1e-3)
+    rng = np.random.default_rng(seed)
+    o = rng.uniform(c - e, c + e, (n, 3))
+    d = rng.uniform(lo, hi, (n, 3)) - o
+    d[n // 2:] = rng.normal(size=(n - n // 2, 3))
+    d /= np.linalg.norm(d, axis=1, keepdims=True)
+    return np.concatenate([o, d], 1).astype(np.float32)

@@ -51,6 +51,26 @@ def test_dp_sum_mode_matches_oracle(ltc_table):
     assert rel_err(h["grad"], o["grad"]) < TOL
 
 
+def test_linear_scan_hits_match_oracle():
+    """Scenes of at most 16 triangles are traced by testing every triangle (no
+    BVH walk): hit ids of the soft-shadow scene's 8 triangles against the
+    oracle's BVH."""
+    from delta_ray_b200 import workloads
+    from scenes import scene_rays
+    wl = workloads.soft_shadow(seed=3, resolution=(32, 32), spp=1, max_bounces=1)
+    rays = scene_rays(wl, 20000, seed=0)
+    tri, t, visits = harness.trace(wl, rays)
+    assert visits == 0  # no BVH node visited
+    sh, lt, tr = oracle.trace(wl, rays)
+    offs = np.cumsum([0] + [s.indices.shape[0] for s in wl.shapes])
+    gid = np.where(sh >= 0, offs[np.maximum(sh, 0)] + lt, -1)
+    assert (gid >= 0).mean() > 0.15
+    same = gid == tri
+    tie = np.isclose(t, tr, rtol=1e-5, atol=1e-6) & ~same
+    assert (same | tie).all(), f"{(~(same | tie)).sum()} rays hit different triangles"
+    assert same.mean() > 0.999
+
+
 def test_traversal_visits_few_nodes():
     """Closest-hit traversal of a 130k-triangle heightfield stays logarithmic."""
     from delta_ray_b200 import workloads

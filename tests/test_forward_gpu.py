@@ -83,3 +83,23 @@ def test_hit_ids_match_oracle():
     tie = np.isclose(t, tr, rtol=1e-5, atol=1e-6) & ~same
     assert (same | tie).all(), f"{(~(same | tie)).sum()} rays hit different triangles"
     assert same.mean() > 0.999
+
+
+def test_hit_ids_match_oracle_linear_scan():
+    """Scenes of at most 16 triangles are traced by testing every triangle:
+    the soft-shadow scene's 8 triangles against the oracle's BVH."""
+    from delta_ray_b200 import workloads
+    from scenes import scene_rays
+    wl = workloads.soft_shadow(seed=3, resolution=(32, 32), spp=1, max_bounces=1)
+    rays = scene_rays(wl, 20000, seed=0)
+    sc = product_scene(wl)
+    tri, t = sc.trace(torch.from_numpy(rays))
+    tri, t = tri.cpu().numpy(), t.cpu().numpy()
+    sh, lt, tr = oracle.trace(wl, rays)
+    offs = np.cumsum([0] + [s.indices.shape[0] for s in wl.shapes])
+    gid = np.where(sh >= 0, offs[np.maximum(sh, 0)] + lt, -1)
+    assert (gid >= 0).mean() > 0.15
+    same = gid == tri
+    tie = np.isclose(t, tr, rtol=1e-5, atol=1e-6) & ~same
+    assert (same | tie).all(), f"{(~(same | tie)).sum()} rays hit different triangles"
+    assert same.mean() > 0.999
