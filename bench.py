@@ -48,6 +48,12 @@ WORKLOADS = {
                             no_reference="the reference's materials are Blinn-Phong only (no GGX lobe)"),
 }
 WORKLOAD = WORKLOADS["soft_shadow"]
+# stages of the work model that run as several kernels
+COMPOSITE_STAGES = {
+    "k_primary_edges": ("k_primary_shade", "k_primary_grad"),
+    "k_edge_traverse": ("k_edge_expand", "k_edge_tasks"),  # the two-stage walk of large edge trees
+    "k_edge_eval": ("k_edge_line", "k_edge_rays", "k_edge_shade"),
+}
 # reference CPU arm: page-in / warm-up steps on a small slice of the same scene
 REF_RES = (32, 32)
 
@@ -308,9 +314,9 @@ def load_traffic(stage):
                     table[parts[0]] = int(parts[1])
     except (OSError, ValueError):
         return None
-    if stage == "k_edge_eval":
-        wave = ("k_edge_line", "k_edge_rays", "k_edge_shade")
-        return sum(table[k] for k in wave) if all(k in table for k in wave) else None
+    parts = COMPOSITE_STAGES.get(stage)
+    if parts:
+        return sum(table[k] for k in parts) if all(k in table for k in parts) else None
     return table.get(stage)
 
 
@@ -490,20 +496,15 @@ def run_b200(args):
         dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
     e2e_value = world * samples / float(e2e_t.item())
 
-    # roofline of the dominant stage; the edge-evaluation wavefront (line
-    # samples, their rays, shading of the rest) counts as one stage
+    # roofline of the dominant stage; a stage run as several kernels
+    # (COMPOSITE_STAGES) counts as one
     peak, peak_kind = load_peaks()
-    # and so does the two-stage traversal of large edge trees (k_edge_expand,
-    # then k_edge_tasks)
-    wave_names = ("k_edge_line", "k_edge_rays", "k_edge_shade")
-    split_names = ("k_edge_expand", "k_edge_tasks")
-    merged = [s_ for s_ in stages if s_[0] not in wave_names + split_names]
-    wave = [s_ for s_ in stages if s_[0] in wave_names]
-    split = [s_ for s_ in stages if s_[0] in split_names]
-    if wave:
-        merged.append(("k_edge_eval", sum(ms for _, ms in wave)))
-    if split:
-        merged.append(("k_edge_traverse", sum(ms for _, ms in split)))
+    parts_of = {k: name for name, parts in COMPOSITE_STAGES.items() for k in parts}
+    merged = {}
+    for name, ms in stages:
+        key = parts_of.get(name, name)
+        merged[key] = merged.get(key, 0.0) + ms
+    merged = list(merged.items())
     dom = max(merged, key=lambda s: s[1]) if merged else ("", 0.0)
     dom_bytes = stage_bytes(dom[0], wl, counts)
     achieved = dom_bytes / (dom[1] / 1e3) / 1e9 if dom[1] > 0 else 0.0

@@ -11,7 +11,9 @@
 //                      dv0/dv1 scatter and dp
 //   k_dp_propagate     one thread per point: the point's dp through its
 //                      triangle and the camera (reference "last edge" rule)
-//   k_primary_edges    one thread per primary-edge sample
+//   k_primary_shade    one thread per primary-edge sample: the two camera rays
+//                      beside the sampled edge point and their shades
+//   k_primary_grad     one thread per primary-edge sample: Jacobians, scatter
 // This file holds the path kernels and the stage sequencing; it is compiled
 // without FMA contraction, so that the first vertex of every path (which
 // decides which edges a shading point sees) has the bits of the reference's
@@ -143,10 +145,12 @@ cudaError_t dr_launch_backward_front(const DevScene &s, int W, int H, int spp, i
     *launches += 1;
     long long npe = primary_edge_samples > 0 ? primary_edge_samples : (long long)spp * W * H;
     if (s.num_prim_edges > 0 && npe > 0) {
-        cudaError_t e = dr_launch_primary_edges(s, W, H, spp, B, seed, d_image, npe, grad, cfg, num_sms, st);
+        // the edge-item queue is free until the traversal: it carries the
+        // primary samples' color differences (16 B each) between the two kernels
+        cudaError_t e = dr_launch_primary_edges(s, W, H, spp, B, seed, d_image, npe, grad, cfg,
+                                                reinterpret_cast<float4 *>(ws.items), ws.cap_items, num_sms, st,
+                                                launches, timer);
         if (e != cudaSuccess) return e;
-        timer->mark(st, "k_primary_edges");
-        *launches += 1;
     }
     if (!traverse) return cudaGetLastError();
     return dr_launch_edge_traverse(s, seed, ws, num_sms, st, launches, timer);

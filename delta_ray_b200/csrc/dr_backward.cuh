@@ -684,6 +684,19 @@ DEV void propagate_dp(const DevScene &s, const PointRecord &pt, int W, int H, in
     d_sample_primary(s.cam, sx, sy, d_o, d_d, g, 0);
 }
 
+// The gradients of one primary-edge sample.
+template <class G> DEV void scatter_primary(const DevScene &s, const PrimaryEdgeResult &pr, G &g) {
+    if (!pr.ok) return;
+    const DevShape &sh = s.shapes[pr.edge.shape];
+    g.add(sh.grad_v + 3 * pr.edge.v0 + 0, pr.dv0.x);
+    g.add(sh.grad_v + 3 * pr.edge.v0 + 1, pr.dv0.y);
+    g.add(sh.grad_v + 3 * pr.edge.v0 + 2, pr.dv0.z);
+    g.add(sh.grad_v + 3 * pr.edge.v1 + 0, pr.dv1.x);
+    g.add(sh.grad_v + 3 * pr.edge.v1 + 1, pr.dv1.y);
+    g.add(sh.grad_v + 3 * pr.edge.v1 + 2, pr.dv1.z);
+    for (int q = 0; q < 16; q++) g.add(16 + q, pr.dw2c[q]);
+}
+
 // Primary-edge sample i (delta_ray.cpp:1478-1522).
 template <int BMAX = 1 << 30, class G>
 DEV void primary_edge_item(const DevScene &s, long long i, int W, int H, int spp, int B, uint64_t seed,
@@ -699,13 +712,50 @@ DEV void primary_edge_item(const DevScene &s, long long i, int W, int H, int spp
     LightSample ls = draw_light(r);
     PrimaryEdgeResult pr;
     primary_edge_sample<BMAX>(s, es, s.prim_edges[id], ls, r, B, d_image, W, H, w / spp, pr);
-    if (!pr.ok) return;
-    const DevShape &sh = s.shapes[pr.edge.shape];
-    g.add(sh.grad_v + 3 * pr.edge.v0 + 0, pr.dv0.x);
-    g.add(sh.grad_v + 3 * pr.edge.v0 + 1, pr.dv0.y);
-    g.add(sh.grad_v + 3 * pr.edge.v0 + 2, pr.dv0.z);
-    g.add(sh.grad_v + 3 * pr.edge.v1 + 0, pr.dv1.x);
-    g.add(sh.grad_v + 3 * pr.edge.v1 + 1, pr.dv1.y);
-    g.add(sh.grad_v + 3 * pr.edge.v1 + 2, pr.dv1.z);
-    for (int q = 0; q < 16; q++) g.add(16 + q, pr.dw2c[q]);
+    scatter_primary(s, pr, g);
+}
+
+// The primary-edge sample i in two halves (k_primary_shade, k_primary_grad),
+// with the same draws and arithmetic as primary_edge_item.  The first returns
+// (rcol - lcol, 1), or w = 0 when the sample ends before its gradient.
+template <int BMAX>
+DEV float4 primary_shade_item(const DevScene &s, long long i, int B, uint64_t seed) {
+    float4 none;
+    none.x = none.y = none.z = none.w = 0.f;
+    if (s.num_prim_edges == 0) return none;
+    Rng r;
+    r.init(seed, kStreamPrimaryEdge, (uint64_t)i, 0);
+    float pmf = 0.f;
+    int id = sample_discrete(s.prim_cdf, s.prim_func, s.prim_func_int, s.num_prim_edges, r.next(), &pmf);
+    float w = pmf > 0.f ? 1.f / pmf : 0.f;
+    if (w <= 0.f) return none;
+    EdgeSample es = draw_edge(r);
+    LightSample ls = draw_light(r);
+    PrimaryGeom pg;
+    if (!primary_edge_geom(s.cam, s, es, s.prim_edges[id], pg)) return none;
+    float3 diff;
+    if (!primary_edge_colors<BMAX>(s, pg, s.prim_edges[id], ls, r, B, diff)) return none;
+    float4 c;
+    c.x = diff.x;
+    c.y = diff.y;
+    c.z = diff.z;
+    c.w = 1.f;
+    return c;
+}
+
+template <class G>
+DEV void primary_grad_item(const DevScene &s, long long i, int W, int H, int spp, uint64_t seed, const float *d_image,
+                           float4 c, G &g) {
+    if (c.w == 0.f) return;
+    Rng r;
+    r.init(seed, kStreamPrimaryEdge, (uint64_t)i, 0);
+    float pmf = 0.f;
+    int id = sample_discrete(s.prim_cdf, s.prim_func, s.prim_func_int, s.num_prim_edges, r.next(), &pmf);
+    float w = 1.f / pmf;
+    EdgeSample es = draw_edge(r);
+    PrimaryGeom pg;
+    primary_edge_geom(s.cam, s, es, s.prim_edges[id], pg);
+    PrimaryEdgeResult pr;
+    primary_edge_grad(s, pg, s.prim_edges[id], f3(c.x, c.y, c.z), d_image, W, H, w / spp, pr);
+    scatter_primary(s, pr, g);
 }

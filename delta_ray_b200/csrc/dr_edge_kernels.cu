@@ -272,15 +272,25 @@ __global__ void __launch_bounds__(128, 4) k_edge_shade(DevScene s, int W, int H,
     block_grad_flush(bg);
 }
 
+// Primary edges (delta_ray.cpp:1478-1522) in two kernels: k_primary_shade
+// samples the edge point and shades the camera rays on its two sides (the
+// code of a forward path), k_primary_grad redraws the sample and turns the
+// color difference into the scene and camera gradients.
 template <int BMAX>
-__global__ void __launch_bounds__(128, 3) k_primary_edges(DevScene s, int W, int H, int spp, int B, uint64_t seed,
-                                                       const float *d_image, long long n, float *grad,
-                                                       GradCacheCfg cfg) {
+__global__ void __launch_bounds__(128, 4) k_primary_shade(DevScene s, int B, uint64_t seed, long long i0, long long n,
+                                                       float4 *out) {
+    for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x)
+        out[k] = primary_shade_item<BMAX>(s, i0 + k, B, seed);
+}
+
+__global__ void __launch_bounds__(128, 4) k_primary_grad(DevScene s, int W, int H, int spp, uint64_t seed,
+                                                      const float *d_image, long long i0, long long n,
+                                                      const float4 *in, float *grad, GradCacheCfg cfg) {
     extern __shared__ float sm[];
     BlockGradWarp bg;
     static_cast<BlockGrad &>(bg) = block_grad_begin(sm, grad, cfg);
-    for (long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (long long)gridDim.x * blockDim.x)
-        primary_edge_item<BMAX>(s, i, W, H, spp, B, seed, d_image, bg);
+    for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x)
+        primary_grad_item(s, i0 + k, W, H, spp, seed, d_image, in[k], bg);
     block_grad_flush(bg);
 }
 
@@ -331,13 +341,23 @@ cudaError_t dr_launch_edge_eval(const DevScene &s, int W, int H, int spp, int B,
 
 cudaError_t dr_launch_primary_edges(const DevScene &s, int W, int H, int spp, int B, uint64_t seed,
                                     const float *d_image, long long n, float *grad, const GradCacheCfg &cfg,
-                                    int num_sms, cudaStream_t st) {
+                                    float4 *scratch, long long cap, int num_sms, cudaStream_t st, int *launches,
+                                    StageTimer *timer) {
     const int bs = 128;
     size_t smem = sizeof(float) * (size_t)(cfg.head + cfg.tail_len);
-    long long nb = std::min<long long>(blocks_for(n, bs), (long long)stage_grid(num_sms) * 4);
-    auto kernel = B == 1 ? k_primary_edges<1> : k_primary_edges<(1 << 30)>;
-    kernel<<<(int)nb, bs, smem, st>>>(s, W, H, spp, B, seed, d_image, n, grad, cfg);
-    return cudaGetLastError();
+    auto shade = B == 1 ? k_primary_shade<1> : k_primary_shade<(1 << 30)>;
+    for (long long i0 = 0; i0 < n; i0 += cap) {
+        long long m = std::min(cap, n - i0);
+        int nb = (int)std::min<long long>(blocks_for(m, bs), (long long)stage_grid(num_sms) * 4);
+        shade<<<nb, bs, 0, st>>>(s, B, seed, i0, m, scratch);
+        timer->mark(st, "k_primary_shade");
+        k_primary_grad<<<nb, bs, smem, st>>>(s, W, H, spp, seed, d_image, i0, m, scratch, grad, cfg);
+        timer->mark(st, "k_primary_grad");
+        *launches += 2;
+        cudaError_t e = cudaGetLastError();
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
 }
 
 // The learned proposal's inputs of each shading point: position normalised to

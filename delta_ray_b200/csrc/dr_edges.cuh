@@ -938,44 +938,59 @@ struct PrimaryEdgeResult {
     float dw2c[16];
 };
 
+// A primary-edge sample in three parts, so that the shading and the
+// Jacobians can run as separate kernels (k_primary_shade, k_primary_grad):
+// primary_edge_geom (the sample's point on the projected edge),
+// primary_edge_colors (the two camera rays beside it and their shades),
+// primary_edge_grad (Jacobians and the scene / camera gradients).
+struct PrimaryGeom {
+    float3 v0, v1, d0, d1, vd, ept3, split_n;
+    float2 s0, s1, ept;
+    float t, delta;
+};
+
+DEV bool primary_edge_geom(const DevCamera &cam, const DevScene &s, const EdgeSample &es, const DevEdge &edge,
+                           PrimaryGeom &g) {
+    g.v0 = edge_v0(s, edge);
+    g.v1 = edge_v1(s, edge);
+    if (!project(cam, g.v0, g.v1, g.s0, g.s1)) return false;
+    g.d0 = unproject(cam, g.s0.x, g.s0.y);
+    g.d1 = unproject(cam, g.s1.x, g.s1.y);
+    g.vd = g.d1 - g.d0;
+    g.t = es.u;
+    float3 l0 = xfm_point(cam.w2c, g.v0), l1 = xfm_point(cam.w2c, g.v1);
+    g.ept3 = g.d0 + g.t * g.vd;
+    float3 elocal = l0 + g.t * l1;  // as written in delta_ray.cpp:403
+    g.ept = project_local(cam, g.ept3);
+    if (!in_screen(cam, g.ept)) return false;
+    g.delta = 1e-4f * length(elocal);
+    g.split_n = normalize(cross(g.d0, g.d1));
+    return true;
+}
+
+// Screen point of the camera ray on side k (0: +split_n, 1: -split_n).
+DEV float2 primary_side_point(const DevCamera &cam, const PrimaryGeom &g, int k) {
+    float3 dir = normalize(k == 0 ? g.ept3 + g.delta * g.split_n : g.ept3 - g.delta * g.split_n);
+    return project_local(cam, dir);
+}
+
+// rcol - lcol of the two sides; false if neither side's ray hits a face of the edge.
 template <int BMAX = 1 << 30>
-DEV void primary_edge_sample(const DevScene &s, const EdgeSample &es, const DevEdge &edge, const LightSample &ls,
-                             const Rng &rng, int B, const float *d_image, int W, int H, float weight,
-                             PrimaryEdgeResult &r) {
-    r.ok = false;
+DEV bool primary_edge_colors(const DevScene &s, const PrimaryGeom &g, const DevEdge &edge, const LightSample &ls,
+                             const Rng &rng, int B, float3 &diff) {
     const DevCamera &cam = s.cam;
-    float3 v0 = edge_v0(s, edge), v1 = edge_v1(s, edge);
-    float2 s0, s1;
-    if (!project(cam, v0, v1, s0, s1)) return;
-    float3 d0 = unproject(cam, s0.x, s0.y), d1 = unproject(cam, s1.x, s1.y);
-    float3 vd = d1 - d0;
-    float t = es.u;
-    float3 l0 = xfm_point(cam.w2c, v0), l1 = xfm_point(cam.w2c, v1);
-    float3 ept3 = d0 + t * vd;
-    float3 elocal = l0 + t * l1;  // as written in delta_ray.cpp:403
-    float2 ept = project_local(cam, ept3);
-    if (!in_screen(cam, ept)) return;
-    int xi = int(ept.x * W), yi = int(ept.y * H);
-    const float *dc = d_image + 3 * ((size_t)yi * W + xi);
-    float3 d_color = f3(dr_ldg(dc), dr_ldg(dc + 1), dr_ldg(dc + 2));
-    float delta = 1e-4f * length(elocal);
-    float3 split_n = normalize(cross(d0, d1));
     // right side (+split_n) then left, through one copy of the code
-    float2 rpt, lpt;
     Ray rray, lray;
     Hit hr, hl;
 #pragma unroll 1
     for (int k = 0; k < 2; k++) {
-        float3 dir = normalize(k == 0 ? ept3 + delta * split_n : ept3 - delta * split_n);
-        float2 pt = project_local(cam, dir);
+        float2 pt = primary_side_point(cam, g, k);
         Ray ray = sample_primary(cam, pt.x, pt.y);
         Hit hh = trace_closest(s, ray.o, ray.d, 1e-3f);
         if (k == 0) {
-            rpt = pt;
             rray = ray;
             hr = hh;
         } else {
-            lpt = pt;
             lray = ray;
             hl = hh;
         }
@@ -984,7 +999,7 @@ DEV void primary_edge_sample(const DevScene &s, const EdgeSample &es, const DevE
               (s.tri_local[hr.tri] == edge.f0 || s.tri_local[hr.tri] == edge.f1);
     bool lc = hl.tri >= 0 && s.tri[hl.tri].w == edge.shape &&
               (s.tri_local[hl.tri] == edge.f0 || s.tri_local[hl.tri] == edge.f1);
-    if (!rc && !lc) return;
+    if (!rc && !lc) return false;
     float3 rcol = f3(0.f), lcol = f3(0.f);
 #pragma unroll 1
     for (int k = 0; k < 2; k++) {
@@ -996,7 +1011,24 @@ DEV void primary_edge_sample(const DevScene &s, const EdgeSample &es, const DevE
         if (k == 0) rcol = col;
         else lcol = col;
     }
-    float3 diff = (rcol - lcol) * weight;
+    diff = rcol - lcol;
+    return true;
+}
+
+// Jacobians of a sample whose sides' colors differ by `cdiff` (rcol - lcol),
+// scaled by `weight`; r.ok false if a perturbed end point leaves the view.
+DEV void primary_edge_grad(const DevScene &s, const PrimaryGeom &g, const DevEdge &edge, float3 cdiff,
+                           const float *d_image, int W, int H, float weight, PrimaryEdgeResult &r) {
+    r.ok = false;
+    const DevCamera &cam = s.cam;
+    const float3 v0 = g.v0, v1 = g.v1, d0 = g.d0, d1 = g.d1, vd = g.vd;
+    const float2 s0 = g.s0, s1 = g.s1, ept = g.ept;
+    const float t = g.t, delta = g.delta;
+    int xi = int(ept.x * W), yi = int(ept.y * H);
+    const float *dc = d_image + 3 * ((size_t)yi * W + xi);
+    float3 d_color = f3(dr_ldg(dc), dr_ldg(dc + 1), dr_ldg(dc + 2));
+    float2 rpt = primary_side_point(cam, g, 0), lpt = primary_side_point(cam, g, 1);
+    float3 diff = cdiff * weight;
     float3 xdiff = diff, ydiff = diff;
     if (lpt.x > rpt.x) xdiff = -xdiff;
     if (lpt.y > rpt.y) ydiff = -ydiff;
@@ -1042,4 +1074,17 @@ DEV void primary_edge_sample(const DevScene &s, const EdgeSample &es, const DevE
     r.dv1 = f3(dv1[0], dv1[1], dv1[2]);
     for (int i = 0; i < 16; i++) r.dw2c[i] = 0.f;
     d_project(cam, v0, v1, g0x, g0y, g1x, g1y, r.dw2c);
+}
+
+// The whole sample (delta_ray.cpp:377-557).
+template <int BMAX = 1 << 30>
+DEV void primary_edge_sample(const DevScene &s, const EdgeSample &es, const DevEdge &edge, const LightSample &ls,
+                             const Rng &rng, int B, const float *d_image, int W, int H, float weight,
+                             PrimaryEdgeResult &r) {
+    r.ok = false;
+    PrimaryGeom g;
+    if (!primary_edge_geom(s.cam, s, es, edge, g)) return;
+    float3 diff;
+    if (!primary_edge_colors<BMAX>(s, g, edge, ls, rng, B, diff)) return;
+    primary_edge_grad(s, g, edge, diff, d_image, W, H, weight, r);
 }

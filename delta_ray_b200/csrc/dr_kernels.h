@@ -120,9 +120,12 @@ cudaError_t dr_launch_accumulate(float *dst, const float *src, long long n, cuda
 cudaError_t dr_launch_edge_eval(const DevScene &s, int W, int H, int spp, int B, uint64_t seed, int dp_mode,
                                 float *grad, const BackwardWorkspace &ws, const GradCacheCfg &cfg, int num_sms,
                                 cudaStream_t st, int *launches, StageTimer *timer);
+// Primary edges as two kernels (k_primary_shade, k_primary_grad) that pass
+// each sample's color difference through `scratch` (cap samples at a time).
 cudaError_t dr_launch_primary_edges(const DevScene &s, int W, int H, int spp, int B, uint64_t seed,
                                     const float *d_image, long long n, float *grad, const GradCacheCfg &cfg,
-                                    int num_sms, cudaStream_t st);
+                                    float4 *scratch, long long cap, int num_sms, cudaStream_t st, int *launches,
+                                    StageTimer *timer);
 cudaError_t dr_launch_backward_back(const DevScene &s, int W, int H, int spp, int B, uint64_t seed, float *grad,
                                     int dp_mode, const BackwardWorkspace &ws, const GradCacheCfg &cfg, int num_sms,
                                     cudaStream_t st, int *launches, StageTimer *timer);
