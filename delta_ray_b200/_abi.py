@@ -5,7 +5,8 @@ package's scene objects (the reference's RenderFunction inputs,
 render_pytorch.py:13-55) into a ``dr_scene_desc`` whose pointers reference
 contiguous float32/int32 copies held by the returned object.  ``device`` is a
 torch.device: ``cpu`` keeps host copies (the library uploads them), a CUDA
-device keeps device copies.
+device keeps device copies, None leaves each array on its own tensor's device
+(converted to the descriptor's dtype where needed).
 """
 import ctypes as C
 
@@ -127,11 +128,13 @@ class SceneDesc:
         self.grad_sizes = []  # (kind, index, numel) in flat-layout order
 
     def _ptr(self, t, dtype, device):
+        """Pointer to t as a contiguous `dtype` array on `device` (None: on the
+        tensor's own device; the library reads host and device memory)."""
         if t is None:
             return None
         if not torch.is_tensor(t):
             t = torch.as_tensor(np.asarray(t))
-        t = t.detach().to(device=device, dtype=dtype).contiguous()
+        t = t.detach().to(device=t.device if device is None else device, dtype=dtype).contiguous()
         self.keep.append(t)
         ctype = C.c_float if dtype == torch.float32 else C.c_int
         return C.cast(C.c_void_p(t.data_ptr()), C.POINTER(ctype))

@@ -165,9 +165,10 @@ struct ProposalState {
 struct dr_scene {
     int device = 0;
     HostScene h;
-    DevBuf vtx, nrm, uv, tri, tri_local, bvh_nodes, bvh_tris, shapes, mats, texels, lights, light_sel_cdf,
-        light_sel_func, light_tri_cdf, light_tri_func, prim_edges, prim_cdf, prim_func, sil_nodes, sil_edges,
-        nrm_nodes, nrm_edges, status, bvh_scratch;
+    // the scene's arrays (geometry, materials, lights, samplers, edge trees,
+    // LBVH nodes) share one allocation; bvh_scratch keeps the LBVH topology
+    // that an update refits
+    DevBuf arena, bvh_scratch;
     std::shared_ptr<DevBuf> ltc, ltc_ggx;
     std::unique_ptr<BackwardQueues> queues;  // taken at the first backward call
     std::unique_ptr<ProposalState> proposal;  // set by dr_scene_set_proposal
@@ -190,6 +191,58 @@ struct dr_scene {
 
 namespace {
 
+// Host-side layout of the scene arena: each array at a 256-byte aligned
+// offset.  Arrays with a host source are packed into a pinned staging buffer
+// and reach the device in one copy.
+struct ArenaLayout {
+    struct Part {
+        const void *src;
+        size_t bytes, off;
+    };
+    std::vector<Part> parts;
+    size_t total = 0;
+    template <typename T> size_t add(const std::vector<T> &v) { return space(sizeof(T) * v.size(), v.data()); }
+    size_t space(size_t bytes, const void *src = nullptr) {
+        size_t off = total;
+        parts.push_back({src, bytes, off});
+        total += (std::max<size_t>(bytes, 16) + 255) & ~size_t(255);
+        return off;
+    }
+};
+
+// Pinned staging buffer of the arena uploads, one per process, grown on demand.
+struct Staging {
+    std::mutex m;
+    void *p = nullptr;
+    size_t bytes = 0;
+};
+Staging &staging() {
+    static Staging s;
+    return s;
+}
+
+void upload_arena(DevBuf &arena, const ArenaLayout &lay, cudaStream_t st) {
+    arena.reserve(lay.total);
+    Staging &sg = staging();
+    std::lock_guard<std::mutex> lk(sg.m);
+    if (sg.bytes < lay.total) {
+        if (sg.p) cudaFreeHost(sg.p);
+        sg.p = nullptr;
+        sg.bytes = 0;
+        check_cuda(cudaMallocHost(&sg.p, lay.total), "cudaMallocHost");
+        sg.bytes = lay.total;
+    }
+    size_t end = 0;  // bytes of the arena that carry host data
+    for (const auto &pt : lay.parts)
+        if (pt.src && pt.bytes) {
+            memcpy((char *)sg.p + pt.off, pt.src, pt.bytes);
+            end = std::max(end, pt.off + pt.bytes);
+        }
+    if (end) check_cuda(cudaMemcpyAsync(arena.p, sg.p, end, cudaMemcpyHostToDevice, st), "scene upload");
+    // the staging buffer is reused by the next upload
+    check_cuda(cudaStreamSynchronize(st), "scene upload");
+}
+
 void upload_scene(dr_scene *sc, cudaStream_t st, bool refit = false) {
     HostScene &h = sc->h;
     check_cuda(cudaSetDevice(sc->device), "cudaSetDevice");
@@ -199,47 +252,40 @@ void upload_scene(dr_scene *sc, cudaStream_t st, bool refit = false) {
     sc->lo = f.lo;
     sc->hi = f.hi;
     sc->num_tris = (int)f.tri.size();
-    sc->vtx.upload(f.vtx);
-    sc->nrm.upload(f.nrm);
-    sc->uv.upload(f.uv);
-    sc->tri.upload(f.tri);
-    sc->tri_local.upload(f.tri_local);
-    sc->shapes.upload(f.shapes);
-    sc->mats.upload(h.mats);
-    sc->texels.upload(h.texels);
-    sc->lights.upload(h.lights);
-    sc->light_sel_cdf.upload(h.light_sel.cdf);
-    sc->light_sel_func.upload(h.light_sel.func);
-    sc->light_tri_cdf.upload(h.light_tri_cdf);
-    sc->light_tri_func.upload(h.light_tri_func);
-    sc->prim_edges.upload(h.prim_edges);
-    sc->prim_cdf.upload(h.prim_dist.cdf);
-    sc->prim_func.upload(h.prim_dist.func);
-    sc->sil_nodes.upload(h.sil_nodes);
-    sc->sil_edges.upload(h.sil_edges);
-    sc->nrm_nodes.upload(h.nrm_nodes);
-    sc->nrm_edges.upload(h.nrm_edges);
+    const int n = sc->num_tris;
+    ArenaLayout lay;
+    const size_t o_vtx = lay.add(f.vtx), o_nrm = lay.add(f.nrm), o_uv = lay.add(f.uv), o_tri = lay.add(f.tri),
+                 o_tri_local = lay.add(f.tri_local), o_shapes = lay.add(f.shapes), o_mats = lay.add(h.mats),
+                 o_texels = lay.add(h.texels), o_lights = lay.add(h.lights),
+                 o_light_sel_cdf = lay.add(h.light_sel.cdf), o_light_sel_func = lay.add(h.light_sel.func),
+                 o_light_tri_cdf = lay.add(h.light_tri_cdf), o_light_tri_func = lay.add(h.light_tri_func),
+                 o_prim_edges = lay.add(h.prim_edges), o_prim_cdf = lay.add(h.prim_dist.cdf),
+                 o_prim_func = lay.add(h.prim_dist.func), o_sil_nodes = lay.add(h.sil_nodes),
+                 o_sil_edges = lay.add(h.sil_edges), o_nrm_nodes = lay.add(h.nrm_nodes),
+                 o_nrm_edges = lay.add(h.nrm_edges);
+    // LBVH nodes and leaves: written by the build / refit kernels
+    const size_t o_bvh_nodes = lay.space(sizeof(float4) * 4 * (size_t)std::max(1, n - 1));
+    const size_t o_bvh_tris = lay.space(sizeof(float4) * 3 * (size_t)std::max(1, n));
+    upload_arena(sc->arena, lay, st);
+    char *base = (char *)sc->arena.p;
     sc->ltc = device_ltc(sc->device, 0, h.ltc);
     sc->ltc_ggx = device_ltc(sc->device, 1, h.ltc_ggx);
-    sc->status.reserve(sizeof(int) * 4);
+    float *vtx = (float *)(base + o_vtx);
+    int4 *tri = (int4 *)(base + o_tri);
+    float4 *bvh_nodes = (float4 *)(base + o_bvh_nodes), *bvh_tris = (float4 *)(base + o_bvh_tris);
     // device LBVH
-    int n = sc->num_tris;
-    sc->bvh_nodes.reserve(sizeof(float4) * 4 * (size_t)std::max(1, n - 1));
-    sc->bvh_tris.reserve(sizeof(float4) * 3 * (size_t)std::max(1, n));
     if (n > 0) {
         // the build's working arrays stay with the scene: an update with new
         // vertex positions refits the same tree (closest hits do not depend on
         // the tree's shape, ties going to the lower triangle id)
         size_t sb = dr_lbvh_scratch_bytes(n);
         if (refit && sc->bvh_built_tris == n && sc->bvh_scratch.bytes >= sb) {
-            check_cuda(dr_refit_lbvh(sc->vtx.as<float>(), sc->tri.as<int4>(), n, sc->bvh_nodes.as<float4>(),
-                                     sc->bvh_tris.as<float4>(), sc->bvh_scratch.p, sc->bvh_scratch.bytes, st,
+            check_cuda(dr_refit_lbvh(vtx, tri, n, bvh_nodes, bvh_tris, sc->bvh_scratch.p, sc->bvh_scratch.bytes, st,
                                      &sc->last_launches),
                        "LBVH refit");
         } else {
             sc->bvh_scratch.reserve(sb);
-            check_cuda(dr_build_lbvh(sc->vtx.as<float>(), sc->tri.as<int4>(), n, f.lo, f.hi,
-                                     sc->bvh_nodes.as<float4>(), sc->bvh_tris.as<float4>(), sc->bvh_scratch.p,
+            check_cuda(dr_build_lbvh(vtx, tri, n, f.lo, f.hi, bvh_nodes, bvh_tris, sc->bvh_scratch.p,
                                      sc->bvh_scratch.bytes, st, &sc->last_launches),
                        "LBVH build");
             sc->bvh_built_tris = n;
@@ -247,28 +293,28 @@ void upload_scene(dr_scene *sc, cudaStream_t st, bool refit = false) {
         check_cuda(cudaStreamSynchronize(st), "LBVH build");
     }
     ScenePtrs ptr;
-    ptr.vtx = sc->vtx.as<float>();
-    ptr.nrm = sc->nrm.as<float>();
-    ptr.uv = sc->uv.as<float>();
-    ptr.tri = sc->tri.as<int4>();
-    ptr.tri_local = sc->tri_local.as<int>();
-    ptr.bvh_nodes = sc->bvh_nodes.as<float4>();
-    ptr.bvh_tris = sc->bvh_tris.as<float4>();
-    ptr.shapes = sc->shapes.as<DevShape>();
-    ptr.mats = sc->mats.as<DevMaterial>();
-    ptr.texels = sc->texels.as<float>();
-    ptr.lights = sc->lights.as<DevLight>();
-    ptr.light_sel_cdf = sc->light_sel_cdf.as<float>();
-    ptr.light_sel_func = sc->light_sel_func.as<float>();
-    ptr.light_tri_cdf = sc->light_tri_cdf.as<float>();
-    ptr.light_tri_func = sc->light_tri_func.as<float>();
-    ptr.prim_edges = sc->prim_edges.as<DevEdge>();
-    ptr.prim_cdf = sc->prim_cdf.as<float>();
-    ptr.prim_func = sc->prim_func.as<float>();
-    ptr.sil_nodes = sc->sil_nodes.as<DevEdgeNode>();
-    ptr.sil_edges = sc->sil_edges.as<DevEdge>();
-    ptr.nrm_nodes = sc->nrm_nodes.as<DevEdgeNode>();
-    ptr.nrm_edges = sc->nrm_edges.as<DevEdge>();
+    ptr.vtx = vtx;
+    ptr.nrm = (float *)(base + o_nrm);
+    ptr.uv = (float *)(base + o_uv);
+    ptr.tri = tri;
+    ptr.tri_local = (int *)(base + o_tri_local);
+    ptr.bvh_nodes = bvh_nodes;
+    ptr.bvh_tris = bvh_tris;
+    ptr.shapes = (DevShape *)(base + o_shapes);
+    ptr.mats = (DevMaterial *)(base + o_mats);
+    ptr.texels = (float *)(base + o_texels);
+    ptr.lights = (DevLight *)(base + o_lights);
+    ptr.light_sel_cdf = (float *)(base + o_light_sel_cdf);
+    ptr.light_sel_func = (float *)(base + o_light_sel_func);
+    ptr.light_tri_cdf = (float *)(base + o_light_tri_cdf);
+    ptr.light_tri_func = (float *)(base + o_light_tri_func);
+    ptr.prim_edges = (DevEdge *)(base + o_prim_edges);
+    ptr.prim_cdf = (float *)(base + o_prim_cdf);
+    ptr.prim_func = (float *)(base + o_prim_func);
+    ptr.sil_nodes = (DevEdgeNode *)(base + o_sil_nodes);
+    ptr.sil_edges = (DevEdge *)(base + o_sil_edges);
+    ptr.nrm_nodes = (DevEdgeNode *)(base + o_nrm_nodes);
+    ptr.nrm_edges = (DevEdge *)(base + o_nrm_edges);
     ptr.ltc = sc->ltc->as<float>();
     ptr.ltc_ggx = sc->ltc_ggx->as<float>();
     fill_devscene(sc->ds, h, f, ptr);

@@ -66,13 +66,18 @@ class RenderOptions:
         self.device = device
 
 
+_FITTED = {}  # model -> the committed fitted LTC table (read once; the library copies it)
+
+
 def _table(t, model):
     """An LTC table argument: "fitted" -> the committed fit of `model`, None -> None."""
     if isinstance(t, str):
         if t != "fitted":
             raise ValueError(f"unknown LTC table {t!r}")
-        from . import ltc
-        return torch.from_numpy(ltc.default_table(model))
+        if model not in _FITTED:
+            from . import ltc
+            _FITTED[model] = torch.from_numpy(ltc.default_table(model))
+        return _FITTED[model]
     return t
 
 
@@ -87,7 +92,9 @@ class Scene:
         self.device = torch.device("cuda", self.device_index)
         self.materials = materials
         self.shapes = shapes
-        self.sd = _abi.SceneDesc.from_scene(cam, materials, shapes, lights, self.device, ltc_table, ltc_table_ggx)
+        # the description is read where it lies (host or device); the library
+        # keeps its own copies, so no tensor is moved for it
+        self.sd = _abi.SceneDesc.from_scene(cam, materials, shapes, lights, None, ltc_table, ltc_table_ggx)
         handle = C.c_void_p()
         with torch.cuda.device(self.device_index):
             torch.cuda.current_stream().synchronize()
@@ -107,7 +114,7 @@ class Scene:
         t0 = self._tables[0] if isinstance(ltc_table, str) and ltc_table == "keep" else _table(ltc_table, 0)
         t1 = self._tables[1] if isinstance(ltc_table_ggx, str) and ltc_table_ggx == "keep" else _table(ltc_table_ggx, 1)
         self._tables = (t0, t1)
-        sd = _abi.SceneDesc.from_scene(cam, materials, shapes, lights, self.device, t0, t1)
+        sd = _abi.SceneDesc.from_scene(cam, materials, shapes, lights, None, t0, t1)
         with torch.cuda.device(self.device_index):
             torch.cuda.current_stream().synchronize()
             _lib.check(_lib.lib().dr_scene_update(self.handle, C.byref(sd.desc)))
@@ -321,6 +328,11 @@ class RenderFunction(torch.autograd.Function):
         W, H, spp, B, seed, opts = ctx.render
         scene = ctx.scene
         flat, _ = scene.backward(W, H, spp, B, seed, grad_img, opts)
+        # inputs all on one device (the host, typically): one copy of the flat
+        # gradient there, then views of it
+        devs = {d for d in ctx.arg_devices if d is not None}
+        if len(devs) == 1:
+            flat = flat.to(devs.pop())
         g = scene.split_grad(flat)
         nm, ns, nl = ctx.counts
         out = [None, None, None, None]  # seed, num_materials, num_shapes, num_lights
