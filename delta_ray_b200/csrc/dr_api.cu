@@ -263,9 +263,26 @@ void upload_scene(dr_scene *sc, cudaStream_t st, bool refit = false) {
                  o_prim_func = lay.add(h.prim_dist.func), o_sil_nodes = lay.add(h.sil_nodes),
                  o_sil_edges = lay.add(h.sil_edges), o_nrm_nodes = lay.add(h.nrm_nodes),
                  o_nrm_edges = lay.add(h.nrm_edges);
-    // LBVH nodes and leaves: written by the build / refit kernels
+    // LBVH nodes and leaves: written by the build / refit kernels, except for
+    // scenes traced without the tree, whose leaves (triangle order) come from here
+    std::vector<float4> leaves;
+    const bool linear = n > 0 && n <= DR_LINEAR_TRIS;
+    if (linear) {
+        leaves.resize(3 * (size_t)n);
+        for (int t = 0; t < n; t++) {
+            const int4 id = f.tri[t];
+            const int v[3] = {id.x, id.y, id.z};
+            for (int k = 0; k < 3; k++) {
+                float4 &q = leaves[3 * t + k];
+                q.x = f.vtx[3 * v[k]];
+                q.y = f.vtx[3 * v[k] + 1];
+                q.z = f.vtx[3 * v[k] + 2];
+                q.w = k == 0 ? dr_i2f(t) : 0.f;
+            }
+        }
+    }
     const size_t o_bvh_nodes = lay.space(sizeof(float4) * 4 * (size_t)std::max(1, n - 1));
-    const size_t o_bvh_tris = lay.space(sizeof(float4) * 3 * (size_t)std::max(1, n));
+    const size_t o_bvh_tris = linear ? lay.add(leaves) : lay.space(sizeof(float4) * 3 * (size_t)std::max(1, n));
     upload_arena(sc->arena, lay, st);
     char *base = (char *)sc->arena.p;
     sc->ltc = device_ltc(sc->device, 0, h.ltc);
@@ -274,7 +291,7 @@ void upload_scene(dr_scene *sc, cudaStream_t st, bool refit = false) {
     int4 *tri = (int4 *)(base + o_tri);
     float4 *bvh_nodes = (float4 *)(base + o_bvh_nodes), *bvh_tris = (float4 *)(base + o_bvh_tris);
     // device LBVH
-    if (n > 0) {
+    if (n > 0 && !linear) {
         // the build's working arrays stay with the scene: an update with new
         // vertex positions refits the same tree (closest hits do not depend on
         // the tree's shape, ties going to the lower triangle id)

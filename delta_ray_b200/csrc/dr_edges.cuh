@@ -252,7 +252,8 @@ DEV float node_dir_weight(const uint16_t *q, const Frame &f, float3 p, const Dev
     return bf16_bits_to_float(q[dir_bin(f, c - p)]);
 }
 
-// Stochastic traversal of one edge tree in one mode (edge_tree.cpp:511-652).
+// Stochastic traversal of one edge tree in one mode (edge_tree.cpp:511-652):
+// CONE true for the cone mode, false for the all mode.
 // emit(tree_edge_index, weight, slot_code) is called for every silhouette
 // edge of every reached leaf, in the reference's order.  Returns false if the
 // stack limit was hit (never for trees of depth < DR_EDGE_STACK).
@@ -286,8 +287,9 @@ template <bool PROP> HD EdgeItem<PROP> edge_item(int node, float bb, float c, fl
 // CUT > 0: interior nodes at depth CUT below the start are handed to
 // defer(node, bb, cpmf, apmf, lpmf) instead of being walked (inside the walk
 // an item's node field carries its depth in bits 27..31).
-template <bool CONE, bool PROP, int CUT = 0, class Emit, class Defer>
-DEV bool traverse_mode(const DevScene &s, const DevEdgeNode *nodes, const DevEdge *edges, bool dir_bounds, float3 wi,
+template <bool PROP, int CUT = 0, class Emit, class Defer>
+DEV bool traverse_mode(const bool CONE, const DevScene &s, const DevEdgeNode *nodes, const DevEdge *edges,
+                       bool dir_bounds, float3 wi,
                        const SurfacePoint &sp, float dl, float sl, float rough, int model, const ConeSpec &cone,
                        const EdgeTask &start, const NodeRng &rng, Emit &emit, const EdgeProposal &pr, int tree,
                        bool learned, Defer &defer) {
@@ -439,13 +441,18 @@ DEV bool traverse_edges(const DevScene &s, float3 wi, int stri, const SurfacePoi
     root.code = 0;
     root.bb = b;
     root.cpmf = root.apmf = root.lpmf = pmf;
-    auto dc = [&](int node, float bb, float c, float a, float l) { defer(node | (tree << 29), bb, c, a, l); };
-    bool ok = traverse_mode<true, PROP, CUT>(s, nodes, edges, tree == 1, wi, sp, dl, sl, rough, m.model, cone, root,
-                                             nrng, em, pr, tree, false, dc);
-    bool learned = PROP ? nrng.draw(1, DR_NODE_MIX_DRAW) < pr.alpha : false;
-    auto da = [&](int node, float bb, float c, float a, float l) { defer(node | (tree << 29) | (1 << 30), bb, c, a, l); };
-    ok &= traverse_mode<false, PROP, CUT>(s, nodes, edges, tree == 1, wi, sp, dl, sl, rough, m.model, cone, root, nrng,
-                                          em, pr, tree, learned, da);
+    // cone mode, then all mode, through one copy of the walk (a loop, not
+    // unrolled: the walk's code is the kernel's hot loop)
+    bool ok = true;
+#pragma unroll 1
+    for (int mode = 0; mode < 2; mode++) {
+        bool learned = PROP && mode == 1 ? nrng.draw(1, DR_NODE_MIX_DRAW) < pr.alpha : false;
+        auto dc = [&](int node, float bb, float c, float a, float l) {
+            defer(node | (tree << 29) | (mode << 30), bb, c, a, l);
+        };
+        ok &= traverse_mode<PROP, CUT>(mode == 0, s, nodes, edges, tree == 1, wi, sp, dl, sl, rough, m.model, cone,
+                                       root, nrng, em, pr, tree, learned, dc);
+    }
     return ok;
 }
 
@@ -464,12 +471,9 @@ DEV bool traverse_subtree(const DevScene &s, float3 wi, int stri, const SurfaceP
     NoDefer nd;
     EdgeTask start = task;
     start.code = task.code & DR_NODE_MASK;  // depth bits cleared: walked to the leaves
-    if (mode == 0)
-        return traverse_mode<true, PROP>(s, nodes, edges, tree == 1, wi, sp, dl, sl, rough, m.model, cone, start,
-                                         nrng, em, pr, tree, false, nd);
-    bool learned = PROP ? nrng.draw(1, DR_NODE_MIX_DRAW) < pr.alpha : false;
-    return traverse_mode<false, PROP>(s, nodes, edges, tree == 1, wi, sp, dl, sl, rough, m.model, cone, start, nrng,
-                                      em, pr, tree, learned, nd);
+    bool learned = PROP && mode == 1 ? nrng.draw(1, DR_NODE_MIX_DRAW) < pr.alpha : false;
+    return traverse_mode<PROP>(mode == 0, s, nodes, edges, tree == 1, wi, sp, dl, sl, rough, m.model, cone, start,
+                               nrng, em, pr, tree, learned, nd);
 }
 
 // LTC matrix lookup (material.h:464-476): nearest entry of the 128x128 table

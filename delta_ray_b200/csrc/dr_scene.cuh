@@ -60,6 +60,11 @@ struct DevEdgeNode {
 // a pixel sample hands at most DR_MAX_LINKS + 1 points to edge sampling.
 #define DR_MAX_LINKS 8
 
+// Scenes of at most DR_LINEAR_TRIS triangles are traced by testing every
+// triangle (dr_trace.cuh); they need the LBVH's leaf array only, which the
+// host fills in triangle order.
+#define DR_LINEAR_TRIS 16
+
 // A subtree of a point's edge-tree traversal, to be walked on its own (the
 // node-keyed draws make its result independent of who walks it and when):
 // the point, node | tree << 29 | mode << 30, the node's bound and the three

@@ -139,7 +139,6 @@ DEV_NOINLINE Hit trace_closest_bvh(const float4 *DR_RESTRICT nodes, const float4
 // ways keep the smallest t, ties going to the smaller triangle id, so they
 // agree unless the walk's widened box test (2 gamma(3)) rounds a hit lying
 // within ~1e-6 of the closest one out of its box.
-#define DR_LINEAR_TRIS 16
 
 DEV_NOINLINE Hit trace_closest_linear(const float4 *DR_RESTRICT tris, int n, float3 o, float3 d, float tnear) {
     Hit h;
