@@ -68,7 +68,7 @@ __device__ __forceinline__ EdgeProposal point_proposal(const BackwardWorkspace &
 // One thread per shading point in [pt_begin, pt_end) walks the point's trees
 // (small trees: every point's walk is short).
 template <bool PROP>
-__global__ void __launch_bounds__(128, 4) k_edge_traverse(DevScene s, uint64_t seed, BackwardWorkspace ws) {
+__global__ void __launch_bounds__(128, 6) k_edge_traverse(DevScene s, uint64_t seed, BackwardWorkspace ws) {
     long long n = min(min((long long)ws.counters->points, ws.cap_points), ws.pt_end);
     long long stride = (long long)gridDim.x * blockDim.x;
     ItemWriter out(ws);
@@ -133,7 +133,7 @@ __global__ void __launch_bounds__(128, 4) k_edge_expand(DevScene s, uint64_t see
 
 // Large trees, second stage: one thread per handed-on subtree.
 template <bool PROP>
-__global__ void __launch_bounds__(128, 4) k_edge_tasks(DevScene s, uint64_t seed, BackwardWorkspace ws) {
+__global__ void __launch_bounds__(128, 6) k_edge_tasks(DevScene s, uint64_t seed, BackwardWorkspace ws) {
     long long n = (long long)min(ws.counters->tasks, (unsigned long long)ws.cap_tasks);
     long long stride = (long long)gridDim.x * blockDim.x;
     ItemWriter out(ws);

@@ -675,16 +675,22 @@ DEV bool edge_rays(const DevScene &s, const EdgeLine &el, const DevEdge &edge, i
     edge_side_dirs(el, edge_v0(s, edge), edge_v1(s, edge), p, sdir, rdir, ldir);
     int hit[2];
     bool conn[2];
-    // both sides through one copy of the trace code: a loop, not unrolled
+    if (s.num_tris > 0 && s.num_tris <= DR_LINEAR_TRIS) {
+        Hit h0, h1;
+        trace_closest_pair_linear(s.bvh_tris, s.num_tris, p, rdir, ldir, 1e-3f, h0, h1);
+        hit[0] = h0.tri;
+        hit[1] = h1.tri;
+    } else {
+        // both sides through one copy of the trace code: a loop, not unrolled
+#pragma unroll 1
+        for (int k = 0; k < 2; k++) hit[k] = trace_closest(s, p, k == 0 ? rdir : ldir, 1e-3f).tri;
+    }
 #pragma unroll 1
     for (int k = 0; k < 2; k++) {
-        float3 dir = k == 0 ? rdir : ldir;
-        Hit hh = trace_closest(s, p, dir, 1e-3f);
-        hit[k] = hh.tri;
         conn[k] = false;
-        if (hh.tri >= 0) {
-            int lt = s.tri_local[hh.tri];
-            conn[k] = s.tri[hh.tri].w == edge.shape && (lt == edge.f0 || lt == edge.f1);
+        if (hit[k] >= 0) {
+            int lt = s.tri_local[hit[k]];
+            conn[k] = s.tri[hit[k]].w == edge.shape && (lt == edge.f0 || lt == edge.f1);
         }
     }
     if (conn[0] == conn[1] || (hit[0] >= 0 && hit[0] == stri) || (hit[1] >= 0 && hit[1] == stri)) return false;

@@ -39,10 +39,21 @@ extern thread_local long long g_dr_visits;
 
 // Moller-Trumbore with no contraction: the exact operation sequence of the
 // oracle's hit test.  Returns false on a miss.
-DEV bool hit_triangle(float4 a, float4 b, float4 c, float3 o, float3 d, float &t_out) {
-    float e1x = fsub_rn(b.x, a.x), e1y = fsub_rn(b.y, a.y), e1z = fsub_rn(b.z, a.z);
-    float e2x = fsub_rn(c.x, a.x), e2y = fsub_rn(c.y, a.y), e2z = fsub_rn(c.z, a.z);
-    float sx = fsub_rn(o.x, a.x), sy = fsub_rn(o.y, a.y), sz = fsub_rn(o.z, a.z);
+// The triangle's edge vectors e1 = b - a, e2 = c - a and the origin offset
+// s = o - a, which rays from one origin share.
+struct TriRay {
+    float e1x, e1y, e1z, e2x, e2y, e2z, sx, sy, sz;
+};
+DEV TriRay tri_ray(float4 a, float4 b, float4 c, float3 o) {
+    TriRay r;
+    r.e1x = fsub_rn(b.x, a.x), r.e1y = fsub_rn(b.y, a.y), r.e1z = fsub_rn(b.z, a.z);
+    r.e2x = fsub_rn(c.x, a.x), r.e2y = fsub_rn(c.y, a.y), r.e2z = fsub_rn(c.z, a.z);
+    r.sx = fsub_rn(o.x, a.x), r.sy = fsub_rn(o.y, a.y), r.sz = fsub_rn(o.z, a.z);
+    return r;
+}
+DEV bool hit_triangle(const TriRay &r, float3 d, float &t_out) {
+    const float e1x = r.e1x, e1y = r.e1y, e1z = r.e1z, e2x = r.e2x, e2y = r.e2y, e2z = r.e2z;
+    const float sx = r.sx, sy = r.sy, sz = r.sz;
     float px = fsub_rn(fmul_rn(d.y, e2z), fmul_rn(d.z, e2y));
     float py = fsub_rn(fmul_rn(d.z, e2x), fmul_rn(d.x, e2z));
     float pz = fsub_rn(fmul_rn(d.x, e2y), fmul_rn(d.y, e2x));
@@ -58,6 +69,9 @@ DEV bool hit_triangle(float4 a, float4 b, float4 c, float3 o, float3 d, float &t
     if (v < 0.f || fadd_rn(u, v) > 1.f) return false;
     t_out = fmul_rn(fadd_rn(fadd_rn(fmul_rn(e2x, qx), fmul_rn(e2y, qy)), fmul_rn(e2z, qz)), inv);
     return true;
+}
+DEV bool hit_triangle(float4 a, float4 b, float4 c, float3 o, float3 d, float &t_out) {
+    return hit_triangle(tri_ray(a, b, c, o), d, t_out);
 }
 
 HD float safe_inv(float x) {
@@ -156,6 +170,28 @@ DEV_NOINLINE Hit trace_closest_linear(const float4 *DR_RESTRICT tris, int n, flo
         }
     }
     return h;
+}
+
+// Closest hits of two rays from one origin (the two sides of an edge sample)
+// by testing every triangle; each triangle's tri_ray serves both rays.
+DEV_NOINLINE void trace_closest_pair_linear(const float4 *DR_RESTRICT tris, int n, float3 o, float3 d0, float3 d1,
+                                            float tnear, Hit &h0, Hit &h1) {
+    h0.tri = h1.tri = -1;
+    h0.t = h1.t = DR_INF;
+    for (int i = 0; i < n; i++) {
+        float4 a = dr_ldg(tris + 3 * i), b = dr_ldg(tris + 3 * i + 1), c = dr_ldg(tris + 3 * i + 2);
+        TriRay r = tri_ray(a, b, c, o);
+        int id = dr_f2i(a.w);
+        float t;
+        if (hit_triangle(r, d0, t) && t > tnear && (t < h0.t || (t == h0.t && id < h0.tri))) {
+            h0.t = t;
+            h0.tri = id;
+        }
+        if (hit_triangle(r, d1, t) && t > tnear && (t < h1.t || (t == h1.t && id < h1.tri))) {
+            h1.t = t;
+            h1.tri = id;
+        }
+    }
 }
 
 DEV Hit trace_closest(const DevScene &s, float3 o, float3 d, float tnear) {
