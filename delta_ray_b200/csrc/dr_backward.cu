@@ -28,7 +28,7 @@
 #include "dr_block_grad.cuh"
 
 template <bool kChains, int BMAX>
-__global__ void __launch_bounds__(128, 5) k_backward_paths(DevScene s, int W, int H, int spp, int B, uint64_t seed,
+__global__ void __launch_bounds__(128, 6) k_backward_paths(DevScene s, int W, int H, int spp, int B, uint64_t seed,
                                                         int lanes_log2, const float *d_image, float *grad, float *img,
                                                         BackwardWorkspace ws, GradCacheCfg cfg) {
     extern __shared__ float sm[];
@@ -88,7 +88,7 @@ __global__ void __launch_bounds__(128, 5) k_backward_paths(DevScene s, int W, in
 // chains only): the dp sums k_edge_shade accumulated for points after the first
 // vertex, whose chains are traced again here, in this IEEE compile unit.
 template <bool kChains>
-__global__ void __launch_bounds__(128) k_dp_propagate(DevScene s, int W, int H, int spp, uint64_t seed, int dp_mode,
+__global__ void __launch_bounds__(128, 6) k_dp_propagate(DevScene s, int W, int H, int spp, uint64_t seed, int dp_mode,
                                                       float *grad, BackwardWorkspace ws, GradCacheCfg cfg) {
     extern __shared__ float sm[];
     BlockGradWarp bg;

@@ -277,13 +277,13 @@ __global__ void __launch_bounds__(128, 4) k_edge_shade(DevScene s, int W, int H,
 // code of a forward path), k_primary_grad redraws the sample and turns the
 // color difference into the scene and camera gradients.
 template <int BMAX>
-__global__ void __launch_bounds__(128, 5) k_primary_shade(DevScene s, int B, uint64_t seed, long long i0, long long n,
+__global__ void __launch_bounds__(128, 6) k_primary_shade(DevScene s, int B, uint64_t seed, long long i0, long long n,
                                                        float4 *out) {
     for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x)
         out[k] = primary_shade_item<BMAX>(s, i0 + k, B, seed);
 }
 
-__global__ void __launch_bounds__(128, 6) k_primary_grad(DevScene s, int W, int H, int spp, uint64_t seed,
+__global__ void __launch_bounds__(128, 8) k_primary_grad(DevScene s, int W, int H, int spp, uint64_t seed,
                                                       const float *d_image, long long i0, long long n,
                                                       const float4 *in, float *grad, GradCacheCfg cfg) {
     extern __shared__ float sm[];
