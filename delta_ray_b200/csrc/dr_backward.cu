@@ -28,7 +28,7 @@
 #include "dr_block_grad.cuh"
 
 template <bool kChains, int BMAX>
-__global__ void __launch_bounds__(128, 7) k_backward_paths(DevScene s, int W, int H, int spp, int B, uint64_t seed,
+__global__ void __launch_bounds__(128, 8) k_backward_paths(DevScene s, int W, int H, int spp, int B, uint64_t seed,
                                                         int lanes_log2, const float *d_image, float *grad, float *img,
                                                         BackwardWorkspace ws, GradCacheCfg cfg) {
     extern __shared__ float sm[];

@@ -183,7 +183,7 @@ cudaError_t dr_launch_trace(const DevScene &s, const float *rays, long long n, i
 // Forward render: one pixel sample per (pixel, lane) and a segmented warp
 // reduction over the 2^lanes_log2 lanes of a pixel.
 // ---------------------------------------------------------------------------
-__global__ void __launch_bounds__(256, 3) k_render_forward(DevScene s, int W, int H, int spp, int B, uint64_t seed,
+__global__ void __launch_bounds__(256, 4) k_render_forward(DevScene s, int W, int H, int spp, int B, uint64_t seed,
                                                         int lanes_log2, float *img) {
     long long gid = (long long)blockIdx.x * blockDim.x + threadIdx.x;
     int G = 1 << lanes_log2;
