@@ -243,6 +243,42 @@ __global__ void __launch_bounds__(128, 4) k_edge_rays(DevScene s, BackwardWorksp
     }
 }
 
+// Scenes traced by testing every triangle (at most DR_LINEAR_TRIS): the rays
+// are cheap, so the line sample and its rays run in one kernel without the
+// survivor queue in between; a kept sample's survivor and hit records go to
+// one slot (hits[slot].x = slot), which k_edge_shade reads as it does the
+// records of k_edge_rays.
+template <bool EXT, bool DIRECT>
+__global__ void __launch_bounds__(128, 4) k_edge_line_rays(DevScene s, uint64_t seed, BackwardWorkspace ws) {
+    long long n = (long long)min(ws.counters->items, (unsigned long long)ws.cap_items);
+    long long stride = (long long)gridDim.x * blockDim.x;
+    // warp-uniform loop: the append is warp-aggregated
+    for (long long base = (long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < n; base += stride) {
+        long long i = base + (threadIdx.x & 31);
+        EdgeLine el;
+        EdgeHits eh;
+        bool ok = false;
+        if (i < n) {
+            int4 it = ws.items[i];
+            PointRecord pt;
+            pt.load(ws.pt + (size_t)it.x * DR_PT_WORDS);
+            int tree = it.y >> 30, ei = it.y & ((1 << 30) - 1);
+            ok = item_line<EXT>(s, pt, tree, ei, seed, el);
+            if (ok) {
+                const DevEdge &edge = tree ? s.nrm_edges[ei] : s.sil_edges[ei];
+                ok = edge_rays(s, el, edge, pt.tri, pt.p, DIRECT, eh);
+            }
+        }
+        __syncwarp();
+        unsigned long long slot = warp_reserve(&ws.counters->hits, ok ? 1 : 0);
+        if (ok) {
+            ws.survivors[2 * slot] = make_float4(__int_as_float((int)i), el.sample_p.x, el.sample_p.y, el.sample_p.z);
+            ws.survivors[2 * slot + 1] = make_float4(el.mwt.x, el.mwt.y, el.mwt.z, el.q);
+            ws.hits[slot] = make_int4((int)slot, eh.r, eh.l, 0);
+        }
+    }
+}
+
 template <bool EXT, bool GI>
 __global__ void __launch_bounds__(128, 4) k_edge_shade(DevScene s, int W, int H, int spp, int B, uint64_t seed,
                                                     int dp_mode, float *grad, BackwardWorkspace ws, GradCacheCfg cfg) {
@@ -325,12 +361,20 @@ cudaError_t dr_launch_edge_eval(const DevScene &s, int W, int H, int spp, int B,
     // the survivor and hit counters (adjacent)
     cudaError_t e = cudaMemsetAsync(&ws.counters->survivors, 0, 2 * sizeof(unsigned long long), st);
     if (e != cudaSuccess) return e;
-    if (ext) k_edge_line<true><<<grid, 128, 0, st>>>(s, seed, ws);
-    else k_edge_line<false><<<grid, 128, 0, st>>>(s, seed, ws);
-    timer->mark(st, "k_edge_line");
-    if (B > 1) k_edge_rays<false><<<grid, 128, 0, st>>>(s, ws);
-    else k_edge_rays<true><<<grid, 128, 0, st>>>(s, ws);
-    timer->mark(st, "k_edge_rays");
+    if (s.num_tris <= DR_LINEAR_TRIS) {
+        auto line_rays = ext ? (B > 1 ? k_edge_line_rays<true, false> : k_edge_line_rays<true, true>)
+                             : (B > 1 ? k_edge_line_rays<false, false> : k_edge_line_rays<false, true>);
+        line_rays<<<grid, 128, 0, st>>>(s, seed, ws);
+        timer->mark(st, "k_edge_line_rays");
+        *launches -= 1;
+    } else {
+        if (ext) k_edge_line<true><<<grid, 128, 0, st>>>(s, seed, ws);
+        else k_edge_line<false><<<grid, 128, 0, st>>>(s, seed, ws);
+        timer->mark(st, "k_edge_line");
+        if (B > 1) k_edge_rays<false><<<grid, 128, 0, st>>>(s, ws);
+        else k_edge_rays<true><<<grid, 128, 0, st>>>(s, ws);
+        timer->mark(st, "k_edge_rays");
+    }
     auto shade = ext ? (B > 1 ? k_edge_shade<true, true> : k_edge_shade<true, false>)
                      : (B > 1 ? k_edge_shade<false, true> : k_edge_shade<false, false>);
     shade<<<grid, 128, smem, st>>>(s, W, H, spp, B, seed, dp_mode, grad, ws, cfg);
