@@ -249,7 +249,7 @@ __global__ void __launch_bounds__(128, 4) k_edge_rays(DevScene s, BackwardWorksp
 // one slot (hits[slot].x = slot), which k_edge_shade reads as it does the
 // records of k_edge_rays.
 template <bool EXT, bool DIRECT>
-__global__ void __launch_bounds__(128, 4) k_edge_line_rays(DevScene s, uint64_t seed, BackwardWorkspace ws) {
+__global__ void __launch_bounds__(128, 8) k_edge_line_rays(DevScene s, uint64_t seed, BackwardWorkspace ws) {
     long long n = (long long)min(ws.counters->items, (unsigned long long)ws.cap_items);
     long long stride = (long long)gridDim.x * blockDim.x;
     // warp-uniform loop: the append is warp-aggregated
