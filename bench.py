@@ -299,6 +299,17 @@ def measure_proposal(dev, K=32, train_calls=60):
     return out
 
 
+def merge_stages(stages):
+    """[(kernel, ms)] -> [(stage, ms)]: the kernels of a composite stage summed
+    under its name (COMPOSITE_STAGES), other kernels kept, first-seen order."""
+    parts_of = {k: name for name, parts in COMPOSITE_STAGES.items() for k in parts}
+    merged = {}
+    for name, ms in stages:
+        key = parts_of.get(name, name)
+        merged[key] = merged.get(key, 0.0) + ms
+    return list(merged.items())
+
+
 def load_traffic(stage):
     """DRAM bytes (read + write) per launch of `stage` from the committed ncu
     summary profiles/dram_traffic.txt ("<kernel> <bytes>" lines), if any; the
@@ -500,12 +511,7 @@ def run_b200(args):
     # roofline of the dominant stage; a stage run as several kernels
     # (COMPOSITE_STAGES) counts as one
     peak, peak_kind = load_peaks()
-    parts_of = {k: name for name, parts in COMPOSITE_STAGES.items() for k in parts}
-    merged = {}
-    for name, ms in stages:
-        key = parts_of.get(name, name)
-        merged[key] = merged.get(key, 0.0) + ms
-    merged = list(merged.items())
+    merged = merge_stages(stages)
     dom = max(merged, key=lambda s: s[1]) if merged else ("", 0.0)
     dom_bytes = stage_bytes(dom[0], wl, counts)
     achieved = dom_bytes / (dom[1] / 1e3) / 1e9 if dom[1] > 0 else 0.0
