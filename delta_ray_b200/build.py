@@ -16,11 +16,16 @@ ROOT = os.path.dirname(HERE)
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libdr_b200.so")
 ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
-# The path half of the backward pass keeps IEEE operation order (no FMA
-# contraction): the first path vertex it stores decides which edges a shading
-# point sees, so it must have the bits of the reference's CPU arithmetic.
-PER_FILE_FLAGS = {"dr_backward.cu": ["-fmad=false"]}
+# The renderer's kernels keep IEEE operation order (no FMA contraction): its
+# branch decisions (hit triangles, edge-tree choices, line-sample tests) then
+# see the bits of the CPU restatement of the reference, which runs the same
+# operations in the same order, so a GPU render takes each sample's branches
+# as the CPU does.  Only the learned proposal's network (dr_mlp.cu), whose
+# output is a sampling weight, is contracted.
+NO_FMA = ["-fmad=false"]
+PER_FILE_FLAGS = {"dr_backward.cu": NO_FMA, "dr_edge_kernels.cu": NO_FMA, "dr_kernels.cu": NO_FMA}
 NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr", "-Xcompiler", "-fPIC",
+              "-Xcompiler", "-ffp-contract=off",
               "-Xcompiler", "-fvisibility=hidden", "-I", os.path.join(ROOT, "include")]
 
 

@@ -5,7 +5,7 @@
 // recomputes the forward intermediates it needs and walks its statements in
 // reverse, with the derivative rules of autodiff.h:84-324 (including its
 // conventions at kinks: fabs, max and min pass the gradient to the selected
-// operand, pow(x, a) differentiates a through log(max(x, 1e-6))).
+// operand, dr_powf(x, a) differentiates a through dr_logf(max(x, 1e-6))).
 //
 // Gradients are written through a sink `G` with add(flat_index, value); the
 // flat layout is the C ABI's (camera at 0, then materials, shapes, lights).
@@ -204,7 +204,7 @@ DEV void d_bsdf(const DevScene &s, int mi, const SurfacePoint &sp, float3 wi, fl
                 e_pos = 2.f / rough > 0.f;
                 e = roughness_to_phong(rough);
                 pz = fmaxf(hl.z, 0.f);
-                P = powf(pz, e);
+                P = dr_powf(pz, e);
                 D = P * (e + 2.f) * DR_INV_2PI;
                 G1i = smith_g1(sp.f, n, h, wi, rough);
                 G1o = smith_g1(sp.f, n, h, wo, rough);
@@ -212,7 +212,7 @@ DEV void d_bsdf(const DevScene &s, int mi, const SurfacePoint &sp, float3 wi, fl
             float Gt = G1i * G1o;
             float cd = dot(h, wo);
             float om = 1.f - cd;
-            float fr = powf(fmaxf(om, 0.f), 5.f);
+            float fr = dr_powf(fmaxf(om, 0.f), 5.f);
             float3 F = f3(ks.x + (1.f - ks.x) * fr, ks.y + (1.f - ks.y) * fr, ks.z + (1.f - ks.z) * fr);
             float denom = 4.f * dot(wi, n);
             float inv_den = 1.f / denom;
@@ -223,7 +223,7 @@ DEV void d_bsdf(const DevScene &s, int mi, const SurfacePoint &sp, float3 wi, fl
             float d_denom = -dFsum * D * Gt * inv_den * inv_den;
             dks = dF * (1.f - fr);
             float d_fr = dF.x * (1.f - ks.x) + dF.y * (1.f - ks.y) + dF.z * (1.f - ks.z);
-            float d_om = om >= 0.f ? d_fr * 5.f * powf(om, 4.f) : 0.f;
+            float d_om = om >= 0.f ? d_fr * 5.f * dr_powf(om, 4.f) : 0.f;
             float d_cd = -d_om;
             float3 dh = d_cd * wo;
             sg.dwo += d_cd * h;
@@ -241,8 +241,8 @@ DEV void d_bsdf(const DevScene &s, int mi, const SurfacePoint &sp, float3 wi, fl
                 d_smith_g1(sp.f, n, h, wo, rough, d_G * G1i, sg.df, dn, dh, sg.dwo, dr);
                 float d_P = d_D * (e + 2.f) * DR_INV_2PI;
                 float d_e = d_D * P * DR_INV_2PI;
-                d_z = d_P * e * powf(pz, e - 1.f);
-                d_e += d_P * P * logf(fmaxf(pz, 1e-6f));
+                d_z = d_P * e * dr_powf(pz, e - 1.f);
+                d_e += d_P * P * dr_logf(fmaxf(pz, 1e-6f));
                 if (e_pos) dr += d_e * (-2.f / (rough * rough));
             }
             sg.dwi += (4.f * d_denom) * n;
@@ -304,15 +304,15 @@ DEV void d_bsdf_pdf(const DevScene &s, int mi, const SurfacePoint &sp, float3 wi
             } else {
                 bool e_pos = 2.f / rough > 0.f;
                 float e = roughness_to_phong(rough);
-                float P = powf(hl.z, e);
+                float P = dr_powf(hl.z, e);
                 float D = P * (e + 2.f) * DR_INV_2PI;
                 d_spmf += d_out * D / Q;
                 float d_D = d_out * spmf / Q;
                 d_Q = -d_out * spmf * D / (Q * Q);
                 float d_P = d_D * (e + 2.f) * DR_INV_2PI;
                 float d_e = d_D * P * DR_INV_2PI;
-                d_hlz = d_P * e * powf(hl.z, e - 1.f);
-                d_e += d_P * P * logf(fmaxf(hl.z, 1e-6f));
+                d_hlz = d_P * e * dr_powf(hl.z, e - 1.f);
+                d_e += d_P * P * dr_logf(fmaxf(hl.z, 1e-6f));
                 if (e_pos) dr += d_e * (-2.f / (rough * rough));
             }
             float d_dwh = 4.f * d_Q * (dwh >= 0.f ? 1.f : -1.f);
@@ -444,9 +444,9 @@ DEV void d_sample_primary(const DevCamera &c, float sx, float sy, float3 d_o, fl
     if (c.fisheye) {
         float x = 2.f * (sx - 0.5f), y = 2.f * (sy - 0.5f);
         float rr = sqrtf(x * x + y * y);
-        float phi = atan2f(y, x);
+        float phi = dr_atan2f(y, x);
         float theta = rr * DR_PI / 2.f;
-        dir = f3(-cosf(phi) * sinf(theta), -sinf(phi) * sinf(theta), cosf(theta));
+        dir = f3(-dr_cosf(phi) * dr_sinf(theta), -dr_sinf(phi) * dr_sinf(theta), dr_cosf(theta));
     } else {
         float ndcx = (sx - 0.5f) * -2.f;
         float ndcy = ad ? ((sy - 0.5f) * -2.f) * (1.f / c.aspect) : (sy - 0.5f) * -2.f / c.aspect;

@@ -590,6 +590,10 @@ template <typename F> dr_status guard(F f) {
 
 }  // namespace
 
+namespace {
+unsigned char *noalloc_scratch();
+}  // namespace
+
 extern "C" {
 
 int dr_abi_version(void) { return DR_ABI_VERSION; }
@@ -609,6 +613,9 @@ dr_status dr_scene_create(const dr_scene_desc *desc, int device, dr_scene **out)
         sc->h.preprocess();
         sc->last_launches = 0;
         upload_scene(sc.get(), 0);
+        // loads the module holding the no-alloc backward's scratch array now,
+        // so that a later no-alloc call on this device takes no memory
+        noalloc_scratch();
         *out = sc.release();
     });
 }
@@ -951,6 +958,17 @@ dr_status dr_mlp_gradient(const float *params_dev, const float *x_dev, const flo
     });
 }
 
+dr_status dr_eval_math(int fn, const float *x_dev, const float *y_dev, float *out_dev, int64_t n, void *stream) {
+    return guard([&]() {
+        if (fn < 0 || fn > 7 || n < 0 || (n > 0 && (!x_dev || !out_dev)))
+            throw DrError(DR_ERR_INVALID_ARGUMENT, "dr_eval_math: bad function number or NULL buffer");
+        if ((fn == 3 || fn == 7) && n > 0 && !y_dev)
+            throw DrError(DR_ERR_INVALID_ARGUMENT, "dr_eval_math: atan2 and pow need y");
+        check_cuda(dr_launch_eval_math(fn, x_dev, y_dev, out_dev, n, (cudaStream_t)stream), "math kernel");
+        check_cuda(cudaStreamSynchronize((cudaStream_t)stream), "math kernel");
+    });
+}
+
 dr_status dr_trace_rays(dr_scene *scene, const float *rays_dev, int64_t n, int *tri_dev, float *t_dev, void *stream) {
     return guard([&]() {
         if (!scene) throw DrError(DR_ERR_INVALID_ARGUMENT, "scene is NULL");
@@ -1026,30 +1044,22 @@ size_t dr_last_error(char *buf, size_t len) {
 namespace {
 constexpr size_t kNoAllocScratchBytes = size_t(32) << 20;  // per device
 constexpr long long kNoAllocMaxSamples = 65536;            // width * height * spp
-constexpr int kNoAllocMaxDevices = 64;
 }  // namespace
 
 static __device__ __align__(256) unsigned char g_noalloc_scratch[kNoAllocScratchBytes];
 
 namespace {
-std::mutex &noalloc_mutex() {
-    static std::mutex *m = new std::mutex();
-    return *m;
-}
-void *g_noalloc_base[kNoAllocMaxDevices] = {};
-
-// Device address of this device's copy of the array, looked up on the first
-// call on each device (the caller has made `device` current).
-unsigned char *noalloc_scratch(int device) {
-    if (device < 0 || device >= kNoAllocMaxDevices) throw DrError(DR_ERR_NOT_SUPPORTED, "device index out of range");
-    std::lock_guard<std::mutex> lk(noalloc_mutex());
-    if (!g_noalloc_base[device]) {
-        void *p = nullptr;
-        check_cuda(cudaGetSymbolAddress(&p, g_noalloc_scratch), "cudaGetSymbolAddress");
-        if (!p) throw DrError(DR_ERR_CUDA, "cudaGetSymbolAddress returned NULL");
-        g_noalloc_base[device] = p;
-    }
-    return (unsigned char *)g_noalloc_base[device];
+// Device address of the current device's copy of the array.  It is looked up
+// on every call rather than cached, so that a context that was reset and made
+// again (cudaDeviceReset) gets the address of its own copy.  The lookup loads
+// the module that holds the array when CUDA loads modules lazily; scene
+// creation makes the same lookup, so that the array's memory is taken there
+// and a no-alloc call never loads a module itself.
+unsigned char *noalloc_scratch() {
+    void *p = nullptr;
+    check_cuda(cudaGetSymbolAddress(&p, g_noalloc_scratch), "cudaGetSymbolAddress");
+    if (!p) throw DrError(DR_ERR_CUDA, "cudaGetSymbolAddress returned NULL");
+    return (unsigned char *)p;
 }
 }  // namespace
 
@@ -1070,14 +1080,15 @@ dr_status dr_render_backward_noalloc(dr_scene *scene, const dr_render_desc *rd, 
         check_cuda(cudaSetDevice(scene->device), "cudaSetDevice");
         cudaStream_t st = (cudaStream_t)stream;
         scene->last_launches = 0;
-        unsigned char *base = noalloc_scratch(scene->device);
+        scene->timings.clear();  // this path records no stage timings
+        unsigned char *base = noalloc_scratch();
         // layout: counters | point records | point keys | items | item weights | item dp | survivors | hits
         auto up = [](size_t b) { return (b + 255) & ~size_t(255); };
         // scenes with specular chains: room for the points of every bounce,
         // up to half the scratch (the rest holds edge items)
         long long cap_points = npix;
-        if (scene->h.specular_bounces && rd->max_bounces >= 2) {
-            long long want = npix * std::min(rd->max_bounces, DR_MAX_LINKS + 1);
+        if (scene->h.specular_bounces && rd->max_bounces >= 1) {
+            long long want = npix * std::min(rd->max_bounces + 1, DR_MAX_LINKS + 1);
             long long fit = (long long)(kNoAllocScratchBytes / 2 / (sizeof(float) * DR_PT_FLOATS + DR_PT_LAST_BYTES));
             cap_points = std::max(npix, std::min(want, fit));
         }

@@ -92,7 +92,7 @@ DEV float d_specular_direction(const DevScene &s, int mi, const Frame &f, float3
                                float3 d_dir, Frame &d_f, float3 &d_wi) {
     const DevMaterial &m = s.mats[mi];
     float phi = 2.f * DR_PI * bs.u1;
-    float sphi = sinf(phi), cphi = cosf(phi);
+    float sphi = dr_sinf(phi), cphi = dr_cosf(phi);
     float ct, dct_dr = 0.f;
     if (m.model == DR_MICROFACET_GGX) {
         float A = ggx_A(rough);
@@ -102,8 +102,8 @@ DEV float d_specular_direction(const DevScene &s, int mi, const Frame &f, float3
     } else {
         float e = roughness_to_phong(rough);
         float ie = 1.f / (e + 2.0f);
-        ct = powf(bs.u0, ie);
-        if (2.f / rough > 0.f && bs.u0 > 0.f) dct_dr = ct * logf(bs.u0) * (-ie * ie) * (-2.f / (rough * rough));
+        ct = dr_powf(bs.u0, ie);
+        if (2.f / rough > 0.f && bs.u0 > 0.f) dct_dr = ct * dr_logf(bs.u0) * (-ie * ie) * (-2.f / (rough * rough));
     }
     float st = sqrtf(fmaxf(1.f - ct * ct, 0.f));
     float3 hl = f3(st * cphi, st * sphi, ct);

@@ -52,6 +52,10 @@ HD unsigned dr_umulhi(unsigned a, unsigned b) {
 }
 #endif
 
+// reproducible sin, cos, atan, atan2, acos, exp, log and pow (same bits on
+// the GPU and in the host builds of this code)
+#include "dr_math.h"
+
 // bit casts usable from __host__ __device__ code
 HD float dr_i2f(int i) {
 #ifdef __CUDA_ARCH__

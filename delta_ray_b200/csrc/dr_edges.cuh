@@ -197,7 +197,7 @@ DEV_NOINLINE float bsdf_bound(const DevEdgeNode &node, float3 wi, const SurfaceP
             maxp = ggx_D(hdn, ggx_A(rough));
         } else {
             float e = roughness_to_phong(rough);
-            maxp = powf(hdn, e) * (e + 2.f) / float(2 * 3.14159265358979323846);
+            maxp = dr_powf(hdn, e) * (e + 2.f) / float(2 * 3.14159265358979323846);
         }
     }
     return cos_max * (dl / DR_PI + sl * maxp);
@@ -212,9 +212,9 @@ DEV_NOINLINE bool contains_silhouette(const DevEdgeNode &node, float3 p) {
     float l = length(d);
     float vt = r / l;
     if (vt >= 1.f) return true;
-    float va = atanf(vt);
+    float va = dr_atanf(vt);
     d = d / l;
-    float ang = acosf(dot(-d, f3(node.axis[0], node.axis[1], node.axis[2])));
+    float ang = dr_acosf(dot(-d, f3(node.axis[0], node.axis[1], node.axis[2])));
     float range = node.angle + va;
     (void)c;
     return ang - range <= float(3.14159265358979323846 / 2.f) && ang + range >= float(3.14159265358979323846 / 2.f);
@@ -231,7 +231,7 @@ DEV bool node_inside(const DevEdgeNode &n, float3 p) {
 
 // The learned edge proposal of one shading point (a project addition): 32
 // bf16 probabilities over directions from the point, in the shading frame:
-// 4 bands of cos(theta) (split at -1/2, 0, 1/2) times 8 azimuth octants
+// 4 bands of dr_cosf(theta) (split at -1/2, 0, 1/2) times 8 azimuth octants
 // (dir_bin).  q == null: the reference's sampling.
 struct EdgeProposal {
     const uint16_t *q;
@@ -481,7 +481,7 @@ DEV bool traverse_subtree(const DevScene &s, float3 wi, int stri, const SurfaceP
 DEV M3 ltc_matrix(const DevScene &s, int mi, const SurfacePoint &sp, float3 wi) {
     float r = get_rough(s, s.mats[mi], sp.uv);
     float ct = dot(wi, sp.f.n);
-    float th = acosf(ct);
+    float th = dr_acosf(ct);
     int rid = int(r * (128 - 1));
     int tid = int(((double)th / (3.14159265358979323846 / 2.f)) * (128 - 1));
     rid = rid < 0 ? 0 : (rid > 127 ? 127 : rid);
@@ -536,7 +536,7 @@ DEV_NOINLINE float lobe_line_density(const M3 &minv, float3 d0, float3 d1, float
     float3 vo = a - l0 * wt;
     float d = length(vo);
     auto I = [&](float l) {
-        return (l / (d * (d * d + l * l)) + atanf(l / d) / (d * d)) * vo.z + (l * l / (d * (d * d + l * l))) * wt.z;
+        return (l / (d * (d * d + l * l)) + dr_atanf(l / d) / (d * d)) * vo.z + (l * l / (d * (d * d + l * l))) * wt.z;
     };
     float norm = I(l1) - I(l0);
     if (norm <= 1e-10f) return 0.f;
@@ -608,7 +608,7 @@ DEV bool edge_line_sample(const DevScene &s, const EdgeSample &es, const DevEdge
     float3 vo = a - l0 * wt;
     float d = length(vo);
     auto I = [&](float l) {
-        return (l / (d * (d * d + l * l)) + atanf(l / d) / (d * d)) * vo.z + (l * l / (d * (d * d + l * l))) * wt.z;
+        return (l / (d * (d * d + l * l)) + dr_atanf(l / d) / (d * d)) * vo.z + (l * l / (d * (d * d + l * l))) * wt.z;
     };
     float Il0 = I(l0), Il1 = I(l1);
     float norm = Il1 - Il0;
@@ -812,14 +812,14 @@ DEV EdgeResult shading_edge_sample(const DevScene &s, const EdgeSample &es, cons
 // Fisheye branches out of line (rarely taken, large trigonometry).
 DEV_NOINLINE float3 unproject_fisheye(float sx, float sy) {
     float x = 2.f * (sx - 0.5f), y = 2.f * (sy - 0.5f);
-    float r = sqrtf(x * x + y * y), phi = atan2f(y, x), theta = r * DR_PI / 2.f;
-    return f3(-cosf(phi) * sinf(theta), -sinf(phi) * sinf(theta), cosf(theta));
+    float r = sqrtf(x * x + y * y), phi = dr_atan2f(y, x), theta = r * DR_PI / 2.f;
+    return f3(-dr_cosf(phi) * dr_sinf(theta), -dr_sinf(phi) * dr_sinf(theta), dr_cosf(theta));
 }
 struct F3Pair { float3 a, b; };
 DEV_NOINLINE F3Pair d_unproject_fisheye(float sx, float sy) {
     float x = 2.f * (sx - 0.5f), y = 2.f * (sy - 0.5f);
-    float r = sqrtf(x * x + y * y), phi = atan2f(y, x), theta = r * DR_PI / 2.f;
-    float sp = sinf(phi), cp = cosf(phi), st = sinf(theta), ct = cosf(theta);
+    float r = sqrtf(x * x + y * y), phi = dr_atan2f(y, x), theta = r * DR_PI / 2.f;
+    float sp = dr_sinf(phi), cp = dr_cosf(phi), st = dr_sinf(theta), ct = dr_cosf(theta);
     float dxdphi = sp * st, dxdth = -cp * ct, dydphi = -cp * st, dydth = -sp * ct, dzdth = -st;
     float dphidx = -y / (r * r), dphidy = x / (r * r);
     float dthdx = (DR_PI / 2.f) * x / r, dthdy = (DR_PI / 2.f) * y / r;
@@ -831,16 +831,16 @@ DEV_NOINLINE F3Pair d_unproject_fisheye(float sx, float sy) {
 DEV_NOINLINE float2 project_local_fisheye(float3 l) {
     float2 r;
     float3 d = normalize(l);
-    float phi = atan2f(d.y, d.x), theta = acosf(d.z), rr = theta * 2.f / DR_PI;
-    r.x = 0.5f * (-rr * cosf(phi) + 1.f);
-    r.y = 0.5f * (-rr * sinf(phi) + 1.f);
+    float phi = dr_atan2f(d.y, d.x), theta = dr_acosf(d.z), rr = theta * 2.f / DR_PI;
+    r.x = 0.5f * (-rr * dr_cosf(phi) + 1.f);
+    r.y = 0.5f * (-rr * dr_sinf(phi) + 1.f);
     return r;
 }
 DEV_NOINLINE float3 d_project_local_fisheye(float3 l, float dx, float dy) {
     float3 d = normalize(l);
-    float phi = atan2f(d.y, d.x), theta = acosf(d.z), r = theta * 2.f / DR_PI;
-    float dr = -0.5f * (cosf(phi) * dx + sinf(phi) * dy);
-    float dphi = 0.5f * r * sinf(phi) * dx - 0.5f * r * cosf(phi) * dy;
+    float phi = dr_atan2f(d.y, d.x), theta = dr_acosf(d.z), r = theta * 2.f / DR_PI;
+    float dr = -0.5f * (dr_cosf(phi) * dx + dr_sinf(phi) * dy);
+    float dphi = 0.5f * r * dr_sinf(phi) * dx - 0.5f * r * dr_cosf(phi) * dy;
     float dtheta = dr * (2.f / DR_PI);
     float dcos = -dtheta / sqrtf(1.f - d.z * d.z);
     float t = d.x * d.x + d.y * d.y;

@@ -76,8 +76,8 @@ struct V2 { float x, y; };
 V2 project_local(const HCam &c, V3 l) {
     if (c.fisheye) {
         V3 d = normalize(l);
-        float phi = std::atan2(d.y, d.x), theta = std::acos(d.z), r = theta * 2.f / DR_PI;
-        return V2{0.5f * (-r * std::cos(phi) + 1.f), 0.5f * (-r * std::sin(phi) + 1.f)};
+        float phi = dr_atan2f(d.y, d.x), theta = dr_acosf(d.z), r = theta * 2.f / DR_PI;
+        return V2{0.5f * (-r * dr_cosf(phi) + 1.f), 0.5f * (-r * dr_sinf(phi) + 1.f)};
     }
     return V2{(-l.x / (l.z * c.fov) + 1.f) * 0.5f, (-l.y / (l.z * c.fov * c.aspect) + 1.f) * 0.5f};
 }
@@ -188,7 +188,7 @@ std::unique_ptr<BuildNode> build_node(std::vector<PrimInfo> &pi, int start, int 
     }
     node->sb = sb;
     node->axis = axis;
-    node->angle = std::acos(cmin);
+    node->angle = dr_acosf(cmin);
     int n = end - start;
     auto leaf = [&]() {
         node->first = start;

@@ -171,6 +171,17 @@ __global__ void k_trace_rays(DevScene s, const float *rays, long long n, int *tr
     t[i] = h.t;
 }
 
+__global__ void k_eval_math(int fn, const float *x, const float *y, float *out, long long n) {
+    long long i = (long long)blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = dr_math_eval(fn, x[i], y ? y[i] : 0.f);
+}
+
+cudaError_t dr_launch_eval_math(int fn, const float *x, const float *y, float *out, long long n, cudaStream_t st) {
+    if (n <= 0) return cudaSuccess;
+    k_eval_math<<<blocks_for(n, 256), 256, 0, st>>>(fn, x, y, out, n);
+    return cudaGetLastError();
+}
+
 cudaError_t dr_launch_trace(const DevScene &s, const float *rays, long long n, int *tri, float *t, cudaStream_t st,
                             int *launches) {
     if (n <= 0) return cudaSuccess;

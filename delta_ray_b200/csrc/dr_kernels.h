@@ -35,6 +35,7 @@ size_t dr_lbvh_scratch_bytes(int n);
 cudaError_t dr_refit_lbvh(const float *vtx, const int4 *tri, int n, float4 *nodes, float4 *leaf_tris, void *scratch,
                           size_t scratch_bytes, cudaStream_t st, int *launches);
 
+cudaError_t dr_launch_eval_math(int fn, const float *x, const float *y, float *out, long long n, cudaStream_t st);
 cudaError_t dr_launch_trace(const DevScene &s, const float *rays, long long n, int *tri, float *t, cudaStream_t st,
                             int *launches);
 

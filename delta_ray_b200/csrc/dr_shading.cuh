@@ -36,9 +36,9 @@ DEV_NOINLINE float3 fisheye_dir(float sx, float sy) {
     float x = 2.f * (sx - 0.5f), y = 2.f * (sy - 0.5f);
     if (x * x + y * y > 1.f) return f3(0.f);
     float rr = sqrtf(x * x + y * y);
-    float phi = atan2f(y, x);
+    float phi = dr_atan2f(y, x);
     float theta = rr * DR_PI / 2.f;
-    float3 dir = f3(-cosf(phi) * sinf(theta), -sinf(phi) * sinf(theta), cosf(theta));
+    float3 dir = f3(-dr_cosf(phi) * dr_sinf(theta), -dr_sinf(phi) * dr_sinf(theta), dr_cosf(theta));
     return normalize(dir);
 }
 
@@ -191,11 +191,11 @@ DEV float3 bsdf(const DevScene &s, int mi, const SurfacePoint &sp, float3 wi, fl
                 G = ggx_g1(n, h, wi, A) * ggx_g1(n, h, wo, A);
             } else {
                 float e = roughness_to_phong(rough);
-                D = powf(fmaxf(hl.z, 0.f), e) * (e + 2.f) / float(2 * 3.14159265358979323846);
+                D = dr_powf(fmaxf(hl.z, 0.f), e) * (e + 2.f) / float(2 * 3.14159265358979323846);
                 G = smith_g1(sp.f, n, h, wi, rough) * smith_g1(sp.f, n, h, wo, rough);
             }
             float cd = dot(h, wo);
-            float fr = powf(fmaxf(1.f - cd, 0.f), 5.f);
+            float fr = dr_powf(fmaxf(1.f - cd, 0.f), 5.f);
             float3 F = f3(ks.x + (1.f - ks.x) * fr, ks.y + (1.f - ks.y) * fr, ks.z + (1.f - ks.z) * fr);
             res += F * D * G / (4.f * dot(wi, n));
         }
@@ -226,7 +226,7 @@ DEV float bsdf_pdf(const DevScene &s, int mi, const SurfacePoint &sp, float3 wi,
                 spdf = spmf * D * hl.z / (4.f * fabsf(dot(wo, h)));
             } else {
                 float e = roughness_to_phong(get_rough(s, m, sp.uv));
-                float D = powf(hl.z, e) * (e + 2.f) / float(2 * 3.14159265358979323846);
+                float D = dr_powf(hl.z, e) * (e + 2.f) / float(2 * 3.14159265358979323846);
                 spdf = spmf * D / (4.f * fabsf(dot(wo, h)));
             }
         }
@@ -237,7 +237,7 @@ DEV float bsdf_pdf(const DevScene &s, int mi, const SurfacePoint &sp, float3 wi,
 DEV float3 cos_hemisphere(float u0, float u1) {  // vector.h:533-538
     float phi = 2.f * DR_PI * u0;
     float tmp = sqrtf(1.f - u1);
-    return f3(cosf(phi) * tmp, sinf(phi) * tmp, sqrtf(u1));
+    return f3(dr_cosf(phi) * tmp, dr_sinf(phi) * tmp, sqrtf(u1));
 }
 
 // Direction sampled at a surface point (material-level sample_bsdf).
@@ -256,13 +256,13 @@ DEV float3 sample_bsdf_dir(const DevScene &s, int mi, const SurfacePoint &sp, fl
     if (sw <= 0.f) return f3(0.f);
     float rough = get_rough(s, m, sp.uv);
     float phi = 2.f * DR_PI * bs.u1;
-    float sphi = sinf(phi), cphi = cosf(phi);
+    float sphi = dr_sinf(phi), cphi = dr_cosf(phi);
     float ct;
     if (m.model == DR_MICROFACET_GGX) {
         float A = ggx_A(rough);
         ct = sqrtf((1.f - bs.u0) / (1.f + (A - 1.f) * bs.u0));
     } else {
-        ct = powf(bs.u0, 1.0f / (roughness_to_phong(rough) + 2.0f));
+        ct = dr_powf(bs.u0, 1.0f / (roughness_to_phong(rough) + 2.0f));
     }
     float st = sqrtf(fmaxf(1.f - ct * ct, 0.f));
     float3 h = to_world(sp.f, f3(st * cphi, st * sphi, ct));

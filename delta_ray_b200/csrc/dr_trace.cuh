@@ -35,7 +35,15 @@ extern thread_local long long g_dr_visits;
 #else
 #define DR_COUNT_VISIT()
 #endif
+// Traversal stack depth.  The stack never overflows: along a root-to-leaf
+// path of the Karras LBVH (dr_bvh.cuh) the nodes' common-prefix lengths
+// (lbvh_delta) strictly increase.  Distinct 30-bit Morton keys give prefix
+// lengths clz(a ^ b) in [2, 31], 30 values; equal keys give 32 + clz(i ^ j)
+// with i, j < n < 2^31, at most 31 values.  So a path has at most 61 internal
+// nodes, each pushes at most one entry, and 64 entries always suffice; the
+// push guards below are never taken.
 #define DR_STACK 64
+static_assert(DR_STACK >= 30 + 31, "LBVH traversal stack shorter than the tree's depth bound");
 
 // Moller-Trumbore with no contraction: the exact operation sequence of the
 // oracle's hit test.  Returns false on a miss.

@@ -259,8 +259,10 @@ DR_API dr_status dr_render_backward_views(dr_scene *scene, int n_views, const dr
  * DR_ERR_OUT_OF_MEMORY, as do specular chains whose shading points outgrow
  * half the array (about 150,000 points).  All calls on
  * one device share the array, so overlapping calls (from several threads or
- * streams) race: serialize them.  The first call on each device looks up the
- * array's address; make it before any stream capture. */
+ * streams) race: serialize them.  Where CUDA loads modules lazily, the
+ * array's memory is taken when the first scene is created on the device
+ * (dr_scene_create looks the array up), not by this call; each call looks up
+ * the address of the current context's copy again. */
 DR_API dr_status dr_render_backward_noalloc(dr_scene *scene, const dr_render_desc *rd, const float *d_image_dev,
                                             float *grad_dev, float *image_dev, void *stream);
 
@@ -271,6 +273,16 @@ DR_API dr_status dr_render_backward_noalloc(dr_scene *scene, const dr_render_des
  * renderer's own traversal. */
 DR_API dr_status dr_trace_rays(dr_scene *scene, const float *rays_dev, int64_t n, int *tri_dev, float *t_dev,
                         void *stream);
+
+/* Check hook (no counterpart in the reference, whose transcendental functions
+ * are the host libm's): evaluates the renderer's reproducible float functions
+ * on the device, out[i] = f(x[i]) or f(x[i], y[i]) for fn 0 sin, 1 cos,
+ * 2 atan, 3 atan2(x, y), 4 acos, 5 exp, 6 log, 7 pow(x, y) (device buffers of
+ * n floats; y may be NULL except for atan2 and pow).  The same functions,
+ * compiled for the host, give the same bits; tests compare the two.  Returns
+ * after the stream has finished. */
+DR_API dr_status dr_eval_math(int fn, const float *x_dev, const float *y_dev, float *out_dev, int64_t n,
+                              void *stream);
 
 /* Tooling: per-stage GPU time of the following render calls.  With
  * profiling on, each render records CUDA events around its kernels and

@@ -35,6 +35,22 @@
 #include <atomic>
 #include <thread>
 
+#include "../delta_ray_b200/csrc/dr_math.h"
+
+// The transcendental functions the restatement evaluates.  In the reference's
+// RNG mode they are the host libm's, as in the compiled reference.  In the
+// Philox mode they are the product's reproducible ones (dr_math.h), whose bits
+// are the same on the GPU and here, so that a sample takes the same branches
+// on both sides.
+static bool g_repro_math = false;
+inline float m_pow(float x, float e) { return g_repro_math ? dr_powf(x, e) : std::pow(x, e); }
+inline float m_log(float x) { return g_repro_math ? dr_logf(x) : std::log(x); }
+inline float m_sin(float x) { return g_repro_math ? dr_sinf(x) : std::sin(x); }
+inline float m_cos(float x) { return g_repro_math ? dr_cosf(x) : std::cos(x); }
+inline float m_acos(float x) { return g_repro_math ? dr_acosf(x) : std::acos(x); }
+inline float m_atan(float x) { return g_repro_math ? dr_atanf(x) : std::atan(x); }
+inline float m_atan2(float y, float x) { return g_repro_math ? dr_atan2f(y, x) : std::atan2(y, x); }
+
 namespace oracle {
 
 static const float kPi = 3.14159265358979323846f;
@@ -112,18 +128,18 @@ inline AD sqrt(const AD &x) {
     float s = std::sqrt(x.v);
     return mk(s, x.id, 0.5f / s);
 }
-inline AD pow(const AD &x, float e) { return mk(std::pow(x.v, e), x.id, e * std::pow(x.v, e - 1.f)); }
+inline AD pow(const AD &x, float e) { return mk(m_pow(x.v, e), x.id, e * m_pow(x.v, e - 1.f)); }
 inline AD pow(const AD &x, const AD &e) {
-    float p = std::pow(x.v, e.v);
-    return mk(p, x.id, e.v * std::pow(x.v, e.v - 1.f), e.id, p * std::log(std::max(x.v, 1e-6f)));
+    float p = m_pow(x.v, e.v);
+    return mk(p, x.id, e.v * m_pow(x.v, e.v - 1.f), e.id, p * m_log(std::max(x.v, 1e-6f)));
 }
 inline AD pow(float x, const AD &e) { return pow(AD(x), e); }
-inline AD sin(const AD &x) { return mk(std::sin(x.v), x.id, std::cos(x.v)); }
-inline AD cos(const AD &x) { return mk(std::cos(x.v), x.id, -std::sin(x.v)); }
-inline AD acos(const AD &x) { return mk(std::acos(x.v), x.id, -std::sqrt(1.f / (1.f - x.v * x.v))); }
+inline AD sin(const AD &x) { return mk(m_sin(x.v), x.id, m_cos(x.v)); }
+inline AD cos(const AD &x) { return mk(m_cos(x.v), x.id, -m_sin(x.v)); }
+inline AD acos(const AD &x) { return mk(m_acos(x.v), x.id, -std::sqrt(1.f / (1.f - x.v * x.v))); }
 inline AD atan2(const AD &y, const AD &x) {
     float t = x.v * x.v + y.v * y.v;
-    return mk(std::atan2(y.v, x.v), y.id, x.v / t, x.id, -y.v / t);
+    return mk(m_atan2(y.v, x.v), y.id, x.v / t, x.id, -y.v / t);
 }
 inline AD fabs(const AD &x) { return x.v >= 0.f ? x : -x; }
 // max/min keep the reference's tie conventions (autodiff.h:301-324)
@@ -137,11 +153,11 @@ inline float max(float x, float y) { return x > y ? x : y; }
 inline float min(float x, float y) { return x < y ? x : y; }
 inline float fabs(float x) { return std::fabs(x); }
 inline float sqrt(float x) { return std::sqrt(x); }
-inline float pow(float x, float e) { return std::pow(x, e); }
-inline float sin(float x) { return std::sin(x); }
-inline float cos(float x) { return std::cos(x); }
-inline float acos(float x) { return std::acos(x); }
-inline float atan2(float y, float x) { return std::atan2(y, x); }
+inline float pow(float x, float e) { return m_pow(x, e); }
+inline float sin(float x) { return m_sin(x); }
+inline float cos(float x) { return m_cos(x); }
+inline float acos(float x) { return m_acos(x); }
+inline float atan2(float y, float x) { return m_atan2(y, x); }
 
 inline float val(float x) { return x; }
 inline float val(const AD &x) { return x.v; }
@@ -687,8 +703,8 @@ template <typename T> Ray<T> sample_primary(const TCam<T> &cam, const V2<T> &s) 
 inline V3f unproject(const Camera &c, const V2f &s) {
     if (c.fisheye) {
         float x = 2.f * (s.x - 0.5f), y = 2.f * (s.y - 0.5f);
-        float r = std::sqrt(x * x + y * y), phi = std::atan2(y, x), theta = r * kPi / 2.f;
-        return V3f{-std::cos(phi) * std::sin(theta), -std::sin(phi) * std::sin(theta), std::cos(theta)};
+        float r = std::sqrt(x * x + y * y), phi = m_atan2(y, x), theta = r * kPi / 2.f;
+        return V3f{-m_cos(phi) * m_sin(theta), -m_sin(phi) * m_sin(theta), m_cos(theta)};
     }
     float ndcx = (s.x - 0.5f) * -2.f, ndcy = (s.y - 0.5f) * -2.f / c.aspect;
     return V3f{c.fov * ndcx, c.fov * ndcy, 1.f};
@@ -696,8 +712,8 @@ inline V3f unproject(const Camera &c, const V2f &s) {
 inline std::pair<V3f, V3f> d_unproject(const Camera &c, const V2f &s) {
     if (c.fisheye) {
         float x = 2.f * (s.x - 0.5f), y = 2.f * (s.y - 0.5f);
-        float r = std::sqrt(x * x + y * y), phi = std::atan2(y, x), theta = r * kPi / 2.f;
-        float sp = std::sin(phi), cp = std::cos(phi), st = std::sin(theta), ct = std::cos(theta);
+        float r = std::sqrt(x * x + y * y), phi = m_atan2(y, x), theta = r * kPi / 2.f;
+        float sp = m_sin(phi), cp = m_cos(phi), st = m_sin(theta), ct = m_cos(theta);
         float dxdphi = sp * st, dxdth = -cp * ct, dydphi = -cp * st, dydth = -sp * ct, dzdth = -st;
         float dphidx = -y / (r * r), dphidy = x / (r * r);
         float dthdx = (kPi / 2.f) * x / r, dthdy = (kPi / 2.f) * y / r;
@@ -709,8 +725,8 @@ inline std::pair<V3f, V3f> d_unproject(const Camera &c, const V2f &s) {
 inline V2f project_local(const Camera &c, const V3f &l) {
     if (c.fisheye) {
         V3f d = normalize(l);
-        float phi = std::atan2(d.y, d.x), theta = std::acos(d.z), r = theta * 2.f / kPi;
-        return V2f{0.5f * (-r * std::cos(phi) + 1.f), 0.5f * (-r * std::sin(phi) + 1.f)};
+        float phi = m_atan2(d.y, d.x), theta = m_acos(d.z), r = theta * 2.f / kPi;
+        return V2f{0.5f * (-r * m_cos(phi) + 1.f), 0.5f * (-r * m_sin(phi) + 1.f)};
     }
     return V2f{(-l.x / (l.z * c.fov) + 1.f) * 0.5f, (-l.y / (l.z * c.fov * c.aspect) + 1.f) * 0.5f};
 }
@@ -723,9 +739,9 @@ inline V3f d_normalize(const V3f &v, const V3f &d) {
 inline V3f d_project_local(const Camera &c, const V3f &l, float dx, float dy) {
     if (c.fisheye) {
         V3f d = normalize(l);
-        float phi = std::atan2(d.y, d.x), theta = std::acos(d.z), r = theta * 2.f / kPi;
-        float dr = -0.5f * (std::cos(phi) * dx + std::sin(phi) * dy);
-        float dphi = 0.5f * r * std::sin(phi) * dx - 0.5f * r * std::cos(phi) * dy;
+        float phi = m_atan2(d.y, d.x), theta = m_acos(d.z), r = theta * 2.f / kPi;
+        float dr = -0.5f * (m_cos(phi) * dx + m_sin(phi) * dy);
+        float dphi = 0.5f * r * m_sin(phi) * dx - 0.5f * r * m_cos(phi) * dy;
         float dtheta = dr * (2.f / kPi);
         float dcos = -dtheta / std::sqrt(1.f - d.z * d.z);
         float t = d.x * d.x + d.y * d.y;
@@ -947,7 +963,7 @@ V3<T> bsdf(const Scene &sc, int mi, const SPoint<T> &sp, const V3<T> &wi, const 
 inline V3f cos_hemisphere(const V2f &s) {  // vector.h:533-538
     float phi = 2.f * kPi * s.x;
     float tmp = std::sqrt(1.f - s.y);
-    return V3f{std::cos(phi) * tmp, std::sin(phi) * tmp, std::sqrt(s.y)};
+    return V3f{m_cos(phi) * tmp, m_sin(phi) * tmp, std::sqrt(s.y)};
 }
 
 struct BSDFSample { V2f uv; float w; };
@@ -1008,7 +1024,7 @@ std::pair<V3<T>, bool> sample_bsdf_dir(const Scene &sc, int mi, const SPoint<T> 
     if (sw <= T(0.f)) return {zero, false};
     T rough = get_roughness(mat, sp.uv, r);
     float phi = 2.f * kPi * bs.uv.y;
-    float sphi = std::sin(phi), cphi = std::cos(phi);
+    float sphi = m_sin(phi), cphi = m_cos(phi);
     T ct;
     if (mat.model == DR_MICROFACET_GGX) {
         T A = ggx_A(rough);
@@ -1334,7 +1350,7 @@ std::unique_ptr<BuildNode> build_edge_node(const std::vector<Edge> &edges, std::
     }
     node->sb = sb;
     node->axis = axis;
-    node->angle = std::acos(cmin);
+    node->angle = m_acos(cmin);
     int n = end - start;
     auto make_leaf = [&]() {
         node->first = (int)ordered.size();
@@ -1582,7 +1598,7 @@ inline float bsdf_bound(const Scene &sc, const EdgeNode &node, const V3f &wi, co
             maxp = ggx_D(hdn, ggx_A(rough));
         } else {
             float e = roughness_to_phong(rough);
-            maxp = std::pow(hdn, e) * (e + 2.f) / float(2 * M_PI);
+            maxp = m_pow(hdn, e) * (e + 2.f) / float(2 * M_PI);
         }
     }
     return cos_max * (dl / kPi + sl * maxp);
@@ -1596,9 +1612,9 @@ inline bool contains_silhouette(const EdgeNode &node, const V3f &p) {
     float l = length(d);
     float vt = r / l;
     if (vt >= 1.f) return true;
-    float va = std::atan(vt);
+    float va = m_atan(vt);
     d = d / l;
-    float ang = std::acos(dot(-d, node.cone_axis));
+    float ang = m_acos(dot(-d, node.cone_axis));
     float range = node.cone_angle + va;
     return ang - range <= float(M_PI / 2.f) && ang + range >= float(M_PI / 2.f);
 }
@@ -1689,7 +1705,7 @@ inline void sample_shading_edges(const Scene &sc, const V3f &wi, const Isect &is
 inline M3 ltc_matrix(const Scene &sc, int mi, const SPoint<float> &sp, const V3f &wi) {
     float r = get_roughness<float>(sc.mats[mi], sp.uv, nullptr);
     float ct = dot(wi, sp.f[2]);
-    float th = std::acos(ct);
+    float th = m_acos(ct);
     int rid = int(r * (128 - 1));
     int tid = int((th / (M_PI / 2.f)) * (128 - 1));
     rid = std::max(0, std::min(127, rid));
@@ -1719,7 +1735,7 @@ inline float lobe_line_density(const M3 &minv, const V3f &d0, const V3f &d1, con
     V3f vo = a - l0 * wt;
     float d = length(vo);
     auto I = [&](float l) {
-        return (l / (d * (d * d + l * l)) + std::atan(l / d) / (d * d)) * vo.z + (l * l / (d * (d * d + l * l))) * wt.z;
+        return (l / (d * (d * d + l * l)) + m_atan(l / d) / (d * d)) * vo.z + (l * l / (d * (d * d + l * l))) * wt.z;
     };
     float norm = I(l1) - I(l0);
     if (norm <= 1e-10f) return 0.f;
@@ -1773,7 +1789,7 @@ inline EdgeResult shading_edge_sample(const Scene &sc, const EdgeSample &es, con
     V3f vo = a - l0 * wt;
     float d = length(vo);
     auto I = [&](float l) {
-        return (l / (d * (d * d + l * l)) + std::atan(l / d) / (d * d)) * vo.z + (l * l / (d * (d * d + l * l))) * wt.z;
+        return (l / (d * (d * d + l * l)) + m_atan(l / d) / (d * d)) * vo.z + (l * l / (d * (d * d + l * l))) * wt.z;
     };
     float Il0 = I(l0), Il1 = I(l1);
     float norm = Il1 - Il0;
@@ -2345,7 +2361,8 @@ int dro_render_parts(const dr_scene_desc *desc, const dr_render_desc *rd, int rn
 // rng_mode 0: the reference's mt19937 scheme with `cores` edge threads;
 // shape_rank (may be NULL) orders shapes in the edge map as the reference's
 // Shape* keys did;
-// rng_mode 1: the product's Philox streams.  d_image == NULL renders forward
+// rng_mode 1: the product's Philox streams and its reproducible transcendental
+// functions (rng_mode 2: the same streams with the host libm).  d_image == NULL renders forward
 // only.  grad (flat layout) may be NULL for forward.  stats[0..1] receive the
 // number of secondary points and sampled edges.
 int dro_render(const dr_scene_desc *desc, const dr_render_desc *rd, int rng_mode, int cores, const float *d_image,
@@ -2355,6 +2372,10 @@ int dro_render(const dr_scene_desc *desc, const dr_render_desc *rd, int rng_mode
 
 int dro_render_parts(const dr_scene_desc *desc, const dr_render_desc *rd, int rng_mode, int cores, const float *d_image,
                      float *image, float *grad, long long *stats, int nthreads, const int *shape_rank, int parts) {
+    // rng_mode 2: the Philox streams with the host libm (a check that the
+    // restatement does not depend on the libm beyond rounding)
+    g_repro_math = rng_mode == 1;
+    if (rng_mode == 2) rng_mode = 1;
     Scene sc;
     build_scene(sc, desc, nullptr, shape_rank);
     sc.detached_pdf = (rd->flags & DR_FLAG_DETACHED_PDF) != 0;

@@ -25,6 +25,7 @@ from delta_ray_b200 import _abi  # noqa: E402
 
 REFERENCE = 0
 PHILOX = 1
+PHILOX_LIBM = 2  # Philox streams, host libm transcendentals (the product's are reproducible ones)
 LIB_PATH = os.path.join(HERE, "_build", "libdr_oracle.so")
 _lib = None
 

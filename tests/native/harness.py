@@ -23,7 +23,8 @@ def build():
     if os.path.exists(LIB) and all(os.path.getmtime(d) <= os.path.getmtime(LIB) for d in deps):
         return LIB
     os.makedirs(os.path.dirname(LIB), exist_ok=True)
-    subprocess.run(["g++", "-std=c++17", "-O2", "-fPIC", "-shared", "-DDR_HOST_BUILD", "-o", LIB, src],
+    subprocess.run(["g++", "-std=c++17", "-O2", "-ffp-contract=off", "-fPIC", "-shared", "-DDR_HOST_BUILD", "-o", LIB,
+                    src],
                    check=True)
     return LIB
 
@@ -40,6 +41,7 @@ def load():
         L.hh_trace.restype = C.c_longlong
         L.hh_set_proposal.argtypes = [C.c_int, C.c_float]
         L.hh_set_split.argtypes = [C.c_int]
+        L.hh_math.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_longlong]
         _lib = L
     return _lib
 
@@ -81,3 +83,16 @@ def set_proposal(seed, alpha):
 def set_split(on):
     """Walk large traversals in two stages (subtrees handed on at depth 4)."""
     load().hh_set_split(int(bool(on)))
+
+
+MATH_FUNCS = {"sin": 0, "cos": 1, "atan": 2, "atan2": 3, "acos": 4, "exp": 5, "log": 6, "pow": 7}
+
+
+def math_eval(name, x, y=None):
+    """The reproducible transcendental functions (csrc/dr_math.h) on the CPU."""
+    L = load()
+    x = np.ascontiguousarray(x, np.float32)
+    yy = None if y is None else np.ascontiguousarray(np.broadcast_to(np.asarray(y, np.float32), x.shape))
+    out = np.empty_like(x)
+    L.hh_math(MATH_FUNCS[name], x.ctypes.data, None if yy is None else yy.ctypes.data, out.ctypes.data, x.size)
+    return out

@@ -277,4 +277,9 @@ long long hh_trace(const dr_scene_desc *desc, const float *rays, int n, int *out
     return g_dr_visits;
 }
 
+// The reproducible transcendental functions (dr_math.h) on n inputs.
+void hh_math(int fn, const float *x, const float *y, float *out, long long n) {
+    for (long long i = 0; i < n; i++) out[i] = dr_math_eval(fn, x[i], y ? y[i] : 0.f);
+}
+
 }  // extern "C"

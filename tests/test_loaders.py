@@ -12,8 +12,9 @@ import numpy as np
 import pytest
 
 from conftest import ROOT
+from refpath import reference_dir
 
-REF_SCENES = "/root/reference/test/scenes"
+REF_SCENES = os.path.join(reference_dir(), "test", "scenes")
 
 
 def _reference_reader():

@@ -3,7 +3,8 @@ library's fixed per-device scratch array, called through the C ABI and
 compared with dr_render_backward on the same scene, seed and adjoint.
 
 The file name sorts last so that the test also runs after every other GPU
-test in the same process (the scratch set-up happens on first use)."""
+test in the same process, and it passes alone in a fresh process as well
+(scene creation loads the module that holds the scratch array)."""
 import ctypes as C
 
 import numpy as np
@@ -32,10 +33,13 @@ def _scene(res, spp, B, seed=2):
     return Scene(cam, mats, shps, lts, 0, None)
 
 
-def _noalloc(L, sc, W, H, spp, B, seed, d_image):
+def _noalloc(L, sc, W, H, spp, B, seed, d_image, grad=None, img=None):
     from delta_ray_b200 import _abi
-    grad = torch.full((sc.grad_total,), float("nan"), dtype=torch.float32, device="cuda")
-    img = torch.empty((H, W, 3), dtype=torch.float32, device="cuda")
+    if grad is None:
+        grad = torch.empty((sc.grad_total,), dtype=torch.float32, device="cuda")
+    grad.fill_(float("nan"))  # the call must overwrite every entry
+    if img is None:
+        img = torch.empty((H, W, 3), dtype=torch.float32, device="cuda")
     rd = _abi.render_desc(W, H, spp, B, seed)
     st = L.dr_render_backward_noalloc(sc.handle, C.byref(rd), C.c_void_p(d_image.data_ptr()),
                                       C.c_void_p(grad.data_ptr()), C.c_void_p(img.data_ptr()), None)
@@ -56,9 +60,16 @@ def test_noalloc_backward_matches_backward_twice(res, spp, B):
     ref_grad, ref_img = sc.backward(W, H, spp, B, seed, d_image, want_image=True)
     ref_grad = ref_grad.cpu().numpy()
     assert np.abs(ref_grad).max() > 0
-    for _ in range(2):  # two calls in a row reuse the same scratch
-        st, grad, img = _noalloc(L, sc, W, H, spp, B, seed, d_image)
+    grad_buf = torch.empty((sc.grad_total,), dtype=torch.float32, device="cuda")
+    img_buf = torch.empty((H, W, 3), dtype=torch.float32, device="cuda")
+    for k in range(2):  # two calls in a row reuse the same scratch
+        torch.cuda.synchronize()
+        free_before = torch.cuda.mem_get_info()[0]
+        st, grad, img = _noalloc(L, sc, W, H, spp, B, seed, d_image, grad_buf, img_buf)
+        free_after = torch.cuda.mem_get_info()[0]
         assert st == 0, _lib.last_error()
+        # the call takes no device memory: the free memory the driver reports is unchanged
+        assert free_after == free_before, (k, free_before, free_after)
         g = grad.cpu().numpy()
         assert np.isfinite(g).all()
         assert rel_err(g, ref_grad) < TOL
