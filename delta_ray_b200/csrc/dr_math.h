@@ -19,9 +19,8 @@
 //   exp  x = k ln2 + r, |r| <= ln2 / 2 (Cody-Waite: ln2 split into a 33-bit
 //        head and a tail), Taylor series to r^13, then times 2^k.
 //   pow  exp(y log x) for x > 0; integer y for x < 0.
-//   atan reflection atan x = pi/2 - atan(1/x) for |x| > 1, two argument
-//        halvings atan x = 2 atan(x / (1 + sqrt(1 + x^2))) (|x| <= 0.199),
-//        series to x^25.
+//   atan table reduction atan x = k pi/32 + atan((x - c) / (1 + x c)),
+//        c = tan(k pi/32), |t| <= tan(pi/64); series to t^15.
 //   atan2, acos  from atan (acos x = 2 atan(sqrt((1 - x) / (1 + x)))).
 //   sin, cos  x = k pi/2 + r (Cody-Waite, 33-bit head of pi/2), |r| <= pi/4,
 //        Taylor series to r^17 / r^16; meant for |x| < 2^20.
@@ -156,22 +155,27 @@ DRM_FN double exp_d(double x) {
     return scale2(p, (int)k);
 }
 
-// arc tangent of a double
-DRM_FN double atan_d(double x) {
-    if (is_nan(x)) return x;
-    bool neg = sign_bit(x);
-    double a = absd(x);
-    bool inv = a > 1.0;
-    if (inv) a = div(1.0, a);
-    a = div(a, add(1.0, root(add(1.0, mul(a, a)))));
-    a = div(a, add(1.0, root(add(1.0, mul(a, a)))));
-    double z = mul(a, a);
-    double p = 0.04;
-    p = add(mul(p, z), -0.043478260869565216);
-    p = add(mul(p, z), 0.047619047619047616);
-    p = add(mul(p, z), -0.05263157894736842);
-    p = add(mul(p, z), 0.058823529411764705);
-    p = add(mul(p, z), -0.06666666666666667);
+// Tables of the arc tangent's argument reduction: c_k = tan(k pi/32) and
+// k pi/32, k = 0..15, rounded to double.
+#define DRM_ATAN_C {0.0, 0.09849140335716425, 0.198912367379658, 0.3033466836073424, 0.41421356237309503, \
+                    0.5345111359507917, 0.6681786379192989, 0.8206787908286604, 1.0, 1.2185035255879764, \
+                    1.496605762665489, 1.8708684117893895, 2.414213562373095, 3.2965582089383205, \
+                    5.027339492125848, 10.15317038760886}
+#define DRM_ATAN_A {0.0, 0.09817477042468103, 0.19634954084936207, 0.2945243112740431, 0.39269908169872414, \
+                    0.4908738521234052, 0.5890486225480862, 0.6872233929727672, 0.7853981633974483, \
+                    0.8835729338221293, 0.9817477042468103, 1.0799224746714915, 1.1780972450961724, \
+                    1.2762720155208536, 1.3744467859455345, 1.4726215563702156}
+#if defined(__CUDACC__)
+static __device__ const double drm_atan_c_dev[16] = DRM_ATAN_C;
+static __device__ const double drm_atan_a_dev[16] = DRM_ATAN_A;
+#endif
+static const double drm_atan_c_host[16] = DRM_ATAN_C;
+static const double drm_atan_a_host[16] = DRM_ATAN_A;
+
+// atan t for |t| <= 0.055, series to t^15
+DRM_FN double atan_series(double t) {
+    double z = mul(t, t);
+    double p = -0.06666666666666667;
     p = add(mul(p, z), 0.07692307692307693);
     p = add(mul(p, z), -0.09090909090909091);
     p = add(mul(p, z), 0.1111111111111111);
@@ -179,8 +183,33 @@ DRM_FN double atan_d(double x) {
     p = add(mul(p, z), 0.2);
     p = add(mul(p, z), -0.3333333333333333);
     p = add(mul(p, z), 1.0);
-    double r = mul(4.0, mul(a, p));
-    if (inv) r = sub(kPio2, r);
+    return mul(t, p);
+}
+
+// arc tangent of a double: atan a = k pi/32 + atan((a - c_k) / (1 + a c_k))
+// with k the nearest multiple (16 comparisons against tan((2k + 1) pi/64)),
+// so that |t| <= tan(pi/64); a > tan(31 pi/64) as pi/2 - atan(1/a).
+DRM_FN double atan_d(double x) {
+    if (is_nan(x)) return x;
+    bool neg = sign_bit(x);
+    double a = absd(x);
+    double r;
+    if (a > 20.355467624987188) {
+        r = sub(kPio2, atan_series(div(1.0, a)));
+    } else {
+        int k = (a > 0.049126849769467254) + (a > 0.14833598753834742) + (a > 0.25048696019130545) +
+                (a > 0.3578057213145241) + (a > 0.4729647758913199) + (a > 0.5993769336819238) +
+                (a > 0.7416505462720354) + (a > 0.9063471690191471) + (a > 1.1033299757334756) +
+                (a > 1.3483439134867201) + (a > 1.668399205583507) + (a > 2.1143223575486405) +
+                (a > 2.7948127724904768) + (a > 3.9922237837700845) + (a > 6.7414524054149885);
+#ifdef __CUDA_ARCH__
+        double c = __ldg(&drm_atan_c_dev[k]), ang = __ldg(&drm_atan_a_dev[k]);
+#else
+        double c = drm_atan_c_host[k], ang = drm_atan_a_host[k];
+#endif
+        double t = div(sub(a, c), add(1.0, mul(a, c)));
+        r = add(ang, atan_series(t));
+    }
     return neg ? -r : r;
 }
 

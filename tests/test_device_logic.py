@@ -9,7 +9,7 @@ CPU build is test infrastructure only: the product never runs it.
 import numpy as np
 import pytest
 
-from conftest import build_golden_scene, golden_cases, load_golden, rel_err
+from conftest import assert_grad_parity, assert_image_parity, build_golden_scene, golden_cases, load_golden, rel_err
 import oracle
 from native import harness
 
@@ -30,7 +30,7 @@ def test_kernel_logic_matches_oracle(case, ltc_table):
     seed = meta["seed"]
     h = harness.render(wl, seed, ltc_table=ltc_table)
     o = oracle.oracle_render(wl, seed, rng_mode=oracle.PHILOX, ltc_table=ltc_table)
-    assert rel_err(h["image"], o["image"]) < TOL
+    assert_image_parity(h["image"], o["image"])
     for parts in (1, 2, 4):
         h = harness.render(wl, seed, gold["d_image"], parts=parts, ltc_table=ltc_table)
         o = oracle.oracle_render(wl, seed, gold["d_image"], rng_mode=oracle.PHILOX, ltc_table=ltc_table,
@@ -40,7 +40,7 @@ def test_kernel_logic_matches_oracle(case, ltc_table):
         if np.abs(o["grad"]).max() == 0:
             assert np.abs(h["grad"]).max() == 0
         else:
-            assert rel_err(h["grad"], o["grad"]) < CASE_TOL.get(case, TOL), f"gradient term {parts}"
+            assert_grad_parity(h["grad"], o["grad"], what=f"gradient term {parts}")
 
 
 def test_dp_sum_mode_matches_oracle(ltc_table):

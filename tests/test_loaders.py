@@ -188,10 +188,10 @@ def test_mitsuba_scene_gpu_matches_oracle(tmp_path):
     """A loaded scene on the CUDA library, forward and backward, against the
     oracle on the same Philox streams."""
     import oracle
-    from conftest import rel_err
     from delta_ray_b200.loaders import load_mitsuba
     from delta_ray_b200.workloads import Workload
-    from test_forward_gpu import pixel_mismatch, product_scene
+    from conftest import assert_grad_parity, assert_image_parity
+    from test_forward_gpu import product_scene
     import torch
     cam, materials, shapes, lights, res = load_mitsuba(_write_scene(tmp_path))
     wl = Workload("mitsuba", cam, materials, shapes, lights, res, 4, 1)
@@ -200,6 +200,6 @@ def test_mitsuba_scene_gpu_matches_oracle(tmp_path):
     img = sc.forward(W, H, 4, 1, 3).cpu().numpy()
     grad, _ = sc.backward(W, H, 4, 1, 3, torch.ones((H, W, 3), device="cuda"))
     o = oracle.oracle_render(wl, 3, np.ones((H, W, 3), np.float32), rng_mode=oracle.PHILOX)
-    assert pixel_mismatch(img, o["image"]).mean() <= 0.01
-    assert rel_err(grad.cpu().numpy(), o["grad"]) < 2e-3
+    assert_image_parity(img, o["image"])
+    assert_grad_parity(grad.cpu().numpy(), o["grad"])
     sc.close()
