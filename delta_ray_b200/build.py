@@ -23,7 +23,8 @@ ARCH = ["-gencode", "arch=compute_100a,code=sm_100a"]
 # as the CPU does.  Only the learned proposal's network (dr_mlp.cu), whose
 # output is a sampling weight, is contracted.
 NO_FMA = ["-fmad=false"]
-PER_FILE_FLAGS = {"dr_backward.cu": NO_FMA, "dr_edge_kernels.cu": NO_FMA, "dr_kernels.cu": NO_FMA}
+PER_FILE_FLAGS = {"dr_backward.cu": NO_FMA, "dr_edge_kernels.cu": NO_FMA, "dr_kernels.cu": NO_FMA,
+                  "dr_scene_build.cu": NO_FMA}
 NVCC_FLAGS = ["-O3", "-lineinfo", "-std=c++17", "--expt-relaxed-constexpr", "-Xcompiler", "-fPIC",
               "-Xcompiler", "-ffp-contract=off",
               "-Xcompiler", "-fvisibility=hidden", "-I", os.path.join(ROOT, "include")]

@@ -17,6 +17,7 @@
 #include <cstring>
 #include <map>
 #include <memory>
+#include <chrono>
 #include <mutex>
 #include <random>
 #include <stdexcept>
@@ -181,6 +182,17 @@ struct dr_scene {
     long long last_points = 0, last_items = 0;
     int num_vertices = 0, num_tris = 0, num_sms = 148;
     int bvh_built_tris = 0;  // triangle count of the LBVH topology kept in bvh_scratch
+    // scenes of more than kGpuEdgeTris triangles build their edges, edge trees
+    // and primary-edge sampler on the GPU (dr_scene_build.cu): the unique
+    // edges (kept while the triangle indices stay the same), the working
+    // lists and scratch, and the arena of the results
+    bool gpu_edges = false;
+    DevBuf edge_topo, edge_lists, edge_scratch, edge_arena;
+    int topo_count = 0;
+    bool topo_dev_valid = false;
+    const DevEdge *kept_dev = nullptr;
+    int num_kept = 0;
+    float edge_build_ms = 0.f;  // host wall time of the last edge build (tooling)
     ~dr_scene() {
         if (timer_ready)
             for (int i = 0; i <= StageTimer::kMax; i++) cudaEventDestroy(timer.ev[i]);
@@ -242,6 +254,8 @@ void upload_arena(DevBuf &arena, const ArenaLayout &lay, cudaStream_t st) {
     // the staging buffer is reused by the next upload
     check_cuda(cudaStreamSynchronize(st), "scene upload");
 }
+
+void build_edges_gpu(dr_scene *sc, cudaStream_t st);
 
 void upload_scene(dr_scene *sc, cudaStream_t st, bool refit = false) {
     HostScene &h = sc->h;
@@ -335,6 +349,105 @@ void upload_scene(dr_scene *sc, cudaStream_t st, bool refit = false) {
     ptr.ltc = sc->ltc->as<float>();
     ptr.ltc_ggx = sc->ltc_ggx->as<float>();
     fill_devscene(sc->ds, h, f, ptr);
+    if (sc->gpu_edges) build_edges_gpu(sc, st);
+}
+
+// Edges of a flattened tree: the last node in depth-first order is a leaf
+// whose range ends at the edge count.
+size_t edge_count_of(const dr_scene *scene, const DevEdgeNode *nodes, int num_nodes) {
+    (void)scene;
+    DevEdgeNode last;
+    check_cuda(cudaMemcpy(&last, nodes + (num_nodes - 1), sizeof(last), cudaMemcpyDeviceToHost), "tree read");
+    return (size_t)last.offset + (size_t)last.nprims;
+}
+
+// Scenes of more than this many triangles build their edge data on the GPU.
+constexpr int kGpuEdgeTris = 8192;
+
+// The edge data of a large scene on the GPU (dr_scene_build.cu): unique
+// edges, the kept / silhouette / normal sets, both edge trees and the
+// primary-edge sampler.  Trees of at most DR_TREE_EXACT_MAX_EDGES edges
+// follow the reference's split rule and are built on the host from the
+// GPU's edge lists (cheap at that size); larger ones on the GPU.
+void build_edges_gpu(dr_scene *sc, cudaStream_t st) {
+    auto t0 = std::chrono::steady_clock::now();
+    HostScene &h = sc->h;
+    DevScene &ds = sc->ds;
+    const int T = sc->num_tris;
+    sc->edge_scratch.reserve(dr_edges_scratch_bytes(T));
+    if (!sc->topo_dev_valid) {
+        sc->edge_topo.reserve(sizeof(DevEdge) * 3 * (size_t)std::max(1, T));
+        check_cuda(dr_extract_edges(ds, sc->num_vertices, sc->edge_topo.as<DevEdge>(), &sc->topo_count,
+                                    sc->edge_scratch.p, sc->edge_scratch.bytes, st, &sc->last_launches),
+                   "edge extraction");
+        sc->topo_dev_valid = true;
+    }
+    const int nt = sc->topo_count;
+    sc->edge_lists.reserve(sizeof(DevEdge) * 3 * (size_t)std::max(1, nt));
+    DevEdge *kept = sc->edge_lists.as<DevEdge>(), *sil = kept + nt, *nrm = sil + nt;
+    int cnt[3];
+    check_cuda(dr_split_edges(ds, sc->edge_topo.as<DevEdge>(), nt, kept, sil, nrm, cnt, sc->edge_scratch.p,
+                              sc->edge_scratch.bytes, st, &sc->last_launches),
+               "edge split");
+    const int nk = cnt[0], ns = cnt[1], nn = cnt[2];
+    const bool gs = ns > DR_TREE_EXACT_MAX_EDGES, gn = nn > DR_TREE_EXACT_MAX_EDGES;
+    std::vector<DevEdgeNode> hs_nodes, hn_nodes;
+    std::vector<DevEdge> hs_edges, hn_edges;
+    auto host_tree = [&](const DevEdge *src, int n, bool dir, std::vector<DevEdgeNode> &nodes,
+                         std::vector<DevEdge> &ordered) {
+        std::vector<DevEdge> list(n);
+        if (n)
+            check_cuda(cudaMemcpy(list.data(), src, sizeof(DevEdge) * n, cudaMemcpyDeviceToHost), "edge download");
+        if (dir) h.build_tree<true>(list, nodes, ordered);
+        else h.build_tree<false>(list, nodes, ordered);
+    };
+    if (!gs) host_tree(sil, ns, false, hs_nodes, hs_edges);
+    if (!gn) host_tree(nrm, nn, true, hn_nodes, hn_edges);
+    // kept | silhouette edges | normal edges | silhouette nodes | normal nodes | primary edges | cdf | func
+    ArenaLayout lay;
+    const size_t o_kept = lay.space(sizeof(DevEdge) * (size_t)nk);
+    const size_t o_se = gs ? lay.space(sizeof(DevEdge) * (size_t)ns) : lay.add(hs_edges);
+    const size_t o_ne = gn ? lay.space(sizeof(DevEdge) * (size_t)nn) : lay.add(hn_edges);
+    const size_t o_sn = gs ? lay.space(sizeof(DevEdgeNode) * 2 * (size_t)ns) : lay.add(hs_nodes);
+    const size_t o_nn = gn ? lay.space(sizeof(DevEdgeNode) * 2 * (size_t)nn) : lay.add(hn_nodes);
+    const size_t o_prim = lay.space(sizeof(DevEdge) * (size_t)nk), o_cdf = lay.space(sizeof(float) * (nk + 1)),
+                 o_func = lay.space(sizeof(float) * (size_t)nk);
+    upload_arena(sc->edge_arena, lay, st);
+    char *b = (char *)sc->edge_arena.p;
+    if (nk)
+        check_cuda(cudaMemcpyAsync(b + o_kept, kept, sizeof(DevEdge) * nk, cudaMemcpyDeviceToDevice, st),
+                   "kept edges");
+    int n_sn = (int)hs_nodes.size(), n_nn = (int)hn_nodes.size();
+    if (gs || gn) sc->edge_scratch.reserve(std::max(sc->edge_scratch.bytes, dr_tree_scratch_bytes(std::max(ns, nn))));
+    if (gs)
+        check_cuda(dr_build_edge_tree(ds, false, sil, ns, (DevEdgeNode *)(b + o_sn), (DevEdge *)(b + o_se), &n_sn,
+                                      sc->edge_scratch.p, sc->edge_scratch.bytes, st, &sc->last_launches),
+                   "silhouette edge tree");
+    if (gn)
+        check_cuda(dr_build_edge_tree(ds, true, nrm, nn, (DevEdgeNode *)(b + o_nn), (DevEdge *)(b + o_ne), &n_nn,
+                                      sc->edge_scratch.p, sc->edge_scratch.bytes, st, &sc->last_launches),
+                   "normal edge tree");
+    int np = 0;
+    float fi = 0.f;
+    check_cuda(dr_build_primary(ds, ds.cam, (const DevEdge *)(b + o_kept), nk, (DevEdge *)(b + o_prim),
+                                (float *)(b + o_cdf), (float *)(b + o_func), &np, &fi, sc->edge_scratch.p,
+                                sc->edge_scratch.bytes, st, &sc->last_launches),
+               "primary-edge sampler");
+    sc->kept_dev = (const DevEdge *)(b + o_kept);
+    sc->num_kept = nk;
+    ds.prim_edges = (const DevEdge *)(b + o_prim);
+    ds.num_prim_edges = np;
+    ds.prim_cdf = (const float *)(b + o_cdf);
+    ds.prim_func = (const float *)(b + o_func);
+    ds.prim_func_int = fi;
+    ds.sil_nodes = (const DevEdgeNode *)(b + o_sn);
+    ds.sil_edges = (const DevEdge *)(b + o_se);
+    ds.num_sil_nodes = ns ? n_sn : 0;
+    ds.nrm_nodes = (const DevEdgeNode *)(b + o_nn);
+    ds.nrm_edges = (const DevEdge *)(b + o_ne);
+    ds.num_nrm_nodes = nn ? n_nn : 0;
+    sc->edge_build_ms =
+        std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
 }
 
 // Shared-memory gradient cache of the backward kernels: everything when the
@@ -610,7 +723,10 @@ dr_status dr_scene_create(const dr_scene_desc *desc, int device, dr_scene **out)
         sc->device = device;
         check_cuda(cudaDeviceGetAttribute(&sc->num_sms, cudaDevAttrMultiProcessorCount, device), "device query");
         load_desc(sc->h, desc, [](auto p, size_t n, const char *w) { return fetch(p, n, w); });
-        sc->h.preprocess();
+        long long ntri = 0;
+        for (auto &sh : sc->h.shapes) ntri += sh.nt;
+        sc->gpu_edges = ntri > kGpuEdgeTris;
+        sc->h.preprocess(!sc->gpu_edges);
         sc->last_launches = 0;
         upload_scene(sc.get(), 0);
         // loads the module holding the no-alloc backward's scratch array now,
@@ -644,7 +760,8 @@ dr_status dr_scene_update(dr_scene *scene, const dr_scene_desc *desc) {
             scene->h.topo_edges = std::move(topo);
             scene->h.topo_valid = true;
         }
-        scene->h.preprocess();
+        if (!same_indices) scene->topo_dev_valid = false;
+        scene->h.preprocess(!scene->gpu_edges);
         scene->last_launches = 0;
         upload_scene(scene, 0, same_indices);
     });
@@ -804,10 +921,33 @@ dr_status dr_render_backward_views(dr_scene *scene, int n_views, const dr_view_d
             // the view's primary-edge sampler (the previous view's kernels have finished)
             std::vector<DevEdge> pe;
             HDist pd;
-            scene->h.primary_for(hc, pe, pd);
-            scene->view_prim_edges.upload(pe);
-            scene->view_prim_cdf.upload(pd.cdf);
-            scene->view_prim_func.upload(pd.func);
+            int n_prim = 0;
+            float prim_func_int = 0.f;
+            if (scene->gpu_edges) {
+                DevCamera dc;
+                std::memcpy(dc.c2w.m, hc.c2w, 64);
+                std::memcpy(dc.w2c.m, hc.w2c, 64);
+                dc.fov = hc.fov;
+                dc.aspect = hc.aspect;
+                dc.clip_near = hc.clip_near;
+                dc.fisheye = hc.fisheye;
+                const int nk = scene->num_kept;
+                scene->view_prim_edges.reserve(sizeof(DevEdge) * std::max(1, nk));
+                scene->view_prim_cdf.reserve(sizeof(float) * (nk + 1));
+                scene->view_prim_func.reserve(sizeof(float) * std::max(1, nk));
+                check_cuda(dr_build_primary(scene->ds, dc, scene->kept_dev, nk, scene->view_prim_edges.as<DevEdge>(),
+                                            scene->view_prim_cdf.as<float>(), scene->view_prim_func.as<float>(),
+                                            &n_prim, &prim_func_int, scene->edge_scratch.p, scene->edge_scratch.bytes,
+                                            st, &scene->last_launches),
+                           "view primary-edge sampler");
+            } else {
+                scene->h.primary_for(hc, pe, pd);
+                scene->view_prim_edges.upload(pe);
+                scene->view_prim_cdf.upload(pd.cdf);
+                scene->view_prim_func.upload(pd.func);
+                n_prim = (int)pe.size();
+                prim_func_int = pd.func_int;
+            }
             DevScene ds = call_scene(scene, &vw.render);
             std::memcpy(ds.cam.c2w.m, hc.c2w, 64);
             std::memcpy(ds.cam.w2c.m, hc.w2c, 64);
@@ -816,10 +956,10 @@ dr_status dr_render_backward_views(dr_scene *scene, int n_views, const dr_view_d
             ds.cam.clip_near = hc.clip_near;
             ds.cam.fisheye = hc.fisheye;
             ds.prim_edges = scene->view_prim_edges.as<DevEdge>();
-            ds.num_prim_edges = (int)pe.size();
+            ds.num_prim_edges = n_prim;
             ds.prim_cdf = scene->view_prim_cdf.as<float>();
             ds.prim_func = scene->view_prim_func.as<float>();
-            ds.prim_func_int = pd.func_int;
+            ds.prim_func_int = prim_func_int;
             backward_on_queues(scene, &vw.render, &ds, vw.d_image, vg, vw.image, st);
             points += scene->last_points;
             items += scene->last_items;
@@ -1014,6 +1154,45 @@ dr_status dr_scene_last_counts(const dr_scene *scene, int64_t *points, int64_t *
         if (!scene || !points || !items) throw DrError(DR_ERR_INVALID_ARGUMENT, "NULL argument");
         *points = scene->last_points;
         *items = scene->last_items;
+    });
+}
+
+dr_status dr_scene_edge_data(const dr_scene *scene, int what, void *out_host, int64_t capacity_bytes,
+                             int64_t *count, float *build_ms) {
+    return guard([&]() {
+        if (!scene || !count) throw DrError(DR_ERR_INVALID_ARGUMENT, "NULL argument");
+        const DevScene &ds = scene->ds;
+        const void *src = nullptr;
+        size_t elem = 0, n = 0;
+        switch (what) {
+        case 0: src = ds.sil_nodes; elem = sizeof(DevEdgeNode); n = ds.num_sil_nodes; break;
+        case 1:
+            src = ds.sil_edges;
+            elem = sizeof(DevEdge);
+            n = ds.num_sil_nodes ? edge_count_of(scene, ds.sil_nodes, ds.num_sil_nodes) : 0;
+            break;
+        case 2: src = ds.nrm_nodes; elem = sizeof(DevEdgeNode); n = ds.num_nrm_nodes; break;
+        case 3:
+            src = ds.nrm_edges;
+            elem = sizeof(DevEdge);
+            n = ds.num_nrm_nodes ? edge_count_of(scene, ds.nrm_nodes, ds.num_nrm_nodes) : 0;
+            break;
+        case 4: src = ds.prim_edges; elem = sizeof(DevEdge); n = ds.num_prim_edges; break;
+        case 5: src = ds.prim_cdf; elem = 4; n = ds.num_prim_edges ? ds.num_prim_edges + 1 : 0; break;
+        case 6: src = ds.prim_func; elem = 4; n = ds.num_prim_edges; break;
+        case 7: break;
+        default: throw DrError(DR_ERR_INVALID_ARGUMENT, "no such edge array");
+        }
+        *count = what == 7 ? 1 : (int64_t)n;
+        if (build_ms) *build_ms = scene->gpu_edges ? scene->edge_build_ms : 0.f;
+        if (!out_host || capacity_bytes <= 0) return;
+        check_cuda(cudaSetDevice(scene->device), "cudaSetDevice");
+        if (what == 7) {
+            if (capacity_bytes >= 4) std::memcpy(out_host, &ds.prim_func_int, 4);
+            return;
+        }
+        size_t bytes = std::min((size_t)capacity_bytes, elem * n);
+        if (bytes) check_cuda(cudaMemcpy(out_host, src, bytes, cudaMemcpyDeviceToHost), "edge data copy");
     });
 }
 

@@ -20,6 +20,7 @@
 #include <string>
 
 #include "../../include/delta_ray_b200.h"
+#include "dr_edge_rules.h"
 #include "dr_scene.cuh"
 
 namespace drhost {
@@ -47,13 +48,26 @@ inline float get(V3 a, int i) { return i == 0 ? a.x : (i == 1 ? a.y : a.z); }
 inline void set(V3 &a, int i, float v) { if (i == 0) a.x = v; else if (i == 1) a.y = v; else a.z = v; }
 inline float luminance(V3 a) { return 0.212671f * a.x + 0.715160f * a.y + 0.072169f * a.z; }
 
+// Total order of floats (-0 before +0), the order of the GPU build's radix
+// sort keys and atomic min / max: boxes and splits built with it do not
+// depend on the order in which values are combined.
+inline float tmin(float a, float b) { return edge_ord_key(b) < edge_ord_key(a) ? b : a; }
+inline float tmax(float a, float b) { return edge_ord_key(b) > edge_ord_key(a) ? b : a; }
+
 struct HAABB {
     V3 lo{INFINITY, INFINITY, INFINITY}, hi{-INFINITY, -INFINITY, -INFINITY};
+    // std::min / std::max, as the reference
     void add(V3 p) {
         lo = v3(std::min(lo.x, p.x), std::min(lo.y, p.y), std::min(lo.z, p.z));
         hi = v3(std::max(hi.x, p.x), std::max(hi.y, p.y), std::max(hi.z, p.z));
     }
     void add(const HAABB &b) { add(b.lo); add(b.hi); }
+    // in the total order (the product's split rule for large trees)
+    void add_t(V3 p) {
+        lo = v3(tmin(lo.x, p.x), tmin(lo.y, p.y), tmin(lo.z, p.z));
+        hi = v3(tmax(hi.x, p.x), tmax(hi.y, p.y), tmax(hi.z, p.z));
+    }
+    void add_t(const HAABB &b) { add_t(b.lo); add_t(b.hi); }
 };
 
 struct HCam {
@@ -165,21 +179,44 @@ struct BuildNode {
 
 struct HostScene;
 
-// edge_tree.cpp:49-173 (median split; std::nth_element with the same
-// comparator so that equal centroids resolve as in the reference).  A leaf
-// covers pi[start, end): leaves in depth-first order cover pi in order, so the
-// edges are laid out as pi once the tree is built.  The two halves of a
-// large node are built on two threads (disjoint ranges of pi; the result is
-// the serial one).
-template <bool DIR>
+// The edge trees' median split (edge_tree.cpp:49-173).  Trees of at most
+// DR_TREE_EXACT_MAX_EDGES edges follow the reference exactly: std::nth_element
+// with the same comparator (equal centroids resolve as in the reference),
+// float normal sums in range order, std::min / std::max boxes.  Larger trees
+// follow the product's rule (PRODUCT), which the GPU build (dr_scene_build.cu)
+// reproduces bit for bit:
+//  - a node's range is ordered by a stable sort on the split coordinate's
+//    total-order key (edge_ord_key) and split at its middle (the same two
+//    halves as nth_element except where edges share the median coordinate);
+//  - the cone axis's normal sum is exact: fixed point (edge_fixed), converted
+//    to float once;
+//  - boxes take total-order minima and maxima (-0 below +0).
+// A leaf covers pi[start, end): leaves in depth-first order cover pi in
+// order, so the edges are laid out as pi once the tree is built.  The two
+// halves of a large node are built on two threads (disjoint ranges of pi; the
+// result is the serial one).
+template <bool DIR, bool PRODUCT>
 std::unique_ptr<BuildNode> build_node(std::vector<PrimInfo> &pi, int start, int end, std::atomic<int> *total,
                                       int depth) {
     auto node = std::make_unique<BuildNode>();
     total->fetch_add(1, std::memory_order_relaxed);
     HAABB sb;
-    for (int i = start; i < end; i++) sb.add(pi[i].sb);
+    for (int i = start; i < end; i++) {
+        if (PRODUCT) sb.add_t(pi[i].sb);
+        else sb.add(pi[i].sb);
+    }
     V3 nsum = v3(0.f, 0.f, 0.f);
-    for (int i = start; i < end; i++) nsum = nsum + pi[i].n0 + pi[i].n1;
+    if (PRODUCT) {
+        long long fs[3] = {0, 0, 0};
+        for (int i = start; i < end; i++) {
+            fs[0] += edge_fixed(pi[i].n0.x) + edge_fixed(pi[i].n1.x);
+            fs[1] += edge_fixed(pi[i].n0.y) + edge_fixed(pi[i].n1.y);
+            fs[2] += edge_fixed(pi[i].n0.z) + edge_fixed(pi[i].n1.z);
+        }
+        nsum = v3(edge_unfixed(fs[0]), edge_unfixed(fs[1]), edge_unfixed(fs[2]));
+    } else {
+        for (int i = start; i < end; i++) nsum = nsum + pi[i].n0 + pi[i].n1;
+    }
     V3 axis = normalize(nsum);
     float cmin = 1.f;
     for (int i = start; i < end; i++) {
@@ -200,39 +237,40 @@ std::unique_ptr<BuildNode> build_node(std::vector<PrimInfo> &pi, int start, int 
     }
     HAABB scb, dcb;
     for (int i = start; i < end; i++) {
-        scb.add(pi[i].sc);
-        if (DIR) dcb.add(pi[i].dc);
-    }
-    int dim = -1;
-    float maxe = -INFINITY;
-    for (int a = 0; a < 3; a++) {
-        float e = get(scb.hi, a) - get(scb.lo, a);
-        if (e > maxe) { dim = a; maxe = e; }
-    }
-    if (DIR) {
-        for (int a = 0; a < 3; a++) {
-            float e = get(dcb.hi, a) - get(dcb.lo, a);
-            if (e > maxe) { dim = a + 3; maxe = e; }
+        if (PRODUCT) {
+            scb.add_t(pi[i].sc);
+            if (DIR) dcb.add_t(pi[i].dc);
+        } else {
+            scb.add(pi[i].sc);
+            if (DIR) dcb.add(pi[i].dc);
         }
     }
-    const HAABB &cb = dim < 3 ? scb : dcb;
-    bool spatial = dim < 3;
-    if (dim >= 3) dim -= 3;
-    if (get(cb.hi, dim) == get(cb.lo, dim)) {
+    int dim = edge_split_dim(scb.lo.x, scb.lo.y, scb.lo.z, scb.hi.x, scb.hi.y, scb.hi.z, DIR, dcb.lo.x, dcb.lo.y,
+                             dcb.lo.z, dcb.hi.x, dcb.hi.y, dcb.hi.z);
+    if (dim < 0) {
         leaf();
         return node;
     }
+    bool spatial = dim < 3;
+    int d = spatial ? dim : dim - 3;
     int mid = (start + end) / 2;
-    std::nth_element(&pi[start], &pi[mid], &pi[end - 1] + 1, [dim, spatial](const PrimInfo &a, const PrimInfo &b) {
-        return spatial ? get(a.sc, dim) < get(b.sc, dim) : get(a.dc, dim) < get(b.dc, dim);
-    });
+    if (PRODUCT) {
+        std::stable_sort(pi.begin() + start, pi.begin() + end, [d, spatial](const PrimInfo &a, const PrimInfo &b) {
+            return spatial ? edge_ord_key(get(a.sc, d)) < edge_ord_key(get(b.sc, d))
+                           : edge_ord_key(get(a.dc, d)) < edge_ord_key(get(b.dc, d));
+        });
+    } else {
+        std::nth_element(&pi[start], &pi[mid], &pi[end - 1] + 1, [d, spatial](const PrimInfo &a, const PrimInfo &b) {
+            return spatial ? get(a.sc, d) < get(b.sc, d) : get(a.dc, d) < get(b.dc, d);
+        });
+    }
     if (n >= 16384 && depth < 4) {
-        std::thread left([&]() { node->c[0] = build_node<DIR>(pi, start, mid, total, depth + 1); });
-        node->c[1] = build_node<DIR>(pi, mid, end, total, depth + 1);
+        std::thread left([&]() { node->c[0] = build_node<DIR, PRODUCT>(pi, start, mid, total, depth + 1); });
+        node->c[1] = build_node<DIR, PRODUCT>(pi, mid, end, total, depth + 1);
         left.join();
     } else {
-        node->c[0] = build_node<DIR>(pi, start, mid, total, depth + 1);
-        node->c[1] = build_node<DIR>(pi, mid, end, total, depth + 1);
+        node->c[0] = build_node<DIR, PRODUCT>(pi, start, mid, total, depth + 1);
+        node->c[1] = build_node<DIR, PRODUCT>(pi, mid, end, total, depth + 1);
     }
     return node;
 }
@@ -318,17 +356,24 @@ struct HostScene {
         nodes.clear();
         ordered.clear();
         if (edges.empty()) return;
+        const bool product = edges.size() > (size_t)DR_TREE_EXACT_MAX_EDGES;
         std::vector<PrimInfo> pi(edges.size());
         HAABB world;
         for (size_t i = 0; i < edges.size(); i++) {
             HAABB b;
-            b.add(ev0(edges[i]));
-            b.add(ev1(edges[i]));
+            if (product) {
+                b.add_t(ev0(edges[i]));
+                b.add_t(ev1(edges[i]));
+            } else {
+                b.add(ev0(edges[i]));
+                b.add(ev1(edges[i]));
+            }
             pi[i].prim = (int)i;
             pi[i].sb = b;
             pi[i].sc = 0.5f * b.lo + 0.5f * b.hi;
             pi[i].n0 = pi[i].n1 = v3(0.f, 0.f, 0.f);
-            world.add(b);
+            if (product) world.add_t(b);
+            else world.add(b);
         }
         if (DIR) {
             float factor = length(world.hi - world.lo) / 8.f;
@@ -342,14 +387,20 @@ struct HostScene {
                 pi[i].n0 = n0;
                 pi[i].n1 = n1;
                 HAABB d;
-                d.add(n0 * factor);
-                d.add(n1 * factor);
+                if (product) {
+                    d.add_t(n0 * factor);
+                    d.add_t(n1 * factor);
+                } else {
+                    d.add(n0 * factor);
+                    d.add(n1 * factor);
+                }
                 pi[i].db = d;
                 pi[i].dc = 0.5f * (d.lo + d.hi);
             }
         }
         std::atomic<int> total(0);
-        auto root = build_node<DIR>(pi, 0, (int)edges.size(), &total, 0);
+        auto root = product ? build_node<DIR, true>(pi, 0, (int)edges.size(), &total, 0)
+                            : build_node<DIR, false>(pi, 0, (int)edges.size(), &total, 0);
         ordered.resize(edges.size());
         for (size_t i = 0; i < edges.size(); i++) ordered[i] = edges[pi[i].prim];
         nodes.resize(total.load());
@@ -381,7 +432,13 @@ struct HostScene {
         if (!lens.empty()) pd.build(lens);
     }
 
-    void preprocess() {
+    // lights (light samplers) and, unless the GPU builds them, the edges
+    void preprocess(bool edges = true) {
+        preprocess_lights();
+        if (edges) preprocess_edges();
+    }
+
+    void preprocess_lights() {
         // lights (scene.cpp:26-52)
         std::vector<float> imp;
         total_light_intensity = 0.f;
@@ -420,6 +477,9 @@ struct HostScene {
             light_tri_func.push_back(0.f);  // keep func and cdf offsets aligned (ntri + 1 slots)
         }
         if (!imp.empty()) light_sel.build(imp);
+    }
+
+    void preprocess_edges() {
         // unique edges in (shape, v0, v1) order (scene.cpp:54-97); they depend
         // on the triangle indices only, so an update with new positions reuses them
         if (!topo_valid) {

@@ -35,6 +35,28 @@ size_t dr_lbvh_scratch_bytes(int n);
 cudaError_t dr_refit_lbvh(const float *vtx, const int4 *tri, int n, float4 *nodes, float4 *leaf_tris, void *scratch,
                           size_t scratch_bytes, cudaStream_t st, int *launches);
 
+// GPU build of a scene's edge data (dr_scene_build.cu).  Each call finishes
+// (synchronizes `st`) before it returns its counts.
+// Unique edges (scene.cpp:54-97) into out (capacity 3 * s.num_tris).
+size_t dr_edges_scratch_bytes(int ntri);
+cudaError_t dr_extract_edges(const DevScene &s, int num_vertices, DevEdge *out, int *count_host, void *scratch,
+                             size_t scratch_bytes, cudaStream_t st, int *launches);
+// The kept edges and the silhouette and normal sets (capacity n each);
+// counts_host: kept, silhouette, normal.  Scratch: dr_edges_scratch_bytes.
+cudaError_t dr_split_edges(const DevScene &s, const DevEdge *topo, int n, DevEdge *kept, DevEdge *sil, DevEdge *nrm,
+                           int counts_host[3], void *scratch, size_t scratch_bytes, cudaStream_t st, int *launches);
+// The primary-edge sampler of camera cam over n kept edges: prim (capacity
+// n), cdf (n + 1), func (n).  Scratch: dr_edges_scratch_bytes.
+cudaError_t dr_build_primary(const DevScene &s, const DevCamera &cam, const DevEdge *kept, int n, DevEdge *prim,
+                             float *cdf, float *func, int *count_host, float *func_int_host, void *scratch,
+                             size_t scratch_bytes, cudaStream_t st, int *launches);
+// A median-split edge tree of n edges (the product's rule, dr_edge_rules.h):
+// nodes (capacity 2n - 1) in the flattened layout, the edges in leaf order.
+size_t dr_tree_scratch_bytes(int n);
+cudaError_t dr_build_edge_tree(const DevScene &s, bool dir, const DevEdge *edges, int n, DevEdgeNode *nodes,
+                               DevEdge *ordered, int *num_nodes_host, void *scratch, size_t scratch_bytes,
+                               cudaStream_t st, int *launches);
+
 cudaError_t dr_launch_eval_math(int fn, const float *x, const float *y, float *out, long long n, cudaStream_t st);
 cudaError_t dr_launch_trace(const DevScene &s, const float *rays, long long n, int *tri, float *t, cudaStream_t st,
                             int *launches);

@@ -12,16 +12,14 @@
 // this header are compiled with -ffp-contract=off), in a fixed order, and
 // rounds the double result to float once.
 //
-// Methods (textbook ones, with coefficients that are exact Taylor
+// The arc tangent family (atan, atan2, acos) is evaluated in float, see
+// below.  Methods (textbook ones, with coefficients that are exact Taylor
 // coefficients rounded to double):
 //   log  x = 2^k m, m in [sqrt(1/2), sqrt(2)]; log m = 2 atanh(s),
 //        s = (m - 1) / (m + 1), |s| <= 0.172, series to s^21.
 //   exp  x = k ln2 + r, |r| <= ln2 / 2 (Cody-Waite: ln2 split into a 33-bit
 //        head and a tail), Taylor series to r^13, then times 2^k.
 //   pow  exp(y log x) for x > 0; integer y for x < 0.
-//   atan table reduction atan x = k pi/32 + atan((x - c) / (1 + x c)),
-//        c = tan(k pi/32), |t| <= tan(pi/64); series to t^15.
-//   atan2, acos  from atan (acos x = 2 atan(sqrt((1 - x) / (1 + x)))).
 //   sin, cos  x = k pi/2 + r (Cody-Waite, 33-bit head of pi/2), |r| <= pi/4,
 //        Taylor series to r^17 / r^16; meant for |x| < 2^20.
 // Before the final rounding the relative error is a few units of 2^-52, so
@@ -155,88 +153,6 @@ DRM_FN double exp_d(double x) {
     return scale2(p, (int)k);
 }
 
-// Tables of the arc tangent's argument reduction: c_k = tan(k pi/32) and
-// k pi/32, k = 0..15, rounded to double.
-#define DRM_ATAN_C {0.0, 0.09849140335716425, 0.198912367379658, 0.3033466836073424, 0.41421356237309503, \
-                    0.5345111359507917, 0.6681786379192989, 0.8206787908286604, 1.0, 1.2185035255879764, \
-                    1.496605762665489, 1.8708684117893895, 2.414213562373095, 3.2965582089383205, \
-                    5.027339492125848, 10.15317038760886}
-#define DRM_ATAN_A {0.0, 0.09817477042468103, 0.19634954084936207, 0.2945243112740431, 0.39269908169872414, \
-                    0.4908738521234052, 0.5890486225480862, 0.6872233929727672, 0.7853981633974483, \
-                    0.8835729338221293, 0.9817477042468103, 1.0799224746714915, 1.1780972450961724, \
-                    1.2762720155208536, 1.3744467859455345, 1.4726215563702156}
-#if defined(__CUDACC__)
-static __device__ const double drm_atan_c_dev[16] = DRM_ATAN_C;
-static __device__ const double drm_atan_a_dev[16] = DRM_ATAN_A;
-#endif
-static const double drm_atan_c_host[16] = DRM_ATAN_C;
-static const double drm_atan_a_host[16] = DRM_ATAN_A;
-
-// atan t for |t| <= 0.055, series to t^15
-DRM_FN double atan_series(double t) {
-    double z = mul(t, t);
-    double p = -0.06666666666666667;
-    p = add(mul(p, z), 0.07692307692307693);
-    p = add(mul(p, z), -0.09090909090909091);
-    p = add(mul(p, z), 0.1111111111111111);
-    p = add(mul(p, z), -0.14285714285714285);
-    p = add(mul(p, z), 0.2);
-    p = add(mul(p, z), -0.3333333333333333);
-    p = add(mul(p, z), 1.0);
-    return mul(t, p);
-}
-
-// arc tangent of a double: atan a = k pi/32 + atan((a - c_k) / (1 + a c_k))
-// with k the nearest multiple (16 comparisons against tan((2k + 1) pi/64)),
-// so that |t| <= tan(pi/64); a > tan(31 pi/64) as pi/2 - atan(1/a).
-DRM_FN double atan_d(double x) {
-    if (is_nan(x)) return x;
-    bool neg = sign_bit(x);
-    double a = absd(x);
-    double r;
-    if (a > 20.355467624987188) {
-        r = sub(kPio2, atan_series(div(1.0, a)));
-    } else {
-        int k = (a > 0.049126849769467254) + (a > 0.14833598753834742) + (a > 0.25048696019130545) +
-                (a > 0.3578057213145241) + (a > 0.4729647758913199) + (a > 0.5993769336819238) +
-                (a > 0.7416505462720354) + (a > 0.9063471690191471) + (a > 1.1033299757334756) +
-                (a > 1.3483439134867201) + (a > 1.668399205583507) + (a > 2.1143223575486405) +
-                (a > 2.7948127724904768) + (a > 3.9922237837700845) + (a > 6.7414524054149885);
-#ifdef __CUDA_ARCH__
-        double c = __ldg(&drm_atan_c_dev[k]), ang = __ldg(&drm_atan_a_dev[k]);
-#else
-        double c = drm_atan_c_host[k], ang = drm_atan_a_host[k];
-#endif
-        double t = div(sub(a, c), add(1.0, mul(a, c)));
-        r = add(ang, atan_series(t));
-    }
-    return neg ? -r : r;
-}
-
-// atan2 with the C99 conventions for zeros and infinities
-DRM_FN double atan2_d(double y, double x) {
-    if (is_nan(x) || is_nan(y)) return x + y;
-    bool ny = sign_bit(y), nx = sign_bit(x);
-    double ay = absd(y), ax = absd(x);
-    double r;
-    if (ay == 0.0) {
-        r = nx ? kPi : 0.0;
-    } else if (ax == 0.0) {
-        r = kPio2;
-    } else if (ay == kInf && ax == kInf) {
-        r = nx ? 2.356194490192345 : 0.7853981633974483;
-    } else {
-        r = ay <= ax ? atan_d(div(ay, ax)) : sub(kPio2, atan_d(div(ax, ay)));
-        if (nx) r = sub(kPi, r);
-    }
-    return ny ? -r : r;
-}
-
-DRM_FN double acos_d(double x) {
-    if (is_nan(x) || x > 1.0 || x < -1.0) return kInf - kInf;
-    return mul(2.0, atan_d(root(div(sub(1.0, x), add(1.0, x)))));
-}
-
 // sine and cosine of r, |r| <= pi/4 (+ rounding)
 DRM_FN double sin_poly(double r) {
     double z = mul(r, r);
@@ -309,9 +225,132 @@ DRM_FN double pow_d(double x, double y) {
 
 DRM_FN float dr_sinf(float x) { return (float)drm::sin_d((double)x); }
 DRM_FN float dr_cosf(float x) { return (float)drm::cos_d((double)x); }
-DRM_FN float dr_atanf(float x) { return (float)drm::atan_d((double)x); }
-DRM_FN float dr_atan2f(float y, float x) { return (float)drm::atan2_d((double)y, (double)x); }
-DRM_FN float dr_acosf(float x) { return (float)drm::acos_d((double)x); }
+
+// The arc tangent family in float (the renderer's line samples call atan in
+// their Newton loop and its edge-tree walks call acos and atan per node, so
+// these stay in single precision; every operation is an IEEE float operation
+// without contraction, so the bits are still the same on the GPU and the
+// host).  atan a = k pi/32 + atan t, t = (a - c_k) / (1 + a c_k), with c_k
+// the float nearest tan(k pi/32), k picked by 16 comparisons so that
+// |t| <= ~tan(pi/64), the angle atan(c_k) as a head and a tail float, and the
+// series to t^9; a > ~tan(31 pi/64) as pi/2 - atan(1/a).  Within about 2 ulp.
+namespace drm {
+#define DRM_ATANF_C {0.0f, 0.09849140048027039f, 0.1989123672246933f, 0.3033466935157776f, 0.4142135679721832f, \
+                     0.534511148929596f, 0.6681786179542542f, 0.8206787705421448f, 1.0f, 1.218503475189209f, \
+                     1.4966057538986206f, 1.870868444442749f, 2.4142136573791504f, 3.296558141708374f, \
+                     5.027339458465576f, 10.153170585632324f}
+#define DRM_ATANF_AH {0.0f, 0.09817476570606232f, 0.19634954631328583f, 0.29452431201934814f, \
+                      0.39269909262657166f, 0.49087387323379517f, 0.5890486240386963f, 0.6872233748435974f, \
+                      0.7853981852531433f, 0.8835729360580444f, 0.9817476868629456f, 1.0799224376678467f, \
+                      1.1780972480773926f, 1.2762720584869385f, 1.3744467496871948f, 1.4726215600967407f}
+#define DRM_ATANF_AL {0.0f, 1.8693642189759885e-09f, -5.612990516823402e-09f, 8.32819413432162e-09f, \
+                      -6.148726860999432e-09f, -1.1015669265646011e-08f, -1.5293277755290546e-08f, \
+                      6.007060626700422e-09f, -2.1855694143368964e-08f, -2.2519143882959725e-08f, \
+                      1.4677898008130796e-08f, 4.425970701049664e-08f, 1.0932094340887488e-08f, \
+                      -4.863122882170501e-08f, 3.4977222895804516e-08f, -1.8240424726201354e-09f}
+#if defined(__CUDACC__)
+static __device__ const float drm_atanf_c_dev[16] = DRM_ATANF_C;
+static __device__ const float drm_atanf_ah_dev[16] = DRM_ATANF_AH;
+static __device__ const float drm_atanf_al_dev[16] = DRM_ATANF_AL;
+#endif
+static const float drm_atanf_c_host[16] = DRM_ATANF_C;
+static const float drm_atanf_ah_host[16] = DRM_ATANF_AH;
+static const float drm_atanf_al_host[16] = DRM_ATANF_AL;
+constexpr float kPio2Hf = 1.5707963705062866f, kPio2Lf = -4.371138828673793e-08f;
+constexpr float kPiHf = 3.1415927410125732f, kPiLf = -8.742277657347586e-08f;
+
+#ifdef __CUDA_ARCH__
+DRM_FN float fadd(float a, float b) { return __fadd_rn(a, b); }
+DRM_FN float fsub(float a, float b) { return __fsub_rn(a, b); }
+DRM_FN float fmul(float a, float b) { return __fmul_rn(a, b); }
+DRM_FN float fdiv(float a, float b) { return __fdiv_rn(a, b); }
+DRM_FN float froot(float a) { return __fsqrt_rn(a); }
+DRM_FN uint32_t fbits(float a) { return __float_as_uint(a); }
+DRM_FN float fabs_(float a) { return __uint_as_float(__float_as_uint(a) & 0x7fffffffu); }
+#else
+DRM_FN float fadd(float a, float b) { return a + b; }
+DRM_FN float fsub(float a, float b) { return a - b; }
+DRM_FN float fmul(float a, float b) { return a * b; }
+DRM_FN float fdiv(float a, float b) { return a / b; }
+DRM_FN float froot(float a) { return __builtin_sqrtf(a); }
+DRM_FN uint32_t fbits(float a) {
+    uint32_t b;
+    std::memcpy(&b, &a, 4);
+    return b;
+}
+DRM_FN float fabs_(float a) {
+    uint32_t b = fbits(a) & 0x7fffffffu;
+    float r;
+    std::memcpy(&r, &b, 4);
+    return r;
+}
+#endif
+
+// atan t - t for |t| <= 0.055: t^3 (-1/3 + t^2/5 - t^4/7 + t^6/9)
+DRM_FN float atanf_tail(float t) {
+    float z = fmul(t, t);
+    float q = 0.1111111119389534f;
+    q = fsub(fmul(q, z), 0.1428571492433548f);
+    q = fadd(fmul(q, z), 0.20000000298023224f);
+    q = fsub(fmul(q, z), 0.3333333432674408f);
+    return fmul(fmul(t, z), q);
+}
+// atan of a >= 0 as head + tail (hi + lo), for the callers that add to it
+DRM_FN float atanf_pos(float a) {
+    if (a > 20.355466842651367f) {
+        float t = fdiv(1.f, a);
+        return fadd(kPio2Hf, fsub(kPio2Lf, fadd(t, atanf_tail(t))));
+    }
+    int k = (a > 0.049126848578453064f) + (a > 0.1483359932899475f) + (a > 0.25048696994781494f) +
+            (a > 0.3578057289123535f) + (a > 0.4729647636413574f) + (a > 0.599376916885376f) +
+            (a > 0.7416505217552185f) + (a > 0.9063471555709839f) + (a > 1.1033300161361694f) +
+            (a > 1.3483439683914185f) + (a > 1.6683992147445679f) + (a > 2.1143224239349365f) +
+            (a > 2.7948126792907715f) + (a > 3.9922237396240234f) + (a > 6.741452217102051f);
+#ifdef __CUDA_ARCH__
+    float c = __ldg(&drm_atanf_c_dev[k]), ah = __ldg(&drm_atanf_ah_dev[k]), al = __ldg(&drm_atanf_al_dev[k]);
+#else
+    float c = drm_atanf_c_host[k], ah = drm_atanf_ah_host[k], al = drm_atanf_al_host[k];
+#endif
+    float t = fdiv(fsub(a, c), fadd(1.f, fmul(a, c)));
+    return fadd(ah, fadd(al, fadd(t, atanf_tail(t))));
+}
+}  // namespace drm
+
+DRM_FN float dr_atanf(float x) {
+    if (x != x) return x;
+    float r = drm::atanf_pos(drm::fabs_(x));
+    return (drm::fbits(x) & 0x80000000u) ? -r : r;
+}
+// atan2 with the C99 conventions for zeros and infinities
+DRM_FN float dr_atan2f(float y, float x) {
+    if (x != x || y != y) return x + y;
+    bool ny = (drm::fbits(y) & 0x80000000u) != 0, nx = (drm::fbits(x) & 0x80000000u) != 0;
+    float ay = drm::fabs_(y), ax = drm::fabs_(x);
+    const float inf = __builtin_huge_valf();
+    float r;
+    if (ay == 0.f) {
+        r = nx ? drm::kPiHf : 0.f;
+    } else if (ax == 0.f) {
+        r = drm::kPio2Hf;
+    } else if (ay == inf && ax == inf) {
+        r = nx ? 2.356194496154785f : 0.7853981852531433f;
+    } else {
+        if (ay <= ax) {
+            r = drm::atanf_pos(drm::fdiv(ay, ax));
+        } else {
+            float q = drm::fdiv(ax, ay);
+            r = drm::fadd(drm::kPio2Hf, drm::fsub(drm::kPio2Lf, drm::atanf_pos(q)));
+        }
+        if (nx) r = drm::fadd(drm::kPiHf, drm::fsub(drm::kPiLf, r));
+    }
+    return ny ? -r : r;
+}
+// acos x = 2 atan(sqrt((1 - x) / (1 + x)))
+DRM_FN float dr_acosf(float x) {
+    if (x != x || x > 1.f || x < -1.f) return __builtin_nanf("");
+    if (x == -1.f) return drm::kPiHf;
+    return drm::fmul(2.f, drm::atanf_pos(drm::froot(drm::fdiv(drm::fsub(1.f, x), drm::fadd(1.f, x)))));
+}
 DRM_FN float dr_expf(float x) { return (float)drm::exp_d((double)x); }
 DRM_FN float dr_logf(float x) { return (float)drm::log_d((double)x); }
 DRM_FN float dr_powf(float x, float y) { return (float)drm::pow_d((double)x, (double)y); }

@@ -297,6 +297,19 @@ DR_API dr_status dr_scene_last_timings(const dr_scene *scene, int index, char *n
  * sampled edges (tooling). */
 DR_API dr_status dr_scene_last_counts(const dr_scene *scene, int64_t *points, int64_t *items);
 
+/* Tooling: one array of the scene's edge data, as built (no counterpart in
+ * the reference, whose edge trees live in its Scene, scene.cpp:91-97):
+ * what 0 silhouette-tree nodes (56 B each: box, cone axis and angle, offset,
+ * edge count, total length, pad), 1 silhouette-tree edges in leaf order
+ * (20 B: shape, v0, v1, f0, f1), 2 normal-tree nodes, 3 normal-tree edges,
+ * 4 primary edges, 5 primary cdf (float), 6 primary func (float), 7 the
+ * primary func integral (one float).  *count receives the element count; up
+ * to capacity_bytes are copied to out_host (may be NULL).  build_ms (may be
+ * NULL) receives the host wall time of the scene's last GPU edge build (0 for
+ * scenes of at most 8192 triangles, which build on the host). */
+DR_API dr_status dr_scene_edge_data(const dr_scene *scene, int what, void *out_host, int64_t capacity_bytes,
+                                    int64_t *count, float *build_ms);
+
 /* Kernel launch count of the last render call on this scene (for tooling). */
 DR_API dr_status dr_scene_last_launch_count(const dr_scene *scene, int *count);
 

@@ -36,6 +36,7 @@
 #include <thread>
 
 #include "../delta_ray_b200/csrc/dr_math.h"
+#include "../delta_ray_b200/csrc/dr_edge_rules.h"
 
 // The transcendental functions the restatement evaluates.  In the reference's
 // RNG mode they are the host libm's, as in the compiled reference.  In the
@@ -43,6 +44,16 @@
 // are the same on the GPU and here, so that a sample takes the same branches
 // on both sides.
 static bool g_repro_math = false;
+// The edge trees' split rule.  The reference's: std::nth_element on the split
+// coordinate, float normal sums in range order, std::min / std::max boxes.
+// In the Philox mode, trees of more than DR_TREE_EXACT_MAX_EDGES edges follow
+// the product's rule (dr_edge_rules.h), which its GPU build reproduces: a
+// stable sort on the split coordinate's total-order key, exact fixed-point
+// normal sums, total-order boxes.  The two rules give the same trees except
+// where edges share a median coordinate (and in the last bits of cone axes);
+// either is unbiased.  g_product_tree is set while such a tree is built.
+static bool g_product_rule = false;
+static bool g_product_tree = false;
 inline float m_pow(float x, float e) { return g_repro_math ? dr_powf(x, e) : std::pow(x, e); }
 inline float m_log(float x) { return g_repro_math ? dr_logf(x) : std::log(x); }
 inline float m_sin(float x) { return g_repro_math ? dr_sinf(x) : std::sin(x); }
@@ -487,13 +498,17 @@ struct Dist1D {
     }
 };
 
+// box minima and maxima: std::min / std::max, or the total order of the
+// product's tree rule (-0 below +0)
+inline float box_min(float a, float b) { return g_product_tree ? (edge_ord_key(b) < edge_ord_key(a) ? b : a) : std::min(a, b); }
+inline float box_max(float a, float b) { return g_product_tree ? (edge_ord_key(b) > edge_ord_key(a) ? b : a) : std::max(a, b); }
 struct AABB {
     V3f lo{INFINITY, INFINITY, INFINITY}, hi{-INFINITY, -INFINITY, -INFINITY};
     void add(const V3f &p) {
-        for (int a = 0; a < 3; a++) { lo[a] = std::min(lo[a], p[a]); hi[a] = std::max(hi[a], p[a]); }
+        for (int a = 0; a < 3; a++) { lo[a] = box_min(lo[a], p[a]); hi[a] = box_max(hi[a], p[a]); }
     }
     void add(const AABB &b) {
-        for (int a = 0; a < 3; a++) { lo[a] = std::min(lo[a], b.lo[a]); hi[a] = std::max(hi[a], b.hi[a]); }
+        for (int a = 0; a < 3; a++) { lo[a] = box_min(lo[a], b.lo[a]); hi[a] = box_max(hi[a], b.hi[a]); }
     }
     V3f corner(int i) const { return V3f{(i & 1) ? hi.x : lo.x, (i & 2) ? hi.y : lo.y, (i & 4) ? hi.z : lo.z}; }
     V3f center() const { return 0.5f * (lo + hi); }
@@ -1328,8 +1343,10 @@ struct BuildNode {
     std::unique_ptr<BuildNode> c[2];
 };
 
-// median-split build (edge_tree.cpp:49-173), partitioning with std::nth_element
-// on the same comparator so that ties resolve as in the reference
+// median-split build (edge_tree.cpp:49-173): in the reference's RNG mode
+// partitioning with std::nth_element on the same comparator, so that ties
+// resolve as in the reference; in the Philox mode with the product's rule
+// (g_product_tree)
 template <bool DIR>
 std::unique_ptr<BuildNode> build_edge_node(const std::vector<Edge> &edges, std::vector<PrimInfo> &pi, int start, int end,
                                            int *total, std::vector<Edge> &ordered) {
@@ -1341,7 +1358,14 @@ std::unique_ptr<BuildNode> build_edge_node(const std::vector<Edge> &edges, std::
         if (DIR) db.add(pi[i].db);
     }
     V3f nsum{0.f, 0.f, 0.f};
-    for (int i = start; i < end; i++) nsum = nsum + pi[i].n0 + pi[i].n1;
+    if (g_product_tree) {
+        long long fs[3] = {0, 0, 0};
+        for (int i = start; i < end; i++)
+            for (int a = 0; a < 3; a++) fs[a] += edge_fixed(pi[i].n0[a]) + edge_fixed(pi[i].n1[a]);
+        nsum = V3f{edge_unfixed(fs[0]), edge_unfixed(fs[1]), edge_unfixed(fs[2])};
+    } else {
+        for (int i = start; i < end; i++) nsum = nsum + pi[i].n0 + pi[i].n1;
+    }
     V3f axis = normalize(nsum);
     float cmin = 1.f;
     for (int i = start; i < end; i++) {
@@ -1386,9 +1410,16 @@ std::unique_ptr<BuildNode> build_edge_node(const std::vector<Edge> &edges, std::
         return node;
     }
     int mid = (start + end) / 2;
-    std::nth_element(&pi[start], &pi[mid], &pi[end - 1] + 1, [dim, spatial](const PrimInfo &a, const PrimInfo &b) {
-        return spatial ? a.sc[dim] < b.sc[dim] : a.dc[dim] < b.dc[dim];
-    });
+    if (g_product_tree) {
+        std::stable_sort(pi.begin() + start, pi.begin() + end, [dim, spatial](const PrimInfo &a, const PrimInfo &b) {
+            return spatial ? edge_ord_key(a.sc[dim]) < edge_ord_key(b.sc[dim])
+                           : edge_ord_key(a.dc[dim]) < edge_ord_key(b.dc[dim]);
+        });
+    } else {
+        std::nth_element(&pi[start], &pi[mid], &pi[end - 1] + 1, [dim, spatial](const PrimInfo &a, const PrimInfo &b) {
+            return spatial ? a.sc[dim] < b.sc[dim] : a.dc[dim] < b.dc[dim];
+        });
+    }
     node->c[0] = build_edge_node<DIR>(edges, pi, start, mid, total, ordered);
     node->c[1] = build_edge_node<DIR>(edges, pi, mid, end, total, ordered);
     return node;
@@ -1423,6 +1454,10 @@ inline int flatten(const Scene &sc, std::vector<EdgeNode> &nodes, const std::vec
 template <bool DIR> EdgeTree build_edge_tree(const Scene &sc, const std::vector<Edge> &edges) {
     EdgeTree t;
     if (edges.empty()) return t;
+    struct Rule {
+        Rule(bool on) { g_product_tree = on; }
+        ~Rule() { g_product_tree = false; }
+    } rule(g_product_rule && edges.size() > (size_t)DR_TREE_EXACT_MAX_EDGES);
     std::vector<PrimInfo> pi(edges.size());
     AABB world;
     for (size_t i = 0; i < edges.size(); i++) {
@@ -2375,6 +2410,7 @@ int dro_render_parts(const dr_scene_desc *desc, const dr_render_desc *rd, int rn
     // rng_mode 2: the Philox streams with the host libm (a check that the
     // restatement does not depend on the libm beyond rounding)
     g_repro_math = rng_mode == 1;
+    g_product_rule = rng_mode != 0;
     if (rng_mode == 2) rng_mode = 1;
     Scene sc;
     build_scene(sc, desc, nullptr, shape_rank);

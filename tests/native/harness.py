@@ -42,6 +42,8 @@ def load():
         L.hh_set_proposal.argtypes = [C.c_int, C.c_float]
         L.hh_set_split.argtypes = [C.c_int]
         L.hh_math.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_longlong]
+        L.hh_scene_edges.argtypes = [C.POINTER(_abi.dr_scene_desc), C.c_int, C.c_void_p, C.c_longlong]
+        L.hh_scene_edges.restype = C.c_longlong
         _lib = L
     return _lib
 
@@ -96,3 +98,20 @@ def math_eval(name, x, y=None):
     out = np.empty_like(x)
     L.hh_math(MATH_FUNCS[name], x.ctypes.data, None if yy is None else yy.ctypes.data, out.ctypes.data, x.size)
     return out
+
+
+EDGE_DATA = {"sil_nodes": (0, 56), "sil_edges": (1, 20), "nrm_nodes": (2, 56), "nrm_edges": (3, 20),
+             "prim_edges": (4, 20), "prim_cdf": (5, 4), "prim_func": (6, 4), "prim_func_int": (7, 4)}
+
+
+def scene_edges(wl, what):
+    """One array of the scene's edge data as the host build makes it, as bytes."""
+    from delta_ray_b200 import _abi
+    L = load()
+    cam, mats, shps, lts = _abi.scene_dicts(wl.camera, wl.materials, wl.shapes, wl.lights)
+    sd = _abi.SceneDesc.from_scene(cam, mats, shps, lts, torch.device("cpu"))
+    code, elem = EDGE_DATA[what]
+    n = L.hh_scene_edges(C.byref(sd.desc), code, None, 0)
+    buf = np.zeros(max(1, n * elem), np.uint8)
+    L.hh_scene_edges(C.byref(sd.desc), code, buf.ctypes.data, buf.size)
+    return buf[:n * elem].tobytes()

@@ -277,6 +277,32 @@ long long hh_trace(const dr_scene_desc *desc, const float *rays, int n, int *out
     return g_dr_visits;
 }
 
+// The scene's edge data as the host builds it (what: 0 silhouette-tree nodes,
+// 1 silhouette-tree edges, 2 normal-tree nodes, 3 normal-tree edges,
+// 4 primary edges, 5 primary cdf, 6 primary func, 7 primary func integral):
+// the bytes are copied to out (up to capacity), the element count returned.
+long long hh_scene_edges(const dr_scene_desc *desc, int what, void *out, long long capacity) {
+    HostSceneBundle b;
+    make_scene(desc, b);
+    const void *src = nullptr;
+    size_t elem = 0, count = 0;
+    const auto &h = b.h;
+    switch (what) {
+    case 0: src = h.sil_nodes.data(); elem = sizeof(DevEdgeNode); count = h.sil_nodes.size(); break;
+    case 1: src = h.sil_edges.data(); elem = sizeof(DevEdge); count = h.sil_edges.size(); break;
+    case 2: src = h.nrm_nodes.data(); elem = sizeof(DevEdgeNode); count = h.nrm_nodes.size(); break;
+    case 3: src = h.nrm_edges.data(); elem = sizeof(DevEdge); count = h.nrm_edges.size(); break;
+    case 4: src = h.prim_edges.data(); elem = sizeof(DevEdge); count = h.prim_edges.size(); break;
+    case 5: src = h.prim_dist.cdf.data(); elem = 4; count = h.prim_dist.cdf.size(); break;
+    case 6: src = h.prim_dist.func.data(); elem = 4; count = h.prim_dist.func.size(); break;
+    case 7: src = &h.prim_dist.func_int; elem = 4; count = 1; break;
+    default: return -1;
+    }
+    size_t bytes = std::min((size_t)capacity, elem * count);
+    if (out && bytes) std::memcpy(out, src, bytes);
+    return (long long)count;
+}
+
 // The reproducible transcendental functions (dr_math.h) on n inputs.
 void hh_math(int fn, const float *x, const float *y, float *out, long long n) {
     for (long long i = 0; i < n; i++) out[i] = dr_math_eval(fn, x[i], y ? y[i] : 0.f);

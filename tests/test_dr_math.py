@@ -1,16 +1,21 @@
 """The reproducible transcendental functions (delta_ray_b200/csrc/dr_math.h).
 
 The renderer evaluates sin, cos, atan, atan2, acos, exp, log and pow with its
-own double-precision routines so that the GPU and the oracle's CPU build round
-them to the same float.  Here, compiled for the CPU, they are checked against
-numpy's double-precision functions rounded to float: at most one float ulp
-apart everywhere, and equal on all but a vanishing share of inputs.  The GPU
+own routines so that the GPU and the oracle's CPU build round them to the same
+float.  Here, compiled for the CPU, they are checked against numpy's
+double-precision functions rounded to float: sin, cos, exp, log and pow
+(evaluated in double) at most one float ulp apart and equal on all but a
+vanishing share of inputs; atan, atan2 and acos (evaluated in float) within 3
+ulp.  The GPU
 test (test_dr_math_gpu.py) checks that the device build gives the same bits.
 """
 import numpy as np
 import pytest
 
 from native import harness
+
+
+FLOAT_EVALUATED = ("atan", "atan2", "acos")
 
 
 def ulp_distance(a, b):
@@ -72,12 +77,16 @@ def test_reproducible_math_is_within_one_ulp_of_double_precision(name):
     got = harness.math_eval(name, x, y)
     ref = numpy_reference(name, x, y)
     d = ulp_distance(got, ref)
-    # sin and cos for |x| near multiples of pi: numpy's float64 results carry
-    # a relative error that is large only where the value is tiny; allow the
-    # share of ties that double rounding can split
-    assert d.max() <= 1, (name, x[d.argmax()], None if y is None else y[d.argmax()], got[d.argmax()],
-                          ref[d.argmax()])
-    assert (d == 0).mean() >= 0.9999, (name, (d != 0).sum())
+    worst = (name, x[d.argmax()], None if y is None else y[d.argmax()], got[d.argmax()], ref[d.argmax()])
+    if name in FLOAT_EVALUATED:
+        # evaluated in float: a few ulp, most results the nearest float
+        assert d.max() <= 3, worst
+        assert (d == 0).mean() >= 0.7, (name, (d != 0).mean())
+    else:
+        # evaluated in double and rounded once: the nearest float but for
+        # values within ~1e-15 of a rounding boundary
+        assert d.max() <= 1, worst
+        assert (d == 0).mean() >= 0.9999, (name, (d != 0).sum())
 
 
 def test_reproducible_math_special_values():
