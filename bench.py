@@ -1,12 +1,20 @@
 #!/usr/bin/env python
 """Forward+backward throughput of the B200 differentiable path tracer.
 
-Workload: the soft-shadow scene (ground + 4-triangle blocker + area light),
-512x512, 16 spp, max_bounces 1 -- one "step" renders the image and runs the
-full backward (path adjoint, secondary edges, primary edges) against an
-all-ones image adjoint.  Metric: pixel samples per second (fwd+bwd).
+Default workload: the glossy heightfield configuration -- a 256 x 256-vertex
+grid (130,050 triangles in 64 patches of their own Blinn-Phong material,
+heights from 6 seeded sinusoid octaves) under two area lights (4 triangles),
+640 x 480, 64 spp, max_bounces 3.  Its image is rendered as 16 batches of
+4 spp, one batch per step: a step renders the batch forward and runs the full
+backward (path adjoints, secondary edges over the edge trees, primary edges)
+against an all-ones image adjoint, with its own seed.  Per-sample work does not
+depend on how a pixel's samples are batched (each pixel sample draws its own
+streams and its primary-edge samples scale with it); the line reports a
+measured check of that (`spp_linearity`).  Metric: pixel samples per second
+(fwd+bwd); `forward` gives forward-only samples per second.
 
     python bench.py [--gpus N] [--steps K] [--warmup W] [--impl b200|reference]
+                    [--workload heightfield|soft_shadow|single_triangle|heightfield_ggx]
 
 N > 1 runs under torchrun; every rank renders its own replica of the workload
 (samples are independent; no collective on the data path), and `value` is the
@@ -29,31 +37,28 @@ sys.path.insert(0, ROOT)
 
 METRIC = "fwd+bwd samples/s"
 UNIT = "samples/s"
-# The headline workload is the soft-shadow scene (8 triangles, 512x512, 16 spp,
-# max_bounces 1).  The heightfield scene (130,050 + 4 triangles, glossy, 2
-# lights, max_bounces 3) runs at 160x120 and 4 spp: its shading points sample
-# about 1,100 edges each under the reference's edge-tree rules, so the full
-# 640x480 x 64 spp image would need 3e10 edge evaluations per backward call.
-# ref_res, ref_spp: image size and samples per pixel of the reference CPU arm's
-# steps (its time is linear in samples).
+# spp: samples per pixel of the configuration's image; step_spp: the batch one
+# step renders (spp / step_spp steps make an image).  ref_res, ref_spp: the
+# reference CPU arm's bounded sample per step -- the same view at a lower
+# resolution (per-sample work does not depend on the resolution; its time is
+# linear in samples, and the arm reports a check of that).
 WORKLOADS = {
-    "soft_shadow": dict(builder="soft_shadow", resolution=(512, 512), spp=16, max_bounces=1, scene_seed=0,
-                        ref_res=(512, 512), ref_spp=16),
-    "heightfield": dict(builder="heightfield", resolution=(160, 120), spp=4, max_bounces=3, scene_seed=0,
-                        ref_res=(80, 60), ref_spp=1),
-    # the same heightfield with GGX lobes; the reference has no GGX material, so
+    "heightfield": dict(builder="heightfield", resolution=(640, 480), spp=64, step_spp=4, max_bounces=3,
+                        scene_seed=0, ref_res=(160, 120), ref_spp=1,
+                        name="glossy heightfield (130,054 triangles, Blinn-Phong)"),
+    "soft_shadow": dict(builder="soft_shadow", resolution=(512, 512), spp=16, step_spp=16, max_bounces=1,
+                        scene_seed=0, ref_res=(512, 512), ref_spp=16, name="soft shadow (8 triangles)"),
+    "single_triangle": dict(builder="single_triangle", resolution=(256, 256), spp=4, step_spp=4, max_bounces=1,
+                            scene_seed=0, ref_res=(256, 256), ref_spp=4, name="single triangle (3 triangles)"),
+    # the heightfield with GGX lobes; the reference has no GGX material, so
     # its arm reports this workload unavailable
-    "heightfield_ggx": dict(builder="heightfield", resolution=(160, 120), spp=4, max_bounces=3, scene_seed=0,
-                            ref_res=None, ref_spp=None, options={"microfacet": "ggx"},
+    "heightfield_ggx": dict(builder="heightfield", resolution=(640, 480), spp=64, step_spp=4, max_bounces=3,
+                            scene_seed=0, ref_res=None, ref_spp=None, options={"microfacet": "ggx"},
+                            name="glossy heightfield (130,054 triangles, GGX)",
                             no_reference="the reference's materials are Blinn-Phong only (no GGX lobe)"),
 }
-WORKLOAD = WORKLOADS["soft_shadow"]
-# stages of the work model that run as several kernels
-COMPOSITE_STAGES = {
-    "k_primary_edges": ("k_primary_shade", "k_primary_grad"),
-    "k_edge_traverse": ("k_edge_expand", "k_edge_tasks"),  # the two-stage walk of large edge trees
-    "k_edge_eval": ("k_edge_line", "k_edge_rays", "k_edge_line_rays", "k_edge_shade"),
-}
+DEFAULT_WORKLOAD = "heightfield"
+WORKLOAD = WORKLOADS[DEFAULT_WORKLOAD]
 # reference CPU arm: page-in / warm-up steps on a small slice of the same scene
 REF_RES = (32, 32)
 
@@ -68,7 +73,7 @@ def parse():
     p.add_argument("--no-proposal", action="store_true", help="skip the learned-vs-plain edge sampling measurement")
     p.add_argument("--proposal-seeds", type=int, default=32, help="seeds per arm of the learned-vs-plain measurement")
     p.add_argument("--proposal-train", type=int, default=60, help="training calls before the learned arm")
-    p.add_argument("--workload", default="soft_shadow", choices=sorted(WORKLOADS))
+    p.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS))
     return p.parse_args()
 
 
@@ -78,18 +83,20 @@ def dist_info():
 
 
 def build_workload(res=None, spp=None):
+    """The workload's scene; spp defaults to one step's batch."""
     from delta_ray_b200 import workloads
     w = WORKLOAD
     return workloads.BUILDERS[w["builder"]](seed=w["scene_seed"], resolution=res or w["resolution"],
-                                            spp=spp or w["spp"], max_bounces=w["max_bounces"],
+                                            spp=spp or w["step_spp"], max_bounces=w["max_bounces"],
                                             **w.get("options", {}))
 
 
 def workload_label():
     w = WORKLOAD
-    opts = "".join(f" {k}={v}" for k, v in w.get("options", {}).items())
-    return (f"{w['builder']} {w['resolution'][0]}x{w['resolution'][1]} {w['spp']}spp "
-            f"max_bounces={w['max_bounces']}{opts} fwd+bwd")
+    batches = w["spp"] // w["step_spp"]
+    per = f" as {batches} steps of {w['step_spp']} spp" if batches > 1 else ""
+    return (f"{w['name']}: {w['resolution'][0]}x{w['resolution'][1]}, {w['spp']} spp{per}, "
+            f"max_bounces={w['max_bounces']}, fwd+bwd")
 
 
 # ---------------------------------------------------------------------------
@@ -157,29 +164,54 @@ def ray_bytes(num_tris):
     return 24 + 16 + 36 + 64 * max(1, math.ceil(math.log2(max(2, num_tris))))
 
 
-def stage_bytes(stage, wl, counts):
-    """Algorithmic bytes of one launch of a backward/forward stage."""
+# bytes per shading vertex: path state read/write (32) + material record (28)
+SHADE_BYTES = 32 + 28
+# a shading-point record as the edge kernels read it (24 floats)
+POINT_BYTES = 96
+# an edge-tree node (edge_tree.h:12-22)
+NODE_BYTES = 40
+
+
+def kernel_bytes(kernel, wl, work):
+    """Algorithmic bytes of one launch of `kernel` (the survey's fixed model:
+    rays at ray_bytes(T) each, shading vertices at SHADE_BYTES, point records,
+    items (20 B), edge-tree nodes visited (40 B), queue records, gradient
+    scatter), from the call's measured work counts (Scene.last_work) and the
+    pixel samples n = W * H * spp.  0 for kernels outside the model."""
     W, H = wl.resolution
     spp, B = wl.spp, wl.max_bounces
     br = ray_bytes(wl.num_triangles)
-    shade = 32 + 28  # path state read/write + material record per shading vertex
     n = W * H * spp
-    points, items = counts
+    P, I = work["points"], work["items"]
     rays_path = 1 + 2 * B  # upper bound: camera ray, then a shadow and a BSDF ray per bounce
-    if stage in ("k_render_forward",):
-        return n * (rays_path * br + B * shade) + W * H * 12
-    if stage == "k_backward_paths":
-        return n * (rays_path * br + B * shade) + W * H * 24 + points * 96
-    if stage == "k_edge_traverse":
-        return points * 96 + items * 20
-    if stage == "k_edge_eval":
-        # two straddling rays, two shadow rays of the emitter evaluations
-        return items * (4 * br + 2 * shade + 96 + 20 + 12)
-    if stage == "k_dp_propagate":
-        return points * (96 + 36 + 12 * 3)
-    if stage == "k_primary_edges":
-        # two camera rays + two shaded paths per sample, plus edge/vertex reads
-        return n * (2 * (1 + rays_path) * br + 2 * B * shade + 24 + 12)
+    # an edge sample's shading: two shadow rays to the emitters, plus the
+    # multi-bounce paths of both sides when B > 1 (1 + 2 (B - 1) rays each)
+    shade_rays = 2 + (2 * (1 + 2 * (B - 1)) if B > 1 else 0)
+    if kernel == "k_render_forward":
+        return n * (rays_path * br + B * SHADE_BYTES) + W * H * 12
+    if kernel == "k_backward_paths":
+        return n * (rays_path * br + B * SHADE_BYTES) + W * H * 24 + P * POINT_BYTES
+    if kernel == "k_primary_shade":  # two camera rays, two shaded paths, the 16-B color difference out
+        return n * (2 * rays_path * br + 2 * B * SHADE_BYTES + 24 + 16)
+    if kernel == "k_primary_grad":  # the color difference in, edge vertices, vertex and camera adds
+        return n * (16 + 24 + 24)
+    if kernel == "k_edge_traverse":
+        return P * POINT_BYTES + I * 20 + work["visits_walk"] * NODE_BYTES
+    if kernel == "k_edge_expand":
+        return P * POINT_BYTES + work["items_first_stage"] * 20 + work["tasks"] * 24 + work["visits_walk"] * NODE_BYTES
+    if kernel == "k_edge_tasks":
+        return (work["tasks"] * (24 + POINT_BYTES) + (I - work["items_first_stage"]) * 20 +
+                work["visits_tasks"] * NODE_BYTES)
+    if kernel == "k_edge_line":  # item, point record, LTC matrix, material; survivor record out
+        return I * (20 + POINT_BYTES + 36 + 28) + work["survivors"] * 32
+    if kernel == "k_edge_rays":  # survivor in, two closest-hit rays, hit record out
+        return work["survivors"] * (32 + 2 * br) + work["shaded"] * 16
+    if kernel == "k_edge_line_rays":
+        return I * (20 + POINT_BYTES + 36 + 28) + work["survivors"] * 2 * br + work["shaded"] * 48
+    if kernel == "k_edge_shade":  # records in, shading rays and vertices, dp out, vertex gradient adds
+        return work["shaded"] * (48 + POINT_BYTES + shade_rays * br + 2 * SHADE_BYTES + 12 + 2 * 12)
+    if kernel == "k_dp_propagate":
+        return P * (POINT_BYTES + 36 + 12 * 3)
     return 0
 
 
@@ -299,57 +331,51 @@ def measure_proposal(dev, K=32, train_calls=60):
     return out
 
 
-def merge_stages(stages):
-    """[(kernel, ms)] -> [(stage, ms)]: the kernels of a composite stage summed
-    under its name (COMPOSITE_STAGES), other kernels kept, first-seen order."""
-    parts_of = {k: name for name, parts in COMPOSITE_STAGES.items() for k in parts}
-    merged = {}
-    for name, ms in stages:
-        key = parts_of.get(name, name)
-        merged[key] = merged.get(key, 0.0) + ms
-    return list(merged.items())
-
-
-def load_traffic(stage):
-    """DRAM bytes (read + write) per launch of `stage` from the committed ncu
-    summary profiles/dram_traffic.txt ("<kernel> <bytes>" lines), if any; the
-    edge-evaluation stage sums its wavefront's three kernels."""
-    if WORKLOAD is not WORKLOADS["soft_shadow"]:
-        return None  # the table was captured on the soft-shadow workload
-    table = {}
+def load_profile(kernel):
+    """DRAM bytes and L2 figures per launch of `kernel` on this workload from
+    the committed ncu summary profiles/kernels_<workload>.txt ("<kernel>
+    <dram bytes> <l2 hit %> <l2 throughput % of peak> <units>" lines; the
+    capture may be of a smaller case of the same scene, so its DRAM bytes are
+    scaled by the units processed: samples, or the items of the call), if any."""
+    path = os.path.join(ROOT, "profiles", f"kernels_{WORKLOAD_KEY}.txt")
     try:
-        with open(os.path.join(ROOT, "profiles", "dram_traffic.txt")) as f:
+        with open(path) as f:
             for line in f:
                 parts = line.split()
-                if len(parts) == 2 and not line.startswith("#"):
-                    table[parts[0]] = int(parts[1])
+                if len(parts) == 5 and parts[0] == kernel and not line.startswith("#"):
+                    return {"dram_bytes": int(parts[1]), "l2_hit_pct": float(parts[2]),
+                            "l2_throughput_pct": float(parts[3]), "units": int(parts[4]),
+                            "source": os.path.relpath(path, ROOT)}
     except (OSError, ValueError):
         return None
-    parts = COMPOSITE_STAGES.get(stage)
-    if parts:  # the kernels of the stage that the captured build launched
-        got = [table[k] for k in parts if k in table]
-        return sum(got) if got else None
-    return table.get(stage)
+    return None
+
+
+WORKLOAD_KEY = DEFAULT_WORKLOAD
 
 
 # ---------------------------------------------------------------------------
 # reference CPU renderer
 # ---------------------------------------------------------------------------
 def reference_step(wl, seed):
+    """One step of the reference's own renderer: the forward call and the
+    backward call (which renders again, render_pytorch.py:247-257).  Returns
+    (forward seconds, backward seconds)."""
     import numpy as np
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import ref_runner
     W, H = wl.resolution
     t0 = time.perf_counter()
     ref_runner.render_reference(wl, seed)
+    t1 = time.perf_counter()
     ref_runner.render_reference(wl, seed, d_image=np.ones((H, W, 3), np.float32))
-    return time.perf_counter() - t0
+    return t1 - t0, time.perf_counter() - t1
 
 
 def cpu_baseline():
     """The reference's own CPU path (oracle/_ref, -O3 -ffast-math, its thread pool
     on all host cores): two timed steps of the workload's scene at its reference
-    size (about 10-20 s of CPU work on 16 cores) after a small page-in step."""
+    sample size (10-30 s of CPU work) after a small page-in step."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
     import ref_runner
     if not ref_runner.reference_available() or WORKLOAD.get("no_reference"):
@@ -359,9 +385,12 @@ def cpu_baseline():
     W, H = wl.resolution
     ts = [reference_step(wl, 1 + i) for i in range(2)]
     samples = W * H * wl.spp
-    return {"value": 2 * samples / sum(ts), "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
+    fwd = sum(t[0] for t in ts)
+    total = sum(t[0] + t[1] for t in ts)
+    return {"value": 2 * samples / total, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
+            "forward": 2 * samples / fwd,
             "sample": f"2 steps of the workload's scene at {W}x{H}, {wl.spp} spp (forward call + backward call), "
-                      f"{sum(ts):.1f} s"}
+                      f"{total:.1f} s"}
 
 
 def run_reference(args):
@@ -382,19 +411,25 @@ def run_reference(args):
     wl = build_workload(WORKLOAD["ref_res"], spp=WORKLOAD["ref_spp"])
     W, H = wl.resolution
     ts = [reference_step(wl, i) for i in range(args.steps)]
-    total = sum(ts)
+    total = sum(a + b for a, b in ts)
+    fwd = sum(a for a, _ in ts)
     samples = W * H * wl.spp
     value = samples * args.steps / total
+    # linearity of the reference's time in samples: one step at twice the spp
+    wl2 = build_workload(WORKLOAD["ref_res"], spp=2 * WORKLOAD["ref_spp"])
+    a2, b2 = reference_step(wl2, 10_000)
+    lin = {"spp": 2 * wl.spp, "value": 2 * samples / (a2 + b2), "ratio_to_value": 2 * samples / (a2 + b2) / value}
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": 1e3 * total / args.steps, "higher_is_better": True,
             "scaling": "weak", "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scene)",
-            "impl": "reference",
-            "config": {"workload": workload_label(), "resolution": [W, H],
-                       "spp": wl.spp,
-                       "max_bounces": wl.max_bounces, "l2": "n/a (CPU)"},
+            "impl": "reference", "forward": samples * args.steps / fwd,
+            "config": {"workload": workload_label(), "resolution": list(WORKLOAD["resolution"]),
+                       "spp": WORKLOAD["spp"], "max_bounces": wl.max_bounces, "l2": "n/a (CPU)"},
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": os.cpu_count(), "kind": "reference",
-                             "sample": f"{W}x{H} x {wl.spp} spp per step (forward call + backward call), "
+                             "sample": f"the same view at {W}x{H} x {wl.spp} spp per step (forward call + backward "
+                                       f"call; per-sample work does not depend on the resolution), "
                                        f"{args.warmup} warm-up steps on a 32x32 slice"},
+            "spp_linearity": lin,
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0}}
     print(json.dumps(line))
     return 0
@@ -403,6 +438,17 @@ def run_reference(args):
 # ---------------------------------------------------------------------------
 # B200 arm
 # ---------------------------------------------------------------------------
+def e2e_params(wl):
+    """The parameters the end-to-end step differentiates: every shape's
+    vertices except the lights', every material's roughness, the lights'
+    intensities."""
+    light_shapes = {l.shape_id for l in wl.lights}
+    params = [s.vertices for i, s in enumerate(wl.shapes) if i not in light_shapes]
+    params += [m.roughness for m in wl.materials]
+    params += [l.intensity for l in wl.lights]
+    return params
+
+
 def run_b200(args):
     import numpy as np
     import torch
@@ -420,7 +466,7 @@ def run_b200(args):
 
     wl = build_workload()
     W, H = wl.resolution
-    spp, B = wl.spp, wl.max_bounces
+    spp, B = wl.spp, wl.max_bounces  # spp: one step's batch
     samples = W * H * spp
     cam, mats, shps, lts = _abi.scene_dicts(wl.camera, wl.materials, wl.shapes, wl.lights)
     scene = Scene(cam, mats, shps, lts, local_rank)
@@ -429,23 +475,39 @@ def run_b200(args):
 
     from delta_ray_b200.distributed import average_gradients, rank_seed
 
-    def step(seed):
+    def step(seed, n_spp=spp):
         # each rank renders its own sample streams; one all-reduce combines the gradients
         s = rank_seed(seed, rank)
-        scene.forward(W, H, spp, B, s)
-        grad, _ = scene.backward(W, H, spp, B, s, d_img)
+        scene.forward(W, H, n_spp, B, s)
+        grad, _ = scene.backward(W, H, n_spp, B, s, d_img)
         if dist:
             average_gradients(grad)
 
+    def timed(fn, count):
+        ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(count)]
+        for k in range(count):
+            flush.zero_()  # L2 flush between timed steps (outside the events)
+            ev[k][0].record()
+            fn(k)
+            ev[k][1].record()
+        torch.cuda.synchronize()
+        return sum(a.elapsed_time(b) for a, b in ev)
+
+    def max_over_ranks(x):
+        t = torch.tensor([x], device=dev)
+        if dist:
+            dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
     for i in range(args.warmup):
         step(1000 + i)
-    # per-stage profile (untimed): stage times and work counts for the roofline
+    # per-kernel profile (untimed): kernel times and work counts for the roofline
     scene.set_profiling(True)
     scene.forward(W, H, spp, B, 7)
     stages = list(scene.last_timings())
     scene.backward(W, H, spp, B, 7, d_img)
     stages += scene.last_timings()
-    counts = scene.last_counts()
+    work = scene.last_work()
     scene.set_profiling(False)
     launches_per_step = 0
     scene.forward(W, H, spp, B, 8)
@@ -458,39 +520,36 @@ def run_b200(args):
         dist.barrier()
     torch.cuda.synchronize()
     clocks.start()
-    ev = [(torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)) for _ in range(args.steps)]
-    for k in range(args.steps):
-        flush.zero_()  # L2 flush between timed steps (outside the events)
-        ev[k][0].record()
-        step(k)
-        ev[k][1].record()
-    torch.cuda.synchronize()
+    total_ms = timed(step, args.steps)
     if dist:
         dist.barrier()
     clk = clocks.stop()
-    total_ms = sum(a.elapsed_time(b) for a, b in ev)
-    t = torch.tensor([total_ms], device=dev)
-    if dist:
-        dist.all_reduce(t, op=dist.ReduceOp.MAX)
-    total_ms = float(t.item())
+    total_ms = max_over_ranks(total_ms)
     ms_per_step = total_ms / args.steps
     value = world * samples / (ms_per_step / 1e3)
+
+    # forward only: the same batches, the forward call alone
+    fwd_ms = max_over_ranks(timed(lambda k: scene.forward(W, H, spp, B, rank_seed(5000 + k, rank)), args.steps))
+    forward_value = world * samples / (fwd_ms / args.steps / 1e3)
+
+    # per-sample work does not depend on the batch: one step of twice the spp
+    lin_ms = max_over_ranks(timed(lambda k: step(9000 + k, 2 * spp), 1))
+    lin_value = world * 2 * samples / (lin_ms / 1e3)
 
     # end to end through the public API with host tensors: upload, scene build,
     # forward, loss read-back, backward, gradients back to the host
     wl_e2e = build_workload()
-    wl_e2e.shapes[1].vertices.requires_grad_(True)
-    wl_e2e.lights[0].intensity.requires_grad_(True)
-    wl_e2e.materials[0].diffuse_reflectance.requires_grad_(True)
+    params = e2e_params(wl_e2e)
+    for x in params:
+        x.requires_grad_(True)
     args_e2e = wl_e2e.serialize()
     h2d = sum(a.numel() * a.element_size() for a in args_e2e if torch.is_tensor(a))
-    d2h = 4 + sum(x.numel() * x.element_size() for x in (wl_e2e.shapes[1].vertices, wl_e2e.lights[0].intensity,
-                                                           wl_e2e.materials[0].diffuse_reflectance))
+    d2h = 4 + sum(x.numel() * x.element_size() for x in params)
 
     def e2e_step(seed):
-        for x in (wl_e2e.shapes[1].vertices, wl_e2e.lights[0].intensity, wl_e2e.materials[0].diffuse_reflectance):
+        for x in params:
             x.grad = None
-        img = RenderFunction.apply(seed, *args_e2e)
+        img = RenderFunction.apply(rank_seed(seed, rank), *args_e2e)
         loss = img.sum()
         loss.item()
         loss.backward()
@@ -502,31 +561,38 @@ def run_b200(args):
     for k in range(e2e_steps):
         e2e_step(600 + k)
     torch.cuda.synchronize()
-    e2e_s = (time.perf_counter() - t0) / e2e_steps
-    e2e_t = torch.tensor([e2e_s], device=dev)
-    if dist:
-        dist.all_reduce(e2e_t, op=dist.ReduceOp.MAX)
-    e2e_value = world * samples / float(e2e_t.item())
+    e2e_s = max_over_ranks((time.perf_counter() - t0) / e2e_steps)
+    e2e_value = world * samples / e2e_s
 
-    # roofline of the dominant stage; a stage run as several kernels
-    # (COMPOSITE_STAGES) counts as one
+    # roofline of the dominant kernel (the longest one of a step)
     peak, peak_kind = load_peaks()
-    merged = merge_stages(stages)
-    dom = max(merged, key=lambda s: s[1]) if merged else ("", 0.0)
-    dom_bytes = stage_bytes(dom[0], wl, counts)
+    dom = max(stages, key=lambda s: s[1]) if stages else ("", 0.0)
+    dom_bytes = kernel_bytes(dom[0], wl, work)
     achieved = dom_bytes / (dom[1] / 1e3) / 1e9 if dom[1] > 0 else 0.0
+    prof = load_profile(dom[0])
+    traffic = None
+    if prof:  # DRAM bytes of the captured launch, scaled to this launch's units
+        units = work["items"] if dom[0].startswith("k_edge") else samples
+        traffic = int(prof["dram_bytes"] * units / max(1, prof["units"]))
     roofline = {"bound": "hbm", "kernel": dom[0], "achieved": achieved, "peak": peak, "unit": "GB/s",
-                "frac": achieved / peak, "peak_kind": peak_kind, "traffic": load_traffic(dom[0]),
+                "frac": achieved / peak, "peak_kind": peak_kind, "traffic": traffic,
                 "algorithmic_bytes_per_launch": dom_bytes,
-                "stage_ms": {n: round(ms, 4) for n, ms in stages},
-                "points": counts[0], "edge_items": counts[1]}
+                "l2": ({"hit_rate_pct": prof["l2_hit_pct"], "throughput_pct_of_peak": prof["l2_throughput_pct"],
+                        "source": prof["source"]} if prof else None),
+                "kernel_ms": {n: round(ms, 4) for n, ms in stages},
+                "kernel_model_gbs": {n: round(kernel_bytes(n, wl, work) / (ms / 1e3) / 1e9, 1)
+                                     for n, ms in stages if ms > 0 and kernel_bytes(n, wl, work) > 0},
+                "work": work}
 
     line = {"metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": args.steps,
             "warmup": args.warmup, "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak",
             "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scene)",
-            "config": {"workload": workload_label(),
-                       "resolution": [W, H], "spp": spp, "max_bounces": B, "triangles": wl.num_triangles,
-                       "parallelism": f"dp{world} (per-rank sample streams, gradient all-reduce)", "l2": "flushed between steps (256 MB write)"},
+            "forward": forward_value,
+            "config": {"workload": workload_label(), "resolution": [W, H], "spp": WORKLOAD["spp"],
+                       "spp_per_step": spp, "max_bounces": B, "triangles": wl.num_triangles,
+                       "parallelism": f"dp{world} (per-rank sample streams, gradient all-reduce)",
+                       "l2": "flushed between steps (256 MB write)"},
+            "spp_linearity": {"spp": 2 * spp, "value": lin_value, "ratio_to_value": lin_value / value},
             "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(h2d), "d2h_bytes_per_step": int(d2h)},
             "gpu_launches": launches_per_step * args.steps, "roofline": roofline, "clocks": clk}
     if rank == 0 and world == 1 and not args.no_proposal:
@@ -545,9 +611,10 @@ def run_b200(args):
 
 
 def main():
-    global WORKLOAD
+    global WORKLOAD, WORKLOAD_KEY
     args = parse()
     WORKLOAD = WORKLOADS[args.workload]
+    WORKLOAD_KEY = args.workload
     if args.impl == "reference":
         return run_reference(args)
     return run_b200(args)

@@ -180,6 +180,11 @@ struct dr_scene {
     bool timer_ready = false;
     std::vector<std::pair<std::string, float>> timings;
     long long last_points = 0, last_items = 0;
+    // work counts of the last backward call: points, items, line samples kept
+    // for rays, samples kept for shading, handed-on subtrees, items of the
+    // first traversal stage, edge-tree nodes visited by the point walks and by
+    // the subtree walks
+    long long last_work[8] = {};
     int num_vertices = 0, num_tris = 0, num_sms = 148;
     int bvh_built_tris = 0;  // triangle count of the LBVH topology kept in bvh_scratch
     // scenes of more than kGpuEdgeTris triangles build their edges, edge trees
@@ -561,10 +566,18 @@ std::pair<long long, long long> run_backward(dr_scene *scene, const dr_render_de
         if (c.status & ~(DR_STATUS_ITEM_OVERFLOW | DR_STATUS_POINT_OVERFLOW))
             throw DrError(DR_ERR_DEVICE_STATUS, "device reported status " + std::to_string(c.status));
     };
+    long long work[8] = {};
     auto back = [&]() {
         check_cuda(dr_launch_backward_back(ds, rd->width, rd->height, rd->spp, rd->max_bounces, rd->seed, grad_dev,
                                            rd->dp_mode, ws, cfg, scene->num_sms, st, &scene->last_launches, timer),
                    "backward launch");
+        // the stage's work counts (the counters of the evaluation wavefront
+        // and the task queue restart with every chunk)
+        read();
+        work[2] += (long long)c.survivors;
+        work[3] += (long long)c.hits;
+        work[4] += (long long)c.tasks;
+        work[5] += (long long)(ds.split_traversal ? c.items_expand : c.items);
     };
     for (int attempt = 0;; attempt++) {
         check_cuda(cudaMemsetAsync(ws.counters, 0, sizeof(BackwardCounters), st), "memset");
@@ -682,6 +695,11 @@ std::pair<long long, long long> run_backward(dr_scene *scene, const dr_render_de
         pr.steps++;
     }
     check_cuda(cudaStreamSynchronize(st), "backward");
+    work[0] = P;
+    work[1] = items;
+    work[6] = (long long)c.visits_walk;
+    work[7] = (long long)c.visits_tasks;
+    std::memcpy(scene->last_work, work, sizeof(work));
     return {P, items};
 }
 
@@ -1193,6 +1211,13 @@ dr_status dr_scene_edge_data(const dr_scene *scene, int what, void *out_host, in
         }
         size_t bytes = std::min((size_t)capacity_bytes, elem * n);
         if (bytes) check_cuda(cudaMemcpy(out_host, src, bytes, cudaMemcpyDeviceToHost), "edge data copy");
+    });
+}
+
+dr_status dr_scene_last_work(const dr_scene *scene, int64_t *counts, int n) {
+    return guard([&]() {
+        if (!scene || !counts || n < 0) throw DrError(DR_ERR_INVALID_ARGUMENT, "NULL argument");
+        for (int i = 0; i < n && i < 8; i++) counts[i] = scene->last_work[i];
     });
 }
 

@@ -522,7 +522,7 @@ DEV ConeSpec light_cone(const DevScene &s, int li, float3 p) {
 // (EdgeTask fields) instead of being walked here.
 template <bool PROP, int CUT = 0, class Emit, class Defer = NoDefer>
 DEV bool traverse_point(const DevScene &s, const PointRecord &pt, uint64_t seed, Emit &emit, const EdgeProposal &pr,
-                        Defer *defer = nullptr) {
+                        Defer *defer = nullptr, int *visits = nullptr) {
     Rng prng;
     prng.init(seed, kStreamEdgePoint, pt.sid, (uint32_t)pt.bounce);
     draw_edge(prng);  // the point's edge sample; eval_item redraws it
@@ -536,14 +536,15 @@ DEV bool traverse_point(const DevScene &s, const PointRecord &pt, uint64_t seed,
         if (w != 0.f) emit(tree, ei, key, w, code);
     };
     NoDefer nd;
-    if constexpr (CUT > 0) return traverse_edges<PROP, CUT>(s, pt.wi, pt.tri, sp, cone, prng, nrng, em, pr, *defer);
-    return traverse_edges<PROP, 0>(s, pt.wi, pt.tri, sp, cone, prng, nrng, em, pr, nd);
+    if constexpr (CUT > 0)
+        return traverse_edges<PROP, CUT>(s, pt.wi, pt.tri, sp, cone, prng, nrng, em, pr, *defer, visits);
+    return traverse_edges<PROP, 0>(s, pt.wi, pt.tri, sp, cone, prng, nrng, em, pr, nd, visits);
 }
 
 // Walks one handed-on subtree of the point (see traverse_point).
 template <bool PROP, class Emit>
 DEV bool traverse_point_task(const DevScene &s, const PointRecord &pt, uint64_t seed, const EdgeTask &task,
-                             Emit &emit, const EdgeProposal &pr) {
+                             Emit &emit, const EdgeProposal &pr, int *visits = nullptr) {
     NodeRng nrng;
     nrng.seed = seed;
     nrng.sid = pt.sid;
@@ -553,7 +554,7 @@ DEV bool traverse_point_task(const DevScene &s, const PointRecord &pt, uint64_t 
     auto em = [&](int tree, int ei, int key, float w, int code) {
         if (w != 0.f) emit(tree, ei, key, w, code);
     };
-    return traverse_subtree<PROP>(s, pt.wi, pt.tri, sp, cone, nrng, task, em, pr);
+    return traverse_subtree<PROP>(s, pt.wi, pt.tri, sp, cone, nrng, task, em, pr, visits);
 }
 
 // One sampled edge (delta_ray.cpp:901-973); returns dp, scatters dv0 / dv1;

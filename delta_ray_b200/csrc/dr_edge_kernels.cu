@@ -67,11 +67,19 @@ __device__ __forceinline__ EdgeProposal point_proposal(const BackwardWorkspace &
 
 // One thread per shading point in [pt_begin, pt_end) walks the point's trees
 // (small trees: every point's walk is short).
+// Adds each warp's node-visit count to a counter (every lane calls it).
+__device__ __forceinline__ void add_visits(unsigned long long *counter, int visits) {
+    unsigned long long v = (unsigned long long)visits;
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_xor_sync(0xffffffffu, v, o);
+    if ((threadIdx.x & 31) == 0 && v) atomicAdd(counter, v);
+}
+
 template <bool PROP>
 __global__ void __launch_bounds__(128, 6) k_edge_traverse(DevScene s, uint64_t seed, BackwardWorkspace ws) {
     long long n = min(min((long long)ws.counters->points, ws.cap_points), ws.pt_end);
     long long stride = (long long)gridDim.x * blockDim.x;
     ItemWriter out(ws);
+    int visits = 0;
     // warp-uniform loop: every lane of a warp takes the same number of trips
     for (long long base = ws.pt_begin + (long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < n;
          base += stride) {
@@ -80,11 +88,12 @@ __global__ void __launch_bounds__(128, 6) k_edge_traverse(DevScene s, uint64_t s
             PointRecord pt;
             pt.load(ws.pt + (size_t)p * DR_PT_WORDS);
             auto emit = [&](int tree, int ei, int j, float w, int code) { out.add((int)p, tree, ei, j, w, code); };
-            if (!traverse_point<PROP>(s, pt, seed, emit, point_proposal(ws, p)))
+            if (!traverse_point<PROP>(s, pt, seed, emit, point_proposal(ws, p), (NoDefer *)nullptr, &visits))
                 set_status(&ws.counters->status, DR_STATUS_STACK_OVERFLOW);
         }
         out.flush_warp();
     }
+    add_visits(&ws.counters->visits_walk, visits);
 }
 
 // Large trees, first stage: each point's walk stops DR_TASK_CUT levels below
@@ -99,6 +108,7 @@ __global__ void __launch_bounds__(128, 4) k_edge_expand(DevScene s, uint64_t see
     long long n = min(min((long long)ws.counters->points, ws.cap_points), ws.pt_end);
     long long stride = (long long)gridDim.x * blockDim.x;
     ItemWriter out(ws);
+    int visits = 0;
     for (long long base = ws.pt_begin + (long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < n;
          base += stride) {
         long long p = base + (threadIdx.x & 31);
@@ -115,7 +125,7 @@ __global__ void __launch_bounds__(128, 4) k_edge_expand(DevScene s, uint64_t see
                 if (first + (unsigned long long)nt <= (unsigned long long)ws.cap_tasks) {
                     for (int k = 0; k < nt; k++) ws.tasks[first + k] = tb[k];
                 } else {  // no room: walk them here
-                    for (int k = 0; k < nt; k++) ok &= traverse_point_task<PROP>(s, pt, seed, tb[k], emit, pr);
+                    for (int k = 0; k < nt; k++) ok &= traverse_point_task<PROP>(s, pt, seed, tb[k], emit, pr, &visits);
                 }
                 nt = 0;
             };
@@ -123,12 +133,13 @@ __global__ void __launch_bounds__(128, 4) k_edge_expand(DevScene s, uint64_t see
                 if (nt == DR_TASK_BUF) flush();
                 tb[nt++] = EdgeTask{(int)p, code, bb, c, a, l};
             };
-            ok &= traverse_point<PROP, DR_TASK_CUT>(s, pt, seed, emit, pr, &defer);
+            ok &= traverse_point<PROP, DR_TASK_CUT>(s, pt, seed, emit, pr, &defer, &visits);
             if (nt > 0) flush();
             if (!ok) set_status(&ws.counters->status, DR_STATUS_STACK_OVERFLOW);
         }
         out.flush_warp();
     }
+    add_visits(&ws.counters->visits_walk, visits);
 }
 
 // Large trees, second stage: one thread per handed-on subtree.
@@ -137,6 +148,7 @@ __global__ void __launch_bounds__(128, 6) k_edge_tasks(DevScene s, uint64_t seed
     long long n = (long long)min(ws.counters->tasks, (unsigned long long)ws.cap_tasks);
     long long stride = (long long)gridDim.x * blockDim.x;
     ItemWriter out(ws);
+    int visits = 0;
     for (long long base = (long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < n; base += stride) {
         long long k = base + (threadIdx.x & 31);
         if (k < n) {
@@ -144,12 +156,13 @@ __global__ void __launch_bounds__(128, 6) k_edge_tasks(DevScene s, uint64_t seed
             PointRecord pt;
             pt.load(ws.pt + (size_t)t.point * DR_PT_WORDS);
             auto emit = [&](int tree, int ei, int j, float w, int code) { out.add(t.point, tree, ei, j, w, code); };
-            if (!traverse_point_task<PROP>(s, pt, seed, t, emit, point_proposal(ws, t.point)))
+            if (!traverse_point_task<PROP>(s, pt, seed, t, emit, point_proposal(ws, t.point), &visits))
                 set_status(&ws.counters->status, DR_STATUS_STACK_OVERFLOW);
         }
         if (out.nb == DR_ITEM_BUF) out.flush_warp();  // keeps lanes' buffers from carrying over long
     }
     out.flush_warp();
+    add_visits(&ws.counters->visits_tasks, visits);
 }
 
 // What follows an item's evaluation: the proposal's training target and the
@@ -339,6 +352,10 @@ cudaError_t dr_launch_edge_traverse(const DevScene &s, uint64_t seed, const Back
         if (prop) k_edge_expand<true><<<stage_grid(num_sms), 128, 0, st>>>(s, seed, ws);
         else k_edge_expand<false><<<stage_grid(num_sms), 128, 0, st>>>(s, seed, ws);
         timer->mark(st, "k_edge_expand");
+        // the item count of the first stage (the roofline's work counts)
+        e = cudaMemcpyAsync(&ws.counters->items_expand, &ws.counters->items, sizeof(unsigned long long),
+                            cudaMemcpyDeviceToDevice, st);
+        if (e != cudaSuccess) return e;
         if (prop) k_edge_tasks<true><<<stage_grid(num_sms), 128, 0, st>>>(s, seed, ws);
         else k_edge_tasks<false><<<stage_grid(num_sms), 128, 0, st>>>(s, seed, ws);
         timer->mark(st, "k_edge_tasks");

@@ -292,7 +292,7 @@ DEV bool traverse_mode(const bool CONE, const DevScene &s, const DevEdgeNode *no
                        bool dir_bounds, float3 wi,
                        const SurfacePoint &sp, float dl, float sl, float rough, int model, const ConeSpec &cone,
                        const EdgeTask &start, const NodeRng &rng, Emit &emit, const EdgeProposal &pr, int tree,
-                       bool learned, Defer &defer) {
+                       bool learned, Defer &defer, int *visits = nullptr) {
     using Item = EdgeItem<PROP>;
     Item st[DR_EDGE_STACK];
     int sp_ = 0;
@@ -303,6 +303,7 @@ DEV bool traverse_mode(const bool CONE, const DevScene &s, const DevEdgeNode *no
         if (it.bb <= 0.f) continue;
         const int nid = it.node & DR_NODE_MASK;
         const DevEdgeNode &node = nodes[nid];
+        if (visits) ++*visits;
         if (node.nprims > 0) {
             float apmf = it.apmf;
             if constexpr (PROP) apmf = pr.alpha * it.lpmf + (1.f - pr.alpha) * it.apmf;
@@ -408,7 +409,8 @@ struct NoDefer {
 
 template <bool PROP, int CUT = 0, class Emit, class Defer>
 DEV bool traverse_edges(const DevScene &s, float3 wi, int stri, const SurfacePoint &sp, const ConeSpec &cone, Rng &rng,
-                        const NodeRng &nrng, Emit &emit, const EdgeProposal &pr, Defer &defer) {
+                        const NodeRng &nrng, Emit &emit, const EdgeProposal &pr, Defer &defer,
+                        int *visits = nullptr) {
     if (dot(wi, sp.f.n) < 0.f) return true;
     int tree;
     float pmf = 1.f;
@@ -451,7 +453,7 @@ DEV bool traverse_edges(const DevScene &s, float3 wi, int stri, const SurfacePoi
             defer(node | (tree << 29) | (mode << 30), bb, c, a, l);
         };
         ok &= traverse_mode<PROP, CUT>(mode == 0, s, nodes, edges, tree == 1, wi, sp, dl, sl, rough, m.model, cone,
-                                       root, nrng, em, pr, tree, learned, dc);
+                                       root, nrng, em, pr, tree, learned, dc, visits);
     }
     return ok;
 }
@@ -460,7 +462,8 @@ DEV bool traverse_edges(const DevScene &s, float3 wi, int stri, const SurfacePoi
 // recomputed: tree and mode come with the task).
 template <bool PROP, class Emit>
 DEV bool traverse_subtree(const DevScene &s, float3 wi, int stri, const SurfacePoint &sp, const ConeSpec &cone,
-                          const NodeRng &nrng, const EdgeTask &task, Emit &emit, const EdgeProposal &pr) {
+                          const NodeRng &nrng, const EdgeTask &task, Emit &emit, const EdgeProposal &pr,
+                          int *visits = nullptr) {
     const int tree = (task.code >> 29) & 1, mode = (task.code >> 30) & 1;
     const DevEdgeNode *nodes = tree ? s.nrm_nodes : s.sil_nodes;
     const DevEdge *edges = tree ? s.nrm_edges : s.sil_edges;
@@ -473,7 +476,7 @@ DEV bool traverse_subtree(const DevScene &s, float3 wi, int stri, const SurfaceP
     start.code = task.code & DR_NODE_MASK;  // depth bits cleared: walked to the leaves
     bool learned = PROP && mode == 1 ? nrng.draw(1, DR_NODE_MIX_DRAW) < pr.alpha : false;
     return traverse_mode<PROP>(mode == 0, s, nodes, edges, tree == 1, wi, sp, dl, sl, rough, m.model, cone, start,
-                               nrng, em, pr, tree, learned, nd);
+                               nrng, em, pr, tree, learned, nd, visits);
 }
 
 // LTC matrix lookup (material.h:464-476): nearest entry of the 128x128 table

@@ -75,6 +75,10 @@ struct BackwardCounters {
     unsigned long long survivors;  // line samples k_edge_line kept for k_edge_rays
     unsigned long long hits;       // samples k_edge_rays kept for k_edge_shade (follows survivors)
     unsigned long long tasks;      // subtrees k_edge_expand handed on to k_edge_tasks
+    // work counts for the roofline's byte model: edge-tree nodes visited by
+    // the point walks (k_edge_traverse / k_edge_expand) and by k_edge_tasks,
+    // and the item count when k_edge_expand finished
+    unsigned long long visits_walk, visits_tasks, items_expand;
 };
 
 struct BackwardWorkspace {

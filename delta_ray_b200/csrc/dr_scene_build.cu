@@ -663,6 +663,8 @@ cudaError_t dr_build_edge_tree(const DevScene &s, bool dir, const DevEdge *edges
     int first = 0, count = 1;
     const int kbits = 32 + bits_for(n + 1);
     while (count > 0) {
+        // a median split halves every range: at most ceil(log2 n) + 1 levels
+        if (levels.size() > 40 || first + count > 2 * n) return cudaErrorIllegalState;
         levels.emplace_back(first, count);
         k_nodes_reset<<<nblocks(count), kBS, 0, st>>>(nodes, first, count);
         if (dir) k_level_reduce<true><<<nblocks(n), kBS, 0, st>>>(elem_node, perm, prims, n, nodes);

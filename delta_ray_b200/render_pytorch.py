@@ -225,6 +225,16 @@ class Scene:
             i += 1
         return out
 
+    def last_work(self):
+        """Work counts of the last backward call (dr_scene_last_work): points,
+        items, ray survivors, shaded samples, subtree tasks, first-stage items,
+        node visits of the point walks and of the subtree walks."""
+        w = (C.c_int64 * 8)()
+        _lib.check(_lib.lib().dr_scene_last_work(self.handle, w, 8))
+        keys = ("points", "items", "survivors", "shaded", "tasks", "items_first_stage", "visits_walk",
+                "visits_tasks")
+        return dict(zip(keys, (int(x) for x in w)))
+
     def last_counts(self):
         p, it = C.c_int64(), C.c_int64()
         _lib.check(_lib.lib().dr_scene_last_counts(self.handle, C.byref(p), C.byref(it)))

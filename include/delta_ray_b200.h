@@ -310,6 +310,15 @@ DR_API dr_status dr_scene_last_counts(const dr_scene *scene, int64_t *points, in
 DR_API dr_status dr_scene_edge_data(const dr_scene *scene, int what, void *out_host, int64_t capacity_bytes,
                                     int64_t *count, float *build_ms);
 
+/* Tooling: work counts of the last backward call (the inputs of a byte model
+ * of its kernels; no counterpart in the reference): counts[0] shading points,
+ * [1] sampled edges, [2] line samples kept for their rays, [3] samples kept
+ * for shading, [4] subtrees handed from the first traversal stage to the
+ * second, [5] edges sampled by the first stage (all, when the traversal runs
+ * in one stage), [6] edge-tree nodes visited by the point walks, [7] nodes
+ * visited by the subtree walks.  Up to n of them are written. */
+DR_API dr_status dr_scene_last_work(const dr_scene *scene, int64_t *counts, int n);
+
 /* Kernel launch count of the last render call on this scene (for tooling). */
 DR_API dr_status dr_scene_last_launch_count(const dr_scene *scene, int *count);
 

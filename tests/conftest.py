@@ -83,5 +83,10 @@ def assert_image_parity(img, ref, rel=IMG_REL):
     ref = np.asarray(ref, np.float64)
     assert img.shape == ref.shape and np.isfinite(img).all()
     tol = rel * np.abs(ref) + 1e-6 * float(np.abs(ref).max()) + 1e-9
-    bad = (np.abs(img - ref) > tol).any(-1)
-    assert not bad.any(), f"{int(bad.sum())} of {bad.size} pixels differ beyond {rel} relative"
+    over = np.abs(img - ref) - tol
+    bad = (over > 0).any(-1)
+    if bad.any():
+        y, x, c = np.unravel_index(np.argmax(over), over.shape)
+        raise AssertionError(f"{int(bad.sum())} of {bad.size} pixels differ beyond {rel} relative; worst at "
+                             f"({x}, {y}) channel {c}: {img[y, x, c]:.9g} vs {ref[y, x, c]:.9g} "
+                             f"(image peak {float(np.abs(ref).max()):.6g})")

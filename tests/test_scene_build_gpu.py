@@ -42,6 +42,28 @@ def device_edges(sc, what):
     return buf[:n.value * elem].tobytes(), ms.value
 
 
+# float fields of each element (32-bit words), the rest are integers
+_FLOAT_WORDS = {"sil_nodes": set(range(10)) | {12}, "nrm_nodes": set(range(10)) | {12}, "prim_cdf": {0},
+                "prim_func": {0}, "prim_func_int": {0}}
+
+
+def _same(what, dev, host):
+    """Equal bit for bit, except that any two NaNs are equal (the silhouette
+    tree's cone axes are NaN by construction, normalize(0), and the CPU and
+    the GPU encode a NaN differently)."""
+    if len(dev) != len(host):
+        return False, -1
+    elem_words = harness.EDGE_DATA[what][1] // 4
+    a = np.frombuffer(dev, np.uint32).reshape(-1, elem_words)
+    b = np.frombuffer(host, np.uint32).reshape(-1, elem_words)
+    eq = a == b
+    for w in _FLOAT_WORDS.get(what, ()):
+        fa, fb = a[:, w].view(np.float32), b[:, w].view(np.float32)
+        eq[:, w] |= np.isnan(fa) & np.isnan(fb)
+    bad = ~eq.all(1)
+    return not bad.any(), int(np.flatnonzero(bad)[0]) if bad.any() else -1
+
+
 def assert_same_edge_data(sc, wl):
     sizes = {}
     for what in ARRAYS:
@@ -49,13 +71,10 @@ def assert_same_edge_data(sc, wl):
         host = harness.scene_edges(wl, what)
         elem = harness.EDGE_DATA[what][1]
         sizes[what] = len(host) // elem
-        if dev != host:
-            a = np.frombuffer(dev, np.uint8)
-            b = np.frombuffer(host, np.uint8)
-            m = min(a.size, b.size)
-            first = int(np.flatnonzero(a[:m] != b[:m])[0]) if (a[:m] != b[:m]).any() else m
-            raise AssertionError(f"{what}: {a.size // elem} vs {b.size // elem} elements, first difference at "
-                                 f"element {first // elem}")
+        ok, first = _same(what, dev, host)
+        if not ok:
+            raise AssertionError(f"{what}: {len(dev) // elem} vs {len(host) // elem} elements, first difference at "
+                                 f"element {first}")
     return sizes
 
 
