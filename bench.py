@@ -74,6 +74,8 @@ def parse():
     p.add_argument("--proposal-seeds", type=int, default=32, help="seeds per arm of the learned-vs-plain measurement")
     p.add_argument("--proposal-train", type=int, default=60, help="training calls before the learned arm")
     p.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS))
+    p.add_argument("--no-inverse", action="store_true", help="skip the inverse-rendering loop measurement")
+    p.add_argument("--inverse-steps", type=int, default=200, help="Adam steps per arm of the inverse-rendering loop")
     return p.parse_args()
 
 
@@ -354,6 +356,26 @@ def load_profile(kernel):
 WORKLOAD_KEY = DEFAULT_WORKLOAD
 
 
+def measure_inverse(steps):
+    """The inverse-rendering loop (delta_ray_b200.inverse) at its reduced
+    setting, plain and with the learned edge proposal: a 64 x 64 height grid
+    (16 roughness patches) fit to 4 views of 128 x 96 rendered at 64 spp, Adam
+    at 4 spp per view per step, max_bounces 2; parameter RMSE over the heights
+    and roughness, and the time to reach RMSE 0.01."""
+    from delta_ray_b200.inverse import FitConfig, fit
+    out = {"setting": "64x64-vertex heightfield (7,938 triangles + 2 light quads), 4 views of 128x96, "
+                      f"targets at 64 spp, {steps} Adam steps (lr 1e-2) at 4 spp, max_bounces 2; "
+                      "heights perturbed by N(0, 0.05), roughness by N(0, 0.1)",
+           "full_configuration": "256x256 grid, 4 views of 1024x1024 at 256 spp, 200 steps at 64 spp, "
+                                 "max_bounces 4: 268 M pixel samples fwd+bwd per step (not run)"}
+    for arm, learned in (("plain", False), ("learned", True)):
+        r = fit(FitConfig(steps=steps, learned=learned))
+        out[arm] = {k: (round(v, 5) if isinstance(v, float) else v) for k, v in r.items()
+                    if k in ("rmse_start", "rmse_final", "rmse_min", "time_to_goal_s", "steps_to_goal", "wall_s",
+                             "samples_per_s")}
+    return out
+
+
 # ---------------------------------------------------------------------------
 # reference CPU renderer
 # ---------------------------------------------------------------------------
@@ -597,6 +619,11 @@ def run_b200(args):
             "gpu_launches": launches_per_step * args.steps, "roofline": roofline, "clocks": clk}
     if rank == 0 and world == 1 and not args.no_proposal:
         line["proposal"] = measure_proposal(dev, K=args.proposal_seeds, train_calls=args.proposal_train)
+    if rank == 0 and world == 1 and not args.no_inverse and WORKLOAD_KEY == DEFAULT_WORKLOAD:
+        try:
+            line["inverse"] = measure_inverse(args.inverse_steps)
+        except Exception as e:  # a report beside the headline, not part of it
+            line["inverse"] = {"error": str(e)[:300]}
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         try:
             line["cpu_baseline"] = cpu_baseline()

@@ -683,10 +683,15 @@ DEV bool edge_rays(const DevScene &s, const EdgeLine &el, const DevEdge &edge, i
         trace_closest_pair_linear(s.bvh_tris, s.num_tris, p, rdir, ldir, 1e-3f, h0, h1);
         hit[0] = h0.tri;
         hit[1] = h1.tri;
+    } else if (s.num_tris > 0) {
+        // both sides in one walk of the LBVH: their directions differ by a few
+        // 1e-3, so they visit nearly the same nodes
+        Hit h0, h1;
+        trace_closest_pair_bvh(s.bvh_nodes, s.bvh_tris, s.bvh_root, p, rdir, ldir, 1e-3f, h0, h1);
+        hit[0] = h0.tri;
+        hit[1] = h1.tri;
     } else {
-        // both sides through one copy of the trace code: a loop, not unrolled
-#pragma unroll 1
-        for (int k = 0; k < 2; k++) hit[k] = trace_closest(s, p, k == 0 ? rdir : ldir, 1e-3f).tri;
+        hit[0] = hit[1] = -1;
     }
 #pragma unroll 1
     for (int k = 0; k < 2; k++) {

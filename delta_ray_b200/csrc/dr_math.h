@@ -15,10 +15,10 @@
 // The arc tangent family (atan, atan2, acos) is evaluated in float, see
 // below.  Methods (textbook ones, with coefficients that are exact Taylor
 // coefficients rounded to double):
-//   log  x = 2^k m, m in [sqrt(1/2), sqrt(2)]; log m = 2 atanh(s),
-//        s = (m - 1) / (m + 1), |s| <= 0.172, series to s^21.
-//   exp  x = k ln2 + r, |r| <= ln2 / 2 (Cody-Waite: ln2 split into a 33-bit
-//        head and a tail), Taylor series to r^13, then times 2^k.
+//   log  Tang's table-driven method: x = 2^k m, log m = log c_j +
+//        log1p(m / c_j - 1) over 64 centres c_j, series to r^8.
+//   exp  Tang's table-driven method: x = (64 m + j) ln2/64 + r (Cody-Waite),
+//        e^x = 2^m 2^(j/64) e^r, series to r^6.
 //   pow  exp(y log x) for x > 0; integer y for x < 0.
 //   sin, cos  x = k pi/2 + r (Cody-Waite, 33-bit head of pi/2), |r| <= pi/4,
 //        Taylor series to r^17 / r^16; meant for |x| < 2^20.
@@ -91,7 +91,78 @@ DRM_FN double scale2(double v, int k) {
     return mul(v, from_bits((int64_t)(k2 + 1023) << 52));
 }
 
-// natural logarithm of a double
+// Tables of the logarithm and the exponential (Tang's table-driven method):
+// DRM_LOG_INV[j] = 1 / c_j rounded to double, c_0 = 1 and c_j = 1 + (j + 1/2)
+// / 64 for j > 0, and DRM_LOG_L[j] = -log(DRM_LOG_INV[j]); DRM_EXP_T[j] =
+// 2^(j/64).  All rounded to double from 60-digit values.
+#define DRM_LOG_INV {1.0, 0.9770992366412213, 0.9624060150375939, 0.9481481481481482, \
+    0.9343065693430657, 0.920863309352518, 0.9078014184397163, 0.8951048951048951, \
+    0.8827586206896552, 0.8707482993197279, 0.8590604026845637, 0.847682119205298, \
+    0.8366013071895425, 0.8258064516129032, 0.8152866242038217, 0.8050314465408805, \
+    0.7950310559006211, 0.7852760736196319, 0.7757575757575758, 0.7664670658682635, \
+    0.757396449704142, 0.7485380116959064, 0.7398843930635838, 0.7314285714285714, \
+    0.7231638418079096, 0.7150837988826816, 0.7071823204419889, 0.6994535519125683, \
+    0.6918918918918919, 0.6844919786096256, 0.6772486772486772, 0.6701570680628273, \
+    0.6632124352331606, 0.6564102564102564, 0.649746192893401, 0.6432160804020101, \
+    0.6368159203980099, 0.6305418719211823, 0.624390243902439, 0.6183574879227053, \
+    0.6124401913875598, 0.6066350710900474, 0.6009389671361502, 0.5953488372093023, \
+    0.5898617511520737, 0.5844748858447488, 0.579185520361991, 0.5739910313901345, \
+    0.5688888888888889, 0.5638766519823789, 0.5589519650655022, 0.5541125541125541, \
+    0.5493562231759657, 0.5446808510638298, 0.540084388185654, 0.5355648535564853, \
+    0.5311203319502075, 0.5267489711934157, 0.5224489795918368, 0.5182186234817814, \
+    0.5140562248995983, 0.5099601593625498, 0.5059288537549407, 0.5019607843137255}
+#define DRM_LOG_L {0.0, 0.023167059281534418, 0.03831886430213666, 0.05324451451881224, \
+    0.06795066190850778, 0.08244366921107454, 0.09672962645855114, 0.11081436634029011, \
+    0.12470347850095725, 0.1384023228591192, 0.151916042025842, 0.16524957289530717, \
+    0.17840765747281825, 0.19139485299962947, 0.20421554142869083, 0.2168739383006143, \
+    0.2293741010648459, 0.24171993688714513, 0.25391520998096345, 0.2659635484971379, \
+    0.2778684510034563, 0.2896332925830427, 0.30126133057816185, 0.3127557100038969, \
+    0.324119468654212, 0.3353555419211378, 0.3464667673462086, 0.3574558889218038, \
+    0.36832556115870757, 0.3790783529349695, 0.38971675114002524, 0.40024316412701266, \
+    0.4106599249852683, 0.42096929464412963, 0.43117346481837143, 0.4412745608048752, \
+    0.4512746441394586, 0.46117571512217015, 0.470979715218791, 0.48068852934575196, \
+    0.4903039880451939, 0.49982786955644926, 0.5092619017898079, 0.5186077642080457, \
+    0.5278670896208424, 0.5370414658968837, 0.5461324375981356, 0.5551415075405016, \
+    0.564070138284803, 0.5729197535617854, 0.5816917396346225, 0.5903874466021763, \
+    0.5990081896460834, 0.6075552502245418, 0.616029877215514, 0.6244332880118936, \
+    0.6327666695710378, 0.6410311794209312, 0.6492279466251097, 0.65735807270836, \
+    0.6654226325450905, 0.6734226752121667, 0.6813592248079031, 0.689233281238809}
+#define DRM_EXP_T {1.0, 1.0108892860517005, 1.0218971486541166, 1.0330248790212284, \
+    1.0442737824274138, 1.0556451783605572, 1.0671404006768237, 1.0787607977571199, \
+    1.0905077326652577, 1.102382583307841, 1.1143867425958924, 1.1265216186082418, \
+    1.1387886347566916, 1.1511892299529827, 1.1637248587775775, 1.1763969916502812, \
+    1.189207115002721, 1.202156731452703, 1.215247359980469, 1.22848053610687, \
+    1.241857812073484, 1.255380757024691, 1.2690509571917332, 1.2828700160787783, \
+    1.2968395546510096, 1.3109612115247644, 1.3252366431597413, 1.339667524053303, \
+    1.3542555469368927, 1.3690024229745905, 1.383909881963832, 1.3989796725383112, \
+    1.4142135623730951, 1.42961333839197, 1.4451808069770467, 1.460917794180647, \
+    1.4768261459394993, 1.4929077282912648, 1.5091644275934228, 1.5255981507445384, \
+    1.5422108254079407, 1.559004400237837, 1.5759808451078865, 1.593142151342267, \
+    1.6104903319492543, 1.6280274218573478, 1.645755478153965, 1.6636765803267364, \
+    1.681792830507429, 1.7001063537185235, 1.718619298122478, 1.7373338352737062, \
+    1.7562521603732995, 1.7753764925265212, 1.7947090750031072, 1.8142521755003989, \
+    1.8340080864093424, 1.8539791250833855, 1.8741676341103, 1.8945759815869656, \
+    1.9152065613971474, 1.9360617934922943, 1.9571441241754002, 1.978456026387951}
+#if defined(__CUDACC__)
+static __device__ const double drm_log_inv_dev[64] = DRM_LOG_INV;
+static __device__ const double drm_log_l_dev[64] = DRM_LOG_L;
+static __device__ const double drm_exp_t_dev[64] = DRM_EXP_T;
+#endif
+static const double drm_log_inv_host[64] = DRM_LOG_INV;
+static const double drm_log_l_host[64] = DRM_LOG_L;
+static const double drm_exp_t_host[64] = DRM_EXP_T;
+#ifdef __CUDA_ARCH__
+#define DRM_TABLE(name, j) __ldg(drm_##name##_dev + (j))
+#else
+#define DRM_TABLE(name, j) (drm_##name##_host[(j)])
+#endif
+constexpr double kLn2By64Hi = 0.01083042469326756;  // ln2 / 64, 32 significant bits
+constexpr double kLn2By64Lo = 2.9815858269852933e-12;
+constexpr double k64ByLn2 = 92.33248261689366;
+
+// natural logarithm of a double: x = 2^k m, m in [1, 2); j = the top 6 bits
+// of m's fraction; log x = k ln2 + L[j] + log1p(m INV[j] - 1), |m INV[j] - 1|
+// < 1/64, log1p by its series to r^8
 DRM_FN double log_d(double x) {
     if (is_nan(x) || x < 0.0) return kInf - kInf;
     if (x == 0.0) return -kInf;
@@ -107,50 +178,38 @@ DRM_FN double log_d(double x) {
     }
     k += e - 1023;
     double m = from_bits((b & 0x000fffffffffffffLL) | 0x3ff0000000000000LL);  // [1, 2)
-    if (m > kSqrt2) {
-        m = mul(m, 0.5);
-        k += 1;
-    }
-    double s = div(sub(m, 1.0), add(m, 1.0));
-    double z = mul(s, s);
-    double p = 0.047619047619047616;
-    p = add(mul(p, z), 0.05263157894736842);
-    p = add(mul(p, z), 0.058823529411764705);
-    p = add(mul(p, z), 0.06666666666666667);
-    p = add(mul(p, z), 0.07692307692307693);
-    p = add(mul(p, z), 0.09090909090909091);
-    p = add(mul(p, z), 0.1111111111111111);
-    p = add(mul(p, z), 0.14285714285714285);
-    p = add(mul(p, z), 0.2);
-    p = add(mul(p, z), 0.3333333333333333);
-    p = add(mul(p, z), 1.0);
-    double lm = mul(2.0, mul(s, p));
+    int j = (int)((b >> 46) & 63);
+    double r = sub(mul(m, DRM_TABLE(log_inv, j)), 1.0);
+    double q = -0.125;
+    q = add(mul(q, r), 0.14285714285714285);
+    q = add(mul(q, r), -0.16666666666666666);
+    q = add(mul(q, r), 0.2);
+    q = add(mul(q, r), -0.25);
+    q = add(mul(q, r), 0.3333333333333333);
+    q = add(mul(q, r), -0.5);
+    q = add(mul(mul(q, r), r), r);
     double dk = (double)k;
-    return add(add(mul(dk, kLn2Hi), lm), mul(dk, kLn2Lo));
+    return add(add(mul(dk, kLn2Hi), DRM_TABLE(log_l, j)), add(q, mul(dk, kLn2Lo)));
 }
 
-// e^x of a double
+// e^x of a double: x = (64 m + j) ln2/64 + r, |r| <= ln2/128 (Cody-Waite);
+// e^x = 2^m T[j] e^r, e^r by its series to r^6
 DRM_FN double exp_d(double x) {
     if (is_nan(x)) return x;
     if (x > 709.0) return kInf;
     if (x < -745.5) return 0.0;
-    double k = round_int(mul(x, kInvLn2));
-    double r = sub(sub(x, mul(k, kLn2Hi)), mul(k, kLn2Lo));
-    double p = 1.6059043836821613e-10;
-    p = add(mul(p, r), 2.08767569878681e-09);
-    p = add(mul(p, r), 2.505210838544172e-08);
-    p = add(mul(p, r), 2.755731922398589e-07);
-    p = add(mul(p, r), 2.7557319223985893e-06);
-    p = add(mul(p, r), 2.48015873015873e-05);
-    p = add(mul(p, r), 0.0001984126984126984);
-    p = add(mul(p, r), 0.001388888888888889);
+    double kd = round_int(mul(x, k64ByLn2));
+    double r = sub(sub(x, mul(kd, kLn2By64Hi)), mul(kd, kLn2By64Lo));
+    double p = 0.001388888888888889;
     p = add(mul(p, r), 0.008333333333333333);
     p = add(mul(p, r), 0.041666666666666664);
     p = add(mul(p, r), 0.16666666666666666);
     p = add(mul(p, r), 0.5);
     p = add(mul(p, r), 1.0);
     p = add(mul(p, r), 1.0);
-    return scale2(p, (int)k);
+    int k = (int)kd;
+    int j = k & 63;
+    return scale2(mul(DRM_TABLE(exp_t, j), p), (k - j) / 64);
 }
 
 // sine and cosine of r, |r| <= pi/4 (+ rounding)

@@ -202,6 +202,68 @@ DEV_NOINLINE void trace_closest_pair_linear(const float4 *DR_RESTRICT tris, int 
     }
 }
 
+// Closest hits of two rays from one origin (the two sides of an edge sample,
+// whose directions differ by a few 1e-3) in one walk of the LBVH: a node is
+// entered when either ray enters one of its boxes before that ray's closest
+// hit so far, nearer child first by the smaller of the two entries, and a
+// leaf's triangle is tested against both rays with shared edge vectors.  Each
+// ray gets the hit its own walk finds: a box the other ray's walk enters holds
+// no closer hit for it (the test is conservative), and the rule (smallest t,
+// ties to the smaller triangle id) does not depend on the order of the tests.
+DEV_NOINLINE void trace_closest_pair_bvh(const float4 *DR_RESTRICT nodes, const float4 *DR_RESTRICT tris, int root,
+                                         float3 o, float3 d0, float3 d1, float tnear, Hit &h0, Hit &h1) {
+    h0.tri = h1.tri = -1;
+    h0.t = h1.t = DR_INF;
+    float3 i0 = f3(safe_inv(d0.x), safe_inv(d0.y), safe_inv(d0.z));
+    float3 i1 = f3(safe_inv(d1.x), safe_inv(d1.y), safe_inv(d1.z));
+    int stack[DR_STACK];
+    int sp = 0;
+    int node = root;
+    while (true) {
+        DR_COUNT_VISIT();
+        if (node < 0) {
+            int leaf = ~node;
+            float4 a = dr_ldg(tris + 3 * leaf), b = dr_ldg(tris + 3 * leaf + 1), c = dr_ldg(tris + 3 * leaf + 2);
+            TriRay r = tri_ray(a, b, c, o);
+            int id = dr_f2i(a.w);
+            float t;
+            if (hit_triangle(r, d0, t) && t > tnear && (t < h0.t || (t == h0.t && id < h0.tri))) {
+                h0.t = t;
+                h0.tri = id;
+            }
+            if (hit_triangle(r, d1, t) && t > tnear && (t < h1.t || (t == h1.t && id < h1.tri))) {
+                h1.t = t;
+                h1.tri = id;
+            }
+            if (sp == 0) break;
+            node = stack[--sp];
+            continue;
+        }
+        const float4 *n = nodes + 4 * node;
+        float4 n0 = dr_ldg(n), n1 = dr_ldg(n + 1), n2 = dr_ldg(n + 2), n3 = dr_ldg(n + 3);
+        float a0 = box_entry(n0.x, n0.y, n0.z, n0.w, n1.x, n1.y, o, i0, h0.t);
+        float b0 = box_entry(n0.x, n0.y, n0.z, n0.w, n1.x, n1.y, o, i1, h1.t);
+        float a1 = box_entry(n1.z, n1.w, n2.x, n2.y, n2.z, n2.w, o, i0, h0.t);
+        float b1 = box_entry(n1.z, n1.w, n2.x, n2.y, n2.z, n2.w, o, i1, h1.t);
+        int c0 = dr_f2i(n3.x), c1 = dr_f2i(n3.y);
+        bool x0 = a0 >= 0.f || b0 >= 0.f, x1 = a1 >= 0.f || b1 >= 0.f;
+        if (x0 && x1) {
+            float e0 = a0 >= 0.f ? (b0 >= 0.f ? fminf(a0, b0) : a0) : b0;
+            float e1 = a1 >= 0.f ? (b1 >= 0.f ? fminf(a1, b1) : a1) : b1;
+            int nearc = e0 <= e1 ? c0 : c1, farc = e0 <= e1 ? c1 : c0;
+            if (sp < DR_STACK) stack[sp++] = farc;
+            node = nearc;
+        } else if (x0) {
+            node = c0;
+        } else if (x1) {
+            node = c1;
+        } else {
+            if (sp == 0) break;
+            node = stack[--sp];
+        }
+    }
+}
+
 DEV Hit trace_closest(const DevScene &s, float3 o, float3 d, float tnear) {
     if (s.num_tris == 0) {
         Hit h;

@@ -132,12 +132,15 @@ def heightfield(seed=0, resolution=(640, 480), spp=64, max_bounces=3, grid=256,
         H += amp * np.sin(freq[0] * X + phase[0]) * np.sin(freq[1] * Z + phase[1])
     npatch = (grid - 1 + patch - 1) // patch
     mats, shapes = [], []
+    gidx = np.arange(grid * grid).reshape(grid, grid)
+    patch_grid_index = []  # per patch shape: the grid index of each of its vertices
     for pj in range(npatch):
         for pi in range(npatch):
             i0, i1 = pi * patch, min((pi + 1) * patch, grid - 1)
             j0, j1 = pj * patch, min((pj + 1) * patch, grid - 1)
             sub = np.stack([X[j0:j1 + 1, i0:i1 + 1], H[j0:j1 + 1, i0:i1 + 1],
                             Z[j0:j1 + 1, i0:i1 + 1]], -1).reshape(-1, 3)
+            patch_grid_index.append(gidx[j0:j1 + 1, i0:i1 + 1].reshape(-1))
             w = i1 - i0 + 1
             idx = []
             for j in range(j1 - j0):
@@ -159,8 +162,11 @@ def heightfield(seed=0, resolution=(640, 480), spp=64, max_bounces=3, grid=256,
     shapes.append(Shape(_t(l1v), _t(l1i, np.int32), None, None, black))
     lights = [Light(len(shapes) - 2, _t([10.0, 10.0, 10.0])),
               Light(len(shapes) - 1, _t([5.0, 5.0, 5.0]))]
+    # meta: the height grid and how the patches' vertices map onto it (the
+    # inverse-rendering loop optimises the grid's heights)
     return Workload("heightfield", cam, mats, shapes, lights, res, int(spp),
-                    int(max_bounces), {"seed": seed})
+                    int(max_bounces), {"seed": seed, "grid": grid, "patch": patch,
+                                       "heights": H.astype(np.float32), "patch_grid_index": patch_grid_index})
 
 
 BUILDERS = {"single_triangle": single_triangle, "soft_shadow": soft_shadow,
