@@ -74,6 +74,9 @@ def parse():
     p.add_argument("--proposal-seeds", type=int, default=32, help="seeds per arm of the learned-vs-plain measurement")
     p.add_argument("--proposal-train", type=int, default=60, help="training calls before the learned arm")
     p.add_argument("--workload", default=DEFAULT_WORKLOAD, choices=sorted(WORKLOADS))
+    p.add_argument("--res", type=int, nargs=2, default=None, metavar=("W", "H"),
+                   help="render this size instead of the workload's (smaller cases for ncu captures)")
+    p.add_argument("--step-spp", type=int, default=None, help="samples per pixel of one step instead of the workload's")
     p.add_argument("--no-inverse", action="store_true", help="skip the inverse-rendering loop measurement")
     p.add_argument("--inverse-steps", type=int, default=200, help="Adam steps per arm of the inverse-rendering loop")
     return p.parse_args()
@@ -240,9 +243,9 @@ MLP_FLOP_PER_QUERY = 21760
 
 def measure_proposal(dev, K=32, train_calls=60):
     """Gradient variance x time, learned vs plain edge sampling, on two scenes:
-    a reduced glossy heightfield (64 x 64-vertex grid, 7,938 triangles, 16
-    patches, 80 x 60, 1 spp, B = 1) and a small one (10 x 10 grid, 162
-    triangles, 96 x 72, 4 spp, B = 1, 3K seeds).  Per scene: K seeds of plain
+    the glossy heightfield configuration's full mesh (130,054 triangles, 64
+    patches, B = 3) at 160 x 120, 1 spp, and a small heightfield (10 x 10
+    grid, 162 triangles, 96 x 72, 4 spp, B = 1, 3K seeds).  Per scene: K seeds of plain
     sampling, K more as a noise calibration (plain vs plain), `train_calls`
     backward calls of online training, then K seeds with the trained proposal.
     Per parameter the variance ratio is var_learned / var_plain; its geometric
@@ -258,8 +261,8 @@ def measure_proposal(dev, K=32, train_calls=60):
     def small_heightfield():
         return workloads.heightfield(seed=8, resolution=(96, 72), spp=4, max_bounces=1, grid=10, patch=10)
 
-    cases = [("heightfield 64x64-vertex grid (7,938 triangles), 80x60, 1 spp, max_bounces=1",
-              lambda: workloads.heightfield(seed=0, resolution=(80, 60), spp=1, max_bounces=1, grid=64, patch=16), K),
+    cases = [("glossy heightfield configuration's mesh (130,054 triangles), 160x120, 1 spp, max_bounces=3",
+              lambda: workloads.heightfield(seed=0, resolution=(160, 120), spp=1, max_bounces=3), K),
              ("heightfield 10x10-vertex grid (162 triangles), 96x72, 4 spp, max_bounces=1", small_heightfield, 3 * K)]
     out = {"gradient": "image sum, dp_mode sum", "mix": 0.8, "train_calls": train_calls,
            "statistic": "geometric mean over parameters of var_learned / var_plain", "higher_is_better": False,
@@ -339,6 +342,8 @@ def load_profile(kernel):
     <dram bytes> <l2 hit %> <l2 throughput % of peak> <units>" lines; the
     capture may be of a smaller case of the same scene, so its DRAM bytes are
     scaled by the units processed: samples, or the items of the call), if any."""
+    if WORKLOAD_KEY is None:
+        return None
     path = os.path.join(ROOT, "profiles", f"kernels_{WORKLOAD_KEY}.txt")
     try:
         with open(path) as f:
@@ -640,8 +645,14 @@ def run_b200(args):
 def main():
     global WORKLOAD, WORKLOAD_KEY
     args = parse()
-    WORKLOAD = WORKLOADS[args.workload]
+    WORKLOAD = dict(WORKLOADS[args.workload])
     WORKLOAD_KEY = args.workload
+    if args.res or args.step_spp:  # a smaller case of the same scene (profiling captures)
+        if args.res:
+            WORKLOAD["resolution"] = tuple(args.res)
+        if args.step_spp:
+            WORKLOAD["step_spp"] = WORKLOAD["spp"] = args.step_spp
+        WORKLOAD_KEY = None  # no profile table, no inverse loop, no proposal report
     if args.impl == "reference":
         return run_reference(args)
     return run_b200(args)

@@ -153,27 +153,54 @@ DEV float3 node_corner(const DevEdgeNode &n, int i) {
     return f3((i & 1) ? n.hi[0] : n.lo[0], (i & 2) ? n.hi[1] : n.lo[1], (i & 4) ? n.hi[2] : n.lo[2]);
 }
 
-DEV_NOINLINE float bsdf_bound(const DevEdgeNode &node, float3 wi, const SurfacePoint &sp, float dl, float sl, float rough,
-                              int model) {
+// What the BSDF bound of an edge-tree node needs of the shading point: its
+// position and normal, the frame around the incoming direction wi (rows
+// t, b = normalize(n x wi), n = wi) and the normal in it, the lobes'
+// luminances and the lobe's exponent or GGX parameter.  Computed once per
+// walk; the per-node arithmetic is that of edge_tree.cpp:345-480.
+struct BoundCtx {
+    float3 p, n;
+    Frame hf;
+    float3 ln;
+    float dl, sl, rough, expo;
+    int model;
+};
+DEV BoundCtx bound_ctx(float3 wi, const SurfacePoint &sp, float dl, float sl, float rough, int model) {
+    BoundCtx c;
+    c.p = sp.p;
+    c.n = sp.f.n;
+    c.dl = dl;
+    c.sl = sl;
+    c.rough = rough;
+    c.model = model;
+    c.expo = 0.f;
+    if (sl > 0.f) {
+        float3 hy = normalize(cross(sp.f.n, wi));
+        c.hf.t = normalize(cross(wi, hy));
+        c.hf.b = hy;
+        c.hf.n = wi;
+        c.ln = to_local(c.hf, sp.f.n);
+        c.expo = model == DR_MICROFACET_GGX ? ggx_A(rough) : roughness_to_phong(rough);
+    }
+    return c;
+}
+
+DEV_NOINLINE float bsdf_bound(const DevEdgeNode &node, const BoundCtx &c) {
     float cos_max = 0.f;
     for (int i = 0; i < 8; i++)
-        if (dot(sp.f.n, node_corner(node, i) - sp.p) > 0.f) {
+        if (dot(c.n, node_corner(node, i) - c.p) > 0.f) {
             cos_max = 1.f;
             break;
         }
     if (cos_max <= 0.f) return 0.f;
     float maxp = 0.f;
-    if (sl > 0.f) {
-        float3 hy = normalize(cross(sp.f.n, wi));
-        Frame hf;
-        hf.t = normalize(cross(wi, hy));
-        hf.b = hy;
-        hf.n = wi;
+    if (c.sl > 0.f) {
+        const Frame &hf = c.hf;
         float3 lo = f3(DR_INF), hi = f3(-DR_INF);
         for (int i = 0; i < 8; i++) {
-            float3 c = to_local(hf, node_corner(node, i) - sp.p);
-            lo = f3(fminf(lo.x, c.x), fminf(lo.y, c.y), fminf(lo.z, c.z));
-            hi = f3(fmaxf(hi.x, c.x), fmaxf(hi.y, c.y), fmaxf(hi.z, c.z));
+            float3 q = to_local(hf, node_corner(node, i) - c.p);
+            lo = f3(fminf(lo.x, q.x), fminf(lo.y, q.y), fminf(lo.z, q.z));
+            hi = f3(fmaxf(hi.x, q.x), fmaxf(hi.y, q.y), fmaxf(hi.z, q.z));
         }
         float cphi = 0.f;
         float hx = hi.x;
@@ -186,21 +213,21 @@ DEV_NOINLINE float bsdf_bound(const DevEdgeNode &node, float3 wi, const SurfaceP
         if (hi.z > 0.f) cto_max = hi.z / (min_sq_bound(lo.x, hi.x) + min_sq_bound(lo.y, hi.y) + hi.z * hi.z);
         else cto_max = hi.z / (max_sq_bound(lo.x, hi.x) + max_sq_bound(lo.y, hi.y) + hi.z * hi.z);
         float cth_min = sqrtf((cto_min + 1.f) / 2.f), cth_max = sqrtf((cto_max + 1.f) / 2.f);
-        float3 ln = to_local(hf, sp.f.n);
+        const float3 ln = c.ln;
         float chmax = cphi >= 0.f ? sqrtf(ln.z * ln.z / (ln.z * ln.z + ln.x * ln.x * cphi * cphi)) : 1.f;
         if (chmax > cth_max) chmax = cth_max;
         else if (chmax < cth_min) chmax = cth_min;
         float shmax = sqrtf(fmaxf(1.f - chmax * chmax, 0.f));
         float hdn = fminf(fabsf(ln.x * shmax * cphi) + ln.z * chmax, 1.f);
-        if (model == DR_MICROFACET_GGX) {
+        if (c.model == DR_MICROFACET_GGX) {
             // the GGX D grows with n.h (A <= 1): its bound is the value at the bound of n.h
-            maxp = ggx_D(hdn, ggx_A(rough));
+            maxp = ggx_D(hdn, c.expo);
         } else {
-            float e = roughness_to_phong(rough);
+            float e = c.expo;
             maxp = dr_powf(hdn, e) * (e + 2.f) / float(2 * 3.14159265358979323846);
         }
     }
-    return cos_max * (dl / DR_PI + sl * maxp);
+    return cos_max * (c.dl / DR_PI + c.sl * maxp);
 }
 
 DEV_NOINLINE bool contains_silhouette(const DevEdgeNode &node, float3 p) {
@@ -294,6 +321,7 @@ DEV bool traverse_mode(const bool CONE, const DevScene &s, const DevEdgeNode *no
                        const EdgeTask &start, const NodeRng &rng, Emit &emit, const EdgeProposal &pr, int tree,
                        bool learned, Defer &defer, int *visits = nullptr) {
     using Item = EdgeItem<PROP>;
+    const BoundCtx bc = bound_ctx(wi, sp, dl, sl, rough, model);
     Item st[DR_EDGE_STACK];
     int sp_ = 0;
     st[sp_++] = edge_item<PROP>(start.code & DR_NODE_MASK, start.bb, start.cpmf, start.apmf, start.lpmf);
@@ -334,8 +362,8 @@ DEV bool traverse_mode(const bool CONE, const DevScene &s, const DevEdgeNode *no
             lcs = contains_silhouette(L, sp.p);
             rcs = contains_silhouette(R, sp.p);
         }
-        float lbb = lcs ? bsdf_bound(L, wi, sp, dl, sl, rough, model) : 0.f;
-        float rbb = rcs ? bsdf_bound(R, wi, sp, dl, sl, rough, model) : 0.f;
+        float lbb = lcs ? bsdf_bound(L, bc) : 0.f;
+        float rbb = rcs ? bsdf_bound(R, bc) : 0.f;
         float il = lcs ? node_importance(L, lbb, sp.p) : 0.f;
         float ir = rcs ? node_importance(R, rbb, sp.p) : 0.f;
         if (il + ir <= 1e-10f) continue;
@@ -436,7 +464,7 @@ DEV bool traverse_edges(const DevScene &s, float3 wi, int stri, const SurfacePoi
     const DevMaterial &m = s.mats[material_of_tri(s, stri)];
     float dl = luminance(get_kd(s, m, sp.uv)), sl = luminance(get_ks(s, m, sp.uv));
     float rough = get_rough(s, m, sp.uv);
-    float b = bsdf_bound(nodes[0], wi, sp, dl, sl, rough, m.model);
+    float b = bsdf_bound(nodes[0], bound_ctx(wi, sp, dl, sl, rough, m.model));
     auto em = [&](int ei, int key, float w, int code) { emit(tree, ei, key, w, code); };
     EdgeTask root;
     root.point = 0;

@@ -44,6 +44,7 @@ def load():
         L.hh_math.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_longlong]
         L.hh_scene_edges.argtypes = [C.POINTER(_abi.dr_scene_desc), C.c_int, C.c_void_p, C.c_longlong]
         L.hh_scene_edges.restype = C.c_longlong
+        L.hh_trace_pairs.argtypes = [C.POINTER(_abi.dr_scene_desc), C.c_void_p, C.c_int, C.c_void_p]
         _lib = L
     return _lib
 
@@ -115,3 +116,15 @@ def scene_edges(wl, what):
     buf = np.zeros(max(1, n * elem), np.uint8)
     L.hh_scene_edges(C.byref(sd.desc), code, buf.ctypes.data, buf.size)
     return buf[:n * elem].tobytes()
+
+
+def trace_pairs(wl, rays):
+    """[n, 9] ray pairs -> [n, 4] hit ids: the paired walk's two, then two single walks'."""
+    from delta_ray_b200 import _abi
+    L = load()
+    cam, mats, shps, lts = _abi.scene_dicts(wl.camera, wl.materials, wl.shapes, wl.lights)
+    sd = _abi.SceneDesc.from_scene(cam, mats, shps, lts, torch.device("cpu"))
+    rays = np.ascontiguousarray(rays, np.float32)
+    out = np.zeros((rays.shape[0], 4), np.int32)
+    L.hh_trace_pairs(C.byref(sd.desc), rays.ctypes.data, rays.shape[0], out.ctypes.data)
+    return out

@@ -303,6 +303,24 @@ long long hh_scene_edges(const dr_scene_desc *desc, int what, void *out, long lo
     return (long long)count;
 }
 
+// Closest hits of n ray pairs [n][9] (origin, two directions) through the
+// paired LBVH walk (trace_closest_pair_bvh) and through two single walks:
+// out [n][4] = pair hit 0, pair hit 1, single hit 0, single hit 1.
+void hh_trace_pairs(const dr_scene_desc *desc, const float *rays, int n, int *out) {
+    HostSceneBundle b;
+    make_scene(desc, b);
+    for (int i = 0; i < n; i++) {
+        const float *r = rays + 9 * i;
+        float3 o = f3(r[0], r[1], r[2]), d0 = f3(r[3], r[4], r[5]), d1 = f3(r[6], r[7], r[8]);
+        Hit h0, h1;
+        trace_closest_pair_bvh(b.ds.bvh_nodes, b.ds.bvh_tris, b.ds.bvh_root, o, d0, d1, 1e-3f, h0, h1);
+        out[4 * i] = h0.tri;
+        out[4 * i + 1] = h1.tri;
+        out[4 * i + 2] = trace_closest_bvh(b.ds.bvh_nodes, b.ds.bvh_tris, b.ds.bvh_root, o, d0, 1e-3f).tri;
+        out[4 * i + 3] = trace_closest_bvh(b.ds.bvh_nodes, b.ds.bvh_tris, b.ds.bvh_root, o, d1, 1e-3f).tri;
+    }
+}
+
 // The reproducible transcendental functions (dr_math.h) on n inputs.
 void hh_math(int fn, const float *x, const float *y, float *out, long long n) {
     for (long long i = 0; i < n; i++) out[i] = dr_math_eval(fn, x[i], y ? y[i] : 0.f);

@@ -231,3 +231,23 @@ def test_icosphere_room_kernel_logic_matches_oracle():
         if parts == 2:
             assert h["stats"][1] == o["stats"][1]
         assert rel_err(h["grad"], o["grad"]) < TOL, parts
+
+
+def test_paired_lbvh_walk_finds_each_rays_own_hit():
+    """An edge sample's two rays (directions ~1e-3 apart) walk the LBVH
+    together: each must get the hit its own walk gets, on 20,000 pairs from
+    above the small heightfield, half of them grazing."""
+    import scenes
+    wl = scenes.heightfield_small(seed=1, grid=40)
+    rng = np.random.default_rng(3)
+    n = 20000
+    o = np.stack([rng.uniform(-5, 5, n), rng.uniform(0.2, 6, n), rng.uniform(-5, 5, n)], 1)
+    t = np.stack([rng.uniform(-5, 5, n), rng.uniform(-0.5, 0.5, n), rng.uniform(-5, 5, n)], 1)
+    d0 = t - o
+    d0[n // 2:, 1] *= 0.02  # grazing
+    d0 /= np.linalg.norm(d0, axis=1, keepdims=True)
+    d1 = d0 + rng.normal(0, 1e-3, d0.shape)
+    d1 /= np.linalg.norm(d1, axis=1, keepdims=True)
+    hits = harness.trace_pairs(wl, np.concatenate([o, d0, d1], 1))
+    assert (hits[:, 0] >= 0).mean() > 0.3
+    assert np.array_equal(hits[:, :2], hits[:, 2:])
