@@ -14,6 +14,7 @@
 #include <algorithm>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -561,6 +562,9 @@ std::pair<long long, long long> run_backward(dr_scene *scene, const dr_render_de
     const GradCacheCfg cfg = grad_cache_cfg(scene->h);
     BackwardCounters c;
     auto read = [&]() {
+        if (timer->failed)
+            throw DrError(DR_ERR_CUDA, std::string("kernel ") + timer->failed + " failed: " +
+                                           cudaGetErrorString(timer->failed_err));
         check_cuda(cudaMemcpyAsync(&c, ws.counters, sizeof(c), cudaMemcpyDeviceToHost, st), "status read");
         check_cuda(cudaStreamSynchronize(st), "backward");
         if (c.status & ~(DR_STATUS_ITEM_OVERFLOW | DR_STATUS_POINT_OVERFLOW))
@@ -739,6 +743,7 @@ dr_status dr_scene_create(const dr_scene_desc *desc, int device, dr_scene **out)
         check_cuda(cudaSetDevice(device), "cudaSetDevice");
         std::unique_ptr<dr_scene> sc(new dr_scene());
         sc->device = device;
+        sc->timer.sync = std::getenv("DR_DEBUG_SYNC") != nullptr;
         check_cuda(cudaDeviceGetAttribute(&sc->num_sms, cudaDevAttrMultiProcessorCount, device), "device query");
         load_desc(sc->h, desc, [](auto p, size_t n, const char *w) { return fetch(p, n, w); });
         long long ntri = 0;
@@ -814,6 +819,9 @@ dr_status dr_render_forward(dr_scene *scene, const dr_render_desc *rd, float *im
         check_cuda(dr_launch_forward(call_scene(scene, rd), rd->width, rd->height, rd->spp, rd->max_bounces, rd->seed, image_dev,
                                      (cudaStream_t)stream, &scene->last_launches, &scene->timer),
                    "forward launch");
+        if (scene->timer.failed)
+            throw DrError(DR_ERR_CUDA, std::string("kernel ") + scene->timer.failed + " failed: " +
+                                           cudaGetErrorString(scene->timer.failed_err));
         collect_timings(scene, (cudaStream_t)stream);
     });
 }

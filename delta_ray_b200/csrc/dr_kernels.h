@@ -8,9 +8,14 @@
 
 // Optional per-stage timing: events recorded on the launch stream around each
 // kernel when `on` is set (costs one event record per stage).
+// With `sync` set (the DR_DEBUG_SYNC environment variable, a diagnostic), every
+// mark synchronizes the stream and remembers the first kernel that failed.
 struct StageTimer {
     static const int kMax = 16;
     bool on = false;
+    bool sync = false;
+    const char *failed = nullptr;
+    cudaError_t failed_err = cudaSuccess;
     int n = 0;
     cudaEvent_t ev[kMax + 1];
     const char *names[kMax];
@@ -19,6 +24,13 @@ struct StageTimer {
         if (on) cudaEventRecord(ev[0], st);
     }
     void mark(cudaStream_t st, const char *name) {
+        if (sync && !failed) {
+            cudaError_t e = cudaStreamSynchronize(st);
+            if (e != cudaSuccess) {
+                failed = name;
+                failed_err = e;
+            }
+        }
         if (!on || n >= kMax) return;
         names[n++] = name;
         cudaEventRecord(ev[n], st);
