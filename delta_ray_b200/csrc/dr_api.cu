@@ -571,8 +571,15 @@ std::pair<long long, long long> run_backward(dr_scene *scene, const dr_render_de
             throw DrError(DR_ERR_DEVICE_STATUS, "device reported status " + std::to_string(c.status));
     };
     long long work[8] = {};
+    // with the DR_DEBUG_SYNC diagnostic, a launch error names the kernel that failed
+    auto check_launch = [&](cudaError_t e, const char *what) {
+        if (e != cudaSuccess && timer->failed)
+            throw DrError(DR_ERR_CUDA, std::string("kernel ") + timer->failed + " failed: " +
+                                           cudaGetErrorString(timer->failed_err));
+        check_cuda(e, what);
+    };
     auto back = [&]() {
-        check_cuda(dr_launch_backward_back(ds, rd->width, rd->height, rd->spp, rd->max_bounces, rd->seed, grad_dev,
+        check_launch(dr_launch_backward_back(ds, rd->width, rd->height, rd->spp, rd->max_bounces, rd->seed, grad_dev,
                                            rd->dp_mode, ws, cfg, scene->num_sms, st, &scene->last_launches, timer),
                    "backward launch");
         // the stage's work counts (the counters of the evaluation wavefront
@@ -588,11 +595,11 @@ std::pair<long long, long long> run_backward(dr_scene *scene, const dr_render_de
         check_cuda(cudaMemsetAsync(grad_dev, 0, sizeof(float) * scene->h.grad_total, st), "memset");
         ws.pt_begin = 0;
         ws.pt_end = ws.cap_points;
-        check_cuda(dr_launch_backward_front(ds, rd->width, rd->height, rd->spp, rd->max_bounces, rd->seed,
-                                            d_image_dev, grad_dev, image_dev, rd->primary_edge_samples, rd->dp_mode,
-                                            ws, cfg, scene->num_sms, st, &scene->last_launches, timer,
-                                            prop == nullptr),
-                   "backward launch");
+        check_launch(dr_launch_backward_front(ds, rd->width, rd->height, rd->spp, rd->max_bounces, rd->seed,
+                                              d_image_dev, grad_dev, image_dev, rd->primary_edge_samples, rd->dp_mode,
+                                              ws, cfg, scene->num_sms, st, &scene->last_launches, timer,
+                                              prop == nullptr),
+                     "backward launch");
         read();
         if (!(c.status & DR_STATUS_POINT_OVERFLOW)) break;
         const long long needed = (long long)c.points;
@@ -654,8 +661,8 @@ std::pair<long long, long long> run_backward(dr_scene *scene, const dr_render_de
             ws.pt_end = p1;
             // reset the item counter and the status word (items, status, pad)
             check_cuda(cudaMemsetAsync(&ws.counters->items, 0, 16, st), "memset");
-            check_cuda(dr_launch_edge_traverse(ds, rd->seed, ws, scene->num_sms, st, &scene->last_launches, timer),
-                       "edge traversal launch");
+            check_launch(dr_launch_edge_traverse(ds, rd->seed, ws, scene->num_sms, st, &scene->last_launches, timer),
+                         "edge traversal launch");
             read();
             if (c.status & DR_STATUS_ITEM_OVERFLOW) {
                 needed = (long long)c.items;

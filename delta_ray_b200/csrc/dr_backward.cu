@@ -18,7 +18,7 @@
 // without FMA contraction, so that the first vertex of every path (which
 // decides which edges a shading point sees) has the bits of the reference's
 // CPU arithmetic.  The edge kernels (dr_edge_kernels.cu) start from the
-// stored vertex and are compiled with contraction.
+// stored vertex and are compiled without contraction too.
 // Gradients of the small, shared parameters (camera, constant materials,
 // light intensities) are reduced per block in shared memory and flushed with
 // one atomic per nonzero entry; per-vertex gradients go straight to global

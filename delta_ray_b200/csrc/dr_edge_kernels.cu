@@ -1,7 +1,7 @@
 // Backward pass, edge half: edge-tree traversal of the shading points, the
 // secondary edge samples they drew, and the primary (screen-space) edges.
-// Compiled with FMA contraction; every input comes from the stored point
-// records, whose bits the path half fixes.
+// Compiled without FMA contraction, like the path half: the edge-tree choices,
+// line samples and ray tests must take the oracle's branches.
 #include "../../include/delta_ray_b200.h"
 #include "dr_backward.cuh"
 #include "dr_block_grad.cuh"
@@ -120,12 +120,15 @@ __global__ void __launch_bounds__(128, 4) k_edge_expand(DevScene s, uint64_t see
             EdgeTask tb[DR_TASK_BUF];
             int nt = 0;
             bool ok = true;
+            // every reserved slot below the queue's capacity is written (the
+            // second stage reads all of them); subtrees beyond it are walked here
             auto flush = [&]() {
                 unsigned long long first = atomicAdd(&ws.counters->tasks, (unsigned long long)nt);
-                if (first + (unsigned long long)nt <= (unsigned long long)ws.cap_tasks) {
-                    for (int k = 0; k < nt; k++) ws.tasks[first + k] = tb[k];
-                } else {  // no room: walk them here
-                    for (int k = 0; k < nt; k++) ok &= traverse_point_task<PROP>(s, pt, seed, tb[k], emit, pr, &visits);
+                for (int k = 0; k < nt; k++) {
+                    if (first + (unsigned long long)k < (unsigned long long)ws.cap_tasks)
+                        ws.tasks[first + k] = tb[k];
+                    else
+                        ok &= traverse_point_task<PROP>(s, pt, seed, tb[k], emit, pr, &visits);
                 }
                 nt = 0;
             };
@@ -159,7 +162,9 @@ __global__ void __launch_bounds__(128, 6) k_edge_tasks(DevScene s, uint64_t seed
             if (!traverse_point_task<PROP>(s, pt, seed, t, emit, point_proposal(ws, t.point), &visits))
                 set_status(&ws.counters->status, DR_STATUS_STACK_OVERFLOW);
         }
-        if (out.nb == DR_ITEM_BUF) out.flush_warp();  // keeps lanes' buffers from carrying over long
+        // keeps lanes' buffers from carrying over long; flush_warp is a warp
+        // collective, so the whole warp decides (the loop is warp-uniform)
+        if (__any_sync(0xffffffffu, out.nb == DR_ITEM_BUF)) out.flush_warp();
     }
     out.flush_warp();
     add_visits(&ws.counters->visits_tasks, visits);

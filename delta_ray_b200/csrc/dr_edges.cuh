@@ -1070,7 +1070,12 @@ DEV void primary_edge_grad(const DevScene &s, const PrimaryGeom &g, const DevEdg
     const float3 v0 = g.v0, v1 = g.v1, d0 = g.d0, d1 = g.d1, vd = g.vd;
     const float2 s0 = g.s0, s1 = g.s1, ept = g.ept;
     const float t = g.t, delta = g.delta;
+    // the edge point is on the screen (in_screen: [0, 1)^2), but ept.x * W
+    // can round up to W when W is a power of two; the reference reads past the
+    // row there (delta_ray.cpp:411-416), this clamps to the last pixel
     int xi = int(ept.x * W), yi = int(ept.y * H);
+    xi = xi < W ? xi : W - 1;
+    yi = yi < H ? yi : H - 1;
     const float *dc = d_image + 3 * ((size_t)yi * W + xi);
     float3 d_color = f3(dr_ldg(dc), dr_ldg(dc + 1), dr_ldg(dc + 2));
     float2 rpt = primary_side_point(cam, g, 0), lpt = primary_side_point(cam, g, 1);

@@ -255,6 +255,53 @@ int hh_render(const dr_scene_desc *desc, const dr_render_desc *rd, const float *
     return 0;
 }
 
+// The edge-tree traversal (no evaluation) of shading points [p0, p1) of a
+// backward render: the path stage runs over the whole image, then only those
+// points are walked, two-stage when `split` (subtrees at depth 8 handed on and
+// walked after the point, as the GPU's k_edge_expand / k_edge_tasks do).
+// Every `step`-th point of the range is walked.  Returns the number of
+// sampled edges; *points receives the point count.
+long long hh_traverse_range(const dr_scene_desc *desc, const dr_render_desc *rd, long long p0, long long p1, int split,
+                            long long *points, long long step) {
+    HostSceneBundle b;
+    make_scene(desc, b);
+    b.ds.specular_chains = b.h.specular_bounces && rd->max_bounces >= 1;
+    const DevScene &s = b.ds;
+    int W = rd->width, H = rd->height, spp = rd->spp, B = rd->max_bounces;
+    std::vector<double> g(b.h.grad_total, 0.0);
+    HostSink sink{&g};
+    std::vector<PointRecord> pts;
+    auto push = [&](const PointRecord &pr) { pts.push_back(pr); };
+    const float3 one = f3(1.f, 1.f, 1.f);
+    for (int y = 0; y < H; y++)
+        for (int x = 0; x < W; x++)
+            for (int si = 0; si < spp; si++) {
+                if (s.specular_chains) backward_pixel_sample<true>(s, x, y, W, H, spp, si, B, rd->seed, one, sink, push);
+                else backward_pixel_sample<false>(s, x, y, W, H, spp, si, B, rd->seed, one, sink, push);
+            }
+    *points = (long long)pts.size();
+    long long n = 0;
+    EdgeProposal pr;
+    pr.q = nullptr;
+    pr.alpha = 0.f;
+    pr.codes = false;
+    auto emit = [&](int, int, int, float, int) { n++; };
+    if (step < 1) step = 1;
+    for (long long p = std::max(0ll, p0); p < std::min((long long)pts.size(), p1); p += step) {
+        if (split) {
+            std::vector<EdgeTask> tasks;
+            auto defer = [&](int code, float bb, float c, float a, float l) {
+                tasks.push_back(EdgeTask{(int)p, code, bb, c, a, l});
+            };
+            traverse_point<false, 8>(s, pts[p], rd->seed, emit, pr, &defer);
+            for (const EdgeTask &t : tasks) traverse_point_task<false>(s, pts[p], rd->seed, t, emit, pr);
+        } else {
+            traverse_point<false>(s, pts[p], rd->seed, emit, pr);
+        }
+    }
+    return n;
+}
+
 void hh_set_split(int on) { g_split = on; }
 
 // The synthetic proposal of later hh_render calls (seed 0: none).
