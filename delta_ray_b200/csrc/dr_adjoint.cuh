@@ -13,13 +13,6 @@
 
 #include "dr_shading.cuh"
 
-#ifdef DR_HOST_BUILD
-#include <cmath>
-HD bool dr_isfinite(float x) { return std::isfinite(x); }
-#else
-DEV bool dr_isfinite(float x) { return isfinite(x); }
-#endif
-
 #define DR_INV_2PI (1.f / float(2 * 3.14159265358979323846))
 
 // Adjoints of a shading point's inputs collected by the material functions.

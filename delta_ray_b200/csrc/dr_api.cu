@@ -87,6 +87,7 @@ struct BackwardQueues {
     DevBuf pt, items, item_w, item_dp, pt_last, counts, survivors, hits, tasks;
     long long cap_items = 0;     // grown on overflow, kept with the buffers
     double points_per_sample = 1;  // shading points per pixel sample the last overflow asked for
+    double items_per_point = 0;    // sampled edges per shading point of the last call (0: none yet)
     cudaEvent_t idle = nullptr;
     ~BackwardQueues() {
         if (idle) cudaEventDestroy(idle);
@@ -557,7 +558,8 @@ template <class Grow, class GrowPoints>
 std::pair<long long, long long> run_backward(dr_scene *scene, const dr_render_desc *rd, const float *d_image_dev,
                                              float *grad_dev, float *image_dev, BackwardWorkspace &ws,
                                              cudaStream_t st, StageTimer *timer, Grow grow, GrowPoints grow_points,
-                                             ProposalState *prop = nullptr, const DevScene *view = nullptr) {
+                                             ProposalState *prop = nullptr, const DevScene *view = nullptr,
+                                             double *items_per_point = nullptr) {
     const DevScene ds = view ? *view : call_scene(scene, rd);
     const GradCacheCfg cfg = grad_cache_cfg(scene->h);
     BackwardCounters c;
@@ -590,6 +592,12 @@ std::pair<long long, long long> run_backward(dr_scene *scene, const dr_render_de
         work[4] += (long long)c.tasks;
         work[5] += (long long)(ds.split_traversal ? c.items_expand : c.items);
     };
+    // when the last call's edges per point predict more items than the queue
+    // can ever hold, the edge stage streams from the start instead of
+    // traversing every point once only to find that out
+    const long long samples = (long long)rd->width * rd->height * rd->spp;
+    const bool stream_first = prop == nullptr && items_per_point && *items_per_point > 0 &&
+                              (double)samples * *items_per_point > (double)kMaxQueueItems;
     for (int attempt = 0;; attempt++) {
         check_cuda(cudaMemsetAsync(ws.counters, 0, sizeof(BackwardCounters), st), "memset");
         check_cuda(cudaMemsetAsync(grad_dev, 0, sizeof(float) * scene->h.grad_total, st), "memset");
@@ -598,7 +606,7 @@ std::pair<long long, long long> run_backward(dr_scene *scene, const dr_render_de
         check_launch(dr_launch_backward_front(ds, rd->width, rd->height, rd->spp, rd->max_bounces, rd->seed,
                                               d_image_dev, grad_dev, image_dev, rd->primary_edge_samples, rd->dp_mode,
                                               ws, cfg, scene->num_sms, st, &scene->last_launches, timer,
-                                              prop == nullptr),
+                                              prop == nullptr && !stream_first),
                      "backward launch");
         read();
         if (!(c.status & DR_STATUS_POINT_OVERFLOW)) break;
@@ -646,12 +654,12 @@ std::pair<long long, long long> run_backward(dr_scene *scene, const dr_render_de
         if (mst) throw DrError(DR_ERR_DEVICE_STATUS, "proposal network reported status " + std::to_string(mst));
     }
     long long items = 0;
-    if (!(c.status & DR_STATUS_ITEM_OVERFLOW)) {
+    if (!stream_first && !(c.status & DR_STATUS_ITEM_OVERFLOW)) {
         timer->mark(st, "host_queue_check");
         back();
         items = (long long)c.items;
     } else {
-        long long needed = (long long)c.items;
+        long long needed = stream_first ? (long long)std::ceil((double)P * *items_per_point) : (long long)c.items;
         long long cap = grow(needed + needed / 8 + 1);
         long long chunk = cap >= needed ? P : std::max(1ll, (long long)((double)P * cap / needed * 0.9));
         long long p0 = 0;
@@ -676,6 +684,9 @@ std::pair<long long, long long> run_backward(dr_scene *scene, const dr_render_de
             }
             back();
             items += (long long)c.items;
+            // the next chunk sized from this one's edges per point
+            if (c.items > 0)
+                chunk = std::max(1ll, (long long)((double)(p1 - p0) * cap / (double)c.items * 0.9));
             p0 = p1;
         }
     }
@@ -706,6 +717,7 @@ std::pair<long long, long long> run_backward(dr_scene *scene, const dr_render_de
         pr.steps++;
     }
     check_cuda(cudaStreamSynchronize(st), "backward");
+    if (items_per_point && P > 0) *items_per_point = (double)items / (double)P;
     work[0] = P;
     work[1] = items;
     work[6] = (long long)c.visits_walk;
@@ -906,7 +918,7 @@ void backward_on_queues(dr_scene *scene, const dr_render_desc *rd, const DevScen
         prop = scene->proposal.get();
     }
     auto counts = run_backward(scene, rd, d_image_dev, grad_dev, image_dev, ws, st, &scene->timer, grow, grow_points,
-                               prop, view);
+                               prop, view, &q.items_per_point);
     scene->last_points = counts.first;
     scene->last_items = counts.second;
 }

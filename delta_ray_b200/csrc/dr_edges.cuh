@@ -367,7 +367,11 @@ DEV bool traverse_mode(const bool CONE, const DevScene &s, const DevEdgeNode *no
         float il = lcs ? node_importance(L, lbb, sp.p) : 0.f;
         float ir = rcs ? node_importance(R, rbb, sp.p) : 0.f;
         if (il + ir <= 1e-10f) continue;
-        bool lhc = box_cone(L.lo, L.hi, cone), rhc = box_cone(R.lo, R.hi, cone);
+        // a node the cone walk cannot reach (cpmf 0) gives its children cpmf
+        // 0 whatever the cone tests say, as long as the importances are
+        // finite: the all walk skips the tests there
+        const bool cone_tests = CONE || it.cpmf != 0.f || !dr_isfinite(il) || !dr_isfinite(ir);
+        bool lhc = cone_tests && box_cone(L.lo, L.hi, cone), rhc = cone_tests && box_cone(R.lo, R.hi, cone);
         bool cone_split = all_split || (lhc && rhc && lcs && rcs && cone.cos_angle > 0.95f);
         float ilc = lhc ? il : 0.f, irc = rhc ? ir : 0.f;
         if (CONE && ilc + irc <= 1e-10f) continue;

@@ -17,6 +17,13 @@
 
 #include "dr_trace.cuh"
 
+#ifdef DR_HOST_BUILD
+#include <cmath>
+HD bool dr_isfinite(float x) { return std::isfinite(x); }
+#else
+DEV bool dr_isfinite(float x) { return isfinite(x); }
+#endif
+
 DEV bool is_light_tri(const DevScene &s, int tri) { return s.shapes[s.tri[tri].w].light >= 0; }
 DEV int light_of_tri(const DevScene &s, int tri) { return s.shapes[s.tri[tri].w].light; }
 DEV int material_of_tri(const DevScene &s, int tri) { return s.shapes[s.tri[tri].w].mat; }

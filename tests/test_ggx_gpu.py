@@ -33,7 +33,12 @@ def test_ggx_matches_oracle(builder, ltc_table):
     grad, _ = sc.backward(W, H, wl.spp, wl.max_bounces, 31, torch.from_numpy(d_image).cuda())
     o = oracle.oracle_render(wl, 31, d_image, rng_mode=oracle.PHILOX, ltc_table=ltc_table, ltc_table_ggx=ggx)
     assert tuple(sc.last_counts()) == tuple(o["stats"])
-    assert_image_parity(img, o["image"])
+    # the forward against the oracle's forward: the oracle's backward values
+    # divide through the reciprocal (autodiff.h:161-180), and a GGX peak at
+    # low roughness (k = z^2 (A - 1) + 1 near 0) turns that rounding into
+    # ~1e-3 on a sample
+    of = oracle.oracle_render(wl, 31, None, rng_mode=oracle.PHILOX, ltc_table=ltc_table, ltc_table_ggx=ggx)
+    assert_image_parity(img, of["image"])
     assert_grad_parity(grad.cpu().numpy(), o["grad"])
     sc.close()
 
