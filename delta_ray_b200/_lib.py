@@ -42,6 +42,7 @@ def lib():
     L.dr_trace_rays.argtypes = [C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p]
     L.dr_eval_math.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p]
     L.dr_scene_last_work.argtypes = [C.c_void_p, C.c_void_p, C.c_int]
+    L.dr_set_item_queue_limit.argtypes = [C.c_int64]
     L.dr_scene_edge_data.argtypes = [C.c_void_p, C.c_int, C.c_void_p, C.c_int64, C.POINTER(C.c_int64),
                                      C.POINTER(C.c_float)]
     L.dr_scene_set_profiling.argtypes = [C.c_void_p, C.c_int]
@@ -58,7 +59,9 @@ def lib():
     L.dr_last_error.restype = C.c_size_t
     for name in ("dr_scene_create", "dr_scene_update", "dr_scene_destroy", "dr_scene_grad_layout",
                  "dr_render_forward", "dr_render_backward", "dr_scene_last_launch_count", "dr_trace_rays",
-                 "dr_scene_set_profiling", "dr_scene_last_timings", "dr_scene_last_counts", "dr_eval_math", "dr_scene_edge_data", "dr_scene_last_work"):
+                 "dr_scene_set_profiling", "dr_scene_last_timings", "dr_scene_last_counts", "dr_eval_math",
+                 "dr_scene_edge_data", "dr_scene_last_work",
+                 "dr_set_item_queue_limit"):
         getattr(L, name).restype = C.c_int
     if L.dr_abi_version() != 2:
         raise ImportError("libdr_b200.so has an unexpected ABI version")

@@ -15,6 +15,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstdlib>
+#include <atomic>
 #include <cstring>
 #include <map>
 #include <memory>
@@ -83,11 +84,22 @@ template <typename T> std::vector<T> fetch(const T *src, size_t count, const cha
 // takes them from there, so a loop that builds a new scene every step (as the
 // reference's RenderFunction does) allocates them once.  Only idle queues are
 // cached; `idle` orders their reuse after the last kernels that touched them.
+// What a backward call leaves for the next one on the same queues about its
+// edge stage: edges per shading point, and, when it streamed, the edges of
+// each of kItemBuckets equal ranges of its points.
+constexpr int kItemBuckets = 1024;
+struct EdgeStats {
+    double items_per_point = 0;  // 0: no call yet
+    std::vector<unsigned long long> buckets;  // empty: the last call did not stream
+    long long bucket_points = 0;              // the points the buckets cover
+    DevBuf dev;                               // the reduction's output
+};
+
 struct BackwardQueues {
-    DevBuf pt, items, item_w, item_dp, pt_last, counts, survivors, hits, tasks;
+    DevBuf pt, items, item_w, item_dp, pt_last, pt_items, counts, survivors, hits, tasks;
     long long cap_items = 0;     // grown on overflow, kept with the buffers
     double points_per_sample = 1;  // shading points per pixel sample the last overflow asked for
-    double items_per_point = 0;    // sampled edges per shading point of the last call (0: none yet)
+    EdgeStats stats;
     cudaEvent_t idle = nullptr;
     ~BackwardQueues() {
         if (idle) cudaEventDestroy(idle);
@@ -527,6 +539,11 @@ void check_render_desc(const dr_scene *sc, const dr_render_desc *rd) {
 // the item, its weight, its dp and its slot in the survivor queue of the
 // evaluation wavefront).  Edge stages with more items stream.
 constexpr long long kMaxQueueItems = (8ll << 30) / 64;
+std::atomic<long long> g_item_queue_limit{0};  // dr_set_item_queue_limit (0: kMaxQueueItems)
+long long max_queue_items() {
+    long long l = g_item_queue_limit.load();
+    return l > 0 ? l : kMaxQueueItems;
+}
 
 void check_backward_args(const dr_scene *scene, const dr_render_desc *rd, const float *d_image_dev,
                          const float *grad_dev) {
@@ -559,7 +576,7 @@ std::pair<long long, long long> run_backward(dr_scene *scene, const dr_render_de
                                              float *grad_dev, float *image_dev, BackwardWorkspace &ws,
                                              cudaStream_t st, StageTimer *timer, Grow grow, GrowPoints grow_points,
                                              ProposalState *prop = nullptr, const DevScene *view = nullptr,
-                                             double *items_per_point = nullptr) {
+                                             EdgeStats *stats = nullptr) {
     const DevScene ds = view ? *view : call_scene(scene, rd);
     const GradCacheCfg cfg = grad_cache_cfg(scene->h);
     BackwardCounters c;
@@ -592,12 +609,24 @@ std::pair<long long, long long> run_backward(dr_scene *scene, const dr_render_de
         work[4] += (long long)c.tasks;
         work[5] += (long long)(ds.split_traversal ? c.items_expand : c.items);
     };
+    // edges per bucket of points [0, P) from ws.pt_items
+    auto read_buckets = [&](long long P, std::vector<unsigned long long> &out) {
+        stats->dev.reserve(sizeof(unsigned long long) * kItemBuckets);
+        check_cuda(dr_launch_item_buckets(ws.pt_items, P, kItemBuckets, stats->dev.as<unsigned long long>(), st),
+                   "item buckets");
+        scene->last_launches += 1;
+        out.resize(kItemBuckets);
+        check_cuda(cudaMemcpyAsync(out.data(), stats->dev.p, sizeof(unsigned long long) * kItemBuckets,
+                                   cudaMemcpyDeviceToHost, st),
+                   "bucket read");
+        check_cuda(cudaStreamSynchronize(st), "item buckets");
+    };
     // when the last call's edges per point predict more items than the queue
     // can ever hold, the edge stage streams from the start instead of
     // traversing every point once only to find that out
     const long long samples = (long long)rd->width * rd->height * rd->spp;
-    const bool stream_first = prop == nullptr && items_per_point && *items_per_point > 0 &&
-                              (double)samples * *items_per_point > (double)kMaxQueueItems;
+    const bool stream_first = prop == nullptr && stats && stats->items_per_point > 0 &&
+                              (double)samples * stats->items_per_point > (double)max_queue_items();
     for (int attempt = 0;; attempt++) {
         check_cuda(cudaMemsetAsync(ws.counters, 0, sizeof(BackwardCounters), st), "memset");
         check_cuda(cudaMemsetAsync(grad_dev, 0, sizeof(float) * scene->h.grad_total, st), "memset");
@@ -654,17 +683,57 @@ std::pair<long long, long long> run_backward(dr_scene *scene, const dr_render_de
         if (mst) throw DrError(DR_ERR_DEVICE_STATUS, "proposal network reported status " + std::to_string(mst));
     }
     long long items = 0;
+    bool streamed = false;
     if (!stream_first && !(c.status & DR_STATUS_ITEM_OVERFLOW)) {
         timer->mark(st, "host_queue_check");
         back();
         items = (long long)c.items;
     } else {
-        long long needed = stream_first ? (long long)std::ceil((double)P * *items_per_point) : (long long)c.items;
+        // The chunks of points whose edges fit the queue.  After a full pass
+        // every point's edges are counted and the streams repeat them exactly,
+        // so the plan from them is exact; from the last call's buckets or its
+        // edges per point it is a forecast, and a chunk that overflows is cut.
+        streamed = true;
+        std::vector<unsigned long long> b;
+        double scale = 1, margin = 0.9;
+        long long needed;
+        if (!stream_first) {
+            needed = (long long)c.items;
+            if (ws.pt_items && stats) {
+                read_buckets(P, b);
+                margin = 0.97;
+            }
+        } else if (!stats->buckets.empty() && stats->bucket_points > 0) {
+            b = stats->buckets;
+            scale = (double)P / (double)stats->bucket_points;
+            unsigned long long t = 0;
+            for (unsigned long long x : b) t += x;
+            needed = (long long)std::ceil((double)t * scale);
+        } else {
+            needed = (long long)std::ceil((double)P * stats->items_per_point);
+        }
         long long cap = grow(needed + needed / 8 + 1);
-        long long chunk = cap >= needed ? P : std::max(1ll, (long long)((double)P * cap / needed * 0.9));
+        std::vector<long long> ends;  // chunk ends, ascending
+        if (!b.empty()) {
+            const double budget = margin * (double)cap / scale;
+            double acc = 0;
+            for (int i = 0; i < (int)b.size(); i++) {
+                if (acc > 0 && acc + (double)b[i] > budget) {
+                    ends.push_back((long long)i * P / (long long)b.size());
+                    acc = 0;
+                }
+                acc += (double)b[i];
+            }
+        } else if (needed > cap) {
+            const long long chunk = std::max(1ll, (long long)((double)P * cap / needed * 0.9));
+            for (long long e = chunk; e < P; e += chunk) ends.push_back(e);
+        }
+        ends.push_back(P);
+        size_t ci = 0;
         long long p0 = 0;
         while (p0 < P) {
-            long long p1 = std::min(P, p0 + chunk);
+            while (ends[ci] <= p0) ci++;
+            const long long p1 = ends[ci];
             ws.pt_begin = p0;
             ws.pt_end = p1;
             // reset the item counter and the status word (items, status, pad)
@@ -679,14 +748,13 @@ std::pair<long long, long long> run_backward(dr_scene *scene, const dr_render_de
                 if (p1 - p0 == 1)
                     throw DrError(DR_ERR_OUT_OF_MEMORY, "one shading point samples " + std::to_string(needed) +
                                                             " edges; the item queue holds " + std::to_string(cap));
-                chunk = std::max(1ll, (long long)((double)(p1 - p0) * cap / needed * 0.9));
+                // the chunk cut to what fits; its rest becomes the next chunk
+                ends.insert(ends.begin() + ci,
+                            p0 + std::max(1ll, (long long)((double)(p1 - p0) * cap / needed * 0.9)));
                 continue;
             }
             back();
             items += (long long)c.items;
-            // the next chunk sized from this one's edges per point
-            if (c.items > 0)
-                chunk = std::max(1ll, (long long)((double)(p1 - p0) * cap / (double)c.items * 0.9));
             p0 = p1;
         }
     }
@@ -717,7 +785,13 @@ std::pair<long long, long long> run_backward(dr_scene *scene, const dr_render_de
         pr.steps++;
     }
     check_cuda(cudaStreamSynchronize(st), "backward");
-    if (items_per_point && P > 0) *items_per_point = (double)items / (double)P;
+    if (stats && P > 0) {
+        stats->items_per_point = (double)items / (double)P;
+        // a streamed call leaves its buckets (every point's count is final now)
+        if (streamed && ws.pt_items) read_buckets(P, stats->buckets);
+        else stats->buckets.clear();
+        stats->bucket_points = P;
+    }
     work[0] = P;
     work[1] = items;
     work[6] = (long long)c.visits_walk;
@@ -751,6 +825,13 @@ unsigned char *noalloc_scratch();
 extern "C" {
 
 int dr_abi_version(void) { return DR_ABI_VERSION; }
+
+dr_status dr_set_item_queue_limit(int64_t items) {
+    return guard([&]() {
+        if (items < 0) throw DrError(DR_ERR_INVALID_ARGUMENT, "negative item queue limit");
+        g_item_queue_limit.store((long long)items);
+    });
+}
 
 dr_status dr_scene_create(const dr_scene_desc *desc, int device, dr_scene **out) {
     return guard([&]() {
@@ -850,10 +931,18 @@ namespace {
 // `view` (may be null) replaces the scene's device view (another camera).
 void backward_on_queues(dr_scene *scene, const dr_render_desc *rd, const DevScene *view, const float *d_image_dev,
                         float *grad_dev, float *image_dev, cudaStream_t st) {
-    if (!scene->queues) scene->queues = take_queues(scene->device, st);
+    if (!scene->queues) {
+        scene->queues = take_queues(scene->device, st);
+        // another scene's edge statistics say nothing about this one
+        EdgeStats &es = scene->queues->stats;
+        es.items_per_point = 0;
+        es.buckets.clear();
+        es.bucket_points = 0;
+    }
     BackwardQueues &q = *scene->queues;
     long long cap_points = initial_point_cap(scene, rd, q.points_per_sample);
-    long long cap_items = std::min(kMaxQueueItems, std::max(q.cap_items, std::max<long long>(cap_points * 4, 1 << 16)));
+    long long cap_items =
+        std::min(max_queue_items(), std::max(q.cap_items, std::max<long long>(cap_points * 4, 1 << 16)));
     q.counts.reserve(sizeof(BackwardCounters));
     if (!q.idle) check_cuda(cudaEventCreateWithFlags(&q.idle, cudaEventDisableTiming), "cudaEventCreate");
     // marks the queues busy up to here on every way out, errors included
@@ -882,6 +971,8 @@ void backward_on_queues(dr_scene *scene, const dr_render_desc *rd, const DevScen
         q.pt_last.reserve(DR_PT_LAST_BYTES * cap_points);
         ws.pt = q.pt.as<float>();
         ws.pt_last = q.pt_last.as<unsigned long long>();
+        q.pt_items.reserve(sizeof(int) * cap_points);
+        ws.pt_items = q.pt_items.as<int>();
         ws.cap_points = cap_points;
     };
     bind_points();
@@ -896,7 +987,7 @@ void backward_on_queues(dr_scene *scene, const dr_render_desc *rd, const DevScen
     // the item queue grows to what the traversal reported, up to its limit
     // (the grown queue is kept for later calls)
     auto grow = [&](long long want) {
-        long long target = std::min(want, kMaxQueueItems);
+        long long target = std::min(want, max_queue_items());
         if (target > cap_items) {
             cap_items = target;
             bind_items();
@@ -918,7 +1009,7 @@ void backward_on_queues(dr_scene *scene, const dr_render_desc *rd, const DevScen
         prop = scene->proposal.get();
     }
     auto counts = run_backward(scene, rd, d_image_dev, grad_dev, image_dev, ws, st, &scene->timer, grow, grow_points,
-                               prop, view, &q.items_per_point);
+                               prop, view, &q.stats);
     scene->last_points = counts.first;
     scene->last_items = counts.second;
 }

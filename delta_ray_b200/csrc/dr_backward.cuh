@@ -541,20 +541,31 @@ DEV bool traverse_point(const DevScene &s, const PointRecord &pt, uint64_t seed,
     return traverse_edges<PROP, 0>(s, pt.wi, pt.tri, sp, cone, prng, nrng, em, pr, nd, visits);
 }
 
-// Walks one handed-on subtree of the point (see traverse_point).
-template <bool PROP, class Emit>
-DEV bool traverse_point_task(const DevScene &s, const PointRecord &pt, uint64_t seed, const EdgeTask &task,
-                             Emit &emit, const EdgeProposal &pr, int *visits = nullptr) {
+// Starts the walk of one handed-on subtree of the point (see traverse_point).
+template <bool PROP>
+DEV void start_point_task(EdgeWalk<PROP> &w, const DevScene &s, const PointRecord &pt, uint64_t seed,
+                          const EdgeTask &task, const EdgeProposal &pr) {
     NodeRng nrng;
     nrng.seed = seed;
     nrng.sid = pt.sid;
     nrng.bounce = (uint32_t)pt.bounce;
     SurfacePoint sp = pt.surface();
     ConeSpec cone = light_cone(s, pt.light, sp.p);
-    auto em = [&](int tree, int ei, int key, float w, int code) {
-        if (w != 0.f) emit(tree, ei, key, w, code);
+    start_subtree<PROP>(w, s, pt.wi, pt.tri, sp, cone, nrng, task, pr);
+}
+
+// Walks one handed-on subtree of the point to the end.
+template <bool PROP, class Emit>
+DEV bool traverse_point_task(const DevScene &s, const PointRecord &pt, uint64_t seed, const EdgeTask &task,
+                             Emit &emit, const EdgeProposal &pr, int *visits = nullptr) {
+    EdgeWalk<PROP> w;
+    start_point_task<PROP>(w, s, pt, seed, task, pr);
+    auto em = [&](int ei, int key, float wt, int code) {
+        if (wt != 0.f) emit(w.tree, ei, key, wt, code);
     };
-    return traverse_subtree<PROP>(s, pt.wi, pt.tri, sp, cone, nrng, task, em, pr, visits);
+    NoDefer nd;
+    while (w.busy()) w.step(em, nd, visits);
+    return w.ok;
 }
 
 // One sampled edge (delta_ray.cpp:901-973); returns dp, scatters dv0 / dv1;

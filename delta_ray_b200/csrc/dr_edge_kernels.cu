@@ -6,7 +6,10 @@
 #include "dr_backward.cuh"
 #include "dr_block_grad.cuh"
 
+#include <cooperative_groups.h>
 #include <cuda_bf16.h>
+
+namespace cg = cooperative_groups;
 
 #define DR_ITEM_BUF 24
 // One thread per shading point in [pt_begin, pt_end).  A point's items collect
@@ -87,9 +90,14 @@ __global__ void __launch_bounds__(128, 6) k_edge_traverse(DevScene s, uint64_t s
         if (p < n) {
             PointRecord pt;
             pt.load(ws.pt + (size_t)p * DR_PT_WORDS);
-            auto emit = [&](int tree, int ei, int j, float w, int code) { out.add((int)p, tree, ei, j, w, code); };
+            int cnt = 0;
+            auto emit = [&](int tree, int ei, int j, float w, int code) {
+                out.add((int)p, tree, ei, j, w, code);
+                cnt++;
+            };
             if (!traverse_point<PROP>(s, pt, seed, emit, point_proposal(ws, p), (NoDefer *)nullptr, &visits))
                 set_status(&ws.counters->status, DR_STATUS_STACK_OVERFLOW);
+            if (ws.pt_items) ws.pt_items[p] = cnt;
         }
         out.flush_warp();
     }
@@ -116,7 +124,11 @@ __global__ void __launch_bounds__(128, 4) k_edge_expand(DevScene s, uint64_t see
             PointRecord pt;
             pt.load(ws.pt + (size_t)p * DR_PT_WORDS);
             const EdgeProposal pr = point_proposal(ws, p);
-            auto emit = [&](int tree, int ei, int j, float w, int code) { out.add((int)p, tree, ei, j, w, code); };
+            int cnt = 0;
+            auto emit = [&](int tree, int ei, int j, float w, int code) {
+                out.add((int)p, tree, ei, j, w, code);
+                cnt++;
+            };
             EdgeTask tb[DR_TASK_BUF];
             int nt = 0;
             bool ok = true;
@@ -139,33 +151,56 @@ __global__ void __launch_bounds__(128, 4) k_edge_expand(DevScene s, uint64_t see
             ok &= traverse_point<PROP, DR_TASK_CUT>(s, pt, seed, emit, pr, &defer, &visits);
             if (nt > 0) flush();
             if (!ok) set_status(&ws.counters->status, DR_STATUS_STACK_OVERFLOW);
+            if (ws.pt_items) ws.pt_items[p] = cnt;  // the subtrees add theirs
         }
         out.flush_warp();
     }
     add_visits(&ws.counters->visits_walk, visits);
 }
 
-// Large trees, second stage: one thread per handed-on subtree.
+// Large trees, second stage: the handed-on subtrees, fetched one per lane.
+// Subtree sizes vary by orders of magnitude, so a lane that finishes its walk
+// takes the next task (lanes that need one share an atomic) while the other
+// lanes of its warp keep stepping theirs: every step of the loop walks one
+// node per busy lane.  A full item buffer reserves its slots with one atomic
+// of its own; the partial buffers go out together at the end.
+__device__ __forceinline__ long long next_task(unsigned long long *counter) {
+    cg::coalesced_group g = cg::coalesced_threads();
+    unsigned long long first = 0;
+    if (g.thread_rank() == 0) first = atomicAdd(counter, (unsigned long long)g.size());
+    return (long long)(g.shfl(first, 0) + g.thread_rank());
+}
+
 template <bool PROP>
 __global__ void __launch_bounds__(128, 6) k_edge_tasks(DevScene s, uint64_t seed, BackwardWorkspace ws) {
-    long long n = (long long)min(ws.counters->tasks, (unsigned long long)ws.cap_tasks);
-    long long stride = (long long)gridDim.x * blockDim.x;
+    const long long n = (long long)min(ws.counters->tasks, (unsigned long long)ws.cap_tasks);
     ItemWriter out(ws);
-    int visits = 0;
-    for (long long base = (long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < n; base += stride) {
-        long long k = base + (threadIdx.x & 31);
-        if (k < n) {
-            EdgeTask t = ws.tasks[k];
+    int visits = 0, point = 0, cnt = 0;
+    bool ok = true;
+    EdgeWalk<PROP> w;
+    auto emit = [&](int ei, int key, float wt, int code) {
+        if (wt != 0.f) {
+            out.add(point, w.tree, ei, key, wt, code);
+            cnt++;
+        }
+    };
+    NoDefer nd;
+    while (true) {
+        if (!w.busy()) {
+            if (cnt > 0 && ws.pt_items) atomicAdd(ws.pt_items + point, cnt);
+            cnt = 0;
+            const long long k = next_task(&ws.counters->task_next);
+            if (k >= n) break;
+            const EdgeTask t = ws.tasks[k];
             PointRecord pt;
             pt.load(ws.pt + (size_t)t.point * DR_PT_WORDS);
-            auto emit = [&](int tree, int ei, int j, float w, int code) { out.add(t.point, tree, ei, j, w, code); };
-            if (!traverse_point_task<PROP>(s, pt, seed, t, emit, point_proposal(ws, t.point), &visits))
-                set_status(&ws.counters->status, DR_STATUS_STACK_OVERFLOW);
+            point = t.point;
+            start_point_task<PROP>(w, s, pt, seed, t, point_proposal(ws, t.point));
         }
-        // keeps lanes' buffers from carrying over long; flush_warp is a warp
-        // collective, so the whole warp decides (the loop is warp-uniform)
-        if (__any_sync(0xffffffffu, out.nb == DR_ITEM_BUF)) out.flush_warp();
+        w.step(emit, nd, &visits);
+        ok &= w.ok;
     }
+    if (!ok) set_status(&ws.counters->status, DR_STATUS_STACK_OVERFLOW);
     out.flush_warp();
     add_visits(&ws.counters->visits_tasks, visits);
 }
@@ -348,6 +383,31 @@ __global__ void __launch_bounds__(128, 8) k_primary_grad(DevScene s, int W, int 
     block_grad_flush(bg);
 }
 
+// Edges sampled per bucket of points: bucket b sums pt_items over points
+// [b P / nb, (b + 1) P / nb).
+__global__ void k_item_buckets(const int *pt_items, long long P, int nb, unsigned long long *out) {
+    const int b = blockIdx.x;
+    const long long p0 = (long long)b * P / nb, p1 = (long long)(b + 1) * P / nb;
+    unsigned long long sum = 0;
+    for (long long p = p0 + threadIdx.x; p < p1; p += blockDim.x) sum += (unsigned long long)(unsigned)pt_items[p];
+    for (int o = 16; o > 0; o >>= 1) sum += __shfl_xor_sync(0xffffffffu, sum, o);
+    __shared__ unsigned long long part[8];
+    if ((threadIdx.x & 31) == 0) part[threadIdx.x >> 5] = sum;
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        unsigned long long t = 0;
+        for (int i = 0; i < (int)(blockDim.x >> 5); i++) t += part[i];
+        out[b] = t;
+    }
+}
+
+cudaError_t dr_launch_item_buckets(const int *pt_items, long long P, int nb, unsigned long long *out,
+                                   cudaStream_t st) {
+    if (nb <= 0) return cudaSuccess;
+    k_item_buckets<<<nb, 256, 0, st>>>(pt_items, P, nb, out);
+    return cudaGetLastError();
+}
+
 cudaError_t dr_launch_edge_traverse(const DevScene &s, uint64_t seed, const BackwardWorkspace &ws, int num_sms,
                                     cudaStream_t st, int *launches, StageTimer *timer) {
     const bool prop = ws.proposal_q != nullptr;
@@ -360,6 +420,8 @@ cudaError_t dr_launch_edge_traverse(const DevScene &s, uint64_t seed, const Back
         // the item count of the first stage (the roofline's work counts)
         e = cudaMemcpyAsync(&ws.counters->items_expand, &ws.counters->items, sizeof(unsigned long long),
                             cudaMemcpyDeviceToDevice, st);
+        if (e != cudaSuccess) return e;
+        e = cudaMemsetAsync(&ws.counters->task_next, 0, sizeof(unsigned long long), st);
         if (e != cudaSuccess) return e;
         if (prop) k_edge_tasks<true><<<stage_grid(num_sms), 128, 0, st>>>(s, seed, ws);
         else k_edge_tasks<false><<<stage_grid(num_sms), 128, 0, st>>>(s, seed, ws);

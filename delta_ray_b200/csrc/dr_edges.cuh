@@ -149,10 +149,6 @@ DEV float min_sq_bound(float lo, float hi) {
 }
 DEV float max_sq_bound(float lo, float hi) { return fmaxf(lo * lo, hi * hi); }
 
-DEV float3 node_corner(const DevEdgeNode &n, int i) {
-    return f3((i & 1) ? n.hi[0] : n.lo[0], (i & 2) ? n.hi[1] : n.lo[1], (i & 4) ? n.hi[2] : n.lo[2]);
-}
-
 // What the BSDF bound of an edge-tree node needs of the shading point: its
 // position and normal, the frame around the incoming direction wi (rows
 // t, b = normalize(n x wi), n = wi) and the normal in it, the lobes'
@@ -185,10 +181,31 @@ DEV BoundCtx bound_ctx(float3 wi, const SurfacePoint &sp, float dl, float sl, fl
     return c;
 }
 
+// The corners' products with a direction, per axis: corner i has the hi
+// coordinate on axis a iff bit a of i is set, and dot(d, corner_i - p) is
+// (x[i & 1] + y[(i >> 1) & 1]) + z[i >> 2], the bits of the per-corner dot.
+struct CornerDots {
+    float x[2], y[2], z[2];
+    DEV float at(int i) const { return (x[i & 1] + y[(i >> 1) & 1]) + z[i >> 2]; }
+};
+DEV CornerDots corner_dots(float3 d, const float *q) {  // q: lo - p, hi - p per axis (x0 x1 y0 y1 z0 z1)
+    CornerDots c;
+    c.x[0] = d.x * q[0];
+    c.x[1] = d.x * q[1];
+    c.y[0] = d.y * q[2];
+    c.y[1] = d.y * q[3];
+    c.z[0] = d.z * q[4];
+    c.z[1] = d.z * q[5];
+    return c;
+}
+
 DEV_NOINLINE float bsdf_bound(const DevEdgeNode &node, const BoundCtx &c) {
+    const float q[6] = {node.lo[0] - c.p.x, node.hi[0] - c.p.x, node.lo[1] - c.p.y,
+                        node.hi[1] - c.p.y, node.lo[2] - c.p.z, node.hi[2] - c.p.z};
+    const CornerDots cn = corner_dots(c.n, q);
     float cos_max = 0.f;
     for (int i = 0; i < 8; i++)
-        if (dot(c.n, node_corner(node, i) - c.p) > 0.f) {
+        if (cn.at(i) > 0.f) {
             cos_max = 1.f;
             break;
         }
@@ -196,11 +213,12 @@ DEV_NOINLINE float bsdf_bound(const DevEdgeNode &node, const BoundCtx &c) {
     float maxp = 0.f;
     if (c.sl > 0.f) {
         const Frame &hf = c.hf;
+        const CornerDots ct = corner_dots(hf.t, q), cb = corner_dots(hf.b, q), cz = corner_dots(hf.n, q);
         float3 lo = f3(DR_INF), hi = f3(-DR_INF);
         for (int i = 0; i < 8; i++) {
-            float3 q = to_local(hf, node_corner(node, i) - c.p);
-            lo = f3(fminf(lo.x, q.x), fminf(lo.y, q.y), fminf(lo.z, q.z));
-            hi = f3(fmaxf(hi.x, q.x), fmaxf(hi.y, q.y), fmaxf(hi.z, q.z));
+            float3 v = f3(ct.at(i), cb.at(i), cz.at(i));  // to_local(hf, corner_i - p)
+            lo = f3(fminf(lo.x, v.x), fminf(lo.y, v.y), fminf(lo.z, v.z));
+            hi = f3(fmaxf(hi.x, v.x), fmaxf(hi.y, v.y), fmaxf(hi.z, v.z));
         }
         float cphi = 0.f;
         float hx = hi.x;
@@ -230,8 +248,30 @@ DEV_NOINLINE float bsdf_bound(const DevEdgeNode &node, const BoundCtx &c) {
     return cos_max * (c.dl / DR_PI + c.sl * maxp);
 }
 
+// Fast sine, cosine and reciprocal square root of the silhouette filter
+// (absolute errors below 1e-6 on its arguments).
+#ifdef DR_HOST_BUILD
+HD float filt_sin(float x) { return std::sin(x); }
+HD float filt_cos(float x) { return std::cos(x); }
+HD float filt_rsqrt(float x) { return 1.f / std::sqrt(x); }
+#else
+DEV float filt_sin(float x) { return __sinf(x); }
+DEV float filt_cos(float x) { return __cosf(x); }
+DEV float filt_rsqrt(float x) { return rsqrtf(x); }
+#endif
+
+// Whether the node's cone of normals, widened by the angle its bounding
+// sphere subtends from p, reaches the directions perpendicular to p - centre:
+// |pi/2 - acos(c)| <= angle + atan(vt) with c = cos(axis, centre - p).  The
+// float evaluation below (reproducible atan and acos, within 3 ulp) is within
+// 1.5e-6 rad of the exact comparison.  A filter decides first where the two
+// sides differ by more than 1e-5 in sine space (so by more in angle, since
+// |d asin| >= |d x|): for angle + atan(vt) < pi/2 the test is |c| <=
+// sin(angle + atan(vt)) = (sin a + vt cos a) / sqrt(1 + vt^2), whose terms it
+// takes from the fast functions; it takes the same answer as the float
+// evaluation and leaves the rest to it, and also every |c| > 1 (rounding
+// can give that; acos is NaN there and the float evaluation answers false).
 DEV_NOINLINE bool contains_silhouette(const DevEdgeNode &node, float3 p) {
-    float3 c = f3(0.5f * (node.lo[0] + node.hi[0]), 0.5f * (node.lo[1] + node.hi[1]), 0.5f * (node.lo[2] + node.hi[2]));
     // bounding sphere as aabb.h:266-270: center (lo + hi) / 2, radius |hi - center|
     float3 cs = f3((node.lo[0] + node.hi[0]) / 2.f, (node.lo[1] + node.hi[1]) / 2.f, (node.lo[2] + node.hi[2]) / 2.f);
     float r = length(f3(node.hi[0], node.hi[1], node.hi[2]) - cs);
@@ -239,11 +279,37 @@ DEV_NOINLINE bool contains_silhouette(const DevEdgeNode &node, float3 p) {
     float l = length(d);
     float vt = r / l;
     if (vt >= 1.f) return true;
-    float va = dr_atanf(vt);
     d = d / l;
+    const float c = dot(-d, f3(node.axis[0], node.axis[1], node.axis[2]));
+    const float a = node.angle, ac = fabsf(c);
+    if (a >= 0.f && a <= 1.5f && ac <= 1.f) {  // NaNs fall through to the float evaluation
+        const float k = filt_rsqrt(1.f + vt * vt), sa = filt_sin(a), ca = filt_cos(a);
+        const float cos_r = (ca - vt * sa) * k, sin_r = (sa + vt * ca) * k;
+        const float margin = 1e-5f;
+        if (cos_r < -margin) return true;  // angle + atan(vt) > pi/2
+        if (cos_r > margin) {
+            if (ac < sin_r - margin) return true;
+            if (ac > sin_r + margin) return false;
+        }
+    }
+    float va = dr_atanf(vt);
+    float ang = dr_acosf(c);
+    float range = node.angle + va;
+    return ang - range <= float(3.14159265358979323846 / 2.f) && ang + range >= float(3.14159265358979323846 / 2.f);
+}
+
+// The float evaluation alone (checks of the filter).
+HD bool contains_silhouette_exact(const DevEdgeNode &node, float3 p) {
+    float3 cs = f3((node.lo[0] + node.hi[0]) / 2.f, (node.lo[1] + node.hi[1]) / 2.f, (node.lo[2] + node.hi[2]) / 2.f);
+    float r = length(f3(node.hi[0], node.hi[1], node.hi[2]) - cs);
+    float3 d = cs - p;
+    float l = length(d);
+    float vt = r / l;
+    if (vt >= 1.f) return true;
+    d = d / l;
+    float va = dr_atanf(vt);
     float ang = dr_acosf(dot(-d, f3(node.axis[0], node.axis[1], node.axis[2])));
     float range = node.angle + va;
-    (void)c;
     return ang - range <= float(3.14159265358979323846 / 2.f) && ang + range >= float(3.14159265358979323846 / 2.f);
 }
 
@@ -311,62 +377,119 @@ template <bool PROP> HD EdgeItem<PROP> edge_item(int node, float bb, float c, fl
 
 #define DR_NODE_MASK ((1 << 27) - 1)
 
+// The walk of one tree in one mode as a resumable state: start() pushes the
+// root or a handed-on subtree, step() takes one node off the stack.  A kernel
+// can interleave walks (a lane that finishes one starts the next while the
+// other lanes of its warp keep stepping); the draws are keyed by node and the
+// items carry their order key, so the sampled edges do not depend on it.
 // CUT > 0: interior nodes at depth CUT below the start are handed to
 // defer(node, bb, cpmf, apmf, lpmf) instead of being walked (inside the walk
 // an item's node field carries its depth in bits 27..31).
-template <bool PROP, int CUT = 0, class Emit, class Defer>
-DEV bool traverse_mode(const bool CONE, const DevScene &s, const DevEdgeNode *nodes, const DevEdge *edges,
-                       bool dir_bounds, float3 wi,
-                       const SurfacePoint &sp, float dl, float sl, float rough, int model, const ConeSpec &cone,
-                       const EdgeTask &start, const NodeRng &rng, Emit &emit, const EdgeProposal &pr, int tree,
-                       bool learned, Defer &defer, int *visits = nullptr) {
+template <bool PROP, int CUT = 0>
+struct EdgeWalk {
     using Item = EdgeItem<PROP>;
-    const BoundCtx bc = bound_ctx(wi, sp, dl, sl, rough, model);
+    const DevScene *s;
+    const DevEdgeNode *nodes;
+    const DevEdge *edges;
+    BoundCtx bc;
+    Frame f;  // shading frame (the proposal's direction bins)
+    ConeSpec cone;
+    NodeRng rng;
+    EdgeProposal pr;
+    int tree;
+    bool cone_mode, dir_bounds, learned, ok;
+    int n = 0;
     Item st[DR_EDGE_STACK];
-    int sp_ = 0;
-    st[sp_++] = edge_item<PROP>(start.code & DR_NODE_MASK, start.bb, start.cpmf, start.apmf, start.lpmf);
-    bool ok = true;
-    while (sp_ > 0) {
-        Item it = st[--sp_];
-        if (it.bb <= 0.f) continue;
-        const int nid = it.node & DR_NODE_MASK;
-        const DevEdgeNode &node = nodes[nid];
-        if (visits) ++*visits;
-        if (node.nprims > 0) {
-            float apmf = it.apmf;
-            if constexpr (PROP) apmf = pr.alpha * it.lpmf + (1.f - pr.alpha) * it.apmf;
-            float denom = it.cpmf * it.cpmf + apmf * apmf;
-            float w = CONE ? it.cpmf / denom : apmf / denom;
-            for (int i = 0; i < node.nprims; i++) {
-                int ei = node.offset + i;
-                if (!is_silhouette(s, sp.p, edges[ei])) continue;
-                int code = 0;
-                if constexpr (PROP)
-                    if (pr.codes) code = dir_bin(sp.f, 0.5f * (edge_v0(s, edges[ei]) + edge_v1(s, edges[ei])) - sp.p);
-                emit(ei, (CONE ? 0 : 1) << 27 | ei, w, code);
-            }
-            continue;
+
+    DEV void start(bool CONE, const DevScene &sc, const DevEdgeNode *nd, const DevEdge *ed, int tr, bool dirb,
+                   float3 wi, const SurfacePoint &sp, float dl, float sl, float rough, int model, const ConeSpec &cn,
+                   const EdgeTask &t, const NodeRng &r, const EdgeProposal &p, bool lrn) {
+        s = &sc;
+        nodes = nd;
+        edges = ed;
+        tree = tr;
+        dir_bounds = dirb;
+        cone_mode = CONE;
+        learned = lrn;
+        bc = bound_ctx(wi, sp, dl, sl, rough, model);
+        f = sp.f;
+        cone = cn;
+        rng = r;
+        pr = p;
+        ok = true;
+        n = 0;
+        st[n++] = edge_item<PROP>(t.code & DR_NODE_MASK, t.bb, t.cpmf, t.apmf, t.lpmf);
+    }
+    DEV bool busy() const { return n > 0; }
+
+    template <class Emit> DEV void leaf(const Item &it, const DevEdgeNode &node, Emit &emit) {
+        const bool CONE = cone_mode;
+        const float3 p = bc.p;
+        float apmf = it.apmf;
+        if constexpr (PROP) apmf = pr.alpha * it.lpmf + (1.f - pr.alpha) * it.apmf;
+        float denom = it.cpmf * it.cpmf + apmf * apmf;
+        float w = CONE ? it.cpmf / denom : apmf / denom;
+        for (int i = 0; i < node.nprims; i++) {
+            int ei = node.offset + i;
+            if (!is_silhouette(*s, p, edges[ei])) continue;
+            int code = 0;
+            if constexpr (PROP)
+                if (pr.codes) code = dir_bin(f, 0.5f * (edge_v0(*s, edges[ei]) + edge_v1(*s, edges[ei])) - p);
+            emit(ei, (CONE ? 0 : 1) << 27 | ei, w, code);
         }
+    }
+
+    // One step: the leaves on top of the stack (up to two), then one interior
+    // node.  A lane whose next node is a leaf goes on to an interior node in
+    // the same step, so the interior evaluation, the costly part, runs with
+    // the lanes of the warp together rather than alternating with the leaves.
+    // emit(tree_edge_index, key, weight, slot_code) for every silhouette edge
+    // of a reached leaf.
+    template <class Emit, class Defer> DEV void step(Emit &emit, Defer &defer, int *visits) {
+        const bool CONE = cone_mode;
+        const float3 p = bc.p;
+        Item it;
+        int nid = 0;
+        bool interior = false;
+#pragma unroll 1
+        for (int k = 0; k < 3 && n > 0; k++) {
+            it = st[--n];
+            if (it.bb <= 0.f) continue;
+            nid = it.node & DR_NODE_MASK;
+            if (visits) ++*visits;
+            if (nodes[nid].nprims == 0) {
+                interior = true;
+                break;
+            }
+            if (k == 2) {  // a third leaf waits for the next step
+                n++;
+                if (visits) --*visits;
+                break;
+            }
+            leaf(it, nodes[nid], emit);
+        }
+        if (!interior) return;
+        const DevEdgeNode &node = nodes[nid];
         if (CUT > 0 && (it.node >> 27) == CUT) {  // hand the subtree on
             float lp = 0.f;
             if constexpr (PROP) lp = it.lpmf;
             defer(nid, it.bb, it.cpmf, it.apmf, lp);
-            continue;
+            return;
         }
         const int cdepth = CUT > 0 ? ((it.node >> 27) + 1) << 27 : 0;  // the children's depth bits
         int li = nid + 1, ri = node.offset;
         const DevEdgeNode &L = nodes[li], &R = nodes[ri];
-        bool all_split = it.bb > 1.f || node_inside(node, sp.p);
+        bool all_split = it.bb > 1.f || node_inside(node, p);
         bool lcs = true, rcs = true;
         if (dir_bounds) {
-            lcs = contains_silhouette(L, sp.p);
-            rcs = contains_silhouette(R, sp.p);
+            lcs = contains_silhouette(L, p);
+            rcs = contains_silhouette(R, p);
         }
         float lbb = lcs ? bsdf_bound(L, bc) : 0.f;
         float rbb = rcs ? bsdf_bound(R, bc) : 0.f;
-        float il = lcs ? node_importance(L, lbb, sp.p) : 0.f;
-        float ir = rcs ? node_importance(R, rbb, sp.p) : 0.f;
-        if (il + ir <= 1e-10f) continue;
+        float il = lcs ? node_importance(L, lbb, p) : 0.f;
+        float ir = rcs ? node_importance(R, rbb, p) : 0.f;
+        if (il + ir <= 1e-10f) return;
         // a node the cone walk cannot reach (cpmf 0) gives its children cpmf
         // 0 whatever the cone tests say, as long as the importances are
         // finite: the all walk skips the tests there
@@ -374,7 +497,7 @@ DEV bool traverse_mode(const bool CONE, const DevScene &s, const DevEdgeNode *no
         bool lhc = cone_tests && box_cone(L.lo, L.hi, cone), rhc = cone_tests && box_cone(R.lo, R.hi, cone);
         bool cone_split = all_split || (lhc && rhc && lcs && rcs && cone.cos_angle > 0.95f);
         float ilc = lhc ? il : 0.f, irc = rhc ? ir : 0.f;
-        if (CONE && ilc + irc <= 1e-10f) continue;
+        if (CONE && ilc + irc <= 1e-10f) return;
         float plc = 0.f, prc = 0.f, pla = 0.f, pra = 0.f;
         if (cone_split) {
             plc = prc = 1.f;
@@ -395,7 +518,7 @@ DEV bool traverse_mode(const bool CONE, const DevScene &s, const DevEdgeNode *no
         if constexpr (PROP) {
             float prl = pra;
             if (!all_split && il > 0.f && ir > 0.f) {
-                float gl = il * node_dir_weight(pr.q, sp.f, sp.p, L), gr = ir * node_dir_weight(pr.q, sp.f, sp.p, R);
+                float gl = il * node_dir_weight(pr.q, f, p, L), gr = ir * node_dir_weight(pr.q, f, p, R);
                 if (gl + gr > 0.f) {
                     pll = gl / (gl + gr);
                     prl = 1.f - pll;
@@ -409,24 +532,38 @@ DEV bool traverse_mode(const bool CONE, const DevScene &s, const DevEdgeNode *no
         }
         bool split = CONE ? cone_split : all_split;
         if (split) {
-            if (sp_ + 2 > DR_EDGE_STACK) {
+            if (n + 2 > DR_EDGE_STACK) {
                 ok = false;
-                continue;
+                return;
             }
             // depth first, left subtree before right
-            if (rcs) st[sp_++] = right;
-            if (lcs) st[sp_++] = left;
+            if (rcs) st[n++] = right;
+            if (lcs) st[n++] = left;
         } else {
             float u = rng.draw(CONE ? 0 : 1, nid);
             bool go_left = CONE ? u < plc : u < (learned ? pll : pla);
-            if (sp_ + 1 > DR_EDGE_STACK) {
+            if (n + 1 > DR_EDGE_STACK) {
                 ok = false;
-                continue;
+                return;
             }
-            st[sp_++] = go_left ? left : right;
+            st[n++] = go_left ? left : right;
         }
     }
-    return ok;
+};
+
+// Stochastic traversal of one edge tree in one mode (edge_tree.cpp:511-652),
+// start to finish: CONE true for the cone mode, false for the all mode.
+// Returns false if the stack limit was hit (never for trees of depth <
+// DR_EDGE_STACK).
+template <bool PROP, int CUT = 0, class Emit, class Defer>
+DEV bool traverse_mode(const bool CONE, const DevScene &s, const DevEdgeNode *nodes, const DevEdge *edges, int tree,
+                       bool dir_bounds, float3 wi, const SurfacePoint &sp, float dl, float sl, float rough, int model,
+                       const ConeSpec &cone, const EdgeTask &start, const NodeRng &rng, Emit &emit,
+                       const EdgeProposal &pr, bool learned, Defer &defer, int *visits = nullptr) {
+    EdgeWalk<PROP, CUT> w;
+    w.start(CONE, s, nodes, edges, tree, dir_bounds, wi, sp, dl, sl, rough, model, cone, start, rng, pr, learned);
+    while (w.busy()) w.step(emit, defer, visits);
+    return w.ok;
 }
 
 // All edges sampled for one shading point (edge_tree.cpp:654-725).
@@ -484,31 +621,28 @@ DEV bool traverse_edges(const DevScene &s, float3 wi, int stri, const SurfacePoi
         auto dc = [&](int node, float bb, float c, float a, float l) {
             defer(node | (tree << 29) | (mode << 30), bb, c, a, l);
         };
-        ok &= traverse_mode<PROP, CUT>(mode == 0, s, nodes, edges, tree == 1, wi, sp, dl, sl, rough, m.model, cone,
-                                       root, nrng, em, pr, tree, learned, dc, visits);
+        ok &= traverse_mode<PROP, CUT>(mode == 0, s, nodes, edges, tree, tree == 1, wi, sp, dl, sl, rough, m.model,
+                                       cone, root, nrng, em, pr, learned, dc, visits);
     }
     return ok;
 }
 
-// Walks one handed-on subtree of a point's traversal (the point's setup is
-// recomputed: tree and mode come with the task).
-template <bool PROP, class Emit>
-DEV bool traverse_subtree(const DevScene &s, float3 wi, int stri, const SurfacePoint &sp, const ConeSpec &cone,
-                          const NodeRng &nrng, const EdgeTask &task, Emit &emit, const EdgeProposal &pr,
-                          int *visits = nullptr) {
+// Starts the walk of one handed-on subtree of a point's traversal (the
+// point's setup is recomputed: tree and mode come with the task).
+template <bool PROP>
+DEV void start_subtree(EdgeWalk<PROP> &w, const DevScene &s, float3 wi, int stri, const SurfacePoint &sp,
+                       const ConeSpec &cone, const NodeRng &nrng, const EdgeTask &task, const EdgeProposal &pr) {
     const int tree = (task.code >> 29) & 1, mode = (task.code >> 30) & 1;
     const DevEdgeNode *nodes = tree ? s.nrm_nodes : s.sil_nodes;
     const DevEdge *edges = tree ? s.nrm_edges : s.sil_edges;
     const DevMaterial &m = s.mats[material_of_tri(s, stri)];
     float dl = luminance(get_kd(s, m, sp.uv)), sl = luminance(get_ks(s, m, sp.uv));
     float rough = get_rough(s, m, sp.uv);
-    auto em = [&](int ei, int key, float w, int code) { emit(tree, ei, key, w, code); };
-    NoDefer nd;
     EdgeTask start = task;
     start.code = task.code & DR_NODE_MASK;  // depth bits cleared: walked to the leaves
     bool learned = PROP && mode == 1 ? nrng.draw(1, DR_NODE_MIX_DRAW) < pr.alpha : false;
-    return traverse_mode<PROP>(mode == 0, s, nodes, edges, tree == 1, wi, sp, dl, sl, rough, m.model, cone, start,
-                               nrng, em, pr, tree, learned, nd, visits);
+    w.start(mode == 0, s, nodes, edges, tree, tree == 1, wi, sp, dl, sl, rough, m.model, cone, start, nrng, pr,
+            learned);
 }
 
 // LTC matrix lookup (material.h:464-476): nearest entry of the 128x128 table

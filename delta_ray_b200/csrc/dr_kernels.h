@@ -91,6 +91,7 @@ struct BackwardCounters {
     // the point walks (k_edge_traverse / k_edge_expand) and by k_edge_tasks,
     // and the item count when k_edge_expand finished
     unsigned long long visits_walk, visits_tasks, items_expand;
+    unsigned long long task_next;  // next task of k_edge_tasks (lanes fetch them one by one)
 };
 
 struct BackwardWorkspace {
@@ -123,6 +124,10 @@ struct BackwardWorkspace {
     // (null: one thread walks each point whole)
     EdgeTask *tasks;
     long long cap_tasks;
+    // [cap_points] edges each point's traversal sampled, written by the point
+    // walk and added to by its subtrees (null: not kept); the streamed edge
+    // stage plans its chunks from them
+    int *pt_items;
     const uint16_t *proposal_q;
     float proposal_alpha;
     float *train_targets;
@@ -152,6 +157,9 @@ cudaError_t dr_launch_proposal_features(const DevScene &s, const BackwardWorkspa
                                         float3 ih, void *x, void *xt, cudaStream_t st);
 cudaError_t dr_launch_edge_traverse(const DevScene &s, uint64_t seed, const BackwardWorkspace &ws, int num_sms,
                                     cudaStream_t st, int *launches, StageTimer *timer);
+// out[b] = edges sampled by points [b P / nb, (b + 1) P / nb) (ws.pt_items)
+cudaError_t dr_launch_item_buckets(const int *pt_items, long long P, int nb, unsigned long long *out,
+                                   cudaStream_t st);
 // dst[0..n) += src[0..n)
 cudaError_t dr_launch_accumulate(float *dst, const float *src, long long n, cudaStream_t st);
 // Launchers of the edge half (dr_edge_kernels.cu).  Edge evaluation is a

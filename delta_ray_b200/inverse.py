@@ -48,6 +48,7 @@ class FitConfig:
     height_noise: float = 0.05    # initial perturbation of the heights (std)
     roughness_noise: float = 0.1  # initial perturbation of the roughness (std)
     rmse_goal: float = 0.01
+    common_seeds: bool = False    # common random numbers: targets at `spp` with each view's seed, reused every step
     learned: bool = False         # train and use the learned edge proposal
     proposal_mix: float = 0.8
     seed: int = 0
@@ -120,16 +121,23 @@ class HeightfieldFit:
     def _dicts(self, cam, mats, shapes):
         return _abi.scene_dicts(cam, mats, shapes, self.wl.lights)
 
+    def view_seed(self, k):
+        """Seed of view k at the current step (the same at every step with
+        common_seeds, and then also the target's)."""
+        return 777 + k if self.cfg.common_seeds else 100_000 * (k + 1) + self.step
+
     def render_targets(self):
-        """Target images of every view at target_spp (forward only)."""
+        """Target images of every view (forward only): target_spp samples, or
+        with common_seeds the fit's spp on the fit's own sample streams."""
         mats, shapes = self._scene_lists(self.true_heights, self.true_rough)
         self.targets = []
         W, H = self.cfg.resolution
+        spp = self.cfg.spp if self.cfg.common_seeds else self.cfg.target_spp
         for k, cam in enumerate(self.cams):
             c, m, s, l = self._dicts(cam, mats, shapes)
             sc = Scene(c, m, s, l, self.cfg.device)
             try:
-                self.targets.append(sc.forward(W, H, self.cfg.target_spp, self.cfg.max_bounces, 777 + k).clone())
+                self.targets.append(sc.forward(W, H, spp, self.cfg.max_bounces, 777 + k).clone())
             finally:
                 sc.close()
         return self.targets
@@ -163,7 +171,7 @@ class HeightfieldFit:
         g_r = torch.zeros(self.n_patch)
         loss = 0.0
         for k, sc in enumerate(self.scenes):
-            seed = 100_000 * (k + 1) + self.step
+            seed = self.view_seed(k)
             img = sc.forward(W, H, cfg.spp, cfg.max_bounces, seed)
             diff = img - self.targets[k]
             loss += float(diff.pow(2).mean())

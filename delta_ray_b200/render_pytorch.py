@@ -22,6 +22,13 @@ import torch
 from . import _abi, _lib
 
 
+def set_item_queue_limit(items=0):
+    """Upper bound on the edge items a backward call holds on the device at
+    once (dr_set_item_queue_limit; 0: the default, 8 GiB worth).  Calls whose
+    points sample more edges run their edge stage in chunks of points."""
+    _lib.check(_lib.lib().dr_set_item_queue_limit(int(items)))
+
+
 class RenderOptions:
     """Optional trailing argument of RenderFunction.apply.
 

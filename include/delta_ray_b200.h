@@ -266,6 +266,16 @@ DR_API dr_status dr_render_backward_views(dr_scene *scene, int n_views, const dr
 DR_API dr_status dr_render_backward_noalloc(dr_scene *scene, const dr_render_desc *rd, const float *d_image_dev,
                                             float *grad_dev, float *image_dev, void *stream);
 
+/* Upper bound on the edge items a dr_render_backward call holds on the
+ * device at once (64 bytes each); 0 restores the default, 8 GiB worth
+ * (134,217,728 items).  A call whose shading points sample more edges runs its
+ * edge stage in chunks of points whose edges fit, planned from the edge
+ * counts of a full pass or of the previous call on the same scene; the
+ * results do not depend on the bound.  Process-wide; a negative bound fails
+ * with DR_ERR_INVALID_ARGUMENT.  No counterpart in the reference, whose CPU
+ * renderer evaluates each edge as it samples it. */
+DR_API dr_status dr_set_item_queue_limit(int64_t items);
+
 /* Closest hits of n rays [n][6] (origin, direction; device memory) on
  * (1e-3, inf): global triangle id (-1 on a miss; ids run over shapes in
  * order, then triangles) and distance.  Replaces the reference's

@@ -44,6 +44,7 @@ def load():
         L.hh_math.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_longlong]
         L.hh_scene_edges.argtypes = [C.POINTER(_abi.dr_scene_desc), C.c_int, C.c_void_p, C.c_longlong]
         L.hh_scene_edges.restype = C.c_longlong
+        L.hh_silhouette.argtypes = [C.c_void_p] * 5 + [C.c_longlong, C.c_void_p]
         L.hh_trace_pairs.argtypes = [C.POINTER(_abi.dr_scene_desc), C.c_void_p, C.c_int, C.c_void_p]
         _lib = L
     return _lib
@@ -128,3 +129,13 @@ def trace_pairs(wl, rays):
     out = np.zeros((rays.shape[0], 4), np.int32)
     L.hh_trace_pairs(C.byref(sd.desc), rays.ctypes.data, rays.shape[0], out.ctypes.data)
     return out
+
+
+def silhouette(lo, hi, axis, angle, p):
+    """contains_silhouette per (node, point): (filtered, float evaluation alone)."""
+    L = load()
+    arrs = [np.ascontiguousarray(np.asarray(a, np.float32)) for a in (lo, hi, axis, angle, p)]
+    n = arrs[3].shape[0]
+    out = np.zeros((n, 2), np.int32)
+    L.hh_silhouette(*[a.ctypes.data for a in arrs], n, out.ctypes.data)
+    return out[:, 0].astype(bool), out[:, 1].astype(bool)

@@ -369,6 +369,25 @@ void hh_trace_pairs(const dr_scene_desc *desc, const float *rays, int n, int *ou
 }
 
 // The reproducible transcendental functions (dr_math.h) on n inputs.
+// The silhouette test of edge-tree nodes, filtered and unfiltered, for n
+// (node, point) pairs: node k from lo[3k..], hi[3k..], axis[3k..], angle[k];
+// point p[3k..].  out[2k] filtered, out[2k + 1] float evaluation alone.
+void hh_silhouette(const float *lo, const float *hi, const float *axis, const float *angle, const float *p,
+                   long long n, int *out) {
+    for (long long k = 0; k < n; k++) {
+        DevEdgeNode nd{};
+        for (int a = 0; a < 3; a++) {
+            nd.lo[a] = lo[3 * k + a];
+            nd.hi[a] = hi[3 * k + a];
+            nd.axis[a] = axis[3 * k + a];
+        }
+        nd.angle = angle[k];
+        float3 q = f3(p[3 * k], p[3 * k + 1], p[3 * k + 2]);
+        out[2 * k] = contains_silhouette(nd, q);
+        out[2 * k + 1] = contains_silhouette_exact(nd, q);
+    }
+}
+
 void hh_math(int fn, const float *x, const float *y, float *out, long long n) {
     for (long long i = 0; i < n; i++) out[i] = dr_math_eval(fn, x[i], y ? y[i] : 0.f);
 }

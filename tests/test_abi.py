@@ -39,6 +39,8 @@ def test_null_arguments_are_rejected_without_a_device():
     assert "NULL" in _lib.last_error()
     with pytest.raises(_lib.DrError):
         _lib.check(L.dr_scene_grad_layout(None, None))
+    assert L.dr_set_item_queue_limit(-1) == 1
+    assert L.dr_set_item_queue_limit(0) == 0
 
 
 def test_render_desc_layout_matches_header():

@@ -18,8 +18,12 @@ def _cfg(**kw):
 
 
 def test_fit_lowers_parameter_error_and_loss():
+    """With common random numbers (the targets rendered on the fit's own
+    sample streams) the image difference comes from the parameters alone; with
+    independent 2-spp streams the gradients of most of the 576 heights are
+    mostly noise at this size, and Adam's steps random-walk them."""
     from delta_ray_b200.inverse import fit
-    res = fit(_cfg(steps=20))
+    res = fit(_cfg(steps=20, common_seeds=True))
     h = res["history"]
     assert res["rmse_final"] < res["rmse_start"]
     losses = [x["loss"] for x in h[1:]]
