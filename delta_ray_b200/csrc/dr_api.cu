@@ -207,6 +207,8 @@ struct dr_scene {
     // lists and scratch, and the arena of the results
     bool gpu_edges = false;
     DevBuf edge_topo, edge_lists, edge_scratch, edge_arena;
+    DevBuf edge_recs;  // silhouette-test records of both trees' edges
+    size_t num_sil_edges = 0, num_nrm_edges = 0;
     int topo_count = 0;
     bool topo_dev_valid = false;
     const DevEdge *kept_dev = nullptr;
@@ -275,6 +277,7 @@ void upload_arena(DevBuf &arena, const ArenaLayout &lay, cudaStream_t st) {
 }
 
 void build_edges_gpu(dr_scene *sc, cudaStream_t st);
+void build_edge_records(dr_scene *sc, cudaStream_t st);
 
 void upload_scene(dr_scene *sc, cudaStream_t st, bool refit = false) {
     HostScene &h = sc->h;
@@ -368,7 +371,23 @@ void upload_scene(dr_scene *sc, cudaStream_t st, bool refit = false) {
     ptr.ltc = sc->ltc->as<float>();
     ptr.ltc_ggx = sc->ltc_ggx->as<float>();
     fill_devscene(sc->ds, h, f, ptr);
+    sc->num_sil_edges = h.sil_edges.size();
+    sc->num_nrm_edges = h.nrm_edges.size();
     if (sc->gpu_edges) build_edges_gpu(sc, st);
+    build_edge_records(sc, st);
+}
+
+// The silhouette-test records of both trees' edges (after every build).
+void build_edge_records(dr_scene *sc, cudaStream_t st) {
+    const size_t ns = sc->num_sil_edges, nn = sc->num_nrm_edges;
+    sc->edge_recs.reserve(sizeof(EdgeRec) * std::max<size_t>(1, ns + nn));
+    EdgeRec *r = sc->edge_recs.as<EdgeRec>();
+    check_cuda(dr_launch_edge_records(sc->ds, sc->ds.sil_edges, (int)ns, r, st), "edge records");
+    check_cuda(dr_launch_edge_records(sc->ds, sc->ds.nrm_edges, (int)nn, r + ns, st), "edge records");
+    check_cuda(cudaStreamSynchronize(st), "edge records");
+    sc->last_launches += 2;
+    sc->ds.sil_rec = r;
+    sc->ds.nrm_rec = r + ns;
 }
 
 // Edges of a flattened tree: the last node in depth-first order is a leaf
@@ -465,6 +484,8 @@ void build_edges_gpu(dr_scene *sc, cudaStream_t st) {
     ds.nrm_nodes = (const DevEdgeNode *)(b + o_nn);
     ds.nrm_edges = (const DevEdge *)(b + o_ne);
     ds.num_nrm_nodes = nn ? n_nn : 0;
+    sc->num_sil_edges = (size_t)ns;
+    sc->num_nrm_edges = (size_t)nn;
     sc->edge_build_ms =
         std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
 }

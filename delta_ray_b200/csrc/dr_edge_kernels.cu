@@ -383,6 +383,17 @@ __global__ void __launch_bounds__(128, 8) k_primary_grad(DevScene s, int W, int 
     block_grad_flush(bg);
 }
 
+__global__ void k_edge_records(DevScene s, const DevEdge *edges, int n, EdgeRec *out) {
+    int i = blockIdx.x * blockDim.x + threadIdx.x;
+    if (i < n) out[i] = edge_record(s, edges[i]);
+}
+
+cudaError_t dr_launch_edge_records(const DevScene &s, const DevEdge *edges, int n, EdgeRec *out, cudaStream_t st) {
+    if (n <= 0) return cudaSuccess;
+    k_edge_records<<<(n + 255) / 256, 256, 0, st>>>(s, edges, n, out);
+    return cudaGetLastError();
+}
+
 // Edges sampled per bucket of points: bucket b sums pt_items over points
 // [b P / nb, (b + 1) P / nb).
 __global__ void k_item_buckets(const int *pt_items, long long P, int nb, unsigned long long *out) {

@@ -40,6 +40,37 @@ DEV bool is_silhouette(const DevScene &s, float3 p, const DevEdge &e) {
     return (f0 && !f1) || (!f0 && f1);
 }
 
+// The silhouette test's record of an edge (see EdgeRec): the same operands
+// is_silhouette computes, so that is_silhouette_rec gives its answer.
+DEV EdgeRec edge_record(const DevScene &s, const DevEdge &e) {
+    EdgeRec r;
+    const bool always = !s.shapes[e.shape].has_n || e.f0 == -1 || e.f1 == -1;
+    float3 v0 = edge_v0(s, e), v1 = edge_v1(s, e), a = v0, b = v1, n0 = f3(0.f), n1 = f3(0.f);
+    if (!always) {
+        a = non_shared_vertex(s, e, e.f0);
+        b = non_shared_vertex(s, e, e.f1);
+        n0 = normalize(cross(v0 - a, v1 - a));
+        n1 = normalize(cross(v1 - b, v0 - b));
+    }
+    r.r[0].x = v0.x, r.r[0].y = v0.y, r.r[0].z = v0.z, r.r[0].w = n0.x;
+    r.r[1].x = v1.x, r.r[1].y = v1.y, r.r[1].z = v1.z, r.r[1].w = n0.y;
+    r.r[2].x = a.x, r.r[2].y = a.y, r.r[2].z = a.z, r.r[2].w = n0.z;
+    r.r[3].x = b.x, r.r[3].y = b.y, r.r[3].z = b.z, r.r[3].w = n1.x;
+    r.r[4].x = n1.y, r.r[4].y = n1.z, r.r[4].z = always ? 1.f : 0.f, r.r[4].w = 0.f;
+    return r;
+}
+
+DEV bool is_silhouette_rec(const EdgeRec *rec, float3 p) {
+    const float4 q0 = dr_ldg(&rec->r[0]), q1 = dr_ldg(&rec->r[1]), q2 = dr_ldg(&rec->r[2]), q3 = dr_ldg(&rec->r[3]),
+                 q4 = dr_ldg(&rec->r[4]);
+    if (q4.z != 0.f) return true;
+    const float3 v0 = f3(q0.x, q0.y, q0.z), v1 = f3(q1.x, q1.y, q1.z), a = f3(q2.x, q2.y, q2.z),
+                 b = f3(q3.x, q3.y, q3.z), n0 = f3(q0.w, q1.w, q2.w), n1 = f3(q3.w, q4.x, q4.y);
+    bool f0 = dot(p - v0, n0) > 0.f && dot(p - v1, n0) > 0.f && dot(p - a, n0) > 0.f;
+    bool f1 = dot(p - v0, n1) > 0.f && dot(p - v1, n1) > 0.f && dot(p - b, n1) > 0.f;
+    return (f0 && !f1) || (!f0 && f1);
+}
+
 // ---------------------------------------------------------------------------
 // Box / cone intersection.  The apex region (per axis: beyond the slab's upper
 // face, inside, below its lower face) selects the silhouette polygon of the
@@ -391,6 +422,7 @@ struct EdgeWalk {
     const DevScene *s;
     const DevEdgeNode *nodes;
     const DevEdge *edges;
+    const EdgeRec *recs;
     BoundCtx bc;
     Frame f;  // shading frame (the proposal's direction bins)
     ConeSpec cone;
@@ -407,6 +439,7 @@ struct EdgeWalk {
         s = &sc;
         nodes = nd;
         edges = ed;
+        recs = tr ? sc.nrm_rec : sc.sil_rec;
         tree = tr;
         dir_bounds = dirb;
         cone_mode = CONE;
@@ -431,7 +464,7 @@ struct EdgeWalk {
         float w = CONE ? it.cpmf / denom : apmf / denom;
         for (int i = 0; i < node.nprims; i++) {
             int ei = node.offset + i;
-            if (!is_silhouette(*s, p, edges[ei])) continue;
+            if (!is_silhouette_rec(recs + ei, p)) continue;
             int code = 0;
             if constexpr (PROP)
                 if (pr.codes) code = dir_bin(f, 0.5f * (edge_v0(*s, edges[ei]) + edge_v1(*s, edges[ei])) - p);
@@ -439,36 +472,22 @@ struct EdgeWalk {
         }
     }
 
-    // One step: the leaves on top of the stack (up to two), then one interior
-    // node.  A lane whose next node is a leaf goes on to an interior node in
-    // the same step, so the interior evaluation, the costly part, runs with
-    // the lanes of the warp together rather than alternating with the leaves.
-    // emit(tree_edge_index, key, weight, slot_code) for every silhouette edge
-    // of a reached leaf.
+    // One step: the node on top of the stack.  emit(tree_edge_index, key,
+    // weight, slot_code) for every silhouette edge of a reached leaf.  (Taking
+    // a lane's leaves together with its next interior node in one step was
+    // measured slower, with the leaf test reading scattered vertices and with
+    // it reading one record per edge.)
     template <class Emit, class Defer> DEV void step(Emit &emit, Defer &defer, int *visits) {
         const bool CONE = cone_mode;
         const float3 p = bc.p;
-        Item it;
-        int nid = 0;
-        bool interior = false;
-#pragma unroll 1
-        for (int k = 0; k < 3 && n > 0; k++) {
-            it = st[--n];
-            if (it.bb <= 0.f) continue;
-            nid = it.node & DR_NODE_MASK;
-            if (visits) ++*visits;
-            if (nodes[nid].nprims == 0) {
-                interior = true;
-                break;
-            }
-            if (k == 2) {  // a third leaf waits for the next step
-                n++;
-                if (visits) --*visits;
-                break;
-            }
+        const Item it = st[--n];
+        if (it.bb <= 0.f) return;
+        const int nid = it.node & DR_NODE_MASK;
+        if (visits) ++*visits;
+        if (nodes[nid].nprims > 0) {
             leaf(it, nodes[nid], emit);
+            return;
         }
-        if (!interior) return;
         const DevEdgeNode &node = nodes[nid];
         if (CUT > 0 && (it.node >> 27) == CUT) {  // hand the subtree on
             float lp = 0.f;
@@ -838,6 +857,35 @@ DEV void edge_side_dirs(const EdgeLine &el, float3 v0, float3 v1, float3 p, floa
     ldir = normalize(sdir - delta * split_n);
 }
 
+// Closest hit among triangles g0 and g1 (g1 < 0: none) under the closest-hit
+// rule, with the operands the LBVH's leaves hold (vertices in index order).
+DEV Hit hit_faces(const DevScene &s, int g0, int g1, float3 o, float3 d, float tnear) {
+    Hit h;
+    h.tri = -1;
+    h.t = DR_INF;
+#pragma unroll 1
+    for (int k = 0; k < 2; k++) {
+        const int g = k ? g1 : g0;
+        if (g < 0) continue;
+        const int4 id = s.tri[g];
+        float4 v[3];
+        const int vi[3] = {id.x, id.y, id.z};
+        for (int j = 0; j < 3; j++) {
+            v[j].x = s.vtx[3 * vi[j]];
+            v[j].y = s.vtx[3 * vi[j] + 1];
+            v[j].z = s.vtx[3 * vi[j] + 2];
+            v[j].w = 0.f;
+        }
+        const float4 a = v[0], b = v[1], c = v[2];
+        float t;
+        if (hit_triangle(a, b, c, o, d, t) && t > tnear && (t < h.t || (t == h.t && g < h.tri))) {
+            h.t = t;
+            h.tri = g;
+        }
+    }
+    return h;
+}
+
 DEV bool edge_rays(const DevScene &s, const EdgeLine &el, const DevEdge &edge, int stri, float3 p, bool direct_only,
                    EdgeHits &out) {
     float3 sdir, rdir, ldir;
@@ -850,8 +898,23 @@ DEV bool edge_rays(const DevScene &s, const EdgeLine &el, const DevEdge &edge, i
         hit[0] = h0.tri;
         hit[1] = h1.tri;
     } else if (s.num_tris > 0) {
-        // both sides in one walk of the LBVH: their directions differ by a few
-        // 1e-3, so they visit nearly the same nodes
+        // The connectivity test first (most samples end there: edges hidden
+        // from p).  A side's closest hit is one of the edge's faces only if
+        // its ray hits one of them, at (ta, ida) by the closest-hit rule, and
+        // no triangle hits ahead of that; a sample goes on only with one side
+        // connected and the other not.  Then both sides' closest hits in one
+        // walk of the LBVH (their directions differ by a few 1e-3, so they
+        // visit nearly the same nodes).
+        const int off = s.shapes[edge.shape].tri_off;
+        const int g0 = off + edge.f0, g1 = edge.f1 >= 0 ? off + edge.f1 : -1;
+        const Hit fr = hit_faces(s, g0, g1, p, rdir, 1e-3f), fl = hit_faces(s, g0, g1, p, ldir, 1e-3f);
+        if (fr.tri < 0 && fl.tri < 0) return false;
+        bool cr = fr.tri >= 0 &&
+                  !trace_before_bvh(s.bvh_nodes, s.bvh_tris, s.bvh_root, p, rdir, 1e-3f, fr.t, fr.tri);
+        if (!cr && fl.tri < 0) return false;
+        bool cl = fl.tri >= 0 &&
+                  !trace_before_bvh(s.bvh_nodes, s.bvh_tris, s.bvh_root, p, ldir, 1e-3f, fl.t, fl.tri);
+        if (cr == cl) return false;
         Hit h0, h1;
         trace_closest_pair_bvh(s.bvh_nodes, s.bvh_tris, s.bvh_root, p, rdir, ldir, 1e-3f, h0, h1);
         hit[0] = h0.tri;

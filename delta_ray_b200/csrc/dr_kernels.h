@@ -11,7 +11,8 @@
 // With `sync` set (the DR_DEBUG_SYNC environment variable, a diagnostic), every
 // mark synchronizes the stream and remembers the first kernel that failed.
 struct StageTimer {
-    static const int kMax = 16;
+    // a streamed edge stage marks six kernels per chunk of points
+    static const int kMax = 1024;
     bool on = false;
     bool sync = false;
     const char *failed = nullptr;
@@ -157,6 +158,8 @@ cudaError_t dr_launch_proposal_features(const DevScene &s, const BackwardWorkspa
                                         float3 ih, void *x, void *xt, cudaStream_t st);
 cudaError_t dr_launch_edge_traverse(const DevScene &s, uint64_t seed, const BackwardWorkspace &ws, int num_sms,
                                     cudaStream_t st, int *launches, StageTimer *timer);
+// The silhouette-test records of n tree edges (dr_edges.cuh: edge_record).
+cudaError_t dr_launch_edge_records(const DevScene &s, const DevEdge *edges, int n, EdgeRec *out, cudaStream_t st);
 // out[b] = edges sampled by points [b P / nb, (b + 1) P / nb) (ws.pt_items)
 cudaError_t dr_launch_item_buckets(const int *pt_items, long long P, int nb, unsigned long long *out,
                                    cudaStream_t st);

@@ -46,6 +46,14 @@ struct DevLight {
 
 struct DevEdge { int shape, v0, v1, f0, f1; };  // local vertex / triangle ids
 
+// What the silhouette test of a tree edge needs, computed once per scene
+// build (dr_edges.cuh: edge_record): its end points v0, v1, the vertices a, b
+// of its two faces opposite it and the faces' unit normals n0, n1;
+// r[0] = (v0, n0.x), r[1] = (v1, n0.y), r[2] = (a, n0.z), r[3] = (b, n1.x),
+// r[4] = (n1.y, n1.z, always, 0): always != 0 for edges that are silhouettes
+// from everywhere (no shading normals, or one face).
+struct EdgeRec { float4 r[5]; };
+
 struct DevEdgeNode {
     float lo[3], hi[3];
     float axis[3], angle;
@@ -113,6 +121,7 @@ struct DevScene {
     const DevEdgeNode *nrm_nodes;
     const DevEdge *nrm_edges;
     int num_nrm_nodes;
+    const EdgeRec *sil_rec, *nrm_rec;  // per tree edge, in the trees' edge order
     const float *ltc;      // 128*128 row-major 3x3, Blinn-Phong lobes
     const float *ltc_ggx;  // the same for GGX lobes
     int grad_total;

@@ -313,6 +313,48 @@ DEV_NOINLINE bool trace_any_bvh(const float4 *DR_RESTRICT nodes, const float4 *D
     return false;
 }
 
+// Whether a triangle hits ahead of (ta, ida) under the closest-hit rule: at t
+// on (tnear, ta), or at ta with a smaller id.  Boxes are culled at ta (the
+// widened test keeps every box holding such a hit), nearer child first.
+DEV_NOINLINE bool trace_before_bvh(const float4 *DR_RESTRICT nodes, const float4 *DR_RESTRICT tris, int root,
+                                   float3 o, float3 d, float tnear, float ta, int ida) {
+    float3 inv = f3(safe_inv(d.x), safe_inv(d.y), safe_inv(d.z));
+    int stack[DR_STACK];
+    int sp = 0;
+    int node = root;
+    while (true) {
+        if (node < 0) {
+            int leaf = ~node;
+            float4 a = dr_ldg(tris + 3 * leaf), b = dr_ldg(tris + 3 * leaf + 1), c = dr_ldg(tris + 3 * leaf + 2);
+            float t;
+            if (hit_triangle(a, b, c, o, d, t) && t > tnear && (t < ta || (t == ta && dr_f2i(a.w) < ida)))
+                return true;
+            if (sp == 0) break;
+            node = stack[--sp];
+            continue;
+        }
+        const float4 *n = nodes + 4 * node;
+        float4 n0 = dr_ldg(n), n1 = dr_ldg(n + 1), n2 = dr_ldg(n + 2), n3 = dr_ldg(n + 3);
+        float e0 = box_entry(n0.x, n0.y, n0.z, n0.w, n1.x, n1.y, o, inv, ta);
+        float e1 = box_entry(n1.z, n1.w, n2.x, n2.y, n2.z, n2.w, o, inv, ta);
+        int c0 = dr_f2i(n3.x), c1 = dr_f2i(n3.y);
+        bool h0 = e0 >= 0.f, h1 = e1 >= 0.f;
+        if (h0 && h1) {
+            int nearc = e0 <= e1 ? c0 : c1, farc = e0 <= e1 ? c1 : c0;
+            if (sp < DR_STACK) stack[sp++] = farc;
+            node = nearc;
+        } else if (h0) {
+            node = c0;
+        } else if (h1) {
+            node = c1;
+        } else {
+            if (sp == 0) break;
+            node = stack[--sp];
+        }
+    }
+    return false;
+}
+
 DEV_NOINLINE bool trace_any_linear(const float4 *DR_RESTRICT tris, int n, float3 o, float3 d, float tnear,
                                    float tfar) {
     for (int i = 0; i < n; i++) {

@@ -83,6 +83,7 @@ struct HostSceneBundle {
     drhost::HostScene h;
     drhost::FlatScene f;
     std::vector<float4> nodes, leaves;
+    std::vector<EdgeRec> recs;
     DevScene ds;
 };
 
@@ -125,6 +126,12 @@ void make_scene(const dr_scene_desc *desc, HostSceneBundle &b) {
     p.ltc = b.h.ltc.data();
     p.ltc_ggx = b.h.ltc_ggx.data();
     drhost::fill_devscene(b.ds, b.h, b.f, p);
+    const size_t ns = b.h.sil_edges.size(), nn = b.h.nrm_edges.size();
+    b.recs.resize(std::max<size_t>(1, ns + nn));
+    for (size_t i = 0; i < ns; i++) b.recs[i] = edge_record(b.ds, b.h.sil_edges[i]);
+    for (size_t i = 0; i < nn; i++) b.recs[ns + i] = edge_record(b.ds, b.h.nrm_edges[i]);
+    b.ds.sil_rec = b.recs.data();
+    b.ds.nrm_rec = b.recs.data() + ns;
 }
 
 }  // namespace
