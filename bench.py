@@ -209,8 +209,10 @@ def kernel_bytes(kernel, wl, work):
                 work["visits_tasks"] * NODE_BYTES)
     if kernel == "k_edge_line":  # item, point record, LTC matrix, material; survivor record out
         return I * (20 + POINT_BYTES + 36 + 28) + work["survivors"] * 32
-    if kernel == "k_edge_rays":  # survivor in, two closest-hit rays, hit record out
-        return work["survivors"] * (32 + 2 * br) + work["shaded"] * 16
+    if kernel == "k_edge_connect":  # survivor in, the two rays' connectivity, candidate record out
+        return work["survivors"] * (32 + 2 * br) + work.get("candidates", 0) * 16
+    if kernel == "k_edge_pairs":  # candidate in, the other side's closest hit, hit record out
+        return work.get("candidates", 0) * (16 + 32 + br + 16)
     if kernel == "k_edge_line_rays":
         return I * (20 + POINT_BYTES + 36 + 28) + work["survivors"] * 2 * br + work["shaded"] * 48
     if kernel == "k_edge_shade":  # records in, shading rays and vertices, dp out, vertex gradient adds

@@ -198,7 +198,7 @@ struct dr_scene {
     // for rays, samples kept for shading, handed-on subtrees, items of the
     // first traversal stage, edge-tree nodes visited by the point walks and by
     // the subtree walks
-    long long last_work[8] = {};
+    long long last_work[9] = {};
     int num_vertices = 0, num_tris = 0, num_sms = 148;
     int bvh_built_tris = 0;  // triangle count of the LBVH topology kept in bvh_scratch
     // scenes of more than kGpuEdgeTris triangles build their edges, edge trees
@@ -610,7 +610,7 @@ std::pair<long long, long long> run_backward(dr_scene *scene, const dr_render_de
         if (c.status & ~(DR_STATUS_ITEM_OVERFLOW | DR_STATUS_POINT_OVERFLOW))
             throw DrError(DR_ERR_DEVICE_STATUS, "device reported status " + std::to_string(c.status));
     };
-    long long work[8] = {};
+    long long work[9] = {};
     // with the DR_DEBUG_SYNC diagnostic, a launch error names the kernel that failed
     auto check_launch = [&](cudaError_t e, const char *what) {
         if (e != cudaSuccess && timer->failed)
@@ -629,6 +629,7 @@ std::pair<long long, long long> run_backward(dr_scene *scene, const dr_render_de
         work[3] += (long long)c.hits;
         work[4] += (long long)c.tasks;
         work[5] += (long long)(ds.split_traversal ? c.items_expand : c.items);
+        work[8] += (long long)c.cands;
     };
     // edges per bucket of points [0, P) from ws.pt_items
     auto read_buckets = [&](long long P, std::vector<unsigned long long> &out) {
@@ -1356,7 +1357,7 @@ dr_status dr_scene_edge_data(const dr_scene *scene, int what, void *out_host, in
 dr_status dr_scene_last_work(const dr_scene *scene, int64_t *counts, int n) {
     return guard([&]() {
         if (!scene || !counts || n < 0) throw DrError(DR_ERR_INVALID_ARGUMENT, "NULL argument");
-        for (int i = 0; i < n && i < 8; i++) counts[i] = scene->last_work[i];
+        for (int i = 0; i < n && i < 9; i++) counts[i] = scene->last_work[i];
     });
 }
 

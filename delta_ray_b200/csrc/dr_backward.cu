@@ -5,8 +5,11 @@
 //   k_edge_traverse    one thread per shading point: edge-tree traversal,
 //                      appends (point, edge, weight) items
 //   k_edge_line        one thread per item: the line sample on the edge
-//   k_edge_rays        one thread per surviving line sample: two straddling
-//                      rays and the tests on their hits
+//   k_edge_connect     surviving line samples fetched one per lane: the
+//                      connectivity of the two straddling rays (the edge's
+//                      faces, bounded occlusion walks)
+//   k_edge_pairs       candidates fetched one per lane: the other side's
+//                      closest hit and the tests on both hits
 //   k_edge_shade       one thread per kept sample: shading of both sides,
 //                      dv0/dv1 scatter and dp
 //   k_dp_propagate     one thread per point: the point's dp through its

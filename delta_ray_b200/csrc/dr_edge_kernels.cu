@@ -11,6 +11,15 @@
 
 namespace cg = cooperative_groups;
 
+// Resident blocks per SM (of 128 threads) of the persistent walk kernels,
+// settable at build time for tuning sweeps.
+#ifndef DR_TASKS_BLOCKS
+#define DR_TASKS_BLOCKS 6
+#endif
+#ifndef DR_CONNECT_BLOCKS
+#define DR_CONNECT_BLOCKS 4
+#endif
+
 #define DR_ITEM_BUF 24
 // One thread per shading point in [pt_begin, pt_end).  A point's items collect
 // in a lane buffer; a full buffer reserves DR_ITEM_BUF slots with one atomic
@@ -172,7 +181,7 @@ __device__ __forceinline__ long long next_task(unsigned long long *counter) {
 }
 
 template <bool PROP>
-__global__ void __launch_bounds__(128, 6) k_edge_tasks(DevScene s, uint64_t seed, BackwardWorkspace ws) {
+__global__ void __launch_bounds__(128, DR_TASKS_BLOCKS) k_edge_tasks(DevScene s, uint64_t seed, BackwardWorkspace ws) {
     const long long n = (long long)min(ws.counters->tasks, (unsigned long long)ws.cap_tasks);
     ItemWriter out(ws);
     int visits = 0, point = 0, cnt = 0;
@@ -235,14 +244,14 @@ __device__ __forceinline__ void finish_item(const DevScene &s, const BackwardWor
     }
 }
 
-// Edge evaluation as a three-kernel wavefront, each stage compacting what it
-// keeps so that the next runs with full warps.  k_edge_line: the line sample
-// of every item (silhouette test, LTC lobe, point on the edge); often half the
-// items end here (edges in the point's own plane, below the lobe's horizon or
-// outside the clipped segment).  k_edge_rays: the two rays of each survivor and
-// the tests on their hits; with direct lighting only, a sample neither of whose
-// rays hits an emitter ends here too.  k_edge_shade: the shading and the
-// Jacobians of the rest.
+// Edge evaluation as a wavefront, each stage compacting what it keeps so that
+// the next runs with full warps.  k_edge_line: the line sample of every item
+// (silhouette test, LTC lobe, point on the edge); often half the items end
+// here (edges in the point's own plane, below the lobe's horizon or outside
+// the clipped segment).  The ray stage (k_edge_connect, k_edge_pairs): the two
+// rays of each survivor and the tests on their hits; with direct lighting
+// only, a sample neither of whose rays hits an emitter ends here too.
+// k_edge_shade: the shading and the Jacobians of the rest.
 //
 // EXT: DR_FLAG_EDGE_LOBE_MIS or proposal training in use; GI: max_bounces > 1
 // (the shade calls of the two sides); the launcher picks the variant.
@@ -270,29 +279,112 @@ __global__ void __launch_bounds__(128, 4) k_edge_line(DevScene s, uint64_t seed,
     }
 }
 
-template <bool DIRECT>
-__global__ void __launch_bounds__(128, 4) k_edge_rays(DevScene s, BackwardWorkspace ws) {
-    long long n = (long long)min(ws.counters->survivors, (unsigned long long)ws.cap_items);
-    long long stride = (long long)gridDim.x * blockDim.x;
-    // warp-uniform loop: the append is warp-aggregated
-    for (long long base = (long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < n; base += stride) {
-        long long k = base + (threadIdx.x & 31);
-        EdgeHits eh;
-        bool ok = false;
-        if (k < n) {
-            float4 a = ws.survivors[2 * k];
-            int4 it = ws.items[__float_as_int(a.x)];
-            // the point's position and triangle: words 0-2 and 17 of its record
-            const float *w = ws.pt + (size_t)it.x * DR_PT_WORDS;
+// The ray stage of an LBVH scene in two kernels.  k_edge_connect decides
+// each line sample's connectivity (the edge's faces and one or two bounded
+// occlusion walks; most samples end here) and queues the few that go on;
+// k_edge_pairs traces the other side's closest hit of those and runs the
+// remaining tests.  Walk lengths vary widely, so both fetch their work one
+// item per lane (a lane takes the next as soon as it is done) rather than a
+// warp's worth at a time.
+__global__ void __launch_bounds__(128, DR_CONNECT_BLOCKS) k_edge_connect(DevScene s, BackwardWorkspace ws) {
+    const long long n = (long long)min(ws.counters->survivors, (unsigned long long)ws.cap_items);
+    // A state machine per lane, stepped by the whole warp.  When at least
+    // half the warp has no walk (or none has), those lanes take line samples
+    // together (a sample's setup and face tests cost about ten walk steps)
+    // until each has one that needs an occlusion walk; otherwise every
+    // walking lane takes one node, at the same point of the code.  (Lanes
+    // that ran their walks to the end before taking the next sample, and
+    // lanes that took one as soon as they were idle, left the warp split
+    // into groups issuing on their own: 5.1 and 3.8 of 32 lanes active.)
+    long long k = 0;
+    int phase = 0;  // 0 no walk, 1 walking the right ray, 2 walking the left ray
+    bool more = true, cr = false;
+    float3 p = f3(0.f), rdir = f3(0.f), ldir = f3(0.f);
+    Hit fr, fl;
+    fr.tri = fl.tri = -1;
+    fr.t = fl.t = 0.f;
+    BeforeWalk w;
+    auto candidate = [&](int side, int face) {
+        const long long j = next_task(&ws.counters->cands);
+        ws.hits[j] = make_int4((int)k, face, side, 0);
+    };
+    while (true) {
+        const unsigned walking = __ballot_sync(0xffffffffu, phase != 0);
+        const unsigned idle = __ballot_sync(0xffffffffu, phase == 0 && more);
+        if (walking == 0 && idle == 0) break;  // every lane's queue has ended
+        const bool fetch = idle != 0 && (__popc(idle) >= 16 || walking == 0);
+        while (fetch && phase == 0 && more) {
+            k = next_task(&ws.counters->ray_next);
+            if (k >= n) {
+                more = false;
+                break;
+            }
+            const float4 a = ws.survivors[2 * k];
+            const int4 it = ws.items[__float_as_int(a.x)];
+            const float *pw = ws.pt + (size_t)it.x * DR_PT_WORDS;  // the point's position: words 0-2
+            const int tree = it.y >> 30, ei = it.y & ((1 << 30) - 1);
+            const DevEdge &edge = tree ? s.nrm_edges[ei] : s.sil_edges[ei];
+            p = f3(pw[0], pw[1], pw[2]);
             EdgeLine el;
             el.sample_p = f3(a.y, a.z, a.w);
-            int tree = it.y >> 30, ei = it.y & ((1 << 30) - 1);
-            const DevEdge &edge = tree ? s.nrm_edges[ei] : s.sil_edges[ei];
-            ok = edge_rays(s, el, edge, dr_f2i(w[17]), f3(w[0], w[1], w[2]), DIRECT, eh);
+            float3 sdir;
+            edge_side_dirs(el, edge_v0(s, edge), edge_v1(s, edge), p, sdir, rdir, ldir);
+            // the connectivity test of edge_connect_bvh, its walks stepped below
+            const int off = s.shapes[edge.shape].tri_off;
+            const int g0 = off + edge.f0, g1 = edge.f1 >= 0 ? off + edge.f1 : -1;
+            fr = hit_faces(s, g0, g1, p, rdir, 1e-3f);
+            fl = hit_faces(s, g0, g1, p, ldir, 1e-3f);
+            if (fr.tri >= 0) {
+                w.begin(s.bvh_root, p, rdir, 1e-3f, fr.t, fr.tri);
+                phase = 1;
+            } else if (fl.tri >= 0) {
+                cr = false;
+                w.begin(s.bvh_root, p, ldir, 1e-3f, fl.t, fl.tri);
+                phase = 2;
+            }
         }
-        __syncwarp();
-        unsigned long long slot = warp_reserve(&ws.counters->hits, ok ? 1 : 0);
-        if (ok) ws.hits[slot] = make_int4((int)k, eh.r, eh.l, 0);
+        if (fetch || phase == 0) continue;
+        const int r = w.step(s.bvh_nodes, s.bvh_tris);
+        if (r == 0) continue;
+        if (phase == 1) {
+            cr = r == 2;  // no triangle ahead of the right face hit
+            if (fl.tri >= 0) {  // the left side decides (both connected, or neither, ends the sample)
+                w.begin(s.bvh_root, p, ldir, 1e-3f, fl.t, fl.tri);
+                phase = 2;
+            } else {
+                if (cr) candidate(0, fr.tri);  // the left ray hits no face: not connected
+                phase = 0;
+            }
+        } else {
+            const bool cl = r == 2;
+            if (cr != cl) candidate(cr ? 0 : 1, cr ? fr.tri : fl.tri);
+            phase = 0;
+        }
+    }
+}
+
+template <bool DIRECT>
+__global__ void __launch_bounds__(128, 4) k_edge_pairs(DevScene s, BackwardWorkspace ws) {
+    const long long n = (long long)min(ws.counters->cands, (unsigned long long)ws.cap_items);
+    while (true) {
+        const long long j = next_task(&ws.counters->pair_next);
+        if (j >= n) break;
+        const int4 c = ws.hits[j];
+        const float4 a = ws.survivors[2 * (long long)c.x];
+        const int4 it = ws.items[__float_as_int(a.x)];
+        // the point's position and triangle: words 0-2 and 17 of its record
+        const float *w = ws.pt + (size_t)it.x * DR_PT_WORDS;
+        const int tree = it.y >> 30, ei = it.y & ((1 << 30) - 1);
+        const DevEdge &edge = tree ? s.nrm_edges[ei] : s.sil_edges[ei];
+        const float3 p = f3(w[0], w[1], w[2]);
+        EdgeLine el;
+        el.sample_p = f3(a.y, a.z, a.w);
+        float3 sdir, rdir, ldir;
+        edge_side_dirs(el, edge_v0(s, edge), edge_v1(s, edge), p, sdir, rdir, ldir);
+        EdgeHits eh;
+        const bool ok = edge_rays_rest(s, dr_f2i(w[17]), p, rdir, ldir, c.z, c.y, DIRECT, eh);
+        ws.hits[j] = make_int4(c.x, ok ? eh.r : -1, ok ? eh.l : -1, ok ? 1 : 0);
+        if (ok) next_task(&ws.counters->hits);  // the count of kept samples
     }
 }
 
@@ -300,7 +392,7 @@ __global__ void __launch_bounds__(128, 4) k_edge_rays(DevScene s, BackwardWorksp
 // are cheap, so the line sample and its rays run in one kernel without the
 // survivor queue in between; a kept sample's survivor and hit records go to
 // one slot (hits[slot].x = slot), which k_edge_shade reads as it does the
-// records of k_edge_rays.
+// records of the ray stage.
 template <bool EXT, bool DIRECT>
 __global__ void __launch_bounds__(128, 8) k_edge_line_rays(DevScene s, uint64_t seed, BackwardWorkspace ws) {
     long long n = (long long)min(ws.counters->items, (unsigned long long)ws.cap_items);
@@ -323,11 +415,12 @@ __global__ void __launch_bounds__(128, 8) k_edge_line_rays(DevScene s, uint64_t 
             }
         }
         __syncwarp();
-        unsigned long long slot = warp_reserve(&ws.counters->hits, ok ? 1 : 0);
+        unsigned long long slot = warp_reserve(&ws.counters->cands, ok ? 1 : 0);
         if (ok) {
             ws.survivors[2 * slot] = make_float4(__int_as_float((int)i), el.sample_p.x, el.sample_p.y, el.sample_p.z);
             ws.survivors[2 * slot + 1] = make_float4(el.mwt.x, el.mwt.y, el.mwt.z, el.q);
-            ws.hits[slot] = make_int4((int)slot, eh.r, eh.l, 0);
+            ws.hits[slot] = make_int4((int)slot, eh.r, eh.l, 1);
+            next_task(&ws.counters->hits);  // the count of kept samples
         }
     }
 }
@@ -337,9 +430,10 @@ __global__ void __launch_bounds__(128, 4) k_edge_shade(DevScene s, int W, int H,
                                                     int dp_mode, float *grad, BackwardWorkspace ws, GradCacheCfg cfg) {
     extern __shared__ float sm[];
     BlockGrad bg = block_grad_begin(sm, grad, cfg);
-    long long n = (long long)min(ws.counters->hits, (unsigned long long)ws.cap_items);
+    long long n = (long long)min(ws.counters->cands, (unsigned long long)ws.cap_items);
     for (long long h = (long long)blockIdx.x * blockDim.x + threadIdx.x; h < n; h += (long long)gridDim.x * blockDim.x) {
         int4 hr = ws.hits[h];
+        if (hr.w == 0) continue;  // a candidate the ray stage dropped
         EdgeHits eh;
         eh.r = hr.y;
         eh.l = hr.z;
@@ -453,8 +547,10 @@ cudaError_t dr_launch_edge_eval(const DevScene &s, int W, int H, int spp, int B,
     size_t smem = sizeof(float) * (size_t)(cfg.head + cfg.tail_len);
     const bool ext = s.edge_lobe_mis || ws.train_targets;
     const int grid = stage_grid(num_sms);
-    // the survivor and hit counters (adjacent)
+    // the survivor and hit counters (adjacent) and those of the ray stage
     cudaError_t e = cudaMemsetAsync(&ws.counters->survivors, 0, 2 * sizeof(unsigned long long), st);
+    if (e != cudaSuccess) return e;
+    e = cudaMemsetAsync(&ws.counters->ray_next, 0, 3 * sizeof(unsigned long long), st);
     if (e != cudaSuccess) return e;
     if (s.num_tris <= DR_LINEAR_TRIS) {
         auto line_rays = ext ? (B > 1 ? k_edge_line_rays<true, false> : k_edge_line_rays<true, true>)
@@ -466,9 +562,12 @@ cudaError_t dr_launch_edge_eval(const DevScene &s, int W, int H, int spp, int B,
         if (ext) k_edge_line<true><<<grid, 128, 0, st>>>(s, seed, ws);
         else k_edge_line<false><<<grid, 128, 0, st>>>(s, seed, ws);
         timer->mark(st, "k_edge_line");
-        if (B > 1) k_edge_rays<false><<<grid, 128, 0, st>>>(s, ws);
-        else k_edge_rays<true><<<grid, 128, 0, st>>>(s, ws);
-        timer->mark(st, "k_edge_rays");
+        k_edge_connect<<<grid, 128, 0, st>>>(s, ws);
+        timer->mark(st, "k_edge_connect");
+        if (B > 1) k_edge_pairs<false><<<grid, 128, 0, st>>>(s, ws);
+        else k_edge_pairs<true><<<grid, 128, 0, st>>>(s, ws);
+        timer->mark(st, "k_edge_pairs");
+        *launches += 1;
     }
     auto shade = ext ? (B > 1 ? k_edge_shade<true, true> : k_edge_shade<true, false>)
                      : (B > 1 ? k_edge_shade<false, true> : k_edge_shade<false, false>);

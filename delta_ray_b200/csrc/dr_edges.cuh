@@ -555,9 +555,10 @@ struct EdgeWalk {
                 ok = false;
                 return;
             }
-            // depth first, left subtree before right
-            if (rcs) st[n++] = right;
-            if (lcs) st[n++] = left;
+            // depth first, left subtree before right; a child of bound 0 would
+            // only be taken off the stack and skipped, so it is not pushed
+            if (rcs && !(rbb <= 0.f)) st[n++] = right;
+            if (lcs && !(lbb <= 0.f)) st[n++] = left;
         } else {
             float u = rng.draw(CONE ? 0 : 1, nid);
             bool go_left = CONE ? u < plc : u < (learned ? pll : pla);
@@ -565,7 +566,7 @@ struct EdgeWalk {
                 ok = false;
                 return;
             }
-            st[n++] = go_left ? left : right;
+            if (!((go_left ? lbb : rbb) <= 0.f)) st[n++] = go_left ? left : right;
         }
     }
 };
@@ -886,51 +887,34 @@ DEV Hit hit_faces(const DevScene &s, int g0, int g1, float3 o, float3 d, float t
     return h;
 }
 
-DEV bool edge_rays(const DevScene &s, const EdgeLine &el, const DevEdge &edge, int stri, float3 p, bool direct_only,
-                   EdgeHits &out) {
-    float3 sdir, rdir, ldir;
-    edge_side_dirs(el, edge_v0(s, edge), edge_v1(s, edge), p, sdir, rdir, ldir);
-    int hit[2];
-    bool conn[2];
-    if (s.num_tris > 0 && s.num_tris <= DR_LINEAR_TRIS) {
-        Hit h0, h1;
-        trace_closest_pair_linear(s.bvh_tris, s.num_tris, p, rdir, ldir, 1e-3f, h0, h1);
-        hit[0] = h0.tri;
-        hit[1] = h1.tri;
-    } else if (s.num_tris > 0) {
-        // The connectivity test first (most samples end there: edges hidden
-        // from p).  A side's closest hit is one of the edge's faces only if
-        // its ray hits one of them, at (ta, ida) by the closest-hit rule, and
-        // no triangle hits ahead of that; a sample goes on only with one side
-        // connected and the other not.  Then both sides' closest hits in one
-        // walk of the LBVH (their directions differ by a few 1e-3, so they
-        // visit nearly the same nodes).
-        const int off = s.shapes[edge.shape].tri_off;
-        const int g0 = off + edge.f0, g1 = edge.f1 >= 0 ? off + edge.f1 : -1;
-        const Hit fr = hit_faces(s, g0, g1, p, rdir, 1e-3f), fl = hit_faces(s, g0, g1, p, ldir, 1e-3f);
-        if (fr.tri < 0 && fl.tri < 0) return false;
-        bool cr = fr.tri >= 0 &&
-                  !trace_before_bvh(s.bvh_nodes, s.bvh_tris, s.bvh_root, p, rdir, 1e-3f, fr.t, fr.tri);
-        if (!cr && fl.tri < 0) return false;
-        bool cl = fl.tri >= 0 &&
-                  !trace_before_bvh(s.bvh_nodes, s.bvh_tris, s.bvh_root, p, ldir, 1e-3f, fl.t, fl.tri);
-        if (cr == cl) return false;
-        Hit h0, h1;
-        trace_closest_pair_bvh(s.bvh_nodes, s.bvh_tris, s.bvh_root, p, rdir, ldir, 1e-3f, h0, h1);
-        hit[0] = h0.tri;
-        hit[1] = h1.tri;
-    } else {
-        hit[0] = hit[1] = -1;
-    }
-#pragma unroll 1
-    for (int k = 0; k < 2; k++) {
-        conn[k] = false;
-        if (hit[k] >= 0) {
-            int lt = s.tri_local[hit[k]];
-            conn[k] = s.tri[hit[k]].w == edge.shape && (lt == edge.f0 || lt == edge.f1);
-        }
-    }
-    if (conn[0] == conn[1] || (hit[0] >= 0 && hit[0] == stri) || (hit[1] >= 0 && hit[1] == stri)) return false;
+// The connectivity test of an edge sample in an LBVH scene (most samples
+// end here: edges hidden from p).  A side's closest hit is one of the edge's
+// faces only if its ray hits one of them, at (ta, ida) by the closest-hit
+// rule, and no triangle hits ahead of that.  True if exactly one side is
+// connected: `side` (0 the right ray, 1 the left) and `face`, its closest hit.
+DEV bool edge_connect_bvh(const DevScene &s, const DevEdge &edge, float3 p, float3 rdir, float3 ldir, int &side,
+                          int &face) {
+    const int off = s.shapes[edge.shape].tri_off;
+    const int g0 = off + edge.f0, g1 = edge.f1 >= 0 ? off + edge.f1 : -1;
+    const Hit fr = hit_faces(s, g0, g1, p, rdir, 1e-3f), fl = hit_faces(s, g0, g1, p, ldir, 1e-3f);
+    if (fr.tri < 0 && fl.tri < 0) return false;
+    const bool cr = fr.tri >= 0 && !trace_before_bvh(s.bvh_nodes, s.bvh_tris, s.bvh_root, p, rdir, 1e-3f, fr.t, fr.tri);
+    if (!cr && fl.tri < 0) return false;
+    const bool cl = fl.tri >= 0 && !trace_before_bvh(s.bvh_nodes, s.bvh_tris, s.bvh_root, p, ldir, 1e-3f, fl.t, fl.tri);
+    if (cr == cl) return false;
+    side = cr ? 0 : 1;
+    face = cr ? fr.tri : fl.tri;
+    return true;
+}
+
+// The tests on the two sides' closest hits after the connectivity test: a
+// side that hits the shading point's own triangle, or a hit point nearly in
+// the plane through p along its ray (degenerate), ends the sample; with
+// direct lighting only, so does a sample neither of whose sides reaches an
+// emitter.
+DEV bool edge_hits_ok(const DevScene &s, int stri, float3 p, float3 rdir, float3 ldir, const int *hit,
+                      bool direct_only) {
+    if ((hit[0] >= 0 && hit[0] == stri) || (hit[1] >= 0 && hit[1] == stri)) return false;
 #pragma unroll 1
     for (int k = 0; k < 2; k++) {
         if (hit[k] < 0) continue;
@@ -940,6 +924,50 @@ DEV bool edge_rays(const DevScene &s, const EdgeLine &el, const DevEdge &edge, i
     }
     if (direct_only && (hit[0] < 0 || light_of_tri(s, hit[0]) < 0) && (hit[1] < 0 || light_of_tri(s, hit[1]) < 0))
         return false;
+    return true;
+}
+
+// The rest of an LBVH scene's sample once one side is connected: the other
+// side's closest hit, then edge_hits_ok.
+DEV bool edge_rays_rest(const DevScene &s, int stri, float3 p, float3 rdir, float3 ldir, int side, int face,
+                        bool direct_only, EdgeHits &out) {
+    int hit[2];
+    hit[side] = face;
+    hit[1 - side] = trace_closest_bvh(s.bvh_nodes, s.bvh_tris, s.bvh_root, p, side ? rdir : ldir, 1e-3f).tri;
+    if (!edge_hits_ok(s, stri, p, rdir, ldir, hit, direct_only)) return false;
+    out.r = hit[0];
+    out.l = hit[1];
+    return true;
+}
+
+DEV bool edge_rays(const DevScene &s, const EdgeLine &el, const DevEdge &edge, int stri, float3 p, bool direct_only,
+                   EdgeHits &out) {
+    float3 sdir, rdir, ldir;
+    edge_side_dirs(el, edge_v0(s, edge), edge_v1(s, edge), p, sdir, rdir, ldir);
+    if (s.num_tris > DR_LINEAR_TRIS) {
+        int side, face;
+        if (!edge_connect_bvh(s, edge, p, rdir, ldir, side, face)) return false;
+        return edge_rays_rest(s, stri, p, rdir, ldir, side, face, direct_only, out);
+    }
+    int hit[2];
+    if (s.num_tris > 0) {
+        Hit h0, h1;
+        trace_closest_pair_linear(s.bvh_tris, s.num_tris, p, rdir, ldir, 1e-3f, h0, h1);
+        hit[0] = h0.tri;
+        hit[1] = h1.tri;
+    } else {
+        hit[0] = hit[1] = -1;
+    }
+    bool conn[2];
+#pragma unroll 1
+    for (int k = 0; k < 2; k++) {
+        conn[k] = false;
+        if (hit[k] >= 0) {
+            int lt = s.tri_local[hit[k]];
+            conn[k] = s.tri[hit[k]].w == edge.shape && (lt == edge.f0 || lt == edge.f1);
+        }
+    }
+    if (conn[0] == conn[1] || !edge_hits_ok(s, stri, p, rdir, ldir, hit, direct_only)) return false;
     out.r = hit[0];
     out.l = hit[1];
     return true;

@@ -85,14 +85,18 @@ struct BackwardCounters {
     unsigned long long items;   // edge items appended by the last k_edge_traverse
     int status;                 // DR_STATUS_* bits
     int pad;
-    unsigned long long survivors;  // line samples k_edge_line kept for k_edge_rays
-    unsigned long long hits;       // samples k_edge_rays kept for k_edge_shade (follows survivors)
+    unsigned long long survivors;  // line samples k_edge_line kept for the ray stage
+    unsigned long long hits;       // samples the ray stage kept for k_edge_shade (follows survivors)
     unsigned long long tasks;      // subtrees k_edge_expand handed on to k_edge_tasks
     // work counts for the roofline's byte model: edge-tree nodes visited by
     // the point walks (k_edge_traverse / k_edge_expand) and by k_edge_tasks,
     // and the item count when k_edge_expand finished
     unsigned long long visits_walk, visits_tasks, items_expand;
     unsigned long long task_next;  // next task of k_edge_tasks (lanes fetch them one by one)
+    // the ray stage: line samples fetched by k_edge_connect, its candidates
+    // (records in `hits`, flagged by k_edge_pairs; `hits` counts the flagged
+    // ones), candidates fetched by k_edge_pairs
+    unsigned long long ray_next, cands, pair_next;
 };
 
 struct BackwardWorkspace {
@@ -118,8 +122,8 @@ struct BackwardWorkspace {
     // line samples that survived the first phase of edge evaluation:
     // [cap_items][2] float4 (item index bits, sample_p; d sample_p / d l, density)
     float4 *survivors;
-    // [cap_items] (survivor index, closest-hit triangle of the right and the
-    // left ray, 0): the line samples whose rays k_edge_rays kept
+    // [cap_items] per candidate of the ray stage (survivor index, closest-hit
+    // triangle of the right and the left ray, kept ? 1 : 0)
     int4 *hits;
     // subtrees of large trees' traversals handed on to a second stage
     // (null: one thread walks each point whole)

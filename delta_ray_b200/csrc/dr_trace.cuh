@@ -313,6 +313,57 @@ DEV_NOINLINE bool trace_any_bvh(const float4 *DR_RESTRICT nodes, const float4 *D
     return false;
 }
 
+// The walk of trace_before_bvh as a resumable state: begin() sets it up,
+// step() takes one node (a box pair or a leaf) and returns 0 while the walk
+// goes on, 1 when a triangle hits ahead of (ta, ida), 2 when none does.
+// Kernels that interleave many such walks step every walking lane together.
+struct BeforeWalk {
+    float3 o, d, inv;
+    float tnear, ta;
+    int ida, sp, node;
+    int stack[DR_STACK];
+    DEV void begin(int root, float3 o_, float3 d_, float tnear_, float ta_, int ida_) {
+        o = o_;
+        d = d_;
+        inv = f3(safe_inv(d.x), safe_inv(d.y), safe_inv(d.z));
+        tnear = tnear_;
+        ta = ta_;
+        ida = ida_;
+        sp = 0;
+        node = root;
+    }
+    DEV int step(const float4 *DR_RESTRICT nodes, const float4 *DR_RESTRICT tris) {
+        if (node < 0) {
+            const int leaf = ~node;
+            float4 a = dr_ldg(tris + 3 * leaf), b = dr_ldg(tris + 3 * leaf + 1), c = dr_ldg(tris + 3 * leaf + 2);
+            float t;
+            if (hit_triangle(a, b, c, o, d, t) && t > tnear && (t < ta || (t == ta && dr_f2i(a.w) < ida))) return 1;
+            if (sp == 0) return 2;
+            node = stack[--sp];
+            return 0;
+        }
+        const float4 *n = nodes + 4 * node;
+        float4 n0 = dr_ldg(n), n1 = dr_ldg(n + 1), n2 = dr_ldg(n + 2), n3 = dr_ldg(n + 3);
+        float e0 = box_entry(n0.x, n0.y, n0.z, n0.w, n1.x, n1.y, o, inv, ta);
+        float e1 = box_entry(n1.z, n1.w, n2.x, n2.y, n2.z, n2.w, o, inv, ta);
+        int c0 = dr_f2i(n3.x), c1 = dr_f2i(n3.y);
+        bool h0 = e0 >= 0.f, h1 = e1 >= 0.f;
+        if (h0 && h1) {
+            int nearc = e0 <= e1 ? c0 : c1, farc = e0 <= e1 ? c1 : c0;
+            if (sp < DR_STACK) stack[sp++] = farc;
+            node = nearc;
+        } else if (h0) {
+            node = c0;
+        } else if (h1) {
+            node = c1;
+        } else {
+            if (sp == 0) return 2;
+            node = stack[--sp];
+        }
+        return 0;
+    }
+};
+
 // Whether a triangle hits ahead of (ta, ida) under the closest-hit rule: at t
 // on (tnear, ta), or at ta with a smaller id.  Boxes are culled at ta (the
 // widened test keeps every box holding such a hit), nearer child first.

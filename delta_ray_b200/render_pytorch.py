@@ -235,11 +235,12 @@ class Scene:
     def last_work(self):
         """Work counts of the last backward call (dr_scene_last_work): points,
         items, ray survivors, shaded samples, subtree tasks, first-stage items,
-        node visits of the point walks and of the subtree walks."""
-        w = (C.c_int64 * 8)()
-        _lib.check(_lib.lib().dr_scene_last_work(self.handle, w, 8))
+        node visits of the point walks and of the subtree walks, candidates of
+        the ray stage (samples that passed its connectivity test)."""
+        w = (C.c_int64 * 9)()
+        _lib.check(_lib.lib().dr_scene_last_work(self.handle, w, 9))
         keys = ("points", "items", "survivors", "shaded", "tasks", "items_first_stage", "visits_walk",
-                "visits_tasks")
+                "visits_tasks", "candidates")
         return dict(zip(keys, (int(x) for x in w)))
 
     def last_counts(self):

@@ -326,7 +326,8 @@ DR_API dr_status dr_scene_edge_data(const dr_scene *scene, int what, void *out_h
  * for shading, [4] subtrees handed from the first traversal stage to the
  * second, [5] edges sampled by the first stage (all, when the traversal runs
  * in one stage), [6] edge-tree nodes visited by the point walks, [7] nodes
- * visited by the subtree walks.  Up to n of them are written. */
+ * visited by the subtree walks, [8] line samples whose connectivity test
+ * passed (candidates of the ray stage).  Up to n of them are written. */
 DR_API dr_status dr_scene_last_work(const dr_scene *scene, int64_t *counts, int n);
 
 /* Kernel launch count of the last render call on this scene (for tooling). */

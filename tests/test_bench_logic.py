@@ -18,12 +18,13 @@ class _Wl:
 
 WORK = {"points": 1_000_000, "items": 1_100_000_000, "survivors": 500_000_000, "shaded": 100_000_000,
         "tasks": 20_000_000, "items_first_stage": 1_000_000, "visits_walk": 400_000_000,
-        "visits_tasks": 3_000_000_000}
+        "visits_tasks": 3_000_000_000, "candidates": 120_000_000}
 
 
 def test_every_kernel_of_a_step_has_model_bytes():
     for k in ("k_render_forward", "k_backward_paths", "k_primary_shade", "k_primary_grad", "k_edge_traverse",
-              "k_edge_expand", "k_edge_tasks", "k_edge_line", "k_edge_rays", "k_edge_line_rays", "k_edge_shade",
+              "k_edge_expand", "k_edge_tasks", "k_edge_line", "k_edge_connect", "k_edge_pairs", "k_edge_line_rays",
+              "k_edge_shade",
               "k_dp_propagate"):
         assert bench.kernel_bytes(k, _Wl, WORK) > 0, k
     assert bench.kernel_bytes("host_queue_check", _Wl, WORK) == 0
@@ -37,7 +38,7 @@ def test_byte_model_counts_nodes_and_rays():
     assert bench.ray_bytes(130054) == 24 + 16 + 36 + 64 * 17
     assert bench.ray_bytes(8) == 24 + 16 + 36 + 64 * 3
     w3 = dict(WORK, survivors=WORK["survivors"] + 10)
-    assert bench.kernel_bytes("k_edge_rays", _Wl, w3) - bench.kernel_bytes("k_edge_rays", _Wl, WORK) == \
+    assert bench.kernel_bytes("k_edge_connect", _Wl, w3) - bench.kernel_bytes("k_edge_connect", _Wl, WORK) == \
         10 * (32 + 2 * bench.ray_bytes(130054))
 
 
@@ -58,7 +59,7 @@ def test_profile_table_reader(tmp_path, monkeypatch):
     monkeypatch.setattr(bench, "WORKLOAD_KEY", "heightfield")
     p = bench.load_profile("k_edge_tasks")
     assert p["dram_bytes"] == 123456 and p["l2_hit_pct"] == 87.5 and p["units"] == 76800
-    assert bench.load_profile("k_edge_rays") is None
+    assert bench.load_profile("k_edge_connect") is None
 
 
 def test_reference_arm_reports_ggx_workload_unavailable():
