@@ -96,7 +96,7 @@ struct EdgeStats {
 };
 
 struct BackwardQueues {
-    DevBuf pt, items, item_w, item_dp, pt_last, pt_items, counts, survivors, hits, tasks;
+    DevBuf pt, items, item_w, item_dp, pt_last, pt_items, counts, survivors, hits, side_rad, tasks, tasks2;
     long long cap_items = 0;     // grown on overflow, kept with the buffers
     double points_per_sample = 1;  // shading points per pixel sample the last overflow asked for
     EdgeStats stats;
@@ -627,14 +627,15 @@ std::pair<long long, long long> run_backward(dr_scene *scene, const dr_render_de
         read();
         work[2] += (long long)c.survivors;
         work[3] += (long long)c.hits;
-        work[4] += (long long)c.tasks;
+        work[4] += (long long)(c.tasks + c.handed_total);
         work[5] += (long long)(ds.split_traversal ? c.items_expand : c.items);
         work[8] += (long long)c.cands;
     };
-    // edges per bucket of points [0, P) from ws.pt_items
-    auto read_buckets = [&](long long P, std::vector<unsigned long long> &out) {
+    // edges per bucket of points [p0, p0 + np) from ws.pt_items
+    auto read_buckets_at = [&](long long p0, long long np, std::vector<unsigned long long> &out) {
         stats->dev.reserve(sizeof(unsigned long long) * kItemBuckets);
-        check_cuda(dr_launch_item_buckets(ws.pt_items, P, kItemBuckets, stats->dev.as<unsigned long long>(), st),
+        check_cuda(dr_launch_item_buckets(ws.pt_items + p0, np, kItemBuckets, stats->dev.as<unsigned long long>(),
+                                          st),
                    "item buckets");
         scene->last_launches += 1;
         out.resize(kItemBuckets);
@@ -642,6 +643,24 @@ std::pair<long long, long long> run_backward(dr_scene *scene, const dr_render_de
                                    cudaMemcpyDeviceToHost, st),
                    "bucket read");
         check_cuda(cudaStreamSynchronize(st), "item buckets");
+    };
+    auto read_buckets = [&](long long P, std::vector<unsigned long long> &out) { read_buckets_at(0, P, out); };
+    // ends of chunks of points [p0, p0 + np) whose edges, by buckets `b` over
+    // that range (scaled by `scale`), stay within `budget`; ascending, inside
+    // (p0, p0 + np)
+    auto plan_ends = [](const std::vector<unsigned long long> &b, long long p0, long long np, double budget,
+                        double scale, std::vector<long long> &ends) {
+        double acc = 0;
+        long long last = p0;
+        for (int i = 0; i < (int)b.size(); i++) {
+            const long long at = p0 + (long long)i * np / (long long)b.size();
+            if (acc > 0 && acc + (double)b[i] * scale > budget && at > last) {
+                ends.push_back(at);
+                last = at;
+                acc = 0;
+            }
+            acc += (double)b[i] * scale;
+        }
     };
     // when the last call's edges per point predict more items than the queue
     // can ever hold, the edge stage streams from the start instead of
@@ -717,7 +736,7 @@ std::pair<long long, long long> run_backward(dr_scene *scene, const dr_render_de
         // edges per point it is a forecast, and a chunk that overflows is cut.
         streamed = true;
         std::vector<unsigned long long> b;
-        double scale = 1, margin = 0.9;
+        double scale = 1, margin = 0.85;
         long long needed;
         if (!stream_first) {
             needed = (long long)c.items;
@@ -737,15 +756,7 @@ std::pair<long long, long long> run_backward(dr_scene *scene, const dr_render_de
         long long cap = grow(needed + needed / 8 + 1);
         std::vector<long long> ends;  // chunk ends, ascending
         if (!b.empty()) {
-            const double budget = margin * (double)cap / scale;
-            double acc = 0;
-            for (int i = 0; i < (int)b.size(); i++) {
-                if (acc > 0 && acc + (double)b[i] > budget) {
-                    ends.push_back((long long)i * P / (long long)b.size());
-                    acc = 0;
-                }
-                acc += (double)b[i];
-            }
+            plan_ends(b, 0, P, margin * (double)cap, scale, ends);
         } else if (needed > cap) {
             const long long chunk = std::max(1ll, (long long)((double)P * cap / needed * 0.9));
             for (long long e = chunk; e < P; e += chunk) ends.push_back(e);
@@ -770,9 +781,17 @@ std::pair<long long, long long> run_backward(dr_scene *scene, const dr_render_de
                 if (p1 - p0 == 1)
                     throw DrError(DR_ERR_OUT_OF_MEMORY, "one shading point samples " + std::to_string(needed) +
                                                             " edges; the item queue holds " + std::to_string(cap));
-                // the chunk cut to what fits; its rest becomes the next chunk
-                ends.insert(ends.begin() + ci,
-                            p0 + std::max(1ll, (long long)((double)(p1 - p0) * cap / needed * 0.9)));
+                // the pass counted every point of the chunk: the chunk is cut
+                // exactly from those counts, and its rest follows in pieces
+                std::vector<long long> cuts;
+                if (ws.pt_items && stats) {
+                    std::vector<unsigned long long> cb;
+                    read_buckets_at(p0, p1 - p0, cb);
+                    plan_ends(cb, p0, p1 - p0, 0.97 * (double)cap, 1.0, cuts);
+                }
+                if (cuts.empty() || cuts.back() >= p1)
+                    cuts.assign(1, p0 + std::max(1ll, (long long)((double)(p1 - p0) * cap / needed * 0.9)));
+                ends.insert(ends.begin() + ci, cuts.begin(), cuts.end());
                 continue;
             }
             back();
@@ -980,12 +999,14 @@ void backward_on_queues(dr_scene *scene, const dr_render_desc *rd, const DevScen
         q.item_dp.reserve(sizeof(float) * 3 * cap_items);
         q.survivors.reserve(sizeof(float4) * 2 * cap_items);
         q.hits.reserve(sizeof(int4) * cap_items);
+        q.side_rad.reserve(sizeof(float4) * 2 * cap_items);
         q.cap_items = cap_items;
         ws.items = q.items.as<int4>();
         ws.item_w = q.item_w.as<float>();
         ws.item_dp = q.item_dp.as<float>();
         ws.survivors = q.survivors.as<float4>();
         ws.hits = q.hits.as<int4>();
+        ws.side_rad = q.side_rad.as<float4>();
         ws.cap_items = cap_items;
     };
     auto bind_points = [&]() {
@@ -1003,7 +1024,9 @@ void backward_on_queues(dr_scene *scene, const dr_render_desc *rd, const DevScen
     if (view ? view->split_traversal : call_scene(scene, rd).split_traversal) {
         long long cap_tasks = std::min(kMaxTasks, std::max(1ll << 16, kTasksPerPoint * cap_points));
         q.tasks.reserve(sizeof(EdgeTask) * cap_tasks);
+        q.tasks2.reserve(sizeof(EdgeTask) * cap_tasks);
         ws.tasks = q.tasks.as<EdgeTask>();
+        ws.tasks2 = q.tasks2.as<EdgeTask>();
         ws.cap_tasks = cap_tasks;
     }
     // the item queue grows to what the traversal reported, up to its limit

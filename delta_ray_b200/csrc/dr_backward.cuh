@@ -584,18 +584,38 @@ DEV bool item_line(const DevScene &s, const PointRecord &pt, int tree, int ei, u
 
 // The item's shading from its line sample; as eval_item.  `hits` (may be
 // null): the closest hits of the sample's two rays, which edge_rays kept.
-template <bool EXT = true, bool MAYBE_GI = true, class G>
+// The two sides' radiance of a kept edge sample (edge_side_radiance), with
+// the item's own light sample and random stream as item_shade draws them.
+DEV bool item_side_radiance(const DevScene &s, const PointRecord &pt, int tree, int ei, int j, int B,
+                            uint64_t seed, const EdgeLine &el, const EdgeHits &hits, float3 &shr, float3 &shl) {
+    Rng irng;
+    irng.init(seed, kStreamEdgeItem, pt.sid, ((uint32_t)pt.bounce << 28) | (uint32_t)j);
+    LightSample els = draw_light(irng);
+    const DevEdge &edge = tree ? s.nrm_edges[ei] : s.sil_edges[ei];
+    return edge_side_radiance(s, el, edge, els, irng, B - pt.bounce - 1, pt.wi, pt.tri, pt.surface(), hits, shr,
+                              shl);
+}
+
+// PRE: the sides' radiance `rad` comes from item_side_radiance (see
+// edge_shade_hits).
+template <bool EXT = true, bool MAYBE_GI = true, class G, bool PRE = false>
 DEV float3 item_shade(const DevScene &s, const PointRecord &pt, int tree, int ei, int j, float w, int spp, int B,
-                      uint64_t seed, G &g, float *mag, const EdgeLine &el, const EdgeHits *hits = nullptr) {
+                      uint64_t seed, G &g, float *mag, const EdgeLine &el, const EdgeHits *hits = nullptr,
+                      const float3 *rad = nullptr) {
     Rng irng;
     irng.init(seed, kStreamEdgeItem, pt.sid, ((uint32_t)pt.bounce << 28) | (uint32_t)j);
     LightSample els = draw_light(irng);
     const DevEdge &edge = tree ? s.nrm_edges[ei] : s.sil_edges[ei];
     float3 weight = f3(1.f) * ((1.f / spp) * w);
-    EdgeResult er = hits ? edge_shade_hits<MAYBE_GI>(s, el, edge, els, irng, B - pt.bounce - 1, pt.wi, pt.tri,
-                                                     pt.surface(), weight, pt.d_color, B == 1, *hits)
-                         : edge_shade_sample<MAYBE_GI>(s, el, edge, els, irng, B - pt.bounce - 1, pt.wi, pt.tri,
-                                                       pt.surface(), weight, pt.d_color, B == 1);
+    EdgeResult er;
+    if constexpr (PRE)
+        er = edge_shade_hits<MAYBE_GI, true>(s, el, edge, els, irng, B - pt.bounce - 1, pt.wi, pt.tri, pt.surface(),
+                                             weight, pt.d_color, B == 1, *hits, rad);
+    else
+        er = hits ? edge_shade_hits<MAYBE_GI>(s, el, edge, els, irng, B - pt.bounce - 1, pt.wi, pt.tri, pt.surface(),
+                                              weight, pt.d_color, B == 1, *hits)
+                  : edge_shade_sample<MAYBE_GI>(s, el, edge, els, irng, B - pt.bounce - 1, pt.wi, pt.tri,
+                                                pt.surface(), weight, pt.d_color, B == 1);
     if (EXT && mag) *mag = abs_sum(er.dv0) + abs_sum(er.dv1);
     if (!is_zero(er.dv0) || !is_zero(er.dv1)) {
         const DevShape &sh = s.shapes[edge.shape];

@@ -17,7 +17,7 @@ namespace cg = cooperative_groups;
 #define DR_TASKS_BLOCKS 6
 #endif
 #ifndef DR_CONNECT_BLOCKS
-#define DR_CONNECT_BLOCKS 4
+#define DR_CONNECT_BLOCKS 8
 #endif
 
 #define DR_ITEM_BUF 24
@@ -119,6 +119,8 @@ __global__ void __launch_bounds__(128, 6) k_edge_traverse(DevScene s, uint64_t s
 // walks them itself).  The node-keyed draws make the sampled edges the same
 // as those of the one-pass walk.
 #define DR_TASK_CUT 8
+// launches of the second stage per chunk (see k_edge_tasks)
+#define DR_TASK_ROUNDS 3
 #define DR_TASK_BUF 8
 template <bool PROP>
 __global__ void __launch_bounds__(128, 4) k_edge_expand(DevScene s, uint64_t seed, BackwardWorkspace ws) {
@@ -180,9 +182,17 @@ __device__ __forceinline__ long long next_task(unsigned long long *counter) {
     return (long long)(g.shfl(first, 0) + g.thread_rank());
 }
 
-template <bool PROP>
-__global__ void __launch_bounds__(128, DR_TASKS_BLOCKS) k_edge_tasks(DevScene s, uint64_t seed, BackwardWorkspace ws) {
-    const long long n = (long long)min(ws.counters->tasks, (unsigned long long)ws.cap_tasks);
+// Rounds: the subtrees come from `in` (*in_n of them); with HAND, a walk
+// that has taken 64 steps with two or more subtrees pending hands the
+// shallowest one (the largest) to `hand_q` (*hand_n) for the next round, so that
+// no lane walks a long subtree alone at the end of the launch.  The last
+// round hands nothing on.
+#define DR_HAND_STEPS 64
+template <bool PROP, bool HAND>
+__global__ void __launch_bounds__(128, DR_TASKS_BLOCKS) k_edge_tasks(DevScene s, uint64_t seed, BackwardWorkspace ws,
+                                                                   const EdgeTask *in, const unsigned long long *in_n,
+                                                                   EdgeTask *hand_q, unsigned long long *hand_n) {
+    const long long n = (long long)min(*in_n, (unsigned long long)ws.cap_tasks);
     ItemWriter out(ws);
     int visits = 0, point = 0, cnt = 0;
     bool ok = true;
@@ -194,20 +204,27 @@ __global__ void __launch_bounds__(128, DR_TASKS_BLOCKS) k_edge_tasks(DevScene s,
         }
     };
     NoDefer nd;
+    int steps = 0;
     while (true) {
         if (!w.busy()) {
             if (cnt > 0 && ws.pt_items) atomicAdd(ws.pt_items + point, cnt);
             cnt = 0;
             const long long k = next_task(&ws.counters->task_next);
             if (k >= n) break;
-            const EdgeTask t = ws.tasks[k];
+            const EdgeTask t = in[k];
             PointRecord pt;
             pt.load(ws.pt + (size_t)t.point * DR_PT_WORDS);
             point = t.point;
             start_point_task<PROP>(w, s, pt, seed, t, point_proposal(ws, t.point));
+            steps = 0;
         }
         w.step(emit, nd, &visits);
         ok &= w.ok;
+        if (HAND && ++steps >= DR_HAND_STEPS && w.n >= 2) {
+            steps = 0;
+            const unsigned long long slot = atomicAdd(hand_n, 1ull);
+            if (slot < (unsigned long long)ws.cap_tasks) hand_q[slot] = w.take_bottom(point);
+        }
     }
     if (!ok) set_status(&ws.counters->status, DR_STATUS_STACK_OVERFLOW);
     out.flush_warp();
@@ -425,7 +442,34 @@ __global__ void __launch_bounds__(128, 8) k_edge_line_rays(DevScene s, uint64_t 
     }
 }
 
-template <bool EXT, bool GI>
+// More than one bounce: the two sides' radiance of every kept sample (the
+// multi-bounce shading) in a kernel of its own, [2 h] and [2 h + 1] of
+// ws.side_rad; k_edge_shade then runs without the path-tracing code, whose
+// size made the fused kernel wait on instruction fetches.
+__global__ void __launch_bounds__(128, 4) k_edge_radiance(DevScene s, int B, uint64_t seed, BackwardWorkspace ws) {
+    long long n = (long long)min(ws.counters->cands, (unsigned long long)ws.cap_items);
+    for (long long h = (long long)blockIdx.x * blockDim.x + threadIdx.x; h < n; h += (long long)gridDim.x * blockDim.x) {
+        int4 hr = ws.hits[h];
+        if (hr.w == 0) continue;
+        EdgeHits eh;
+        eh.r = hr.y;
+        eh.l = hr.z;
+        float4 a = ws.survivors[2 * (long long)hr.x];
+        long long i = __float_as_int(a.x);
+        EdgeLine el;
+        el.sample_p = f3(a.y, a.z, a.w);
+        int4 it = ws.items[i];
+        PointRecord pt;
+        pt.load(ws.pt + (size_t)it.x * DR_PT_WORDS);
+        float3 shr, shl;
+        item_side_radiance(s, pt, it.y >> 30, it.y & ((1 << 30) - 1), it.z, B, seed, el, eh, shr, shl);
+        ws.side_rad[2 * h] = make_float4(shr.x, shr.y, shr.z, shl.x);
+        ws.side_rad[2 * h + 1] = make_float4(shl.y, shl.z, 0.f, 0.f);
+    }
+}
+
+// PRE: the sides' radiance comes from k_edge_radiance.
+template <bool EXT, bool GI, bool PRE>
 __global__ void __launch_bounds__(128, 4) k_edge_shade(DevScene s, int W, int H, int spp, int B, uint64_t seed,
                                                     int dp_mode, float *grad, BackwardWorkspace ws, GradCacheCfg cfg) {
     extern __shared__ float sm[];
@@ -449,7 +493,15 @@ __global__ void __launch_bounds__(128, 4) k_edge_shade(DevScene s, int W, int H,
         pt.load(ws.pt + (size_t)it.x * DR_PT_WORDS);
         int tree = it.y >> 30, ei = it.y & ((1 << 30) - 1);
         float mag = 0.f;
-        float3 dp = item_shade<EXT, GI>(s, pt, tree, ei, it.z, ws.item_w[i], spp, B, seed, bg, &mag, el, &eh);
+        float3 dp;
+        if constexpr (PRE) {
+            const float4 r0 = ws.side_rad[2 * h], r1 = ws.side_rad[2 * h + 1];
+            const float3 rad[2] = {f3(r0.x, r0.y, r0.z), f3(r0.w, r1.x, r1.y)};
+            dp = item_shade<EXT, GI, BlockGrad, true>(s, pt, tree, ei, it.z, ws.item_w[i], spp, B, seed, bg, &mag, el,
+                                                     &eh, rad);
+        } else {
+            dp = item_shade<EXT, GI>(s, pt, tree, ei, it.z, ws.item_w[i], spp, B, seed, bg, &mag, el, &eh);
+        }
         finish_item<EXT>(s, ws, it, i, pt, dp, mag, W, H, spp, seed, dp_mode, bg);
     }
     block_grad_flush(bg);
@@ -475,6 +527,17 @@ __global__ void __launch_bounds__(128, 8) k_primary_grad(DevScene s, int W, int 
     for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < n; k += (long long)gridDim.x * blockDim.x)
         primary_grad_item(s, i0 + k, W, H, spp, seed, d_image, in[k], bg);
     block_grad_flush(bg);
+}
+
+__global__ void k_add_count(unsigned long long *dst, const unsigned long long *src, unsigned long long cap) {
+    *dst += *src < cap ? *src : cap;
+}
+
+// *dst += min(*src, cap) on the device (the entries a queue received)
+cudaError_t dr_launch_accumulate_count(unsigned long long *dst, const unsigned long long *src, long long cap,
+                                       cudaStream_t st) {
+    k_add_count<<<1, 1, 0, st>>>(dst, src, (unsigned long long)cap);
+    return cudaGetLastError();
 }
 
 __global__ void k_edge_records(DevScene s, const DevEdge *edges, int n, EdgeRec *out) {
@@ -518,6 +581,7 @@ cudaError_t dr_launch_edge_traverse(const DevScene &s, uint64_t seed, const Back
     const bool prop = ws.proposal_q != nullptr;
     if (ws.tasks && s.split_traversal) {
         cudaError_t e = cudaMemsetAsync(&ws.counters->tasks, 0, sizeof(unsigned long long), st);
+        if (e == cudaSuccess) e = cudaMemsetAsync(&ws.counters->handed_total, 0, sizeof(unsigned long long), st);
         if (e != cudaSuccess) return e;
         if (prop) k_edge_expand<true><<<stage_grid(num_sms), 128, 0, st>>>(s, seed, ws);
         else k_edge_expand<false><<<stage_grid(num_sms), 128, 0, st>>>(s, seed, ws);
@@ -526,12 +590,32 @@ cudaError_t dr_launch_edge_traverse(const DevScene &s, uint64_t seed, const Back
         e = cudaMemcpyAsync(&ws.counters->items_expand, &ws.counters->items, sizeof(unsigned long long),
                             cudaMemcpyDeviceToDevice, st);
         if (e != cudaSuccess) return e;
-        e = cudaMemsetAsync(&ws.counters->task_next, 0, sizeof(unsigned long long), st);
-        if (e != cudaSuccess) return e;
-        if (prop) k_edge_tasks<true><<<stage_grid(num_sms), 128, 0, st>>>(s, seed, ws);
-        else k_edge_tasks<false><<<stage_grid(num_sms), 128, 0, st>>>(s, seed, ws);
-        timer->mark(st, "k_edge_tasks");
-        *launches += 2;
+        // the subtrees in rounds: the first stage's, then those handed on
+        // (ping-pong between the two queues); one round without a second queue
+        const int rounds = ws.tasks2 ? DR_TASK_ROUNDS : 1;
+        const EdgeTask *in = ws.tasks;
+        const unsigned long long *in_n = &ws.counters->tasks;
+        for (int r = 0; r < rounds; r++) {
+            EdgeTask *out = (r & 1) ? ws.tasks : ws.tasks2;
+            unsigned long long *out_n = &ws.counters->handed[r & 1];
+            e = cudaMemsetAsync(&ws.counters->task_next, 0, sizeof(unsigned long long), st);
+            if (e == cudaSuccess) e = cudaMemsetAsync(out_n, 0, sizeof(unsigned long long), st);
+            if (e != cudaSuccess) return e;
+            const bool hand = r + 1 < rounds;
+            auto k = prop ? (hand ? k_edge_tasks<true, true> : k_edge_tasks<true, false>)
+                          : (hand ? k_edge_tasks<false, true> : k_edge_tasks<false, false>);
+            k<<<stage_grid(num_sms), 128, 0, st>>>(s, seed, ws, in, in_n, out, out_n);
+            timer->mark(st, "k_edge_tasks");
+            *launches += 1;
+            if (hand) {
+                e = dr_launch_accumulate_count(&ws.counters->handed_total, out_n, ws.cap_tasks, st);
+                if (e != cudaSuccess) return e;
+                *launches += 1;
+            }
+            in = out;
+            in_n = out_n;
+        }
+        *launches += 1;
         return cudaGetLastError();
     }
     if (prop) k_edge_traverse<true><<<stage_grid(num_sms), 128, 0, st>>>(s, seed, ws);
@@ -569,8 +653,16 @@ cudaError_t dr_launch_edge_eval(const DevScene &s, int W, int H, int spp, int B,
         timer->mark(st, "k_edge_pairs");
         *launches += 1;
     }
-    auto shade = ext ? (B > 1 ? k_edge_shade<true, true> : k_edge_shade<true, false>)
-                     : (B > 1 ? k_edge_shade<false, true> : k_edge_shade<false, false>);
+    const bool pre = B > 1 && ws.side_rad != nullptr;
+    if (pre) {
+        k_edge_radiance<<<grid, 128, 0, st>>>(s, B, seed, ws);
+        timer->mark(st, "k_edge_radiance");
+        *launches += 1;
+    }
+    auto shade = ext ? (B > 1 ? (pre ? k_edge_shade<true, true, true> : k_edge_shade<true, true, false>)
+                              : k_edge_shade<true, false, false>)
+                     : (B > 1 ? (pre ? k_edge_shade<false, true, true> : k_edge_shade<false, true, false>)
+                              : k_edge_shade<false, false, false>);
     shade<<<grid, 128, smem, st>>>(s, W, H, spp, B, seed, dp_mode, grad, ws, cfg);
     timer->mark(st, "k_edge_shade");
     *launches += 3;

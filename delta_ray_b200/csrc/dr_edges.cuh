@@ -455,6 +455,24 @@ struct EdgeWalk {
     }
     DEV bool busy() const { return n > 0; }
 
+    // Takes the shallowest pending subtree (the bottom of the stack, the
+    // largest) off the walk, as a task of point `point` for another lane.
+    // Only walks without a depth cut (CUT == 0) hand subtrees on.
+    DEV EdgeTask take_bottom(int point) {
+        const Item b = st[0];
+        EdgeTask t;
+        t.point = point;
+        t.code = (b.node & DR_NODE_MASK) | (tree << 29) | ((cone_mode ? 0 : 1) << 30);
+        t.bb = b.bb;
+        t.cpmf = b.cpmf;
+        t.apmf = b.apmf;
+        t.lpmf = 0.f;
+        if constexpr (PROP) t.lpmf = b.lpmf;
+        for (int i = 1; i < n; i++) st[i - 1] = st[i];
+        n--;
+        return t;
+    }
+
     template <class Emit> DEV void leaf(const Item &it, const DevEdgeNode &node, Emit &emit) {
         const bool CONE = cone_mode;
         const float3 p = bc.p;
@@ -977,10 +995,43 @@ DEV bool edge_rays(const DevScene &s, const EdgeLine &el, const DevEdge &edge, i
 // (with more bounces) the radiance seen on each side, the BSDF toward the
 // edge, and the Jacobians of the sample w.r.t. the shading point and the
 // edge's end points.
-template <bool MAYBE_GI = true>
+// The radiance each side of an edge sample receives beyond its closest hit
+// (more bounces than one), divided by the squared distance and times the
+// cosine at the hit, as edge_shade_hits uses it; false (and zeros) when the
+// BSDF toward the edge is negligible, where edge_shade_hits ends the sample.
+DEV bool edge_side_radiance(const DevScene &s, const EdgeLine &el_, const DevEdge &edge, const LightSample &ls,
+                            const Rng &rng, int nbounces, float3 wi, int stri, const SurfacePoint &sp,
+                            const EdgeHits &hits, float3 &shr, float3 &shl) {
+    shr = shl = f3(0.f);
+    float3 v0 = edge_v0(s, edge), v1 = edge_v1(s, edge);
+    float3 sdir, rdir, ldir;
+    edge_side_dirs(el_, v0, v1, sp.p, sdir, rdir, ldir);
+    if (sum(bsdf(s, material_of_tri(s, stri), sp, wi, sdir)) < 1e-6f) return false;
+#pragma unroll 1
+    for (int k = 0; k < 2; k++) {
+        int tri = k == 0 ? hits.r : hits.l;
+        SurfacePoint pp;
+        if (tri >= 0) pp = intersect_tri(load_tri(s, tri), sp.p, k == 0 ? rdir : ldir);
+        float3 sh = shade(s, -sdir, tri, pp, ls, rng, nbounces, false);
+        if (tri >= 0) {
+            float3 dir = pp.p - sp.p;
+            float d2 = length_sq(dir);
+            if (d2 > 0.f) sh = sh / fmaxf(d2, 1e-2f) * fabsf(dot(normalize(dir), pp.ng));
+            else sh = f3(0.f);
+        }
+        if (k == 0) shr = sh;
+        else shl = sh;
+    }
+    return true;
+}
+
+// PRE: the two sides' radiance comes from edge_side_radiance, computed by an
+// earlier kernel (rad[0] right, rad[1] left), and shade() is not compiled in.
+template <bool MAYBE_GI = true, bool PRE = false>
 DEV EdgeResult edge_shade_hits(const DevScene &s, const EdgeLine &el_, const DevEdge &edge, const LightSample &ls,
                                const Rng &rng, int nbounces, float3 wi, int stri, const SurfacePoint &sp,
-                               float3 weight, float3 d_color, bool direct_only, const EdgeHits &hits) {
+                               float3 weight, float3 d_color, bool direct_only, const EdgeHits &hits,
+                               const float3 *rad = nullptr) {
     EdgeResult none;
     none.dp = none.dv0 = none.dv1 = f3(0.f);
     const float3 sample_p = el_.sample_p;
@@ -994,7 +1045,12 @@ DEV EdgeResult edge_shade_hits(const DevScene &s, const EdgeLine &el_, const Dev
     float3 eb = bsdf(s, mi, sp, wi, sdir);
     if (sum(eb) < 1e-6f) return none;
     float3 shr = f3(0.f), shl = f3(0.f);
-    if (MAYBE_GI && !direct_only) {
+    if (PRE) {
+        if (MAYBE_GI && !direct_only) {
+            shr = rad[0];
+            shl = rad[1];
+        }
+    } else if (MAYBE_GI && !direct_only) {
 #pragma unroll 1
         for (int k = 0; k < 2; k++) {
             int tri = k == 0 ? hits.r : hits.l;

@@ -97,6 +97,9 @@ struct BackwardCounters {
     // (records in `hits`, flagged by k_edge_pairs; `hits` counts the flagged
     // ones), candidates fetched by k_edge_pairs
     unsigned long long ray_next, cands, pair_next;
+    // subtrees handed on between rounds of k_edge_tasks (two queues, used in
+    // turn) and their total
+    unsigned long long handed[2], handed_total;
 };
 
 struct BackwardWorkspace {
@@ -125,10 +128,16 @@ struct BackwardWorkspace {
     // [cap_items] per candidate of the ray stage (survivor index, closest-hit
     // triangle of the right and the left ray, kept ? 1 : 0)
     int4 *hits;
+    // [cap_items][2] the two sides' radiance per candidate (k_edge_radiance;
+    // null: k_edge_shade shades the sides itself)
+    float4 *side_rad;
     // subtrees of large trees' traversals handed on to a second stage
     // (null: one thread walks each point whole)
     EdgeTask *tasks;
     long long cap_tasks;
+    // [cap_tasks] the second queue of the rounds of k_edge_tasks (null: one
+    // round, no subtree handed on)
+    EdgeTask *tasks2;
     // [cap_points] edges each point's traversal sampled, written by the point
     // walk and added to by its subtrees (null: not kept); the streamed edge
     // stage plans its chunks from them

@@ -323,8 +323,8 @@ DR_API dr_status dr_scene_edge_data(const dr_scene *scene, int what, void *out_h
 /* Tooling: work counts of the last backward call (the inputs of a byte model
  * of its kernels; no counterpart in the reference): counts[0] shading points,
  * [1] sampled edges, [2] line samples kept for their rays, [3] samples kept
- * for shading, [4] subtrees handed from the first traversal stage to the
- * second, [5] edges sampled by the first stage (all, when the traversal runs
+ * for shading, [4] subtrees walked by the second traversal stage (handed
+ * on by the first stage or between the second stage's rounds), [5] edges sampled by the first stage (all, when the traversal runs
  * in one stage), [6] edge-tree nodes visited by the point walks, [7] nodes
  * visited by the subtree walks, [8] line samples whose connectivity test
  * passed (candidates of the ray stage).  Up to n of them are written. */
