@@ -552,7 +552,7 @@ void check_render_desc(const dr_scene *sc, const dr_render_desc *rd) {
     if (rd->flags &
         ~(int)(DR_FLAG_FULL_PIXEL_JITTER | DR_FLAG_DETACHED_PDF | DR_FLAG_EDGE_LOBE_MIS | DR_FLAG_LEARNED_PROPOSAL))
         throw DrError(DR_ERR_INVALID_ARGUMENT, "unknown render flags");
-    if (rd->max_bounces > 64) throw DrError(DR_ERR_NOT_SUPPORTED, "max_bounces above 64");
+    if (rd->max_bounces > 256) throw DrError(DR_ERR_NOT_SUPPORTED, "max_bounces above 256");
     if (sc->ds.num_lights == 0) throw DrError(DR_ERR_INVALID_ARGUMENT, "scene has no lights");
 }
 

@@ -141,8 +141,14 @@ cudaError_t dr_launch_backward_front(const DevScene &s, int W, int H, int spp, i
         if (e != cudaSuccess) return e;
     }
     // variants: specular chains or not, direct lighting (B = 1) or not
-    auto kernel = s.specular_chains ? (B == 1 ? k_backward_paths<true, 1> : k_backward_paths<true, DR_MAX_BOUNCES>)
-                                    : (B == 1 ? k_backward_paths<false, 1> : k_backward_paths<false, DR_MAX_BOUNCES>);
+    // deeper than the records' 64 bounces: the checkpointed form, segments of
+    // 16 bounces traced again for the suffix sweep and the replay
+    auto kernel = s.specular_chains
+                      ? (B == 1 ? k_backward_paths<true, 1>
+                                : (B > DR_MAX_BOUNCES ? k_backward_paths<true, -16> : k_backward_paths<true, DR_MAX_BOUNCES>))
+                      : (B == 1 ? k_backward_paths<false, 1>
+                                : (B > DR_MAX_BOUNCES ? k_backward_paths<false, -16>
+                                                      : k_backward_paths<false, DR_MAX_BOUNCES>));
     kernel<<<blocks_for(threads, bs), bs, smem, st>>>(s, W, H, spp, B, seed, lanes_log2, d_image, grad, img, ws, cfg);
     timer->mark(st, "k_backward_paths");
     *launches += 1;

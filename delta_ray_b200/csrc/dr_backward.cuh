@@ -27,6 +27,8 @@
 #include "dr_edges.cuh"
 
 #define DR_MAX_BOUNCES 64
+// the checkpointed form (BMAX < 0): up to DR_CKPT_SEGS segments of -BMAX bounces
+#define DR_CKPT_SEGS 16
 #define DR_PT_WORDS 24
 
 // Secondary shading point record (packed floats; ints stored as bits).
@@ -252,6 +254,87 @@ DEV void sweep_links(const DevScene &s, SpecLink *links, int n, VertexGrad &v0, 
 // each vertex's local adjoints, then a reverse sweep over the specular links
 // pushes vertex k + 1's adjoints through its intersection and the sampled
 // direction to vertex k, the roughness and the hit triangle.
+// The trace's state before a bounce: where a trace resumes (a checkpoint).
+struct PathState {
+    Rng r;           // the pixel sample's stream at this bounce
+    int ctri;        // the current vertex's triangle
+    SurfacePoint csp;
+    float3 cwi, thr;  // incoming direction; throughput so far (with roulette)
+    bool all_spec;    // every sample so far was specular
+};
+
+// Bounce b of the trace (pass 1): the record (next hit, radiance X added at
+// this vertex, throughput factor r, roulette probability q), the state moved
+// on to the next vertex.  color (may be null) receives the bounce's radiance
+// in the trace's own order of additions; push (may be null) the vertex
+// reached when it is a secondary-edge shading point.  False when the path
+// ends at this bounce (the record is then the last, possibly with a hit).
+template <bool kChains, class Push>
+DEV bool trace_bounce(const DevScene &s, const LightSample &ls, float3 wi, int b, int B, PathState &ps,
+                      BounceRecord &rec, float3 *color, bool want_grad, float3 d_color, uint64_t sid, int light_pick,
+                      Push *push) {
+    SecondarySample ss = draw_secondary(ps.r);
+    float3 N = nee(s, ls, wi, ps.ctri, ps.csp);
+    if (color) *color += ps.thr * N;
+    rec.next_tri = -1;
+    rec.X = N;
+    rec.r = f3(0.f);
+    rec.q = 1.f;
+    bool spec;
+    float3 dir = sampled_direction(s, ss.bsdf, ps.cwi, ps.ctri, ps.csp, spec);
+    if (abs_sum(dir) <= 0.f) return false;
+    Hit bh = trace_closest(s, ps.csp.p, dir, 1e-3f);
+    if (bh.tri < 0) return false;
+    // a specular sample's hit keeps the reference's AD arithmetic (its
+    // position decides which edges a later shading point sees)
+    SurfacePoint nsp = intersect_tri(load_tri(s, bh.tri), ps.csp.p, dir, nullptr, spec);
+    float3 wo = normalize(nsp.p - ps.csp.p);
+    int mi = material_of_tri(s, ps.ctri);
+    float pdf = bsdf_pdf(s, mi, ps.csp, ps.cwi, wo);
+    if (pdf <= 0.f) return false;
+    float3 f = bsdf(s, mi, ps.csp, ps.cwi, wo);
+    if (sum(f) <= 0.f) return false;
+    rec.next_tri = bh.tri;
+    int nli = light_of_tri(s, bh.tri);
+    if (nli >= 0 && dot(nsp.f.n, -wo) > 0.f) {
+        float lpdf = light_pdf(s, bh.tri) * length_sq(nsp.p - ps.csp.p) / fabsf(dot(wo, nsp.ng));
+        float mis = sq(pdf) / (sq(lpdf) + sq(pdf));
+        float3 em = f * light_intensity(s, nli) * (mis / pdf);
+        if (color) *color += ps.thr * em;
+        rec.X += em;
+    }
+    float3 rb = f / pdf;
+    ps.thr = ps.thr * rb;
+    if (b >= 5) {
+        float q = fminf(max3(ps.thr), 0.95f);
+        if (ss.rr >= q) return false;
+        ps.thr = ps.thr / q;
+        rb = rb / q;
+        rec.q = q;
+    }
+    rec.r = rb;
+    ps.all_spec = ps.all_spec && spec;
+    ps.cwi = -wo;
+    ps.ctri = bh.tri;
+    ps.csp = nsp;
+    // vertex b + 1 is a secondary-edge shading point while every sample was specular
+    if (kChains && push && want_grad && ps.all_spec && b + 1 < B && b + 1 <= DR_MAX_LINKS) {
+        PointRecord pr;
+        pr.p = nsp.p;
+        pr.n = nsp.f.n;
+        pr.ng = nsp.ng;
+        pr.uv = nsp.uv;
+        pr.wi = ps.cwi;
+        pr.d_color = d_color * ps.thr;  // the edge weight carries the path throughput
+        pr.tri = bh.tri;
+        pr.sid = sid;
+        pr.light = light_pick;
+        pr.bounce = b + 1;
+        (*push)(pr);
+    }
+    return true;
+}
+
 // kChains = false compiles the variant for scenes without specular samples
 // (no chain bookkeeping); both give the same result on such scenes.
 // BMAX bounds max_bounces at compile time (1 for direct lighting, whose
@@ -276,19 +359,19 @@ DEV float3 backward_pixel_sample(const DevScene &s, int x, int y, int W, int H, 
     const float3 wi = -ray.d;
     const int light_pick =
         sample_discrete(s.light_sel_cdf, s.light_sel_func, s.light_sel_func_int, s.num_lights, ls.sel, nullptr);
-    // ---- pass 1: trace, keep the bounces ----
-    if (B > BMAX) B = BMAX;
-    BounceRecord rec[BMAX];
+    // ---- pass 1: trace, keep the bounces (or checkpoints) ----
+    constexpr int CK = BMAX < 0 ? -BMAX : 0;  // segment length of the checkpointed form
+    constexpr int NREC = CK ? CK : BMAX;
+    constexpr int NCK = CK ? DR_CKPT_SEGS : 1;
+    if (B > (CK ? CK * NCK : BMAX)) B = CK ? CK * NCK : BMAX;
+    BounceRecord rec[NREC];
+    PathState ck[NCK];
     int nb = 0;
     float3 color = f3(0.f);
     int li0 = light_of_tri(s, h0.tri);
     bool prim_emit = li0 >= 0 && dot(sp0.f.n, wi) > 0.f;
     if (prim_emit) color += light_intensity(s, li0);
-    float3 thr = f3(1.f), cwi = wi;
-    int ctri = h0.tri;
-    SurfacePoint csp = sp0;
     bool want_grad = !is_zero(d_color);
-    bool all_spec = true;  // every sample so far was specular
     if (want_grad && B >= 1) {
         PointRecord pr;
         pr.p = sp0.p;
@@ -303,76 +386,51 @@ DEV float3 backward_pixel_sample(const DevScene &s, int x, int y, int W, int H, 
         pr.bounce = 0;
         push_point(pr);
     }
+    PathState ps;
+    ps.r = r;
+    ps.ctri = h0.tri;
+    ps.csp = sp0;
+    ps.cwi = wi;
+    ps.thr = f3(1.f);
+    ps.all_spec = true;
     for (int b = 0; b < B; b++) {
-        SecondarySample ss = draw_secondary(r);
-        float3 N = nee(s, ls, wi, ctri, csp);
-        color += thr * N;
+        if (CK && b % (CK ? CK : 1) == 0) ck[b / (CK ? CK : 1)] = ps;
         nb = b + 1;
-        rec[b].next_tri = -1;
-        rec[b].X = N;
-        rec[b].r = f3(0.f);
-        rec[b].q = 1.f;
-        bool spec;
-        float3 dir = sampled_direction(s, ss.bsdf, cwi, ctri, csp, spec);
-        if (abs_sum(dir) <= 0.f) break;
-        Hit bh = trace_closest(s, csp.p, dir, 1e-3f);
-        if (bh.tri < 0) break;
-        // a specular sample's hit keeps the reference's AD arithmetic (its
-        // position decides which edges a later shading point sees)
-        SurfacePoint nsp = intersect_tri(load_tri(s, bh.tri), csp.p, dir, nullptr, spec);
-        float3 wo = normalize(nsp.p - csp.p);
-        int mi = material_of_tri(s, ctri);
-        float pdf = bsdf_pdf(s, mi, csp, cwi, wo);
-        if (pdf <= 0.f) break;
-        float3 f = bsdf(s, mi, csp, cwi, wo);
-        if (sum(f) <= 0.f) break;
-        rec[b].next_tri = bh.tri;
-        int nli = light_of_tri(s, bh.tri);
-        if (nli >= 0 && dot(nsp.f.n, -wo) > 0.f) {
-            float lpdf = light_pdf(s, bh.tri) * length_sq(nsp.p - csp.p) / fabsf(dot(wo, nsp.ng));
-            float mis = sq(pdf) / (sq(lpdf) + sq(pdf));
-            float3 em = f * light_intensity(s, nli) * (mis / pdf);
-            color += thr * em;
-            rec[b].X += em;
-        }
-        float3 rb = f / pdf;
-        thr = thr * rb;
-        if (b >= 5) {
-            float q = fminf(max3(thr), 0.95f);
-            if (ss.rr >= q) break;
-            thr = thr / q;
-            rb = rb / q;
-            rec[b].q = q;
-        }
-        rec[b].r = rb;
-        all_spec = all_spec && spec;
-        cwi = -wo;
-        ctri = bh.tri;
-        csp = nsp;
-        // vertex b + 1 is a secondary-edge shading point while every sample was specular
-        if (kChains && want_grad && all_spec && b + 1 < B && b + 1 <= DR_MAX_LINKS) {
-            PointRecord pr;
-            pr.p = nsp.p;
-            pr.n = nsp.f.n;
-            pr.ng = nsp.ng;
-            pr.uv = nsp.uv;
-            pr.wi = cwi;
-            pr.d_color = d_color * thr;  // the edge weight carries the path throughput
-            pr.tri = bh.tri;
-            pr.sid = sid;
-            pr.light = light_pick;
-            pr.bounce = b + 1;
-            push_point(pr);
-        }
+        if (!trace_bounce<kChains>(s, ls, wi, b, B, ps, rec[CK ? b % (CK ? CK : 1) : b], &color, want_grad, d_color,
+                                   sid, light_pick, &push_point))
+            break;
     }
     color = color * sw;
     if (!want_grad) return color;  // render_sample_fast: no derivatives, no edges
     // ---- suffix radiance S_{k+1}, stored in rec[k].X ----
-    float3 S = f3(0.f);
-    for (int k = nb - 1; k >= 0; k--) {
-        float3 Sk = rec[k].X + rec[k].r * S;
-        rec[k].X = S;  // now holds S_{k+1}
-        S = Sk;
+    // Checkpointed: a segment's records are traced again from its checkpoint
+    // (the same streams, so the same bits); the sweep keeps only the suffix at
+    // each segment's start, and pass 2 traces each segment once more.
+    float3 sseg[NCK + 1];
+    const int nseg = CK ? (nb + (CK ? CK : 1) - 1) / (CK ? CK : 1) : 0;
+    auto retrace = [&](int j) {  // rec[0, len) of segment j
+        PathState q = ck[j];
+        const int b0 = j * (CK ? CK : 1), len = nb - b0 < (CK ? CK : 1) ? nb - b0 : (CK ? CK : 1);
+        for (int i = 0; i < len; i++)
+            trace_bounce<kChains, Push>(s, ls, wi, b0 + i, B, q, rec[i], nullptr, want_grad, d_color, sid, light_pick,
+                                        nullptr);
+        return len;
+    };
+    if (CK) {
+        float3 S = f3(0.f);
+        sseg[nseg] = S;
+        for (int j = nseg - 1; j >= 0; j--) {
+            const int len = retrace(j);
+            for (int i = len - 1; i >= 0; i--) S = rec[i].X + rec[i].r * S;
+            sseg[j] = S;
+        }
+    } else {
+        float3 S = f3(0.f);
+        for (int k = nb - 1; k >= 0; k--) {
+            float3 Sk = rec[k].X + rec[k].r * S;
+            rec[k].X = S;  // now holds S_{k+1}
+            S = Sk;
+        }
     }
     // ---- pass 2: replay with adjoints ----
     const float3 dC = d_color * sw;
@@ -391,11 +449,20 @@ DEV float3 backward_pixel_sample(const DevScene &s, int x, int y, int W, int H, 
     bool vlive = true;         // the current vertex's geometry is differentiable
     bool wi_live = true;       // the current vertex's incoming direction is differentiable
     Rng rr = r_sec;
-    thr = f3(1.f);
-    cwi = wi;
-    ctri = h0.tri;
-    csp = sp0;
+    float3 thr = f3(1.f), cwi = wi;
+    int ctri = h0.tri;
+    SurfacePoint csp = sp0;
     for (int k = 0; k < nb; k++) {
+        if (CK && k % (CK ? CK : 1) == 0) {  // the segment's records, each X turned into S_{k+1}
+            const int j = k / (CK ? CK : 1), len = retrace(j);
+            float3 S = sseg[j + 1];
+            for (int i = len - 1; i >= 0; i--) {
+                float3 Si = rec[i].X + rec[i].r * S;
+                rec[i].X = S;
+                S = Si;
+            }
+        }
+        const BounceRecord &rk = rec[CK ? k % (CK ? CK : 1) : k];
         SecondarySample ss = draw_secondary(rr);
         float3 a = dC * thr;
         VertexGrad *vg = !vlive ? nullptr : (vlink < 0 ? &v0g : &links[vlink].vg);
@@ -412,7 +479,7 @@ DEV float3 backward_pixel_sample(const DevScene &s, int x, int y, int W, int H, 
                 vg->dp += dp;
             }
         }
-        int nt = rec[k].next_tri;
+        int nt = rk.next_tri;
         if (nt < 0) break;
         int mi = material_of_tri(s, ctri);
         SurfacePoint use = csp;
@@ -443,8 +510,8 @@ DEV float3 backward_pixel_sample(const DevScene &s, int x, int y, int W, int H, 
             d_pdf -= dot(a * f, I) * mis / (pdf * pdf);
         }
         // r_k = f / (pdf q): its adjoint is dC T_k S_{k+1}
-        float3 dr = a * rec[k].X;
-        float q = rec[k].q;
+        float3 dr = a * rk.X;
+        float q = rk.q;
         if (!is_zero(dr)) {
             d_f += dr * (1.f / (pdf * q));
             d_pdf -= dot(dr, f) / (pdf * pdf * q);
@@ -480,7 +547,7 @@ DEV float3 backward_pixel_sample(const DevScene &s, int x, int y, int W, int H, 
             L.dwo = L.wo_live ? gb.dwo : f3(0.f);
             next_link = nlinks++;
         }
-        thr = thr * rec[k].r;
+        thr = thr * rk.r;
         wi_live = wi_live && spec;
         vlive = next_link >= 0;
         vlink = next_link;
@@ -579,7 +646,7 @@ DEV bool item_line(const DevScene &s, const PointRecord &pt, int tree, int ei, u
     prng.init(seed, kStreamEdgePoint, pt.sid, (uint32_t)pt.bounce);
     EdgeSample es = draw_edge(prng);
     const DevEdge &edge = tree ? s.nrm_edges[ei] : s.sil_edges[ei];
-    return edge_line_sample<EXT>(s, es, edge, pt.wi, pt.tri, pt.surface(), el);
+    return edge_line_sample<EXT>(s, es, edge, pt.wi, pt.tri, pt.surface(), el, (tree ? s.nrm_rec : s.sil_rec) + ei);
 }
 
 // The item's shading from its line sample; as eval_item.  `hits` (may be

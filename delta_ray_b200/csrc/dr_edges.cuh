@@ -212,6 +212,25 @@ DEV BoundCtx bound_ctx(float3 wi, const SurfacePoint &sp, float dl, float sl, fl
     return c;
 }
 
+// Functions of the filters that decide a node test before its exact
+// evaluation: the silhouette filter's sine, cosine and reciprocal square root
+// (absolute errors below 1e-6 on its arguments) and the bound filter's log2
+// and exp2 (a few ulps).  The filters only ever decide with margins well above
+// those errors.
+#ifdef DR_HOST_BUILD
+HD float filt_sin(float x) { return std::sin(x); }
+HD float filt_cos(float x) { return std::cos(x); }
+HD float filt_rsqrt(float x) { return 1.f / std::sqrt(x); }
+HD float filt_log2(float x) { return std::log2(x); }
+HD float filt_exp2(float x) { return std::exp2(x); }
+#else
+DEV float filt_sin(float x) { return __sinf(x); }
+DEV float filt_cos(float x) { return __cosf(x); }
+DEV float filt_rsqrt(float x) { return rsqrtf(x); }
+DEV float filt_log2(float x) { return log2f(x); }
+DEV float filt_exp2(float x) { return exp2f(x); }
+#endif
+
 // The corners' products with a direction, per axis: corner i has the hi
 // coordinate on axis a iff bit a of i is set, and dot(d, corner_i - p) is
 // (x[i & 1] + y[(i >> 1) & 1]) + z[i >> 2], the bits of the per-corner dot.
@@ -230,7 +249,17 @@ DEV CornerDots corner_dots(float3 d, const float *q) {  // q: lo - p, hi - p per
     return c;
 }
 
-DEV_NOINLINE float bsdf_bound(const DevEdgeNode &node, const BoundCtx &c) {
+// fast_m (may be null) asks for the filtered form, used where only the
+// bound's side of 1 and of 0 matters: a Blinn-Phong lobe's pow(hdn, e) is then
+// taken as exp2f(e log2f(hdn)), within the relative bound m = (16 + |e log2
+// hdn|) 2^-22 of the reproducible pow (the float functions' few ulps, the
+// rounding of the operations after it, with a wide margin).  If the bound so
+// taken is within m of 1, or not clearly above 0, the reproducible pow is
+// evaluated on the same hdn and *fast_m is 0; otherwise the returned bound is
+// on the exact one's side of 1 and of 0, within relative m of it, and *fast_m
+// is m.  Without fast_m, or for other lobes, the exact bound (*fast_m 0).
+DEV_NOINLINE float bsdf_bound(const DevEdgeNode &node, const BoundCtx &c, float *fast_m = nullptr) {
+    if (fast_m) *fast_m = 0.f;
     const float q[6] = {node.lo[0] - c.p.x, node.hi[0] - c.p.x, node.lo[1] - c.p.y,
                         node.hi[1] - c.p.y, node.lo[2] - c.p.z, node.hi[2] - c.p.z};
     const CornerDots cn = corner_dots(c.n, q);
@@ -272,24 +301,30 @@ DEV_NOINLINE float bsdf_bound(const DevEdgeNode &node, const BoundCtx &c) {
             // the GGX D grows with n.h (A <= 1): its bound is the value at the bound of n.h
             maxp = ggx_D(hdn, c.expo);
         } else {
-            float e = c.expo;
-            maxp = dr_powf(hdn, e) * (e + 2.f) / float(2 * 3.14159265358979323846);
+            const float e = c.expo;
+            if (fast_m) {
+                const float y = e * filt_log2(hdn);
+                if (y < -160.f) {  // the pow underflows to 0 either way
+                    maxp = 0.f;
+                } else {
+                    const float m = (16.f + fabsf(y)) * 2.384185791e-7f;
+                    const float bf = cos_max * (c.dl / DR_PI + c.sl * (filt_exp2(y) * (e + 2.f) /
+                                                                        float(2 * 3.14159265358979323846)));
+                    if (m < 0.01f && bf > 1e-30f && (bf * (1.f - m) > 1.f || bf * (1.f + m) <= 1.f)) {
+                        *fast_m = m;
+                        return bf;
+                    }
+                    maxp = dr_powf(hdn, e) * (e + 2.f) / float(2 * 3.14159265358979323846);
+                }
+            } else {
+                maxp = dr_powf(hdn, e) * (e + 2.f) / float(2 * 3.14159265358979323846);
+            }
         }
     }
     return cos_max * (c.dl / DR_PI + c.sl * maxp);
 }
 
-// Fast sine, cosine and reciprocal square root of the silhouette filter
-// (absolute errors below 1e-6 on its arguments).
-#ifdef DR_HOST_BUILD
-HD float filt_sin(float x) { return std::sin(x); }
-HD float filt_cos(float x) { return std::cos(x); }
-HD float filt_rsqrt(float x) { return 1.f / std::sqrt(x); }
-#else
-DEV float filt_sin(float x) { return __sinf(x); }
-DEV float filt_cos(float x) { return __cosf(x); }
-DEV float filt_rsqrt(float x) { return rsqrtf(x); }
-#endif
+
 
 // Whether the node's cone of normals, widened by the angle its bounding
 // sphere subtends from p, reaches the directions perpendicular to p - centre:
@@ -522,10 +557,26 @@ struct EdgeWalk {
             lcs = contains_silhouette(L, p);
             rcs = contains_silhouette(R, p);
         }
-        float lbb = lcs ? bsdf_bound(L, bc) : 0.f;
-        float rbb = rcs ? bsdf_bound(R, bc) : 0.f;
+        // The children of an all-split node in the all walk, off the cone
+        // walk's path (cpmf 0): their bounds only meet thresholds (above 1,
+        // above 0, the importance cutoff), so they may come filtered.
+        const bool filt = !CONE && all_split && it.cpmf == 0.f;
+        float lm = 0.f, rm = 0.f;
+        float lbb = lcs ? bsdf_bound(L, bc, filt ? &lm : nullptr) : 0.f;
+        float rbb = rcs ? bsdf_bound(R, bc, filt ? &rm : nullptr) : 0.f;
         float il = lcs ? node_importance(L, lbb, p) : 0.f;
         float ir = rcs ? node_importance(R, rbb, p) : 0.f;
+        if (lm > 0.f || rm > 0.f) {
+            // the cutoff and the cone tests' finiteness check as the exact
+            // bounds decide them: exact bounds where a filtered one could differ
+            const float m = 2.f * fmaxf(lm, rm) + 1e-6f, sum = il + ir;
+            if (!(sum > 1e-10f * (1.f + m) || sum < 1e-10f * (1.f - m)) || !(il < 1e30f) || !(ir < 1e30f)) {
+                lbb = lcs ? bsdf_bound(L, bc) : 0.f;
+                rbb = rcs ? bsdf_bound(R, bc) : 0.f;
+                il = lcs ? node_importance(L, lbb, p) : 0.f;
+                ir = rcs ? node_importance(R, rbb, p) : 0.f;
+            }
+        }
         if (il + ir <= 1e-10f) return;
         // a node the cone walk cannot reach (cpmf 0) gives its children cpmf
         // 0 whatever the cone tests say, as long as the importances are
@@ -775,12 +826,14 @@ struct EdgeLine {
     float q;          // density of l: the picked lobe's pmf times its line pdf (or the lobe mixture)
 };
 
+// rec (may be null): the edge's silhouette-test record, which gives the
+// answer of is_silhouette from one contiguous read.
 template <bool EXT = true>
 DEV bool edge_line_sample(const DevScene &s, const EdgeSample &es, const DevEdge &edge, float3 wi, int stri,
-                          const SurfacePoint &sp, EdgeLine &out) {
+                          const SurfacePoint &sp, EdgeLine &out, const EdgeRec *rec = nullptr) {
     const bool none = false;
     if (stri < 0) return none;
-    if (!is_silhouette(s, sp.p, edge)) return none;
+    if (!(rec ? is_silhouette_rec(rec, sp.p) : is_silhouette(s, sp.p, edge))) return none;
     float3 v0 = edge_v0(s, edge), v1 = edge_v1(s, edge);
     if (abs_sum(v1 - v0) == 1e-10f) return none;
     int mi = material_of_tri(s, stri);

@@ -41,6 +41,7 @@ def load():
         L.hh_trace.restype = C.c_longlong
         L.hh_set_proposal.argtypes = [C.c_int, C.c_float]
         L.hh_set_split.argtypes = [C.c_int]
+        L.hh_set_checkpoints.argtypes = [C.c_int]
         L.hh_math.argtypes = [C.c_int, C.c_void_p, C.c_void_p, C.c_void_p, C.c_longlong]
         L.hh_scene_edges.argtypes = [C.POINTER(_abi.dr_scene_desc), C.c_int, C.c_void_p, C.c_longlong]
         L.hh_scene_edges.restype = C.c_longlong
@@ -82,6 +83,12 @@ def trace(wl, rays):
 def set_proposal(seed, alpha):
     """Synthetic learned proposal of later renders (seed 0: none)."""
     load().hh_set_proposal(int(seed), float(alpha))
+
+
+def set_checkpoints(k):
+    """Later renders trace paths in the checkpointed form (segments of k = 4,
+    8 or 16 bounces, up to 16 segments; 0: per-bounce records, up to 64)."""
+    load().hh_set_checkpoints(int(k))
 
 
 def set_split(on):

@@ -19,6 +19,9 @@ static float g_prop_alpha = 0.f;
 // there on as tasks and walk those after all points (the GPU's two-stage
 // traversal of large trees)
 static int g_split = 0;
+// hh_set_checkpoints(k): later hh_render calls trace paths in the checkpointed
+// form, segments of k bounces (0: the per-bounce records)
+static int g_ckpt = 0;
 
 #include "../../delta_ray_b200/csrc/dr_backward.cuh"
 #include "../../delta_ray_b200/csrc/dr_bvh.cuh"
@@ -158,6 +161,15 @@ int hh_render(const dr_scene_desc *desc, const dr_render_desc *rd, const float *
     auto push = [&](const PointRecord &pr) { pts.push_back(pr); };
     // the kernels' two instantiations, chosen as the launchers choose them
     auto sample = [&](int x, int y, int si, float3 dc, HostSink &gs) {
+        if (g_ckpt == 4)
+            return s.specular_chains ? backward_pixel_sample<true, -4>(s, x, y, W, H, spp, si, B, seed, dc, gs, push)
+                                     : backward_pixel_sample<false, -4>(s, x, y, W, H, spp, si, B, seed, dc, gs, push);
+        if (g_ckpt == 8)
+            return s.specular_chains ? backward_pixel_sample<true, -8>(s, x, y, W, H, spp, si, B, seed, dc, gs, push)
+                                     : backward_pixel_sample<false, -8>(s, x, y, W, H, spp, si, B, seed, dc, gs, push);
+        if (g_ckpt == 16)
+            return s.specular_chains ? backward_pixel_sample<true, -16>(s, x, y, W, H, spp, si, B, seed, dc, gs, push)
+                                     : backward_pixel_sample<false, -16>(s, x, y, W, H, spp, si, B, seed, dc, gs, push);
         return s.specular_chains ? backward_pixel_sample<true>(s, x, y, W, H, spp, si, B, seed, dc, gs, push)
                                  : backward_pixel_sample<false>(s, x, y, W, H, spp, si, B, seed, dc, gs, push);
     };
@@ -310,6 +322,7 @@ long long hh_traverse_range(const dr_scene_desc *desc, const dr_render_desc *rd,
 }
 
 void hh_set_split(int on) { g_split = on; }
+void hh_set_checkpoints(int k) { g_ckpt = k; }
 
 // The synthetic proposal of later hh_render calls (seed 0: none).
 void hh_set_proposal(int seed, float alpha) {
