@@ -188,6 +188,8 @@ struct dr_scene {
     std::unique_ptr<BackwardQueues> queues;  // taken at the first backward call
     std::unique_ptr<ProposalState> proposal;  // set by dr_scene_set_proposal
     DevBuf view_grad, view_prim_edges, view_prim_cdf, view_prim_func;  // dr_render_backward_views
+    std::vector<std::unique_ptr<DevBuf>> batch_prim;  // per view of a batched call: primary edges, cdf, func
+    DevBuf view_table;                                 // its ViewParams
     float3 lo, hi;                            // scene bounds
     DevScene ds;
     StageTimer timer;
@@ -592,13 +594,28 @@ long long initial_point_cap(const dr_scene *scene, const dr_render_desc *rd, dou
 // samples) outgrow their queue, `grow_points(n)` is asked for room for n and
 // the front runs again (the same points: the streams are deterministic).
 // Returns (shading points, edge items).
+// One view's front stage in a batched multi-view backward call: its device
+// view (camera, primary-edge sampler, camera-gradient offset, index), render
+// settings, adjoint and image.
+struct FrontCall {
+    DevScene ds;
+    dr_render_desc rd;
+    const float *d_image;
+    float *image;
+};
+
+// fronts (may be null): a batched multi-view call.  Each view's front stage
+// runs in turn into the shared point queue, then one edge stage serves every
+// view's points (ws.views gives each point its view's settings); the
+// gradient has grad_len floats (the scene's, then one camera block per view).
 template <class Grow, class GrowPoints>
 std::pair<long long, long long> run_backward(dr_scene *scene, const dr_render_desc *rd, const float *d_image_dev,
                                              float *grad_dev, float *image_dev, BackwardWorkspace &ws,
                                              cudaStream_t st, StageTimer *timer, Grow grow, GrowPoints grow_points,
                                              ProposalState *prop = nullptr, const DevScene *view = nullptr,
-                                             EdgeStats *stats = nullptr) {
-    const DevScene ds = view ? *view : call_scene(scene, rd);
+                                             EdgeStats *stats = nullptr, const std::vector<FrontCall> *fronts = nullptr,
+                                             long long grad_len = 0) {
+    const DevScene ds = fronts ? (*fronts)[0].ds : view ? *view : call_scene(scene, rd);
     const GradCacheCfg cfg = grad_cache_cfg(scene->h);
     BackwardCounters c;
     auto read = [&]() {
@@ -665,19 +682,35 @@ std::pair<long long, long long> run_backward(dr_scene *scene, const dr_render_de
     // when the last call's edges per point predict more items than the queue
     // can ever hold, the edge stage streams from the start instead of
     // traversing every point once only to find that out
-    const long long samples = (long long)rd->width * rd->height * rd->spp;
+    long long samples = (long long)rd->width * rd->height * rd->spp;
+    if (fronts) {
+        samples = 0;
+        for (const FrontCall &f : *fronts) samples += (long long)f.rd.width * f.rd.height * f.rd.spp;
+    }
     const bool stream_first = prop == nullptr && stats && stats->items_per_point > 0 &&
                               (double)samples * stats->items_per_point > (double)max_queue_items();
     for (int attempt = 0;; attempt++) {
         check_cuda(cudaMemsetAsync(ws.counters, 0, sizeof(BackwardCounters), st), "memset");
-        check_cuda(cudaMemsetAsync(grad_dev, 0, sizeof(float) * scene->h.grad_total, st), "memset");
+        check_cuda(cudaMemsetAsync(grad_dev, 0, sizeof(float) * (grad_len > 0 ? grad_len : scene->h.grad_total), st),
+                   "memset");
         ws.pt_begin = 0;
         ws.pt_end = ws.cap_points;
-        check_launch(dr_launch_backward_front(ds, rd->width, rd->height, rd->spp, rd->max_bounces, rd->seed,
-                                              d_image_dev, grad_dev, image_dev, rd->primary_edge_samples, rd->dp_mode,
-                                              ws, cfg, scene->num_sms, st, &scene->last_launches, timer,
-                                              prop == nullptr && !stream_first),
-                     "backward launch");
+        if (fronts) {
+            for (size_t k = 0; k < fronts->size(); k++) {
+                const FrontCall &f = (*fronts)[k];
+                check_launch(dr_launch_backward_front(f.ds, f.rd.width, f.rd.height, f.rd.spp, f.rd.max_bounces,
+                                                      f.rd.seed, f.d_image, grad_dev, f.image,
+                                                      f.rd.primary_edge_samples, f.rd.dp_mode, ws, cfg,
+                                                      scene->num_sms, st, &scene->last_launches, timer, false, k == 0),
+                             "backward launch");
+            }
+        } else {
+            check_launch(dr_launch_backward_front(ds, rd->width, rd->height, rd->spp, rd->max_bounces, rd->seed,
+                                                  d_image_dev, grad_dev, image_dev, rd->primary_edge_samples,
+                                                  rd->dp_mode, ws, cfg, scene->num_sms, st, &scene->last_launches,
+                                                  timer, prop == nullptr && !stream_first),
+                         "backward launch");
+        }
         read();
         if (!(c.status & DR_STATUS_POINT_OVERFLOW)) break;
         const long long needed = (long long)c.points;
@@ -686,6 +719,13 @@ std::pair<long long, long long> run_backward(dr_scene *scene, const dr_render_de
                                                     std::to_string(ws.cap_points) + ")");
     }
     const long long P = std::min((long long)c.points, ws.cap_points);
+    if (fronts && !stream_first) {
+        // the views' points walked together
+        timer->mark(st, "host_point_count");
+        check_launch(dr_launch_edge_traverse(ds, rd->seed, ws, scene->num_sms, st, &scene->last_launches, timer),
+                     "edge traversal launch");
+        read();
+    }
     if (prop) {
         // the proposal: features and slot probabilities of every point, then
         // the traversal that draws edges with them
@@ -971,7 +1011,9 @@ namespace {
 // The backward pass of dr_render_backward on the library's cached queues;
 // `view` (may be null) replaces the scene's device view (another camera).
 void backward_on_queues(dr_scene *scene, const dr_render_desc *rd, const DevScene *view, const float *d_image_dev,
-                        float *grad_dev, float *image_dev, cudaStream_t st) {
+                        float *grad_dev, float *image_dev, cudaStream_t st,
+                        const std::vector<FrontCall> *fronts = nullptr, long long grad_len = 0,
+                        const ViewParams *views_dev = nullptr) {
     if (!scene->queues) {
         scene->queues = take_queues(scene->device, st);
         // another scene's edge statistics say nothing about this one
@@ -982,6 +1024,15 @@ void backward_on_queues(dr_scene *scene, const dr_render_desc *rd, const DevScen
     }
     BackwardQueues &q = *scene->queues;
     long long cap_points = initial_point_cap(scene, rd, q.points_per_sample);
+    double samples_total = (double)rd->width * rd->height * rd->spp;
+    if (fronts) {
+        cap_points = 0;
+        samples_total = 0;
+        for (const FrontCall &f : *fronts) {
+            cap_points += initial_point_cap(scene, &f.rd, q.points_per_sample);
+            samples_total += (double)f.rd.width * f.rd.height * f.rd.spp;
+        }
+    }
     long long cap_items =
         std::min(max_queue_items(), std::max(q.cap_items, std::max<long long>(cap_points * 4, 1 << 16)));
     q.counts.reserve(sizeof(BackwardCounters));
@@ -1043,7 +1094,7 @@ void backward_on_queues(dr_scene *scene, const dr_render_desc *rd, const DevScen
     // kept for later calls)
     auto grow_points = [&](long long want) {
         cap_points = want + want / 16 + 1;
-        q.points_per_sample = (double)cap_points / ((double)rd->width * rd->height * rd->spp);
+        q.points_per_sample = (double)cap_points / samples_total;
         bind_points();
         return cap_points;
     };
@@ -1053,8 +1104,9 @@ void backward_on_queues(dr_scene *scene, const dr_render_desc *rd, const DevScen
             throw DrError(DR_ERR_INVALID_ARGUMENT, "DR_FLAG_LEARNED_PROPOSAL without dr_scene_set_proposal");
         prop = scene->proposal.get();
     }
+    ws.views = views_dev;
     auto counts = run_backward(scene, rd, d_image_dev, grad_dev, image_dev, ws, st, &scene->timer, grow, grow_points,
-                               prop, view, &q.stats);
+                               prop, view, &q.stats, fronts, grad_len);
     scene->last_points = counts.first;
     scene->last_items = counts.second;
 }
@@ -1082,12 +1134,10 @@ dr_status dr_render_backward_views(dr_scene *scene, int n_views, const dr_view_d
         scene->last_launches = 0;
         const long long total = scene->h.grad_total;
         check_cuda(cudaMemsetAsync(grad_dev, 0, sizeof(float) * total, st), "memset");
-        scene->view_grad.reserve(sizeof(float) * total);
-        float *vg = scene->view_grad.as<float>();
-        long long points = 0, items = 0;
-        for (int v = 0; v < n_views; v++) {
+        // view v's device scene: its camera and a primary-edge sampler built
+        // from it into the given buffers
+        auto setup_view = [&](int v, DevBuf &pe_buf, DevBuf &pc_buf, DevBuf &pf_buf) {
             const dr_view_desc &vw = views[v];
-            check_backward_args(scene, &vw.render, vw.d_image, vg);
             HCam hc;
             auto m16 = [&](const float *p, float *dst, const char *what) {
                 std::vector<float> m = fetch(p, 16, what);
@@ -1099,9 +1149,6 @@ dr_status dr_render_backward_views(dr_scene *scene, int n_views, const dr_view_d
             hc.aspect = vw.camera.aspect_ratio;
             hc.clip_near = vw.camera.clip_near;
             hc.fisheye = vw.camera.fisheye != 0;
-            // the view's primary-edge sampler (the previous view's kernels have finished)
-            std::vector<DevEdge> pe;
-            HDist pd;
             int n_prim = 0;
             float prim_func_int = 0.f;
             if (scene->gpu_edges) {
@@ -1113,19 +1160,21 @@ dr_status dr_render_backward_views(dr_scene *scene, int n_views, const dr_view_d
                 dc.clip_near = hc.clip_near;
                 dc.fisheye = hc.fisheye;
                 const int nk = scene->num_kept;
-                scene->view_prim_edges.reserve(sizeof(DevEdge) * std::max(1, nk));
-                scene->view_prim_cdf.reserve(sizeof(float) * (nk + 1));
-                scene->view_prim_func.reserve(sizeof(float) * std::max(1, nk));
-                check_cuda(dr_build_primary(scene->ds, dc, scene->kept_dev, nk, scene->view_prim_edges.as<DevEdge>(),
-                                            scene->view_prim_cdf.as<float>(), scene->view_prim_func.as<float>(),
-                                            &n_prim, &prim_func_int, scene->edge_scratch.p, scene->edge_scratch.bytes,
-                                            st, &scene->last_launches),
+                pe_buf.reserve(sizeof(DevEdge) * std::max(1, nk));
+                pc_buf.reserve(sizeof(float) * (nk + 1));
+                pf_buf.reserve(sizeof(float) * std::max(1, nk));
+                check_cuda(dr_build_primary(scene->ds, dc, scene->kept_dev, nk, pe_buf.as<DevEdge>(),
+                                            pc_buf.as<float>(), pf_buf.as<float>(), &n_prim, &prim_func_int,
+                                            scene->edge_scratch.p, scene->edge_scratch.bytes, st,
+                                            &scene->last_launches),
                            "view primary-edge sampler");
             } else {
+                std::vector<DevEdge> pe;
+                HDist pd;
                 scene->h.primary_for(hc, pe, pd);
-                scene->view_prim_edges.upload(pe);
-                scene->view_prim_cdf.upload(pd.cdf);
-                scene->view_prim_func.upload(pd.func);
+                pe_buf.upload(pe);
+                pc_buf.upload(pd.cdf);
+                pf_buf.upload(pd.func);
                 n_prim = (int)pe.size();
                 prim_func_int = pd.func_int;
             }
@@ -1136,20 +1185,80 @@ dr_status dr_render_backward_views(dr_scene *scene, int n_views, const dr_view_d
             ds.cam.aspect = hc.aspect;
             ds.cam.clip_near = hc.clip_near;
             ds.cam.fisheye = hc.fisheye;
-            ds.prim_edges = scene->view_prim_edges.as<DevEdge>();
+            ds.prim_edges = pe_buf.as<DevEdge>();
             ds.num_prim_edges = n_prim;
-            ds.prim_cdf = scene->view_prim_cdf.as<float>();
-            ds.prim_func = scene->view_prim_func.as<float>();
+            ds.prim_cdf = pc_buf.as<float>();
+            ds.prim_func = pf_buf.as<float>();
             ds.prim_func_int = prim_func_int;
-            backward_on_queues(scene, &vw.render, &ds, vw.d_image, vg, vw.image, st);
-            points += scene->last_points;
-            items += scene->last_items;
-            check_cuda(dr_launch_accumulate(grad_dev + 64, vg + 64, total - 64, st), "gradient sum");
+            return ds;
+        };
+        for (int v = 0; v < n_views; v++)
+            check_backward_args(scene, &views[v].render, views[v].d_image, grad_dev);
+        // One edge stage for every view when they differ only in camera,
+        // size, samples, seed and adjoint (the kernels take those per point).
+        bool batched = n_views > 1;
+        for (int v = 1; v < n_views && batched; v++) {
+            const dr_render_desc &a = views[0].render, &b = views[v].render;
+            batched = a.max_bounces == b.max_bounces && a.flags == b.flags && a.dp_mode == b.dp_mode;
+        }
+        if (views && n_views > 0 && (views[0].render.flags & DR_FLAG_LEARNED_PROPOSAL)) batched = false;
+        long long points = 0, items = 0;
+        if (batched) {
+            const long long glen = total + 64ll * n_views;
+            scene->view_grad.reserve(sizeof(float) * glen);
+            float *vg = scene->view_grad.as<float>();
+            while ((int)scene->batch_prim.size() < 3 * n_views)
+                scene->batch_prim.emplace_back(new DevBuf());
+            std::vector<FrontCall> fronts(n_views);
+            std::vector<ViewParams> table(n_views);
+            for (int v = 0; v < n_views; v++) {
+                FrontCall &f = fronts[v];
+                f.ds = setup_view(v, *scene->batch_prim[3 * v], *scene->batch_prim[3 * v + 1],
+                                  *scene->batch_prim[3 * v + 2]);
+                f.ds.cam_off = (int)(total + 64ll * v);
+                f.ds.view_id = v;
+                f.rd = views[v].render;
+                f.d_image = views[v].d_image;
+                f.image = views[v].image;
+                ViewParams &t = table[v];
+                t.cam = f.ds.cam;
+                t.W = f.rd.width;
+                t.H = f.rd.height;
+                t.spp = f.rd.spp;
+                t.cam_off = f.ds.cam_off;
+                t.seed = f.rd.seed;
+            }
+            scene->view_table.upload(table);
+            backward_on_queues(scene, &fronts[0].rd, &fronts[0].ds, fronts[0].d_image, vg, nullptr, st, &fronts, glen,
+                               scene->view_table.as<ViewParams>());
+            points = scene->last_points;
+            items = scene->last_items;
+            // the views' summed gradient (camera block zero) and their camera blocks
+            check_cuda(cudaMemcpyAsync(grad_dev + 64, vg + 64, sizeof(float) * (total - 64), cudaMemcpyDeviceToDevice,
+                                       st),
+                       "gradient copy");
             if (camera_grads_dev)
-                check_cuda(cudaMemcpyAsync(camera_grads_dev + 64 * (size_t)v, vg, 64 * sizeof(float),
+                check_cuda(cudaMemcpyAsync(camera_grads_dev, vg + total, sizeof(float) * 64 * (size_t)n_views,
                                            cudaMemcpyDeviceToDevice, st),
-                           "camera gradient");
-            check_cuda(cudaStreamSynchronize(st), "view");
+                           "camera gradients");
+            check_cuda(cudaStreamSynchronize(st), "views");
+        } else {
+            scene->view_grad.reserve(sizeof(float) * total);
+            float *vg = scene->view_grad.as<float>();
+            for (int v = 0; v < n_views; v++) {
+                const dr_view_desc &vw = views[v];
+                // the view's sampler (the previous view's kernels have finished)
+                DevScene ds = setup_view(v, scene->view_prim_edges, scene->view_prim_cdf, scene->view_prim_func);
+                backward_on_queues(scene, &vw.render, &ds, vw.d_image, vg, vw.image, st);
+                points += scene->last_points;
+                items += scene->last_items;
+                check_cuda(dr_launch_accumulate(grad_dev + 64, vg + 64, total - 64, st), "gradient sum");
+                if (camera_grads_dev)
+                    check_cuda(cudaMemcpyAsync(camera_grads_dev + 64 * (size_t)v, vg, 64 * sizeof(float),
+                                               cudaMemcpyDeviceToDevice, st),
+                               "camera gradient");
+                check_cuda(cudaStreamSynchronize(st), "view");
+            }
         }
         scene->last_points = points;
         scene->last_items = items;

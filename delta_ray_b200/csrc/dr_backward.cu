@@ -112,7 +112,8 @@ __global__ void __launch_bounds__(128, 6) k_dp_propagate(DevScene s, int W, int 
         }
         PointRecord pt;
         pt.load(ws.pt + (size_t)p * DR_PT_WORDS);
-        propagate_dp<kChains>(s, pt, W, H, spp, seed, dp, bg);
+        const PointView v = point_view(ws, pt.view, W, H, spp, seed);
+        propagate_dp<kChains>(s, pt, v.W, v.H, v.spp, v.seed, dp, bg, v.cam, v.cam_off);
     }
     block_grad_flush(bg);
 }
@@ -128,12 +129,12 @@ int path_lanes_log2(int spp) {
 cudaError_t dr_launch_backward_front(const DevScene &s, int W, int H, int spp, int B, uint64_t seed,
                                      const float *d_image, float *grad, float *img, long long primary_edge_samples,
                                      int dp_mode, const BackwardWorkspace &ws, const GradCacheCfg &cfg, int num_sms,
-                                     cudaStream_t st, int *launches, StageTimer *timer, bool traverse) {
+                                     cudaStream_t st, int *launches, StageTimer *timer, bool traverse, bool first) {
     const int bs = 128;
     size_t smem = sizeof(float) * (size_t)(cfg.head + cfg.tail_len);
     int lanes_log2 = path_lanes_log2(spp);
     long long threads = ((long long)W * H) << lanes_log2;
-    timer->begin(st);
+    if (first) timer->begin(st);  // a later view's front stage of a batched call continues the timing
     if (dp_mode != DR_DP_SUM || s.specular_chains) {
         // LAST: one key per point; SUM with chains: a float4 dp sum per point
         size_t per = dp_mode == DR_DP_SUM ? DR_PT_LAST_BYTES : sizeof(unsigned long long);

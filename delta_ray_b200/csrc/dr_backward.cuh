@@ -40,6 +40,7 @@ struct PointRecord {
     uint64_t sid;
     int light;
     int bounce;
+    int view = 0;  // the view of a batched multi-view call (0 otherwise)
     HD void store(float *w) const {
         w[0] = p.x; w[1] = p.y; w[2] = p.z;
         w[3] = n.x; w[4] = n.y; w[5] = n.z;
@@ -52,7 +53,7 @@ struct PointRecord {
         w[19] = dr_i2f((int)(uint32_t)(sid >> 32));
         w[20] = dr_i2f(light);
         w[21] = dr_i2f(bounce);
-        w[22] = 0.f;
+        w[22] = dr_i2f(view);
         w[23] = 0.f;
     }
     HD void load(const float *w) {
@@ -67,6 +68,7 @@ struct PointRecord {
         sid = (uint64_t)(uint32_t)dr_f2i(w[18]) | ((uint64_t)(uint32_t)dr_f2i(w[19]) << 32);
         light = dr_f2i(w[20]);
         bounce = dr_f2i(w[21]);
+        view = dr_f2i(w[22]);
     }
     HD SurfacePoint surface() const {
         SurfacePoint sp;
@@ -330,6 +332,7 @@ DEV bool trace_bounce(const DevScene &s, const LightSample &ls, float3 wi, int b
         pr.sid = sid;
         pr.light = light_pick;
         pr.bounce = b + 1;
+        pr.view = s.view_id;
         (*push)(pr);
     }
     return true;
@@ -384,6 +387,7 @@ DEV float3 backward_pixel_sample(const DevScene &s, int x, int y, int W, int H, 
         pr.sid = sid;
         pr.light = light_pick;
         pr.bounce = 0;
+        pr.view = s.view_id;
         push_point(pr);
     }
     PathState ps;
@@ -564,7 +568,7 @@ DEV float3 backward_pixel_sample(const DevScene &s, int x, int y, int W, int H, 
     d_d -= d_wi;
     scatter_tri_vertices(s, h0.tri, tg.v0, tg.v1, tg.v2, g);
     if (td0.has_n) scatter_tri_normals(s, h0.tri, tg.n0, g);
-    d_sample_primary(s.cam, sx, sy, d_o, d_d, g, 0);
+    d_sample_primary(s.cam, sx, sy, d_o, d_d, g, s.cam_off);
     return color;
 }
 
@@ -711,14 +715,19 @@ DEV float3 eval_item(const DevScene &s, const PointRecord &pt, int tree, int ei,
 // triangles' positions (the second sweep of delta_ray.cpp:975-1002, which
 // scatters neither normals nor material parameters).  A point after the first
 // vertex was reached by specular samples only: its chain is traced again.
+// cam (may be null): the point's camera and camera-gradient offset when it is
+// not the scene's (a view of a batched multi-view call).
 template <bool kChains, class G>
-DEV void propagate_dp(const DevScene &s, const PointRecord &pt, int W, int H, int spp, uint64_t seed, float3 dp, G &g) {
+DEV void propagate_dp(const DevScene &s, const PointRecord &pt, int W, int H, int spp, uint64_t seed, float3 dp, G &g,
+                      const DevCamera *cam = nullptr, int cam_off = 0) {
+    const DevCamera &pc = cam ? *cam : s.cam;
+    const int pco = cam ? cam_off : s.cam_off;
     uint64_t pix = pt.sid / (uint64_t)spp;
     int x = (int)(pix % (uint64_t)W), y = (int)(pix / (uint64_t)W);
     Rng r;
     float sx, sy;
     pixel_sample_position(x, y, W, H, spp, pt.sid, seed, s.full_pixel_jitter != 0, sx, sy, r);
-    Ray ray = sample_primary(s.cam, sx, sy, true);
+    Ray ray = sample_primary(pc, sx, sy, true);
     VertexGrad v0;
     v0.zero();
     float3 d_wi = f3(0.f);
@@ -780,7 +789,7 @@ DEV void propagate_dp(const DevScene &s, const PointRecord &pt, int W, int H, in
     d_intersect_tri(td, ray.o, ray.d, fw, v0.dp, f3(0.f), v0.df, v0.duv, tg, d_o, d_d);
     d_d -= d_wi;
     scatter_tri_vertices(s, tri0, tg.v0, tg.v1, tg.v2, g);
-    d_sample_primary(s.cam, sx, sy, d_o, d_d, g, 0);
+    d_sample_primary(pc, sx, sy, d_o, d_d, g, pco);
 }
 
 // The gradients of one primary-edge sample.
@@ -793,7 +802,7 @@ template <class G> DEV void scatter_primary(const DevScene &s, const PrimaryEdge
     g.add(sh.grad_v + 3 * pr.edge.v1 + 0, pr.dv1.x);
     g.add(sh.grad_v + 3 * pr.edge.v1 + 1, pr.dv1.y);
     g.add(sh.grad_v + 3 * pr.edge.v1 + 2, pr.dv1.z);
-    for (int q = 0; q < 16; q++) g.add(16 + q, pr.dw2c[q]);
+    for (int q = 0; q < 16; q++) g.add(s.cam_off + 16 + q, pr.dw2c[q]);
 }
 
 // Primary-edge sample i (delta_ray.cpp:1478-1522).

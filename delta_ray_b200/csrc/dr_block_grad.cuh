@@ -81,4 +81,37 @@ inline int blocks_for(long long n, int bs) { return (int)((n + bs - 1) / bs); }
 // resident-grid size for the grid-stride stages: a few blocks per SM
 inline int stage_grid(int num_sms) { return num_sms * 12; }
 
+// A shading point's render settings: its view's in a batched multi-view call
+// (ws.views), else the call's.  cam is null for the scene's own camera.
+struct PointView {
+    int W, H, spp;
+    uint64_t seed;
+    const DevCamera *cam;
+    int cam_off;
+};
+__device__ __forceinline__ PointView point_view(const BackwardWorkspace &ws, int view, int W, int H, int spp,
+                                                uint64_t seed) {
+    PointView v;
+    if (ws.views) {
+        const ViewParams &p = ws.views[view];
+        v.W = p.W;
+        v.H = p.H;
+        v.spp = p.spp;
+        v.seed = p.seed;
+        v.cam = &p.cam;
+        v.cam_off = p.cam_off;
+    } else {
+        v.W = W;
+        v.H = H;
+        v.spp = spp;
+        v.seed = seed;
+        v.cam = nullptr;
+        v.cam_off = 0;
+    }
+    return v;
+}
+__device__ __forceinline__ uint64_t point_seed(const BackwardWorkspace &ws, int view, uint64_t seed) {
+    return ws.views ? ws.views[view].seed : seed;
+}
+
 }  // namespace

@@ -104,7 +104,8 @@ __global__ void __launch_bounds__(128, 6) k_edge_traverse(DevScene s, uint64_t s
                 out.add((int)p, tree, ei, j, w, code);
                 cnt++;
             };
-            if (!traverse_point<PROP>(s, pt, seed, emit, point_proposal(ws, p), (NoDefer *)nullptr, &visits))
+            if (!traverse_point<PROP>(s, pt, point_seed(ws, pt.view, seed), emit, point_proposal(ws, p),
+                                      (NoDefer *)nullptr, &visits))
                 set_status(&ws.counters->status, DR_STATUS_STACK_OVERFLOW);
             if (ws.pt_items) ws.pt_items[p] = cnt;
         }
@@ -151,7 +152,7 @@ __global__ void __launch_bounds__(128, 4) k_edge_expand(DevScene s, uint64_t see
                     if (first + (unsigned long long)k < (unsigned long long)ws.cap_tasks)
                         ws.tasks[first + k] = tb[k];
                     else
-                        ok &= traverse_point_task<PROP>(s, pt, seed, tb[k], emit, pr, &visits);
+                        ok &= traverse_point_task<PROP>(s, pt, point_seed(ws, pt.view, seed), tb[k], emit, pr, &visits);
                 }
                 nt = 0;
             };
@@ -159,7 +160,7 @@ __global__ void __launch_bounds__(128, 4) k_edge_expand(DevScene s, uint64_t see
                 if (nt == DR_TASK_BUF) flush();
                 tb[nt++] = EdgeTask{(int)p, code, bb, c, a, l};
             };
-            ok &= traverse_point<PROP, DR_TASK_CUT>(s, pt, seed, emit, pr, &defer, &visits);
+            ok &= traverse_point<PROP, DR_TASK_CUT>(s, pt, point_seed(ws, pt.view, seed), emit, pr, &defer, &visits);
             if (nt > 0) flush();
             if (!ok) set_status(&ws.counters->status, DR_STATUS_STACK_OVERFLOW);
             if (ws.pt_items) ws.pt_items[p] = cnt;  // the subtrees add theirs
@@ -215,7 +216,7 @@ __global__ void __launch_bounds__(128, DR_TASKS_BLOCKS) k_edge_tasks(DevScene s,
             PointRecord pt;
             pt.load(ws.pt + (size_t)t.point * DR_PT_WORDS);
             point = t.point;
-            start_point_task<PROP>(w, s, pt, seed, t, point_proposal(ws, t.point));
+            start_point_task<PROP>(w, s, pt, point_seed(ws, pt.view, seed), t, point_proposal(ws, t.point));
             steps = 0;
         }
         w.step(emit, nd, &visits);
@@ -245,7 +246,8 @@ __device__ __forceinline__ void finish_item(const DevScene &s, const BackwardWor
     if (is_zero(dp)) return;
     if (dp_mode == DR_DP_SUM) {
         if (pt.bounce == 0) {
-            propagate_dp<false>(s, pt, W, H, spp, seed, dp, bg);
+            const PointView v = point_view(ws, pt.view, W, H, spp, seed);
+            propagate_dp<false>(s, pt, v.W, v.H, v.spp, v.seed, dp, bg, v.cam, v.cam_off);
         } else {  // after specular samples: summed here, the chain is traced by k_dp_propagate
             float *a = reinterpret_cast<float *>(ws.pt_last) + 4 * (size_t)it.x;
             atomicAdd(a, dp.x);
@@ -285,7 +287,7 @@ __global__ void __launch_bounds__(128, 4) k_edge_line(DevScene s, uint64_t seed,
             int4 it = ws.items[i];
             PointRecord pt;
             pt.load(ws.pt + (size_t)it.x * DR_PT_WORDS);
-            ok = item_line<EXT>(s, pt, it.y >> 30, it.y & ((1 << 30) - 1), seed, el);
+            ok = item_line<EXT>(s, pt, it.y >> 30, it.y & ((1 << 30) - 1), point_seed(ws, pt.view, seed), el);
         }
         __syncwarp();
         unsigned long long slot = warp_reserve(&ws.counters->survivors, ok ? 1 : 0);
@@ -347,10 +349,7 @@ __global__ void __launch_bounds__(128, DR_CONNECT_BLOCKS) k_edge_connect(DevScen
             float3 sdir;
             edge_side_dirs(el, edge_v0(s, edge), edge_v1(s, edge), p, sdir, rdir, ldir);
             // the connectivity test of edge_connect_bvh, its walks stepped below
-            const int off = s.shapes[edge.shape].tri_off;
-            const int g0 = off + edge.f0, g1 = edge.f1 >= 0 ? off + edge.f1 : -1;
-            fr = hit_faces(s, g0, g1, p, rdir, 1e-3f);
-            fl = hit_faces(s, g0, g1, p, ldir, 1e-3f);
+            hit_faces_pair(s, edge, p, rdir, ldir, 1e-3f, fr, fl);
             if (fr.tri >= 0) {
                 w.begin(s.bvh_root, p, rdir, 1e-3f, fr.t, fr.tri);
                 phase = 1;
@@ -425,7 +424,7 @@ __global__ void __launch_bounds__(128, 8) k_edge_line_rays(DevScene s, uint64_t 
             PointRecord pt;
             pt.load(ws.pt + (size_t)it.x * DR_PT_WORDS);
             int tree = it.y >> 30, ei = it.y & ((1 << 30) - 1);
-            ok = item_line<EXT>(s, pt, tree, ei, seed, el);
+            ok = item_line<EXT>(s, pt, tree, ei, point_seed(ws, pt.view, seed), el);
             if (ok) {
                 const DevEdge &edge = tree ? s.nrm_edges[ei] : s.sil_edges[ei];
                 ok = edge_rays(s, el, edge, pt.tri, pt.p, DIRECT, eh);
@@ -462,7 +461,8 @@ __global__ void __launch_bounds__(128, 4) k_edge_radiance(DevScene s, int B, uin
         PointRecord pt;
         pt.load(ws.pt + (size_t)it.x * DR_PT_WORDS);
         float3 shr, shl;
-        item_side_radiance(s, pt, it.y >> 30, it.y & ((1 << 30) - 1), it.z, B, seed, el, eh, shr, shl);
+        item_side_radiance(s, pt, it.y >> 30, it.y & ((1 << 30) - 1), it.z, B, point_seed(ws, pt.view, seed), el, eh,
+                           shr, shl);
         ws.side_rad[2 * h] = make_float4(shr.x, shr.y, shr.z, shl.x);
         ws.side_rad[2 * h + 1] = make_float4(shl.y, shl.z, 0.f, 0.f);
     }
@@ -492,15 +492,16 @@ __global__ void __launch_bounds__(128, 4) k_edge_shade(DevScene s, int W, int H,
         PointRecord pt;
         pt.load(ws.pt + (size_t)it.x * DR_PT_WORDS);
         int tree = it.y >> 30, ei = it.y & ((1 << 30) - 1);
+        const PointView v = point_view(ws, pt.view, W, H, spp, seed);
         float mag = 0.f;
         float3 dp;
         if constexpr (PRE) {
             const float4 r0 = ws.side_rad[2 * h], r1 = ws.side_rad[2 * h + 1];
             const float3 rad[2] = {f3(r0.x, r0.y, r0.z), f3(r0.w, r1.x, r1.y)};
-            dp = item_shade<EXT, GI, BlockGrad, true>(s, pt, tree, ei, it.z, ws.item_w[i], spp, B, seed, bg, &mag, el,
-                                                     &eh, rad);
+            dp = item_shade<EXT, GI, BlockGrad, true>(s, pt, tree, ei, it.z, ws.item_w[i], v.spp, B, v.seed, bg, &mag,
+                                                     el, &eh, rad);
         } else {
-            dp = item_shade<EXT, GI>(s, pt, tree, ei, it.z, ws.item_w[i], spp, B, seed, bg, &mag, el, &eh);
+            dp = item_shade<EXT, GI>(s, pt, tree, ei, it.z, ws.item_w[i], v.spp, B, v.seed, bg, &mag, el, &eh);
         }
         finish_item<EXT>(s, ws, it, i, pt, dp, mag, W, H, spp, seed, dp_mode, bg);
     }

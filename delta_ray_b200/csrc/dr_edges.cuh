@@ -929,12 +929,16 @@ DEV void edge_side_dirs(const EdgeLine &el, float3 v0, float3 v1, float3 p, floa
     ldir = normalize(sdir - delta * split_n);
 }
 
-// Closest hit among triangles g0 and g1 (g1 < 0: none) under the closest-hit
-// rule, with the operands the LBVH's leaves hold (vertices in index order).
-DEV Hit hit_faces(const DevScene &s, int g0, int g1, float3 o, float3 d, float tnear) {
-    Hit h;
-    h.tri = -1;
-    h.t = DR_INF;
+// The closest hit among the edge's faces, under the closest-hit rule and with
+// the operands the LBVH's leaves hold (vertices in index order), for both
+// sides' rays, which share their origin: each face's edge vectors and origin
+// offset serve both rays.
+DEV void hit_faces_pair(const DevScene &s, const DevEdge &edge, float3 o, float3 dr, float3 dl, float tnear, Hit &hr,
+                        Hit &hl) {
+    const int off = s.shapes[edge.shape].tri_off;
+    const int g0 = off + edge.f0, g1 = edge.f1 >= 0 ? off + edge.f1 : -1;
+    hr.tri = hl.tri = -1;
+    hr.t = hl.t = DR_INF;
 #pragma unroll 1
     for (int k = 0; k < 2; k++) {
         const int g = k ? g1 : g0;
@@ -948,15 +952,19 @@ DEV Hit hit_faces(const DevScene &s, int g0, int g1, float3 o, float3 d, float t
             v[j].z = s.vtx[3 * vi[j] + 2];
             v[j].w = 0.f;
         }
-        const float4 a = v[0], b = v[1], c = v[2];
+        const TriRay r = tri_ray(v[0], v[1], v[2], o);
         float t;
-        if (hit_triangle(a, b, c, o, d, t) && t > tnear && (t < h.t || (t == h.t && g < h.tri))) {
-            h.t = t;
-            h.tri = g;
+        if (hit_triangle(r, dr, t) && t > tnear && (t < hr.t || (t == hr.t && g < hr.tri))) {
+            hr.t = t;
+            hr.tri = g;
+        }
+        if (hit_triangle(r, dl, t) && t > tnear && (t < hl.t || (t == hl.t && g < hl.tri))) {
+            hl.t = t;
+            hl.tri = g;
         }
     }
-    return h;
 }
+
 
 // The connectivity test of an edge sample in an LBVH scene (most samples
 // end here: edges hidden from p).  A side's closest hit is one of the edge's
@@ -965,9 +973,8 @@ DEV Hit hit_faces(const DevScene &s, int g0, int g1, float3 o, float3 d, float t
 // connected: `side` (0 the right ray, 1 the left) and `face`, its closest hit.
 DEV bool edge_connect_bvh(const DevScene &s, const DevEdge &edge, float3 p, float3 rdir, float3 ldir, int &side,
                           int &face) {
-    const int off = s.shapes[edge.shape].tri_off;
-    const int g0 = off + edge.f0, g1 = edge.f1 >= 0 ? off + edge.f1 : -1;
-    const Hit fr = hit_faces(s, g0, g1, p, rdir, 1e-3f), fl = hit_faces(s, g0, g1, p, ldir, 1e-3f);
+    Hit fr, fl;
+    hit_faces_pair(s, edge, p, rdir, ldir, 1e-3f, fr, fl);
     if (fr.tri < 0 && fl.tri < 0) return false;
     const bool cr = fr.tri >= 0 && !trace_before_bvh(s.bvh_nodes, s.bvh_tris, s.bvh_root, p, rdir, 1e-3f, fr.t, fr.tri);
     if (!cr && fl.tri < 0) return false;

@@ -102,6 +102,15 @@ struct BackwardCounters {
     unsigned long long handed[2], handed_total;
 };
 
+// A view of a batched multi-view backward call: what the edge stage needs of
+// the view its shading points came from.
+struct ViewParams {
+    DevCamera cam;
+    int W, H, spp;
+    int cam_off;  // the view's camera block in the flat gradient
+    uint64_t seed;
+};
+
 struct BackwardWorkspace {
     float *pt;                   // [cap_points][DR_PT_FLOATS] shading-point records
     long long cap_points;
@@ -138,6 +147,9 @@ struct BackwardWorkspace {
     // [cap_tasks] the second queue of the rounds of k_edge_tasks (null: one
     // round, no subtree handed on)
     EdgeTask *tasks2;
+    // per view of a batched multi-view call (null: the call's own settings);
+    // each point's settings are views[point.view]
+    const ViewParams *views;
     // [cap_points] edges each point's traversal sampled, written by the point
     // walk and added to by its subtrees (null: not kept); the streamed edge
     // stage plans its chunks from them
@@ -162,7 +174,8 @@ struct GradCacheCfg {
 cudaError_t dr_launch_backward_front(const DevScene &s, int W, int H, int spp, int B, uint64_t seed,
                                      const float *d_image, float *grad, float *img, long long primary_edge_samples,
                                      int dp_mode, const BackwardWorkspace &ws, const GradCacheCfg &cfg, int num_sms,
-                                     cudaStream_t st, int *launches, StageTimer *timer, bool traverse = true);
+                                     cudaStream_t st, int *launches, StageTimer *timer, bool traverse = true,
+                                     bool first = true);
 // Features of the learned edge proposal for points [0, n): x[n][16] bf16
 // (position normalised by the scene centre c and inverse half extent ih,
 // shading normal, roughness, incoming direction, zeros); points

@@ -84,6 +84,10 @@ struct EdgeTask {
 
 struct DevScene {
     DevCamera cam;
+    // flat-gradient offset of the camera's block (0; in a batched multi-view
+    // call, the view's own block after the scene's gradient) and the view's
+    // index, which its shading points carry
+    int cam_off, view_id;
     // geometry
     const float *vtx;  // [V][3] global
     const float *nrm;  // [V][3] or null

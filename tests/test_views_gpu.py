@@ -11,11 +11,15 @@ from conftest import rel_err
 pytestmark = pytest.mark.gpu
 
 
-def _views(wl):
+def _views(wl, around=False):
     from delta_ray_b200 import workloads
     specs = [([0, 5, -4.5], [0, 3, 0], 60.0, (48, 40), 4, 3),
              ([3.5, 6, -3], [0, 2, 0.5], 55.0, (32, 32), 2, 5),
              ([-3, 2.5, 3.5], [0.5, 2.5, -1], 70.0, (40, 24), 8, 7)]
+    if around:  # looking at the origin from a circle (the heightfield)
+        specs = [([0, 7, -10.5], [0, 0, 0], 45.0, (48, 40), 4, 3),
+                 ([9.1, 7, 5.25], [0, 0, 0], 45.0, (32, 32), 2, 5),
+                 ([-9.1, 7, 5.25], [0, 0, 0], 45.0, (40, 24), 8, 7)]
     rng = np.random.default_rng(2)
     views = []
     for eye, tgt, fov, res, spp, seed in specs:
@@ -25,27 +29,45 @@ def _views(wl):
     return views
 
 
-def test_views_match_one_call_per_view():
+def _case(name):
     import scenes
+    from delta_ray_b200 import workloads
+    if name == "icosphere_room":
+        return scenes.icosphere_room(seed=3, n_spheres=8, subdiv=(1, 2), max_bounces=2)
+    # 7,938 triangles: GPU-built edge trees, subtrees walked by the second stage
+    return workloads.heightfield(seed=2, resolution=(48, 40), spp=2, max_bounces=2, grid=64, patch=16)
+
+
+@pytest.mark.parametrize("name,mixed", [("icosphere_room", False), ("heightfield", False), ("icosphere_room", True)])
+def test_views_match_one_call_per_view(name, mixed):
+    """Views with the same bounce count and flags run batched (their points
+    share one edge stage); `mixed` gives one view another bounce count, which
+    runs the views one after another."""
     from delta_ray_b200 import _abi
     from delta_ray_b200.render_pytorch import Scene
-    wl = scenes.icosphere_room(seed=3, n_spheres=8, subdiv=(1, 2), max_bounces=2)
-    views = _views(wl)
+    wl = _case(name)
+    views = _views(wl, around=name == "heightfield")
+    if mixed:
+        views[1]["max_bounces"] = wl.max_bounces + 1
     _, mats, shps, lts = _abi.scene_dicts(wl.camera, wl.materials, wl.shapes, wl.lights)
     sc = Scene(_abi.scene_dicts(wl.camera, [], [], [])[0], mats, shps, lts, 0, None)
     for _ in range(2):  # the second call reuses the queues and the view buffers
         grad, cam_grads = sc.backward_views(views)
+        counts = tuple(sc.last_counts())
         grad, cam_grads = grad.cpu().numpy(), cam_grads.cpu().numpy()
         assert np.all(grad[:64] == 0) and np.isfinite(grad).all()
         ref = np.zeros_like(grad)
+        ref_counts = np.zeros(2, np.int64)
         for k, v in enumerate(views):
             s1 = Scene(_abi.scene_dicts(v["camera"], [], [], [])[0], mats, shps, lts, 0, None)
             g1, _ = s1.backward(v["width"], v["height"], v["spp"], v["max_bounces"], v["seed"],
                                 torch.from_numpy(v["d_image"]))
+            ref_counts += np.array(s1.last_counts())
             g1 = g1.cpu().numpy()
             ref[64:] += g1[64:]
             assert rel_err(cam_grads[k], g1[:64]) < 1e-4, k
             s1.close()
+        assert counts == tuple(ref_counts)
         assert np.abs(ref).max() > 0
         assert rel_err(grad, ref) < 1e-4
     sc.close()
