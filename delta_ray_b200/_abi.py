@@ -92,6 +92,14 @@ class dr_view_desc(C.Structure):
                 ("image", C.c_void_p)]
 
 
+class dr_tuning(C.Structure):
+    _fields_ = [("hand_steps", C.c_int32), ("task_rounds", C.c_int32), ("queue_items", C.c_int64)]
+
+
+class dr_tune_report(C.Structure):
+    _fields_ = [("best", dr_tuning), ("best_ms", C.c_float), ("start_ms", C.c_float), ("trials", C.c_int32)]
+
+
 class dr_proposal_desc(C.Structure):
     _fields_ = [("train", C.c_int), ("mix", C.c_float), ("learning_rate", C.c_float), ("train_points", C.c_int64),
                 ("params", C.c_void_p)]

@@ -56,12 +56,16 @@ def lib():
     L.dr_scene_proposal_state.argtypes = [C.c_void_p, C.c_void_p, C.POINTER(C.c_float), C.POINTER(C.c_int64)]
     L.dr_mlp_forward.argtypes = [C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p]
     L.dr_mlp_gradient.argtypes = [C.c_void_p, C.c_void_p, C.c_void_p, C.c_int64, C.c_void_p, C.c_void_p, C.c_void_p]
+    L.dr_scene_get_tuning.argtypes = [C.c_void_p, C.POINTER(_abi.dr_tuning)]
+    L.dr_scene_set_tuning.argtypes = [C.c_void_p, C.POINTER(_abi.dr_tuning)]
+    L.dr_scene_autotune.argtypes = [C.c_void_p, C.POINTER(_abi.dr_render_desc), C.c_void_p, C.c_void_p, C.c_int,
+                                    C.POINTER(_abi.dr_tune_report), C.c_void_p]
     L.dr_last_error.restype = C.c_size_t
     for name in ("dr_scene_create", "dr_scene_update", "dr_scene_destroy", "dr_scene_grad_layout",
                  "dr_render_forward", "dr_render_backward", "dr_scene_last_launch_count", "dr_trace_rays",
                  "dr_scene_set_profiling", "dr_scene_last_timings", "dr_scene_last_counts", "dr_eval_math",
                  "dr_scene_edge_data", "dr_scene_last_work",
-                 "dr_set_item_queue_limit"):
+                 "dr_set_item_queue_limit", "dr_scene_get_tuning", "dr_scene_set_tuning", "dr_scene_autotune"):
         getattr(L, name).restype = C.c_int
     if L.dr_abi_version() != 2:
         raise ImportError("libdr_b200.so has an unexpected ABI version")

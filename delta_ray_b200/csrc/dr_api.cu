@@ -222,6 +222,7 @@ struct dr_scene {
         give_back_queues(device, std::move(queues));
     }
     int last_launches = 0;
+    dr_tuning tune{64, 3, 0};  // dr_scene_set_tuning
 };
 
 namespace {
@@ -567,6 +568,12 @@ long long max_queue_items() {
     long long l = g_item_queue_limit.load();
     return l > 0 ? l : kMaxQueueItems;
 }
+// the bound of one scene's calls: its tuned bound if it has one, and the
+// process-wide bound, whichever is smaller
+long long queue_limit(const dr_scene *scene) {
+    const long long l = max_queue_items(), t = scene->tune.queue_items;
+    return t > 0 && t < l ? t : l;
+}
 
 void check_backward_args(const dr_scene *scene, const dr_render_desc *rd, const float *d_image_dev,
                          const float *grad_dev) {
@@ -688,7 +695,7 @@ std::pair<long long, long long> run_backward(dr_scene *scene, const dr_render_de
         for (const FrontCall &f : *fronts) samples += (long long)f.rd.width * f.rd.height * f.rd.spp;
     }
     const bool stream_first = prop == nullptr && stats && stats->items_per_point > 0 &&
-                              (double)samples * stats->items_per_point > (double)max_queue_items();
+                              (double)samples * stats->items_per_point > (double)queue_limit(scene);
     for (int attempt = 0;; attempt++) {
         check_cuda(cudaMemsetAsync(ws.counters, 0, sizeof(BackwardCounters), st), "memset");
         check_cuda(cudaMemsetAsync(grad_dev, 0, sizeof(float) * (grad_len > 0 ? grad_len : scene->h.grad_total), st),
@@ -1034,7 +1041,7 @@ void backward_on_queues(dr_scene *scene, const dr_render_desc *rd, const DevScen
         }
     }
     long long cap_items =
-        std::min(max_queue_items(), std::max(q.cap_items, std::max<long long>(cap_points * 4, 1 << 16)));
+        std::min(queue_limit(scene), std::max(q.cap_items, std::max<long long>(cap_points * 4, 1 << 16)));
     q.counts.reserve(sizeof(BackwardCounters));
     if (!q.idle) check_cuda(cudaEventCreateWithFlags(&q.idle, cudaEventDisableTiming), "cudaEventCreate");
     // marks the queues busy up to here on every way out, errors included
@@ -1044,6 +1051,8 @@ void backward_on_queues(dr_scene *scene, const dr_render_desc *rd, const DevScen
         ~MarkIdle() { cudaEventRecord(e, st); }
     } mark_idle{q.idle, st};
     BackwardWorkspace ws{};
+    ws.hand_steps = scene->tune.hand_steps;
+    ws.task_rounds = scene->tune.task_rounds;
     auto bind_items = [&]() {
         q.items.reserve(sizeof(int4) * cap_items);
         q.item_w.reserve(sizeof(float) * cap_items);
@@ -1083,7 +1092,7 @@ void backward_on_queues(dr_scene *scene, const dr_render_desc *rd, const DevScen
     // the item queue grows to what the traversal reported, up to its limit
     // (the grown queue is kept for later calls)
     auto grow = [&](long long want) {
-        long long target = std::min(want, max_queue_items());
+        long long target = std::min(want, queue_limit(scene));
         if (target > cap_items) {
             cap_items = target;
             bind_items();
@@ -1122,6 +1131,100 @@ dr_status dr_render_backward(dr_scene *scene, const dr_render_desc *rd, const fl
         backward_on_queues(scene, rd, nullptr, d_image_dev, grad_dev, image_dev, st);
         collect_timings(scene, st);
     });
+}
+
+dr_status dr_scene_get_tuning(const dr_scene *scene, dr_tuning *out) {
+    return guard([&]() {
+        if (!scene || !out) throw DrError(DR_ERR_INVALID_ARGUMENT, "scene or out is NULL");
+        *out = scene->tune;
+    });
+}
+
+dr_status dr_scene_set_tuning(dr_scene *scene, const dr_tuning *tuning) {
+    return guard([&]() {
+        if (!scene || !tuning) throw DrError(DR_ERR_INVALID_ARGUMENT, "scene or tuning is NULL");
+        if (tuning->hand_steps < 1 || tuning->hand_steps > 4096 || tuning->task_rounds < 1 ||
+            tuning->task_rounds > 8 || tuning->queue_items < 0)
+            throw DrError(DR_ERR_INVALID_ARGUMENT, "tuning out of range (hand_steps 1..4096, task_rounds 1..8, "
+                                                   "queue_items >= 0)");
+        scene->tune = *tuning;
+    });
+}
+
+dr_status dr_scene_autotune(dr_scene *scene, const dr_render_desc *rd, const float *d_image_dev, float *grad_dev,
+                            int max_trials, dr_tune_report *report, void *stream) {
+    dr_tuning start{};
+    bool started = false;
+    dr_status status = guard([&]() {
+        check_backward_args(scene, rd, d_image_dev, grad_dev);
+        if (max_trials < 1) throw DrError(DR_ERR_INVALID_ARGUMENT, "max_trials must be positive");
+        check_cuda(cudaSetDevice(scene->device), "cudaSetDevice");
+        cudaStream_t st = (cudaStream_t)stream;
+        start = scene->tune;
+        started = true;
+        // one backward call under the scene's current setting, host wall time
+        // up to the end of its stream work (what a caller waits for)
+        auto run = [&]() {
+            check_cuda(cudaStreamSynchronize(st), "cudaStreamSynchronize");
+            const auto t0 = std::chrono::steady_clock::now();
+            scene->last_launches = 0;
+            backward_on_queues(scene, rd, nullptr, d_image_dev, grad_dev, nullptr, st);
+            check_cuda(cudaStreamSynchronize(st), "cudaStreamSynchronize");
+            return std::chrono::duration<float, std::milli>(std::chrono::steady_clock::now() - t0).count();
+        };
+        run();  // queues sized and edge counts kept for the chunk plans
+        int trials = 0;
+        auto time_of = [&](const dr_tuning &t) {
+            scene->tune = t;
+            trials++;
+            return std::min(run(), run());
+        };
+        dr_tuning best = start;
+        float best_ms = time_of(start);
+        const float start_ms = best_ms;
+        auto consider = [&](dr_tuning t) {
+            if (trials >= max_trials) return;
+            if (t.hand_steps == best.hand_steps && t.task_rounds == best.task_rounds &&
+                t.queue_items == best.queue_items)
+                return;
+            const float ms = time_of(t);
+            if (ms < best_ms) {
+                best_ms = ms;
+                best = t;
+            }
+        };
+        // the subtree stage's rounds and hand-on steps matter only where
+        // points hand subtrees to it
+        if (scene->last_work[4] > 0) {
+            for (int r : {1, 2, 3, 4}) {
+                dr_tuning t = best;
+                t.task_rounds = r;
+                consider(t);
+            }
+            if (best.task_rounds > 1)
+                for (int h : {16, 32, 64, 128, 256}) {
+                    dr_tuning t = best;
+                    t.hand_steps = h;
+                    consider(t);
+                }
+        }
+        // smaller item queues: more chunks, each one's queues nearer to L2
+        const long long base = std::min(max_queue_items(), std::max<long long>(scene->last_items, 1 << 16));
+        for (int d : {2, 4, 8}) {
+            dr_tuning t = best;
+            t.queue_items = std::max<long long>(base / d, 1 << 16);
+            consider(t);
+        }
+        scene->tune = best;
+        if (report) {
+            report->best = best;
+            report->best_ms = best_ms;
+            report->start_ms = start_ms;
+            report->trials = trials;
+        }
+    });
+    if (status != DR_OK && started) scene->tune = start;  // a failed search leaves the setting as it was
+    return status;
 }
 
 dr_status dr_render_backward_views(dr_scene *scene, int n_views, const dr_view_desc *views, float *grad_dev,

@@ -120,8 +120,6 @@ __global__ void __launch_bounds__(128, 6) k_edge_traverse(DevScene s, uint64_t s
 // walks them itself).  The node-keyed draws make the sampled edges the same
 // as those of the one-pass walk.
 #define DR_TASK_CUT 8
-// launches of the second stage per chunk (see k_edge_tasks)
-#define DR_TASK_ROUNDS 3
 #define DR_TASK_BUF 8
 template <bool PROP>
 __global__ void __launch_bounds__(128, 4) k_edge_expand(DevScene s, uint64_t seed, BackwardWorkspace ws) {
@@ -183,12 +181,11 @@ __device__ __forceinline__ long long next_task(unsigned long long *counter) {
     return (long long)(g.shfl(first, 0) + g.thread_rank());
 }
 
-// Rounds: the subtrees come from `in` (*in_n of them); with HAND, a walk
-// that has taken 64 steps with two or more subtrees pending hands the
-// shallowest one (the largest) to `hand_q` (*hand_n) for the next round, so that
-// no lane walks a long subtree alone at the end of the launch.  The last
-// round hands nothing on.
-#define DR_HAND_STEPS 64
+// Rounds (ws.task_rounds launches per chunk): the subtrees come from `in`
+// (*in_n of them); with HAND, a walk that has taken ws.hand_steps steps with
+// two or more subtrees pending hands the shallowest one (the largest) to
+// `hand_q` (*hand_n) for the next round, so that no lane walks a long subtree
+// alone at the end of the launch.  The last round hands nothing on.
 template <bool PROP, bool HAND>
 __global__ void __launch_bounds__(128, DR_TASKS_BLOCKS) k_edge_tasks(DevScene s, uint64_t seed, BackwardWorkspace ws,
                                                                    const EdgeTask *in, const unsigned long long *in_n,
@@ -221,7 +218,7 @@ __global__ void __launch_bounds__(128, DR_TASKS_BLOCKS) k_edge_tasks(DevScene s,
         }
         w.step(emit, nd, &visits);
         ok &= w.ok;
-        if (HAND && ++steps >= DR_HAND_STEPS && w.n >= 2) {
+        if (HAND && ++steps >= ws.hand_steps && w.n >= 2) {
             steps = 0;
             const unsigned long long slot = atomicAdd(hand_n, 1ull);
             if (slot < (unsigned long long)ws.cap_tasks) hand_q[slot] = w.take_bottom(point);
@@ -265,11 +262,12 @@ __device__ __forceinline__ void finish_item(const DevScene &s, const BackwardWor
 
 // Edge evaluation as a wavefront, each stage compacting what it keeps so that
 // the next runs with full warps.  k_edge_line: the line sample of every item
-// (silhouette test, LTC lobe, point on the edge); often half the items end
-// here (edges in the point's own plane, below the lobe's horizon or outside
-// the clipped segment).  The ray stage (k_edge_connect, k_edge_pairs): the two
-// rays of each survivor and the tests on their hits; with direct lighting
-// only, a sample neither of whose rays hits an emitter ends here too.
+// (silhouette test, LTC lobe, point on the edge) and the hits of its two rays
+// on the edge's own faces; often most items end here (edges in the point's
+// own plane, below the lobe's horizon or outside the clipped segment, rays
+// that miss both faces).  The ray stage (k_edge_connect, k_edge_pairs): the
+// occlusion of each survivor's rays and the tests on their hits; with direct
+// lighting only, a sample neither of whose rays hits an emitter ends here too.
 // k_edge_shade: the shading and the Jacobians of the rest.
 //
 // EXT: DR_FLAG_EDGE_LOBE_MIS or proposal training in use; GI: max_bounces > 1
@@ -287,7 +285,19 @@ __global__ void __launch_bounds__(128, 4) k_edge_line(DevScene s, uint64_t seed,
             int4 it = ws.items[i];
             PointRecord pt;
             pt.load(ws.pt + (size_t)it.x * DR_PT_WORDS);
-            ok = item_line<EXT>(s, pt, it.y >> 30, it.y & ((1 << 30) - 1), point_seed(ws, pt.view, seed), el);
+            const int tree = it.y >> 30, ei = it.y & ((1 << 30) - 1);
+            ok = item_line<EXT>(s, pt, tree, ei, point_seed(ws, pt.view, seed), el);
+            if (ok) {
+                // the connectivity test's first part: a sample neither of whose
+                // rays hits one of the edge's faces is connected on no side
+                // (three in four samples of a large mesh end here)
+                const DevEdge &edge = tree ? s.nrm_edges[ei] : s.sil_edges[ei];
+                float3 sdir, rdir, ldir;
+                edge_side_dirs(el, edge_v0(s, edge), edge_v1(s, edge), pt.p, sdir, rdir, ldir);
+                Hit fr, fl;
+                hit_faces_pair(s, edge, pt.p, rdir, ldir, 1e-3f, fr, fl);
+                ok = fr.tri >= 0 || fl.tri >= 0;
+            }
         }
         __syncwarp();
         unsigned long long slot = warp_reserve(&ws.counters->survivors, ok ? 1 : 0);
@@ -593,7 +603,7 @@ cudaError_t dr_launch_edge_traverse(const DevScene &s, uint64_t seed, const Back
         if (e != cudaSuccess) return e;
         // the subtrees in rounds: the first stage's, then those handed on
         // (ping-pong between the two queues); one round without a second queue
-        const int rounds = ws.tasks2 ? DR_TASK_ROUNDS : 1;
+        const int rounds = ws.tasks2 ? ws.task_rounds : 1;
         const EdgeTask *in = ws.tasks;
         const unsigned long long *in_n = &ws.counters->tasks;
         for (int r = 0; r < rounds; r++) {

@@ -147,6 +147,10 @@ struct BackwardWorkspace {
     // [cap_tasks] the second queue of the rounds of k_edge_tasks (null: one
     // round, no subtree handed on)
     EdgeTask *tasks2;
+    // the subtree walks of k_edge_tasks: steps a walk takes before it hands
+    // its shallowest pending subtree on, and launches (rounds) per chunk of
+    // points (the scene's tuning, dr_scene_set_tuning)
+    int hand_steps = 64, task_rounds = 3;
     // per view of a batched multi-view call (null: the call's own settings);
     // each point's settings are views[point.view]
     const ViewParams *views;

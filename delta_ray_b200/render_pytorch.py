@@ -155,6 +155,39 @@ class Scene:
                 C.c_void_p(img.data_ptr()) if img is not None else None, self._stream()))
         return grad, img
 
+    def tuning(self):
+        """The scene's queue settings (dr_scene_get_tuning): hand_steps,
+        task_rounds, queue_items."""
+        t = _abi.dr_tuning()
+        _lib.check(_lib.lib().dr_scene_get_tuning(self.handle, C.byref(t)))
+        return {"hand_steps": t.hand_steps, "task_rounds": t.task_rounds, "queue_items": t.queue_items}
+
+    def set_tuning(self, hand_steps=64, task_rounds=3, queue_items=0):
+        """Sets the scene's queue settings (dr_scene_set_tuning); the
+        defaults are the library's."""
+        t = _abi.dr_tuning(int(hand_steps), int(task_rounds), int(queue_items))
+        _lib.check(_lib.lib().dr_scene_set_tuning(self.handle, C.byref(t)))
+
+    def autotune(self, width, height, spp, max_bounces, seed, d_image, opts=None, max_trials=16):
+        """Times backward calls of this render under several queue settings
+        and keeps the fastest on the scene (dr_scene_autotune).  Returns the
+        chosen setting with best_ms, start_ms and trials."""
+        opts = opts or RenderOptions()
+        d_image = d_image.detach().to(device=self.device, dtype=torch.float32).contiguous()
+        if tuple(d_image.shape) != (height, width, 3):
+            raise ValueError(f"d_image must be [{height}, {width}, 3]")
+        grad = torch.empty(self.grad_total, dtype=torch.float32, device=self.device)
+        rd = _abi.render_desc(width, height, spp, max_bounces, seed, opts.primary_edge_samples, opts.dp_mode,
+                              opts.flags)
+        rep = _abi.dr_tune_report()
+        with torch.cuda.device(self.device_index):
+            _lib.check(_lib.lib().dr_scene_autotune(self.handle, C.byref(rd), C.c_void_p(d_image.data_ptr()),
+                                                    C.c_void_p(grad.data_ptr()), int(max_trials), C.byref(rep),
+                                                    self._stream()))
+        b = rep.best
+        return {"hand_steps": b.hand_steps, "task_rounds": b.task_rounds, "queue_items": b.queue_items,
+                "best_ms": rep.best_ms, "start_ms": rep.start_ms, "trials": rep.trials}
+
     def backward_views(self, views, opts=None):
         """Backward render of several views in one call.  views: a list of
         dicts with keys camera (a Camera or a scene_dicts camera dict),
@@ -234,7 +267,9 @@ class Scene:
 
     def last_work(self):
         """Work counts of the last backward call (dr_scene_last_work): points,
-        items, ray survivors, shaded samples, subtree tasks, first-stage items,
+        items, line samples passed to the ray stage (for large meshes: those
+        whose rays hit one of the edge's faces), shaded samples, subtree tasks,
+        first-stage items,
         node visits of the point walks and of the subtree walks, candidates of
         the ray stage (samples that passed its connectivity test)."""
         w = (C.c_int64 * 9)()

@@ -276,6 +276,52 @@ DR_API dr_status dr_render_backward_noalloc(dr_scene *scene, const dr_render_des
  * renderer evaluates each edge as it samples it. */
 DR_API dr_status dr_set_item_queue_limit(int64_t items);
 
+/* A scene's queue settings for its backward calls (no counterpart in the
+ * reference, whose CPU renderer has no work queues).
+ *   hand_steps: node steps a subtree walk of the second traversal stage takes
+ *     before it hands its shallowest pending subtree on to the next round
+ *     (1..4096; default 64);
+ *   task_rounds: launches of that stage per chunk of shading points, the last
+ *     handing nothing on (1..8; default 3);
+ *   queue_items: bound on the edge items the scene's calls hold at once (0,
+ *     the default: the process-wide bound of dr_set_item_queue_limit; else
+ *     the smaller of the two).
+ * No setting changes which edges are sampled or what they contribute: the
+ * counts and the image are the same under every setting, the gradient up to
+ * float round-off (atomic adds sum in another order). */
+typedef struct {
+    int32_t hand_steps;
+    int32_t task_rounds;
+    int64_t queue_items;
+} dr_tuning;
+
+DR_API dr_status dr_scene_get_tuning(const dr_scene *scene, dr_tuning *out);
+/* Out-of-range values fail with DR_ERR_INVALID_ARGUMENT. */
+DR_API dr_status dr_scene_set_tuning(dr_scene *scene, const dr_tuning *tuning);
+
+/* What dr_scene_autotune measured: the setting it chose, its time per
+ * backward call, the time of the setting the scene had before (ms, host wall
+ * time to the end of the call's stream work) and the settings it timed. */
+typedef struct {
+    dr_tuning best;
+    float best_ms;
+    float start_ms;
+    int32_t trials;
+} dr_tune_report;
+
+/* Chooses the scene's queue settings by timing backward calls of this render
+ * (arguments as dr_render_backward; grad_dev holds the last call's gradient
+ * afterwards).  Coordinate search from the current setting: subtree rounds
+ * 1-4, then hand-on steps 16-256 (only where points hand subtrees on), then
+ * item-queue bounds of 1/2, 1/4 and 1/8 of the last call's items (smaller
+ * chunks of the edge stage, whose queues sit nearer to L2); each setting
+ * timed as the faster of two calls, at most max_trials settings.  The fastest
+ * stays set on the scene, so calls of the same kind (an inverse-rendering
+ * loop) can be tuned once, before the loop.  report may be NULL.  On failure
+ * the scene keeps the setting it had. */
+DR_API dr_status dr_scene_autotune(dr_scene *scene, const dr_render_desc *rd, const float *d_image_dev,
+                                   float *grad_dev, int max_trials, dr_tune_report *report, void *stream);
+
 /* Closest hits of n rays [n][6] (origin, direction; device memory) on
  * (1e-3, inf): global triangle id (-1 on a miss; ids run over shapes in
  * order, then triangles) and distance.  Replaces the reference's
@@ -322,10 +368,12 @@ DR_API dr_status dr_scene_edge_data(const dr_scene *scene, int what, void *out_h
 
 /* Tooling: work counts of the last backward call (the inputs of a byte model
  * of its kernels; no counterpart in the reference): counts[0] shading points,
- * [1] sampled edges, [2] line samples kept for their rays, [3] samples kept
- * for shading, [4] subtrees walked by the second traversal stage (handed
- * on by the first stage or between the second stage's rounds), [5] edges sampled by the first stage (all, when the traversal runs
- * in one stage), [6] edge-tree nodes visited by the point walks, [7] nodes
+ * [1] sampled edges, [2] line samples kept for their rays (in scenes
+ * traced through the LBVH: those whose rays hit one of the edge's faces),
+ * [3] samples kept for shading, [4] subtrees walked by the second traversal
+ * stage (handed on by the first stage or between the second stage's rounds),
+ * [5] edges sampled by the first stage (all, when the traversal runs in one
+ * stage), [6] edge-tree nodes visited by the point walks, [7] nodes
  * visited by the subtree walks, [8] line samples whose connectivity test
  * passed (candidates of the ray stage).  Up to n of them are written. */
 DR_API dr_status dr_scene_last_work(const dr_scene *scene, int64_t *counts, int n);
