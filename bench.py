@@ -207,6 +207,14 @@ def kernel_bytes(kernel, wl, work):
     if kernel == "k_edge_tasks":
         return (work["tasks"] * (24 + POINT_BYTES) + (I - work["items_first_stage"]) * 20 +
                 work["visits_tasks"] * NODE_BYTES)
+    # the level walk of the same subtrees: the points' contexts, the subtrees'
+    # nodes, the items of their leaves
+    if kernel == "k_walk_ctx":
+        return P * POINT_BYTES
+    if kernel == "k_edge_level":
+        return work["tasks"] * 24 + work["visits_tasks"] * NODE_BYTES
+    if kernel == "k_edge_leaves":
+        return (I - work["items_first_stage"]) * 20
     if kernel == "k_edge_line":  # item, point record, LTC matrix, material; survivor record out
         return I * (20 + POINT_BYTES + 36 + 28) + work["survivors"] * 32
     if kernel == "k_edge_connect":  # survivor in, the two rays' connectivity, candidate record out

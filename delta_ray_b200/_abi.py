@@ -93,7 +93,8 @@ class dr_view_desc(C.Structure):
 
 
 class dr_tuning(C.Structure):
-    _fields_ = [("hand_steps", C.c_int32), ("task_rounds", C.c_int32), ("queue_items", C.c_int64)]
+    _fields_ = [("hand_steps", C.c_int32), ("task_rounds", C.c_int32), ("queue_items", C.c_int64),
+                ("depth_first", C.c_int32), ("reserved", C.c_int32)]
 
 
 class dr_tune_report(C.Structure):

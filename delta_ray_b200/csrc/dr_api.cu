@@ -97,6 +97,7 @@ struct EdgeStats {
 
 struct BackwardQueues {
     DevBuf pt, items, item_w, item_dp, pt_last, pt_items, counts, survivors, hits, side_rad, tasks, tasks2;
+    DevBuf walk_ctx, leafq;  // the level walk of the subtrees
     long long cap_items = 0;     // grown on overflow, kept with the buffers
     double points_per_sample = 1;  // shading points per pixel sample the last overflow asked for
     EdgeStats stats;
@@ -200,7 +201,7 @@ struct dr_scene {
     // for rays, samples kept for shading, handed-on subtrees, items of the
     // first traversal stage, edge-tree nodes visited by the point walks and by
     // the subtree walks
-    long long last_work[9] = {};
+    long long last_work[10] = {};
     int num_vertices = 0, num_tris = 0, num_sms = 148;
     int bvh_built_tris = 0;  // triangle count of the LBVH topology kept in bvh_scratch
     // scenes of more than kGpuEdgeTris triangles build their edges, edge trees
@@ -222,7 +223,7 @@ struct dr_scene {
         give_back_queues(device, std::move(queues));
     }
     int last_launches = 0;
-    dr_tuning tune{64, 3, 0};  // dr_scene_set_tuning
+    dr_tuning tune{64, 3, 0, 0, 0};  // dr_scene_set_tuning
 };
 
 namespace {
@@ -527,8 +528,10 @@ void collect_timings(dr_scene *sc, cudaStream_t st) {
 // Edge trees above this many nodes are walked in two stages (k_edge_expand,
 // k_edge_tasks): their points' walks are long and uneven.
 constexpr int kSplitTraversalNodes = 4096;
-// Task queue of the two-stage walk: up to 64 subtrees per point, at most 1 GiB.
-constexpr long long kTasksPerPoint = 64, kMaxTasks = (1ll << 30) / sizeof(EdgeTask);
+// Queues of the two-stage walk (the first stage's subtrees, each level's nodes
+// in two halves by class, the leaves): up to 128 entries per point, at most
+// 4 GiB each; a node that finds no room is walked depth first by its lane.
+constexpr long long kTasksPerPoint = 128, kMaxTasks = (4ll << 30) / sizeof(EdgeTask);
 
 // The scene's device view with this call's per-render settings.
 DevScene call_scene(const dr_scene *sc, const dr_render_desc *rd) {
@@ -563,6 +566,9 @@ void check_render_desc(const dr_scene *sc, const dr_render_desc *rd) {
 // the item, its weight, its dp and its slot in the survivor queue of the
 // evaluation wavefront).  Edge stages with more items stream.
 constexpr long long kMaxQueueItems = (8ll << 30) / 64;
+// the first call's probe of the edge counts (run_backward): every 16th point,
+// in calls of at least 2^20 pixel samples
+constexpr long long kProbeStride = 16, kProbeMinSamples = 1ll << 20;
 std::atomic<long long> g_item_queue_limit{0};  // dr_set_item_queue_limit (0: kMaxQueueItems)
 long long max_queue_items() {
     long long l = g_item_queue_limit.load();
@@ -634,7 +640,7 @@ std::pair<long long, long long> run_backward(dr_scene *scene, const dr_render_de
         if (c.status & ~(DR_STATUS_ITEM_OVERFLOW | DR_STATUS_POINT_OVERFLOW))
             throw DrError(DR_ERR_DEVICE_STATUS, "device reported status " + std::to_string(c.status));
     };
-    long long work[9] = {};
+    long long work[10] = {};
     // with the DR_DEBUG_SYNC diagnostic, a launch error names the kernel that failed
     auto check_launch = [&](cudaError_t e, const char *what) {
         if (e != cudaSuccess && timer->failed)
@@ -696,6 +702,12 @@ std::pair<long long, long long> run_backward(dr_scene *scene, const dr_render_de
     }
     const bool stream_first = prop == nullptr && stats && stats->items_per_point > 0 &&
                               (double)samples * stats->items_per_point > (double)queue_limit(scene);
+    // a scene's first call of many samples (no edge counts yet) first walks
+    // every kProbeStride-th point only: their edge counts forecast the
+    // others', and a call whose forecast overflows the queue streams from
+    // that forecast instead of walking every point once to count its edges
+    const bool probe = !stream_first && prop == nullptr && stats && stats->items_per_point <= 0 && ws.pt_items &&
+                       samples >= kProbeMinSamples;
     for (int attempt = 0;; attempt++) {
         check_cuda(cudaMemsetAsync(ws.counters, 0, sizeof(BackwardCounters), st), "memset");
         check_cuda(cudaMemsetAsync(grad_dev, 0, sizeof(float) * (grad_len > 0 ? grad_len : scene->h.grad_total), st),
@@ -715,7 +727,7 @@ std::pair<long long, long long> run_backward(dr_scene *scene, const dr_render_de
             check_launch(dr_launch_backward_front(ds, rd->width, rd->height, rd->spp, rd->max_bounces, rd->seed,
                                                   d_image_dev, grad_dev, image_dev, rd->primary_edge_samples,
                                                   rd->dp_mode, ws, cfg, scene->num_sms, st, &scene->last_launches,
-                                                  timer, prop == nullptr && !stream_first),
+                                                  timer, prop == nullptr && !stream_first && !probe),
                          "backward launch");
         }
         read();
@@ -726,8 +738,25 @@ std::pair<long long, long long> run_backward(dr_scene *scene, const dr_render_de
                                                     std::to_string(ws.cap_points) + ")");
     }
     const long long P = std::min((long long)c.points, ws.cap_points);
-    if (fronts && !stream_first) {
-        // the views' points walked together
+    bool probe_streams = false;
+    long long probe_needed = 0;
+    if (probe) {
+        timer->mark(st, "host_point_count");
+        check_cuda(cudaMemsetAsync(ws.pt_items, 0, sizeof(int) * (size_t)std::max(P, 1ll), st), "memset");
+        ws.pt_stride = kProbeStride;
+        check_launch(dr_launch_edge_traverse(ds, rd->seed, ws, scene->num_sms, st, &scene->last_launches, timer),
+                     "edge traversal launch");
+        read();
+        ws.pt_stride = 1;
+        // the items counter counts past the queue's end
+        probe_needed = (long long)c.items * kProbeStride;
+        probe_streams = (double)probe_needed > 0.8 * (double)queue_limit(scene);
+        check_cuda(cudaMemsetAsync(&ws.counters->items, 0, 16, st), "memset");
+        check_cuda(cudaMemsetAsync(&ws.counters->tasks, 0, sizeof(unsigned long long), st), "memset");
+    }
+    if ((fronts && !stream_first) || (probe && !probe_streams)) {
+        // the views' points walked together (or every point after a probe
+        // that forecast room for all of their edges)
         timer->mark(st, "host_point_count");
         check_launch(dr_launch_edge_traverse(ds, rd->seed, ws, scene->num_sms, st, &scene->last_launches, timer),
                      "edge traversal launch");
@@ -772,7 +801,7 @@ std::pair<long long, long long> run_backward(dr_scene *scene, const dr_render_de
     }
     long long items = 0;
     bool streamed = false;
-    if (!stream_first && !(c.status & DR_STATUS_ITEM_OVERFLOW)) {
+    if (!stream_first && !probe_streams && !(c.status & DR_STATUS_ITEM_OVERFLOW)) {
         timer->mark(st, "host_queue_check");
         back();
         items = (long long)c.items;
@@ -785,7 +814,12 @@ std::pair<long long, long long> run_backward(dr_scene *scene, const dr_render_de
         std::vector<unsigned long long> b;
         double scale = 1, margin = 0.85;
         long long needed;
-        if (!stream_first) {
+        if (probe_streams) {
+            // the probe's counts, every kProbeStride-th point's
+            read_buckets(P, b);
+            scale = (double)kProbeStride;
+            needed = probe_needed;
+        } else if (!stream_first) {
             needed = (long long)c.items;
             if (ws.pt_items && stats) {
                 read_buckets(P, b);
@@ -884,6 +918,7 @@ std::pair<long long, long long> run_backward(dr_scene *scene, const dr_render_de
     work[1] = items;
     work[6] = (long long)c.visits_walk;
     work[7] = (long long)c.visits_tasks;
+    work[9] = (long long)c.spilled;
     std::memcpy(scene->last_work, work, sizeof(work));
     return {P, items};
 }
@@ -940,9 +975,11 @@ dr_status dr_scene_create(const dr_scene_desc *desc, int device, dr_scene **out)
         sc->h.preprocess(!sc->gpu_edges);
         sc->last_launches = 0;
         upload_scene(sc.get(), 0);
-        // loads the module holding the no-alloc backward's scratch array now,
-        // so that a later no-alloc call on this device takes no memory
+        // loads the module holding the no-alloc backward's scratch array and
+        // the kernels a backward call launches now, so that a later no-alloc
+        // call on this device takes no memory
         noalloc_scratch();
+        check_cuda(dr_preload_backward_kernels(), "kernel preload");
         *out = sc.release();
     });
 }
@@ -1053,6 +1090,8 @@ void backward_on_queues(dr_scene *scene, const dr_render_desc *rd, const DevScen
     BackwardWorkspace ws{};
     ws.hand_steps = scene->tune.hand_steps;
     ws.task_rounds = scene->tune.task_rounds;
+    ws.level_walk = scene->tune.depth_first ? 0 : 1;
+    const bool split = view ? view->split_traversal : call_scene(scene, rd).split_traversal;
     auto bind_items = [&]() {
         q.items.reserve(sizeof(int4) * cap_items);
         q.item_w.reserve(sizeof(float) * cap_items);
@@ -1076,18 +1115,27 @@ void backward_on_queues(dr_scene *scene, const dr_render_desc *rd, const DevScen
         ws.pt_last = q.pt_last.as<unsigned long long>();
         q.pt_items.reserve(sizeof(int) * cap_points);
         ws.pt_items = q.pt_items.as<int>();
+        if (split && ws.level_walk) {
+            q.walk_ctx.reserve(sizeof(float4) * DR_CTX_F4 * cap_points);
+            ws.walk_ctx = q.walk_ctx.as<float4>();
+        }
         ws.cap_points = cap_points;
     };
     bind_points();
     ws.counters = q.counts.as<BackwardCounters>();
     bind_items();
-    if (view ? view->split_traversal : call_scene(scene, rd).split_traversal) {
+    if (split) {
         long long cap_tasks = std::min(kMaxTasks, std::max(1ll << 16, kTasksPerPoint * cap_points));
         q.tasks.reserve(sizeof(EdgeTask) * cap_tasks);
         q.tasks2.reserve(sizeof(EdgeTask) * cap_tasks);
         ws.tasks = q.tasks.as<EdgeTask>();
         ws.tasks2 = q.tasks2.as<EdgeTask>();
         ws.cap_tasks = cap_tasks;
+        if (ws.level_walk) {
+            q.leafq.reserve(sizeof(EdgeTask) * cap_tasks);
+            ws.leafq = q.leafq.as<EdgeTask>();
+            ws.cap_leaves = cap_tasks;
+        }
     }
     // the item queue grows to what the traversal reported, up to its limit
     // (the grown queue is kept for later calls)
@@ -1144,9 +1192,10 @@ dr_status dr_scene_set_tuning(dr_scene *scene, const dr_tuning *tuning) {
     return guard([&]() {
         if (!scene || !tuning) throw DrError(DR_ERR_INVALID_ARGUMENT, "scene or tuning is NULL");
         if (tuning->hand_steps < 1 || tuning->hand_steps > 4096 || tuning->task_rounds < 1 ||
-            tuning->task_rounds > 8 || tuning->queue_items < 0)
+            tuning->task_rounds > 8 || tuning->queue_items < 0 || tuning->depth_first < 0 ||
+            tuning->depth_first > 1 || tuning->reserved != 0)
             throw DrError(DR_ERR_INVALID_ARGUMENT, "tuning out of range (hand_steps 1..4096, task_rounds 1..8, "
-                                                   "queue_items >= 0)");
+                                                   "queue_items >= 0, depth_first 0 or 1, reserved 0)");
         scene->tune = *tuning;
     });
 }
@@ -1185,7 +1234,7 @@ dr_status dr_scene_autotune(dr_scene *scene, const dr_render_desc *rd, const flo
         auto consider = [&](dr_tuning t) {
             if (trials >= max_trials) return;
             if (t.hand_steps == best.hand_steps && t.task_rounds == best.task_rounds &&
-                t.queue_items == best.queue_items)
+                t.queue_items == best.queue_items && t.depth_first == best.depth_first)
                 return;
             const float ms = time_of(t);
             if (ms < best_ms) {
@@ -1193,15 +1242,21 @@ dr_status dr_scene_autotune(dr_scene *scene, const dr_render_desc *rd, const flo
                 best = t;
             }
         };
-        // the subtree stage's rounds and hand-on steps matter only where
-        // points hand subtrees to it
+        // the subtree stage's walk, and for the depth-first one its rounds
+        // and hand-on steps, matter only where points hand subtrees to it
         if (scene->last_work[4] > 0) {
-            for (int r : {1, 2, 3, 4}) {
+            for (int d : {0, 1}) {
                 dr_tuning t = best;
-                t.task_rounds = r;
+                t.depth_first = d;
                 consider(t);
             }
-            if (best.task_rounds > 1)
+            if (best.depth_first)
+                for (int r : {1, 2, 3, 4}) {
+                    dr_tuning t = best;
+                    t.task_rounds = r;
+                    consider(t);
+                }
+            if (best.depth_first && best.task_rounds > 1)
                 for (int h : {16, 32, 64, 128, 256}) {
                     dr_tuning t = best;
                     t.hand_steps = h;
@@ -1592,7 +1647,7 @@ dr_status dr_scene_edge_data(const dr_scene *scene, int what, void *out_host, in
 dr_status dr_scene_last_work(const dr_scene *scene, int64_t *counts, int n) {
     return guard([&]() {
         if (!scene || !counts || n < 0) throw DrError(DR_ERR_INVALID_ARGUMENT, "NULL argument");
-        for (int i = 0; i < n && i < 9; i++) counts[i] = scene->last_work[i];
+        for (int i = 0; i < n && i < 10; i++) counts[i] = scene->last_work[i];
     });
 }
 

@@ -182,3 +182,19 @@ cudaError_t dr_launch_backward_back(const DevScene &s, int W, int H, int spp, in
     }
     return cudaGetLastError();
 }
+
+// Loads every kernel a backward call can launch (see dr_preload_edge_kernels).
+cudaError_t dr_preload_backward_kernels() {
+    const void *k[] = {
+        (const void *)k_backward_paths<true, 1>, (const void *)k_backward_paths<true, DR_MAX_BOUNCES>,
+        (const void *)k_backward_paths<true, -16>, (const void *)k_backward_paths<false, 1>,
+        (const void *)k_backward_paths<false, DR_MAX_BOUNCES>, (const void *)k_backward_paths<false, -16>,
+        (const void *)k_dp_propagate<true>, (const void *)k_dp_propagate<false>,
+    };
+    for (const void *f : k) {
+        cudaFuncAttributes a;
+        const cudaError_t e = cudaFuncGetAttributes(&a, f);
+        if (e != cudaSuccess) return e;
+    }
+    return dr_preload_edge_kernels();
+}

@@ -77,6 +77,13 @@ __device__ __forceinline__ EdgeProposal point_proposal(const BackwardWorkspace &
     return pr;
 }
 
+// The points a traversal launch walks: pt_begin, pt_begin + pt_stride, ...
+// below min(pt_end, the points the path stage pushed); returns their number.
+__device__ __forceinline__ long long strided_points(const BackwardWorkspace &ws) {
+    const long long n = min(min((long long)ws.counters->points, ws.cap_points), ws.pt_end);
+    return n > ws.pt_begin ? (n - ws.pt_begin + ws.pt_stride - 1) / ws.pt_stride : 0;
+}
+
 // One thread per shading point in [pt_begin, pt_end) walks the point's trees
 // (small trees: every point's walk is short).
 // Adds each warp's node-visit count to a counter (every lane calls it).
@@ -88,15 +95,15 @@ __device__ __forceinline__ void add_visits(unsigned long long *counter, int visi
 
 template <bool PROP>
 __global__ void __launch_bounds__(128, 6) k_edge_traverse(DevScene s, uint64_t seed, BackwardWorkspace ws) {
-    long long n = min(min((long long)ws.counters->points, ws.cap_points), ws.pt_end);
+    const long long m = strided_points(ws);
     long long stride = (long long)gridDim.x * blockDim.x;
     ItemWriter out(ws);
     int visits = 0;
     // warp-uniform loop: every lane of a warp takes the same number of trips
-    for (long long base = ws.pt_begin + (long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < n;
-         base += stride) {
-        long long p = base + (threadIdx.x & 31);
-        if (p < n) {
+    for (long long base = (long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < m; base += stride) {
+        const long long k = base + (threadIdx.x & 31);
+        const long long p = ws.pt_begin + k * ws.pt_stride;
+        if (k < m) {
             PointRecord pt;
             pt.load(ws.pt + (size_t)p * DR_PT_WORDS);
             int cnt = 0;
@@ -123,14 +130,14 @@ __global__ void __launch_bounds__(128, 6) k_edge_traverse(DevScene s, uint64_t s
 #define DR_TASK_BUF 8
 template <bool PROP>
 __global__ void __launch_bounds__(128, 4) k_edge_expand(DevScene s, uint64_t seed, BackwardWorkspace ws) {
-    long long n = min(min((long long)ws.counters->points, ws.cap_points), ws.pt_end);
+    const long long m = strided_points(ws);
     long long stride = (long long)gridDim.x * blockDim.x;
     ItemWriter out(ws);
     int visits = 0;
-    for (long long base = ws.pt_begin + (long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < n;
-         base += stride) {
-        long long p = base + (threadIdx.x & 31);
-        if (p < n) {
+    for (long long base = (long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < m; base += stride) {
+        const long long k = base + (threadIdx.x & 31);
+        const long long p = ws.pt_begin + k * ws.pt_stride;
+        if (k < m) {
             PointRecord pt;
             pt.load(ws.pt + (size_t)p * DR_PT_WORDS);
             const EdgeProposal pr = point_proposal(ws, p);
@@ -226,6 +233,306 @@ __global__ void __launch_bounds__(128, DR_TASKS_BLOCKS) k_edge_tasks(DevScene s,
     }
     if (!ok) set_status(&ws.counters->status, DR_STATUS_STACK_OVERFLOW);
     out.flush_warp();
+    add_visits(&ws.counters->visits_tasks, visits);
+}
+
+// ---------------------------------------------------------------------------
+// The subtrees walked level by level.  Each launch of k_edge_level takes one
+// level of nodes of every handed-on subtree (a queue of EdgeTask, one node of
+// one point's walk each), decides their children exactly as the depth-first
+// walk does (node_children) and queues the children it walks: interior ones
+// for the next level, leaves for k_edge_leaves.  Every lane of a warp works on
+// a node of the same kind at the same point of the code (the depth-first
+// walk's lanes ran 8-10 of 32 on average: leaves, interior nodes, task fetches
+// and hand-offs in one loop), and no walk stack is kept.  What a node's
+// decision needs of its shading point comes from the point's walk context
+// (k_walk_ctx, 176 B), read from L2.  The node draws are keyed by node, so
+// the sampled edges are those of the depth-first walk.
+
+// Walk context of one point, DR_CTX_F4 float4: 0-4 the bound context (p, n,
+// the frame around wi, the normal in it), 5 roughness, exponent, model, the
+// light cone's cosine, 6 the cone's axis and the learned-descent flag,
+// 7 the node draws' key (sample id, bounce) and the view, 8-10 the shading
+// frame (the proposal's direction bins).
+
+template <bool PROP>
+__global__ void __launch_bounds__(128, 8) k_walk_ctx(DevScene s, uint64_t seed, BackwardWorkspace ws) {
+    const long long m = strided_points(ws);
+    for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < m;
+         k += (long long)gridDim.x * blockDim.x) {
+        const long long p = ws.pt_begin + k * ws.pt_stride;
+        PointRecord pt;
+        pt.load(ws.pt + (size_t)p * DR_PT_WORDS);
+        // as start_point_task / start_subtree
+        const SurfacePoint sp = pt.surface();
+        const DevMaterial &mt = s.mats[material_of_tri(s, pt.tri)];
+        const float dl = luminance(get_kd(s, mt, sp.uv)), sl = luminance(get_ks(s, mt, sp.uv));
+        const float rough = get_rough(s, mt, sp.uv);
+        const BoundCtx bc = bound_ctx(pt.wi, sp, dl, sl, rough, mt.model);
+        const ConeSpec cone = light_cone(s, pt.light, sp.p);
+        float learned = 0.f;
+        if constexpr (PROP) {
+            NodeRng r;
+            r.seed = point_seed(ws, pt.view, seed);
+            r.sid = pt.sid;
+            r.bounce = (uint32_t)pt.bounce;
+            learned = r.draw(1, DR_NODE_MIX_DRAW) < ws.proposal_alpha ? 1.f : 0.f;
+        }
+        const bool lobe = sl > 0.f;  // the frame around wi is set only with a specular lobe
+        const Frame hf = lobe ? bc.hf : Frame{f3(0.f), f3(0.f), f3(0.f)};
+        const float3 ln = lobe ? bc.ln : f3(0.f);
+        float4 *o = ws.walk_ctx + (size_t)p * DR_CTX_F4;
+        o[0] = make_float4(bc.p.x, bc.p.y, bc.p.z, bc.n.x);
+        o[1] = make_float4(bc.n.y, bc.n.z, bc.dl, bc.sl);
+        o[2] = make_float4(hf.t.x, hf.t.y, hf.t.z, hf.b.x);
+        o[3] = make_float4(hf.b.y, hf.b.z, hf.n.x, hf.n.y);
+        o[4] = make_float4(hf.n.z, ln.x, ln.y, ln.z);
+        o[5] = make_float4(bc.rough, bc.expo, __int_as_float(bc.model), cone.cos_angle);
+        o[6] = make_float4(cone.d.x, cone.d.y, cone.d.z, learned);
+        o[7] = make_float4(__uint_as_float((uint32_t)pt.sid), __uint_as_float((uint32_t)(pt.sid >> 32)),
+                           __uint_as_float((uint32_t)pt.bounce), __int_as_float(pt.view));
+        if constexpr (PROP) {
+            o[8] = make_float4(sp.f.t.x, sp.f.t.y, sp.f.t.z, sp.f.b.x);
+            o[9] = make_float4(sp.f.b.y, sp.f.b.z, sp.f.n.x, sp.f.n.y);
+            o[10] = make_float4(sp.f.n.z, 0.f, 0.f, 0.f);
+        }
+    }
+}
+
+// A point's walk context: what node_children needs (`f` only with PROP).
+struct WalkPoint {
+    BoundCtx bc;
+    ConeSpec cone;
+    NodeRng rng;
+    Frame f;
+    bool learned;
+};
+template <bool PROP>
+__device__ __forceinline__ WalkPoint load_walk_point(const BackwardWorkspace &ws, int point, uint64_t seed) {
+    const float4 *c = ws.walk_ctx + (size_t)point * DR_CTX_F4;
+    const float4 a = c[0], b = c[1], d2 = c[2], d3 = c[3], d4 = c[4], d5 = c[5], d6 = c[6], d7 = c[7];
+    WalkPoint w;
+    w.bc.p = f3(a.x, a.y, a.z);
+    w.bc.n = f3(a.w, b.x, b.y);
+    w.bc.dl = b.z;
+    w.bc.sl = b.w;
+    w.bc.hf.t = f3(d2.x, d2.y, d2.z);
+    w.bc.hf.b = f3(d2.w, d3.x, d3.y);
+    w.bc.hf.n = f3(d3.z, d3.w, d4.x);
+    w.bc.ln = f3(d4.y, d4.z, d4.w);
+    w.bc.rough = d5.x;
+    w.bc.expo = d5.y;
+    w.bc.model = __float_as_int(d5.z);
+    w.cone.o = w.bc.p;
+    w.cone.d = f3(d6.x, d6.y, d6.z);
+    w.cone.cos_angle = d5.w;
+    w.learned = d6.w != 0.f;
+    w.rng.sid = (uint64_t)__float_as_uint(d7.x) | ((uint64_t)__float_as_uint(d7.y) << 32);
+    w.rng.bounce = __float_as_uint(d7.z);
+    w.rng.seed = point_seed(ws, __float_as_int(d7.w), seed);
+    if constexpr (PROP) {
+        const float4 f8 = c[8], f9 = c[9], f10 = c[10];
+        w.f.t = f3(f8.x, f8.y, f8.z);
+        w.f.b = f3(f8.w, f9.x, f9.y);
+        w.f.n = f3(f9.z, f9.w, f10.x);
+    } else {
+        w.f.t = w.f.b = w.f.n = f3(0.f);
+    }
+    return w;
+}
+
+template <bool PROP> __device__ __forceinline__ EdgeTask child_task(int point, int hi, const EdgeItem<PROP> &c) {
+    EdgeTask t;
+    t.point = point;
+    t.code = c.node | hi;
+    t.bb = c.bb;
+    t.cpmf = c.cpmf;
+    t.apmf = c.apmf;
+    t.lpmf = 0.f;
+    if constexpr (PROP) t.lpmf = c.lpmf;
+    return t;
+}
+
+// A subtree that found no room in a level's queue: the lane walks it depth
+// first (its items through `spill`).  Out of line: the rare path keeps its
+// registers and stack to itself.
+template <bool PROP>
+__device__ __noinline__ void walk_here(const DevScene &s, uint64_t seed, const BackwardWorkspace &ws, const EdgeTask &t,
+                          ItemWriter &spill, int *visits, bool &ok) {
+    PointRecord pt;
+    pt.load(ws.pt + (size_t)t.point * DR_PT_WORDS);
+    int cnt = 0;
+    auto emit = [&](int tree, int ei, int j, float w, int code) {
+        spill.add(t.point, tree, ei, j, w, code);
+        cnt++;
+    };
+    ok &= traverse_point_task<PROP>(s, pt, point_seed(ws, pt.view, seed), t, emit, point_proposal(ws, t.point),
+                                    visits);
+    if (cnt > 0 && ws.pt_items) atomicAdd(ws.pt_items + t.point, cnt);
+    atomicAdd(&ws.counters->spilled, 1ull);
+}
+
+// The class of a node in the level queues: 0 for nodes whose decision takes
+// the exact bounds and the cone tests (the cone walk's, and the all walk's on
+// the cone walk's path), 1 for the all walk's others (filtered bounds, no cone
+// tests).  Each class fills its own half of a queue, so that a warp's lanes
+// mostly run the same code.
+template <bool PROP> __device__ __forceinline__ int node_class(int mode, const EdgeItem<PROP> &c) {
+    return (mode == 0 || c.cpmf != 0.f) ? 0 : 1;
+}
+
+#ifndef DR_LEVEL_BLOCKS
+#define DR_LEVEL_BLOCKS 8
+#endif
+// `in` holds in_n[0] nodes of class 0 from its start and (in_n1 != null)
+// in_n1[0] of class 1 from its middle; out_n[c] counts the class-c nodes
+// queued in `out`'s half c.
+template <bool PROP>
+__global__ void __launch_bounds__(128, DR_LEVEL_BLOCKS) k_edge_level(DevScene s, uint64_t seed, BackwardWorkspace ws,
+                                                                   const EdgeTask *in, const unsigned long long *in_n,
+                                                                   const unsigned long long *in_n1, EdgeTask *out,
+                                                                   unsigned long long *out_n) {
+    const unsigned long long half = (unsigned long long)ws.cap_tasks / 2;
+    const long long n0 = (long long)min(*in_n, in_n1 ? half : (unsigned long long)ws.cap_tasks);
+    const long long n = n0 + (in_n1 ? (long long)min(*in_n1, half) : 0);
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    ItemWriter spill(ws);
+    int visits = 0;
+    bool ok = true;
+    // warp-uniform loop: the queue appends are warp-aggregated
+    for (long long base = (long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < n; base += stride) {
+        const long long i = base + (threadIdx.x & 31);
+        EdgeTask kid[2], lf[2];
+        int nk = 0, nl = 0, kc[2] = {0, 0};
+        if (i < n) {
+            const EdgeTask t = in[i < n0 ? i : (long long)half + (i - n0)];
+            const int tree = (t.code >> 29) & 1, mode = (t.code >> 30) & 1, nid = t.code & DR_NODE_MASK;
+            const DevEdgeNode *nodes = tree ? s.nrm_nodes : s.sil_nodes;
+            const DevEdgeNode &node = nodes[nid];
+            if (!(t.bb <= 0.f)) {
+                if (node.nprims > 0) {
+                    lf[nl++] = t;  // a leaf handed on as it is
+                } else {
+                    ++visits;
+                    const WalkPoint w = load_walk_point<PROP>(ws, t.point, seed);
+                    const EdgeItem<PROP> it = edge_item<PROP>(nid, t.bb, t.cpmf, t.apmf, t.lpmf);
+                    ChildPick<PROP> c;
+                    const EdgeProposal pr = point_proposal(ws, t.point);
+                    if (node_children<PROP>(nodes, w.bc, w.cone, w.rng, pr, w.f, mode == 0, tree == 1,
+                                            PROP && mode == 1 && w.learned, it, node, nid, c)) {
+                        const int hi = (tree << 29) | (mode << 30);
+                        if (c.push_l) {
+                            if (c.l_leaf) {
+                                lf[nl++] = child_task<PROP>(t.point, hi, c.left);
+                            } else {
+                                kc[nk] = node_class<PROP>(mode, c.left);
+                                kid[nk++] = child_task<PROP>(t.point, hi, c.left);
+                            }
+                        }
+                        if (c.push_r) {
+                            if (c.r_leaf) {
+                                lf[nl++] = child_task<PROP>(t.point, hi, c.right);
+                            } else {
+                                kc[nk] = node_class<PROP>(mode, c.right);
+                                kid[nk++] = child_task<PROP>(t.point, hi, c.right);
+                            }
+                        }
+                    }
+                }
+            }
+        }
+        __syncwarp();
+        const int n1 = (nk > 0 && kc[0]) + (nk > 1 && kc[1]);
+        unsigned long long ko[2];
+        ko[0] = warp_reserve(out_n, nk - n1);
+        ko[1] = warp_reserve(out_n + 1, n1);
+        const unsigned long long kl = warp_reserve(&ws.counters->leaf_n, nl);
+        for (int j = 0; j < nk; j++) {
+            const unsigned long long slot = ko[kc[j]]++;
+            if (slot < half) out[kc[j] ? half + slot : slot] = kid[j];
+            else walk_here<PROP>(s, seed, ws, kid[j], spill, &visits, ok);
+        }
+        for (int j = 0; j < nl; j++) {
+            if (kl + j < (unsigned long long)ws.cap_leaves) ws.leafq[kl + j] = lf[j];
+            else walk_here<PROP>(s, seed, ws, lf[j], spill, &visits, ok);
+        }
+        spill.flush_warp();
+    }
+    if (!ok) set_status(&ws.counters->status, DR_STATUS_STACK_OVERFLOW);
+    add_visits(&ws.counters->visits_tasks, visits);
+}
+
+// The leaves a level reached: each leaf's silhouette edges (the edge records'
+// test) as items, weighted as EdgeWalk::leaf weighs them; the warp appends
+// them together, one edge of every lane's leaf at a time.
+template <bool PROP>
+__global__ void __launch_bounds__(128, 8) k_edge_leaves(DevScene s, BackwardWorkspace ws) {
+    const long long n = (long long)min(ws.counters->leaf_n, (unsigned long long)ws.cap_leaves);
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    const unsigned long long cap = (unsigned long long)ws.cap_items;
+    int visits = 0;
+    for (long long base = (long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < n; base += stride) {
+        const long long i = base + (threadIdx.x & 31);
+        int point = -1, tree = 0, mode = 0, off = 0, np = 0;
+        float w = 0.f;
+        float3 p = f3(0.f);
+        Frame f;
+        bool codes = false;
+        if (i < n) {
+            const EdgeTask t = ws.leafq[i];
+            tree = (t.code >> 29) & 1;
+            mode = (t.code >> 30) & 1;
+            const DevEdgeNode &node = (tree ? s.nrm_nodes : s.sil_nodes)[t.code & DR_NODE_MASK];
+            point = t.point;
+            off = node.offset;
+            np = node.nprims;
+            ++visits;
+            const float4 c0 = ws.walk_ctx[(size_t)point * DR_CTX_F4];
+            p = f3(c0.x, c0.y, c0.z);
+            float apmf = t.apmf;
+            if constexpr (PROP) apmf = ws.proposal_alpha * t.lpmf + (1.f - ws.proposal_alpha) * t.apmf;
+            const float denom = t.cpmf * t.cpmf + apmf * apmf;
+            w = mode == 0 ? t.cpmf / denom : apmf / denom;
+            if constexpr (PROP) {
+                codes = ws.train_targets != nullptr;
+                if (codes) {
+                    const float4 *c = ws.walk_ctx + (size_t)point * DR_CTX_F4;
+                    const float4 f8 = c[8], f9 = c[9], f10 = c[10];
+                    f.t = f3(f8.x, f8.y, f8.z);
+                    f.b = f3(f8.w, f9.x, f9.y);
+                    f.n = f3(f9.z, f9.w, f10.x);
+                }
+            }
+            if (w == 0.f) np = 0;  // no item of weight 0 is kept
+        }
+        const EdgeRec *recs = tree ? s.nrm_rec : s.sil_rec;
+        const DevEdge *edges = tree ? s.nrm_edges : s.sil_edges;
+        int cnt = 0;
+        const int most = __reduce_max_sync(0xffffffffu, (unsigned)np);
+        for (int k = 0; k < most; k++) {
+            const int ei = off + k;
+            const bool e = k < np && is_silhouette_rec(recs + ei, p);
+            int code = 0;
+            if constexpr (PROP)
+                if (e && codes) code = dir_bin(f, 0.5f * (edge_v0(s, edges[ei]) + edge_v1(s, edges[ei])) - p);
+            const unsigned long long slot = warp_reserve(&ws.counters->items, e ? 1 : 0);
+            if (e) {
+                if (slot < cap) {
+                    ws.items[slot] = make_int4(point, (tree << 30) | ei, (mode << 27) | ei, code);
+                    ws.item_w[slot] = w;
+                } else {
+                    set_status(&ws.counters->status, DR_STATUS_ITEM_OVERFLOW);
+                }
+                cnt++;
+            }
+        }
+        if (ws.pt_items) {  // lanes of the same point add their counts together
+            const unsigned grp = __match_any_sync(0xffffffffu, point);
+            const unsigned sum = __reduce_add_sync(grp, (unsigned)cnt);
+            if ((int)(threadIdx.x & 31) == __ffs(grp) - 1 && point >= 0 && sum > 0)
+                atomicAdd(ws.pt_items + point, (int)sum);
+        }
+    }
     add_visits(&ws.counters->visits_tasks, visits);
 }
 
@@ -601,6 +908,50 @@ cudaError_t dr_launch_edge_traverse(const DevScene &s, uint64_t seed, const Back
         e = cudaMemcpyAsync(&ws.counters->items_expand, &ws.counters->items, sizeof(unsigned long long),
                             cudaMemcpyDeviceToDevice, st);
         if (e != cudaSuccess) return e;
+        if (ws.level_walk && ws.walk_ctx && ws.leafq && ws.tasks2) {
+            // the subtrees level by level: ping-pong between the two queues,
+            // each level's leaves after it; the host looks every 8 levels
+            // whether a level queued nothing (a walk ends within its tree's
+            // depth, a few dozen levels)
+            if (prop) k_walk_ctx<true><<<stage_grid(num_sms), 128, 0, st>>>(s, seed, ws);
+            else k_walk_ctx<false><<<stage_grid(num_sms), 128, 0, st>>>(s, seed, ws);
+            timer->mark(st, "k_walk_ctx");
+            *launches += 1;
+            // the first stage's subtrees fill `tasks` from its start; the levels
+            // fill their queues by class
+            const EdgeTask *in = ws.tasks;
+            const unsigned long long *in_n = &ws.counters->tasks, *in_n1 = nullptr;
+            for (int level = 0;; level++) {
+                EdgeTask *out = (level & 1) ? ws.tasks : ws.tasks2;
+                unsigned long long *out_n = ws.counters->level_n[level & 1];
+                e = cudaMemsetAsync(out_n, 0, 2 * sizeof(unsigned long long), st);
+                if (e == cudaSuccess) e = cudaMemsetAsync(&ws.counters->leaf_n, 0, sizeof(unsigned long long), st);
+                if (e != cudaSuccess) return e;
+                if (prop)
+                    k_edge_level<true><<<num_sms * DR_LEVEL_BLOCKS, 128, 0, st>>>(s, seed, ws, in, in_n, in_n1, out, out_n);
+                else
+                    k_edge_level<false><<<num_sms * DR_LEVEL_BLOCKS, 128, 0, st>>>(s, seed, ws, in, in_n, in_n1, out, out_n);
+                timer->mark(st, "k_edge_level");
+                if (prop) k_edge_leaves<true><<<num_sms * 8, 128, 0, st>>>(s, ws);
+                else k_edge_leaves<false><<<num_sms * 8, 128, 0, st>>>(s, ws);
+                timer->mark(st, "k_edge_leaves");
+                *launches += 2;
+                in = out;
+                in_n = out_n;
+                in_n1 = out_n + 1;
+                if ((level & 7) == 7) {
+                    unsigned long long left[2] = {0, 0};
+                    e = cudaMemcpyAsync(left, in_n, sizeof(left), cudaMemcpyDeviceToHost, st);
+                    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+                    if (e != cudaSuccess) return e;
+                    if (left[0] + left[1] == 0) break;
+                    // node ids have 27 bits: no tree is deeper than that
+                    if (level >= 4096) return cudaErrorInvalidValue;
+                }
+            }
+            *launches += 1;
+            return cudaGetLastError();
+        }
         // the subtrees in rounds: the first stage's, then those handed on
         // (ping-pong between the two queues); one round without a second queue
         const int rounds = ws.tasks2 ? ws.task_rounds : 1;
@@ -730,4 +1081,36 @@ cudaError_t dr_launch_proposal_features(const DevScene &s, const BackwardWorkspa
     k_proposal_features<<<(unsigned)((n + 127) / 128), 128, 0, st>>>(s, ws, n, c, ih, (__nv_bfloat16 *)x,
                                                                       (__nv_bfloat16 *)xt);
     return cudaGetLastError();
+}
+
+// Loads every kernel of the edge half that a backward call can launch.  CUDA
+// loads a kernel lazily, at its first launch, and the load takes device
+// memory for its code; dr_scene_create calls this so that a later
+// dr_render_backward_noalloc call finds its kernels loaded.
+cudaError_t dr_preload_edge_kernels() {
+    const void *k[] = {
+        (const void *)k_edge_traverse<false>, (const void *)k_edge_traverse<true>,
+        (const void *)k_edge_expand<false>, (const void *)k_edge_expand<true>,
+        (const void *)k_edge_tasks<false, false>, (const void *)k_edge_tasks<false, true>,
+        (const void *)k_edge_tasks<true, false>, (const void *)k_edge_tasks<true, true>,
+        (const void *)k_walk_ctx<false>, (const void *)k_walk_ctx<true>,
+        (const void *)k_edge_level<false>, (const void *)k_edge_level<true>,
+        (const void *)k_edge_leaves<false>, (const void *)k_edge_leaves<true>,
+        (const void *)k_edge_line_rays<false, false>, (const void *)k_edge_line_rays<false, true>,
+        (const void *)k_edge_line_rays<true, false>, (const void *)k_edge_line_rays<true, true>,
+        (const void *)k_edge_line<false>, (const void *)k_edge_line<true>,
+        (const void *)k_edge_connect, (const void *)k_edge_pairs<false>, (const void *)k_edge_pairs<true>,
+        (const void *)k_edge_radiance,
+        (const void *)k_edge_shade<false, false, false>, (const void *)k_edge_shade<false, true, false>,
+        (const void *)k_edge_shade<false, true, true>, (const void *)k_edge_shade<true, false, false>,
+        (const void *)k_edge_shade<true, true, false>, (const void *)k_edge_shade<true, true, true>,
+        (const void *)k_primary_shade<1>, (const void *)k_primary_shade<(1 << 30)>,
+        (const void *)k_primary_grad, (const void *)k_add_count, (const void *)k_item_buckets,
+    };
+    for (const void *f : k) {
+        cudaFuncAttributes a;
+        const cudaError_t e = cudaFuncGetAttributes(&a, f);
+        if (e != cudaSuccess) return e;
+    }
+    return cudaSuccess;
 }

@@ -441,6 +441,108 @@ template <bool PROP> HD EdgeItem<PROP> edge_item(int node, float bb, float c, fl
     return it;
 }
 
+// The children of an interior node as the traversal decides them
+// (edge_tree.cpp:560-650): both when the node splits, else the one drawn in
+// proportion to the importances.  Returns 0 when neither is walked (both
+// importances vanish), 1 for a split, 2 for a draw; push_l / push_r say which
+// children are walked (a child whose silhouette test fails or whose bound is
+// 0 is not), l_leaf / r_leaf whether they are leaves.  Shared by the
+// depth-first walk (EdgeWalk) and the level-by-level walk (k_edge_level).
+template <bool PROP> struct ChildPick {
+    EdgeItem<PROP> left, right;
+    bool push_l, push_r, l_leaf, r_leaf;
+};
+template <bool PROP>
+DEV int node_children(const DevEdgeNode *nodes, const BoundCtx &bc, const ConeSpec &cone, const NodeRng &rng,
+                      const EdgeProposal &pr, const Frame &f, const bool CONE, bool dir_bounds, bool learned,
+                      const EdgeItem<PROP> &it, const DevEdgeNode &node, int nid, ChildPick<PROP> &c) {
+    const float3 p = bc.p;
+    c.push_l = c.push_r = false;
+    int li = nid + 1, ri = node.offset;
+    const DevEdgeNode &L = nodes[li], &R = nodes[ri];
+    bool all_split = it.bb > 1.f || node_inside(node, p);
+    bool lcs = true, rcs = true;
+    if (dir_bounds) {
+        lcs = contains_silhouette(L, p);
+        rcs = contains_silhouette(R, p);
+    }
+    // The children of an all-split node in the all walk, off the cone
+    // walk's path (cpmf 0): their bounds only meet thresholds (above 1,
+    // above 0, the importance cutoff), so they may come filtered.
+    const bool filt = !CONE && all_split && it.cpmf == 0.f;
+    float lm = 0.f, rm = 0.f;
+    float lbb = lcs ? bsdf_bound(L, bc, filt ? &lm : nullptr) : 0.f;
+    float rbb = rcs ? bsdf_bound(R, bc, filt ? &rm : nullptr) : 0.f;
+    float il = lcs ? node_importance(L, lbb, p) : 0.f;
+    float ir = rcs ? node_importance(R, rbb, p) : 0.f;
+    if (lm > 0.f || rm > 0.f) {
+        // the cutoff and the cone tests' finiteness check as the exact
+        // bounds decide them: exact bounds where a filtered one could differ
+        const float m = 2.f * fmaxf(lm, rm) + 1e-6f, sum = il + ir;
+        if (!(sum > 1e-10f * (1.f + m) || sum < 1e-10f * (1.f - m)) || !(il < 1e30f) || !(ir < 1e30f)) {
+            lbb = lcs ? bsdf_bound(L, bc) : 0.f;
+            rbb = rcs ? bsdf_bound(R, bc) : 0.f;
+            il = lcs ? node_importance(L, lbb, p) : 0.f;
+            ir = rcs ? node_importance(R, rbb, p) : 0.f;
+        }
+    }
+    if (il + ir <= 1e-10f) return 0;
+    // a node the cone walk cannot reach (cpmf 0) gives its children cpmf
+    // 0 whatever the cone tests say, as long as the importances are
+    // finite: the all walk skips the tests there
+    const bool cone_tests = CONE || it.cpmf != 0.f || !dr_isfinite(il) || !dr_isfinite(ir);
+    bool lhc = cone_tests && box_cone(L.lo, L.hi, cone), rhc = cone_tests && box_cone(R.lo, R.hi, cone);
+    bool cone_split = all_split || (lhc && rhc && lcs && rcs && cone.cos_angle > 0.95f);
+    float ilc = lhc ? il : 0.f, irc = rhc ? ir : 0.f;
+    if (CONE && ilc + irc <= 1e-10f) return 0;
+    float plc = 0.f, prc = 0.f, pla = 0.f, pra = 0.f;
+    if (cone_split) {
+        plc = prc = 1.f;
+    } else if (ilc + irc > 1e-10f) {
+        plc = ilc / (ilc + irc);
+        prc = 1.f - plc;
+    }
+    if (all_split) {
+        pla = pra = 1.f;
+    } else {
+        pla = il / (il + ir);
+        pra = 1.f - pla;
+    }
+    // the proposal's choice (both children important, no split): importance
+    // times the learned weight of the direction towards each child
+    float pll = pla;
+    if constexpr (PROP) {
+        float prl = pra;
+        if (!all_split && il > 0.f && ir > 0.f) {
+            float gl = il * node_dir_weight(pr.q, f, p, L), gr = ir * node_dir_weight(pr.q, f, p, R);
+            if (gl + gr > 0.f) {
+                pll = gl / (gl + gr);
+                prl = 1.f - pll;
+            }
+        }
+        c.left = edge_item<PROP>(li, lbb, plc * it.cpmf, pla * it.apmf, pll * it.lpmf);
+        c.right = edge_item<PROP>(ri, rbb, prc * it.cpmf, pra * it.apmf, prl * it.lpmf);
+    } else {
+        c.left = edge_item<PROP>(li, lbb, plc * it.cpmf, pla * it.apmf, 0.f);
+        c.right = edge_item<PROP>(ri, rbb, prc * it.cpmf, pra * it.apmf, 0.f);
+    }
+    bool split = CONE ? cone_split : all_split;
+    c.l_leaf = L.nprims > 0;
+    c.r_leaf = R.nprims > 0;
+    if (split) {
+        // a child of bound 0 would only be taken off the stack and skipped,
+        // so it is not pushed
+        c.push_r = rcs && !(rbb <= 0.f);
+        c.push_l = lcs && !(lbb <= 0.f);
+        return 1;
+    }
+    float u = rng.draw(CONE ? 0 : 1, nid);
+    bool go_left = CONE ? u < plc : u < (learned ? pll : pla);
+    if (go_left) c.push_l = !(lbb <= 0.f);
+    else c.push_r = !(rbb <= 0.f);
+    return 2;
+}
+
 #define DR_NODE_MASK ((1 << 27) - 1)
 
 // The walk of one tree in one mode as a resumable state: start() pushes the
@@ -532,7 +634,6 @@ struct EdgeWalk {
     // it reading one record per edge.)
     template <class Emit, class Defer> DEV void step(Emit &emit, Defer &defer, int *visits) {
         const bool CONE = cone_mode;
-        const float3 p = bc.p;
         const Item it = st[--n];
         if (it.bb <= 0.f) return;
         const int nid = it.node & DR_NODE_MASK;
@@ -549,94 +650,20 @@ struct EdgeWalk {
             return;
         }
         const int cdepth = CUT > 0 ? ((it.node >> 27) + 1) << 27 : 0;  // the children's depth bits
-        int li = nid + 1, ri = node.offset;
-        const DevEdgeNode &L = nodes[li], &R = nodes[ri];
-        bool all_split = it.bb > 1.f || node_inside(node, p);
-        bool lcs = true, rcs = true;
-        if (dir_bounds) {
-            lcs = contains_silhouette(L, p);
-            rcs = contains_silhouette(R, p);
+        ChildPick<PROP> c;
+        const int r = node_children<PROP>(nodes, bc, cone, rng, pr, f, CONE, dir_bounds, learned, it, node, nid, c);
+        if (r == 0) return;
+        if (n + (r == 1 ? 2 : 1) > DR_EDGE_STACK) {
+            ok = false;
+            return;
         }
-        // The children of an all-split node in the all walk, off the cone
-        // walk's path (cpmf 0): their bounds only meet thresholds (above 1,
-        // above 0, the importance cutoff), so they may come filtered.
-        const bool filt = !CONE && all_split && it.cpmf == 0.f;
-        float lm = 0.f, rm = 0.f;
-        float lbb = lcs ? bsdf_bound(L, bc, filt ? &lm : nullptr) : 0.f;
-        float rbb = rcs ? bsdf_bound(R, bc, filt ? &rm : nullptr) : 0.f;
-        float il = lcs ? node_importance(L, lbb, p) : 0.f;
-        float ir = rcs ? node_importance(R, rbb, p) : 0.f;
-        if (lm > 0.f || rm > 0.f) {
-            // the cutoff and the cone tests' finiteness check as the exact
-            // bounds decide them: exact bounds where a filtered one could differ
-            const float m = 2.f * fmaxf(lm, rm) + 1e-6f, sum = il + ir;
-            if (!(sum > 1e-10f * (1.f + m) || sum < 1e-10f * (1.f - m)) || !(il < 1e30f) || !(ir < 1e30f)) {
-                lbb = lcs ? bsdf_bound(L, bc) : 0.f;
-                rbb = rcs ? bsdf_bound(R, bc) : 0.f;
-                il = lcs ? node_importance(L, lbb, p) : 0.f;
-                ir = rcs ? node_importance(R, rbb, p) : 0.f;
-            }
+        if (CUT > 0) {
+            c.left.node |= cdepth;
+            c.right.node |= cdepth;
         }
-        if (il + ir <= 1e-10f) return;
-        // a node the cone walk cannot reach (cpmf 0) gives its children cpmf
-        // 0 whatever the cone tests say, as long as the importances are
-        // finite: the all walk skips the tests there
-        const bool cone_tests = CONE || it.cpmf != 0.f || !dr_isfinite(il) || !dr_isfinite(ir);
-        bool lhc = cone_tests && box_cone(L.lo, L.hi, cone), rhc = cone_tests && box_cone(R.lo, R.hi, cone);
-        bool cone_split = all_split || (lhc && rhc && lcs && rcs && cone.cos_angle > 0.95f);
-        float ilc = lhc ? il : 0.f, irc = rhc ? ir : 0.f;
-        if (CONE && ilc + irc <= 1e-10f) return;
-        float plc = 0.f, prc = 0.f, pla = 0.f, pra = 0.f;
-        if (cone_split) {
-            plc = prc = 1.f;
-        } else if (ilc + irc > 1e-10f) {
-            plc = ilc / (ilc + irc);
-            prc = 1.f - plc;
-        }
-        if (all_split) {
-            pla = pra = 1.f;
-        } else {
-            pla = il / (il + ir);
-            pra = 1.f - pla;
-        }
-        // the proposal's choice (both children important, no split): importance
-        // times the learned weight of the direction towards each child
-        float pll = pla;
-        Item left, right;
-        if constexpr (PROP) {
-            float prl = pra;
-            if (!all_split && il > 0.f && ir > 0.f) {
-                float gl = il * node_dir_weight(pr.q, f, p, L), gr = ir * node_dir_weight(pr.q, f, p, R);
-                if (gl + gr > 0.f) {
-                    pll = gl / (gl + gr);
-                    prl = 1.f - pll;
-                }
-            }
-            left = edge_item<PROP>(li | cdepth, lbb, plc * it.cpmf, pla * it.apmf, pll * it.lpmf);
-            right = edge_item<PROP>(ri | cdepth, rbb, prc * it.cpmf, pra * it.apmf, prl * it.lpmf);
-        } else {
-            left = edge_item<PROP>(li | cdepth, lbb, plc * it.cpmf, pla * it.apmf, 0.f);
-            right = edge_item<PROP>(ri | cdepth, rbb, prc * it.cpmf, pra * it.apmf, 0.f);
-        }
-        bool split = CONE ? cone_split : all_split;
-        if (split) {
-            if (n + 2 > DR_EDGE_STACK) {
-                ok = false;
-                return;
-            }
-            // depth first, left subtree before right; a child of bound 0 would
-            // only be taken off the stack and skipped, so it is not pushed
-            if (rcs && !(rbb <= 0.f)) st[n++] = right;
-            if (lcs && !(lbb <= 0.f)) st[n++] = left;
-        } else {
-            float u = rng.draw(CONE ? 0 : 1, nid);
-            bool go_left = CONE ? u < plc : u < (learned ? pll : pla);
-            if (n + 1 > DR_EDGE_STACK) {
-                ok = false;
-                return;
-            }
-            if (!((go_left ? lbb : rbb) <= 0.f)) st[n++] = go_left ? left : right;
-        }
+        // depth first, left subtree before right
+        if (c.push_r) st[n++] = c.right;
+        if (c.push_l) st[n++] = c.left;
     }
 };
 

@@ -11,8 +11,9 @@
 // With `sync` set (the DR_DEBUG_SYNC environment variable, a diagnostic), every
 // mark synchronizes the stream and remembers the first kernel that failed.
 struct StageTimer {
-    // a streamed edge stage marks six kernels per chunk of points
-    static const int kMax = 1024;
+    // a streamed edge stage marks its kernels once per chunk of points, the
+    // level walk's two once per level
+    static const int kMax = 4096;
     bool on = false;
     bool sync = false;
     const char *failed = nullptr;
@@ -100,6 +101,11 @@ struct BackwardCounters {
     // subtrees handed on between rounds of k_edge_tasks (two queues, used in
     // turn) and their total
     unsigned long long handed[2], handed_total;
+    // leaves the level walk's launch queued for k_edge_leaves; the nodes it
+    // queued for the next level, per class (front and back half of the
+    // queue, two queues used in turn); subtrees a full queue left to a lane's
+    // depth-first walk
+    unsigned long long leaf_n, level_n[2][2], spilled;
 };
 
 // A view of a batched multi-view backward call: what the edge stage needs of
@@ -127,6 +133,9 @@ struct BackwardWorkspace {
     // points [pt_begin, min(pt_end, counters->points)) go through the edge
     // stage (traversal, edge evaluation, k_dp_propagate) of one launch
     long long pt_begin, pt_end;
+    // the traversal kernels walk every pt_stride-th point of that range only
+    // (the first call's forecast of the edge counts); 1 otherwise
+    long long pt_stride = 1;
     // learned edge proposal (null: the reference's sampling): [cap_points][32]
     // bf16 slot probabilities, the mixture weight, and the training targets of
     // points p = k * train_stride, k < train_n ([train_n][32] f32 contribution
@@ -151,6 +160,15 @@ struct BackwardWorkspace {
     // its shallowest pending subtree on, and launches (rounds) per chunk of
     // points (the scene's tuning, dr_scene_set_tuning)
     int hand_steps = 64, task_rounds = 3;
+    // the level-by-level walk of the subtrees (level_walk != 0; otherwise
+    // k_edge_tasks walks each depth first): every point's walk context
+    // ([cap_points][DR_CTX_F4] float4, k_walk_ctx) and the queue of the
+    // leaves each level reached (cap_leaves entries); the levels' own queues
+    // are `tasks` and `tasks2`, used in turn
+    int level_walk = 1;
+    float4 *walk_ctx;
+    EdgeTask *leafq;
+    long long cap_leaves;
     // per view of a batched multi-view call (null: the call's own settings);
     // each point's settings are views[point.view]
     const ViewParams *views;
@@ -186,6 +204,10 @@ cudaError_t dr_launch_backward_front(const DevScene &s, int W, int H, int spp, i
 // p = k * train_stride (k < train_n) are also written to xt[k].
 cudaError_t dr_launch_proposal_features(const DevScene &s, const BackwardWorkspace &ws, long long n, float3 c,
                                         float3 ih, void *x, void *xt, cudaStream_t st);
+// Load every kernel a backward call can launch (CUDA loads kernels lazily, at
+// their first launch, taking device memory for their code).
+cudaError_t dr_preload_backward_kernels();
+cudaError_t dr_preload_edge_kernels();
 cudaError_t dr_launch_edge_traverse(const DevScene &s, uint64_t seed, const BackwardWorkspace &ws, int num_sms,
                                     cudaStream_t st, int *launches, StageTimer *timer);
 // The silhouette-test records of n tree edges (dr_edges.cuh: edge_record).
@@ -209,6 +231,9 @@ cudaError_t dr_launch_primary_edges(const DevScene &s, int W, int H, int spp, in
 cudaError_t dr_launch_backward_back(const DevScene &s, int W, int H, int spp, int B, uint64_t seed, float *grad,
                                     int dp_mode, const BackwardWorkspace &ws, const GradCacheCfg &cfg, int num_sms,
                                     cudaStream_t st, int *launches, StageTimer *timer);
+
+// float4 of one point's walk context in BackwardWorkspace::walk_ctx.
+#define DR_CTX_F4 11
 
 // Words of one packed secondary-point record in BackwardWorkspace::pt.
 #define DR_PT_FLOATS 24

@@ -49,6 +49,10 @@ class FitConfig:
     roughness_noise: float = 0.1  # initial perturbation of the roughness (std)
     rmse_goal: float = 0.01
     common_seeds: bool = False    # common random numbers: targets at `spp` with each view's seed, reused every step
+    # unbiased estimators (every sampled edge's position derivative summed,
+    # the sampling pdf held constant, lobe mixture weights for edge samples,
+    # sub-pixel samples over the whole pixel); False: the reference's
+    unbiased: bool = True
     learned: bool = False         # train and use the learned edge proposal
     proposal_mix: float = 0.8
     seed: int = 0
@@ -121,6 +125,15 @@ class HeightfieldFit:
     def _dicts(self, cam, mats, shapes):
         return _abi.scene_dicts(cam, mats, shapes, self.wl.lights)
 
+    def options(self, backward=False):
+        """Render options of the fit's forward or backward calls (the learned
+        proposal only draws the backward call's edges)."""
+        learned = backward and self.cfg.learned
+        if not self.cfg.unbiased:
+            return RenderOptions(learned_proposal=learned)
+        return RenderOptions(dp_mode=_abi.DR_DP_SUM, detached_pdf=True, edge_lobe_mis=True, full_pixel_jitter=True,
+                             learned_proposal=learned)
+
     def view_seed(self, k):
         """Seed of view k at the current step (the same at every step with
         common_seeds, and then also the target's)."""
@@ -137,7 +150,7 @@ class HeightfieldFit:
             c, m, s, l = self._dicts(cam, mats, shapes)
             sc = Scene(c, m, s, l, self.cfg.device)
             try:
-                self.targets.append(sc.forward(W, H, spp, self.cfg.max_bounces, 777 + k).clone())
+                self.targets.append(sc.forward(W, H, spp, self.cfg.max_bounces, 777 + k, self.options()).clone())
             finally:
                 sc.close()
         return self.targets
@@ -166,13 +179,13 @@ class HeightfieldFit:
         W, H = cfg.resolution
         mats, shapes = self._scene_lists(self.heights, self.rough)
         self._ensure_scenes(mats, shapes)
-        opts = RenderOptions(learned_proposal=cfg.learned)
+        opts, fwd_opts = self.options(backward=True), self.options()
         g_h = torch.zeros_like(self.true_heights)
         g_r = torch.zeros(self.n_patch)
         loss = 0.0
         for k, sc in enumerate(self.scenes):
             seed = self.view_seed(k)
-            img = sc.forward(W, H, cfg.spp, cfg.max_bounces, seed)
+            img = sc.forward(W, H, cfg.spp, cfg.max_bounces, seed, fwd_opts)
             diff = img - self.targets[k]
             loss += float(diff.pow(2).mean())
             d_img = (2.0 / diff.numel()) * diff

@@ -157,15 +157,16 @@ class Scene:
 
     def tuning(self):
         """The scene's queue settings (dr_scene_get_tuning): hand_steps,
-        task_rounds, queue_items."""
+        task_rounds, queue_items, depth_first."""
         t = _abi.dr_tuning()
         _lib.check(_lib.lib().dr_scene_get_tuning(self.handle, C.byref(t)))
-        return {"hand_steps": t.hand_steps, "task_rounds": t.task_rounds, "queue_items": t.queue_items}
+        return {"hand_steps": t.hand_steps, "task_rounds": t.task_rounds, "queue_items": t.queue_items,
+                "depth_first": t.depth_first}
 
-    def set_tuning(self, hand_steps=64, task_rounds=3, queue_items=0):
+    def set_tuning(self, hand_steps=64, task_rounds=3, queue_items=0, depth_first=0):
         """Sets the scene's queue settings (dr_scene_set_tuning); the
         defaults are the library's."""
-        t = _abi.dr_tuning(int(hand_steps), int(task_rounds), int(queue_items))
+        t = _abi.dr_tuning(int(hand_steps), int(task_rounds), int(queue_items), int(depth_first), 0)
         _lib.check(_lib.lib().dr_scene_set_tuning(self.handle, C.byref(t)))
 
     def autotune(self, width, height, spp, max_bounces, seed, d_image, opts=None, max_trials=16):
@@ -186,7 +187,8 @@ class Scene:
                                                     self._stream()))
         b = rep.best
         return {"hand_steps": b.hand_steps, "task_rounds": b.task_rounds, "queue_items": b.queue_items,
-                "best_ms": rep.best_ms, "start_ms": rep.start_ms, "trials": rep.trials}
+                "depth_first": b.depth_first, "best_ms": rep.best_ms, "start_ms": rep.start_ms,
+                "trials": rep.trials}
 
     def backward_views(self, views, opts=None):
         """Backward render of several views in one call.  views: a list of
@@ -271,11 +273,12 @@ class Scene:
         whose rays hit one of the edge's faces), shaded samples, subtree tasks,
         first-stage items,
         node visits of the point walks and of the subtree walks, candidates of
-        the ray stage (samples that passed its connectivity test)."""
-        w = (C.c_int64 * 9)()
-        _lib.check(_lib.lib().dr_scene_last_work(self.handle, w, 9))
+        the ray stage (samples that passed its connectivity test), subtrees
+        walked depth first after a full level queue."""
+        w = (C.c_int64 * 10)()
+        _lib.check(_lib.lib().dr_scene_last_work(self.handle, w, 10))
         keys = ("points", "items", "survivors", "shaded", "tasks", "items_first_stage", "visits_walk",
-                "visits_tasks", "candidates")
+                "visits_tasks", "candidates", "spilled")
         return dict(zip(keys, (int(x) for x in w)))
 
     def last_counts(self):

@@ -259,10 +259,11 @@ DR_API dr_status dr_render_backward_views(dr_scene *scene, int n_views, const dr
  * DR_ERR_OUT_OF_MEMORY, as do specular chains whose shading points outgrow
  * half the array (about 150,000 points).  All calls on
  * one device share the array, so overlapping calls (from several threads or
- * streams) race: serialize them.  Where CUDA loads modules lazily, the
- * array's memory is taken when the first scene is created on the device
- * (dr_scene_create looks the array up), not by this call; each call looks up
- * the address of the current context's copy again. */
+ * streams) race: serialize them.  Where CUDA loads modules and kernels
+ * lazily, the array's memory and the kernels' code are taken when a scene is
+ * created on the device (dr_scene_create looks the array up and loads every
+ * kernel a backward call launches), not by this call; each call looks up the
+ * address of the current context's copy again. */
 DR_API dr_status dr_render_backward_noalloc(dr_scene *scene, const dr_render_desc *rd, const float *d_image_dev,
                                             float *grad_dev, float *image_dev, void *stream);
 
@@ -277,15 +278,21 @@ DR_API dr_status dr_render_backward_noalloc(dr_scene *scene, const dr_render_des
 DR_API dr_status dr_set_item_queue_limit(int64_t items);
 
 /* A scene's queue settings for its backward calls (no counterpart in the
- * reference, whose CPU renderer has no work queues).
- *   hand_steps: node steps a subtree walk of the second traversal stage takes
- *     before it hands its shallowest pending subtree on to the next round
+ * reference, whose CPU renderer has no work queues).  Large edge trees are
+ * walked in two stages: each point's walk down to 8 levels below the roots,
+ * then the subtrees there.
+ *   depth_first: 0 (the default) walks those subtrees level by level, one
+ *     launch per level over every subtree's nodes of that level; 1 walks
+ *     each subtree depth first, one lane per subtree;
+ *   hand_steps: with depth_first, the node steps a subtree walk takes before
+ *     it hands its shallowest pending subtree on to the next round
  *     (1..4096; default 64);
- *   task_rounds: launches of that stage per chunk of shading points, the last
- *     handing nothing on (1..8; default 3);
+ *   task_rounds: with depth_first, launches of the subtree stage per chunk of
+ *     shading points, the last handing nothing on (1..8; default 3);
  *   queue_items: bound on the edge items the scene's calls hold at once (0,
  *     the default: the process-wide bound of dr_set_item_queue_limit; else
- *     the smaller of the two).
+ *     the smaller of the two);
+ *   reserved: 0.
  * No setting changes which edges are sampled or what they contribute: the
  * counts and the image are the same under every setting, the gradient up to
  * float round-off (atomic adds sum in another order). */
@@ -293,6 +300,8 @@ typedef struct {
     int32_t hand_steps;
     int32_t task_rounds;
     int64_t queue_items;
+    int32_t depth_first;
+    int32_t reserved;
 } dr_tuning;
 
 DR_API dr_status dr_scene_get_tuning(const dr_scene *scene, dr_tuning *out);
@@ -311,8 +320,9 @@ typedef struct {
 
 /* Chooses the scene's queue settings by timing backward calls of this render
  * (arguments as dr_render_backward; grad_dev holds the last call's gradient
- * afterwards).  Coordinate search from the current setting: subtree rounds
- * 1-4, then hand-on steps 16-256 (only where points hand subtrees on), then
+ * afterwards).  Coordinate search from the current setting: the subtree walk,
+ * and for the depth-first one its rounds 1-4 and hand-on steps 16-256 (only
+ * where points hand subtrees on), then
  * item-queue bounds of 1/2, 1/4 and 1/8 of the last call's items (smaller
  * chunks of the edge stage, whose queues sit nearer to L2); each setting
  * timed as the faster of two calls, at most max_trials settings.  The fastest
@@ -371,11 +381,14 @@ DR_API dr_status dr_scene_edge_data(const dr_scene *scene, int what, void *out_h
  * [1] sampled edges, [2] line samples kept for their rays (in scenes
  * traced through the LBVH: those whose rays hit one of the edge's faces),
  * [3] samples kept for shading, [4] subtrees walked by the second traversal
- * stage (handed on by the first stage or between the second stage's rounds),
+ * stage (handed on by the first stage, and with the depth-first walk between
+ * its rounds),
  * [5] edges sampled by the first stage (all, when the traversal runs in one
  * stage), [6] edge-tree nodes visited by the point walks, [7] nodes
  * visited by the subtree walks, [8] line samples whose connectivity test
- * passed (candidates of the ray stage).  Up to n of them are written. */
+ * passed (candidates of the ray stage), [9] subtrees the level walk left to
+ * a lane's depth-first walk because a level's queue was full.  Up to n of
+ * them are written. */
 DR_API dr_status dr_scene_last_work(const dr_scene *scene, int64_t *counts, int n);
 
 /* Kernel launch count of the last render call on this scene (for tooling). */

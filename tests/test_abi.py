@@ -41,7 +41,7 @@ def test_null_arguments_are_rejected_without_a_device():
         _lib.check(L.dr_scene_grad_layout(None, None))
     assert L.dr_set_item_queue_limit(-1) == 1
     assert L.dr_set_item_queue_limit(0) == 0
-    t = _abi.dr_tuning(64, 3, 0)
+    t = _abi.dr_tuning(64, 3, 0, 0, 0)
     assert L.dr_scene_set_tuning(None, C.byref(t)) == 1
     assert L.dr_scene_get_tuning(None, C.byref(t)) == 1
     rep = _abi.dr_tune_report()
@@ -50,8 +50,8 @@ def test_null_arguments_are_rejected_without_a_device():
 
 def test_tuning_structs_match_header():
     from delta_ray_b200 import _abi
-    assert C.sizeof(_abi.dr_tuning) == 16
-    assert C.sizeof(_abi.dr_tune_report) == 16 + 4 + 4 + 4 + 4  # padded to 8 bytes
+    assert C.sizeof(_abi.dr_tuning) == 24
+    assert C.sizeof(_abi.dr_tune_report) == 24 + 4 + 4 + 4 + 4  # padded to 8 bytes
 
 
 def test_render_desc_layout_matches_header():

@@ -23,7 +23,8 @@ WORK = {"points": 1_000_000, "items": 1_100_000_000, "survivors": 500_000_000, "
 
 def test_every_kernel_of_a_step_has_model_bytes():
     for k in ("k_render_forward", "k_backward_paths", "k_primary_shade", "k_primary_grad", "k_edge_traverse",
-              "k_edge_expand", "k_edge_tasks", "k_edge_line", "k_edge_connect", "k_edge_pairs", "k_edge_line_rays",
+              "k_edge_expand", "k_edge_tasks", "k_walk_ctx", "k_edge_level", "k_edge_leaves", "k_edge_line",
+              "k_edge_connect", "k_edge_pairs", "k_edge_line_rays",
               "k_edge_shade",
               "k_dp_propagate"):
         assert bench.kernel_bytes(k, _Wl, WORK) > 0, k
@@ -35,6 +36,7 @@ def test_byte_model_counts_nodes_and_rays():
     24 + 16 + 36 + 64 ceil(log2 T) bytes."""
     w2 = dict(WORK, visits_tasks=WORK["visits_tasks"] + 1000)
     assert bench.kernel_bytes("k_edge_tasks", _Wl, w2) - bench.kernel_bytes("k_edge_tasks", _Wl, WORK) == 40_000
+    assert bench.kernel_bytes("k_edge_level", _Wl, w2) - bench.kernel_bytes("k_edge_level", _Wl, WORK) == 40_000
     assert bench.ray_bytes(130054) == 24 + 16 + 36 + 64 * 17
     assert bench.ray_bytes(8) == 24 + 16 + 36 + 64 * 3
     w3 = dict(WORK, survivors=WORK["survivors"] + 10)

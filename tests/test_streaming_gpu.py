@@ -68,3 +68,43 @@ def test_streamed_edge_stage_matches_one_pass(name):
         finally:
             set_item_queue_limit(0)
             sc.close()
+
+
+def test_first_call_probe_forecasts_the_edge_counts():
+    """A scene's first call of 2^20 or more pixel samples has no edge counts
+    to plan its edge stage from: it walks every 16th shading point first and
+    forecasts the others' counts from theirs.  With room for the forecast it
+    then walks every point in one pass; without (a bounded item queue) it
+    streams chunks planned from the forecast, cutting those that overflow.
+    Either way the call gives the results of a later call on the same scene,
+    which plans from its predecessor's counts."""
+    from delta_ray_b200 import workloads
+    from delta_ray_b200.render_pytorch import set_item_queue_limit
+    wl = workloads.heightfield(seed=3, resolution=(256, 256), spp=16, max_bounces=1, grid=32, patch=8)
+    W, H = wl.resolution
+    assert W * H * wl.spp >= 1 << 20
+    d_image = torch.from_numpy(np.random.default_rng(7).uniform(0.5, 1.5, (H, W, 3)).astype(np.float32)).cuda()
+
+    def call(sc):
+        g, img = sc.backward(W, H, wl.spp, wl.max_bounces, 13, d_image, want_image=True)
+        return g.cpu().numpy(), img.cpu().numpy(), tuple(sc.last_counts())
+
+    sc = _scene(wl)
+    try:
+        g1, img1, c1 = call(sc)  # probe, then one pass
+        g0, img0, counts = call(sc)  # planned from the first call's counts
+        assert c1 == counts and np.array_equal(img1, img0) and rel_err(g1, g0) < 1e-5
+    finally:
+        sc.close()
+    items = counts[1]
+    for div in (3, 12):
+        set_item_queue_limit(max(1 << 16, items // div))
+        sc = _scene(wl)
+        try:
+            g, img, c = call(sc)  # probe, then chunks from its forecast
+            assert c == counts, div
+            assert np.array_equal(img, img0), div
+            assert rel_err(g, g0) < 1e-5, div
+        finally:
+            set_item_queue_limit(0)
+            sc.close()
