@@ -375,12 +375,13 @@ def measure_inverse(steps):
     """The inverse-rendering loop (delta_ray_b200.inverse) at its reduced
     setting, plain and with the learned edge proposal: a 64 x 64 height grid
     (16 roughness patches) fit to 4 views of 128 x 96 rendered at 64 spp, Adam
-    at 4 spp per view per step, max_bounces 2; parameter RMSE over the heights
-    and roughness, and the time to reach RMSE 0.01."""
+    (lr 3e-3) at 8 spp per view per step, direct lighting (FitConfig's
+    defaults); parameter RMSE over the heights and roughness, the time to
+    reach RMSE 0.01, the image loss of the first and last step."""
     from delta_ray_b200.inverse import FitConfig, fit
     out = {"setting": "64x64-vertex heightfield (7,938 triangles + 2 light quads), 4 views of 128x96, "
-                      f"targets at 64 spp, {steps} Adam steps (lr 1e-2) at 4 spp, max_bounces 2; "
-                      "heights perturbed by N(0, 0.05), roughness by N(0, 0.1)",
+                      f"targets at 64 spp, {steps} Adam steps (lr 3e-3) at 8 spp, max_bounces 1, unbiased "
+                      "estimator options; heights perturbed by N(0, 0.05), roughness by N(0, 0.1)",
            "full_configuration": "256x256 grid, 4 views of 1024x1024 at 256 spp, 200 steps at 64 spp, "
                                  "max_bounces 4: 268 M pixel samples fwd+bwd per step (not run)"}
     for arm, learned in (("plain", False), ("learned", True)):
@@ -388,6 +389,9 @@ def measure_inverse(steps):
         out[arm] = {k: (round(v, 5) if isinstance(v, float) else v) for k, v in r.items()
                     if k in ("rmse_start", "rmse_final", "rmse_min", "time_to_goal_s", "steps_to_goal", "wall_s",
                              "samples_per_s")}
+        h = r["history"]
+        out[arm]["loss_first_last"] = [round(h[1]["loss"], 5), round(h[-1]["loss"], 5)]
+        out[arm]["step_of_min"] = min(h, key=lambda x: x["rmse"])["step"]
     return out
 
 

@@ -323,6 +323,7 @@ void upload_scene(dr_scene *sc, cudaStream_t st, bool refit = false) {
     }
     const size_t o_bvh_nodes = lay.space(sizeof(float4) * 4 * (size_t)std::max(1, n - 1));
     const size_t o_bvh_tris = linear ? lay.add(leaves) : lay.space(sizeof(float4) * 3 * (size_t)std::max(1, n));
+    const size_t o_bvh_wide = lay.space(sizeof(float4) * DR_WIDE_F4 * (size_t)(linear ? 1 : std::max(1, n - 1)));
     upload_arena(sc->arena, lay, st);
     char *base = (char *)sc->arena.p;
     sc->ltc = device_ltc(sc->device, 0, h.ltc);
@@ -347,6 +348,7 @@ void upload_scene(dr_scene *sc, cudaStream_t st, bool refit = false) {
                        "LBVH build");
             sc->bvh_built_tris = n;
         }
+        check_cuda(dr_widen_lbvh(bvh_nodes, n, (float4 *)(base + o_bvh_wide), st, &sc->last_launches), "LBVH widen");
         check_cuda(cudaStreamSynchronize(st), "LBVH build");
     }
     ScenePtrs ptr;
@@ -357,6 +359,7 @@ void upload_scene(dr_scene *sc, cudaStream_t st, bool refit = false) {
     ptr.tri_local = (int *)(base + o_tri_local);
     ptr.bvh_nodes = bvh_nodes;
     ptr.bvh_tris = bvh_tris;
+    ptr.bvh_wide = n > 1 && !linear ? (const float4 *)(base + o_bvh_wide) : nullptr;
     ptr.shapes = (DevShape *)(base + o_shapes);
     ptr.mats = (DevMaterial *)(base + o_mats);
     ptr.texels = (float *)(base + o_texels);

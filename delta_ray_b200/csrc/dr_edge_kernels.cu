@@ -677,7 +677,7 @@ __global__ void __launch_bounds__(128, DR_CONNECT_BLOCKS) k_edge_connect(DevScen
             }
         }
         if (fetch || phase == 0) continue;
-        const int r = w.step(s.bvh_nodes, s.bvh_tris);
+        const int r = w.step(s.bvh_nodes, s.bvh_wide, s.bvh_tris);
         if (r == 0) continue;
         if (phase == 1) {
             cr = r == 2;  // no triangle ahead of the right face hit

@@ -1003,9 +1003,9 @@ DEV bool edge_connect_bvh(const DevScene &s, const DevEdge &edge, float3 p, floa
     Hit fr, fl;
     hit_faces_pair(s, edge, p, rdir, ldir, 1e-3f, fr, fl);
     if (fr.tri < 0 && fl.tri < 0) return false;
-    const bool cr = fr.tri >= 0 && !trace_before_bvh(s.bvh_nodes, s.bvh_tris, s.bvh_root, p, rdir, 1e-3f, fr.t, fr.tri);
+    const bool cr = fr.tri >= 0 && !trace_before(s, p, rdir, 1e-3f, fr.t, fr.tri);
     if (!cr && fl.tri < 0) return false;
-    const bool cl = fl.tri >= 0 && !trace_before_bvh(s.bvh_nodes, s.bvh_tris, s.bvh_root, p, ldir, 1e-3f, fl.t, fl.tri);
+    const bool cl = fl.tri >= 0 && !trace_before(s, p, ldir, 1e-3f, fl.t, fl.tri);
     if (cr == cl) return false;
     side = cr ? 0 : 1;
     face = cr ? fr.tri : fl.tri;
@@ -1038,7 +1038,7 @@ DEV bool edge_rays_rest(const DevScene &s, int stri, float3 p, float3 rdir, floa
                         bool direct_only, EdgeHits &out) {
     int hit[2];
     hit[side] = face;
-    hit[1 - side] = trace_closest_bvh(s.bvh_nodes, s.bvh_tris, s.bvh_root, p, side ? rdir : ldir, 1e-3f).tri;
+    hit[1 - side] = trace_closest(s, p, side ? rdir : ldir, 1e-3f).tri;
     if (!edge_hits_ok(s, stri, p, rdir, ldir, hit, direct_only)) return false;
     out.r = hit[0];
     out.l = hit[1];

@@ -717,7 +717,7 @@ struct ScenePtrs {
     const float *vtx, *nrm, *uv;
     const int4 *tri;
     const int *tri_local;
-    const float4 *bvh_nodes, *bvh_tris;
+    const float4 *bvh_nodes, *bvh_tris, *bvh_wide = nullptr;
     const DevShape *shapes;
     const DevMaterial *mats;
     const float *texels;
@@ -749,6 +749,7 @@ inline void fill_devscene(DevScene &ds, const HostScene &h, const FlatScene &f, 
     ds.num_tris = n;
     ds.bvh_nodes = p.bvh_nodes;
     ds.bvh_tris = p.bvh_tris;
+    ds.bvh_wide = p.bvh_wide;
     ds.bvh_root = n > 1 ? 0 : ~0;
     ds.shapes = p.shapes;
     ds.num_shapes = (int)h.shapes.size();

@@ -44,6 +44,10 @@ struct StageTimer {
 cudaError_t dr_build_lbvh(const float *vtx, const int4 *tri, int n, float3 lo, float3 hi, float4 *nodes,
                           float4 *leaf_tris, void *scratch, size_t scratch_bytes, cudaStream_t st, int *launches);
 size_t dr_lbvh_scratch_bytes(int n);
+// The 4-wide form of an LBVH over n triangles (DR_WIDE_F4 float4 per
+// internal node, DevScene::bvh_wide), from its binary nodes; after every build
+// and refit.
+cudaError_t dr_widen_lbvh(const float4 *nodes, int n, float4 *wide, cudaStream_t st, int *launches);
 // Recomputes the boxes of an LBVH built by dr_build_lbvh over the same
 // triangles (same scratch, kept since the build) for new vertex positions.
 cudaError_t dr_refit_lbvh(const float *vtx, const int4 *tri, int n, float4 *nodes, float4 *leaf_tris, void *scratch,

@@ -82,6 +82,13 @@ struct EdgeTask {
     float bb, cpmf, apmf, lpmf;
 };
 
+// A 4-wide node of the LBVH (DevScene::bvh_wide): float4 0-5 the four child
+// boxes by coordinate (lo.x of children 0-3, lo.y, lo.z, hi.x, hi.y, hi.z),
+// float4 6 the children (internal node ids, ~leaf for leaves, DR_WIDE_EMPTY
+// for an empty slot), float4 7 unused (a node fills one 128-byte line).
+#define DR_WIDE_F4 8
+#define DR_WIDE_EMPTY 0x7fffffff
+
 struct DevScene {
     DevCamera cam;
     // flat-gradient offset of the camera's block (0; in a batched multi-view
@@ -99,6 +106,10 @@ struct DevScene {
     const float4 *bvh_nodes;  // 4 float4 per internal node (two child boxes + child ids)
     const float4 *bvh_tris;   // 3 float4 per leaf, leaf order (xyz, .w of the first = tri id)
     int bvh_root;             // >= 0 internal node, < 0 leaf (~leaf slot)
+    // the same tree read four children at a time: for each internal node, its
+    // children's children (a leaf child stands for itself) as one 4-wide node,
+    // DR_WIDE_F4 float4 (null: the walks read the binary nodes)
+    const float4 *bvh_wide;
     // shapes, materials, lights
     const DevShape *shapes;
     int num_shapes;

@@ -272,6 +272,10 @@ DEV Hit trace_closest(const DevScene &s, float3 o, float3 d, float tnear) {
         return h;
     }
     if (s.num_tris <= DR_LINEAR_TRIS) return trace_closest_linear(s.bvh_tris, s.num_tris, o, d, tnear);
+    // closest hits walk the binary nodes: a lane's own loop over them ran
+    // faster than over the 4-wide nodes (the kernels that trace closest hits
+    // measured 18-24 % slower with the 4-wide walk); the warp-stepped
+    // occlusion walks of k_edge_connect take the 4-wide one (fewer steps)
     return trace_closest_bvh(s.bvh_nodes, s.bvh_tris, s.bvh_root, o, d, tnear);
 }
 
@@ -313,6 +317,67 @@ DEV_NOINLINE bool trace_any_bvh(const float4 *DR_RESTRICT nodes, const float4 *D
     return false;
 }
 
+// Steps of the walks over the LBVH's 4-wide form (see trace_before_wide);
+// their stack holds up to three children per 4-wide level.
+#define DR_WIDE_STACK 96
+
+// The children of wide node w whose boxes the ray enters before tmax, nearest
+// first: n of them in c[0..n).
+struct WideKids {
+    int n;
+    int c[4];
+};
+DEV void wide_swap(float &ka, int &ca, float &kb, int &cb) {
+    if (kb < ka) {
+        const float k = ka;
+        ka = kb;
+        kb = k;
+        const int c = ca;
+        ca = cb;
+        cb = c;
+    }
+}
+DEV WideKids wide_kids(const float4 *DR_RESTRICT w, float3 o, float3 inv, float tmax) {
+    const float4 lx = dr_ldg(w), ly = dr_ldg(w + 1), lz = dr_ldg(w + 2);
+    const float4 hx = dr_ldg(w + 3), hy = dr_ldg(w + 4), hz = dr_ldg(w + 5), rf = dr_ldg(w + 6);
+    int c0 = dr_f2i(rf.x), c1 = dr_f2i(rf.y), c2 = dr_f2i(rf.z), c3 = dr_f2i(rf.w);
+    float k0 = c0 != DR_WIDE_EMPTY ? box_entry(lx.x, ly.x, lz.x, hx.x, hy.x, hz.x, o, inv, tmax) : -1.f;
+    float k1 = c1 != DR_WIDE_EMPTY ? box_entry(lx.y, ly.y, lz.y, hx.y, hy.y, hz.y, o, inv, tmax) : -1.f;
+    float k2 = c2 != DR_WIDE_EMPTY ? box_entry(lx.z, ly.z, lz.z, hx.z, hy.z, hz.z, o, inv, tmax) : -1.f;
+    float k3 = c3 != DR_WIDE_EMPTY ? box_entry(lx.w, ly.w, lz.w, hx.w, hy.w, hz.w, o, inv, tmax) : -1.f;
+    WideKids r;
+    r.n = (k0 >= 0.f) + (k1 >= 0.f) + (k2 >= 0.f) + (k3 >= 0.f);
+    // misses sort last
+    k0 = k0 >= 0.f ? k0 : DR_INF;
+    k1 = k1 >= 0.f ? k1 : DR_INF;
+    k2 = k2 >= 0.f ? k2 : DR_INF;
+    k3 = k3 >= 0.f ? k3 : DR_INF;
+    wide_swap(k0, c0, k1, c1);
+    wide_swap(k2, c2, k3, c3);
+    wide_swap(k0, c0, k2, c2);
+    wide_swap(k1, c1, k3, c3);
+    wide_swap(k1, c1, k2, c2);
+    r.c[0] = c0;
+    r.c[1] = c1;
+    r.c[2] = c2;
+    r.c[3] = c3;
+    return r;
+}
+// The next node of a wide walk after wide node children k: the nearest, with
+// the others stacked; false when the stack is empty too.
+DEV bool wide_next(const WideKids &k, int *stack, int &sp, int &node) {
+    if (k.n == 0) {
+        if (sp == 0) return false;
+        node = stack[--sp];
+        return true;
+    }
+    if (k.n > 3 && sp < DR_WIDE_STACK) stack[sp++] = k.c[3];
+    if (k.n > 2 && sp < DR_WIDE_STACK) stack[sp++] = k.c[2];
+    if (k.n > 1 && sp < DR_WIDE_STACK) stack[sp++] = k.c[1];
+    node = k.c[0];
+    return true;
+}
+
 // The walk of trace_before_bvh as a resumable state: begin() sets it up,
 // step() takes one node (a box pair or a leaf) and returns 0 while the walk
 // goes on, 1 when a triangle hits ahead of (ta, ida), 2 when none does.
@@ -321,7 +386,7 @@ struct BeforeWalk {
     float3 o, d, inv;
     float tnear, ta;
     int ida, sp, node;
-    int stack[DR_STACK];
+    int stack[DR_WIDE_STACK];
     DEV void begin(int root, float3 o_, float3 d_, float tnear_, float ta_, int ida_) {
         o = o_;
         d = d_;
@@ -332,7 +397,8 @@ struct BeforeWalk {
         sp = 0;
         node = root;
     }
-    DEV int step(const float4 *DR_RESTRICT nodes, const float4 *DR_RESTRICT tris) {
+    // wide (may be null): the 4-wide form of the tree, walked in its place
+    DEV int step(const float4 *DR_RESTRICT nodes, const float4 *DR_RESTRICT wide, const float4 *DR_RESTRICT tris) {
         if (node < 0) {
             const int leaf = ~node;
             float4 a = dr_ldg(tris + 3 * leaf), b = dr_ldg(tris + 3 * leaf + 1), c = dr_ldg(tris + 3 * leaf + 2);
@@ -342,6 +408,7 @@ struct BeforeWalk {
             node = stack[--sp];
             return 0;
         }
+        if (wide) return wide_next(wide_kids(wide + (size_t)DR_WIDE_F4 * node, o, inv, ta), stack, sp, node) ? 0 : 2;
         const float4 *n = nodes + 4 * node;
         float4 n0 = dr_ldg(n), n1 = dr_ldg(n + 1), n2 = dr_ldg(n + 2), n3 = dr_ldg(n + 3);
         float e0 = box_entry(n0.x, n0.y, n0.z, n0.w, n1.x, n1.y, o, inv, ta);
@@ -406,6 +473,43 @@ DEV_NOINLINE bool trace_before_bvh(const float4 *DR_RESTRICT nodes, const float4
     return false;
 }
 
+// ---------------------------------------------------------------------------
+// Walks of the 4-wide form of the LBVH (DevScene::bvh_wide), taken by the
+// warp-stepped occlusion walks (BeforeWalk) and by trace_before; closest and
+// any hits walk the binary nodes (see trace_closest).  Each step tests
+// a node's (up to) four children, the binary walk's two levels at once, in
+// the same boxes, and goes on with the nearest child entered, the others
+// stacked nearest on top.  The hits are those of the binary walks: a box is
+// culled only beyond the best hit so far, and the closest-hit rule (smallest
+// t, ties to the smaller triangle id) does not depend on the order.
+DEV_NOINLINE bool trace_before_wide(const float4 *DR_RESTRICT wide, const float4 *DR_RESTRICT tris, int root,
+                                    float3 o, float3 d, float tnear, float ta, int ida) {
+    const float3 inv = f3(safe_inv(d.x), safe_inv(d.y), safe_inv(d.z));
+    int stack[DR_WIDE_STACK];
+    int sp = 0;
+    int node = root;
+    while (true) {
+        if (node < 0) {
+            const int leaf = ~node;
+            float4 a = dr_ldg(tris + 3 * leaf), b = dr_ldg(tris + 3 * leaf + 1), c = dr_ldg(tris + 3 * leaf + 2);
+            float t;
+            if (hit_triangle(a, b, c, o, d, t) && t > tnear && (t < ta || (t == ta && dr_f2i(a.w) < ida)))
+                return true;
+            if (sp == 0) break;
+            node = stack[--sp];
+            continue;
+        }
+        if (!wide_next(wide_kids(wide + (size_t)DR_WIDE_F4 * node, o, inv, ta), stack, sp, node)) break;
+    }
+    return false;
+}
+
+// trace_before_bvh on the scene's tree (the 4-wide form where there is one)
+DEV bool trace_before(const DevScene &s, float3 o, float3 d, float tnear, float ta, int ida) {
+    if (s.bvh_wide) return trace_before_wide(s.bvh_wide, s.bvh_tris, s.bvh_root, o, d, tnear, ta, ida);
+    return trace_before_bvh(s.bvh_nodes, s.bvh_tris, s.bvh_root, o, d, tnear, ta, ida);
+}
+
 DEV_NOINLINE bool trace_any_linear(const float4 *DR_RESTRICT tris, int n, float3 o, float3 d, float tnear,
                                    float tfar) {
     for (int i = 0; i < n; i++) {
@@ -419,6 +523,8 @@ DEV_NOINLINE bool trace_any_linear(const float4 *DR_RESTRICT tris, int n, float3
 DEV bool trace_any(const DevScene &s, float3 o, float3 d, float tnear, float tfar) {
     if (s.num_tris == 0) return false;
     if (s.num_tris <= DR_LINEAR_TRIS) return trace_any_linear(s.bvh_tris, s.num_tris, o, d, tnear, tfar);
+    // binary, as closest hits (the 4-wide any-hit walk made the shading
+    // kernels' shadow rays 8 % slower)
     return trace_any_bvh(s.bvh_nodes, s.bvh_tris, s.bvh_root, o, d, tnear, tfar);
 }
 

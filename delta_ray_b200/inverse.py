@@ -41,10 +41,13 @@ class FitConfig:
     resolution: tuple = (128, 96)
     views: int = 4
     target_spp: int = 64
-    spp: int = 4                  # per view per step
-    max_bounces: int = 2
+    spp: int = 8                  # per view per step
+    # direct lighting: with more bounces the reference's edge estimator gives
+    # the heights a gradient along a common height shift that finite
+    # differences of the loss do not show, and the fit drifts along it
+    max_bounces: int = 1
     steps: int = 200
-    lr: float = 1e-2
+    lr: float = 3e-3
     height_noise: float = 0.05    # initial perturbation of the heights (std)
     roughness_noise: float = 0.1  # initial perturbation of the roughness (std)
     rmse_goal: float = 0.01
@@ -53,6 +56,10 @@ class FitConfig:
     # the sampling pdf held constant, lobe mixture weights for edge samples,
     # sub-pixel samples over the whole pixel); False: the reference's
     unbiased: bool = True
+    # weight of a smoothness prior on the heights: smooth * the sum over
+    # neighbouring grid vertices of their squared height difference, added to
+    # the image loss (0: none)
+    smooth: float = 0.0
     learned: bool = False         # train and use the learned edge proposal
     proposal_mix: float = 0.8
     seed: int = 0
@@ -194,6 +201,8 @@ class HeightfieldFit:
             for i in range(self.n_patch):
                 g_h.index_add_(0, self.index[i], parts["d_vertices"][i][:, 1])
                 g_r[i] += parts["d_roughness"][i].reshape(())
+        if cfg.smooth > 0.0:
+            g_h += cfg.smooth * self.smooth_grad()
         self.opt.zero_grad()
         self.heights.grad = g_h
         self.rough.grad = g_r
@@ -202,6 +211,20 @@ class HeightfieldFit:
             self.rough.clamp_(0.02, 1.0)
         self.step += 1
         return loss
+
+    def smooth_grad(self):
+        """Gradient of the sum over neighbouring grid vertices of their
+        squared height difference."""
+        g = self.cfg.grid
+        h = self.heights.detach().reshape(g, g)
+        out = torch.zeros_like(h)
+        dx = h[:, 1:] - h[:, :-1]
+        dz = h[1:, :] - h[:-1, :]
+        out[:, 1:] += 2 * dx
+        out[:, :-1] -= 2 * dx
+        out[1:, :] += 2 * dz
+        out[:-1, :] -= 2 * dz
+        return out.reshape(-1)
 
     # -- checkpoints ---------------------------------------------------------
     def state_dict(self):
