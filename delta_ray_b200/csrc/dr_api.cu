@@ -98,6 +98,7 @@ struct EdgeStats {
 struct BackwardQueues {
     DevBuf pt, items, item_w, item_dp, pt_last, pt_items, counts, survivors, hits, side_rad, tasks, tasks2;
     DevBuf walk_ctx, leafq;  // the level walk of the subtrees
+    DevBuf line_ctx;         // the points' line-sample setups
     long long cap_items = 0;     // grown on overflow, kept with the buffers
     double points_per_sample = 1;  // shading points per pixel sample the last overflow asked for
     EdgeStats stats;
@@ -1095,6 +1096,7 @@ void backward_on_queues(dr_scene *scene, const dr_render_desc *rd, const DevScen
     ws.task_rounds = scene->tune.task_rounds;
     ws.level_walk = scene->tune.depth_first ? 0 : 1;
     const bool split = view ? view->split_traversal : call_scene(scene, rd).split_traversal;
+    const bool lbvh = (view ? view->num_tris : call_scene(scene, rd).num_tris) > DR_LINEAR_TRIS;
     auto bind_items = [&]() {
         q.items.reserve(sizeof(int4) * cap_items);
         q.item_w.reserve(sizeof(float) * cap_items);
@@ -1121,6 +1123,10 @@ void backward_on_queues(dr_scene *scene, const dr_render_desc *rd, const DevScen
         if (split && ws.level_walk) {
             q.walk_ctx.reserve(sizeof(float4) * DR_CTX_F4 * cap_points);
             ws.walk_ctx = q.walk_ctx.as<float4>();
+        }
+        if (lbvh) {
+            q.line_ctx.reserve(sizeof(float4) * DR_LCTX_F4 * cap_points);
+            ws.line_ctx = q.line_ctx.as<float4>();
         }
         ws.cap_points = cap_points;
     };

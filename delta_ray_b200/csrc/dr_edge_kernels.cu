@@ -579,6 +579,32 @@ __device__ __forceinline__ void finish_item(const DevScene &s, const BackwardWor
 //
 // EXT: DR_FLAG_EDGE_LOBE_MIS or proposal training in use; GI: max_bounces > 1
 // (the shade calls of the two sides); the launcher picks the variant.
+// Each point's line-sample setup (line_setup: the point's edge draw, lobe
+// pick and LTC transforms), the same for all of its thousands of edges: the
+// line kernel reads it instead of setting it up per edge.  Layout, float4:
+// 0-2 minv and 3-5 m with the lobe's pick probability, the draw's u, ok and
+// the point's position in the last words of the two matrices' rows.
+__global__ void __launch_bounds__(128, 8) k_line_ctx(DevScene s, uint64_t seed, BackwardWorkspace ws) {
+    const long long n = min(min((long long)ws.counters->points, ws.cap_points), ws.pt_end);
+    for (long long p = ws.pt_begin + (long long)blockIdx.x * blockDim.x + threadIdx.x; p < n;
+         p += (long long)gridDim.x * blockDim.x) {
+        PointRecord pt;
+        pt.load(ws.pt + (size_t)p * DR_PT_WORDS);
+        Rng prng;
+        prng.init(point_seed(ws, pt.view, seed), kStreamEdgePoint, pt.sid, (uint32_t)pt.bounce);
+        const EdgeSample es = draw_edge(prng);
+        const LineSetup ls = line_setup(s, es, pt.wi, pt.tri, pt.surface());
+        const float *a = ls.minv.m, *b = ls.m.m;
+        float4 *o = ws.line_ctx + (size_t)p * DR_LCTX_F4;
+        o[0] = make_float4(a[0], a[1], a[2], a[3]);
+        o[1] = make_float4(a[4], a[5], a[6], a[7]);
+        o[2] = make_float4(a[8], b[0], b[1], b[2]);
+        o[3] = make_float4(b[3], b[4], b[5], b[6]);
+        o[4] = make_float4(b[7], b[8], ls.mpmf, es.u);
+        o[5] = make_float4(ls.ok ? 1.f : 0.f, pt.p.x, pt.p.y, pt.p.z);
+    }
+}
+
 template <bool EXT>
 __global__ void __launch_bounds__(128, 4) k_edge_line(DevScene s, uint64_t seed, BackwardWorkspace ws) {
     long long n = (long long)min(ws.counters->items, (unsigned long long)ws.cap_items);
@@ -590,10 +616,31 @@ __global__ void __launch_bounds__(128, 4) k_edge_line(DevScene s, uint64_t seed,
         bool ok = false;
         if (i < n) {
             int4 it = ws.items[i];
-            PointRecord pt;
-            pt.load(ws.pt + (size_t)it.x * DR_PT_WORDS);
             const int tree = it.y >> 30, ei = it.y & ((1 << 30) - 1);
-            ok = item_line<EXT>(s, pt, tree, ei, point_seed(ws, pt.view, seed), el);
+            PointRecord pt;
+            if (!EXT && ws.line_ctx) {
+                const float4 *c = ws.line_ctx + (size_t)it.x * DR_LCTX_F4;
+                const float4 c0 = c[0], c1 = c[1], c2 = c[2], c3 = c[3], c4 = c[4], c5 = c[5];
+                LineSetup ls;
+                const float ma[9] = {c0.x, c0.y, c0.z, c0.w, c1.x, c1.y, c1.z, c1.w, c2.x};
+                const float mb[9] = {c2.y, c2.z, c2.w, c3.x, c3.y, c3.z, c3.w, c4.x, c4.y};
+                for (int k = 0; k < 9; k++) {
+                    ls.minv.m[k] = ma[k];
+                    ls.m.m[k] = mb[k];
+                }
+                ls.mpmf = c4.z;
+                EdgeSample es;
+                es.u = c4.w;
+                es.bsdf_component = 0.f;  // the lobe pick is in the setup
+                pt.p = f3(c5.y, c5.z, c5.w);
+                const DevEdge &edge = tree ? s.nrm_edges[ei] : s.sil_edges[ei];
+                SurfacePoint unused;
+                ok = c5.x != 0.f && line_sample_from<false>(s, ls, es, edge, pt.p, unused, f3(0.f), el,
+                                                             (tree ? s.nrm_rec : s.sil_rec) + ei);
+            } else {
+                pt.load(ws.pt + (size_t)it.x * DR_PT_WORDS);
+                ok = item_line<EXT>(s, pt, tree, ei, point_seed(ws, pt.view, seed), el);
+            }
             if (ok) {
                 // the connectivity test's first part: a sample neither of whose
                 // rays hits one of the edge's faces is connected on no side
@@ -1005,6 +1052,11 @@ cudaError_t dr_launch_edge_eval(const DevScene &s, int W, int H, int spp, int B,
         timer->mark(st, "k_edge_line_rays");
         *launches -= 1;
     } else {
+        if (!ext && ws.line_ctx) {
+            k_line_ctx<<<grid, 128, 0, st>>>(s, seed, ws);
+            timer->mark(st, "k_line_ctx");
+            *launches += 1;
+        }
         if (ext) k_edge_line<true><<<grid, 128, 0, st>>>(s, seed, ws);
         else k_edge_line<false><<<grid, 128, 0, st>>>(s, seed, ws);
         timer->mark(st, "k_edge_line");
@@ -1098,7 +1150,7 @@ cudaError_t dr_preload_edge_kernels() {
         (const void *)k_edge_leaves<false>, (const void *)k_edge_leaves<true>,
         (const void *)k_edge_line_rays<false, false>, (const void *)k_edge_line_rays<false, true>,
         (const void *)k_edge_line_rays<true, false>, (const void *)k_edge_line_rays<true, true>,
-        (const void *)k_edge_line<false>, (const void *)k_edge_line<true>,
+        (const void *)k_edge_line<false>, (const void *)k_edge_line<true>, (const void *)k_line_ctx,
         (const void *)k_edge_connect, (const void *)k_edge_pairs<false>, (const void *)k_edge_pairs<true>,
         (const void *)k_edge_radiance,
         (const void *)k_edge_shade<false, false, false>, (const void *)k_edge_shade<false, true, false>,

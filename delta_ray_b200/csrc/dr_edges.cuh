@@ -853,38 +853,64 @@ struct EdgeLine {
     float q;          // density of l: the picked lobe's pmf times its line pdf (or the lobe mixture)
 };
 
-// rec (may be null): the edge's silhouette-test record, which gives the
-// answer of is_silhouette from one contiguous read.
-template <bool EXT = true>
-DEV bool edge_line_sample(const DevScene &s, const EdgeSample &es, const DevEdge &edge, float3 wi, int stri,
-                          const SurfacePoint &sp, EdgeLine &out, const EdgeRec *rec = nullptr) {
-    const bool none = false;
-    if (stri < 0) return none;
-    if (!(rec ? is_silhouette_rec(rec, sp.p) : is_silhouette(s, sp.p, edge))) return none;
-    float3 v0 = edge_v0(s, edge), v1 = edge_v1(s, edge);
-    if (abs_sum(v1 - v0) == 1e-10f) return none;
-    int mi = material_of_tri(s, stri);
+// What a line sample needs of its shading point and of the point's edge draw
+// (the same for every edge the point sampled): the picked lobe's transform
+// into its LTC space (minv) and back (m) and the lobe's pick probability; for
+// the lobe mixture weight also both lobes' pick probabilities, the shading
+// frame and the material.  ok false: the point samples no edge (no surface,
+// or a black material).
+struct LineSetup {
+    M3 minv, m, frame;
+    float mpmf, dpmf, spmf;
+    int mi;
+    bool ok;
+};
+DEV LineSetup line_setup(const DevScene &s, const EdgeSample &es, float3 wi, int stri, const SurfacePoint &sp) {
+    LineSetup ls;
+    ls.ok = false;
+    if (stri < 0) return ls;
+    const int mi = material_of_tri(s, stri);
     const DevMaterial &mat = s.mats[mi];
     float3 kd = get_kd(s, mat, sp.uv), ks = get_ks(s, mat, sp.uv);
     float dw = luminance(kd), sw = luminance(ks), ws = dw + sw;
-    if (ws <= 0.f) return none;
+    if (ws <= 0.f) return ls;
     float dpmf = dw / ws, spmf = sw / ws;
     float3 n = sp.f.n;
     float3 fx = normalize(wi - n * dot(wi, n));
     float3 fy = cross(n, fx);
     M3 frame = m3_rows(fx, fy, n);
-    M3 m, minv;
-    float mpmf;
     if (es.bsdf_component <= dpmf) {
-        minv = frame;
-        m = inverse(minv);
-        mpmf = dpmf;
+        ls.minv = frame;
+        ls.m = inverse(ls.minv);
+        ls.mpmf = dpmf;
     } else {
-        minv = mul(inverse(ltc_matrix(s, mi, sp, wi)), frame);
-        m = inverse(minv);
-        mpmf = spmf;
+        ls.minv = mul(inverse(ltc_matrix(s, mi, sp, wi)), frame);
+        ls.m = inverse(ls.minv);
+        ls.mpmf = spmf;
     }
-    float3 a = mul(minv, v0 - sp.p), b = mul(minv, v1 - sp.p);
+    ls.frame = frame;
+    ls.dpmf = dpmf;
+    ls.spmf = spmf;
+    ls.mi = mi;
+    ls.ok = true;
+    return ls;
+}
+
+// The line sample of one edge from its point's setup (delta_ray.cpp:88-187):
+// the edge clipped to the lobe's upper hemisphere in LTC space, the point on
+// it drawn by inverting the line integral's CDF (Newton steps guarded by
+// bisection), its density.  EXT adds the lobe mixture weight (sp and wi are
+// read only then).  rec (may be null): the edge's silhouette-test record,
+// which gives the answer of is_silhouette from one contiguous read.
+template <bool EXT = true>
+DEV bool line_sample_from(const DevScene &s, const LineSetup &ls, const EdgeSample &es, const DevEdge &edge, float3 p,
+                          const SurfacePoint &sp, float3 wi, EdgeLine &out, const EdgeRec *rec) {
+    const bool none = false;
+    if (!(rec ? is_silhouette_rec(rec, p) : is_silhouette(s, p, edge))) return none;
+    float3 v0 = edge_v0(s, edge), v1 = edge_v1(s, edge);
+    if (abs_sum(v1 - v0) == 1e-10f) return none;
+    const M3 &minv = ls.minv, &m = ls.m;
+    float3 a = mul(minv, v0 - p), b = mul(minv, v1 - p);
     if (a.z <= 0.f && b.z <= 0.f) return none;
     if (a.z < 0.f) a = (a * b.z - b * a.z) / (b.z - a.z);
     if (b.z < 0.f) b = (a * b.z - b * a.z) / (b.z - a.z);
@@ -925,17 +951,26 @@ DEV bool edge_line_sample(const DevScene &s, const EdgeSample &es, const DevEdge
     // DR_FLAG_EDGE_LOBE_MIS: the one-sample balance heuristic over the two
     // lobes, pmf_sel pdf_sel(l) + pmf_other pdf_other(l); the reference divides
     // by pmf_sel pdf_sel(l) alone
-    float q_mix = mpmf * pdf(l);
+    float q_mix = ls.mpmf * pdf(l);
     if (EXT && s.edge_lobe_mis) {
-        bool sel_diffuse = es.bsdf_component <= dpmf;
-        float opmf = sel_diffuse ? spmf : dpmf;
+        bool sel_diffuse = es.bsdf_component <= ls.dpmf;
+        float opmf = sel_diffuse ? ls.spmf : ls.dpmf;
         if (opmf > 0.f)
-            q_mix += opmf * other_lobe_density(s, mi, sp, wi, frame, sel_diffuse, v0, v1, sample_p, mul(m, wt));
+            q_mix += opmf * other_lobe_density(s, ls.mi, sp, wi, ls.frame, sel_diffuse, v0, v1, sample_p, mul(m, wt));
     }
     out.sample_p = sample_p;
     out.mwt = mul(m, wt);
     out.q = q_mix;
     return true;
+}
+
+// rec (may be null): the edge's silhouette-test record.
+template <bool EXT = true>
+DEV bool edge_line_sample(const DevScene &s, const EdgeSample &es, const DevEdge &edge, float3 wi, int stri,
+                          const SurfacePoint &sp, EdgeLine &out, const EdgeRec *rec = nullptr) {
+    const LineSetup ls = line_setup(s, es, wi, stri, sp);
+    if (!ls.ok) return false;
+    return line_sample_from<EXT>(s, ls, es, edge, sp.p, sp, wi, out, rec);
 }
 
 // The two rays of an edge sample, one on each side of the edge: their closest

@@ -171,6 +171,9 @@ struct BackwardWorkspace {
     // are `tasks` and `tasks2`, used in turn
     int level_walk = 1;
     float4 *walk_ctx;
+    // [cap_points][DR_LCTX_F4] each point's line-sample setup (k_line_ctx;
+    // null: k_edge_line sets it up per edge)
+    float4 *line_ctx;
     EdgeTask *leafq;
     long long cap_leaves;
     // per view of a batched multi-view call (null: the call's own settings);
@@ -238,6 +241,8 @@ cudaError_t dr_launch_backward_back(const DevScene &s, int W, int H, int spp, in
 
 // float4 of one point's walk context in BackwardWorkspace::walk_ctx.
 #define DR_CTX_F4 11
+// float4 of one point's line-sample setup in BackwardWorkspace::line_ctx.
+#define DR_LCTX_F4 6
 
 // Words of one packed secondary-point record in BackwardWorkspace::pt.
 #define DR_PT_FLOATS 24
