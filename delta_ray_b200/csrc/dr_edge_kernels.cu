@@ -255,46 +255,99 @@ __global__ void __launch_bounds__(128, DR_TASKS_BLOCKS) k_edge_tasks(DevScene s,
 // 7 the node draws' key (sample id, bounce) and the view, 8-10 the shading
 // frame (the proposal's direction bins).
 
+// The point's two walks start at the root of the tree its draw picks
+// (traverse_edges: edge_tree.cpp:685-725): the root tasks of the cone and the
+// all walk, with the root's bound and the tree's pick probability, go to the
+// first level's queue (`tasks`), and the point's edge count starts at 0.
 template <bool PROP>
 __global__ void __launch_bounds__(128, 8) k_walk_ctx(DevScene s, uint64_t seed, BackwardWorkspace ws) {
     const long long m = strided_points(ws);
-    for (long long k = (long long)blockIdx.x * blockDim.x + threadIdx.x; k < m;
-         k += (long long)gridDim.x * blockDim.x) {
-        const long long p = ws.pt_begin + k * ws.pt_stride;
-        PointRecord pt;
-        pt.load(ws.pt + (size_t)p * DR_PT_WORDS);
-        // as start_point_task / start_subtree
-        const SurfacePoint sp = pt.surface();
-        const DevMaterial &mt = s.mats[material_of_tri(s, pt.tri)];
-        const float dl = luminance(get_kd(s, mt, sp.uv)), sl = luminance(get_ks(s, mt, sp.uv));
-        const float rough = get_rough(s, mt, sp.uv);
-        const BoundCtx bc = bound_ctx(pt.wi, sp, dl, sl, rough, mt.model);
-        const ConeSpec cone = light_cone(s, pt.light, sp.p);
-        float learned = 0.f;
-        if constexpr (PROP) {
-            NodeRng r;
-            r.seed = point_seed(ws, pt.view, seed);
-            r.sid = pt.sid;
-            r.bounce = (uint32_t)pt.bounce;
-            learned = r.draw(1, DR_NODE_MIX_DRAW) < ws.proposal_alpha ? 1.f : 0.f;
+    const long long stride = (long long)gridDim.x * blockDim.x;
+    // warp-uniform loop: the root tasks' append is warp-aggregated
+    for (long long base = (long long)blockIdx.x * blockDim.x + (threadIdx.x & ~31); base < m; base += stride) {
+        const long long k = base + (threadIdx.x & 31);
+        EdgeTask root;
+        int nroot = 0;
+        if (k < m) {
+            const long long p = ws.pt_begin + k * ws.pt_stride;
+            PointRecord pt;
+            pt.load(ws.pt + (size_t)p * DR_PT_WORDS);
+            // as start_point_task / start_subtree
+            const SurfacePoint sp = pt.surface();
+            const DevMaterial &mt = s.mats[material_of_tri(s, pt.tri)];
+            const float dl = luminance(get_kd(s, mt, sp.uv)), sl = luminance(get_ks(s, mt, sp.uv));
+            const float rough = get_rough(s, mt, sp.uv);
+            const BoundCtx bc = bound_ctx(pt.wi, sp, dl, sl, rough, mt.model);
+            const uint64_t pseed = point_seed(ws, pt.view, seed);
+            if (dot(pt.wi, sp.f.n) >= 0.f && (s.num_nrm_nodes > 0 || s.num_sil_nodes > 0)) {
+                // the tree pick draws after the point's edge sample, as traverse_point
+                Rng prng;
+                prng.init(pseed, kStreamEdgePoint, pt.sid, (uint32_t)pt.bounce);
+                draw_edge(prng);
+                int tree;
+                float pmf = 1.f;
+                if (s.num_nrm_nodes == 0) {
+                    tree = 0;
+                } else if (s.num_sil_nodes == 0) {
+                    tree = 1;
+                } else {
+                    float ni = s.nrm_nodes[0].total_length, si = s.sil_nodes[0].total_length;
+                    float np = ni / (ni + si), spm = si / (ni + si);
+                    float u = prng.next();
+                    if (u < np) {
+                        tree = 1;
+                        pmf = np;
+                    } else {
+                        tree = 0;
+                        pmf = spm;
+                    }
+                }
+                root.point = (int)p;
+                root.code = tree << 29;
+                root.bb = bsdf_bound((tree ? s.nrm_nodes : s.sil_nodes)[0], bc);
+                root.cpmf = root.apmf = root.lpmf = pmf;
+                nroot = 2;
+            }
+            if (ws.pt_items) ws.pt_items[p] = 0;  // the leaves add the point's edges
+            const ConeSpec cone = light_cone(s, pt.light, sp.p);
+            float learned = 0.f;
+            if constexpr (PROP) {
+                NodeRng r;
+                r.seed = point_seed(ws, pt.view, seed);
+                r.sid = pt.sid;
+                r.bounce = (uint32_t)pt.bounce;
+                learned = r.draw(1, DR_NODE_MIX_DRAW) < ws.proposal_alpha ? 1.f : 0.f;
+            }
+            const bool lobe = sl > 0.f;  // the frame around wi is set only with a specular lobe
+            const Frame hf = lobe ? bc.hf : Frame{f3(0.f), f3(0.f), f3(0.f)};
+            const float3 ln = lobe ? bc.ln : f3(0.f);
+            float4 *o = ws.walk_ctx + (size_t)p * DR_CTX_F4;
+            o[0] = make_float4(bc.p.x, bc.p.y, bc.p.z, bc.n.x);
+            o[1] = make_float4(bc.n.y, bc.n.z, bc.dl, bc.sl);
+            o[2] = make_float4(hf.t.x, hf.t.y, hf.t.z, hf.b.x);
+            o[3] = make_float4(hf.b.y, hf.b.z, hf.n.x, hf.n.y);
+            o[4] = make_float4(hf.n.z, ln.x, ln.y, ln.z);
+            o[5] = make_float4(bc.rough, bc.expo, __int_as_float(bc.model), cone.cos_angle);
+            o[6] = make_float4(cone.d.x, cone.d.y, cone.d.z, learned);
+            o[7] = make_float4(__uint_as_float((uint32_t)pt.sid), __uint_as_float((uint32_t)(pt.sid >> 32)),
+                               __uint_as_float((uint32_t)pt.bounce), __int_as_float(pt.view));
+            if constexpr (PROP) {
+                o[8] = make_float4(sp.f.t.x, sp.f.t.y, sp.f.t.z, sp.f.b.x);
+                o[9] = make_float4(sp.f.b.y, sp.f.b.z, sp.f.n.x, sp.f.n.y);
+                o[10] = make_float4(sp.f.n.z, 0.f, 0.f, 0.f);
+            }
         }
-        const bool lobe = sl > 0.f;  // the frame around wi is set only with a specular lobe
-        const Frame hf = lobe ? bc.hf : Frame{f3(0.f), f3(0.f), f3(0.f)};
-        const float3 ln = lobe ? bc.ln : f3(0.f);
-        float4 *o = ws.walk_ctx + (size_t)p * DR_CTX_F4;
-        o[0] = make_float4(bc.p.x, bc.p.y, bc.p.z, bc.n.x);
-        o[1] = make_float4(bc.n.y, bc.n.z, bc.dl, bc.sl);
-        o[2] = make_float4(hf.t.x, hf.t.y, hf.t.z, hf.b.x);
-        o[3] = make_float4(hf.b.y, hf.b.z, hf.n.x, hf.n.y);
-        o[4] = make_float4(hf.n.z, ln.x, ln.y, ln.z);
-        o[5] = make_float4(bc.rough, bc.expo, __int_as_float(bc.model), cone.cos_angle);
-        o[6] = make_float4(cone.d.x, cone.d.y, cone.d.z, learned);
-        o[7] = make_float4(__uint_as_float((uint32_t)pt.sid), __uint_as_float((uint32_t)(pt.sid >> 32)),
-                           __uint_as_float((uint32_t)pt.bounce), __int_as_float(pt.view));
-        if constexpr (PROP) {
-            o[8] = make_float4(sp.f.t.x, sp.f.t.y, sp.f.t.z, sp.f.b.x);
-            o[9] = make_float4(sp.f.b.y, sp.f.b.z, sp.f.n.x, sp.f.n.y);
-            o[10] = make_float4(sp.f.n.z, 0.f, 0.f, 0.f);
+        __syncwarp();
+        // the cone walk's root (mode 0), then the all walk's (mode 1)
+        const unsigned long long slot = warp_reserve(&ws.counters->tasks, nroot);
+        for (int j = 0; j < nroot; j++) {
+            if (slot + j >= (unsigned long long)ws.cap_tasks) {  // room for two per point: never short
+                set_status(&ws.counters->status, DR_STATUS_STACK_OVERFLOW);
+                break;
+            }
+            EdgeTask t = root;
+            t.code |= j << 30;
+            ws.tasks[slot + j] = t;
         }
     }
 }
@@ -948,24 +1001,17 @@ cudaError_t dr_launch_edge_traverse(const DevScene &s, uint64_t seed, const Back
         cudaError_t e = cudaMemsetAsync(&ws.counters->tasks, 0, sizeof(unsigned long long), st);
         if (e == cudaSuccess) e = cudaMemsetAsync(&ws.counters->handed_total, 0, sizeof(unsigned long long), st);
         if (e != cudaSuccess) return e;
-        if (prop) k_edge_expand<true><<<stage_grid(num_sms), 128, 0, st>>>(s, seed, ws);
-        else k_edge_expand<false><<<stage_grid(num_sms), 128, 0, st>>>(s, seed, ws);
-        timer->mark(st, "k_edge_expand");
-        // the item count of the first stage (the roofline's work counts)
-        e = cudaMemcpyAsync(&ws.counters->items_expand, &ws.counters->items, sizeof(unsigned long long),
-                            cudaMemcpyDeviceToDevice, st);
-        if (e != cudaSuccess) return e;
         if (ws.level_walk && ws.walk_ctx && ws.leafq && ws.tasks2) {
-            // the subtrees level by level: ping-pong between the two queues,
-            // each level's leaves after it; the host looks every 8 levels
-            // whether a level queued nothing (a walk ends within its tree's
-            // depth, a few dozen levels)
+            // the walks level by level from the roots: ping-pong between the
+            // two queues, each level's leaves after it; the host looks every
+            // 8 levels whether a level queued nothing (a walk ends within its
+            // tree's depth, a few dozen levels)
             if (prop) k_walk_ctx<true><<<stage_grid(num_sms), 128, 0, st>>>(s, seed, ws);
             else k_walk_ctx<false><<<stage_grid(num_sms), 128, 0, st>>>(s, seed, ws);
             timer->mark(st, "k_walk_ctx");
             *launches += 1;
-            // the first stage's subtrees fill `tasks` from its start; the levels
-            // fill their queues by class
+            // the roots fill `tasks` from its start; the levels fill their
+            // queues by class
             const EdgeTask *in = ws.tasks;
             const unsigned long long *in_n = &ws.counters->tasks, *in_n1 = nullptr;
             for (int level = 0;; level++) {
@@ -999,6 +1045,13 @@ cudaError_t dr_launch_edge_traverse(const DevScene &s, uint64_t seed, const Back
             *launches += 1;
             return cudaGetLastError();
         }
+        if (prop) k_edge_expand<true><<<stage_grid(num_sms), 128, 0, st>>>(s, seed, ws);
+        else k_edge_expand<false><<<stage_grid(num_sms), 128, 0, st>>>(s, seed, ws);
+        timer->mark(st, "k_edge_expand");
+        // the item count of the first stage (the roofline's work counts)
+        e = cudaMemcpyAsync(&ws.counters->items_expand, &ws.counters->items, sizeof(unsigned long long),
+                            cudaMemcpyDeviceToDevice, st);
+        if (e != cudaSuccess) return e;
         // the subtrees in rounds: the first stage's, then those handed on
         // (ping-pong between the two queues); one round without a second queue
         const int rounds = ws.tasks2 ? ws.task_rounds : 1;
