@@ -19,6 +19,15 @@ namespace cg = cooperative_groups;
 #ifndef DR_CONNECT_BLOCKS
 #define DR_CONNECT_BLOCKS 8
 #endif
+// and of the line and side-radiance kernels (a sweep at the 640x480
+// heightfield: radiance 3 / 4 / 6 blocks 264 / 249 / 223 ms per step; line
+// 4 and 6 the same; connect 6 slower than 8, the level walk 6 and 8 the same)
+#ifndef DR_LINE_BLOCKS
+#define DR_LINE_BLOCKS 4
+#endif
+#ifndef DR_RADIANCE_BLOCKS
+#define DR_RADIANCE_BLOCKS 6
+#endif
 
 #define DR_ITEM_BUF 24
 // One thread per shading point in [pt_begin, pt_end).  A point's items collect
@@ -659,7 +668,7 @@ __global__ void __launch_bounds__(128, 8) k_line_ctx(DevScene s, uint64_t seed, 
 }
 
 template <bool EXT>
-__global__ void __launch_bounds__(128, 4) k_edge_line(DevScene s, uint64_t seed, BackwardWorkspace ws) {
+__global__ void __launch_bounds__(128, DR_LINE_BLOCKS) k_edge_line(DevScene s, uint64_t seed, BackwardWorkspace ws) {
     long long n = (long long)min(ws.counters->items, (unsigned long long)ws.cap_items);
     long long stride = (long long)gridDim.x * blockDim.x;
     // warp-uniform loop: the survivor append is warp-aggregated
@@ -862,7 +871,8 @@ __global__ void __launch_bounds__(128, 8) k_edge_line_rays(DevScene s, uint64_t 
 // multi-bounce shading) in a kernel of its own, [2 h] and [2 h + 1] of
 // ws.side_rad; k_edge_shade then runs without the path-tracing code, whose
 // size made the fused kernel wait on instruction fetches.
-__global__ void __launch_bounds__(128, 4) k_edge_radiance(DevScene s, int B, uint64_t seed, BackwardWorkspace ws) {
+__global__ void __launch_bounds__(128, DR_RADIANCE_BLOCKS) k_edge_radiance(DevScene s, int B, uint64_t seed,
+                                                                    BackwardWorkspace ws) {
     long long n = (long long)min(ws.counters->cands, (unsigned long long)ws.cap_items);
     for (long long h = (long long)blockIdx.x * blockDim.x + threadIdx.x; h < n; h += (long long)gridDim.x * blockDim.x) {
         int4 hr = ws.hits[h];
