@@ -318,8 +318,11 @@ DEV_NOINLINE bool trace_any_bvh(const float4 *DR_RESTRICT nodes, const float4 *D
 }
 
 // Steps of the walks over the LBVH's 4-wide form (see trace_before_wide);
-// their stack holds up to three children per 4-wide level.
+// their stack holds up to three children per 4-wide level, and a path of at
+// most 61 binary levels crosses at most 31 of those: 93 entries always
+// suffice, so the push guards are never taken.
 #define DR_WIDE_STACK 96
+static_assert(DR_WIDE_STACK >= 3 * ((30 + 31 + 1) / 2), "4-wide traversal stack shorter than its depth bound");
 
 // The children of wide node w whose boxes the ray enters before tmax, nearest
 // first: n of them in c[0..n).
