@@ -434,14 +434,15 @@ __device__ __noinline__ void walk_here(const DevScene &s, uint64_t seed, const B
     atomicAdd(&ws.counters->spilled, 1ull);
 }
 
-// The class of a node in the level queues: 1 for the nodes whose children's
-// bounds may come filtered (the all walk's split nodes off the cone walk's
-// path: no cone tests, no exact pow unless a filtered bound is too close to a
-// threshold), 0 for the others (exact bounds; cone tests on the cone walk's
-// path; a draw where the node does not split).  Each class fills its own half
-// of a queue, so that a warp's lanes mostly run the same code.
-template <bool PROP> __device__ __forceinline__ int node_class(int mode, const EdgeItem<PROP> &c, bool split) {
-    return (mode == 1 && c.cpmf == 0.f && split) ? 1 : 0;
+// The class of a node in the level queues: 0 for nodes whose decision takes
+// the exact bounds and the cone tests (the cone walk's, and the all walk's on
+// the cone walk's path), 1 for the all walk's others (no cone tests; filtered
+// bounds where they split).  Each class fills its own half of a queue, so that
+// a warp's lanes mostly run the same code.  (Splitting instead by whether the
+// node's children take filtered bounds was slower: 490-520 -> 586 ms per step
+// at the 640x480 heightfield.)
+template <bool PROP> __device__ __forceinline__ int node_class(int mode, const EdgeItem<PROP> &c) {
+    return (mode == 0 || c.cpmf != 0.f) ? 0 : 1;
 }
 
 #ifndef DR_LEVEL_BLOCKS
@@ -488,7 +489,7 @@ __global__ void __launch_bounds__(128, DR_LEVEL_BLOCKS) k_edge_level(DevScene s,
                             if (c.l_leaf) {
                                 lf[nl++] = child_task<PROP>(t.point, hi, c.left);
                             } else {
-                                kc[nk] = node_class<PROP>(mode, c.left, c.l_split);
+                                kc[nk] = node_class<PROP>(mode, c.left);
                                 kid[nk++] = child_task<PROP>(t.point, hi, c.left);
                             }
                         }
@@ -496,7 +497,7 @@ __global__ void __launch_bounds__(128, DR_LEVEL_BLOCKS) k_edge_level(DevScene s,
                             if (c.r_leaf) {
                                 lf[nl++] = child_task<PROP>(t.point, hi, c.right);
                             } else {
-                                kc[nk] = node_class<PROP>(mode, c.right, c.r_split);
+                                kc[nk] = node_class<PROP>(mode, c.right);
                                 kid[nk++] = child_task<PROP>(t.point, hi, c.right);
                             }
                         }

@@ -446,13 +446,11 @@ template <bool PROP> HD EdgeItem<PROP> edge_item(int node, float bb, float c, fl
 // proportion to the importances.  Returns 0 when neither is walked (both
 // importances vanish), 1 for a split, 2 for a draw; push_l / push_r say which
 // children are walked (a child whose silhouette test fails or whose bound is
-// 0 is not), l_leaf / r_leaf whether they are leaves, l_split / r_split
-// whether they split in the all walk (their bound above 1, or p inside their
-// box).  Shared by the depth-first walk (EdgeWalk) and the level-by-level
-// walk (k_edge_level).
+// 0 is not), l_leaf / r_leaf whether they are leaves.  Shared by the
+// depth-first walk (EdgeWalk) and the level-by-level walk (k_edge_level).
 template <bool PROP> struct ChildPick {
     EdgeItem<PROP> left, right;
-    bool push_l, push_r, l_leaf, r_leaf, l_split, r_split;
+    bool push_l, push_r, l_leaf, r_leaf;
 };
 template <bool PROP>
 DEV int node_children(const DevEdgeNode *nodes, const BoundCtx &bc, const ConeSpec &cone, const NodeRng &rng,
@@ -531,8 +529,6 @@ DEV int node_children(const DevEdgeNode *nodes, const BoundCtx &bc, const ConeSp
     bool split = CONE ? cone_split : all_split;
     c.l_leaf = L.nprims > 0;
     c.r_leaf = R.nprims > 0;
-    c.l_split = lbb > 1.f || node_inside(L, p);
-    c.r_split = rbb > 1.f || node_inside(R, p);
     if (split) {
         // a child of bound 0 would only be taken off the stack and skipped,
         // so it is not pushed
