@@ -20,8 +20,9 @@ namespace cg = cooperative_groups;
 #define DR_CONNECT_BLOCKS 8
 #endif
 // and of the line and side-radiance kernels (a sweep at the 640x480
-// heightfield: radiance 3 / 4 / 6 blocks 264 / 249 / 223 ms per step; line
-// 4 and 6 the same; connect 6 slower than 8, the level walk 6 and 8 the same)
+// heightfield: radiance 3 / 4 / 6 / 8 blocks 264 / 249 / 223 / 234 ms per
+// step; line 4 and 6 the same; connect 6 / 8 / 10: 458 / 436 / 516; the
+// level walk 6 and 8 the same)
 #ifndef DR_LINE_BLOCKS
 #define DR_LINE_BLOCKS 4
 #endif
