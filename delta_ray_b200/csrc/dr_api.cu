@@ -570,9 +570,10 @@ void check_render_desc(const dr_scene *sc, const dr_render_desc *rd) {
 // the item, its weight, its dp and its slot in the survivor queue of the
 // evaluation wavefront).  Edge stages with more items stream.
 constexpr long long kMaxQueueItems = (8ll << 30) / 64;
-// the first call's probe of the edge counts (run_backward): every 16th point,
-// in calls of at least 2^20 pixel samples
-constexpr long long kProbeStride = 16, kProbeMinSamples = 1ll << 20;
+// the first call's probe of the edge counts (run_backward): every 32nd point,
+// in calls of at least 2^20 pixel samples (about 30 probed points per bucket
+// of the chunk plan at 640x480, 4 spp; the forecast's margin covers the rest)
+constexpr long long kProbeStride = 32, kProbeMinSamples = 1ll << 20;
 std::atomic<long long> g_item_queue_limit{0};  // dr_set_item_queue_limit (0: kMaxQueueItems)
 long long max_queue_items() {
     long long l = g_item_queue_limit.load();

@@ -72,7 +72,7 @@ def test_streamed_edge_stage_matches_one_pass(name):
 
 def test_first_call_probe_forecasts_the_edge_counts():
     """A scene's first call of 2^20 or more pixel samples has no edge counts
-    to plan its edge stage from: it walks every 16th shading point first and
+    to plan its edge stage from: it walks every 32nd shading point first and
     forecasts the others' counts from theirs.  With room for the forecast it
     then walks every point in one pass; without (a bounded item queue) it
     streams chunks planned from the forecast, cutting those that overflow.
