@@ -162,56 +162,11 @@ cudaError_t dr_refit_lbvh(const float *vtx, const int4 *tri, int n, float4 *node
 
 size_t dr_lbvh_scratch_bytes(int n) { return lbvh_layout(nullptr, n).used; }
 
-// One 4-wide node per internal node p: p's two children, each internal child
-// replaced by its own two children (with the boxes its node holds for them).
-// A walk from the root only ever reads the wide nodes of the root and of
-// nodes two levels apart, so every binary node is tested in the same boxes
-// as in the binary walk.
+// One 4-wide node per internal node (widen_node).
 __global__ void k_bvh_widen(const float4 *nodes, int n_internal, float4 *wide) {
     const int p = blockIdx.x * blockDim.x + threadIdx.x;
     if (p >= n_internal) return;
-    float lo[3][4], hi[3][4];
-    int ref[4];
-    int k = 0;
-    const float4 *np = nodes + 4 * p;
-    const float4 a0 = np[0], a1 = np[1], a2 = np[2], a3 = np[3];
-    const float pb[2][6] = {{a0.x, a0.y, a0.z, a0.w, a1.x, a1.y}, {a1.z, a1.w, a2.x, a2.y, a2.z, a2.w}};
-    const int pc[2] = {dr_f2i(a3.x), dr_f2i(a3.y)};
-    for (int j = 0; j < 2; j++) {
-        if (pc[j] < 0) {  // a leaf child stands for itself
-            for (int ax = 0; ax < 3; ax++) {
-                lo[ax][k] = pb[j][ax];
-                hi[ax][k] = pb[j][3 + ax];
-            }
-            ref[k++] = pc[j];
-            continue;
-        }
-        const float4 *cp = nodes + 4 * pc[j];
-        const float4 b0 = cp[0], b1 = cp[1], b2 = cp[2], b3 = cp[3];
-        const float cb[2][6] = {{b0.x, b0.y, b0.z, b0.w, b1.x, b1.y}, {b1.z, b1.w, b2.x, b2.y, b2.z, b2.w}};
-        const int cc[2] = {dr_f2i(b3.x), dr_f2i(b3.y)};
-        for (int g = 0; g < 2; g++) {
-            for (int ax = 0; ax < 3; ax++) {
-                lo[ax][k] = cb[g][ax];
-                hi[ax][k] = cb[g][3 + ax];
-            }
-            ref[k++] = cc[g];
-        }
-    }
-    for (; k < 4; k++) {
-        for (int ax = 0; ax < 3; ax++) {
-            lo[ax][k] = 1.f;  // an empty box; the walks skip the slot by its id
-            hi[ax][k] = 0.f;
-        }
-        ref[k] = DR_WIDE_EMPTY;
-    }
-    float4 *w = wide + (size_t)DR_WIDE_F4 * p;
-    for (int ax = 0; ax < 3; ax++) {
-        w[ax] = make_float4(lo[ax][0], lo[ax][1], lo[ax][2], lo[ax][3]);
-        w[3 + ax] = make_float4(hi[ax][0], hi[ax][1], hi[ax][2], hi[ax][3]);
-    }
-    w[6] = make_float4(dr_i2f(ref[0]), dr_i2f(ref[1]), dr_i2f(ref[2]), dr_i2f(ref[3]));
-    w[7] = make_float4(0.f, 0.f, 0.f, 0.f);
+    widen_node(nodes, p, wide + (size_t)DR_WIDE_F4 * p);
 }
 
 cudaError_t dr_widen_lbvh(const float4 *nodes, int n, float4 *wide, cudaStream_t st, int *launches) {

@@ -317,6 +317,64 @@ DEV_NOINLINE bool trace_any_bvh(const float4 *DR_RESTRICT nodes, const float4 *D
     return false;
 }
 
+// The 4-wide node of internal node p (DevScene::bvh_wide, DR_WIDE_F4 float4 at
+// w): p's two children, each internal child replaced by its own two children
+// with the boxes its node holds for them.  A walk from the root only reads
+// the wide nodes of the root and of nodes two levels apart, so every binary
+// node is tested in the same boxes as in the binary walk.
+HD void widen_node(const float4 *nodes, int p, float4 *w) {
+    float lo[3][4], hi[3][4];
+    int ref[4];
+    int k = 0;
+    const float4 *np = nodes + 4 * p;
+    const float4 a0 = np[0], a1 = np[1], a2 = np[2], a3 = np[3];
+    const float pb[2][6] = {{a0.x, a0.y, a0.z, a0.w, a1.x, a1.y}, {a1.z, a1.w, a2.x, a2.y, a2.z, a2.w}};
+    const int pc[2] = {dr_f2i(a3.x), dr_f2i(a3.y)};
+    for (int j = 0; j < 2; j++) {
+        if (pc[j] < 0) {  // a leaf child stands for itself
+            for (int ax = 0; ax < 3; ax++) {
+                lo[ax][k] = pb[j][ax];
+                hi[ax][k] = pb[j][3 + ax];
+            }
+            ref[k++] = pc[j];
+            continue;
+        }
+        const float4 *cp = nodes + 4 * pc[j];
+        const float4 b0 = cp[0], b1 = cp[1], b2 = cp[2], b3 = cp[3];
+        const float cb[2][6] = {{b0.x, b0.y, b0.z, b0.w, b1.x, b1.y}, {b1.z, b1.w, b2.x, b2.y, b2.z, b2.w}};
+        const int cc[2] = {dr_f2i(b3.x), dr_f2i(b3.y)};
+        for (int g = 0; g < 2; g++) {
+            for (int ax = 0; ax < 3; ax++) {
+                lo[ax][k] = cb[g][ax];
+                hi[ax][k] = cb[g][3 + ax];
+            }
+            ref[k++] = cc[g];
+        }
+    }
+    for (; k < 4; k++) {
+        for (int ax = 0; ax < 3; ax++) {
+            lo[ax][k] = 1.f;  // an empty box; the walks skip the slot by its id
+            hi[ax][k] = 0.f;
+        }
+        ref[k] = DR_WIDE_EMPTY;
+    }
+    for (int ax = 0; ax < 3; ax++) {
+        w[ax].x = lo[ax][0];
+        w[ax].y = lo[ax][1];
+        w[ax].z = lo[ax][2];
+        w[ax].w = lo[ax][3];
+        w[3 + ax].x = hi[ax][0];
+        w[3 + ax].y = hi[ax][1];
+        w[3 + ax].z = hi[ax][2];
+        w[3 + ax].w = hi[ax][3];
+    }
+    w[6].x = dr_i2f(ref[0]);
+    w[6].y = dr_i2f(ref[1]);
+    w[6].z = dr_i2f(ref[2]);
+    w[6].w = dr_i2f(ref[3]);
+    w[7].x = w[7].y = w[7].z = w[7].w = 0.f;
+}
+
 // Steps of the walks over the LBVH's 4-wide form (see trace_before_wide);
 // their stack holds up to three children per 4-wide level, and a path of at
 // most 61 binary levels crosses at most 31 of those: 93 entries always

@@ -47,6 +47,8 @@ def load():
         L.hh_scene_edges.restype = C.c_longlong
         L.hh_silhouette.argtypes = [C.c_void_p] * 5 + [C.c_longlong, C.c_void_p]
         L.hh_trace_pairs.argtypes = [C.POINTER(_abi.dr_scene_desc), C.c_void_p, C.c_int, C.c_void_p]
+        L.hh_trace_before.argtypes = [C.POINTER(_abi.dr_scene_desc), C.c_void_p, C.c_void_p, C.c_void_p, C.c_int,
+                                      C.c_void_p]
         _lib = L
     return _lib
 
@@ -135,6 +137,22 @@ def trace_pairs(wl, rays):
     rays = np.ascontiguousarray(rays, np.float32)
     out = np.zeros((rays.shape[0], 4), np.int32)
     L.hh_trace_pairs(C.byref(sd.desc), rays.ctypes.data, rays.shape[0], out.ctypes.data)
+    return out
+
+
+def trace_before(wl, rays, ta, ida):
+    """Whether a triangle hits ahead of (ta, ida) for rays [n, 6], through the
+    binary LBVH walk and through the 4-wide walk: [n, 2] int."""
+    from delta_ray_b200 import _abi
+    L = load()
+    cam, mats, shps, lts = _abi.scene_dicts(wl.camera, wl.materials, wl.shapes, wl.lights)
+    sd = _abi.SceneDesc.from_scene(cam, mats, shps, lts, torch.device("cpu"))
+    rays = np.ascontiguousarray(rays, np.float32)
+    ta = np.ascontiguousarray(ta, np.float32)
+    ida = np.ascontiguousarray(ida, np.int32)
+    out = np.zeros((rays.shape[0], 2), np.int32)
+    L.hh_trace_before(C.byref(sd.desc), rays.ctypes.data, ta.ctypes.data, ida.ctypes.data, rays.shape[0],
+                      out.ctypes.data)
     return out
 
 

@@ -388,6 +388,23 @@ void hh_trace_pairs(const dr_scene_desc *desc, const float *rays, int n, int *ou
     }
 }
 
+// The occlusion test of the ray stage (a triangle hitting ahead of (ta, ida))
+// through the binary walk and through the 4-wide walk, for rays [n][6] with
+// their ta[n], ida[n]: out [n][2].
+void hh_trace_before(const dr_scene_desc *desc, const float *rays, const float *ta, const int *ida, int n, int *out) {
+    HostSceneBundle b;
+    make_scene(desc, b);
+    const int ni = b.ds.num_tris - 1;
+    std::vector<float4> wide((size_t)DR_WIDE_F4 * std::max(ni, 1));
+    for (int p = 0; p < ni; p++) widen_node(b.ds.bvh_nodes, p, wide.data() + (size_t)DR_WIDE_F4 * p);
+    for (int i = 0; i < n; i++) {
+        const float *r = rays + 6 * i;
+        const float3 o = f3(r[0], r[1], r[2]), d = f3(r[3], r[4], r[5]);
+        out[2 * i] = trace_before_bvh(b.ds.bvh_nodes, b.ds.bvh_tris, b.ds.bvh_root, o, d, 1e-3f, ta[i], ida[i]);
+        out[2 * i + 1] = trace_before_wide(wide.data(), b.ds.bvh_tris, b.ds.bvh_root, o, d, 1e-3f, ta[i], ida[i]);
+    }
+}
+
 // The reproducible transcendental functions (dr_math.h) on n inputs.
 // The silhouette test of edge-tree nodes, filtered and unfiltered, for n
 // (node, point) pairs: node k from lo[3k..], hi[3k..], axis[3k..], angle[k];
